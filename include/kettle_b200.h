@@ -1,0 +1,285 @@
+/*
+ * kettle_b200.h — C-ABI of the B200 circuit-propagation engine.
+ *
+ * Plain C, no torch or CUDA types in any signature: states are opaque handles,
+ * gates and Pauli strings are flat records, all sizes are explicit.  Every
+ * function returns an int32 status (KT_OK = 0, negative on error); the message
+ * of the most recent error on the calling thread is returned by kt_last_error().
+ * Device code never traps: failures surface as status codes.
+ *
+ * The entry points replace these reference interfaces (paths relative to the
+ * kettle project root):
+ *   kt_sv_apply          ket::simulate(const QuantumCircuit&, Statevector&, std::optional<int>)
+ *                        include/kettle/simulation/simulate.hpp:41, loop at
+ *                        source/kettle_internal/simulation/simulate.cpp:265-521
+ *   kt_dm_apply          ket::simulate(const QuantumCircuit&, DensityMatrix&, std::optional<int>)
+ *                        include/kettle/simulation/simulate_density_matrix.hpp:46
+ *   kt_sv_expect         ket::expectation_value(const PauliOperator&, const Statevector&)
+ *                        include/kettle/operator/pauli/pauli_operator.hpp:82-84,
+ *                        source/kettle_internal/operator/pauli/pauli_operator.cpp:76-103
+ *   kt_sv_probabilities  ket::calculate_probabilities_raw(const Statevector&, const QuantumNoise*)
+ *                        include/kettle/calculations/probabilities.hpp:43
+ *   kt_sv_sample         the sampler behind ket::perform_measurements_as_counts / _as_memory
+ *                        include/kettle/calculations/measurements.hpp:41-97,
+ *                        source/kettle_internal/calculations/measurements.cpp:235-311
+ *   kt_sv_measure_probs / kt_sv_collapse
+ *                        the M gate, source/kettle_internal/simulation/measure.hpp:34-55,
+ *                        source/kettle_internal/simulation/measure.cpp:22-68
+ *   kt_pairs_single / kt_pairs_double
+ *                        ket::internal::SingleQubitGatePairGenerator / DoubleQubitGatePairGenerator
+ *                        source/kettle_internal/simulation/gate_pair_generator.hpp:25-160
+ *   kt_sv_inner          ket::inner_product, source/kettle_internal/state/state.cpp:159-172
+ *   kt_adjoint_*         no reference counterpart (new capability; the consumer is the
+ *                        VQE cost function of example/algorithms/vqe_basic.cpp:61-96)
+ *   kt_batch_*           no reference counterpart (new capability)
+ */
+#ifndef KETTLE_B200_H
+#define KETTLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define KT_OK 0
+#define KT_ERR_INVALID (-1)      /* bad argument (qubit out of range, null pointer, ...) */
+#define KT_ERR_CUDA (-2)         /* a CUDA runtime call failed                          */
+#define KT_ERR_NOMEM (-3)        /* device allocation failed                            */
+#define KT_ERR_QUBITS (-4)       /* circuit / state qubit-count mismatch                */
+#define KT_ERR_TIMEOUT (-5)      /* a bounded device wait ran out                       */
+#define KT_ERR_UNSUPPORTED (-6)  /* valid request this build does not implement         */
+
+/* ---- amplitude storage types ----------------------------------------- */
+#define KT_C128 0 /* complex<double>: interleaved (re, im) doubles */
+#define KT_C64 1  /* complex<float>:  interleaved (re, im) floats; reductions stay FP64 */
+
+/* ---- gate record -------------------------------------------------------
+ * `op` is the numeric value of ket::Gate (include/kettle/gates/primitive_gate.hpp:19-52):
+ *   H=0 X=1 Y=2 Z=3 S=4 SDAG=5 T=6 TDAG=7 SX=8 SXDAG=9 RX=10 RY=11 RZ=12 P=13
+ *   CH=14 CX=15 CY=16 CZ=17 CS=18 CSDAG=19 CT=20 CTDAG=21 CSX=22 CSXDAG=23
+ *   CRX=24 CRY=25 CRZ=26 CP=27 U=28 CU=29 M=30
+ * It carries what ket::GateInfo carries (primitive_gate.hpp:71-79): target
+ * (GateInfo::arg0 for one-target gates, arg1 for controlled gates), control,
+ * angle (arg2), and the 2x2 unitary for U/CU (row-major, interleaved re/im:
+ * u = {m00.re, m00.im, m01.re, m01.im, m10.re, m10.im, m11.re, m11.im}).
+ * For M, `control` holds the classical bit index.
+ * `param` >= 0 takes the angle from params[param] instead of `angle`; that is
+ * how a circuit's ParameterID-bound gates are evaluated once per call
+ * (source/kettle_internal/parameter/parameter_expression.cpp:84-99). */
+#define KT_OP_H 0
+#define KT_OP_X 1
+#define KT_OP_Y 2
+#define KT_OP_Z 3
+#define KT_OP_S 4
+#define KT_OP_SDAG 5
+#define KT_OP_T 6
+#define KT_OP_TDAG 7
+#define KT_OP_SX 8
+#define KT_OP_SXDAG 9
+#define KT_OP_RX 10
+#define KT_OP_RY 11
+#define KT_OP_RZ 12
+#define KT_OP_P 13
+#define KT_OP_CH 14
+#define KT_OP_CX 15
+#define KT_OP_CY 16
+#define KT_OP_CZ 17
+#define KT_OP_CS 18
+#define KT_OP_CSDAG 19
+#define KT_OP_CT 20
+#define KT_OP_CTDAG 21
+#define KT_OP_CSX 22
+#define KT_OP_CSXDAG 23
+#define KT_OP_CRX 24
+#define KT_OP_CRY 25
+#define KT_OP_CRZ 26
+#define KT_OP_CP 27
+#define KT_OP_U 28
+#define KT_OP_CU 29
+#define KT_OP_M 30
+
+typedef struct kt_gate {
+    uint8_t op;
+    uint8_t reserved0;
+    uint16_t reserved1;
+    uint32_t target;
+    uint32_t control;
+    int32_t param;
+    double angle;
+    double u[8];
+} kt_gate; /* 88 bytes */
+
+/* ---- Pauli string record -----------------------------------------------
+ * ket::SparsePauliString (include/kettle/operator/pauli/sparse_pauli_string.hpp:42-125)
+ * as bit masks: bit q of x_mask is set where the term is X or Y, bit q of
+ * z_mask where it is Z or Y.  `phase` is ket::PauliPhase (PLUS_ONE=0,
+ * PLUS_EYE=1, MINUS_ONE=2, MINUS_EYE=3; PAULI_PHASE_MAP at :32-37).
+ * Applied to a basis state: P|i> = i^{#Y} (-1)^{popcount(i & z_mask)} |i ^ x_mask>,
+ * with Y = [[0,-i],[i,0]] as in apply_y_gate (simulation/operations.cpp:32-44). */
+typedef struct kt_pauli {
+    uint64_t x_mask;
+    uint64_t z_mask;
+    int32_t phase;
+    int32_t reserved;
+} kt_pauli;
+
+/* ---- errors / device ---------------------------------------------------- */
+const char* kt_last_error(void);
+int32_t kt_version(void);
+int32_t kt_device_synchronize(void);
+
+/* Draw n canonical uniforms with std::mt19937(seed) and
+ * std::generate_canonical<double, 53> — exactly the draws the reference's
+ * ProbabilitySampler_ makes (measurements.cpp:288-311, prng.cpp:9-19) before
+ * scaling them by its distribution bound.  Host-only helper. */
+int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
+
+/* ---- statevector handle --------------------------------------------------
+ * A statevector of n qubits lives on the current CUDA device as 2^n amplitudes,
+ * little-endian (bit q of the index = qubit q), contiguous.  kt_sv_create
+ * allocates it and sets |0...0> (Statevector(n), state.cpp:21-28). */
+typedef struct kt_sv_s* kt_sv;
+
+int32_t kt_sv_create(int32_t n_qubits, int32_t dtype, kt_sv* out);
+/* Non-owning handle over caller memory (e.g. a torch tensor's data pointer). */
+int32_t kt_sv_wrap(void* device_amps, int32_t n_qubits, int32_t dtype, kt_sv* out);
+int32_t kt_sv_destroy(kt_sv sv);
+/* All work of this handle is ordered on `stream` (a cudaStream_t; NULL = legacy default). */
+int32_t kt_sv_set_stream(kt_sv sv, void* stream);
+int32_t kt_sv_info(kt_sv sv, int32_t* n_qubits, int32_t* dtype, void** device_amps);
+/* Set |index> (Statevector(std::string), state.cpp:55-66). */
+int32_t kt_sv_set_basis(kt_sv sv, uint64_t index);
+/* Host amplitudes are always complex128, interleaved; converted on the device for KT_C64. */
+int32_t kt_sv_upload(kt_sv sv, const double* host_amps, uint64_t n_amps);
+int32_t kt_sv_download(kt_sv sv, double* host_amps, uint64_t n_amps);
+int32_t kt_sv_copy(kt_sv dst, kt_sv src);
+
+/* Apply a gate stream.  mode: 0 = fused (default), 1 = one sweep per gate.
+ * M gates are rejected here (they need a host coin; use kt_sv_measure_probs
+ * and kt_sv_collapse).  Returns KT_ERR_INVALID for a qubit outside [0, n). */
+#define KT_APPLY_FUSED 0
+#define KT_APPLY_PER_GATE 1
+int32_t kt_sv_apply(kt_sv sv, const kt_gate* gates, int64_t n_gates,
+                    const double* params, int64_t n_params, int32_t mode);
+
+/* What the most recent kt_sv_apply / kt_dm_apply on this handle launched:
+ * kernel launches and the algorithmic HBM bytes they move (read + write of
+ * the amplitudes each launch must touch).  Instrumentation; no reference
+ * counterpart. */
+int32_t kt_sv_apply_stats(kt_sv sv, int64_t* launches, double* alg_bytes);
+
+/* <psi| sum_k c_k P_k |psi>; coeffs interleaved complex128 (nullable = all 1).
+ * out_terms (nullable): per-string phase*<P_k> (complex, interleaved);
+ * out_total: sum_k c_k phase_k <P_k>, complex, as the reference returns. */
+int32_t kt_sv_expect(kt_sv sv, const kt_pauli* strings, int64_t n_strings,
+                     const double* coeffs, double* out_terms, double* out_total);
+
+/* |a_i|^2 with the reference's rounding (no FMA), then optional per-qubit
+ * readout noise applied qubit by qubit (probabilities.cpp:49-71,110-124).
+ * noise: n doubles in [0,1] or NULL.  host_out: 2^n doubles. */
+int32_t kt_sv_probabilities(kt_sv sv, const double* noise, double* host_out);
+
+/* Inverse-CDF sampling.  canonicals[s] in [0,1) are scaled by the reference's
+ * bound (cdf_last - offset, measurements.cpp:235-256,288-295) and searched
+ * with lower_bound semantics.  The result equals the reference's sequential
+ * std::partial_sum CDF bit for bit: the device certifies each draw against a
+ * rigorous rounding bound and recomputes with an exact sequential scan when
+ * a draw cannot be certified (mode 0); mode 1 always uses the sequential scan.
+ * n_rescanned (nullable) reports whether the sequential scan ran (0/1). */
+int32_t kt_sv_sample(kt_sv sv, const double* noise, const double* canonicals,
+                     int64_t n_shots, uint64_t* out_indices, int32_t mode,
+                     int32_t* n_rescanned);
+
+/* M gate, split at the host coin: P(0), P(1) of `qubit`; then keep `outcome`
+ * and scale by `scale` (the reference uses sqrt(1/P(outcome))). */
+int32_t kt_sv_measure_probs(kt_sv sv, uint32_t qubit, double* p0, double* p1);
+int32_t kt_sv_collapse(kt_sv sv, uint32_t qubit, int32_t outcome, double scale);
+
+int32_t kt_sv_norm_sq(kt_sv sv, double* out);
+int32_t kt_sv_inner(kt_sv bra, kt_sv ket, double* out_re_im);
+
+/* ---- pair enumeration (reference order, bit-exact) --------------------------
+ * Pairs k0 .. k0+count-1 of SingleQubitGatePairGenerator(t, n).next() and of
+ * DoubleQubitGatePairGenerator(c, t, n).next() (`quad` = 0, 2 indices per pair)
+ * or .next_unset_and_set() (`quad` = 1, 4 indices), computed on the device
+ * by bit arithmetic; host_out receives 2 (or 4) uint64 per pair. */
+int32_t kt_pairs_single(uint32_t n_qubits, uint32_t target, uint64_t k0,
+                        uint64_t count, uint64_t* host_out);
+int32_t kt_pairs_double(uint32_t n_qubits, uint32_t control, uint32_t target,
+                        int32_t quad, uint64_t k0, uint64_t count,
+                        uint64_t* host_out);
+
+/* ---- density matrix handle ------------------------------------------------
+ * rho is N x N (N = 2^n) complex, column-major (element (r, c) at r + c*N) as
+ * ket::DensityMatrix's Eigen::MatrixXcd (density_matrix.hpp:109).  It is kept
+ * as a 2n-qubit vector: U on qubit q acts on index bit q and conj(U) on bit
+ * q + n, which is U rho U^dagger (simulate_density_matrix.cpp:42-548). */
+typedef struct kt_dm_s* kt_dm;
+
+int32_t kt_dm_create(int32_t n_qubits, int32_t dtype, kt_dm* out);
+int32_t kt_dm_destroy(kt_dm dm);
+int32_t kt_dm_set_stream(kt_dm dm, void* stream);
+/* rho = |index><index| (DensityMatrix(std::string), density_matrix.cpp:139-148). */
+int32_t kt_dm_set_basis(kt_dm dm, uint64_t index);
+int32_t kt_dm_upload(kt_dm dm, const double* host_colmajor, uint64_t n_elems);
+int32_t kt_dm_download(kt_dm dm, double* host_colmajor, uint64_t n_elems);
+int32_t kt_dm_apply(kt_dm dm, const kt_gate* gates, int64_t n_gates,
+                    const double* params, int64_t n_params, int32_t mode);
+/* Tr(P_k rho) per string and sum_k c_k phase_k Tr(P_k rho) (new: the reference
+ * has no density-matrix expectation value). */
+int32_t kt_dm_expect(kt_dm dm, const kt_pauli* strings, int64_t n_strings,
+                     const double* coeffs, double* out_terms, double* out_total);
+int32_t kt_dm_trace(kt_dm dm, double* out_re_im);
+/* diagonal of rho as probabilities (for sampling a density matrix) */
+int32_t kt_dm_probabilities(kt_dm dm, double* host_out);
+
+/* ---- adjoint differentiation (new) -------------------------------------------
+ * E(theta) = <psi(theta)| H |psi(theta)>, psi = U_G ... U_1 |psi0>.
+ * kt_adjoint_forward runs the circuit on `sv` and returns Re E (FP64);
+ * kt_adjoint_backward then returns dE/dparams[j] for every parameter slot
+ * (gates bound through kt_gate.param; literal gates contribute nothing),
+ * sweeping the gates backwards with one FP64 inner product per
+ * parameterised gate.  `work` needs room for two more statevectors of the
+ * same size (lambda and a scratch); checkpoint_every > 0 stores a copy of
+ * the forward state every that many gates when memory allows and restores
+ * psi from it on the way back instead of relying on un-applying alone. */
+typedef struct kt_adjoint_s* kt_adjoint;
+int32_t kt_adjoint_create(kt_sv sv, int32_t checkpoint_every, kt_adjoint* out);
+int32_t kt_adjoint_destroy(kt_adjoint adj);
+int32_t kt_adjoint_forward(kt_adjoint adj, const kt_gate* gates, int64_t n_gates,
+                           const double* params, int64_t n_params,
+                           const kt_pauli* strings, int64_t n_strings,
+                           const double* coeffs, double* energy);
+int32_t kt_adjoint_backward(kt_adjoint adj, double* grad, int64_t n_params);
+
+/* ---- batches (new) -------------------------------------------------------------
+ * Many independent small circuits (each with its own qubit count, gate list,
+ * parameters and Hamiltonian) evaluated by one persistent kernel launch:
+ * energies[b] and, with grads != NULL, dE_b/dparams (concatenated per item in
+ * the order of param_offsets). */
+typedef struct kt_batch_item {
+    int32_t n_qubits;
+    int32_t reserved;
+    int64_t gate_offset;   /* into the gates array   */
+    int64_t n_gates;
+    int64_t param_offset;  /* into params / grads    */
+    int64_t n_params;
+    int64_t string_offset; /* into strings / coeffs  */
+    int64_t n_strings;
+} kt_batch_item;
+
+int32_t kt_batch_run(const kt_batch_item* items, int64_t n_items,
+                     const kt_gate* gates, int64_t n_gates_total,
+                     const double* params, int64_t n_params_total,
+                     const kt_pauli* strings, const double* coeffs,
+                     int64_t n_strings_total, int32_t dtype,
+                     double* energies, double* grads, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KETTLE_B200_H */

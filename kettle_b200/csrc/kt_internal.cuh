@@ -1,0 +1,134 @@
+// kt_internal.cuh — internal declarations shared by the engine's translation units.
+//
+// Layout in HBM: a statevector of n qubits is 2^n amplitudes, contiguous,
+// little-endian (bit q of the index is qubit q), stored as interleaved
+// (re, im) pairs: double2 for complex128, float2 for complex64.  A density
+// matrix of n qubits is the same thing over 2n index bits (row bits 0..n-1,
+// column bits n..2n-1), i.e. Eigen's column-major element order.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "kettle_b200.h"
+
+namespace kt
+{
+
+// ---------------------------------------------------------------------------
+// errors
+void set_error(int32_t code, const std::string& msg);
+int32_t cuda_fail(cudaError_t e, const char* where);
+
+#define KT_CUDA(call)                                   \
+    do {                                                \
+        cudaError_t kt_e_ = (call);                     \
+        if (kt_e_ != cudaSuccess) {                     \
+            return ::kt::cuda_fail(kt_e_, #call);       \
+        }                                               \
+    } while (0)
+
+#define KT_CHECK_LAUNCH(where)                          \
+    do {                                                \
+        cudaError_t kt_e_ = cudaGetLastError();         \
+        if (kt_e_ != cudaSuccess) {                     \
+            return ::kt::cuda_fail(kt_e_, where);       \
+        }                                               \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device state
+struct DevBuf
+{
+    void* ptr {nullptr};
+    size_t bytes {0};
+    // grow-only scratch; contents are not preserved across growth
+    int32_t reserve(size_t need);
+    void release();
+};
+
+struct State
+{
+    int n_bits {0};          // index bits (n for a statevector, 2n for a density matrix)
+    int dtype {KT_C128};
+    void* amps {nullptr};
+    bool owned {false};
+    cudaStream_t stream {nullptr};
+    DevBuf scratch;          // reductions, CDF, plans
+    DevBuf scratch2;
+    int64_t last_launches {0};   // kernels launched by the last apply
+    double last_alg_bytes {0.0};  // algorithmic bytes of the last apply
+    uint64_t n_amps() const { return uint64_t {1} << n_bits; }
+    size_t amp_bytes() const { return dtype == KT_C128 ? 16 : 8; }
+};
+
+// ---------------------------------------------------------------------------
+// lowered gates: what the kernels consume.  Angles are resolved, matrices
+// built once on the host (the reference recomputes cos/sin for every pair,
+// simulation/operations.cpp:116-117).
+enum GateKind : int32_t
+{
+    KIND_GEN = 0,   // general 2x2
+    KIND_DIAG = 1,  // diag(m00, m11)
+    KIND_ANTI = 2,  // [[0, m01], [m10, 0]]
+};
+
+struct LGate
+{
+    int32_t kind;
+    int32_t target;
+    int32_t control;   // -1 = none
+    int32_t flags;     // bit0: m00 == 1 exactly (DIAG gates that leave |0> alone)
+    double m[8];       // row-major interleaved complex: m00, m01, m10, m11
+};
+
+// Build the matrix of one gate record (the reference's matrices,
+// gates/common_u_gates.cpp) and classify it.  Returns KT_OK or an error.
+int32_t lower_gate(const kt_gate& g, const double* params, int64_t n_params, int n_qubits, LGate* out);
+int32_t lower_gates(const kt_gate* gates, int64_t n_gates, const double* params, int64_t n_params,
+                    int n_qubits, std::vector<LGate>& out);
+
+// conj(U) on (t + shift, c + shift): the column half of U rho U^dagger.
+LGate conj_shifted(const LGate& g, int shift);
+
+// ---------------------------------------------------------------------------
+// kernels (launchers return KT_OK or a CUDA error status)
+int32_t launch_set_basis(State& s, uint64_t index);
+int32_t launch_convert_to_state(State& s, const double* dev_c128, uint64_t n);     // c128 staging -> state
+int32_t launch_convert_from_state(const State& s, double* dev_c128, uint64_t n);   // state -> c128 staging
+int32_t launch_gate_sweep(State& s, const LGate& g);
+double sweep_alg_bytes(const State& s, const LGate& g);
+int32_t launch_pairs(uint32_t n, uint32_t c, uint32_t t, int kind, uint64_t k0, uint64_t count, uint64_t* dev_out,
+                     cudaStream_t stream);
+
+// fused blocks
+struct FusedPlan;
+int32_t apply_fused(State& s, const std::vector<LGate>& gates);
+
+// reductions
+int32_t expect_paulis(State& s, const kt_pauli* strings, int64_t n_strings, const double* coeffs,
+                      double* out_terms, double* out_total);
+int32_t dm_expect_paulis(State& s, int n_qubits, const kt_pauli* strings, int64_t n_strings, const double* coeffs,
+                         double* out_terms, double* out_total);
+int32_t norm_sq(State& s, double* out);
+int32_t inner_product(State& bra, State& ket, double* out);
+int32_t measure_probs(State& s, uint32_t q, double* p0, double* p1);
+int32_t collapse(State& s, uint32_t q, int32_t outcome, double scale);
+int32_t probabilities(State& s, const double* noise, double* host_out);
+int32_t sample(State& s, const double* noise, const double* canonicals, int64_t n_shots, uint64_t* out, int32_t mode,
+               int32_t* n_rescanned);
+int32_t dm_trace(State& s, int n_qubits, double* out);
+int32_t dm_diagonal(State& s, int n_qubits, double* host_out);
+
+// pin-memory staging helper for host <-> device copies
+int32_t copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t st);
+int32_t copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t st);
+
+constexpr int SM_COUNT_B200 = 148;
+int sm_count();
+
+}  // namespace kt

@@ -1,0 +1,57 @@
+"""The C-ABI library loads and exports every symbol include/kettle_b200.h
+declares; host-only helpers work without a GPU; device calls on a machine
+without a GPU fail with a status and a message instead of crashing."""
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from kettle_b200 import capi
+
+
+def _declared():
+    text = (ROOT / "include" / "kettle_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(kt_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = capi.lib()
+    declared = _declared()
+    assert len(declared) >= 38
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    assert sorted(capi.exported_symbols()) == _declared()
+
+
+def test_record_layouts():
+    assert capi.GATE_DTYPE.itemsize == 88
+    assert capi.PAULI_DTYPE.itemsize == 24
+    assert capi.GATE_DTYPE.fields["angle"][1] == 16
+    assert capi.GATE_DTYPE.fields["u"][1] == 24
+
+
+def test_version_and_error_strings():
+    assert capi.lib().kt_version() >= 100
+    # a bad argument is rejected on the host, before any device work
+    with pytest.raises(capi.KettleError) as e:
+        capi.pairs_single(3, 5)
+    assert "target" in str(e.value)
+
+
+def test_no_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(capi.KettleError) as e:
+        capi.Statevector(4)
+    assert e.value.code in (-2, -3)
+
+
+def test_canonicals_helper_is_host_only():
+    v = capi.canonicals_mt19937(5489, 10)
+    assert np.all((v >= 0) & (v < 1))

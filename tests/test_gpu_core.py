@@ -1,0 +1,340 @@
+"""GPU parity: the CUDA engine, called through the C-ABI, against the oracle.
+
+Tolerances: complex128 amplitudes and expectation values within 1e-12
+(absolute, states are normalised); pair indices and sampled outcomes
+bit-exact; complex64 results are reported against the complex128 oracle with
+a loose bound (1e-4) since the bulk storage is single precision.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import basis, random_state
+from kettle_b200 import capi
+from kettle_b200 import workloads as W
+from kettle_b200.capi import KT_APPLY_FUSED, KT_APPLY_PER_GATE, KT_C64, KT_C128, OP
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+ALL_OPS = [g for g in capi.GATES if g != "M"]
+
+
+def _gate_for(name, t, c, rng):
+    if name in ("U", "CU"):
+        return W.gate(name, t, control=c, u=W.haar_unitary2(rng))
+    if name in capi.ANGLE_GATES:
+        return W.gate(name, t, control=c, angle=float(rng.uniform(0, 2 * math.pi)))
+    return W.gate(name, t, control=c)
+
+
+def _run(n, init, gates, params=None, mode=KT_APPLY_FUSED, dtype=KT_C128):
+    sv = capi.Statevector(n, dtype)
+    sv.upload(init)
+    sv.apply(gates, params, mode)
+    out = sv.download()
+    sv.close()
+    return out
+
+
+def inverse(gates):
+    """Gate list of the inverse circuit (reversed, each gate replaced by its adjoint)."""
+    adj = {"S": "SDAG", "SDAG": "S", "T": "TDAG", "TDAG": "T", "SX": "SXDAG", "SXDAG": "SX",
+           "CS": "CSDAG", "CSDAG": "CS", "CT": "CTDAG", "CTDAG": "CT", "CSX": "CSXDAG", "CSXDAG": "CSX"}
+    out = gates[::-1].copy()
+    for g in out:
+        name = capi.GATES[g["op"]]
+        if name in adj:
+            g["op"] = OP[adj[name]]
+        elif name in capi.ANGLE_GATES:
+            g["angle"] = -g["angle"]
+        elif name in ("U", "CU"):
+            u = g["u"]
+            m = np.array([[u[0] + 1j * u[1], u[2] + 1j * u[3]], [u[4] + 1j * u[5], u[6] + 1j * u[7]]]).conj().T
+            g["u"][:] = [m[0, 0].real, m[0, 0].imag, m[0, 1].real, m[0, 1].imag,
+                         m[1, 0].real, m[1, 0].imag, m[1, 1].real, m[1, 1].imag]
+    return out
+
+
+# --- pair enumeration ----------------------------------------------------------
+
+def test_pairs_small_exhaustive(engine, port, golden):
+    for n in range(1, 8):
+        for t in range(n):
+            assert np.array_equal(capi.pairs_single(n, t), port.pairs_single(n, t))
+            for c in range(n):
+                if c == t or n < 2:
+                    continue
+                for quad in (False, True):
+                    assert np.array_equal(capi.pairs_double(n, c, t, quad), port.pairs_double(n, c, t, quad))
+    for a, b in ((10, 15), (7, 10), (3, 7), (0, 5), (9, 13)):
+        assert np.array_equal(capi.pairs_single(5, 3, a, b - a), golden[f"pairs_ss_5_3_{a}_{b}"])
+        assert np.array_equal(capi.pairs_double(6, 2, 3, False, a, b - a), golden[f"pairs_ds_6_2_3_{a}_{b}"])
+
+
+def test_pairs_large_windows(engine, port):
+    rng = np.random.default_rng(7)
+    for n in (20, 30, 33):
+        for _ in range(4):
+            t = int(rng.integers(n))
+            k0 = int(rng.integers(1 << (n - 1))) // 2
+            assert np.array_equal(capi.pairs_single(n, t, k0, 4096), port.pairs_single(n, t, k0, 4096))
+            c = int((t + 1 + rng.integers(n - 1)) % n)
+            k0 = int(rng.integers(1 << (n - 2))) // 2
+            for quad in (False, True):
+                assert np.array_equal(capi.pairs_double(n, c, t, quad, k0, 4096),
+                                      port.pairs_double(n, c, t, quad, k0, 4096))
+
+
+# --- gate sweeps -----------------------------------------------------------------
+
+@pytest.mark.parametrize("mode", [KT_APPLY_PER_GATE, KT_APPLY_FUSED])
+def test_every_gate_every_position(engine, port, mode):
+    rng = np.random.default_rng(11)
+    for n in (1, 2, 3, 5):
+        for name in ALL_OPS:
+            ctl = name in capi.CONTROLLED
+            if ctl and n < 2:
+                continue
+            for t in range(n):
+                for c in (range(n) if ctl else [0]):
+                    if ctl and c == t:
+                        continue
+                    init = random_state(n, int(rng.integers(1 << 30)))
+                    g = _gate_for(name, t, c, rng)
+                    got = _run(n, init, g, mode=mode)
+                    want = port.apply(n, init, g)
+                    assert np.abs(got - want).max() < 1e-14, (name, n, t, c)
+
+
+@pytest.mark.parametrize("n,layers,mixed", [(10, 12, False), (10, 8, True), (14, 6, True), (17, 4, True)])
+@pytest.mark.parametrize("mode", [KT_APPLY_PER_GATE, KT_APPLY_FUSED])
+def test_random_circuits_c128(engine, port, n, layers, mixed, mode):
+    g = W.random_layers(n, layers, seed=100 + n, mixed=mixed)
+    init = basis(n)
+    got = _run(n, init, g, mode=mode)
+    want = port.apply(n, init, g)
+    assert np.abs(got - want).max() < TOL
+
+
+def test_golden_circuits(engine, golden):
+    for key in golden:
+        if key.startswith("circ_") and key.endswith("_gates"):
+            stem = key[: -len("_gates")]
+            n = int(stem.split("_")[1])
+            got = _run(n, basis(n), golden[key])
+            assert np.abs(got - golden[stem + "_amps"]).max() < TOL, stem
+
+
+def test_parameterised_circuit(engine, port, golden):
+    g, p = golden["hea_5_3_gates"], golden["hea_5_3_params"]
+    got = _run(5, basis(5), g, p)
+    assert np.abs(got - golden["hea_5_3_amps"]).max() < TOL
+    g2, p2 = W.hea(12, 4, seed=3)
+    assert np.abs(_run(12, basis(12), g2, p2) - port.apply(12, basis(12), g2, p2)).max() < TOL
+
+
+def test_complex64_against_c128_oracle(engine, port):
+    n = 14
+    g = W.random_layers(n, 6, seed=5, mixed=True)
+    got = _run(n, basis(n), g, dtype=KT_C64)
+    want = port.apply(n, basis(n), g)
+    err = np.abs(got - want).max()
+    assert err < 1e-4, err
+
+
+def test_inverse_circuit_returns_to_start(engine):
+    n = 22
+    g = W.random_layers(n, 6, seed=9, mixed=True)
+    both = np.concatenate([g, inverse(g)])
+    sv = capi.Statevector(n)
+    sv.apply(both)
+    amps = sv.download()
+    assert abs(amps[0] - 1.0) < 1e-11
+    assert np.abs(amps[1:]).max() < 1e-11
+
+
+def test_fused_matches_per_gate_large(engine):
+    n = 26
+    g = W.random_layers(n, 3, seed=21, mixed=True)
+    a = capi.Statevector(n)
+    b = capi.Statevector(n)
+    a.apply(g, mode=KT_APPLY_FUSED)
+    b.apply(g, mode=KT_APPLY_PER_GATE)
+    x, y = a.download(), b.download()
+    assert np.abs(x - y).max() < TOL
+    assert abs(a.norm_sq() - 1.0) < 1e-11
+
+
+def test_bad_gates_rejected(engine):
+    sv = capi.Statevector(4)
+    with pytest.raises(capi.KettleError):
+        sv.apply(W.gate("H", 4))
+    with pytest.raises(capi.KettleError):
+        sv.apply(W.gate("CX", 1, control=1))
+    with pytest.raises(capi.KettleError):
+        sv.apply(W.gate("M", 0))
+    with pytest.raises(capi.KettleError):
+        sv.apply(W.gate("RX", 0, param=3), params=np.zeros(2))
+    # the state is untouched and still usable
+    assert abs(sv.download()[0] - 1) == 0
+
+
+# --- expectation values -------------------------------------------------------------
+
+def test_expectation_random(engine, port):
+    for n, seed in ((6, 1), (12, 2), (16, 3)):
+        psi = port.apply(n, basis(n), W.random_layers(n, 4, seed=seed, mixed=True))
+        strs, cs = W.random_paulis(n, 60, seed)
+        sv = capi.Statevector(n)
+        sv.upload(psi)
+        terms, total = sv.expect(strs, cs)
+        want_t, want = port.expect(n, psi, strs, cs)
+        assert np.abs(terms - want_t).max() < TOL
+        assert abs(total - want) < TOL * 10
+
+
+def test_expectation_kats(engine, kats):
+    for case in kats["expect"]:
+        n = case["n"]
+        strs, cs = [], []
+        for (cr, ci), terms in case["ops"]:
+            strs.append(W.pauli(n, {int(k): v for k, v in terms.items()}))
+            cs.append(complex(cr, ci))
+        sv = capi.Statevector(n)
+        sv.upload(np.array([complex(a, b) for a, b in case["state"]]))
+        _, total = sv.expect(np.concatenate(strs), np.array(cs))
+        assert abs(total - complex(*case["expected"])) < 1e-14, case["cite"]
+
+
+def test_expectation_phases_and_shared_masks(engine, port):
+    n = 9
+    psi = random_state(n, 4)
+    strs = np.concatenate([W.pauli(n, {0: "X", 3: "Y"}, phase=ph) for ph in range(4)] +
+                          [W.pauli(n, {0: "X", 3: "X", 5: "Z"}), W.pauli(n, {0: "Y", 3: "Y"}),
+                           W.pauli(n, {}), W.pauli(n, {8: "Z", 2: "Z"})])
+    sv = capi.Statevector(n)
+    sv.upload(psi)
+    t, _ = sv.expect(strs)
+    want, _ = port.expect(n, psi, strs)
+    assert np.abs(t - want).max() < TOL
+
+
+def test_expectation_c64(engine, port):
+    n = 12
+    psi = port.apply(n, basis(n), W.random_layers(n, 4, seed=8, mixed=True))
+    strs, cs = W.random_paulis(n, 40, 8)
+    sv = capi.Statevector(n, KT_C64)
+    sv.upload(psi)
+    _, total = sv.expect(strs, cs)
+    _, want = port.expect(n, psi, strs, cs)
+    assert abs(total - want) < 1e-5
+
+
+# --- probabilities, sampling, M ------------------------------------------------------------
+
+def test_probabilities_bit_exact(engine, port, golden):
+    a = golden["circ_6_8_0_11_amps"]
+    sv = capi.Statevector(6)
+    sv.upload(a)
+    assert np.array_equal(sv.probabilities(), port.probabilities(6, a))
+    assert np.array_equal(sv.probabilities(golden["noise_vec"]), golden["noise_probs"])
+
+
+def test_sampling_bit_exact_golden(engine, port, golden):
+    for key in golden:
+        if key.startswith("circ_") and key.endswith("_amps"):
+            stem = key[: -len("_amps")]
+            n = int(stem.split("_")[1])
+            sv = capi.Statevector(n)
+            sv.upload(golden[key])
+            for seed in (1, 42):
+                for mode in (0, 1):
+                    idx, _ = sv.sample(port.canonicals(seed, 512), mode=mode)
+                    assert np.array_equal(idx, golden[f"{stem}_samples_{seed}"]), (stem, seed, mode)
+
+
+def test_sampling_bit_exact_random(engine, port):
+    for n, seed in ((12, 1), (18, 2), (20, 3)):
+        psi = port.apply(n, basis(n), W.random_layers(n, 6, seed=seed))
+        sv = capi.Statevector(n)
+        sv.upload(psi)
+        can = port.canonicals(seed, 4096)
+        idx, rescanned = sv.sample(can)
+        want = port.sample(n, port.probabilities(n, psi), can)
+        assert np.array_equal(idx, want)
+        noise = np.linspace(0, 0.1, n)
+        idx2, _ = sv.sample(can, noise=noise)
+        assert np.array_equal(idx2, port.sample(n, port.probabilities(n, psi, noise), can))
+
+
+def test_sampling_edge_cases(engine, port):
+    for vec in ([0.6, 0.8, 0, 0], [0, 1.0, 0, 0, 0, 0, 0, 0], [1.0, 0, 0, 0], [0, 0, 0, 1.0]):
+        v = np.array(vec, dtype=np.complex128)
+        n = int(np.log2(v.size))
+        sv = capi.Statevector(n)
+        sv.upload(v)
+        can = np.concatenate([port.canonicals(3, 64), [0.0, np.nextafter(1.0, 0.0)]])
+        for mode in (0, 1):
+            idx, _ = sv.sample(can, mode=mode)
+            assert np.array_equal(idx, port.sample(n, port.probabilities(n, v), can)), (vec, mode)
+
+
+def test_measure_gate(engine, port, golden):
+    a0 = golden["meas_pre_amps"]
+    for (seed, q), o, a1 in zip(golden["meas_seed_qubit"], golden["meas_outcome"], golden["meas_amps"]):
+        sv = capi.Statevector(5)
+        sv.upload(a0)
+        p0, p1 = sv.measure_probs(int(q))
+        _, _, wp0, wp1 = port.measure(5, a0, int(q), 0.5)
+        assert abs(p0 - wp0) < 1e-14 and abs(p1 - wp1) < 1e-14
+        c0 = port.canonicals(int(seed), 1)[0]
+        outcome = 0 if c0 <= p0 / (p0 + p1) else 1
+        assert outcome == o
+        sv.collapse(int(q), outcome, math.sqrt(1.0 / (p0 if outcome == 0 else p1)))
+        assert np.abs(sv.download() - a1).max() < 1e-14
+
+
+def test_norm_and_inner(engine):
+    n = 10
+    x, y = random_state(n, 1), random_state(n, 2)
+    a, b = capi.Statevector(n), capi.Statevector(n)
+    a.upload(x)
+    b.upload(y)
+    assert abs(a.norm_sq() - 1.0) < 1e-14
+    assert abs(a.inner(b) - np.vdot(x, y)) < 1e-14
+
+
+# --- density matrix -----------------------------------------------------------------------
+
+@pytest.mark.parametrize("n,layers", [(3, 3), (4, 2), (6, 3)])
+@pytest.mark.parametrize("mode", [KT_APPLY_PER_GATE, KT_APPLY_FUSED])
+def test_density_matrix(engine, port, n, layers, mode):
+    g = W.random_layers(n, layers, seed=40 + n, mixed=True)
+    dm = capi.DensityMatrix(n)
+    dm.apply(g, mode=mode)
+    got = dm.download()
+    rho0 = np.zeros((1 << n, 1 << n), dtype=np.complex128)
+    rho0[0, 0] = 1
+    want = port.simulate_dm(n, rho0, g)
+    assert np.abs(got - want).max() < TOL
+    strs, cs = W.random_paulis(n, 30, n)
+    t, total = dm.expect(strs, cs)
+    wt, wtotal = port.dm_expect(n, want, strs, cs)
+    assert np.abs(t - wt).max() < TOL and abs(total - wtotal) < TOL
+    # pure-state identity: Tr(P |psi><psi|) = <psi|P|psi>
+    psi = port.apply(n, basis(n), g)
+    st, _ = port.expect(n, psi, strs, cs)
+    assert np.abs(t - st).max() < TOL
+    assert abs(dm.trace() - 1.0) < TOL
+
+
+def test_density_matrix_golden(engine, golden):
+    for key in golden:
+        if key.startswith("dm_") and key.endswith("_gates"):
+            stem = key[: -len("_gates")]
+            n = int(stem.split("_")[1])
+            dm = capi.DensityMatrix(n)
+            dm.apply(golden[key])
+            assert np.abs(dm.download() - golden[stem + "_rho"]).max() < TOL
