@@ -321,3 +321,44 @@ def pairs_double(n: int, c: int, t: int, quad: bool = False, k0: int = 0, count:
     out = np.empty((count, 4 if quad else 2), dtype=np.uint64)
     check(lib().kt_pairs_double(n, c, t, 1 if quad else 0, k0, count, ptr(out)))
     return out
+
+
+class Adjoint:
+    """Adjoint gradient of E = Re <psi|H|psi> for a parameterised circuit (kt_adjoint).
+
+    forward() runs the circuit on the given statevector (from its current
+    state) and returns E; backward() returns dE/dparams and leaves the
+    statevector un-applied back to its initial state."""
+
+    def __init__(self, sv: Statevector, checkpoint_every: int = 0):
+        h = P()
+        check(lib().kt_adjoint_create(sv.handle, checkpoint_every, C.byref(h)))
+        self._h = h
+        self.sv = sv
+        self.n_params = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().kt_adjoint_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, gates, params, strings, coeffs=None) -> float:
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        s = np.ascontiguousarray(strings, dtype=PAULI_DTYPE)
+        c = None if coeffs is None else np.ascontiguousarray(coeffs, dtype=np.complex128)
+        e = C.c_double()
+        check(lib().kt_adjoint_forward(self._h, ptr(g), g.size, ptr(p), p.size, ptr(s), s.size, ptr(c), C.byref(e)))
+        self.n_params = p.size
+        return e.value
+
+    def backward(self) -> np.ndarray:
+        out = np.zeros(self.n_params, dtype=np.float64)
+        check(lib().kt_adjoint_backward(self._h, ptr(out), out.size))
+        return out

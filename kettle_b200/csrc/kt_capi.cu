@@ -11,17 +11,6 @@ namespace kt
 const char* last_error_cstr();
 }
 
-struct kt_sv_s
-{
-    kt::State st;
-};
-
-struct kt_dm_s
-{
-    kt::State st;  // 2n index bits
-    int n {0};
-};
-
 namespace
 {
 

@@ -132,3 +132,15 @@ constexpr int SM_COUNT_B200 = 148;
 int sm_count();
 
 }  // namespace kt
+
+// the opaque handles of the C-ABI
+struct kt_sv_s
+{
+    kt::State st;
+};
+
+struct kt_dm_s
+{
+    kt::State st;  // 2n index bits
+    int n {0};
+};

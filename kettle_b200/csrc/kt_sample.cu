@@ -242,34 +242,210 @@ __global__ void k_sample_fast(const double* __restrict__ p, const double* __rest
 }
 
 // exact tier -------------------------------------------------------------------
-// std::partial_sum: cdf[0] = p[0]; cdf[i] = cdf[i-1] + p[i] (one thread).
-__global__ void k_seq_cdf(const double* __restrict__ p, uint64_t N, double* __restrict__ cdf)
+// The sequential sum s_i = fl(s_{i-1} + p_i) of std::partial_sum, computed
+// exactly by one block.  While s stays in one binade [2^E, 2^(E+1)) every
+// representable value is a multiple of u = 2^(E-52), so (no tie, no binade
+// exit) fl(s + p) = s + rint(p / u) * u exactly: a run of additions is an
+// integer prefix sum, which the block computes in parallel (uint64 units).
+// An element whose p/u is an exact tie (.5), is large (>= 2^50 units), or
+// whose running sum leaves the binade is added with one IEEE add instead,
+// after which the block continues from the new (exact) s.  Each 8192-element
+// tile costs one block scan, plus one round per such element.
+constexpr int XS_THREADS = 1024;
+constexpr int XS_EPT = 16;
+constexpr int XS_TILE = XS_THREADS * XS_EPT;
+
+__device__ __forceinline__ unsigned long long block_excl_scan_u64(unsigned long long v, unsigned long long* sh,
+                                                                  unsigned long long& total)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) {
-        return;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffU, x, o);
+        if (lane >= o) {
+            x += y;
+        }
     }
-    double acc = p[0];
-    cdf[0] = acc;
-    for (uint64_t i = 1; i < N; ++i) {
-        acc = __dadd_rn(acc, p[i]);
-        cdf[i] = acc;
+    if (lane == 31) {
+        sh[warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long w = (lane < XS_THREADS / 32) ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffU, w, o);
+            if (lane >= o) {
+                w += y;
+            }
+        }
+        sh[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    total = sh[XS_THREADS / 32 - 1];
+    const unsigned long long before = (warp > 0) ? sh[warp - 1] : 0ULL;
+    const unsigned long long r = before + x - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(XS_THREADS) k_exact_cdf(const double* __restrict__ p, uint64_t N, double* __restrict__ cdf)
+{
+    __shared__ unsigned long long sh[32];
+    __shared__ double s_sh;
+    __shared__ unsigned long long i_sh;
+    __shared__ unsigned int viol_sh;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        s_sh = p[0];
+        cdf[0] = p[0];
+        i_sh = 1;
+    }
+    __syncthreads();
+    constexpr unsigned long long TWO53 = 1ULL << 53;
+    while (true) {
+        const uint64_t i = i_sh;
+        const double s = s_sh;
+        if (i >= N) {
+            break;
+        }
+        if (s < 0x1p-900) {
+            // zero or tiny running value (subnormal spacing, huge 1/ulp): plain IEEE steps
+            if (t == 0) {
+                const double nv = __dadd_rn(s, p[i]);
+                s_sh = nv;
+                cdf[i] = nv;
+                i_sh = i + 1;
+            }
+            __syncthreads();
+            continue;
+        }
+        int E;
+        frexp(s, &E);                       // s in [2^(E-1), 2^E)
+        const double inv_u = ldexp(1.0, 53 - E);  // 1 / ulp(s)
+        const double u = ldexp(1.0, E - 53);
+        const unsigned long long m = static_cast<unsigned long long>(s * inv_u);  // exact, in [2^52, 2^53)
+        // this thread's elements: i + t*EPT + k
+        unsigned long long r[XS_EPT];
+        unsigned int bad = XS_TILE;  // first flagged local index
+        unsigned long long run = 0;
+        const uint64_t b0 = i + static_cast<uint64_t>(t) * XS_EPT;
+#pragma unroll
+        for (int k = 0; k < XS_EPT; ++k) {
+            const uint64_t g = b0 + k;
+            double q = 0.0;
+            if (g < N) {
+                q = p[g] * inv_u;
+            }
+            const double f = floor(q);
+            const bool tie = (q - f) == 0.5;
+            const bool big = !(q < 1125899906842624.0);  // 2^50 (also catches inf)
+            if ((tie || big) && g < N && bad == XS_TILE) {
+                bad = t * XS_EPT + k;
+            }
+            r[k] = big ? 0ULL : static_cast<unsigned long long>(rint(q));
+            run += r[k];
+        }
+        unsigned long long total;
+        const unsigned long long excl = block_excl_scan_u64(run, sh, total);
+        // binade exit: first element whose running sum reaches 2^53 units
+        unsigned long long acc = m + excl;
+#pragma unroll
+        for (int k = 0; k < XS_EPT; ++k) {
+            acc += r[k];
+            const unsigned int li = t * XS_EPT + k;
+            if (acc >= TWO53 && li < bad) {
+                bad = li;
+            }
+        }
+        if (t == 0) {
+            viol_sh = XS_TILE;
+        }
+        __syncthreads();
+        atomicMin(&viol_sh, bad);
+        __syncthreads();
+        const uint64_t tile_len = (N - i) < XS_TILE ? (N - i) : XS_TILE;
+        const unsigned int v = viol_sh < tile_len ? viol_sh : static_cast<unsigned int>(tile_len);
+        // commit the elements before v
+        acc = m + excl;
+#pragma unroll
+        for (int k = 0; k < XS_EPT; ++k) {
+            acc += r[k];
+            const unsigned int li = t * XS_EPT + k;
+            if (li < v) {
+                cdf[i + li] = static_cast<double>(acc) * u;
+            }
+        }
+        // the value before element v, for thread 0's IEEE step
+        if (v < tile_len) {
+            // running value just before v: the thread owning v - 1 knows it
+            const unsigned int last = v;  // element index to add with an IEEE add
+            if (last == 0) {
+                if (t == 0) {
+                    const double nv = __dadd_rn(s, p[i]);
+                    cdf[i] = nv;
+                    s_sh = nv;
+                    i_sh = i + 1;
+                }
+            } else {
+                const unsigned int owner = (last - 1) / XS_EPT;
+                if (static_cast<unsigned int>(t) == owner) {
+                    unsigned long long a2 = m + excl;
+                    for (int k = 0; k < XS_EPT; ++k) {
+                        if (t * XS_EPT + k < last) {
+                            a2 += r[k];
+                        }
+                    }
+                    const double before = static_cast<double>(a2) * u;
+                    const double nv = __dadd_rn(before, p[i + last]);
+                    cdf[i + last] = nv;
+                    s_sh = nv;
+                    i_sh = i + last + 1;
+                }
+            }
+        } else {
+            if (t == 0) {
+                s_sh = static_cast<double>(m + total) * u;
+                i_sh = i + tile_len;
+            }
+        }
+        __syncthreads();
     }
 }
 
-// cumulative_end_offset_ (measurements.cpp:235-256) and the distribution bound
-__global__ void k_seq_bound(const double* __restrict__ cdf, uint64_t N, double* __restrict__ bound)
+// cumulative_end_offset_ (measurements.cpp:235-256): the last value strictly
+// below `last`, found as the largest index holding one.
+__global__ void k_last_below(const double* __restrict__ cdf, uint64_t N, unsigned long long* __restrict__ idx1)
+{
+    const double last = cdf[N - 1];
+    unsigned long long best = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i + 1 < N; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (cdf[i] < last) {
+            best = static_cast<unsigned long long>(i) + 1;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_down_sync(0xffffffffU, best, o);
+        best = y > best ? y : best;
+    }
+    if ((threadIdx.x & 31) == 0 && best != 0) {
+        atomicMax(idx1, best);
+    }
+}
+
+// the distribution bound last - (last - second) * 1e-4 (measurements.cpp:288-295)
+__global__ void k_seq_bound(const double* __restrict__ cdf, uint64_t N, const unsigned long long* __restrict__ idx1,
+                            double* __restrict__ bound)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) {
         return;
     }
     const double last = cdf[N - 1];
-    double second = 0.0;
-    for (uint64_t i = N - 1; i > 0; --i) {
-        if (cdf[i - 1] < last) {
-            second = cdf[i - 1];
-            break;
-        }
-    }
+    const unsigned long long j = *idx1;
+    const double second = (j == 0) ? 0.0 : cdf[j - 1];
     const double offset = __dmul_rn(__dsub_rn(last, second), 1.0e-4);
     *bound = __dsub_rn(last, offset);
 }
@@ -344,7 +520,13 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
         return rc;
     }
     int unc = 0;
-    if (mode == 0) {
+    // The certified tier pays off while the worst-case rounding bound of a
+    // sequential sum, ~N * 2^-53, stays far below a typical probability ~1/N.
+    const bool try_fast = (mode == 0) && N <= (uint64_t {1} << 22);
+    if (!try_fast) {
+        unc = 1;
+    }
+    if (try_fast) {
         KT_CUDA(cudaMemsetAsync(d_nz, 0, 8, s.stream));
         KT_CUDA(cudaMemsetAsync(d_unc, 0, 4, s.stream));
         const uint64_t threads = n_chunks * 32;
@@ -361,10 +543,14 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
             return rc;
         }
     }
-    if (mode != 0 || unc != 0) {
-        k_seq_cdf<<<1, 32, 0, s.stream>>>(dp, N, dcdf);
-        KT_CHECK_LAUNCH("k_seq_cdf");
-        k_seq_bound<<<1, 32, 0, s.stream>>>(dcdf, N, d_bound);
+    if (unc != 0) {
+        k_exact_cdf<<<1, XS_THREADS, 0, s.stream>>>(dp, N, dcdf);
+        KT_CHECK_LAUNCH("k_exact_cdf");
+        KT_CUDA(cudaMemsetAsync(d_nz, 0, 8, s.stream));
+        const unsigned lb_blocks = static_cast<unsigned>(std::min<uint64_t>((N + 255) / 256, sm_count() * 8ULL));
+        k_last_below<<<lb_blocks, 256, 0, s.stream>>>(dcdf, N, d_nz);
+        KT_CHECK_LAUNCH("k_last_below");
+        k_seq_bound<<<1, 32, 0, s.stream>>>(dcdf, N, d_nz, d_bound);
         KT_CHECK_LAUNCH("k_seq_bound");
         k_seq_search<<<static_cast<unsigned>((ns + 127) / 128), 128, 0, s.stream>>>(dcdf, N, d_bound, d_canon, n_shots,
                                                                                      d_out);

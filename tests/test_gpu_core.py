@@ -338,3 +338,40 @@ def test_density_matrix_golden(engine, golden):
             dm = capi.DensityMatrix(n)
             dm.apply(golden[key])
             assert np.abs(dm.download() - golden[stem + "_rho"]).max() < TOL
+
+
+def test_sampling_exact_tier_adversarial(engine, port):
+    """The exact scan (mode 1, and every N above 2^22) against std::partial_sum
+    semantics on vectors with exact ties, zeros, tiny and dyadic values."""
+    rng = np.random.default_rng(17)
+    cases = []
+    v = np.zeros(1 << 12, dtype=np.complex128)
+    v[::3] = 2.0 ** -rng.integers(3, 40, size=v[::3].size)        # dyadic: exact ties in many binades
+    cases.append(v)
+    w = (rng.standard_normal(1 << 13) * 1e-160).astype(np.complex128)  # tiny running sums first
+    w[5000:] = rng.standard_normal((1 << 13) - 5000)
+    cases.append(w)
+    z = np.zeros(1 << 11, dtype=np.complex128)
+    z[700] = 1.0
+    z[701:710] = 2.0 ** -30
+    cases.append(z)
+    cases.append(random_state(14, 3))
+    for vec in cases:
+        n = int(np.log2(vec.size))
+        sv = capi.Statevector(n)
+        sv.upload(vec)
+        can = np.concatenate([port.canonicals(5, 2000), [0.0, np.nextafter(1.0, 0.0)]])
+        idx, rescanned = sv.sample(can, mode=1)
+        assert rescanned == 1
+        assert np.array_equal(idx, port.sample(n, port.probabilities(n, vec), can))
+
+
+def test_sampling_large_state_exact(engine, port):
+    n = 24
+    psi = random_state(n, 21)
+    sv = capi.Statevector(n)
+    sv.upload(psi)
+    can = port.canonicals(77, 4096)
+    idx, rescanned = sv.sample(can)
+    assert rescanned == 1  # above 2^22 amplitudes the exact scan runs directly
+    assert np.array_equal(idx, port.sample(n, port.probabilities(n, psi), can))
