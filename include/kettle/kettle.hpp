@@ -1,0 +1,6 @@
+// kettle.hpp — umbrella header of the B200 engine's kettle-compatible C++20 API.
+// Code written against the reference's <kettle/kettle.hpp> (namespace ket)
+// compiles against this header for the circuit-propagation API it covers.
+#pragma once
+
+#include "kettle/ket_b200.hpp"

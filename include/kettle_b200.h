@@ -137,6 +137,15 @@ int32_t kt_device_synchronize(void);
  * scaling them by its distribution bound.  Host-only helper. */
 int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
 
+/* Launch-shape knobs of the engine (no reference counterpart), set by the
+ * autotuner (kettle_b200/autotune.py) or from KT_TUNING="name=value,...":
+ *   fused_ctas_per_sm  1 or 2   register budget of the fused block kernel
+ *   fused_tile_bits    9..12    tile qubits per fused block (complex128)
+ *   fused_max_ops      1..256   gates per fused block
+ * Unknown names return KT_ERR_INVALID. */
+int32_t kt_tuning_set(const char* name, int64_t value);
+int32_t kt_tuning_get(const char* name, int64_t* value);
+
 /* ---- statevector handle --------------------------------------------------
  * A statevector of n qubits lives on the current CUDA device as 2^n amplitudes,
  * little-endian (bit q of the index = qubit q), contiguous.  kt_sv_create

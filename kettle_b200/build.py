@@ -93,6 +93,13 @@ def build_front_end(verbose: bool = False, force: bool = False) -> pathlib.Path:
         text = _run(cmd)
         if verbose and text.strip():
             print(text)
+    # the drop-in demonstration program against this front end
+    demo_src = ROOT / "tests" / "cpp" / "dropin_main.cpp"
+    demo = LIB / "dropin_b200"
+    if demo_src.exists() and (force or _stale(demo, [demo_src, out] + headers)):
+        cxx = shutil.which("g++") or "g++"
+        _run([cxx, "-std=c++20", "-O2", f"-I{INCLUDE}", str(demo_src), f"-L{LIB}", "-lket_b200", "-lkettle_b200",
+              "-Wl,-rpath,$ORIGIN", "-o", str(demo)])
     return out
 
 
@@ -103,7 +110,7 @@ def build_oracle(verbose: bool = False) -> None:
     _run([make, "-C", str(ROOT / "oracle"), "port"])
     ref = pathlib.Path(os.environ.get("KETTLE_REFERENCE", "/root/reference"))
     if (ref / "CMakeLists.txt").exists():
-        _run([make, "-C", str(ROOT / "oracle"), "ref", f"REF={ref}", f"-j{min(8, os.cpu_count() or 4)}"])
+        _run([make, "-C", str(ROOT / "oracle"), "ref", "dropin", f"REF={ref}", f"-j{min(8, os.cpu_count() or 4)}"])
 
 
 def ptxas_report() -> str:

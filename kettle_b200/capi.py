@@ -57,6 +57,8 @@ _SIGS = {
     "kt_version": ([], I32),
     "kt_device_synchronize": ([], I32),
     "kt_canonicals_mt19937": ([U32, I64, P], I32),
+    "kt_tuning_set": ([C.c_char_p, I64], I32),
+    "kt_tuning_get": ([C.c_char_p, C.POINTER(I64)], I32),
     "kt_sv_create": ([I32, I32, C.POINTER(P)], I32),
     "kt_sv_wrap": ([P, I32, I32, C.POINTER(P)], I32),
     "kt_sv_destroy": ([P], I32),
@@ -133,6 +135,16 @@ def canonicals_mt19937(seed: int, n: int) -> np.ndarray:
     out = np.empty(n, dtype=np.float64)
     check(lib().kt_canonicals_mt19937(seed & 0xFFFFFFFF, n, ptr(out)))
     return out
+
+
+def tuning_set(name: str, value: int) -> None:
+    check(lib().kt_tuning_set(name.encode(), int(value)))
+
+
+def tuning_get(name: str) -> int:
+    v = I64(0)
+    check(lib().kt_tuning_get(name.encode(), C.byref(v)))
+    return int(v.value)
 
 
 def as_complex_interleaved(a: np.ndarray) -> np.ndarray:

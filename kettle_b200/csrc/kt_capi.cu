@@ -165,6 +165,21 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out)
     });
 }
 
+int32_t kt_tuning_set(const char* name, int64_t value)
+{
+    return kt::tuning_set(name, value) ? KT_OK : invalid("unknown tuning knob");
+}
+
+int32_t kt_tuning_get(const char* name, int64_t* value)
+{
+    long long v = 0;
+    if (value == nullptr || !kt::tuning_get(name, &v)) {
+        return invalid("unknown tuning knob");
+    }
+    *value = v;
+    return KT_OK;
+}
+
 // ---- statevector --------------------------------------------------------------
 
 int32_t kt_sv_create(int32_t n_qubits, int32_t dtype, kt_sv* out)

@@ -17,8 +17,13 @@
 //    A non-diagonal gate is applied in registers when its target is a register
 //    bit; the planner groups the block's gates into phases with a fixed
 //    register set (chosen by next use) and a shared-memory transpose between
-//    phases.  Shared memory is XOR-swizzled so the transposes are free of bank
-//    conflicts when the lane bits are chosen with distinct residues.
+//    phases.  Shared memory is XOR-swizzled (a linear map, so addresses are
+//    XORs of per-bit terms) and the lane bits are chosen so the transposes are
+//    free of bank conflicts.
+//  * Everything that depends only on the layout is resolved on the host: for
+//    each gate the register slot of its target, a bit mask of the registers
+//    whose control bit is set, the thread-index bits of a control or a diagonal
+//    target that is a thread bit.  The kernel does no per-amplitude index math.
 //  * Loads and stores use a layout whose lane bits are the L lowest qubits:
 //    each warp instruction touches whole 128-byte lines.
 #include <algorithm>
@@ -35,24 +40,45 @@ namespace
 {
 
 constexpr int KMAX = 14;
-constexpr int MAX_OPS_PER_BLOCK = 512;
+constexpr int RBMAX = 5;
+constexpr int TBMAX = 8;
+constexpr int MAX_OPS_PER_BLOCK = 256;
+constexpr int MAX_PHASES_PER_BLOCK = 64;
+
+enum OpKind : uint8_t
+{
+    OP_GEN = 0,    // general complex 2x2
+    OP_GENR = 1,   // real 2x2 (H, RY, real U)
+    OP_ANTI = 2,   // [[0, m01], [m10, 0]]
+    OP_SWAP = 3,   // X / CX
+    OP_DIAG = 4,   // diag(m00, m11)
+    OP_DIAG1 = 5,  // diag(1, m11)
+};
+
+constexpr uint8_t NO_SLOT = 0xFF;
 
 template <typename T>
 struct FOp
 {
-    int32_t kind;        // KIND_GEN / KIND_DIAG / KIND_ANTI
-    int32_t tslot;       // GEN/ANTI: register slot of the target; DIAG: tile bit of the target or -1
-    uint32_t cmask_loc;  // control as tile bits
-    int32_t flags;       // bit0: DIAG with m00 == 1
-    uint64_t cmask_glob; // control as global bits (outside the tile)
-    uint64_t tglob;      // DIAG target outside the tile: its global bit
+    uint8_t kind;
+    uint8_t tslot;    // register slot of the target (NO_SLOT: the target is not a register bit)
+    uint16_t pad0;
+    uint32_t ract;    // registers whose in-register control holds (all ones when none)
+    uint32_t r1;      // diagonal gate on a register bit: registers whose target bit is 1
+    uint32_t cthr;    // control as thread-index bits (0: none)
+    uint32_t tthr;    // diagonal target as thread-index bits (0: none)
+    uint32_t pad1;
+    uint64_t cglob;   // control outside the tile (0: none)
+    uint64_t tglob;   // diagonal target outside the tile (0: none)
     T m[8];
 };
 
 struct FPhase
 {
-    int8_t slot_bit[KMAX];  // slot -> tile bit; slots [0, RB) are register bits, [RB, K) thread bits
-    int16_t pad;
+    uint64_t rstride[RBMAX];   // global stride of each register slot
+    uint64_t tstride[TBMAX];   // global stride of each thread-index bit
+    uint32_t rsw[RBMAX];       // swizzled shared-memory term of each register slot
+    uint32_t tsw[TBMAX];       // swizzled shared-memory term of each thread-index bit
     int32_t op_begin;
     int32_t op_end;
 };
@@ -63,59 +89,58 @@ struct FBlock
     int32_t nfree;
     int32_t phase_begin;
     int32_t phase_end;
+    int32_t op_begin;
+    int32_t op_end;
     int32_t qubit[KMAX];    // tile bit -> qubit
     int32_t freebit[64];    // qubits outside the tile, ascending
 };
 
-// tile bit configuration per amplitude type
+// tile configuration per amplitude type
 template <typename T>
 struct Cfg;
 template <>
 struct Cfg<double>
 {
     static constexpr int RB = 4;     // 16 amplitudes per thread
-    static constexpr int TBMAX = 8;  // 256 threads
     static constexpr int L = 3;      // 8 x 16 B = 128 B runs
-    static constexpr int LANES = 3;  // lane bits that must differ in residue (16-B smem accesses)
+    static constexpr int G = 3;      // swizzle group (16-byte elements: 8 per 128-byte bank row)
 };
 template <>
 struct Cfg<float>
 {
     static constexpr int RB = 5;     // 32 amplitudes per thread
-    static constexpr int TBMAX = 8;
     static constexpr int L = 4;      // 16 x 8 B = 128 B runs
-    static constexpr int LANES = 4;
+    static constexpr int G = 4;      // 8-byte elements: 16 per bank row
 };
 
-// XOR swizzle of a tile index for bank-conflict-free transposes: the low G bits
-// are XORed with a fold of the higher bits (G = 3 for 16-byte, 4 for 8-byte elements).
-template <int G>
-__device__ __forceinline__ uint32_t swz(uint32_t l)
+// XOR swizzle: the low G bits are XORed with a fold of the higher bits.  It is
+// linear over GF(2), so swz(a ^ b) = swz(a) ^ swz(b).
+__host__ __device__ inline uint32_t swz(uint32_t l, int G)
 {
     uint32_t f = 0;
-#pragma unroll
     for (int s = G; s < 32; s += G) {
         f ^= l >> s;
     }
     return l ^ (f & ((1u << G) - 1));
 }
 
-template <int RB>
-__device__ __forceinline__ uint32_t rloc(int i, const uint32_t (&rbit)[RB])
+template <int RB, typename U>
+__device__ __forceinline__ U xor_terms(int i, const U (&terms)[RBMAX])
 {
-    uint32_t l = 0;
+    U a = 0;
 #pragma unroll
     for (int s = 0; s < RB; ++s) {
         if (i & (1 << s)) {
-            l |= rbit[s];
+            a ^= terms[s];
         }
     }
-    return l;
+    return a;
 }
 
-template <typename C, int RB, int S>
+// --- register-level gate bodies -------------------------------------------------
+template <typename C, int RB, int S, bool MASKED>
 __device__ __forceinline__ void gen_pairs(C (&v)[1 << RB], const C m00, const C m01, const C m10, const C m11,
-                                          uint32_t tloc, const uint32_t (&rbit)[RB], uint32_t cm)
+                                          uint32_t ract)
 {
 #pragma unroll
     for (int i = 0; i < (1 << RB); ++i) {
@@ -123,8 +148,7 @@ __device__ __forceinline__ void gen_pairs(C (&v)[1 << RB], const C m00, const C 
             continue;
         }
         const int j = i | (1 << S);
-        const uint32_t l = tloc | rloc<RB>(i, rbit);
-        if ((l & cm) == cm) {
+        if (!MASKED || ((ract >> i) & 1u)) {
             const C a = v[i];
             const C b = v[j];
             v[i] = cfma(m01, b, cmul(m00, a));
@@ -133,9 +157,9 @@ __device__ __forceinline__ void gen_pairs(C (&v)[1 << RB], const C m00, const C 
     }
 }
 
-template <typename C, int RB, int S>
-__device__ __forceinline__ void anti_pairs(C (&v)[1 << RB], const C m01, const C m10, bool pure_swap, uint32_t tloc,
-                                           const uint32_t (&rbit)[RB], uint32_t cm)
+template <typename C, typename T, int RB, int S, bool MASKED>
+__device__ __forceinline__ void genr_pairs(C (&v)[1 << RB], const T m00, const T m01, const T m10, const T m11,
+                                           uint32_t ract)
 {
 #pragma unroll
     for (int i = 0; i < (1 << RB); ++i) {
@@ -143,11 +167,33 @@ __device__ __forceinline__ void anti_pairs(C (&v)[1 << RB], const C m01, const C
             continue;
         }
         const int j = i | (1 << S);
-        const uint32_t l = tloc | rloc<RB>(i, rbit);
-        if ((l & cm) == cm) {
+        if (!MASKED || ((ract >> i) & 1u)) {
             const C a = v[i];
             const C b = v[j];
-            if (pure_swap) {
+            C x, y;
+            x.x = fma(m01, b.x, m00 * a.x);
+            x.y = fma(m01, b.y, m00 * a.y);
+            y.x = fma(m11, b.x, m10 * a.x);
+            y.y = fma(m11, b.y, m10 * a.y);
+            v[i] = x;
+            v[j] = y;
+        }
+    }
+}
+
+template <typename C, int RB, int S, bool MASKED, bool PURE>
+__device__ __forceinline__ void anti_pairs(C (&v)[1 << RB], const C m01, const C m10, uint32_t ract)
+{
+#pragma unroll
+    for (int i = 0; i < (1 << RB); ++i) {
+        if (i & (1 << S)) {
+            continue;
+        }
+        const int j = i | (1 << S);
+        if (!MASKED || ((ract >> i) & 1u)) {
+            const C a = v[i];
+            const C b = v[j];
+            if (PURE) {
                 v[i] = b;
                 v[j] = a;
             } else {
@@ -158,150 +204,160 @@ __device__ __forceinline__ void anti_pairs(C (&v)[1 << RB], const C m01, const C
     }
 }
 
+#define KT_SLOT_SWITCH(RB, SLOT, CALL)                           \
+    switch (SLOT) {                                              \
+        case 0: { constexpr int S_ = 0; CALL; } break;           \
+        case 1: { constexpr int S_ = 1; CALL; } break;           \
+        case 2: { constexpr int S_ = 2; CALL; } break;           \
+        case 3: { constexpr int S_ = 3; CALL; } break;           \
+        default:                                                 \
+            if constexpr (RB > 4) {                              \
+                constexpr int S_ = (RB > 4) ? 4 : 0;             \
+                CALL;                                            \
+            }                                                    \
+            break;                                               \
+    }
+
 template <typename T, int RB>
-__device__ __forceinline__ void apply_op(typename CxT<T>::type (&v)[1 << RB], const FOp<T>* __restrict__ opp,
-                                         uint32_t tloc, const uint32_t (&rbit)[RB], uint64_t base)
+__device__ __forceinline__ void apply_op(typename CxT<T>::type (&v)[1 << RB], const FOp<T>& op, uint32_t t,
+                                         uint64_t base)
 {
     using C = typename CxT<T>::type;
-    const int kind = opp->kind;
-    const uint64_t cg = opp->cmask_glob;
-    if ((base & cg) != cg) {
-        return;  // control outside the tile is 0 for this whole tile
+    constexpr uint32_t ALL = (RB >= 5) ? 0xFFFFFFFFu : ((1u << (1 << RB)) - 1u);
+    if ((base & op.cglob) != op.cglob) {
+        return;  // control outside the tile is 0 for the whole tile
     }
-    const uint32_t cm = opp->cmask_loc;
-    const int ts = opp->tslot;
-    if (kind == KIND_DIAG) {
-        const C d0 = make_cx<T>(opp->m[0], opp->m[1]);
-        const C d1 = make_cx<T>(opp->m[6], opp->m[7]);
-        const bool one = opp->flags & 1;
-        const uint64_t tg = opp->tglob;
-        if (ts < 0) {
-            // target outside the tile: one factor for the whole tile
-            const bool b = (base & tg) != 0;
-            if (!b && one) {
-                return;
-            }
-            const C d = b ? d1 : d0;
+    if ((t & op.cthr) != op.cthr) {
+        return;  // control on a thread bit is 0 for this thread
+    }
+    const uint32_t ract = op.ract;
+    const bool masked = ract != ALL;
+    const int kind = op.kind;
+    const int ts = op.tslot;
+    if (kind >= OP_DIAG) {
+        const C d1 = make_cx<T>(op.m[6], op.m[7]);
+        if (ts != NO_SLOT) {
+            const uint32_t on1 = ract & op.r1;
+            const uint32_t on0 = ract & ~op.r1;
+            if (kind == OP_DIAG1) {
 #pragma unroll
-            for (int i = 0; i < (1 << RB); ++i) {
-                const uint32_t l = tloc | rloc<RB>(i, rbit);
-                if ((l & cm) == cm) {
-                    v[i] = cmul(d, v[i]);
+                for (int i = 0; i < (1 << RB); ++i) {
+                    if ((on1 >> i) & 1u) {
+                        v[i] = cmul(d1, v[i]);
+                    }
+                }
+            } else {
+                const C d0 = make_cx<T>(op.m[0], op.m[1]);
+#pragma unroll
+                for (int i = 0; i < (1 << RB); ++i) {
+                    if ((on1 >> i) & 1u) {
+                        v[i] = cmul(d1, v[i]);
+                    } else if ((on0 >> i) & 1u) {
+                        v[i] = cmul(d0, v[i]);
+                    }
                 }
             }
             return;
         }
+        // target is a thread bit or outside the tile: one factor for all of this thread's registers
+        const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
+        if (!b && kind == OP_DIAG1) {
+            return;
+        }
+        const C d = b ? d1 : make_cx<T>(op.m[0], op.m[1]);
+        if (!masked) {
 #pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            const uint32_t l = tloc | rloc<RB>(i, rbit);
-            if ((l & cm) == cm) {
-                if ((l >> ts) & 1) {
-                    v[i] = cmul(d1, v[i]);
-                } else if (!one) {
-                    v[i] = cmul(d0, v[i]);
+            for (int i = 0; i < (1 << RB); ++i) {
+                v[i] = cmul(d, v[i]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < (1 << RB); ++i) {
+                if ((ract >> i) & 1u) {
+                    v[i] = cmul(d, v[i]);
                 }
             }
         }
         return;
     }
-    const C m01 = make_cx<T>(opp->m[2], opp->m[3]);
-    const C m10 = make_cx<T>(opp->m[4], opp->m[5]);
-    if (kind == KIND_ANTI) {
-        const bool pure = opp->flags & 2;
-        switch (ts) {
-            case 0: anti_pairs<C, RB, 0>(v, m01, m10, pure, tloc, rbit, cm); break;
-            case 1: anti_pairs<C, RB, 1>(v, m01, m10, pure, tloc, rbit, cm); break;
-            case 2: anti_pairs<C, RB, 2>(v, m01, m10, pure, tloc, rbit, cm); break;
-            case 3: anti_pairs<C, RB, 3>(v, m01, m10, pure, tloc, rbit, cm); break;
-            default:
-                if constexpr (RB > 4) {
-                    anti_pairs<C, RB, (RB > 4 ? 4 : 0)>(v, m01, m10, pure, tloc, rbit, cm);
-                }
-                break;
+    if (kind == OP_SWAP) {
+        const C z = make_cx<T>(0, 0);
+        if (masked) {
+            KT_SLOT_SWITCH(RB, ts, (anti_pairs<C, RB, S_, true, true>(v, z, z, ract)))
+        } else {
+            KT_SLOT_SWITCH(RB, ts, (anti_pairs<C, RB, S_, false, true>(v, z, z, ract)))
         }
         return;
     }
-    const C m00 = make_cx<T>(opp->m[0], opp->m[1]);
-    const C m11 = make_cx<T>(opp->m[6], opp->m[7]);
-    switch (ts) {
-        case 0: gen_pairs<C, RB, 0>(v, m00, m01, m10, m11, tloc, rbit, cm); break;
-        case 1: gen_pairs<C, RB, 1>(v, m00, m01, m10, m11, tloc, rbit, cm); break;
-        case 2: gen_pairs<C, RB, 2>(v, m00, m01, m10, m11, tloc, rbit, cm); break;
-        case 3: gen_pairs<C, RB, 3>(v, m00, m01, m10, m11, tloc, rbit, cm); break;
-        default:
-            if constexpr (RB > 4) {
-                gen_pairs<C, RB, (RB > 4 ? 4 : 0)>(v, m00, m01, m10, m11, tloc, rbit, cm);
-            }
-            break;
-    }
-}
-
-// register-bit strides (global) and the thread offset of a layout
-template <int RB>
-__device__ __forceinline__ void layout_global(const FPhase& ph, const FBlock& bk, int K, uint32_t t,
-                                              uint64_t (&rstride)[RB], uint64_t& toff)
-{
-#pragma unroll
-    for (int s = 0; s < RB; ++s) {
-        rstride[s] = uint64_t {1} << bk.qubit[ph.slot_bit[s]];
-    }
-    toff = 0;
-    for (int s = RB; s < K; ++s) {
-        if ((t >> (s - RB)) & 1) {
-            toff |= uint64_t {1} << bk.qubit[ph.slot_bit[s]];
+    if (kind == OP_ANTI) {
+        const C m01 = make_cx<T>(op.m[2], op.m[3]);
+        const C m10 = make_cx<T>(op.m[4], op.m[5]);
+        if (masked) {
+            KT_SLOT_SWITCH(RB, ts, (anti_pairs<C, RB, S_, true, false>(v, m01, m10, ract)))
+        } else {
+            KT_SLOT_SWITCH(RB, ts, (anti_pairs<C, RB, S_, false, false>(v, m01, m10, ract)))
         }
+        return;
     }
-}
-
-template <int RB>
-__device__ __forceinline__ void layout_local(const FPhase& ph, int K, uint32_t t, uint32_t (&rbit)[RB], uint32_t& tloc)
-{
-#pragma unroll
-    for (int s = 0; s < RB; ++s) {
-        rbit[s] = 1u << ph.slot_bit[s];
-    }
-    tloc = 0;
-    for (int s = RB; s < K; ++s) {
-        if ((t >> (s - RB)) & 1) {
-            tloc |= 1u << ph.slot_bit[s];
+    if (kind == OP_GENR) {
+        const T a00 = op.m[0], a01 = op.m[2], a10 = op.m[4], a11 = op.m[6];
+        if (masked) {
+            KT_SLOT_SWITCH(RB, ts, (genr_pairs<C, T, RB, S_, true>(v, a00, a01, a10, a11, ract)))
+        } else {
+            KT_SLOT_SWITCH(RB, ts, (genr_pairs<C, T, RB, S_, false>(v, a00, a01, a10, a11, ract)))
         }
+        return;
+    }
+    const C m00 = make_cx<T>(op.m[0], op.m[1]);
+    const C m01 = make_cx<T>(op.m[2], op.m[3]);
+    const C m10 = make_cx<T>(op.m[4], op.m[5]);
+    const C m11 = make_cx<T>(op.m[6], op.m[7]);
+    if (masked) {
+        KT_SLOT_SWITCH(RB, ts, (gen_pairs<C, RB, S_, true>(v, m00, m01, m10, m11, ract)))
+    } else {
+        KT_SLOT_SWITCH(RB, ts, (gen_pairs<C, RB, S_, false>(v, m00, m01, m10, m11, ract)))
     }
 }
 
-template <int RB>
-__device__ __forceinline__ uint64_t roff(int i, const uint64_t (&rstride)[RB])
-{
-    uint64_t o = 0;
-#pragma unroll
-    for (int s = 0; s < RB; ++s) {
-        if (i & (1 << s)) {
-            o |= rstride[s];
-        }
-    }
-    return o;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256, 2) k_fused(typename CxT<T>::type* __restrict__ a, const FBlock* __restrict__ blk,
+// MINB: CTAs per SM the register budget is sized for (2: <= 128 registers,
+// 1: the compiler's natural allocation); chosen per run by the tuning table.
+template <typename T, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_fused(typename CxT<T>::type* __restrict__ a, const FBlock* __restrict__ blk,
                                                   const FPhase* __restrict__ phases, const FOp<T>* __restrict__ ops,
                                                   uint64_t n_tiles)
 {
     using C = typename CxT<T>::type;
     constexpr int RB = Cfg<T>::RB;
     constexpr int R = 1 << RB;
-    constexpr int G = (sizeof(C) == 16) ? 3 : 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* sm = reinterpret_cast<C*>(smem_raw);
 
     __shared__ FBlock bk;
-    if (threadIdx.x == 0) {
+    __shared__ FPhase sph[MAX_PHASES_PER_BLOCK];
+    const uint32_t t = threadIdx.x;
+    if (t == 0) {
         bk = *blk;
     }
     __syncthreads();
     const int K = bk.K;
-    const uint32_t t = threadIdx.x;
-    const int pb = bk.phase_begin;
-    const int pe = bk.phase_end;
+    const int TB = K - RB;
+    const int np = bk.phase_end - bk.phase_begin;
+    const int no = bk.op_end - bk.op_begin;
+    C* sm = reinterpret_cast<C*>(smem_raw);
+    FOp<T>* sops = reinterpret_cast<FOp<T>*>(smem_raw + (sizeof(C) << K));
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(phases + bk.phase_begin);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(sph);
+        for (int w = t; w < np * static_cast<int>(sizeof(FPhase) / 4); w += blockDim.x) {
+            dst[w] = src[w];
+        }
+        const uint32_t* so = reinterpret_cast<const uint32_t*>(ops + bk.op_begin);
+        uint32_t* dop = reinterpret_cast<uint32_t*>(sops);
+        for (int w = t; w < no * static_cast<int>(sizeof(FOp<T>) / 4); w += blockDim.x) {
+            dop[w] = so[w];
+        }
+    }
+    __syncthreads();
+    const int op0 = bk.op_begin;
 
     for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         uint64_t base = 0;
@@ -312,49 +368,73 @@ __global__ void __launch_bounds__(256, 2) k_fused(typename CxT<T>::type* __restr
         }
         C v[R];
         {
-            const FPhase ph = phases[pb];
-            uint64_t rs[RB];
-            uint64_t toff;
-            layout_global<RB>(ph, bk, K, t, rs, toff);
+            const FPhase& ph = sph[0];
+            uint64_t toff = 0;
+            for (int j = 0; j < TB; ++j) {
+                if ((t >> j) & 1) {
+                    toff += ph.tstride[j];
+                }
+            }
             const C* src = a + base + toff;
 #pragma unroll
             for (int i = 0; i < R; ++i) {
-                v[i] = src[roff<RB>(i, rs)];
+                uint64_t o = 0;
+#pragma unroll
+                for (int s = 0; s < RB; ++s) {
+                    if (i & (1 << s)) {
+                        o += ph.rstride[s];
+                    }
+                }
+                v[i] = src[o];
             }
         }
-        uint32_t rbit[RB];
-        uint32_t tloc;
-        for (int p = pb; p < pe; ++p) {
-            const FPhase ph = phases[p];
-            if (p > pb) {
-                // transpose: registers (old layout) -> smem -> registers (new layout)
-#pragma unroll
-                for (int i = 0; i < R; ++i) {
-                    sm[swz<G>(tloc | rloc<RB>(i, rbit))] = v[i];
+        uint32_t tsw_prev = 0;
+        for (int p = 0; p < np; ++p) {
+            const FPhase& ph = sph[p];
+            uint32_t tsw = 0;
+            for (int j = 0; j < TB; ++j) {
+                if ((t >> j) & 1) {
+                    tsw ^= ph.tsw[j];
                 }
-                __syncthreads();
-                layout_local<RB>(ph, K, t, rbit, tloc);
-#pragma unroll
-                for (int i = 0; i < R; ++i) {
-                    v[i] = sm[swz<G>(tloc | rloc<RB>(i, rbit))];
-                }
-                __syncthreads();
-            } else {
-                layout_local<RB>(ph, K, t, rbit, tloc);
             }
+            if (p > 0) {
+                // transpose: registers (previous layout) -> smem -> registers (this layout)
+                const FPhase& pp = sph[p - 1];
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    sm[tsw_prev ^ xor_terms<RB>(i, pp.rsw)] = v[i];
+                }
+                __syncthreads();
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    v[i] = sm[tsw ^ xor_terms<RB>(i, ph.rsw)];
+                }
+                __syncthreads();
+            }
+            tsw_prev = tsw;
             for (int o = ph.op_begin; o < ph.op_end; ++o) {
-                apply_op<T, RB>(v, ops + o, tloc, rbit, base);
+                apply_op<T, RB>(v, sops[o - op0], t, base);
             }
         }
         {
-            const FPhase ph = phases[pe - 1];
-            uint64_t rs[RB];
-            uint64_t toff;
-            layout_global<RB>(ph, bk, K, t, rs, toff);
+            const FPhase& ph = sph[np - 1];
+            uint64_t toff = 0;
+            for (int j = 0; j < TB; ++j) {
+                if ((t >> j) & 1) {
+                    toff += ph.tstride[j];
+                }
+            }
             C* dst = a + base + toff;
 #pragma unroll
             for (int i = 0; i < R; ++i) {
-                dst[roff<RB>(i, rs)] = v[i];
+                uint64_t o = 0;
+#pragma unroll
+                for (int s = 0; s < RB; ++s) {
+                    if (i & (1 << s)) {
+                        o += ph.rstride[s];
+                    }
+                }
+                dst[o] = v[i];
             }
         }
     }
@@ -378,7 +458,7 @@ uint64_t bit(int q)
 // Greedy block formation: in circuit order, take each gate that does not
 // share a qubit with a gate skipped before it and whose target (when it must
 // be in the tile) fits in the K-qubit set.
-std::vector<PlanBlock> form_blocks(const std::vector<LGate>& g, int n, int K, int L)
+std::vector<PlanBlock> form_blocks(const std::vector<LGate>& g, int n, int K, int L, size_t max_ops)
 {
     std::vector<PlanBlock> out;
     std::vector<int> pend(g.size());
@@ -394,7 +474,7 @@ std::vector<PlanBlock> form_blocks(const std::vector<LGate>& g, int n, int K, in
             const int idx = pend[k];
             const LGate& x = g[idx];
             const uint64_t touch = bit(x.target) | (x.control >= 0 ? bit(x.control) : 0);
-            if ((touch & blocked) != 0 || take.size() >= static_cast<size_t>(MAX_OPS_PER_BLOCK)) {
+            if ((touch & blocked) != 0 || take.size() >= max_ops) {
                 blocked |= touch;
                 rest.push_back(idx);
             } else {
@@ -430,14 +510,11 @@ std::vector<PlanBlock> form_blocks(const std::vector<LGate>& g, int n, int K, in
     return out;
 }
 
-struct Layout
-{
-    std::vector<int> regs;   // RB tile bits
-};
-
-// Thread-slot order: lanes first (distinct residues mod LANES, preferring the
-// low tile bits, which are the contiguous qubits), then the remaining bits.
-void make_slots(const std::vector<int>& regs, int K, int LANES, int8_t* slot_bit)
+// Slot order of a layout: register bits, then the lane bits (distinct
+// residues mod G so a quarter/half warp hits distinct shared-memory banks;
+// the L lowest tile bits when none of them is a register bit, which also
+// makes global accesses coalesced), then the remaining thread bits.
+void make_slots(const std::vector<int>& regs, int K, int G, int8_t* slot_bit)
 {
     std::vector<bool> is_reg(K, false);
     for (int r : regs) {
@@ -449,24 +526,23 @@ void make_slots(const std::vector<int>& regs, int K, int LANES, int8_t* slot_bit
     }
     std::vector<int> lanes;
     std::vector<bool> used(K, false);
-    // prefer tile bits 0..LANES-1 when none is a register bit
     bool low_free = true;
-    for (int b = 0; b < LANES; ++b) {
+    for (int b = 0; b < G; ++b) {
         low_free = low_free && !is_reg[b];
     }
     if (low_free) {
-        for (int b = 0; b < LANES; ++b) {
+        for (int b = 0; b < G; ++b) {
             lanes.push_back(b);
         }
     } else {
-        std::vector<bool> res_used(LANES, false);
-        for (int b = 0; b < K && static_cast<int>(lanes.size()) < LANES; ++b) {
-            if (!is_reg[b] && !res_used[b % LANES]) {
-                res_used[b % LANES] = true;
+        std::vector<bool> res_used(G, false);
+        for (int b = 0; b < K && static_cast<int>(lanes.size()) < G; ++b) {
+            if (!is_reg[b] && !res_used[b % G]) {
+                res_used[b % G] = true;
                 lanes.push_back(b);
             }
         }
-        for (int b = 0; b < K && static_cast<int>(lanes.size()) < LANES; ++b) {
+        for (int b = 0; b < K && static_cast<int>(lanes.size()) < G; ++b) {
             if (!is_reg[b] && std::find(lanes.begin(), lanes.end(), b) == lanes.end()) {
                 lanes.push_back(b);
             }
@@ -497,7 +573,8 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>
 {
     constexpr int RB = Cfg<T>::RB;
     constexpr int L = Cfg<T>::L;
-    constexpr int LANES = Cfg<T>::LANES;
+    constexpr int G = Cfg<T>::G;
+    constexpr uint32_t ALL = (RB >= 5) ? 0xFFFFFFFFu : ((1u << (1 << RB)) - 1u);
     const int K = pb.K;
     std::vector<int> loc(n, -1);
     for (int j = 0; j < K; ++j) {
@@ -515,7 +592,7 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>
             fb.freebit[nf++] = q;
         }
     }
-    // ops and the register bit each needs (-1 = none)
+    // the tile bit each gate needs as a register bit (-1 = none)
     const size_t m = pb.gates.size();
     std::vector<int> need(m, -1);
     for (size_t k = 0; k < m; ++k) {
@@ -533,7 +610,8 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>
         return SIZE_MAX;
     };
     // register set for a phase starting at `from`: the RB needed bits used
-    // soonest, then (to keep the load/store layout coalesced) bits >= L.
+    // soonest, then current bits by next use, then bits >= L (keeps the
+    // load/store layout coalesced)
     auto choose = [&](size_t from, const std::vector<int>& keep) -> std::vector<int> {
         std::vector<int> regs;
         for (size_t k = from; k < m && static_cast<int>(regs.size()) < RB; ++k) {
@@ -566,74 +644,123 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>
         std::sort(regs.begin(), regs.end());
         return regs;
     };
-    std::vector<std::pair<std::vector<int>, std::pair<size_t, size_t>>> ph;  // (regs, [begin, end))
+    struct PhaseSpec
+    {
+        std::vector<int> regs;
+        size_t begin, end;
+    };
+    std::vector<PhaseSpec> ph;
     std::vector<int> cur = choose(0, {});
     if (has_low(cur)) {
-        ph.push_back({io_regs(), {0, 0}});
+        ph.push_back({io_regs(), 0, 0});
     }
     size_t start = 0;
     for (size_t k = 0; k < m; ++k) {
         if (need[k] >= 0 && std::find(cur.begin(), cur.end(), need[k]) == cur.end()) {
-            ph.push_back({cur, {start, k}});
-            // keep the current bits whose next use is soonest as fillers
+            ph.push_back({cur, start, k});
             std::vector<int> keep = cur;
             std::sort(keep.begin(), keep.end(), [&](int x, int y) { return next_use(x, k) < next_use(y, k); });
             cur = choose(k, keep);
             start = k;
         }
     }
-    ph.push_back({cur, {start, m}});
+    ph.push_back({cur, start, m});
     if (has_low(cur)) {
-        ph.push_back({io_regs(), {m, m}});
+        ph.push_back({io_regs(), m, m});
     }
-    // emit
+    // phases
+    const int TB = K - RB;
+    const size_t op_base = plan.ops.size();
     fb.phase_begin = static_cast<int32_t>(plan.phases.size());
-    for (auto& [regs, range] : ph) {
+    std::vector<std::vector<int8_t>> slots;
+    for (auto& spec : ph) {
+        int8_t sb[KMAX] = {};
+        make_slots(spec.regs, K, G, sb);
+        slots.emplace_back(sb, sb + K);
         FPhase fp {};
-        make_slots(regs, K, LANES, fp.slot_bit);
-        fp.op_begin = static_cast<int32_t>(plan.ops.size() + range.first);
-        fp.op_end = static_cast<int32_t>(plan.ops.size() + range.second);
+        for (int s = 0; s < RB; ++s) {
+            fp.rstride[s] = bit(pb.qubits[sb[s]]);
+            fp.rsw[s] = swz(1u << sb[s], G);
+        }
+        for (int j = 0; j < TB; ++j) {
+            fp.tstride[j] = bit(pb.qubits[sb[RB + j]]);
+            fp.tsw[j] = swz(1u << sb[RB + j], G);
+        }
+        fp.op_begin = static_cast<int32_t>(op_base + spec.begin);
+        fp.op_end = static_cast<int32_t>(op_base + spec.end);
         plan.phases.push_back(fp);
     }
     fb.phase_end = static_cast<int32_t>(plan.phases.size());
     plan.transposes += static_cast<int>(ph.size()) - 1;
-    // ops (in block order, with the register slot of the target in its phase)
+    // ops, resolved against the layout of their phase
     size_t pi = 0;
     for (size_t k = 0; k < m; ++k) {
-        while (!(k >= ph[pi].second.first && k < ph[pi].second.second)) {
+        while (!(k >= ph[pi].begin && k < ph[pi].end)) {
             ++pi;
         }
+        const auto& sb = slots[pi];
+        auto reg_slot = [&](int tilebit) -> int {
+            for (int s = 0; s < RB; ++s) {
+                if (sb[s] == tilebit) return s;
+            }
+            return -1;
+        };
+        auto thread_bit = [&](int tilebit) -> int {
+            for (int j = 0; j < TB; ++j) {
+                if (sb[RB + j] == tilebit) return j;
+            }
+            return -1;
+        };
         const LGate& x = g[pb.gates[k]];
         FOp<T> op {};
-        op.kind = x.kind;
-        op.flags = x.flags & 1;
-        if (x.kind == KIND_ANTI && x.m[2] == 1.0 && x.m[3] == 0.0 && x.m[4] == 1.0 && x.m[5] == 0.0) {
-            op.flags |= 2;  // pure swap (X / CX)
-        }
+        op.tslot = NO_SLOT;
+        op.ract = ALL;
         if (x.control >= 0) {
-            if (loc[x.control] >= 0) {
-                op.cmask_loc = 1u << loc[x.control];
+            const int lc = loc[x.control];
+            if (lc < 0) {
+                op.cglob = bit(x.control);
+            } else if (const int s = reg_slot(lc); s >= 0) {
+                uint32_t mask = 0;
+                for (int i = 0; i < (1 << RB); ++i) {
+                    if ((i >> s) & 1) mask |= 1u << i;
+                }
+                op.ract = mask;
             } else {
-                op.cmask_glob = bit(x.control);
+                op.cthr = 1u << thread_bit(lc);
             }
         }
+        const bool real = x.m[1] == 0.0 && x.m[3] == 0.0 && x.m[5] == 0.0 && x.m[7] == 0.0;
         if (x.kind == KIND_DIAG) {
-            if (loc[x.target] >= 0) {
-                op.tslot = loc[x.target];
-            } else {
-                op.tslot = -1;
+            op.kind = (x.flags & 1) ? OP_DIAG1 : OP_DIAG;
+            const int lt = loc[x.target];
+            if (lt < 0) {
                 op.tglob = bit(x.target);
+            } else if (const int s = reg_slot(lt); s >= 0) {
+                op.tslot = static_cast<uint8_t>(s);
+                uint32_t mask = 0;
+                for (int i = 0; i < (1 << RB); ++i) {
+                    if ((i >> s) & 1) mask |= 1u << i;
+                }
+                op.r1 = mask;
+            } else {
+                op.tthr = 1u << thread_bit(lt);
             }
         } else {
-            const auto& regs = ph[pi].first;
-            const auto it = std::find(regs.begin(), regs.end(), loc[x.target]);
-            op.tslot = static_cast<int32_t>(it - regs.begin());  // regs are slots 0..RB-1 in order
+            op.tslot = static_cast<uint8_t>(reg_slot(loc[x.target]));
+            if (x.kind == KIND_ANTI) {
+                const bool pure = x.m[2] == 1.0 && x.m[3] == 0.0 && x.m[4] == 1.0 && x.m[5] == 0.0;
+                op.kind = pure ? OP_SWAP : OP_ANTI;
+            } else {
+                op.kind = real ? OP_GENR : OP_GEN;
+            }
         }
         for (int e = 0; e < 8; ++e) {
             op.m[e] = static_cast<T>(x.m[e]);
         }
         plan.ops.push_back(op);
     }
+    fb.op_begin = static_cast<int32_t>(op_base);
+    fb.op_end = static_cast<int32_t>(plan.ops.size());
     plan.blocks.push_back(fb);
 }
 
@@ -644,7 +771,8 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     constexpr int RB = Cfg<T>::RB;
     constexpr int L = Cfg<T>::L;
     const int n = s.n_bits;
-    const int K = std::min(n, RB + Cfg<T>::TBMAX);
+    const int k_pref = std::min(RB + TBMAX, tuning().fused_tile_bits + (RB - 4));
+    const int K = std::min(n, k_pref);
     if (n < RB + 5 || gates.empty()) {
         for (const auto& g : gates) {
             if (const int32_t rc = launch_gate_sweep(s, g); rc != KT_OK) {
@@ -653,10 +781,19 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
         }
         return KT_OK;
     }
-    const auto blocks = form_blocks(gates, n, K, L);
+    auto blocks = form_blocks(gates, n, K, L,
+                              static_cast<size_t>(std::min(MAX_OPS_PER_BLOCK, tuning().fused_max_ops)));
     Plan<T> plan;
     for (const auto& b : blocks) {
         plan_block<T>(b, gates, n, plan);
+    }
+    // a block with more phases than the kernel's table holds is split in two
+    // (never happens with MAX_OPS_PER_BLOCK ops and RB >= 4, checked here)
+    for (const auto& fb : plan.blocks) {
+        if (fb.phase_end - fb.phase_begin > MAX_PHASES_PER_BLOCK) {
+            set_error(KT_ERR_INVALID, "fused block planner produced too many phases");
+            return KT_ERR_INVALID;
+        }
     }
     // upload the plan: blocks | phases | ops
     auto al = [](size_t v) { return (v + 255) & ~size_t {255}; };
@@ -676,29 +813,39 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
         std::memcpy(host.data() + off_o, plan.ops.data(), plan.ops.size() * sizeof(FOp<T>));
     }
     char* dev = static_cast<char*>(s.scratch.ptr);
+    // pageable source: staged by the time the call returns, so `host` may go away
     KT_CUDA(cudaMemcpyAsync(dev, host.data(), need, cudaMemcpyHostToDevice, s.stream));
     const auto* d_blk = reinterpret_cast<const FBlock*>(dev);
     const auto* d_ph = reinterpret_cast<const FPhase*>(dev + off_p);
     const auto* d_ops = reinterpret_cast<const FOp<T>*>(dev + off_o);
     const int threads = 1 << (K - RB);
-    const size_t smem = (size_t {1} << K) * sizeof(C);
-    static bool attr_set = false;
-    if (!attr_set) {
-        KT_CUDA(cudaFuncSetAttribute(k_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
-        attr_set = true;
+    const int minb = tuning().fused_ctas_per_sm == 1 ? 1 : 2;
+    static bool attr_set[2] = {false, false};
+    if (!attr_set[minb - 1]) {
+        if (minb == 1) {
+            KT_CUDA(cudaFuncSetAttribute(k_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        } else {
+            KT_CUDA(cudaFuncSetAttribute(k_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        }
+        attr_set[minb - 1] = true;
     }
     const uint64_t n_tiles = uint64_t {1} << (n - K);
-    const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * 2);
+    const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * minb);
     const double pass_bytes = 2.0 * static_cast<double>(sizeof(C)) * static_cast<double>(s.n_amps());
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
-        k_fused<T><<<static_cast<unsigned>(grid), threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b, d_ph,
-                                                                            d_ops, n_tiles);
+        const auto& fb = plan.blocks[b];
+        const size_t smem = (size_t {1} << K) * sizeof(C) + static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOp<T>);
+        if (minb == 1) {
+            k_fused<T, 1><<<static_cast<unsigned>(grid), threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b,
+                                                                                   d_ph, d_ops, n_tiles);
+        } else {
+            k_fused<T, 2><<<static_cast<unsigned>(grid), threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b,
+                                                                                   d_ph, d_ops, n_tiles);
+        }
         KT_CHECK_LAUNCH("k_fused");
         s.last_launches += 1;
         s.last_alg_bytes += pass_bytes;
     }
-    // (the pageable host copy is staged by the time cudaMemcpyAsync returns,
-    // so `host` may go out of scope while the kernels run)
     return KT_OK;
 }
 

@@ -131,6 +131,18 @@ int32_t copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t st);
 constexpr int SM_COUNT_B200 = 148;
 int sm_count();
 
+// Launch-shape knobs chosen by the autotuner (kettle_b200/autotune.py) and
+// set through kt_tuning_set, or from KT_TUNING="name=value,..." at first use.
+struct Tuning
+{
+    int fused_ctas_per_sm {2};   // register budget of the fused kernel: 2 (<=128 regs) or 1
+    int fused_tile_bits {12};    // K for complex128 (complex64 uses K + 1), clamped to the kernel's range
+    int fused_max_ops {256};     // gates per fused block
+};
+Tuning& tuning();
+bool tuning_set(const char* name, long long value);
+bool tuning_get(const char* name, long long* value);
+
 }  // namespace kt
 
 // the opaque handles of the C-ABI

@@ -1,5 +1,7 @@
 // kt_lower.cpp — host side: error state, scratch buffers and gate lowering.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <sstream>
 
@@ -72,6 +74,74 @@ int sm_count()
         }
     }
     return cached;
+}
+
+namespace
+{
+
+bool set_knob(Tuning& t, const std::string& name, long long v)
+{
+    if (name == "fused_ctas_per_sm") {
+        t.fused_ctas_per_sm = (v == 1) ? 1 : 2;
+    } else if (name == "fused_tile_bits") {
+        t.fused_tile_bits = static_cast<int>(std::max(9LL, std::min(12LL, v)));
+    } else if (name == "fused_max_ops") {
+        t.fused_max_ops = static_cast<int>(std::max(1LL, std::min(256LL, v)));
+    } else {
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+Tuning& tuning()
+{
+    static Tuning t = [] {
+        Tuning d;
+        if (const char* env = std::getenv("KT_TUNING")) {
+            std::string s {env};
+            size_t pos = 0;
+            while (pos < s.size()) {
+                const size_t end = s.find(',', pos);
+                const std::string kv = s.substr(pos, end == std::string::npos ? std::string::npos : end - pos);
+                const size_t eq = kv.find('=');
+                if (eq != std::string::npos) {
+                    set_knob(d, kv.substr(0, eq), std::atoll(kv.c_str() + eq + 1));
+                }
+                if (end == std::string::npos) {
+                    break;
+                }
+                pos = end + 1;
+            }
+        }
+        return d;
+    }();
+    return t;
+}
+
+bool tuning_set(const char* name, long long value)
+{
+    return name != nullptr && set_knob(tuning(), name, value);
+}
+
+bool tuning_get(const char* name, long long* value)
+{
+    if (name == nullptr || value == nullptr) {
+        return false;
+    }
+    const std::string n {name};
+    const Tuning& t = tuning();
+    if (n == "fused_ctas_per_sm") {
+        *value = t.fused_ctas_per_sm;
+    } else if (n == "fused_tile_bits") {
+        *value = t.fused_tile_bits;
+    } else if (n == "fused_max_ops") {
+        *value = t.fused_max_ops;
+    } else {
+        return false;
+    }
+    return true;
 }
 
 int32_t copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t st)

@@ -1,0 +1,1336 @@
+// ket_b200.cpp — host implementation of the ket:: drop-in API over the C-ABI.
+#include "kettle/ket_b200.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <iomanip>
+#include <numeric>
+#include <sstream>
+
+namespace ket
+{
+
+namespace
+{
+
+void check(int32_t rc)
+{
+    if (rc != KT_OK) {
+        throw std::runtime_error {std::string {kt_last_error()}};
+    }
+}
+
+auto gate_name(Gate g) -> const char*
+{
+    static const char* names[] = {"H",   "X",   "Y",     "Z",  "S",     "SDAG", "T",     "TDAG", "SX",  "SXDAG", "RX",
+                                  "RY",  "RZ",  "P",     "CH", "CX",    "CY",   "CZ",    "CS",   "CSDAG", "CT",
+                                  "CTDAG", "CSX", "CSXDAG", "CRX", "CRY", "CRZ", "CP", "U", "CU", "M"};
+    return names[static_cast<int>(g)];
+}
+
+bool is_controlled(Gate g)
+{
+    return (g >= Gate::CH && g <= Gate::CP) || g == Gate::CU;
+}
+
+bool is_power_of_2(std::size_t v)
+{
+    return v > 0 && (v & (v - 1)) == 0;
+}
+
+void check_bitstring(const std::string& s)
+{
+    if (s.empty() || !std::all_of(s.begin(), s.end(), [](char c) { return c == '0' || c == '1'; })) {
+        throw std::runtime_error {"Received bitstring with inputs that aren't '0' or '1'\n"};
+    }
+}
+
+auto to_record(const GateInfo& gi, const param::ParameterDataMap& pmap) -> kt_gate
+{
+    kt_gate r {};
+    r.op = static_cast<uint8_t>(gi.gate);
+    r.param = -1;
+    if (gi.gate == Gate::M) {
+        r.target = static_cast<uint32_t>(gi.arg0);
+        r.control = static_cast<uint32_t>(gi.arg1);
+        return r;
+    }
+    if (is_controlled(gi.gate)) {
+        r.control = static_cast<uint32_t>(gi.arg0);
+        r.target = static_cast<uint32_t>(gi.arg1);
+    } else {
+        r.target = static_cast<uint32_t>(gi.arg0);
+    }
+    r.angle = gi.arg2;
+    if (gi.parameter) {
+        const auto it = pmap.find(*gi.parameter);
+        if (it == pmap.end() || !it->second.value) {
+            throw std::runtime_error {"ERROR: cannot perform simulation with an uninitialized parameter value.\n"};
+        }
+        r.angle = *it->second.value;
+    }
+    if (gi.unitary) {
+        const Matrix2X2& m = *gi.unitary;
+        const std::complex<double> e[4] = {m.elem00, m.elem01, m.elem10, m.elem11};
+        for (int i = 0; i < 4; ++i) {
+            r.u[2 * i] = e[i].real();
+            r.u[2 * i + 1] = e[i].imag();
+        }
+    }
+    return r;
+}
+
+auto make_prng(std::optional<int> seed) -> std::mt19937
+{
+    // ket::internal::get_prng_ (common/prng.cpp:9-19)
+    if (seed) {
+        return std::mt19937 {static_cast<std::mt19937::result_type>(seed.value())};
+    }
+    auto device = std::random_device {};
+    return std::mt19937 {device()};
+}
+
+}  // namespace
+
+// ---- matrices ------------------------------------------------------------------------
+
+auto conjugate_transpose(const Matrix2X2& m) -> Matrix2X2
+{
+    return {std::conj(m.elem00), std::conj(m.elem10), std::conj(m.elem01), std::conj(m.elem11)};
+}
+
+auto operator*(const Matrix2X2& a, const Matrix2X2& b) -> Matrix2X2
+{
+    return {a.elem00 * b.elem00 + a.elem01 * b.elem10, a.elem00 * b.elem01 + a.elem01 * b.elem11,
+            a.elem10 * b.elem00 + a.elem11 * b.elem10, a.elem10 * b.elem01 + a.elem11 * b.elem11};
+}
+
+auto almost_eq(const std::complex<double>& l, const std::complex<double>& r, double tol_sq) noexcept -> bool
+{
+    const double dr = l.real() - r.real();
+    const double di = l.imag() - r.imag();
+    return (dr * dr + di * di) < tol_sq;
+}
+
+auto almost_eq(const Matrix2X2& l, const Matrix2X2& r, double tol_sq) noexcept -> bool
+{
+    return almost_eq(l.elem00, r.elem00, tol_sq) && almost_eq(l.elem01, r.elem01, tol_sq) &&
+           almost_eq(l.elem10, r.elem10, tol_sq) && almost_eq(l.elem11, r.elem11, tol_sq);
+}
+
+namespace
+{
+constexpr double SQ12 = 0.70710678118654752440;
+}
+
+auto h_gate() noexcept -> Matrix2X2 { return {{SQ12, 0}, {SQ12, 0}, {SQ12, 0}, {-SQ12, 0}}; }
+auto x_gate() noexcept -> Matrix2X2 { return {{0, 0}, {1, 0}, {1, 0}, {0, 0}}; }
+auto y_gate() noexcept -> Matrix2X2 { return {{0, 0}, {0, -1}, {0, 1}, {0, 0}}; }
+auto z_gate() noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {-1, 0}}; }
+auto s_gate() noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {0, 1}}; }
+auto sdag_gate() noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {0, -1}}; }
+auto t_gate() noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {SQ12, SQ12}}; }
+auto tdag_gate() noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {SQ12, -SQ12}}; }
+auto sx_gate() noexcept -> Matrix2X2 { return {{0.5, 0.5}, {0.5, -0.5}, {0.5, -0.5}, {0.5, 0.5}}; }
+auto sxdag_gate() noexcept -> Matrix2X2 { return {{0.5, -0.5}, {0.5, 0.5}, {0.5, 0.5}, {0.5, -0.5}}; }
+auto rx_gate(double a) noexcept -> Matrix2X2
+{
+    const double c = std::cos(a / 2.0), s = std::sin(a / 2.0);
+    return {{c, 0}, {0, -s}, {0, -s}, {c, 0}};
+}
+auto ry_gate(double a) noexcept -> Matrix2X2
+{
+    const double c = std::cos(a / 2.0), s = std::sin(a / 2.0);
+    return {{c, 0}, {-s, 0}, {s, 0}, {c, 0}};
+}
+auto rz_gate(double a) noexcept -> Matrix2X2
+{
+    const double c = std::cos(a / 2.0), s = std::sin(a / 2.0);
+    return {{c, -s}, {0, 0}, {0, 0}, {c, s}};
+}
+auto p_gate(double a) noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {std::cos(a), std::sin(a)}}; }
+
+// ---- parameters ----------------------------------------------------------------------
+
+auto param::ParameterIdHash::operator()(const ParameterID& id) const noexcept -> std::size_t
+{
+    std::size_t out = 0;
+    for (const auto byte : id) {
+        out = (out * 31) ^ byte;
+    }
+    return out;
+}
+
+// ---- circuit ---------------------------------------------------------------------------
+
+QuantumCircuit::QuantumCircuit(std::size_t n_qubits, std::size_t n_bits)
+    : n_qubits_ {n_qubits}
+    , n_bits_ {n_bits}
+{}
+
+QuantumCircuit::QuantumCircuit(std::size_t n_qubits)
+    : n_qubits_ {n_qubits}
+    , n_bits_ {n_qubits}
+{}
+
+void QuantumCircuit::pop_back()
+{
+    if (elements_.empty()) {
+        throw std::runtime_error {"ERROR: called `pop_back()` on a `QuantumCircuit` instance with no circuit elements.\n"};
+    }
+    elements_.pop_back();
+}
+
+void QuantumCircuit::set_parameter_value(const param::ParameterID& id, double angle)
+{
+    if (!parameter_data_.contains(id)) {
+        throw std::out_of_range {"ERROR: no parameter found with the provided id.\n"};
+    }
+    parameter_data_[id].value = angle;
+}
+
+void QuantumCircuit::check_qubit_range_(std::size_t index, const char* qubit_name, const char* gate_name_s) const
+{
+    // circuit/circuit.cpp check_qubit_range_
+    if (index >= n_qubits_) {
+        std::stringstream err;
+        err << "The index for the " << qubit_name << " at which the '" << gate_name_s << "' gate is applied, is out of bounds.\n";
+        err << "n_qubits             = " << n_qubits_ << '\n';
+        err << "provided qubit index = " << index << '\n';
+        throw std::runtime_error {err.str()};
+    }
+}
+
+void QuantumCircuit::check_bit_range_(std::size_t bit_index) const
+{
+    if (bit_index >= n_bits_) {
+        std::stringstream err;
+        err << "The bit index at which the 'M' gate is applied, is out of bounds.\n";
+        err << "n_bits             = " << n_bits_ << '\n';
+        err << "provided bit index = " << bit_index << '\n';
+        throw std::runtime_error {err.str()};
+    }
+}
+
+auto QuantumCircuit::new_parameter_(std::optional<double> value) -> param::ParameterID
+{
+    // a fresh random 16-byte id (parameter/parameter.cpp, parameter_internal.hpp)
+    auto prng = make_prng(std::nullopt);
+    auto dist = std::uniform_int_distribution<int> {0, 255};
+    param::ParameterID id {};
+    for (auto& b : id) {
+        b = static_cast<std::uint8_t>(dist(prng));
+    }
+    std::stringstream name;
+    name << "theta" << parameter_count_++;
+    parameter_data_[id] = param::ParameterData {.value = value, .name = name.str(), .count = 1};
+    return id;
+}
+
+void QuantumCircuit::use_parameter_(const param::ParameterID& id)
+{
+    auto it = parameter_data_.find(id);
+    if (it != parameter_data_.end()) {
+        ++it->second.count;
+        return;
+    }
+    std::stringstream name;
+    name << "theta" << parameter_count_++;
+    parameter_data_[id] = param::ParameterData {.value = std::nullopt, .name = name.str(), .count = 1};
+}
+
+void QuantumCircuit::add_one_(Gate g, std::size_t target)
+{
+    check_qubit_range_(target, "qubit", gate_name(g));
+    elements_.push_back(GateInfo {g, target, 0, 0.0, std::nullopt, std::nullopt});
+}
+
+void QuantumCircuit::add_one_angle_(Gate g, std::size_t target, double angle)
+{
+    check_qubit_range_(target, "qubit", gate_name(g));
+    elements_.push_back(GateInfo {g, target, 0, angle, std::nullopt, std::nullopt});
+}
+
+auto QuantumCircuit::add_one_param_(Gate g, std::size_t target, double angle) -> param::ParameterID
+{
+    check_qubit_range_(target, "qubit", gate_name(g));
+    const auto id = new_parameter_(angle);
+    elements_.push_back(GateInfo {g, target, 0, 0.0, std::nullopt, id});
+    return id;
+}
+
+void QuantumCircuit::add_one_param_id_(Gate g, std::size_t target, const param::ParameterID& id)
+{
+    check_qubit_range_(target, "qubit", gate_name(g));
+    use_parameter_(id);
+    elements_.push_back(GateInfo {g, target, 0, 0.0, std::nullopt, id});
+}
+
+void QuantumCircuit::add_ctrl_(Gate g, std::size_t control, std::size_t target)
+{
+    check_qubit_range_(control, "control qubit", gate_name(g));
+    check_qubit_range_(target, "target qubit", gate_name(g));
+    elements_.push_back(GateInfo {g, control, target, 0.0, std::nullopt, std::nullopt});
+}
+
+void QuantumCircuit::add_ctrl_angle_(Gate g, std::size_t control, std::size_t target, double angle)
+{
+    check_qubit_range_(control, "control qubit", gate_name(g));
+    check_qubit_range_(target, "target qubit", gate_name(g));
+    elements_.push_back(GateInfo {g, control, target, angle, std::nullopt, std::nullopt});
+}
+
+auto QuantumCircuit::add_ctrl_param_(Gate g, std::size_t control, std::size_t target, double angle) -> param::ParameterID
+{
+    check_qubit_range_(control, "control qubit", gate_name(g));
+    check_qubit_range_(target, "target qubit", gate_name(g));
+    const auto id = new_parameter_(angle);
+    elements_.push_back(GateInfo {g, control, target, 0.0, std::nullopt, id});
+    return id;
+}
+
+void QuantumCircuit::add_ctrl_param_id_(Gate g, std::size_t control, std::size_t target, const param::ParameterID& id)
+{
+    check_qubit_range_(control, "control qubit", gate_name(g));
+    check_qubit_range_(target, "target qubit", gate_name(g));
+    use_parameter_(id);
+    elements_.push_back(GateInfo {g, control, target, 0.0, std::nullopt, id});
+}
+
+#define KET_DEF_ONE(name, G)                                                    \
+    void QuantumCircuit::add_##name##_gate(std::size_t t) { add_one_(Gate::G, t); } \
+    void QuantumCircuit::add_##name##_gate(const std::vector<std::size_t>& idx) \
+    {                                                                           \
+        for (auto t : idx) add_one_(Gate::G, t);                                \
+    }
+KET_DEF_ONE(h, H)
+KET_DEF_ONE(x, X)
+KET_DEF_ONE(y, Y)
+KET_DEF_ONE(z, Z)
+KET_DEF_ONE(s, S)
+KET_DEF_ONE(sdag, SDAG)
+KET_DEF_ONE(t, T)
+KET_DEF_ONE(tdag, TDAG)
+KET_DEF_ONE(sx, SX)
+KET_DEF_ONE(sxdag, SXDAG)
+#undef KET_DEF_ONE
+
+#define KET_DEF_ANGLE(name, G)                                                                              \
+    void QuantumCircuit::add_##name##_gate(std::size_t t, double a) { add_one_angle_(Gate::G, t, a); }     \
+    auto QuantumCircuit::add_##name##_gate(std::size_t t, double a, param::parameterized) -> param::ParameterID \
+    {                                                                                                       \
+        return add_one_param_(Gate::G, t, a);                                                               \
+    }                                                                                                       \
+    void QuantumCircuit::add_##name##_gate(std::size_t t, const param::ParameterID& id)                    \
+    {                                                                                                       \
+        add_one_param_id_(Gate::G, t, id);                                                                  \
+    }                                                                                                       \
+    void QuantumCircuit::add_##name##_gate(const std::vector<std::pair<std::size_t, double>>& pairs)       \
+    {                                                                                                       \
+        for (const auto& [t, a] : pairs) add_one_angle_(Gate::G, t, a);                                     \
+    }
+KET_DEF_ANGLE(rx, RX)
+KET_DEF_ANGLE(ry, RY)
+KET_DEF_ANGLE(rz, RZ)
+KET_DEF_ANGLE(p, P)
+#undef KET_DEF_ANGLE
+
+#define KET_DEF_CTRL(name, G)                                                                          \
+    void QuantumCircuit::add_##name##_gate(std::size_t c, std::size_t t) { add_ctrl_(Gate::G, c, t); } \
+    void QuantumCircuit::add_##name##_gate(const std::vector<std::pair<std::size_t, std::size_t>>& ps) \
+    {                                                                                                  \
+        for (const auto& [c, t] : ps) add_ctrl_(Gate::G, c, t);                                        \
+    }
+KET_DEF_CTRL(ch, CH)
+KET_DEF_CTRL(cx, CX)
+KET_DEF_CTRL(cy, CY)
+KET_DEF_CTRL(cz, CZ)
+KET_DEF_CTRL(cs, CS)
+KET_DEF_CTRL(csdag, CSDAG)
+KET_DEF_CTRL(ct, CT)
+KET_DEF_CTRL(ctdag, CTDAG)
+KET_DEF_CTRL(csx, CSX)
+KET_DEF_CTRL(csxdag, CSXDAG)
+#undef KET_DEF_CTRL
+
+#define KET_DEF_CTRL_ANGLE(name, G)                                                                                 \
+    void QuantumCircuit::add_##name##_gate(std::size_t c, std::size_t t, double a) { add_ctrl_angle_(Gate::G, c, t, a); } \
+    auto QuantumCircuit::add_##name##_gate(std::size_t c, std::size_t t, double a, param::parameterized)            \
+        -> param::ParameterID                                                                                       \
+    {                                                                                                               \
+        return add_ctrl_param_(Gate::G, c, t, a);                                                                   \
+    }                                                                                                               \
+    void QuantumCircuit::add_##name##_gate(std::size_t c, std::size_t t, const param::ParameterID& id)             \
+    {                                                                                                               \
+        add_ctrl_param_id_(Gate::G, c, t, id);                                                                      \
+    }                                                                                                               \
+    void QuantumCircuit::add_##name##_gate(const std::vector<std::tuple<std::size_t, std::size_t, double>>& ts)    \
+    {                                                                                                               \
+        for (const auto& [c, t, a] : ts) add_ctrl_angle_(Gate::G, c, t, a);                                         \
+    }
+KET_DEF_CTRL_ANGLE(crx, CRX)
+KET_DEF_CTRL_ANGLE(cry, CRY)
+KET_DEF_CTRL_ANGLE(crz, CRZ)
+KET_DEF_CTRL_ANGLE(cp, CP)
+#undef KET_DEF_CTRL_ANGLE
+
+void QuantumCircuit::add_u_gate(const Matrix2X2& gate, std::size_t target)
+{
+    check_qubit_range_(target, "qubit", "U");
+    elements_.push_back(GateInfo {Gate::U, target, 0, 0.0, gate, std::nullopt});
+}
+
+void QuantumCircuit::add_u_gate(const Matrix2X2& gate, const std::vector<std::size_t>& indices)
+{
+    for (auto t : indices) {
+        add_u_gate(gate, t);
+    }
+}
+
+void QuantumCircuit::add_cu_gate(const Matrix2X2& gate, std::size_t control, std::size_t target)
+{
+    check_qubit_range_(control, "control qubit", "CU");
+    check_qubit_range_(target, "target qubit", "CU");
+    elements_.push_back(GateInfo {Gate::CU, control, target, 0.0, gate, std::nullopt});
+}
+
+void QuantumCircuit::add_cu_gate(const Matrix2X2& gate, const std::vector<std::pair<std::size_t, std::size_t>>& pairs)
+{
+    for (const auto& [c, t] : pairs) {
+        add_cu_gate(gate, c, t);
+    }
+}
+
+void QuantumCircuit::add_m_gate(std::size_t target)
+{
+    add_m_gate(target, target);
+}
+
+void QuantumCircuit::add_m_gate(const std::vector<std::size_t>& indices)
+{
+    for (auto t : indices) {
+        add_m_gate(t, t);
+    }
+}
+
+void QuantumCircuit::add_m_gate(std::size_t target, std::size_t bit_index)
+{
+    check_qubit_range_(target, "qubit", "M");
+    check_bit_range_(bit_index);
+    elements_.push_back(GateInfo {Gate::M, target, bit_index, 0.0, std::nullopt, std::nullopt});
+}
+
+// ---- bitstrings -------------------------------------------------------------------------
+
+auto endian_flip(std::size_t value, std::size_t n_relevant_bits) -> std::size_t
+{
+    std::size_t backward = 0;
+    for (std::size_t i = 0; i < n_relevant_bits; ++i) {
+        backward = (backward << 1U) | (value & 1U);
+        value >>= 1U;
+    }
+    return backward;
+}
+
+auto bitstring_to_state_index(const std::string& bitstring, Endian input_endian) -> std::size_t
+{
+    check_bitstring(bitstring);
+    std::size_t big = 0;
+    for (char c : bitstring) {
+        big = (big << 1U) + (c == '1' ? 1U : 0U);
+    }
+    return input_endian == Endian::BIG ? big : endian_flip(big, bitstring.size());
+}
+
+auto state_index_to_bitstring(std::size_t i_state, std::size_t n_qubits, Endian endian) -> std::string
+{
+    std::string out(n_qubits, '0');
+    for (std::size_t q = 0; q < n_qubits; ++q) {
+        const char c = ((i_state >> q) & 1U) ? '1' : '0';
+        if (endian == Endian::LITTLE) {
+            out[q] = c;
+        } else {
+            out[n_qubits - q - 1] = c;
+        }
+    }
+    return out;
+}
+
+// ---- Statevector ------------------------------------------------------------------------------
+
+Statevector::Statevector(std::size_t n_qubits, DType dtype)
+    : n_qubits_ {n_qubits}
+    , n_states_ {std::size_t {1} << n_qubits}
+    , dtype_ {dtype}
+{
+    if (n_qubits_ == 0) {
+        throw std::runtime_error {"There must be at least 1 qubit in the Statevector.\n"};
+    }
+    check(kt_sv_create(static_cast<int32_t>(n_qubits_), static_cast<int32_t>(dtype_), &handle_));
+}
+
+Statevector::Statevector(std::vector<std::complex<double>> coefficients, Endian input_endian,
+                         double normalization_tolerance, DType dtype)
+    : dtype_ {dtype}
+{
+    // state/state.cpp:30-118: size, power of two, normalisation, endianness
+    if (coefficients.size() < 2) {
+        throw std::runtime_error {"There must be at least 2 coefficients, representing the states for one qubit.\n"};
+    }
+    if (!is_power_of_2(coefficients.size())) {
+        std::stringstream err;
+        err << "The provided coefficients must have a size equal to a power of 2.\n";
+        err << "Found size = " << coefficients.size();
+        throw std::runtime_error {err.str()};
+    }
+    double sum = 0.0;
+    for (const auto& c : coefficients) {
+        sum += std::norm(c);
+    }
+    if (!(std::fabs(sum - 1.0) < normalization_tolerance)) {
+        std::stringstream err;
+        err << "The provided coefficients are not properly normalized.\n";
+        err << "Found sum of squared norms : " << std::fixed << std::setprecision(14) << sum;
+        throw std::runtime_error {err.str()};
+    }
+    n_states_ = coefficients.size();
+    n_qubits_ = static_cast<std::size_t>(__builtin_ctzll(n_states_));
+    if (input_endian == Endian::BIG) {
+        for (std::size_t i = 0; i < n_states_; ++i) {
+            const auto j = endian_flip(i, n_qubits_);
+            if (i < j) {
+                std::swap(coefficients[i], coefficients[j]);
+            }
+        }
+    }
+    check(kt_sv_create(static_cast<int32_t>(n_qubits_), static_cast<int32_t>(dtype_), &handle_));
+    check(kt_sv_upload(handle_, reinterpret_cast<const double*>(coefficients.data()), n_states_));
+    host_ = std::move(coefficients);
+    host_valid_ = (dtype_ == DType::C128);
+}
+
+Statevector::Statevector(const std::string& computational_state, Endian input_endian, DType dtype)
+    : n_qubits_ {computational_state.size()}
+    , n_states_ {std::size_t {1} << computational_state.size()}
+    , dtype_ {dtype}
+{
+    check_bitstring(computational_state);
+    const auto index = bitstring_to_state_index(computational_state, input_endian);
+    check(kt_sv_create(static_cast<int32_t>(n_qubits_), static_cast<int32_t>(dtype_), &handle_));
+    check(kt_sv_set_basis(handle_, index));
+}
+
+Statevector::Statevector(const Statevector& other)
+    : n_qubits_ {other.n_qubits_}
+    , n_states_ {other.n_states_}
+    , dtype_ {other.dtype_}
+{
+    check(kt_sv_create(static_cast<int32_t>(n_qubits_), static_cast<int32_t>(dtype_), &handle_));
+    check(kt_sv_copy(handle_, other.device()));
+    host_ = other.host_;
+    host_valid_ = other.host_valid_;
+}
+
+Statevector::Statevector(Statevector&& other) noexcept
+    : n_qubits_ {other.n_qubits_}
+    , n_states_ {other.n_states_}
+    , dtype_ {other.dtype_}
+    , handle_ {other.handle_}
+    , host_ {std::move(other.host_)}
+    , host_valid_ {other.host_valid_}
+    , host_dirty_ {other.host_dirty_}
+{
+    other.handle_ = nullptr;
+}
+
+auto Statevector::operator=(const Statevector& other) -> Statevector&
+{
+    if (this != &other) {
+        Statevector tmp {other};
+        *this = std::move(tmp);
+    }
+    return *this;
+}
+
+auto Statevector::operator=(Statevector&& other) noexcept -> Statevector&
+{
+    if (this != &other) {
+        if (handle_ != nullptr) {
+            kt_sv_destroy(handle_);
+        }
+        n_qubits_ = other.n_qubits_;
+        n_states_ = other.n_states_;
+        dtype_ = other.dtype_;
+        handle_ = other.handle_;
+        host_ = std::move(other.host_);
+        host_valid_ = other.host_valid_;
+        host_dirty_ = other.host_dirty_;
+        other.handle_ = nullptr;
+    }
+    return *this;
+}
+
+Statevector::~Statevector()
+{
+    if (handle_ != nullptr) {
+        kt_sv_destroy(handle_);
+    }
+}
+
+void Statevector::pull_() const
+{
+    if (host_dirty_ || host_valid_) {
+        return;
+    }
+    host_.resize(n_states_);
+    check(kt_sv_download(handle_, reinterpret_cast<double*>(host_.data()), n_states_));
+    host_valid_ = true;
+}
+
+auto Statevector::device() const -> kt_sv
+{
+    if (host_dirty_) {
+        check(kt_sv_upload(handle_, reinterpret_cast<const double*>(host_.data()), n_states_));
+        host_dirty_ = false;
+        host_valid_ = (dtype_ == DType::C128);
+    }
+    return handle_;
+}
+
+void Statevector::mark_device_modified() const
+{
+    host_valid_ = false;
+}
+
+void Statevector::check_index_(std::size_t index) const
+{
+    if (index >= n_states_) {
+        throw std::runtime_error {"Out-of-bounds access for the quantum state.\n"};
+    }
+}
+
+auto Statevector::operator[](std::size_t index) const -> const std::complex<double>&
+{
+    pull_();
+    return host_[index];
+}
+
+auto Statevector::operator[](std::size_t index) -> std::complex<double>&
+{
+    pull_();
+    host_dirty_ = true;
+    return host_[index];
+}
+
+auto Statevector::at(std::size_t index) const -> const std::complex<double>&
+{
+    check_index_(index);
+    return (*this)[index];
+}
+
+auto Statevector::at(std::size_t index) -> std::complex<double>&
+{
+    check_index_(index);
+    return (*this)[index];
+}
+
+auto Statevector::at(const std::string& bitstring, Endian endian) const -> const std::complex<double>&
+{
+    const auto i = bitstring_to_state_index(bitstring, endian);
+    check_index_(i);
+    return (*this)[i];
+}
+
+auto Statevector::at(const std::string& bitstring, Endian endian) -> std::complex<double>&
+{
+    const auto i = bitstring_to_state_index(bitstring, endian);
+    check_index_(i);
+    return (*this)[i];
+}
+
+auto almost_eq(const Statevector& left, const Statevector& right, double tolerance_sq) noexcept -> bool
+{
+    if (left.n_qubits() != right.n_qubits()) {
+        return false;
+    }
+    for (std::size_t i = 0; i < left.n_states(); ++i) {
+        if (!almost_eq(left[i], right[i], tolerance_sq)) {
+            return false;
+        }
+    }
+    return true;
+}
+
+auto inner_product(const Statevector& bra, const Statevector& ket_state) -> std::complex<double>
+{
+    if (bra.n_states() != ket_state.n_states()) {
+        throw std::runtime_error {"ERROR: cannot calculate inner product between two states of different sizes.\n"};
+    }
+    double out[2];
+    check(kt_sv_inner(bra.device(), ket_state.device(), out));
+    return {out[0], out[1]};
+}
+
+auto inner_product_norm_squared(const Statevector& left, const Statevector& right) -> double
+{
+    return std::norm(inner_product(left, right));
+}
+
+// ---- DensityMatrix ------------------------------------------------------------------------------
+
+DensityMatrix::DensityMatrix(HostMatrix matrix, const density_matrix_nocheck&, DType dtype)
+    : n_states_ {static_cast<std::size_t>(matrix.cols())}
+    , dtype_ {dtype}
+{
+    if (matrix.rows() != matrix.cols() || !is_power_of_2(n_states_) || n_states_ < 2) {
+        throw std::runtime_error {"The provided coefficients must have a size equal to a power of 2.\n"};
+    }
+    n_qubits_ = static_cast<std::size_t>(__builtin_ctzll(n_states_));
+    check(kt_dm_create(static_cast<int32_t>(n_qubits_), static_cast<int32_t>(dtype_), &handle_));
+    check(kt_dm_upload(handle_, reinterpret_cast<const double*>(matrix.data()), n_states_ * n_states_));
+    host_ = std::move(matrix);
+    host_valid_ = (dtype_ == DType::C128);
+}
+
+DensityMatrix::DensityMatrix(const std::string& bitstring, Endian input_endian, DType dtype)
+    : n_qubits_ {bitstring.size()}
+    , n_states_ {std::size_t {1} << bitstring.size()}
+    , dtype_ {dtype}
+{
+    const auto index = bitstring_to_state_index(bitstring, input_endian);
+    check(kt_dm_create(static_cast<int32_t>(n_qubits_), static_cast<int32_t>(dtype_), &handle_));
+    check(kt_dm_set_basis(handle_, index));
+}
+
+DensityMatrix::DensityMatrix(const DensityMatrix& other)
+    : n_qubits_ {other.n_qubits_}
+    , n_states_ {other.n_states_}
+    , dtype_ {other.dtype_}
+{
+    other.pull_();
+    check(kt_dm_create(static_cast<int32_t>(n_qubits_), static_cast<int32_t>(dtype_), &handle_));
+    check(kt_dm_upload(handle_, reinterpret_cast<const double*>(other.host_.data()), n_states_ * n_states_));
+    host_ = other.host_;
+    host_valid_ = true;
+}
+
+DensityMatrix::DensityMatrix(DensityMatrix&& other) noexcept
+    : n_qubits_ {other.n_qubits_}
+    , n_states_ {other.n_states_}
+    , dtype_ {other.dtype_}
+    , handle_ {other.handle_}
+    , host_ {std::move(other.host_)}
+    , host_valid_ {other.host_valid_}
+    , host_dirty_ {other.host_dirty_}
+{
+    other.handle_ = nullptr;
+}
+
+auto DensityMatrix::operator=(const DensityMatrix& other) -> DensityMatrix&
+{
+    if (this != &other) {
+        DensityMatrix tmp {other};
+        *this = std::move(tmp);
+    }
+    return *this;
+}
+
+auto DensityMatrix::operator=(DensityMatrix&& other) noexcept -> DensityMatrix&
+{
+    if (this != &other) {
+        if (handle_ != nullptr) {
+            kt_dm_destroy(handle_);
+        }
+        n_qubits_ = other.n_qubits_;
+        n_states_ = other.n_states_;
+        dtype_ = other.dtype_;
+        handle_ = other.handle_;
+        host_ = std::move(other.host_);
+        host_valid_ = other.host_valid_;
+        host_dirty_ = other.host_dirty_;
+        other.handle_ = nullptr;
+    }
+    return *this;
+}
+
+DensityMatrix::~DensityMatrix()
+{
+    if (handle_ != nullptr) {
+        kt_dm_destroy(handle_);
+    }
+}
+
+void DensityMatrix::pull_() const
+{
+    if (host_dirty_ || host_valid_) {
+        return;
+    }
+    const auto N = static_cast<std::ptrdiff_t>(n_states_);
+    if (host_.rows() != N) {
+        host_ = HostMatrix {N, N};
+    }
+    check(kt_dm_download(handle_, reinterpret_cast<double*>(host_.data()), n_states_ * n_states_));
+    host_valid_ = true;
+}
+
+auto DensityMatrix::matrix() const -> const HostMatrix&
+{
+    pull_();
+    return host_;
+}
+
+auto DensityMatrix::matrix() -> HostMatrix&
+{
+    pull_();
+    host_dirty_ = true;
+    return host_;
+}
+
+auto DensityMatrix::device() const -> kt_dm
+{
+    if (host_dirty_) {
+        check(kt_dm_upload(handle_, reinterpret_cast<const double*>(host_.data()), n_states_ * n_states_));
+        host_dirty_ = false;
+        host_valid_ = (dtype_ == DType::C128);
+    }
+    return handle_;
+}
+
+void DensityMatrix::mark_device_modified() const
+{
+    host_valid_ = false;
+}
+
+auto DensityMatrix::trace() const -> std::complex<double>
+{
+    double out[2];
+    check(kt_dm_trace(device(), out));
+    return {out[0], out[1]};
+}
+
+auto statevector_to_density_matrix(const Statevector& sv) -> DensityMatrix
+{
+    // density_matrix.cpp:170-185: rho(i0, i1) = psi[i0] conj(psi[i1])
+    const auto N = static_cast<std::ptrdiff_t>(sv.n_states());
+    HostMatrix m {N, N};
+    for (std::ptrdiff_t i0 = 0; i0 < N; ++i0) {
+        for (std::ptrdiff_t i1 = 0; i1 < N; ++i1) {
+            m(i0, i1) = sv[static_cast<std::size_t>(i0)] * std::conj(sv[static_cast<std::size_t>(i1)]);
+        }
+    }
+    return DensityMatrix {std::move(m), density_matrix_nocheck {}, sv.dtype()};
+}
+
+// ---- simulation -------------------------------------------------------------------------------
+
+namespace
+{
+
+void check_valid_number_of_qubits(std::size_t circuit_n, std::size_t state_n)
+{
+    // simulation/simulate.cpp:523-532
+    if (circuit_n != state_n) {
+        throw std::runtime_error {"Invalid simulation; circuit and state have different number of qubits."};
+    }
+    if (circuit_n == 0) {
+        throw std::runtime_error {"Cannot simulate a circuit or state with zero qubits."};
+    }
+}
+
+// the circuit's gates as records, split at M gates
+template <typename ApplyFn, typename MeasureFn>
+void run_segments(const QuantumCircuit& circuit, ApplyFn&& apply, MeasureFn&& measure)
+{
+    std::vector<kt_gate> seg;
+    for (const auto& gi : circuit.circuit_elements()) {
+        if (gi.gate == Gate::M) {
+            if (!seg.empty()) {
+                apply(seg);
+                seg.clear();
+            }
+            measure(gi.arg0, gi.arg1);
+            continue;
+        }
+        seg.push_back(to_record(gi, circuit.parameter_data_map()));
+    }
+    if (!seg.empty()) {
+        apply(seg);
+    }
+}
+
+}  // namespace
+
+void StatevectorSimulator::run(const QuantumCircuit& circuit, Statevector& state, std::optional<int> prng_seed)
+{
+    check_valid_number_of_qubits(circuit.n_qubits(), state.n_qubits());
+    cregister_.emplace(circuit.n_bits());
+    kt_sv h = state.device();
+    run_segments(
+        circuit,
+        [&](const std::vector<kt_gate>& seg) {
+            check(kt_sv_apply(h, seg.data(), static_cast<int64_t>(seg.size()), nullptr, 0, KT_APPLY_FUSED));
+        },
+        [&](std::size_t qubit, std::size_t bit) {
+            // measure.hpp:34-55: P(0), P(1); a fresh prng per M gate; discrete draw; collapse
+            double p0 = 0.0, p1 = 0.0;
+            check(kt_sv_measure_probs(h, static_cast<uint32_t>(qubit), &p0, &p1));
+            auto prng = make_prng(prng_seed);
+            auto coin = std::discrete_distribution<int> {{p0, p1}};
+            const int outcome = coin(prng);
+            const double norm = std::sqrt(1.0 / (outcome == 0 ? p0 : p1));
+            check(kt_sv_collapse(h, static_cast<uint32_t>(qubit), outcome, norm));
+            cregister_->set(bit, outcome);
+        });
+    state.mark_device_modified();
+    has_been_run_ = true;
+}
+
+auto StatevectorSimulator::classical_register() const -> const ClassicalRegister&
+{
+    if (!cregister_) {
+        throw std::runtime_error {"ERROR: Cannot access classical register; no simulation has been run\n"};
+    }
+    return *cregister_;
+}
+
+auto StatevectorSimulator::classical_register() -> ClassicalRegister&
+{
+    if (!cregister_) {
+        throw std::runtime_error {"ERROR: Cannot access classical register; no simulation has been run\n"};
+    }
+    return *cregister_;
+}
+
+void DensityMatrixSimulator::run(const QuantumCircuit& circuit, DensityMatrix& state, std::optional<int>)
+{
+    check_valid_number_of_qubits(circuit.n_qubits(), state.n_qubits());
+    if (circuit.n_qubits() != n_qubits_) {
+        throw std::runtime_error {"Invalid simulation; circuit and state have different number of qubits."};
+    }
+    cregister_.emplace(circuit.n_bits());
+    kt_dm h = state.device();
+    run_segments(
+        circuit,
+        [&](const std::vector<kt_gate>& seg) {
+            check(kt_dm_apply(h, seg.data(), static_cast<int64_t>(seg.size()), nullptr, 0, KT_APPLY_FUSED));
+        },
+        [&](std::size_t, std::size_t) {
+            throw std::runtime_error {"ERROR: M gates on a DensityMatrix are not supported by the B200 engine.\n"};
+        });
+    state.mark_device_modified();
+    has_been_run_ = true;
+}
+
+auto DensityMatrixSimulator::classical_register() const -> const ClassicalRegister&
+{
+    if (!cregister_) {
+        throw std::runtime_error {"ERROR: Cannot access classical register; no simulation has been run\n"};
+    }
+    return *cregister_;
+}
+
+void simulate(const QuantumCircuit& circuit, Statevector& state, std::optional<int> prng_seed)
+{
+    auto sim = StatevectorSimulator {};
+    sim.run(circuit, state, prng_seed);
+}
+
+void simulate(const QuantumCircuit& circuit, DensityMatrix& state, std::optional<int> prng_seed)
+{
+    auto sim = DensityMatrixSimulator {state.n_qubits()};
+    sim.run(circuit, state, prng_seed);
+}
+
+// ---- Pauli ---------------------------------------------------------------------------------------
+
+const std::unordered_map<PauliPhase, std::complex<double>> PAULI_PHASE_MAP = {
+    {PauliPhase::PLUS_ONE, {1.0, 0.0}},
+    {PauliPhase::PLUS_EYE, {0.0, 1.0}},
+    {PauliPhase::MINUS_ONE, {-1.0, 0.0}},
+    {PauliPhase::MINUS_EYE, {0.0, -1.0}},
+};
+
+SparsePauliString::SparsePauliString(std::size_t n_qubits, PauliPhase phase)
+    : n_qubits_ {n_qubits}
+    , phase_ {phase}
+{
+    if (n_qubits_ == 0) {
+        throw std::runtime_error {"ERROR: SparsePauliString cannot be constructed with 0 qubits.\n"};
+    }
+}
+
+SparsePauliString::SparsePauliString(std::vector<std::pair<std::size_t, PauliTerm>> terms, std::size_t n_qubits,
+                                     PauliPhase phase)
+    : n_qubits_ {n_qubits}
+    , phase_ {phase}
+    , terms_ {std::move(terms)}
+{
+    if (n_qubits_ == 0) {
+        throw std::runtime_error {"ERROR: SparsePauliString cannot be constructed with 0 qubits.\n"};
+    }
+}
+
+SparsePauliString::SparsePauliString(const std::vector<PauliTerm>& pauli_terms, PauliPhase phase)
+    : n_qubits_ {pauli_terms.size()}
+    , phase_ {phase}
+{
+    if (n_qubits_ == 0) {
+        throw std::runtime_error {"ERROR: SparsePauliString cannot be constructed with 0 qubits.\n"};
+    }
+    for (std::size_t i = 0; i < pauli_terms.size(); ++i) {
+        terms_.emplace_back(i, pauli_terms[i]);
+    }
+}
+
+SparsePauliString::SparsePauliString(const std::initializer_list<PauliTerm>& pauli_terms, PauliPhase phase)
+    : SparsePauliString {std::vector<PauliTerm> {pauli_terms}, phase}
+{}
+
+auto SparsePauliString::at(std::size_t qubit_index) const -> PauliTerm
+{
+    for (const auto& [q, t] : terms_) {
+        if (q == qubit_index && qubit_index < n_qubits_) {
+            return t;
+        }
+    }
+    throw std::runtime_error {"ERROR: no Pauli term found for provided qubit index.\n"};
+}
+
+void SparsePauliString::add(std::size_t qubit_index, PauliTerm term)
+{
+    if (qubit_index >= n_qubits_) {
+        throw std::runtime_error {"ERROR: cannot perform operation on SparsePauliString with index beyond qubit range.\n"};
+    }
+    if (contains_index(qubit_index)) {
+        throw std::runtime_error {"ERROR: Pauli term is already present in the string\n"};
+    }
+    terms_.emplace_back(qubit_index, term);
+}
+
+void SparsePauliString::overwrite(std::size_t qubit_index, PauliTerm term)
+{
+    if (qubit_index >= n_qubits_) {
+        throw std::runtime_error {"ERROR: cannot perform operation on SparsePauliString with index beyond qubit range.\n"};
+    }
+    for (auto& [q, t] : terms_) {
+        if (q == qubit_index) {
+            t = term;
+            return;
+        }
+    }
+    terms_.emplace_back(qubit_index, term);
+}
+
+void SparsePauliString::remove(std::size_t qubit_index)
+{
+    for (auto it = terms_.begin(); it != terms_.end(); ++it) {
+        if (it->first == qubit_index) {
+            terms_.erase(it);
+            return;
+        }
+    }
+}
+
+auto SparsePauliString::contains_index(std::size_t qubit_index) const noexcept -> bool
+{
+    return std::any_of(terms_.begin(), terms_.end(), [&](const auto& p) { return p.first == qubit_index; });
+}
+
+auto SparsePauliString::to_record() const -> kt_pauli
+{
+    // Left-multiply each term onto i^k X^x Z^z in application order:
+    //   X: x ^= 1;  Z: (-1)^x, z ^= 1;  Y = i X Z: i (-1)^x, x ^= 1, z ^= 1.
+    // The record's convention is i^{#Y} X^x Z^z with Y where x & z, so the
+    // record phase is k - popcount(x & z) plus the string's own phase.
+    uint64_t x = 0, z = 0;
+    int k = 0;
+    for (const auto& [q, t] : terms_) {
+        if (q >= n_qubits_ || q >= 64) {
+            throw std::runtime_error {"ERROR: cannot perform operation on SparsePauliString with index beyond qubit range.\n"};
+        }
+        const uint64_t b = uint64_t {1} << q;
+        switch (t) {
+            case PauliTerm::X: x ^= b; break;
+            case PauliTerm::Z:
+                if (x & b) k += 2;
+                z ^= b;
+                break;
+            case PauliTerm::Y:
+                k += 1;
+                if (x & b) k += 2;
+                x ^= b;
+                z ^= b;
+                break;
+            default: break;
+        }
+    }
+    kt_pauli r {};
+    r.x_mask = x;
+    r.z_mask = z;
+    const int ny = __builtin_popcountll(x & z);
+    r.phase = ((static_cast<int>(phase_) + k - ny) % 4 + 4) % 4;
+    return r;
+}
+
+PauliOperator::PauliOperator(std::size_t n_qubits)
+    : n_qubits_ {n_qubits}
+{}
+
+PauliOperator::PauliOperator(std::vector<WeightedPauliString> weighted)
+    : n_qubits_ {0}
+    , strings_ {std::move(weighted)}
+{
+    if (strings_.empty()) {
+        throw std::runtime_error {
+            "ERROR: construction of `PauliOperator` with only WeightedPauliString instances requires\n"
+            "a non-empty vector.\n"};
+    }
+    for (std::size_t i = 1; i < strings_.size(); ++i) {
+        if (strings_[i].pauli_string.n_qubits() != strings_[0].pauli_string.n_qubits()) {
+            throw std::runtime_error {
+                "ERROR: construction of `PauliOperator` with WeightedPauliString instances requires\n"
+                "all pauli strings to have the same number of qubits.\n"};
+        }
+    }
+    n_qubits_ = strings_[0].pauli_string.n_qubits();
+}
+
+PauliOperator::PauliOperator(const std::initializer_list<WeightedPauliString>& weighted)
+    : PauliOperator {std::vector<WeightedPauliString> {weighted}}
+{}
+
+void PauliOperator::add(WeightedPauliString value)
+{
+    strings_.emplace_back(std::move(value));
+}
+
+void PauliOperator::add(std::complex<double> coefficient, SparsePauliString pauli_string)
+{
+    strings_.push_back(WeightedPauliString {coefficient, std::move(pauli_string)});
+}
+
+void PauliOperator::remove(std::size_t index)
+{
+    if (index >= strings_.size()) {
+        throw std::runtime_error {"ERROR: attempted to remove out of bounds element from PauliOperator.\n"};
+    }
+    strings_.erase(strings_.begin() + static_cast<std::ptrdiff_t>(index));
+}
+
+namespace
+{
+
+void records_of(const PauliOperator& op, std::size_t n_state, std::vector<kt_pauli>& recs, std::vector<double>& coeffs)
+{
+    recs.clear();
+    coeffs.clear();
+    for (const auto& [c, s] : op.weighted_pauli_strings()) {
+        if (s.n_qubits() != n_state) {
+            throw std::runtime_error {"Invalid simulation; SparsePauliString and state have different number of qubits."};
+        }
+        recs.push_back(s.to_record());
+        coeffs.push_back(c.real());
+        coeffs.push_back(c.imag());
+    }
+}
+
+}  // namespace
+
+auto expectation_value(const PauliOperator& op, const Statevector& state) -> std::complex<double>
+{
+    std::vector<kt_pauli> recs;
+    std::vector<double> coeffs;
+    records_of(op, state.n_qubits(), recs, coeffs);
+    double total[2] = {0.0, 0.0};
+    check(kt_sv_expect(state.device(), recs.data(), static_cast<int64_t>(recs.size()), coeffs.data(), nullptr, total));
+    return {total[0], total[1]};
+}
+
+auto expectation_value(const SparsePauliString& s, const Statevector& state) -> std::complex<double>
+{
+    if (s.n_qubits() != state.n_qubits()) {
+        throw std::runtime_error {"Invalid simulation; SparsePauliString and state have different number of qubits."};
+    }
+    const kt_pauli rec = s.to_record();
+    double term[2] = {0.0, 0.0};
+    check(kt_sv_expect(state.device(), &rec, 1, nullptr, term, nullptr));
+    return {term[0], term[1]};
+}
+
+auto expectation_value(const PauliOperator& op, const DensityMatrix& state) -> std::complex<double>
+{
+    std::vector<kt_pauli> recs;
+    std::vector<double> coeffs;
+    records_of(op, state.n_qubits(), recs, coeffs);
+    double total[2] = {0.0, 0.0};
+    check(kt_dm_expect(state.device(), recs.data(), static_cast<int64_t>(recs.size()), coeffs.data(), nullptr, total));
+    return {total[0], total[1]};
+}
+
+// ---- probabilities and measurements ---------------------------------------------------------
+
+QuantumNoise::QuantumNoise(std::size_t n_qubits)
+    : n_qubits_ {n_qubits}
+    , noise_(n_qubits, 0.0)
+{}
+
+void QuantumNoise::set(std::size_t index, double noise)
+{
+    if (index >= n_qubits_) {
+        throw std::runtime_error {"ERROR: Out-of-bounds access for QuantumNoise probability."};
+    }
+    if (!(0.0 <= noise && noise <= 1.0)) {
+        throw std::runtime_error {"ERROR: Cannot set probability in QuantumNoise object outside of [0, 1]."};
+    }
+    noise_[index] = noise;
+}
+
+auto QuantumNoise::get(std::size_t index) const -> const double&
+{
+    if (index >= n_qubits_) {
+        throw std::runtime_error {"ERROR: Out-of-bounds access for QuantumNoise probability."};
+    }
+    return noise_[index];
+}
+
+auto calculate_probabilities_raw(const Statevector& state, const QuantumNoise* noise) -> std::vector<double>
+{
+    std::vector<double> out(state.n_states());
+    check(kt_sv_probabilities(state.device(), noise ? noise->values().data() : nullptr, out.data()));
+    return out;
+}
+
+auto calculate_probabilities(const Statevector& state, const QuantumNoise* noise) -> std::map<std::string, double>
+{
+    const auto raw = calculate_probabilities_raw(state, noise);
+    std::map<std::string, double> out;
+    for (std::size_t i = 0; i < raw.size(); ++i) {
+        out[state_index_to_bitstring(i, state.n_qubits(), Endian::LITTLE)] = raw[i];
+    }
+    return out;
+}
+
+auto perform_measurements_as_memory(const Statevector& state, std::size_t n_shots, const QuantumNoise* noise,
+                                    std::optional<int> seed) -> std::vector<std::size_t>
+{
+    // ProbabilitySampler_ (measurements.cpp:288-311): one mt19937 for all shots,
+    // each shot one generate_canonical draw scaled by the CDF bound on the device
+    auto prng = make_prng(seed);
+    std::vector<double> canon(n_shots);
+    for (auto& c : canon) {
+        c = std::generate_canonical<double, std::numeric_limits<double>::digits>(prng);
+    }
+    std::vector<uint64_t> idx(n_shots);
+    int32_t rescanned = 0;
+    check(kt_sv_sample(state.device(), noise ? noise->values().data() : nullptr, canon.data(),
+                       static_cast<int64_t>(n_shots), idx.data(), 0, &rescanned));
+    return {idx.begin(), idx.end()};
+}
+
+auto perform_measurements_as_counts_raw(const Statevector& state, std::size_t n_shots, const QuantumNoise* noise,
+                                        std::optional<int> seed) -> std::map<std::size_t, std::size_t>
+{
+    return memory_to_counts(perform_measurements_as_memory(state, n_shots, noise, seed));
+}
+
+auto perform_measurements_as_counts_marginal(const Statevector& state, std::size_t n_shots,
+                                             const std::vector<std::size_t>& marginal_qubits,
+                                             const QuantumNoise* noise, std::optional<int> seed)
+    -> std::map<std::string, std::size_t>
+{
+    const auto n = state.n_qubits();
+    std::vector<char> marginal(n, 0);
+    for (auto q : marginal_qubits) {
+        if (q >= n) {
+            throw std::runtime_error {"ERROR: marginal qubit index out of range."};
+        }
+        marginal[q] = 1;
+    }
+    std::map<std::string, std::size_t> out;
+    for (auto i : perform_measurements_as_memory(state, n_shots, noise, seed)) {
+        // state_index_to_bitstring_marginal_ (state/marginal.cpp:19-45): character q = qubit q, 'x' if marginal
+        std::string s(n, '0');
+        for (std::size_t q = 0; q < n; ++q) {
+            s[q] = marginal[q] ? 'x' : (((i >> q) & 1U) ? '1' : '0');
+        }
+        ++out[s];
+    }
+    return out;
+}
+
+auto perform_measurements_as_counts(const Statevector& state, std::size_t n_shots, const QuantumNoise* noise,
+                                    std::optional<int> seed) -> std::map<std::string, std::size_t>
+{
+    return perform_measurements_as_counts_marginal(state, n_shots, {}, noise, seed);
+}
+
+auto memory_to_counts(const std::vector<std::size_t>& measurements) -> std::map<std::size_t, std::size_t>
+{
+    std::map<std::size_t, std::size_t> m;
+    for (auto i : measurements) {
+        ++m[i];
+    }
+    return m;
+}
+
+auto memory_to_fractions(const std::vector<std::size_t>& measurements) -> std::map<std::size_t, double>
+{
+    std::map<std::size_t, double> m;
+    for (auto i : measurements) {
+        m[i] += 1.0;
+    }
+    const auto n = static_cast<double>(measurements.size());
+    for (auto& [k, v] : m) {
+        v /= n;
+    }
+    return m;
+}
+
+// ---- adjoint ---------------------------------------------------------------------------------------
+
+auto adjoint_gradient(const QuantumCircuit& circuit, const Statevector& initial, const PauliOperator& hamiltonian,
+                      int checkpoint_every) -> EnergyAndGradient
+{
+    check_valid_number_of_qubits(circuit.n_qubits(), initial.n_qubits());
+    // every parameter-bound gate gets its own slot; the chain rule sums slots per parameter
+    std::vector<kt_gate> recs;
+    std::vector<double> values;
+    std::vector<param::ParameterID> slot_id;
+    for (const auto& gi : circuit.circuit_elements()) {
+        if (gi.gate == Gate::M) {
+            throw std::runtime_error {"ERROR: the adjoint gradient needs a circuit without M gates.\n"};
+        }
+        kt_gate r = to_record(gi, circuit.parameter_data_map());
+        if (gi.parameter) {
+            r.param = static_cast<int32_t>(values.size());
+            values.push_back(r.angle);
+            slot_id.push_back(*gi.parameter);
+        }
+        recs.push_back(r);
+    }
+    std::vector<kt_pauli> strs;
+    std::vector<double> coeffs;
+    records_of(hamiltonian, initial.n_qubits(), strs, coeffs);
+    Statevector work {initial};
+    kt_adjoint adj = nullptr;
+    check(kt_adjoint_create(work.device(), checkpoint_every, &adj));
+    EnergyAndGradient out {};
+    std::vector<double> grad(values.size(), 0.0);
+    int32_t rc = kt_adjoint_forward(adj, recs.data(), static_cast<int64_t>(recs.size()), values.data(),
+                                    static_cast<int64_t>(values.size()), strs.data(), static_cast<int64_t>(strs.size()),
+                                    coeffs.data(), &out.energy);
+    if (rc == KT_OK) {
+        rc = kt_adjoint_backward(adj, grad.data(), static_cast<int64_t>(grad.size()));
+    }
+    kt_adjoint_destroy(adj);
+    check(rc);
+    for (const auto& [id, data] : circuit.parameter_data_map()) {
+        out.gradient[id] = 0.0;
+    }
+    for (std::size_t s = 0; s < grad.size(); ++s) {
+        out.gradient[slot_id[s]] += grad[s];
+    }
+    return out;
+}
+
+}  // namespace ket

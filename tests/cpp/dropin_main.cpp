@@ -1,0 +1,158 @@
+// dropin_main.cpp — one program, two builds.
+//
+// Uses only the kettle API (namespace ket, <kettle/kettle.hpp>).  It is
+// compiled against the reference library (oracle/_ref, from the reference's
+// own sources) and against this engine's C++ front end; tests/test_gpu_dropin.py
+// runs both and compares what they print.
+//
+//   dropin <n_qubits> <layers> <seed>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include <kettle/kettle.hpp>
+
+namespace
+{
+
+struct SplitMix
+{
+    std::uint64_t s;
+    auto next() -> std::uint64_t
+    {
+        std::uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+        return z ^ (z >> 31);
+    }
+    auto uniform() -> double { return static_cast<double>(next() >> 11) * 0x1.0p-53; }
+    auto below(std::uint64_t k) -> std::size_t { return static_cast<std::size_t>(next() % k); }
+};
+
+auto unitary(SplitMix& r) -> ket::Matrix2X2
+{
+    const double a = 6.283185307179586 * r.uniform(), b = 6.283185307179586 * r.uniform();
+    const double c = 6.283185307179586 * r.uniform(), psi = std::asin(std::sqrt(r.uniform()));
+    const std::complex<double> g {std::cos(a), std::sin(a)}, eb {std::cos(b), std::sin(b)}, ec {std::cos(c), std::sin(c)};
+    return ket::Matrix2X2 {.elem00 = g * std::cos(psi) * eb, .elem01 = g * std::sin(psi) * ec,
+                           .elem10 = -g * std::sin(psi) / ec, .elem11 = g * std::cos(psi) / eb};
+}
+
+void build(ket::QuantumCircuit& c, std::size_t n, int layers, SplitMix& r)
+{
+    for (int l = 0; l < layers; ++l) {
+        for (std::size_t q = 0; q < n; ++q) {
+            switch (r.below(6)) {
+                case 0: c.add_h_gate(q); break;
+                case 1: c.add_rx_gate(q, 6.283185307179586 * r.uniform()); break;
+                case 2: c.add_ry_gate(q, 6.283185307179586 * r.uniform()); break;
+                case 3: c.add_rz_gate(q, 6.283185307179586 * r.uniform()); break;
+                case 4: c.add_u_gate(unitary(r), q); break;
+                default: c.add_sx_gate(q); break;
+            }
+        }
+        for (std::size_t q = static_cast<std::size_t>(l % 2); q + 1 < n; q += 2) {
+            c.add_cx_gate(q, q + 1);
+        }
+        for (std::size_t k = 0; k < n / 2; ++k) {
+            const std::size_t a = r.below(n);
+            std::size_t b = r.below(n - 1);
+            if (b >= a) {
+                ++b;
+            }
+            switch (r.below(6)) {
+                case 0: c.add_crx_gate(a, b, 6.283185307179586 * r.uniform()); break;
+                case 1: c.add_cry_gate(a, b, 6.283185307179586 * r.uniform()); break;
+                case 2: c.add_crz_gate(a, b, 6.283185307179586 * r.uniform()); break;
+                case 3: c.add_cp_gate(a, b, 6.283185307179586 * r.uniform()); break;
+                case 4: c.add_cz_gate(a, b); break;
+                default: c.add_cu_gate(unitary(r), a, b); break;
+            }
+        }
+    }
+}
+
+auto hamiltonian(std::size_t n, SplitMix& r) -> ket::PauliOperator
+{
+    std::vector<ket::WeightedPauliString> terms;
+    for (int k = 0; k < 40; ++k) {
+        auto s = ket::SparsePauliString {n};
+        for (std::size_t q = 0; q < n; ++q) {
+            const auto t = r.below(4);
+            if (t == 1) s.add(q, ket::PauliTerm::X);
+            if (t == 2) s.add(q, ket::PauliTerm::Y);
+            if (t == 3) s.add(q, ket::PauliTerm::Z);
+        }
+        terms.push_back(ket::WeightedPauliString {{r.uniform() - 0.5, r.uniform() - 0.5}, s});
+    }
+    return ket::PauliOperator {terms};
+}
+
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    if (argc < 4) {
+        std::fprintf(stderr, "usage: dropin n layers seed\n");
+        return 2;
+    }
+    const auto n = static_cast<std::size_t>(std::atoi(argv[1]));
+    const int layers = std::atoi(argv[2]);
+    const int seed = std::atoi(argv[3]);
+    SplitMix r {static_cast<std::uint64_t>(seed)};
+
+    // 1. statevector propagation with shared parameters
+    auto circuit = ket::QuantumCircuit {n};
+    build(circuit, n, layers, r);
+    const auto id = circuit.add_ry_gate(0, 0.25, ket::param::parameterized {});
+    circuit.add_rz_gate(n - 1, id);
+    circuit.add_crx_gate(n - 1, 0, id);
+    circuit.set_parameter_value(id, 0.75);
+    auto sv = ket::Statevector {n};
+    ket::simulate(circuit, sv);
+    for (std::size_t i = 0; i < sv.n_states(); ++i) {
+        std::printf("amp %zu %.17g %.17g\n", i, sv[i].real(), sv[i].imag());
+    }
+
+    // 2. Pauli expectation value
+    const auto op = hamiltonian(n, r);
+    const auto e = ket::expectation_value(op, sv);
+    std::printf("expect %.17g %.17g\n", e.real(), e.imag());
+
+    // 3. shot sampling (bit-exact given the seed)
+    const auto counts = ket::perform_measurements_as_counts(sv, 4096, nullptr, seed);
+    for (const auto& [bits, cnt] : counts) {
+        std::printf("count %s %zu\n", bits.c_str(), cnt);
+    }
+
+    // 4. mid-circuit measurement
+    auto mc = ket::QuantumCircuit {n};
+    build(mc, n, 2, r);
+    mc.add_m_gate(0);
+    mc.add_h_gate(0);
+    mc.add_m_gate(n - 1);
+    auto msv = ket::Statevector {n};
+    auto sim = ket::StatevectorSimulator {};
+    sim.run(mc, msv, seed);
+    std::printf("cbit0 %d cbitN %d\n", sim.classical_register().get(0), sim.classical_register().get(n - 1));
+    for (std::size_t i = 0; i < msv.n_states(); ++i) {
+        std::printf("mamp %zu %.17g %.17g\n", i, msv[i].real(), msv[i].imag());
+    }
+
+    // 5. density matrix propagation
+    const std::size_t nd = n < 5 ? n : 5;
+    auto dc = ket::QuantumCircuit {nd};
+    build(dc, nd, 3, r);
+    auto dm = ket::DensityMatrix {std::string(nd, '0')};
+    ket::simulate(dc, dm);
+    const auto& m = dm.matrix();
+    for (long rr = 0; rr < static_cast<long>(dm.n_states()); ++rr) {
+        for (long cc = 0; cc < static_cast<long>(dm.n_states()); ++cc) {
+            std::printf("rho %ld %ld %.17g %.17g\n", rr, cc, m(rr, cc).real(), m(rr, cc).imag());
+        }
+    }
+    return 0;
+}

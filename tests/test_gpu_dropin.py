@@ -1,0 +1,56 @@
+"""Drop-in check: tests/cpp/dropin_main.cpp uses only the kettle C++ API.
+Built against the reference (oracle/_ref/dropin_ref, from the reference's own
+sources) and against this engine's ket:: front end (kettle_b200/lib/dropin_b200),
+both binaries must print the same results: amplitudes, expectation value and
+density matrix within 1e-12, sampled counts and measured bits identical."""
+import pathlib
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+REF_BIN = ROOT / "oracle" / "_ref" / "dropin_ref"
+OUR_BIN = ROOT / "kettle_b200" / "lib" / "dropin_b200"
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(exe, *args):
+    out = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    rec = {"amp": {}, "mamp": {}, "rho": {}, "count": {}, "expect": None, "cbits": None}
+    for line in out.stdout.splitlines():
+        f = line.split()
+        if f[0] in ("amp", "mamp"):
+            rec[f[0]][int(f[1])] = complex(float(f[2]), float(f[3]))
+        elif f[0] == "rho":
+            rec["rho"][(int(f[1]), int(f[2]))] = complex(float(f[3]), float(f[4]))
+        elif f[0] == "count":
+            rec["count"][f[1]] = int(f[2])
+        elif f[0] == "expect":
+            rec["expect"] = complex(float(f[1]), float(f[2]))
+        elif f[0] == "cbit0":
+            rec["cbits"] = (int(f[1]), int(f[3]))
+    return rec
+
+
+@pytest.mark.parametrize("n,layers,seed", [(6, 4, 1), (11, 6, 2), (14, 3, 3)])
+def test_dropin_same_results(engine, n, layers, seed):
+    if not REF_BIN.exists():
+        pytest.skip("reference build of the drop-in program is absent")
+    assert OUR_BIN.exists(), "engine build of the drop-in program is missing"
+    ref = _run(REF_BIN, n, layers, seed)
+    our = _run(OUR_BIN, n, layers, seed)
+    a = np.array([ref["amp"][i] for i in sorted(ref["amp"])])
+    b = np.array([our["amp"][i] for i in sorted(our["amp"])])
+    assert np.abs(a - b).max() < 1e-12
+    assert abs(ref["expect"] - our["expect"]) < 1e-12
+    assert ref["count"] == our["count"]
+    assert ref["cbits"] == our["cbits"]
+    ma = np.array([ref["mamp"][i] for i in sorted(ref["mamp"])])
+    mb = np.array([our["mamp"][i] for i in sorted(our["mamp"])])
+    assert np.abs(ma - mb).max() < 1e-12
+    ra = np.array([ref["rho"][k] for k in sorted(ref["rho"])])
+    rb = np.array([our["rho"][k] for k in sorted(our["rho"])])
+    assert np.abs(ra - rb).max() < 1e-12
