@@ -62,9 +62,10 @@ struct FOp
 {
     uint8_t kind;
     uint8_t tslot;    // register slot of the target (NO_SLOT: the target is not a register bit)
-    uint16_t pad0;
-    uint32_t ract;    // registers whose in-register control holds (all ones when none)
-    uint32_t r1;      // diagonal gate on a register bit: registers whose target bit is 1
+    uint8_t cslot;    // register slot of the control (NO_SLOT: none, or not a register bit)
+    uint8_t pad0;
+    uint32_t pad2;
+    uint32_t pad3;
     uint32_t cthr;    // control as thread-index bits (0: none)
     uint32_t tthr;    // diagonal target as thread-index bits (0: none)
     uint32_t pad1;
@@ -138,185 +139,222 @@ __device__ __forceinline__ U xor_terms(int i, const U (&terms)[RBMAX])
 }
 
 // --- register-level gate bodies -------------------------------------------------
-template <typename C, int RB, int S, bool MASKED>
-__device__ __forceinline__ void gen_pairs(C (&v)[1 << RB], const C m00, const C m01, const C m10, const C m11,
-                                          uint32_t ract)
+// S: register slot of the target; CS: register slot of the control (-1: none).
+// Both are template arguments, so a body is straight-line code that touches
+// exactly the amplitudes its gate changes (no per-amplitude predicates).
+template <int S, int CS>
+__device__ __forceinline__ constexpr bool lower_of_pair(int i)
 {
-#pragma unroll
-    for (int i = 0; i < (1 << RB); ++i) {
-        if (i & (1 << S)) {
-            continue;
-        }
-        const int j = i | (1 << S);
-        if (!MASKED || ((ract >> i) & 1u)) {
-            const C a = v[i];
-            const C b = v[j];
-            v[i] = cfma(m01, b, cmul(m00, a));
-            v[j] = cfma(m11, b, cmul(m10, a));
-        }
-    }
+    return !(i & (1 << S)) && (CS < 0 || (i & (1 << CS)));
 }
 
-template <typename C, typename T, int RB, int S, bool MASKED>
-__device__ __forceinline__ void genr_pairs(C (&v)[1 << RB], const T m00, const T m01, const T m10, const T m11,
-                                           uint32_t ract)
+template <int CS>
+__device__ __forceinline__ constexpr bool ctrl_on(int i)
 {
-#pragma unroll
-    for (int i = 0; i < (1 << RB); ++i) {
-        if (i & (1 << S)) {
-            continue;
-        }
-        const int j = i | (1 << S);
-        if (!MASKED || ((ract >> i) & 1u)) {
-            const C a = v[i];
-            const C b = v[j];
-            C x, y;
-            x.x = fma(m01, b.x, m00 * a.x);
-            x.y = fma(m01, b.y, m00 * a.y);
-            y.x = fma(m11, b.x, m10 * a.x);
-            y.y = fma(m11, b.y, m10 * a.y);
-            v[i] = x;
-            v[j] = y;
-        }
-    }
+    return CS < 0 || (i & (1 << CS));
 }
 
-template <typename C, int RB, int S, bool MASKED, bool PURE>
-__device__ __forceinline__ void anti_pairs(C (&v)[1 << RB], const C m01, const C m10, uint32_t ract)
+template <typename T, int RB>
+struct GenF
 {
+    using C = typename CxT<T>::type;
+    C (&v)[1 << RB];
+    C m00, m01, m10, m11;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
 #pragma unroll
-    for (int i = 0; i < (1 << RB); ++i) {
-        if (i & (1 << S)) {
-            continue;
-        }
-        const int j = i | (1 << S);
-        if (!MASKED || ((ract >> i) & 1u)) {
-            const C a = v[i];
-            const C b = v[j];
-            if (PURE) {
-                v[i] = b;
-                v[j] = a;
-            } else {
-                v[i] = cmul(m01, b);
-                v[j] = cmul(m10, a);
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (lower_of_pair<S, CS>(i)) {
+                const int j = i | (1 << S);
+                const C a = v[i];
+                const C b = v[j];
+                v[i] = cfma(m01, b, cmul(m00, a));
+                v[j] = cfma(m11, b, cmul(m10, a));
             }
         }
     }
+};
+
+template <typename T, int RB>
+struct GenRF
+{
+    using C = typename CxT<T>::type;
+    C (&v)[1 << RB];
+    T m00, m01, m10, m11;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (lower_of_pair<S, CS>(i)) {
+                const int j = i | (1 << S);
+                const C a = v[i];
+                const C b = v[j];
+                C x, y;
+                x.x = fma(m01, b.x, m00 * a.x);
+                x.y = fma(m01, b.y, m00 * a.y);
+                y.x = fma(m11, b.x, m10 * a.x);
+                y.y = fma(m11, b.y, m10 * a.y);
+                v[i] = x;
+                v[j] = y;
+            }
+        }
+    }
+};
+
+template <typename T, int RB, bool PURE>
+struct AntiF
+{
+    using C = typename CxT<T>::type;
+    C (&v)[1 << RB];
+    C m01, m10;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (lower_of_pair<S, CS>(i)) {
+                const int j = i | (1 << S);
+                const C a = v[i];
+                const C b = v[j];
+                if (PURE) {
+                    v[i] = b;
+                    v[j] = a;
+                } else {
+                    v[i] = cmul(m01, b);
+                    v[j] = cmul(m10, a);
+                }
+            }
+        }
+    }
+};
+
+// diagonal gate whose target is register slot S
+template <typename T, int RB, bool ONE>
+struct DiagRegF
+{
+    using C = typename CxT<T>::type;
+    C (&v)[1 << RB];
+    C d0, d1;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (ctrl_on<CS>(i)) {
+                if (i & (1 << S)) {
+                    v[i] = cmul(d1, v[i]);
+                } else if (!ONE) {
+                    v[i] = cmul(d0, v[i]);
+                }
+            }
+        }
+    }
+};
+
+// one factor for every register of this thread (target is a thread bit or outside the tile)
+template <typename T, int RB>
+struct DiagAllF
+{
+    using C = typename CxT<T>::type;
+    C (&v)[1 << RB];
+    C d;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (ctrl_on<CS>(i)) {
+                v[i] = cmul(d, v[i]);
+            }
+        }
+    }
+};
+
+template <int RB, int S, typename F>
+__device__ __forceinline__ void dispatch_c(int cs, F& f)
+{
+    switch (cs) {
+        case 0: if constexpr (S != 0) { f.template run<S, 0>(); } break;
+        case 1: if constexpr (S != 1) { f.template run<S, 1>(); } break;
+        case 2: if constexpr (S != 2) { f.template run<S, 2>(); } break;
+        case 3: if constexpr (S != 3) { f.template run<S, 3>(); } break;
+        case 4: if constexpr (RB > 4 && S != 4) { f.template run<S, (RB > 4 ? 4 : 0)>(); } break;
+        default: f.template run<S, -1>(); break;
+    }
 }
 
-#define KT_SLOT_SWITCH(RB, SLOT, CALL)                           \
-    switch (SLOT) {                                              \
-        case 0: { constexpr int S_ = 0; CALL; } break;           \
-        case 1: { constexpr int S_ = 1; CALL; } break;           \
-        case 2: { constexpr int S_ = 2; CALL; } break;           \
-        case 3: { constexpr int S_ = 3; CALL; } break;           \
-        default:                                                 \
-            if constexpr (RB > 4) {                              \
-                constexpr int S_ = (RB > 4) ? 4 : 0;             \
-                CALL;                                            \
-            }                                                    \
-            break;                                               \
+template <int RB, typename F>
+__device__ __forceinline__ void dispatch_sc(int s, int cs, F& f)
+{
+    switch (s) {
+        case 0: dispatch_c<RB, 0>(cs, f); break;
+        case 1: dispatch_c<RB, 1>(cs, f); break;
+        case 2: dispatch_c<RB, 2>(cs, f); break;
+        case 3: dispatch_c<RB, 3>(cs, f); break;
+        default: if constexpr (RB > 4) { dispatch_c<RB, (RB > 4 ? 4 : 0)>(cs, f); } break;
     }
+}
 
 template <typename T, int RB>
 __device__ __forceinline__ void apply_op(typename CxT<T>::type (&v)[1 << RB], const FOp<T>& op, uint32_t t,
                                          uint64_t base)
 {
     using C = typename CxT<T>::type;
-    constexpr uint32_t ALL = (RB >= 5) ? 0xFFFFFFFFu : ((1u << (1 << RB)) - 1u);
     if ((base & op.cglob) != op.cglob) {
         return;  // control outside the tile is 0 for the whole tile
     }
     if ((t & op.cthr) != op.cthr) {
         return;  // control on a thread bit is 0 for this thread
     }
-    const uint32_t ract = op.ract;
-    const bool masked = ract != ALL;
     const int kind = op.kind;
     const int ts = op.tslot;
-    if (kind >= OP_DIAG) {
-        const C d1 = make_cx<T>(op.m[6], op.m[7]);
-        if (ts != NO_SLOT) {
-            const uint32_t on1 = ract & op.r1;
-            const uint32_t on0 = ract & ~op.r1;
-            if (kind == OP_DIAG1) {
-#pragma unroll
-                for (int i = 0; i < (1 << RB); ++i) {
-                    if ((on1 >> i) & 1u) {
-                        v[i] = cmul(d1, v[i]);
-                    }
-                }
-            } else {
-                const C d0 = make_cx<T>(op.m[0], op.m[1]);
-#pragma unroll
-                for (int i = 0; i < (1 << RB); ++i) {
-                    if ((on1 >> i) & 1u) {
-                        v[i] = cmul(d1, v[i]);
-                    } else if ((on0 >> i) & 1u) {
-                        v[i] = cmul(d0, v[i]);
-                    }
-                }
-            }
+    const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
+    switch (kind) {
+        case OP_GEN: {
+            GenF<T, RB> f {v, make_cx<T>(op.m[0], op.m[1]), make_cx<T>(op.m[2], op.m[3]),
+                           make_cx<T>(op.m[4], op.m[5]), make_cx<T>(op.m[6], op.m[7])};
+            dispatch_sc<RB>(ts, cs, f);
             return;
         }
-        // target is a thread bit or outside the tile: one factor for all of this thread's registers
-        const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
-        if (!b && kind == OP_DIAG1) {
+        case OP_GENR: {
+            GenRF<T, RB> f {v, op.m[0], op.m[2], op.m[4], op.m[6]};
+            dispatch_sc<RB>(ts, cs, f);
             return;
         }
-        const C d = b ? d1 : make_cx<T>(op.m[0], op.m[1]);
-        if (!masked) {
-#pragma unroll
-            for (int i = 0; i < (1 << RB); ++i) {
-                v[i] = cmul(d, v[i]);
-            }
+        case OP_ANTI: {
+            AntiF<T, RB, false> f {v, make_cx<T>(op.m[2], op.m[3]), make_cx<T>(op.m[4], op.m[5])};
+            dispatch_sc<RB>(ts, cs, f);
+            return;
+        }
+        case OP_SWAP: {
+            AntiF<T, RB, true> f {v, make_cx<T>(0, 0), make_cx<T>(0, 0)};
+            dispatch_sc<RB>(ts, cs, f);
+            return;
+        }
+        default:
+            break;
+    }
+    // diagonal
+    const C d1 = make_cx<T>(op.m[6], op.m[7]);
+    const C d0 = make_cx<T>(op.m[0], op.m[1]);
+    if (ts != NO_SLOT) {
+        if (kind == OP_DIAG1) {
+            DiagRegF<T, RB, true> f {v, d0, d1};
+            dispatch_sc<RB>(ts, cs, f);
         } else {
-#pragma unroll
-            for (int i = 0; i < (1 << RB); ++i) {
-                if ((ract >> i) & 1u) {
-                    v[i] = cmul(d, v[i]);
-                }
-            }
+            DiagRegF<T, RB, false> f {v, d0, d1};
+            dispatch_sc<RB>(ts, cs, f);
         }
         return;
     }
-    if (kind == OP_SWAP) {
-        const C z = make_cx<T>(0, 0);
-        if (masked) {
-            KT_SLOT_SWITCH(RB, ts, (anti_pairs<C, RB, S_, true, true>(v, z, z, ract)))
-        } else {
-            KT_SLOT_SWITCH(RB, ts, (anti_pairs<C, RB, S_, false, true>(v, z, z, ract)))
-        }
+    const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
+    if (!b && kind == OP_DIAG1) {
         return;
     }
-    if (kind == OP_ANTI) {
-        const C m01 = make_cx<T>(op.m[2], op.m[3]);
-        const C m10 = make_cx<T>(op.m[4], op.m[5]);
-        if (masked) {
-            KT_SLOT_SWITCH(RB, ts, (anti_pairs<C, RB, S_, true, false>(v, m01, m10, ract)))
-        } else {
-            KT_SLOT_SWITCH(RB, ts, (anti_pairs<C, RB, S_, false, false>(v, m01, m10, ract)))
-        }
-        return;
-    }
-    if (kind == OP_GENR) {
-        const T a00 = op.m[0], a01 = op.m[2], a10 = op.m[4], a11 = op.m[6];
-        if (masked) {
-            KT_SLOT_SWITCH(RB, ts, (genr_pairs<C, T, RB, S_, true>(v, a00, a01, a10, a11, ract)))
-        } else {
-            KT_SLOT_SWITCH(RB, ts, (genr_pairs<C, T, RB, S_, false>(v, a00, a01, a10, a11, ract)))
-        }
-        return;
-    }
-    const C m00 = make_cx<T>(op.m[0], op.m[1]);
-    const C m01 = make_cx<T>(op.m[2], op.m[3]);
-    const C m10 = make_cx<T>(op.m[4], op.m[5]);
-    const C m11 = make_cx<T>(op.m[6], op.m[7]);
-    if (masked) {
-        KT_SLOT_SWITCH(RB, ts, (gen_pairs<C, RB, S_, true>(v, m00, m01, m10, m11, ract)))
-    } else {
-        KT_SLOT_SWITCH(RB, ts, (gen_pairs<C, RB, S_, false>(v, m00, m01, m10, m11, ract)))
-    }
+    DiagAllF<T, RB> f {v, b ? d1 : d0};
+    dispatch_c<RB, 99>(cs, f);
 }
 
 // MINB: CTAs per SM the register budget is sized for (2: <= 128 registers,
@@ -714,17 +752,13 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>
         const LGate& x = g[pb.gates[k]];
         FOp<T> op {};
         op.tslot = NO_SLOT;
-        op.ract = ALL;
+        op.cslot = NO_SLOT;
         if (x.control >= 0) {
             const int lc = loc[x.control];
             if (lc < 0) {
                 op.cglob = bit(x.control);
             } else if (const int s = reg_slot(lc); s >= 0) {
-                uint32_t mask = 0;
-                for (int i = 0; i < (1 << RB); ++i) {
-                    if ((i >> s) & 1) mask |= 1u << i;
-                }
-                op.ract = mask;
+                op.cslot = static_cast<uint8_t>(s);
             } else {
                 op.cthr = 1u << thread_bit(lc);
             }
@@ -737,11 +771,6 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>
                 op.tglob = bit(x.target);
             } else if (const int s = reg_slot(lt); s >= 0) {
                 op.tslot = static_cast<uint8_t>(s);
-                uint32_t mask = 0;
-                for (int i = 0; i < (1 << RB); ++i) {
-                    if ((i >> s) & 1) mask |= 1u << i;
-                }
-                op.r1 = mask;
             } else {
                 op.tthr = 1u << thread_bit(lt);
             }
