@@ -145,6 +145,67 @@ def cpu_baseline(n, gates, per_layer, sample_gates=3):
                       f"at {n} qubits, ket::simulate timed alone ({t:.2f} s); layers = gates / {per_layer:.1f}"}
 
 
+def adjoint_bench(stream, n=24, layers=8, ps_params=24, reps=3):
+    """Adjoint gradient of the 24-qubit, 8-layer hardware-efficient ansatz (384
+    parameters) for the XXZ chain, against the parameter-shift rule evaluated
+    with the engine's own forward passes on the same GPU."""
+    import torch
+    from kettle_b200 import capi
+    from kettle_b200 import workloads as W
+
+    gates, params = W.hea(n, layers, seed=SEED)
+    strings, coeffs = W.xxz_chain(n, seed=SEED)
+    sv = capi.Statevector(n, capi.KT_C128, stream=stream.cuda_stream)
+    adj = capi.Adjoint(sv)
+
+    def grad_once():
+        sv.set_basis(0)
+        e = adj.forward(gates, params, strings, coeffs)
+        return e, adj.backward()
+
+    def energy(p):
+        sv.set_basis(0)
+        sv.apply(gates, p)
+        _, tot = sv.expect(strings, coeffs)
+        return tot.real
+
+    for _ in range(2):
+        grad_once()
+        energy(params)
+    torch.cuda.synchronize()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(reps):
+        e, g = grad_once()
+    a1.record(stream)
+    torch.cuda.synchronize()
+    t_adj = a0.elapsed_time(a1) / reps / 1e3
+    idx = np.linspace(0, params.size - 1, ps_params).astype(int)
+    ps = np.zeros(idx.size)
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for j, k in enumerate(idx):
+        pp, pm = params.copy(), params.copy()
+        pp[k] += np.pi / 2
+        pm[k] -= np.pi / 2
+        ps[j] = 0.5 * (energy(pp) - energy(pm))
+    p1.record(stream)
+    torch.cuda.synchronize()
+    t_eval = p0.elapsed_time(p1) / (2 * idx.size) / 1e3
+    t_ps = t_eval * 2 * params.size
+    adj.close()
+    sv.close()
+    return {"qubits": n, "layers": layers, "params": int(params.size), "hamiltonian_terms": int(strings.size),
+            "energy": e, "adjoint_ms": t_adj * 1e3, "adjoint_grads_per_s": params.size / t_adj,
+            "param_shift_eval_ms": t_eval * 1e3, "param_shift_grads_per_s": params.size / t_ps,
+            "speedup_vs_param_shift": t_ps / t_adj,
+            "max_abs_dgrad_vs_param_shift": float(np.abs(g[idx] - ps).max()),
+            "param_shift_sample": f"{2 * idx.size} of the {2 * params.size} shifted evaluations timed "
+                                  f"(every {params.size // idx.size}th parameter), time scaled to {2 * params.size}"}
+
+
 def run_reference(args):
     world, rank, _ = dist_setup(args.gpus)
     if rank != 0:
@@ -296,6 +357,8 @@ def run_engine(args):
                     "path": "kt_sv_set_basis + kt_sv_apply(host gate records) + kt_sv_sample(4096 host uniforms)"},
             "gpu_launches": int((launches + 1) * args.steps),
             "clocks": clk.summary()}
+    if not args.no_adjoint:
+        line["adjoint"] = adjoint_bench(stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(n, gates, per_layer)
@@ -321,6 +384,7 @@ def main():
     ap.add_argument("--mode", default="fused", choices=["fused", "per-gate"])
     ap.add_argument("--ref-gates", type=int, default=3, help="gates in the reference arm's sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the 24-qubit adjoint vs parameter-shift leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -174,6 +174,13 @@ int32_t kt_sv_copy(kt_sv dst, kt_sv src);
 int32_t kt_sv_apply(kt_sv sv, const kt_gate* gates, int64_t n_gates,
                     const double* params, int64_t n_params, int32_t mode);
 
+/* Host-only dry run of the fused planner (no device work, no reference
+ * counterpart): the fused blocks, layout phases, gate ops and shared-memory
+ * transposes kt_sv_apply would use for this gate stream on n_qubits. */
+int32_t kt_plan_stats(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates,
+                      const double* params, int64_t n_params, int64_t* blocks, int64_t* phases,
+                      int64_t* ops, int64_t* transposes);
+
 /* What the most recent kt_sv_apply / kt_dm_apply on this handle launched:
  * kernel launches and the algorithmic HBM bytes they move (read + write of
  * the amplitudes each launch must touch).  Instrumentation; no reference

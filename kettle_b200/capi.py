@@ -70,6 +70,7 @@ _SIGS = {
     "kt_sv_copy": ([P, P], I32),
     "kt_sv_apply": ([P, P, I64, P, I64, I32], I32),
     "kt_sv_apply_stats": ([P, C.POINTER(I64), DP], I32),
+    "kt_plan_stats": ([I32, I32, P, I64, P, I64, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)], I32),
     "kt_sv_expect": ([P, P, I64, P, P, P], I32),
     "kt_sv_probabilities": ([P, P, P], I32),
     "kt_sv_sample": ([P, P, P, I64, P, I32, C.POINTER(I32)], I32),
@@ -135,6 +136,16 @@ def canonicals_mt19937(seed: int, n: int) -> np.ndarray:
     out = np.empty(n, dtype=np.float64)
     check(lib().kt_canonicals_mt19937(seed & 0xFFFFFFFF, n, ptr(out)))
     return out
+
+
+def plan_stats(n_qubits: int, gates: np.ndarray, params: np.ndarray | None = None, dtype: int = KT_C128) -> dict:
+    """Host-only dry run of the fused planner (no GPU needed)."""
+    g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+    p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+    out = [I64(0) for _ in range(4)]
+    check(lib().kt_plan_stats(n_qubits, dtype, ptr(g), g.size, ptr(p), 0 if p is None else p.size,
+                              *[C.byref(o) for o in out]))
+    return dict(zip(("blocks", "phases", "ops", "transposes"), (int(o.value) for o in out)))
 
 
 def tuning_set(name: str, value: int) -> None:

@@ -317,6 +317,27 @@ int32_t kt_sv_apply(kt_sv sv, const kt_gate* gates, int64_t n_gates, const doubl
     });
 }
 
+int32_t kt_plan_stats(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates, const double* params,
+                      int64_t n_params, int64_t* blocks, int64_t* phases, int64_t* ops, int64_t* transposes)
+{
+    return guard([&]() -> int32_t {
+        if (blocks == nullptr || phases == nullptr || ops == nullptr || transposes == nullptr) {
+            return invalid("null output pointer");
+        }
+        if (const int32_t rc = check_dtype(dtype); rc != KT_OK) {
+            return rc;
+        }
+        if (n_qubits < 1 || n_qubits > 40 || n_gates < 0 || (n_gates > 0 && gates == nullptr)) {
+            return invalid("bad qubit count or gate array");
+        }
+        std::vector<kt::LGate> lg;
+        if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, n_qubits, lg); rc != KT_OK) {
+            return rc;
+        }
+        return kt::plan_stats(n_qubits, dtype, lg, blocks, phases, ops, transposes);
+    });
+}
+
 int32_t kt_sv_apply_stats(kt_sv sv, int64_t* launches, double* alg_bytes)
 {
     if (sv == nullptr) {

@@ -885,4 +885,45 @@ int32_t apply_fused(State& s, const std::vector<LGate>& gates)
     return s.dtype == KT_C128 ? run_fused<double>(s, gates) : run_fused<float>(s, gates);
 }
 
+namespace
+{
+
+template <typename T>
+void plan_only(int n, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases, int64_t* ops, int64_t* transposes)
+{
+    constexpr int RB = Cfg<T>::RB;
+    constexpr int L = Cfg<T>::L;
+    const int k_pref = std::min(RB + TBMAX, tuning().fused_tile_bits + (RB - 4));
+    const int K = std::min(n, k_pref);
+    if (n < RB + 5) {
+        *blocks = 0;
+        *phases = 0;
+        *ops = 0;
+        *transposes = 0;
+        return;
+    }
+    const auto pbs = form_blocks(gates, n, K, L, static_cast<size_t>(std::min(MAX_OPS_PER_BLOCK, tuning().fused_max_ops)));
+    Plan<T> plan;
+    for (const auto& b : pbs) {
+        plan_block<T>(b, gates, n, plan);
+    }
+    *blocks = static_cast<int64_t>(plan.blocks.size());
+    *phases = static_cast<int64_t>(plan.phases.size());
+    *ops = static_cast<int64_t>(plan.ops.size());
+    *transposes = plan.transposes;
+}
+
+}  // namespace
+
+int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases,
+                   int64_t* ops, int64_t* transposes)
+{
+    if (dtype == KT_C128) {
+        plan_only<double>(n, gates, blocks, phases, ops, transposes);
+    } else {
+        plan_only<float>(n, gates, blocks, phases, ops, transposes);
+    }
+    return KT_OK;
+}
+
 }  // namespace kt

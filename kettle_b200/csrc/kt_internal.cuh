@@ -108,6 +108,9 @@ int32_t launch_pairs(uint32_t n, uint32_t c, uint32_t t, int kind, uint64_t k0, 
 // fused blocks
 struct FusedPlan;
 int32_t apply_fused(State& s, const std::vector<LGate>& gates);
+// host-only: what the fused planner makes of a gate stream
+int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases,
+                   int64_t* ops, int64_t* transposes);
 
 // reductions
 int32_t expect_paulis(State& s, const kt_pauli* strings, int64_t n_strings, const double* coeffs,

@@ -1,0 +1,57 @@
+"""The fused-block planner is host logic: it runs here without a GPU
+(kt_plan_stats).  Every gate must land in exactly one block, the block count
+must drop well below the gate count on the benchmark circuits, and the plan
+must react to the tuning knobs."""
+import time
+
+import numpy as np
+
+from kettle_b200 import capi
+from kettle_b200 import workloads as W
+
+
+def test_every_gate_is_planned_once():
+    for n, layers, mixed in ((10, 6, True), (16, 4, True), (22, 3, False), (30, 2, True)):
+        g = W.random_layers(n, layers, seed=n, mixed=mixed)
+        st = capi.plan_stats(n, g)
+        assert st["ops"] == len(g)
+        assert 1 <= st["blocks"] <= len(g)
+        assert st["phases"] >= st["blocks"]
+
+
+def test_small_states_use_per_gate_sweeps():
+    g = W.random_layers(8, 3, seed=1)
+    assert capi.plan_stats(8, g) == {"blocks": 0, "phases": 0, "ops": 0, "transposes": 0}
+
+
+def test_fusion_depth_on_benchmark_circuit():
+    g = W.random_layers(30, 40, seed=2024, mixed=True)
+    t0 = time.perf_counter()
+    st = capi.plan_stats(30, g)
+    dt = time.perf_counter() - t0
+    assert st["blocks"] < len(g) / 15          # at least ~15 gates per HBM pass
+    assert dt < 2.0                            # planning is cheap next to a 30-qubit step
+    c64 = capi.plan_stats(30, g, dtype=capi.KT_C64)
+    assert c64["blocks"] <= st["blocks"]       # one more tile qubit for complex64
+
+
+def test_tuning_knobs_change_the_plan():
+    g = W.random_layers(26, 6, seed=3, mixed=True)
+    base = capi.plan_stats(26, g)
+    old = capi.tuning_get("fused_max_ops")
+    try:
+        capi.tuning_set("fused_max_ops", 8)
+        small = capi.plan_stats(26, g)
+    finally:
+        capi.tuning_set("fused_max_ops", old)
+    assert small["blocks"] >= len(g) // 8
+    assert small["blocks"] > base["blocks"]
+    assert capi.plan_stats(26, g) == base
+
+
+def test_diagonal_gates_cost_no_tile_qubit():
+    # a long run of diagonal gates on every qubit fits in a single block
+    n = 24
+    recs = [W.gate("RZ", q, angle=0.1 * q) for q in range(n)] + [W.gate("CZ", (q + 1) % n, control=q) for q in range(n)]
+    st = capi.plan_stats(n, np.concatenate(recs))
+    assert st["blocks"] == 1
