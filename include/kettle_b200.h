@@ -193,6 +193,25 @@ int32_t kt_sv_apply_stats(kt_sv sv, int64_t* launches, double* alg_bytes);
 int32_t kt_sv_expect(kt_sv sv, const kt_pauli* strings, int64_t n_strings,
                      const double* coeffs, double* out_terms, double* out_total);
 
+/* Allocation-free variant of kt_sv_expect (no counterpart in the reference).
+ * For callers that cannot let the library call cudaMalloc: a host that keeps
+ * all device memory in its own pool or arena, or a loop that must not
+ * allocate once running.  It takes the amplitudes as a raw device pointer
+ * (2^n_qubits elements of `dtype`, on the current device), computes the same
+ * per-string values and weighted total as kt_sv_expect, and keeps its scratch
+ * in one fixed device array inside the library (about 1.3 MB, held by every
+ * GPU that loads the library until the process exits), so it calls no
+ * cudaMalloc or cudaFree.  At most KT_NOALLOC_MAX_STRINGS strings per call;
+ * more is rejected with KT_ERR_INVALID.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls share the one
+ * array, so calls that overlap on the GPU (other streams, other host threads)
+ * race; order them on one stream.  Returns after the results are on the host. */
+#define KT_NOALLOC_MAX_STRINGS 512
+int32_t kt_sv_expect_noalloc(const void* device_amps, int32_t n_qubits, int32_t dtype,
+                             const kt_pauli* strings, int64_t n_strings, const double* coeffs,
+                             double* out_terms, double* out_total, void* stream);
+
 /* |a_i|^2 with the reference's rounding (no FMA), then optional per-qubit
  * readout noise applied qubit by qubit (probabilities.cpp:49-71,110-124).
  * noise: n doubles in [0,1] or NULL.  host_out: 2^n doubles. */

@@ -72,6 +72,7 @@ _SIGS = {
     "kt_sv_apply_stats": ([P, C.POINTER(I64), DP], I32),
     "kt_plan_stats": ([I32, I32, P, I64, P, I64, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)], I32),
     "kt_sv_expect": ([P, P, I64, P, P, P], I32),
+    "kt_sv_expect_noalloc": ([P, I32, I32, P, I64, P, P, P, P], I32),
     "kt_sv_probabilities": ([P, P, P], I32),
     "kt_sv_sample": ([P, P, P, I64, P, I32, C.POINTER(I32)], I32),
     "kt_sv_measure_probs": ([P, U32, DP, DP], I32),

@@ -476,6 +476,48 @@ int32_t expect_paulis(State& s, const kt_pauli* strings, int64_t n_strings, cons
     return KT_OK;
 }
 
+// The Pauli-expectation kernels on caller-provided device tables (used by the
+// allocation-free entry point): k_pauli over `n_slots` slots, then the
+// per-string finalisation into `terms` (slot order).
+int32_t pauli_terms_launch(const void* amps, int n, int32_t dtype, const void* slots, int n_slots,
+                           const uint64_t* xm, const uint64_t* zm, const int32_t* phase, int64_t n_strings,
+                           double* partial, int blocks, double* terms, cudaStream_t stream)
+{
+    const auto* sl = static_cast<const PauliSlot*>(slots);
+    for (int s0 = 0; s0 < n_slots; s0 += 65535) {
+        const unsigned ny = static_cast<unsigned>(std::min(65535, n_slots - s0));
+        if (dtype == KT_C128) {
+            k_pauli<double2><<<dim3(blocks, ny), RED_THREADS, 0, stream>>>(static_cast<const double2*>(amps), n, sl + s0,
+                                                                          zm, partial);
+        } else {
+            k_pauli<float2><<<dim3(blocks, ny), RED_THREADS, 0, stream>>>(static_cast<const float2*>(amps), n, sl + s0,
+                                                                         zm, partial);
+        }
+        KT_CHECK_LAUNCH("k_pauli");
+    }
+    k_pauli_finalize<<<static_cast<unsigned>((n_strings + 127) / 128), 128, 0, stream>>>(partial, blocks, xm, zm, phase,
+                                                                                         n_strings, terms);
+    KT_CHECK_LAUNCH("k_pauli_finalize");
+    return KT_OK;
+}
+
+int32_t weighted_total_launch(const double* terms, const double* coeffs, int64_t n, double* total, cudaStream_t stream)
+{
+    k_weighted_total<<<1, 32, 0, stream>>>(terms, coeffs, n, total);
+    KT_CHECK_LAUNCH("k_weighted_total");
+    return KT_OK;
+}
+
+int pauli_slot_bytes()
+{
+    return static_cast<int>(sizeof(PauliSlot));
+}
+
+int pauli_slot_width()
+{
+    return PAULI_MAXG;
+}
+
 int32_t norm_sq(State& s, double* out)
 {
     double r[2];
