@@ -230,6 +230,7 @@ struct kt_adjoint_s
     std::vector<HGroup> hgroups;
     std::vector<HTerm> hterms;
     kt::DevBuf dev;     // hsum tables, partials, gradients
+    kt::DevBuf fused_work;  // plans and partials of the fused sweep
     bool forward_done {false};
 };
 
@@ -329,6 +330,7 @@ int32_t kt_adjoint_destroy(kt_adjoint a)
         a->lam.scratch.release();
         a->lam.scratch2.release();
         a->dev.release();
+        a->fused_work.release();
         delete a;
     }
     return KT_OK;
@@ -517,6 +519,56 @@ int32_t kt_adjoint_backward(kt_adjoint a, double* grad, int64_t n_params)
         std::vector<int32_t> row_slot;
         row_slot.reserve(n_grad);
         int row = n_grad;
+        const int rb_fused = (psi.dtype == KT_C128) ? 3 : 4;
+        if (kt::tuning().adjoint_fused != 0 && psi.n_bits >= rb_fused + 5) {
+            // fused blocks per checkpoint segment, last segment first; rows in forward order
+            std::vector<int32_t> row_of(static_cast<size_t>(G), -1);
+            for (int64_t g = 0, r = 0; g < G; ++g) {
+                if (a->gates[g].slot >= 0) {
+                    row_of[g] = static_cast<int32_t>(r++);
+                }
+            }
+            const int64_t seg = (k > 0) ? k : std::max<int64_t>(G, 1);
+            const int64_t n_seg = (G + seg - 1) / seg;
+            for (int64_t j = n_seg - 1; j >= 0; --j) {
+                const int64_t g0 = j * seg;
+                const int64_t g1 = std::min<int64_t>(G, g0 + seg);
+                if (j < n_seg - 1 && k > 0 && static_cast<size_t>(j) < a->checkpoints.size()) {
+                    // psi is exactly the forward state after gates [0, g1)
+                    KT_CUDA(cudaMemcpyAsync(psi.amps, a->checkpoints[j], bytes, cudaMemcpyDeviceToDevice, psi.stream));
+                }
+                std::vector<kt::AdjGate> sweep;
+                sweep.reserve(static_cast<size_t>(g1 - g0));
+                for (int64_t g = g1 - 1; g >= g0; --g) {
+                    kt::AdjGate ag {};
+                    ag.adj = a->gates[g].adj;
+                    std::copy(a->gates[g].d, a->gates[g].d + 8, ag.d);
+                    ag.row = row_of[g];
+                    sweep.push_back(ag);
+                }
+                if (const int32_t rc = kt::adjoint_sweep_fused(psi, lam, sweep, d_out, a->fused_work); rc != KT_OK) {
+                    return rc;
+                }
+            }
+            std::vector<double> rows_f(static_cast<size_t>(std::max(1, n_grad)));
+            if (n_grad > 0) {
+                if (const int32_t rc = kt::copy_d2h(rows_f.data(), d_out, n_grad * sizeof(double), psi.stream);
+                    rc != KT_OK) {
+                    return rc;
+                }
+            } else {
+                KT_CUDA(cudaStreamSynchronize(psi.stream));
+            }
+            std::fill(grad, grad + n_params, 0.0);
+            int rr = 0;
+            for (const auto& bg : a->gates) {
+                if (bg.slot >= 0) {
+                    grad[bg.slot] += rows_f[rr++];
+                }
+            }
+            a->forward_done = false;
+            return KT_OK;
+        }
         for (int64_t g = G - 1; g >= 0; --g) {
             const BGate& bg = a->gates[g];
             double* part = nullptr;

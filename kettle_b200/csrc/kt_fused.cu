@@ -72,6 +72,27 @@ struct FOp
     uint64_t cglob;   // control outside the tile (0: none)
     uint64_t tglob;   // diagonal target outside the tile (0: none)
     T m[8];
+    static constexpr bool HAS_D = false;
+};
+
+// an op of the adjoint sweep: m = U^dagger, d = dU/dtheta, row = gradient row (-1: none)
+template <typename T>
+struct FOpA
+{
+    uint8_t kind;
+    uint8_t tslot;
+    uint8_t cslot;
+    uint8_t pad0;
+    int32_t row;
+    uint32_t pad3;
+    uint32_t cthr;
+    uint32_t tthr;
+    uint32_t pad1;
+    uint64_t cglob;
+    uint64_t tglob;
+    T m[8];
+    T d[8];
+    static constexpr bool HAS_D = true;
 };
 
 struct FPhase
@@ -597,22 +618,29 @@ void make_slots(const std::vector<int>& regs, int K, int G, int8_t* slot_bit)
     }
 }
 
-template <typename T>
+template <typename T, typename OPT = FOp<T>>
 struct Plan
 {
     std::vector<FBlock> blocks;
     std::vector<FPhase> phases;
-    std::vector<FOp<T>> ops;
+    std::vector<OPT> ops;
     int transposes {0};
 };
 
-template <typename T>
-void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>& plan)
+// per-gate extras of the adjoint sweep: dU/dtheta and the gradient row (-1: none)
+struct AdjExtra
 {
-    constexpr int RB = Cfg<T>::RB;
-    constexpr int L = Cfg<T>::L;
-    constexpr int G = Cfg<T>::G;
-    constexpr uint32_t ALL = (RB >= 5) ? 0xFFFFFFFFu : ((1u << (1 << RB)) - 1u);
+    double d[8];
+    int32_t row;
+};
+
+template <typename T, typename CFG = Cfg<T>, typename OPT = FOp<T>>
+void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T, OPT>& plan,
+                const AdjExtra* extra = nullptr)
+{
+    constexpr int RB = CFG::RB;
+    constexpr int L = CFG::L;
+    constexpr int G = CFG::G;
     const int K = pb.K;
     std::vector<int> loc(n, -1);
     for (int j = 0; j < K; ++j) {
@@ -750,7 +778,7 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>
             return -1;
         };
         const LGate& x = g[pb.gates[k]];
-        FOp<T> op {};
+        OPT op {};
         op.tslot = NO_SLOT;
         op.cslot = NO_SLOT;
         if (x.control >= 0) {
@@ -785,6 +813,13 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T>
         }
         for (int e = 0; e < 8; ++e) {
             op.m[e] = static_cast<T>(x.m[e]);
+        }
+        if constexpr (OPT::HAS_D) {
+            const AdjExtra& ex = extra[pb.gates[k]];
+            op.row = ex.row;
+            for (int e = 0; e < 8; ++e) {
+                op.d[e] = static_cast<T>(ex.d[e]);
+            }
         }
         plan.ops.push_back(op);
     }
@@ -878,7 +913,487 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     return KT_OK;
 }
 
+// ===========================================================================
+// Fused adjoint sweep.  The gates arrive in backward order as U^dagger with
+// their derivative dU/dtheta; a block un-applies all its gates to psi and
+// lambda tile by tile and reduces, for each parameterised gate,
+// Re <lambda| D psi> (psi already un-applied through that gate, lambda not
+// yet) into per-warp shared-memory slots; each CTA writes one partial per
+// gradient row, finalised in a fixed order.  Moving a gate past gates on
+// other qubits leaves every term unchanged (U_B commutes with D_A), so the
+// forward planner's reordering is valid here too.
+
+template <typename T>
+struct CfgA;
+template <>
+struct CfgA<double>
+{
+    static constexpr int RB = 3;  // 8 amplitudes of psi and 8 of lambda per thread
+    static constexpr int L = 3;
+    static constexpr int G = 3;
+};
+template <>
+struct CfgA<float>
+{
+    static constexpr int RB = 4;
+    static constexpr int L = 4;
+    static constexpr int G = 4;
+};
+
+constexpr int ADJ_WARPS = 8;          // 256 threads
+constexpr int ADJ_MAX_ROWS = 256;     // parameterised gates per block
+
+template <typename T, int RB>
+struct GradGenF
+{
+    using C = typename CxT<T>::type;
+    const C (&l)[1 << RB];
+    const C (&p)[1 << RB];
+    C d00, d01, d10, d11;
+    double acc;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (lower_of_pair<S, CS>(i)) {
+                const int j = i | (1 << S);
+                const C e0 = cfma(d01, p[j], cmul(d00, p[i]));
+                const C e1 = cfma(d11, p[j], cmul(d10, p[i]));
+                const double2 a0 = to_d2(l[i]), a1 = to_d2(l[j]);
+                const double2 b0 = to_d2(e0), b1 = to_d2(e1);
+                acc += a0.x * b0.x + a0.y * b0.y + a1.x * b1.x + a1.y * b1.y;
+            }
+        }
+    }
+};
+
+template <typename T, int RB>
+struct GradDiagRegF
+{
+    using C = typename CxT<T>::type;
+    const C (&l)[1 << RB];
+    const C (&p)[1 << RB];
+    C d0, d1;
+    double acc;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (ctrl_on<CS>(i)) {
+                const C e = cmul((i & (1 << S)) ? d1 : d0, p[i]);
+                const double2 a = to_d2(l[i]), b = to_d2(e);
+                acc += a.x * b.x + a.y * b.y;
+            }
+        }
+    }
+};
+
+template <typename T, int RB>
+struct GradDiagAllF
+{
+    using C = typename CxT<T>::type;
+    const C (&l)[1 << RB];
+    const C (&p)[1 << RB];
+    C d;
+    double acc;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (ctrl_on<CS>(i)) {
+                const C e = cmul(d, p[i]);
+                const double2 a = to_d2(l[i]), b = to_d2(e);
+                acc += a.x * b.x + a.y * b.y;
+            }
+        }
+    }
+};
+
+// apply the op's U^dagger to one register array (the forward gate bodies)
+template <typename T, int RB, typename OPT>
+__device__ __forceinline__ void apply_u(typename CxT<T>::type (&v)[1 << RB], const OPT& op, uint32_t t, uint64_t base)
+{
+    using C = typename CxT<T>::type;
+    const int kind = op.kind;
+    const int ts = op.tslot;
+    const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
+    switch (kind) {
+        case OP_GEN: {
+            GenF<T, RB> f {v, make_cx<T>(op.m[0], op.m[1]), make_cx<T>(op.m[2], op.m[3]), make_cx<T>(op.m[4], op.m[5]),
+                           make_cx<T>(op.m[6], op.m[7])};
+            dispatch_sc<RB>(ts, cs, f);
+            return;
+        }
+        case OP_GENR: {
+            GenRF<T, RB> f {v, op.m[0], op.m[2], op.m[4], op.m[6]};
+            dispatch_sc<RB>(ts, cs, f);
+            return;
+        }
+        case OP_ANTI: {
+            AntiF<T, RB, false> f {v, make_cx<T>(op.m[2], op.m[3]), make_cx<T>(op.m[4], op.m[5])};
+            dispatch_sc<RB>(ts, cs, f);
+            return;
+        }
+        case OP_SWAP: {
+            AntiF<T, RB, true> f {v, make_cx<T>(0, 0), make_cx<T>(0, 0)};
+            dispatch_sc<RB>(ts, cs, f);
+            return;
+        }
+        default:
+            break;
+    }
+    const C d1 = make_cx<T>(op.m[6], op.m[7]);
+    const C d0 = make_cx<T>(op.m[0], op.m[1]);
+    if (ts != NO_SLOT) {
+        if (kind == OP_DIAG1) {
+            DiagRegF<T, RB, true> f {v, d0, d1};
+            dispatch_sc<RB>(ts, cs, f);
+        } else {
+            DiagRegF<T, RB, false> f {v, d0, d1};
+            dispatch_sc<RB>(ts, cs, f);
+        }
+        return;
+    }
+    const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
+    if (!b && kind == OP_DIAG1) {
+        return;
+    }
+    DiagAllF<T, RB> f {v, b ? d1 : d0};
+    dispatch_c<RB, 99>(cs, f);
+}
+
+// Re <lambda| D psi> over this thread's registers for a parameterised op
+template <typename T, int RB, typename OPT>
+__device__ __forceinline__ double grad_term(const typename CxT<T>::type (&l)[1 << RB],
+                                            const typename CxT<T>::type (&p)[1 << RB], const OPT& op, uint32_t t,
+                                            uint64_t base)
+{
+    const int kind = op.kind;
+    const int ts = op.tslot;
+    const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
+    if (kind < OP_DIAG) {
+        GradGenF<T, RB> f {l, p, make_cx<T>(op.d[0], op.d[1]), make_cx<T>(op.d[2], op.d[3]), make_cx<T>(op.d[4], op.d[5]),
+                           make_cx<T>(op.d[6], op.d[7]), 0.0};
+        dispatch_sc<RB>(ts, cs, f);
+        return f.acc;
+    }
+    const auto d0 = make_cx<T>(op.d[0], op.d[1]);
+    const auto d1 = make_cx<T>(op.d[6], op.d[7]);
+    if (ts != NO_SLOT) {
+        GradDiagRegF<T, RB> f {l, p, d0, d1, 0.0};
+        dispatch_sc<RB>(ts, cs, f);
+        return f.acc;
+    }
+    const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
+    GradDiagAllF<T, RB> f {l, p, b ? d1 : d0, 0.0};
+    dispatch_c<RB, 99>(cs, f);
+    return f.acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_fused_adj(typename CxT<T>::type* __restrict__ psi,
+                                                      typename CxT<T>::type* __restrict__ lam,
+                                                      const FBlock* __restrict__ blk, const FPhase* __restrict__ phases,
+                                                      const FOpA<T>* __restrict__ ops, int n_rows,
+                                                      double* __restrict__ partial, uint64_t n_tiles)
+{
+    using C = typename CxT<T>::type;
+    constexpr int RB = CfgA<T>::RB;
+    constexpr int R = 1 << RB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ FBlock bk;
+    __shared__ FPhase sph[MAX_PHASES_PER_BLOCK];
+    const uint32_t t = threadIdx.x;
+    if (t == 0) {
+        bk = *blk;
+    }
+    __syncthreads();
+    const int K = bk.K;
+    const int TB = K - RB;
+    const int np = bk.phase_end - bk.phase_begin;
+    const int no = bk.op_end - bk.op_begin;
+    const size_t tile_bytes = sizeof(C) << K;
+    C* smp = reinterpret_cast<C*>(smem_raw);
+    C* sml = reinterpret_cast<C*>(smem_raw + tile_bytes);
+    FOpA<T>* sops = reinterpret_cast<FOpA<T>*>(smem_raw + 2 * tile_bytes);
+    double* acc = reinterpret_cast<double*>(smem_raw + 2 * tile_bytes + static_cast<size_t>(no) * sizeof(FOpA<T>));
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(phases + bk.phase_begin);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(sph);
+        for (int w = t; w < np * static_cast<int>(sizeof(FPhase) / 4); w += blockDim.x) {
+            dst[w] = src[w];
+        }
+        const uint32_t* so = reinterpret_cast<const uint32_t*>(ops + bk.op_begin);
+        uint32_t* dop = reinterpret_cast<uint32_t*>(sops);
+        for (int w = t; w < no * static_cast<int>(sizeof(FOpA<T>) / 4); w += blockDim.x) {
+            dop[w] = so[w];
+        }
+        for (int w = t; w < n_rows * ADJ_WARPS; w += blockDim.x) {
+            acc[w] = 0.0;
+        }
+    }
+    __syncthreads();
+    const int op0 = bk.op_begin;
+    const int lane = t & 31;
+    const int warp = t >> 5;
+
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        uint64_t base = 0;
+        for (int k = 0; k < bk.nfree; ++k) {
+            if ((tile >> k) & 1) {
+                base |= uint64_t {1} << bk.freebit[k];
+            }
+        }
+        C vp[R];
+        C vl[R];
+        {
+            const FPhase& ph = sph[0];
+            uint64_t toff = 0;
+            for (int j = 0; j < TB; ++j) {
+                if ((t >> j) & 1) {
+                    toff += ph.tstride[j];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                uint64_t o = 0;
+#pragma unroll
+                for (int s = 0; s < RB; ++s) {
+                    if (i & (1 << s)) {
+                        o += ph.rstride[s];
+                    }
+                }
+                vp[i] = psi[base + toff + o];
+                vl[i] = lam[base + toff + o];
+            }
+        }
+        uint32_t tsw_prev = 0;
+        for (int p = 0; p < np; ++p) {
+            const FPhase& ph = sph[p];
+            uint32_t tsw = 0;
+            for (int j = 0; j < TB; ++j) {
+                if ((t >> j) & 1) {
+                    tsw ^= ph.tsw[j];
+                }
+            }
+            if (p > 0) {
+                const FPhase& pp = sph[p - 1];
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const uint32_t a = tsw_prev ^ xor_terms<RB>(i, pp.rsw);
+                    smp[a] = vp[i];
+                    sml[a] = vl[i];
+                }
+                __syncthreads();
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const uint32_t a = tsw ^ xor_terms<RB>(i, ph.rsw);
+                    vp[i] = smp[a];
+                    vl[i] = sml[a];
+                }
+                __syncthreads();
+            }
+            tsw_prev = tsw;
+            for (int o = ph.op_begin; o < ph.op_end; ++o) {
+                const FOpA<T>& op = sops[o - op0];
+                if ((base & op.cglob) != op.cglob) {
+                    continue;  // control outside the tile is 0: nothing changes, the derivative term is 0
+                }
+                const bool on = (t & op.cthr) == op.cthr;
+                if (on) {
+                    apply_u<T, RB>(vp, op, t, base);
+                }
+                if (op.row >= 0) {
+                    double g = on ? grad_term<T, RB>(vl, vp, op, t, base) : 0.0;
+#pragma unroll
+                    for (int s = 16; s > 0; s >>= 1) {
+                        g += __shfl_down_sync(0xffffffffU, g, s);
+                    }
+                    if (lane == 0) {
+                        acc[op.row * ADJ_WARPS + warp] += g;
+                    }
+                }
+                if (on) {
+                    apply_u<T, RB>(vl, op, t, base);
+                }
+            }
+        }
+        {
+            const FPhase& ph = sph[np - 1];
+            uint64_t toff = 0;
+            for (int j = 0; j < TB; ++j) {
+                if ((t >> j) & 1) {
+                    toff += ph.tstride[j];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                uint64_t o = 0;
+#pragma unroll
+                for (int s = 0; s < RB; ++s) {
+                    if (i & (1 << s)) {
+                        o += ph.rstride[s];
+                    }
+                }
+                psi[base + toff + o] = vp[i];
+                lam[base + toff + o] = vl[i];
+            }
+        }
+    }
+    __syncthreads();
+    for (int r = t; r < n_rows; r += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < ADJ_WARPS; ++w) {
+            s += acc[r * ADJ_WARPS + w];
+        }
+        partial[static_cast<size_t>(r) * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// grad[rows[r]] = 2 * sum_b partial[r][b] in fixed order
+__global__ void k_adj_rows(const double* __restrict__ partial, int n_blocks, const int32_t* __restrict__ rows, int n_rows,
+                           double* __restrict__ grad)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) {
+        return;
+    }
+    double s = 0.0;
+    for (int b = 0; b < n_blocks; ++b) {
+        s += partial[static_cast<size_t>(r) * n_blocks + b];
+    }
+    grad[rows[r]] = 2.0 * s;
+}
+
+template <typename T>
+int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& gates, double* dev_grad,
+                          DevBuf& work)
+{
+    using C = typename CxT<T>::type;
+    constexpr int RB = CfgA<T>::RB;
+    constexpr int L = CfgA<T>::L;
+    const int n = psi.n_bits;
+    const int K = std::min(n, RB + TBMAX);
+    std::vector<LGate> lg;
+    std::vector<AdjExtra> ex;
+    lg.reserve(gates.size());
+    ex.reserve(gates.size());
+    for (const auto& g : gates) {
+        lg.push_back(g.adj);
+        AdjExtra e {};
+        std::memcpy(e.d, g.d, sizeof(e.d));
+        e.row = g.row;
+        ex.push_back(e);
+    }
+    // cap the ops of a block so its gradient rows fit the shared-memory slots
+    const auto pbs = form_blocks(lg, n, K, L, static_cast<size_t>(std::min(ADJ_MAX_ROWS, tuning().fused_max_ops)));
+    Plan<T, FOpA<T>> plan;
+    std::vector<std::vector<int32_t>> rows_of_block;
+    for (const auto& pb : pbs) {
+        // local row numbers inside the block
+        std::vector<int32_t> rows;
+        std::vector<AdjExtra> local(ex.size());
+        for (int gi : pb.gates) {
+            if (ex[gi].row >= 0) {
+                AdjExtra e = ex[gi];
+                e.row = static_cast<int32_t>(rows.size());
+                rows.push_back(ex[gi].row);
+                local[gi] = e;
+            } else {
+                local[gi] = ex[gi];
+            }
+        }
+        plan_block<T, CfgA<T>, FOpA<T>>(pb, lg, n, plan, local.data());
+        rows_of_block.push_back(std::move(rows));
+    }
+    for (const auto& fb : plan.blocks) {
+        if (fb.phase_end - fb.phase_begin > MAX_PHASES_PER_BLOCK) {
+            set_error(KT_ERR_INVALID, "fused adjoint planner produced too many phases");
+            return KT_ERR_INVALID;
+        }
+    }
+    const uint64_t n_tiles = uint64_t {1} << (n - K);
+    const int grid = static_cast<int>(std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * 2));
+    // device layout: blocks | phases | ops | rows | partials
+    auto al = [](size_t v) { return (v + 255) & ~size_t {255}; };
+    size_t n_rows_total = 0;
+    size_t max_rows = 1;
+    for (const auto& r : rows_of_block) {
+        n_rows_total += r.size();
+        max_rows = std::max(max_rows, r.size());
+    }
+    const size_t nb = plan.blocks.size() * sizeof(FBlock);
+    const size_t np = plan.phases.size() * sizeof(FPhase);
+    const size_t no = std::max<size_t>(1, plan.ops.size()) * sizeof(FOpA<T>);
+    const size_t off_p = al(nb);
+    const size_t off_o = al(off_p + np);
+    const size_t off_r = al(off_o + no);
+    const size_t off_part = al(off_r + std::max<size_t>(1, n_rows_total) * 4);
+    const size_t need = al(off_part + max_rows * grid * 8);
+    if (const int32_t rc = work.reserve(need); rc != KT_OK) {
+        return rc;
+    }
+    std::vector<unsigned char> host(off_part, 0);
+    std::memcpy(host.data(), plan.blocks.data(), nb);
+    std::memcpy(host.data() + off_p, plan.phases.data(), np);
+    if (!plan.ops.empty()) {
+        std::memcpy(host.data() + off_o, plan.ops.data(), plan.ops.size() * sizeof(FOpA<T>));
+    }
+    {
+        size_t w = 0;
+        for (const auto& r : rows_of_block) {
+            std::memcpy(host.data() + off_r + w * 4, r.data(), r.size() * 4);
+            w += r.size();
+        }
+    }
+    char* dev = static_cast<char*>(work.ptr);
+    KT_CUDA(cudaMemcpyAsync(dev, host.data(), off_part, cudaMemcpyHostToDevice, psi.stream));
+    const auto* d_blk = reinterpret_cast<const FBlock*>(dev);
+    const auto* d_ph = reinterpret_cast<const FPhase*>(dev + off_p);
+    const auto* d_ops = reinterpret_cast<const FOpA<T>*>(dev + off_o);
+    const auto* d_rows = reinterpret_cast<const int32_t*>(dev + off_r);
+    auto* d_part = reinterpret_cast<double*>(dev + off_part);
+    static bool attr = false;
+    if (!attr) {
+        KT_CUDA(cudaFuncSetAttribute(k_fused_adj<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024));
+        attr = true;
+    }
+    const int threads = 1 << (K - RB);
+    size_t row_off = 0;
+    for (size_t b = 0; b < plan.blocks.size(); ++b) {
+        const auto& fb = plan.blocks[b];
+        const int nr = static_cast<int>(rows_of_block[b].size());
+        const size_t smem = 2 * (size_t {1} << K) * sizeof(C) + static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOpA<T>) +
+                            static_cast<size_t>(nr) * ADJ_WARPS * sizeof(double);
+        k_fused_adj<T><<<grid, threads, smem, psi.stream>>>(static_cast<C*>(psi.amps), static_cast<C*>(lam.amps), d_blk + b,
+                                                            d_ph, d_ops, nr, d_part, n_tiles);
+        KT_CHECK_LAUNCH("k_fused_adj");
+        if (nr > 0) {
+            k_adj_rows<<<(nr + 127) / 128, 128, 0, psi.stream>>>(d_part, grid, d_rows + row_off, nr, dev_grad);
+            KT_CHECK_LAUNCH("k_adj_rows");
+        }
+        row_off += static_cast<size_t>(nr);
+        psi.last_launches += 1;
+        psi.last_alg_bytes += 4.0 * sizeof(C) * static_cast<double>(psi.n_amps());
+    }
+    return KT_OK;
+}
+
 }  // namespace
+
+int32_t adjoint_sweep_fused(State& psi, State& lam, const std::vector<AdjGate>& gates, double* dev_grad, DevBuf& work)
+{
+    const int rb = psi.dtype == KT_C128 ? CfgA<double>::RB : CfgA<float>::RB;
+    if (psi.n_bits < rb + 5) {
+        set_error(KT_ERR_UNSUPPORTED, "fused adjoint sweep needs at least RB + 5 qubits");
+        return KT_ERR_UNSUPPORTED;
+    }
+    return psi.dtype == KT_C128 ? run_adjoint_sweep<double>(psi, lam, gates, dev_grad, work)
+                                : run_adjoint_sweep<float>(psi, lam, gates, dev_grad, work);
+}
 
 int32_t apply_fused(State& s, const std::vector<LGate>& gates)
 {

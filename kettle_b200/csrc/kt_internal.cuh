@@ -108,6 +108,15 @@ int32_t launch_pairs(uint32_t n, uint32_t c, uint32_t t, int kind, uint64_t k0, 
 // fused blocks
 struct FusedPlan;
 int32_t apply_fused(State& s, const std::vector<LGate>& gates);
+// adjoint sweep gates, in backward order: U^dagger, dU/dtheta and the gradient row (-1: none)
+struct AdjGate
+{
+    LGate adj;
+    double d[8];
+    int32_t row;
+};
+// un-apply `gates` to psi and lambda with fused blocks; dev_grad[row] = 2 Re <lambda|D psi>
+int32_t adjoint_sweep_fused(State& psi, State& lam, const std::vector<AdjGate>& gates, double* dev_grad, DevBuf& work);
 // host-only: what the fused planner makes of a gate stream
 int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases,
                    int64_t* ops, int64_t* transposes);
@@ -141,6 +150,7 @@ struct Tuning
     int fused_ctas_per_sm {2};   // register budget of the fused kernel: 2 (<=128 regs) or 1
     int fused_tile_bits {12};    // K for complex128 (complex64 uses K + 1), clamped to the kernel's range
     int fused_max_ops {256};     // gates per fused block
+    int adjoint_fused {1};       // 1: fused backward blocks, 0: one kernel per gate
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);

@@ -85,6 +85,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.fused_ctas_per_sm = (v == 1) ? 1 : 2;
     } else if (name == "fused_tile_bits") {
         t.fused_tile_bits = static_cast<int>(std::max(9LL, std::min(12LL, v)));
+    } else if (name == "adjoint_fused") {
+        t.adjoint_fused = (v != 0) ? 1 : 0;
     } else if (name == "fused_max_ops") {
         t.fused_max_ops = static_cast<int>(std::max(1LL, std::min(256LL, v)));
     } else {
@@ -136,6 +138,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.fused_ctas_per_sm;
     } else if (n == "fused_tile_bits") {
         *value = t.fused_tile_bits;
+    } else if (n == "adjoint_fused") {
+        *value = t.adjoint_fused;
     } else if (n == "fused_max_ops") {
         *value = t.fused_max_ops;
     } else {
