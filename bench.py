@@ -206,6 +206,92 @@ def adjoint_bench(stream, n=24, layers=8, ps_params=24, reps=3):
                                   f"(every {params.size // idx.size}th parameter), time scaled to {2 * params.size}"}
 
 
+def batch_bench(stream, count=4096, reps=2, sample_every=32):
+    """Energies and adjoint gradients of `count` hardware-efficient-ansatz
+    instances (qubits uniform over 10..22, 2..10 layers, 50 random Pauli
+    strings each) through one kt_batch evaluation (a CUDA graph holding the
+    persistent launches), complex128 and complex64, against the same instances
+    evaluated one at a time through kt_adjoint (every `sample_every`-th
+    instance timed, the time scaled to all of them)."""
+    import torch
+    from kettle_b200 import capi
+    from kettle_b200 import workloads as W
+
+    circuits, params = W.hea_batch(count, seed=SEED)
+    items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
+    out = {"instances": count, "qubits": "uniform 10..22", "layers": "uniform 2..10", "strings_per_instance": 50,
+           "params": int(n_params), "gates": int(gates.size),
+           "step": "one evaluation: parameter upload, all energies and gradients, download (CUDA events)"}
+    results = {}
+    for name, dt in (("c128", capi.KT_C128), ("c64", capi.KT_C64)):
+        t0 = time.perf_counter()
+        b = capi.Batch(items, gates, strings, coeffs, n_params, dtype=dt)
+        plan_s = time.perf_counter() - t0
+        b.set_stream(stream.cuda_stream)
+        for _ in range(2):
+            b.evaluate(params)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            e, g = b.evaluate(params)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        st = b.stats()
+        results[name] = (e, g)
+        out[name] = {"ms": ms, "instances_per_s": count / (ms / 1e3), "create_s": plan_s,
+                     "alg_gbs": st["alg_bytes"] / (ms / 1e3) / 1e9, "shared_memory_items": st["small_items"],
+                     "hbm_items": st["large_items"], "waves": st["waves"], "jobs": st["jobs"], "units": st["units"],
+                     "launches_per_evaluation": st["launches"], "device_gb": st["device_bytes"] / 1e9}
+        b.close()
+    # one at a time through kt_adjoint (fused forward and backward), complex128
+    offs = np.cumsum([0] + [c[2] for c in circuits])
+    sel = list(range(0, count, sample_every))
+    handles = {}
+    for k in sel:
+        n = circuits[k][0]
+        if n not in handles:
+            sv = capi.Statevector(n, capi.KT_C128, stream=stream.cuda_stream)
+            handles[n] = (sv, capi.Adjoint(sv))
+
+    def one(k):
+        n, g_k, np_k, s_k, c_k = circuits[k]
+        sv, adj = handles[n]
+        sv.set_basis(0)
+        e_k = adj.forward(g_k, params[offs[k]:offs[k + 1]], s_k, c_k)
+        return e_k, adj.backward()
+
+    for k in sel[:4]:
+        one(k)
+    torch.cuda.synchronize()
+    o0 = torch.cuda.Event(enable_timing=True)
+    o1 = torch.cuda.Event(enable_timing=True)
+    o0.record(stream)
+    single = [one(k) for k in sel]
+    o1.record(stream)
+    torch.cuda.synchronize()
+    for sv, adj in handles.values():
+        adj.close()
+        sv.close()
+    per_item_ms = o0.elapsed_time(o1) / len(sel)
+    e128, g128 = results["c128"]
+    e64, g64 = results["c64"]
+    de = max(abs(e128[k] - single[j][0]) for j, k in enumerate(sel))
+    dg = max(float(np.abs(g128[offs[k]:offs[k + 1]] - single[j][1]).max()) for j, k in enumerate(sel))
+    one_s = per_item_ms * count / 1e3
+    out["one_at_a_time"] = {"instances_per_s": count / one_s, "ms_per_instance": per_item_ms,
+                            "sample": f"{len(sel)} of {count} instances (every {sample_every}th) through "
+                                      "kt_adjoint forward+backward, time scaled to all"}
+    out["speedup_vs_one_at_a_time_c128"] = one_s / (out["c128"]["ms"] / 1e3)
+    out["max_abs_denergy_vs_one_at_a_time"] = float(de)
+    out["max_abs_dgrad_vs_one_at_a_time"] = float(dg)
+    out["c64_vs_c128"] = {"max_abs_denergy": float(np.abs(e64 - e128).max()),
+                          "max_abs_dgrad": float(np.abs(g64 - g128).max())}
+    return out
+
+
 def run_reference(args):
     world, rank, _ = dist_setup(args.gpus)
     if rank != 0:
@@ -357,8 +443,11 @@ def run_engine(args):
                     "path": "kt_sv_set_basis + kt_sv_apply(host gate records) + kt_sv_sample(4096 host uniforms)"},
             "gpu_launches": int((launches + 1) * args.steps),
             "clocks": clk.summary()}
+    sv.close()
     if not args.no_adjoint:
         line["adjoint"] = adjoint_bench(stream)
+    if args.batch > 0:
+        line["batch"] = batch_bench(stream, count=args.batch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(n, gates, per_layer)
@@ -366,7 +455,6 @@ def run_engine(args):
             line["cpu_baseline"] = {"value": None, "error": str(exc)}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sv.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -385,6 +473,8 @@ def main():
     ap.add_argument("--ref-gates", type=int, default=3, help="gates in the reference arm's sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the 24-qubit adjoint vs parameter-shift leg")
+    ap.add_argument("--batch", type=int, default=4096,
+                    help="instances in the batched energy+gradient leg (0 skips it)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

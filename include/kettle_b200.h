@@ -291,10 +291,24 @@ int32_t kt_adjoint_forward(kt_adjoint adj, const kt_gate* gates, int64_t n_gates
 int32_t kt_adjoint_backward(kt_adjoint adj, double* grad, int64_t n_params);
 
 /* ---- batches (new) -------------------------------------------------------------
- * Many independent small circuits (each with its own qubit count, gate list,
- * parameters and Hamiltonian) evaluated by one persistent kernel launch:
- * energies[b] and, with grads != NULL, dE_b/dparams (concatenated per item in
- * the order of param_offsets). */
+ * Many independent circuits, each with its own qubit count (1..30), gate
+ * list, parameter slots and Hamiltonian, every one starting from |0...0>:
+ * E_b = Re <psi_b| sum_k c_k P_k |psi_b> and, with gradients, dE/dparams.
+ * Item b's gates bind parameter slot s (kt_gate.param) to
+ * params[param_offset + s].  grads[p] is the sum of dE_b/dparams[p] over all
+ * items whose gates bind p: with disjoint parameter ranges that is each
+ * item's own gradient.  Gradients assume real coefficients (Hermitian H).
+ * M gates are rejected.  No reference counterpart.
+ *
+ * kt_batch_create plans every item once (angles stay symbolic), allocates all
+ * device memory, and captures one evaluation as a CUDA graph: parameter
+ * upload, a kernel that writes the gate matrices from the parameters, one
+ * persistent launch for items whose two states fit in shared memory
+ * (q <= 12 complex128, q <= 13 complex64), one persistent launch per memory
+ * wave for the others, FP64 finalisation and the download.
+ * kt_batch_evaluate replays it on the batch's stream and returns when the
+ * results are on the host; KT_ERR_TIMEOUT if a bounded device wait ran out.
+ * kt_batch_run = create + evaluate + destroy. */
 typedef struct kt_batch_item {
     int32_t n_qubits;
     int32_t reserved;
@@ -305,6 +319,26 @@ typedef struct kt_batch_item {
     int64_t string_offset; /* into strings / coeffs  */
     int64_t n_strings;
 } kt_batch_item;
+
+typedef struct kt_batch_s* kt_batch;
+int32_t kt_batch_create(const kt_batch_item* items, int64_t n_items,
+                        const kt_gate* gates, int64_t n_gates_total,
+                        int64_t n_params_total, const kt_pauli* strings,
+                        const double* coeffs, int64_t n_strings_total,
+                        int32_t dtype, int32_t with_grad, kt_batch* out);
+int32_t kt_batch_set_stream(kt_batch b, void* stream);
+/* params: n_params_total values; energies: n_items; grads (nullable; needs
+ * with_grad): n_params_total. */
+int32_t kt_batch_evaluate(kt_batch b, const double* params, double* energies,
+                          double* grads);
+/* What the batch was planned into (instrumentation): shared-memory and HBM
+ * items, memory waves, jobs (fused blocks and Hamiltonian passes), work
+ * units, kernel launches per evaluation, algorithmic HBM bytes per
+ * evaluation, device bytes held. */
+int32_t kt_batch_stats(kt_batch b, int64_t* small_items, int64_t* large_items,
+                       int64_t* waves, int64_t* jobs, int64_t* units,
+                       int64_t* launches, double* alg_bytes, double* device_bytes);
+int32_t kt_batch_destroy(kt_batch b);
 
 int32_t kt_batch_run(const kt_batch_item* items, int64_t n_items,
                      const kt_gate* gates, int64_t n_gates_total,

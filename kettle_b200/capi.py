@@ -95,6 +95,11 @@ _SIGS = {
     "kt_adjoint_destroy": ([P], I32),
     "kt_adjoint_forward": ([P, P, I64, P, I64, P, I64, P, DP], I32),
     "kt_adjoint_backward": ([P, P, I64], I32),
+    "kt_batch_create": ([P, I64, P, I64, I64, P, P, I64, I32, I32, C.POINTER(P)], I32),
+    "kt_batch_set_stream": ([P, P], I32),
+    "kt_batch_evaluate": ([P, P, P, P], I32),
+    "kt_batch_stats": ([P] + [C.POINTER(I64)] * 6 + [DP, DP], I32),
+    "kt_batch_destroy": ([P], I32),
     "kt_batch_run": ([P, I64, P, I64, P, I64, P, P, I64, I32, P, P, P], I32),
 }
 
@@ -385,4 +390,80 @@ class Adjoint:
     def backward(self) -> np.ndarray:
         out = np.zeros(self.n_params, dtype=np.float64)
         check(lib().kt_adjoint_backward(self._h, ptr(out), out.size))
+        return out
+
+
+def batch_items(circuits) -> tuple:
+    """Concatenate per-item (n_qubits, gates, n_params, strings, coeffs) into the
+    flat arrays kt_batch_create takes: (items, gates, strings, coeffs, n_params_total).
+    Each item's parameters follow the previous item's (disjoint ranges)."""
+    items = np.zeros(len(circuits), dtype=BATCH_ITEM_DTYPE)
+    g_parts, s_parts, c_parts = [], [], []
+    g_off = p_off = s_off = 0
+    for b, (n, gates, n_params, strings, coeffs) in enumerate(circuits):
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        s = np.ascontiguousarray(strings, dtype=PAULI_DTYPE)
+        c = np.ones(s.size, dtype=np.complex128) if coeffs is None else np.asarray(coeffs, dtype=np.complex128)
+        items[b] = (n, 0, g_off, g.size, p_off, n_params, s_off, s.size)
+        g_parts.append(g)
+        s_parts.append(s)
+        c_parts.append(c)
+        g_off += g.size
+        p_off += n_params
+        s_off += s.size
+    gates = np.concatenate(g_parts) if g_parts else np.zeros(0, dtype=GATE_DTYPE)
+    return items, gates, np.concatenate(s_parts), np.concatenate(c_parts), p_off
+
+
+class Batch:
+    """Energies (and adjoint gradients) of many independent circuits (kt_batch).
+
+    `items` is a BATCH_ITEM_DTYPE array over the flat `gates`, `strings` and
+    `coeffs` arrays (see batch_items); planning, allocation and the CUDA graph
+    happen here, evaluate() replays the graph for a parameter vector."""
+
+    def __init__(self, items, gates, strings, coeffs, n_params: int, dtype: int = KT_C128, with_grad: bool = True):
+        it = np.ascontiguousarray(items, dtype=BATCH_ITEM_DTYPE)
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        s = np.ascontiguousarray(strings, dtype=PAULI_DTYPE)
+        c = None if coeffs is None else np.ascontiguousarray(coeffs, dtype=np.complex128)
+        h = P()
+        check(lib().kt_batch_create(ptr(it), it.size, ptr(g), g.size, int(n_params), ptr(s), ptr(c), s.size, dtype,
+                                    1 if with_grad else 0, C.byref(h)))
+        self._h = h
+        self.n_items = it.size
+        self.n_params = int(n_params)
+        self.with_grad = with_grad
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().kt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream: int | None):
+        check(lib().kt_batch_set_stream(self._h, stream))
+
+    def evaluate(self, params) -> tuple:
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        if p.size != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters, got {p.size}")
+        e = np.empty(self.n_items, dtype=np.float64)
+        g = np.empty(self.n_params, dtype=np.float64) if self.with_grad else None
+        check(lib().kt_batch_evaluate(self._h, ptr(p), ptr(e), ptr(g)))
+        return e, g
+
+    def stats(self) -> dict:
+        v = [I64() for _ in range(6)]
+        a, d = C.c_double(), C.c_double()
+        check(lib().kt_batch_stats(self._h, *[C.byref(x) for x in v], C.byref(a), C.byref(d)))
+        keys = ("small_items", "large_items", "waves", "jobs", "units", "launches")
+        out = {k: x.value for k, x in zip(keys, v)}
+        out["alg_bytes"] = a.value
+        out["device_bytes"] = d.value
         return out

@@ -182,33 +182,6 @@ __global__ void k_grad_finalize(const double* __restrict__ partial, int n_blocks
     out[r] = 2.0 * s;
 }
 
-// analytic dU/dtheta of the rotation gates (matrices of gates/common_u_gates.cpp)
-bool derivative(int op, double th, double* d)
-{
-    std::fill(d, d + 8, 0.0);
-    const double c = std::cos(th / 2.0), s = std::sin(th / 2.0);
-    switch (op) {
-        case KT_OP_RX: case KT_OP_CRX:
-            // [[c, -i s], [-i s, c]]' = [[-s/2, -i c/2], [-i c/2, -s/2]]
-            d[0] = -0.5 * s; d[3] = -0.5 * c; d[5] = -0.5 * c; d[6] = -0.5 * s;
-            return true;
-        case KT_OP_RY: case KT_OP_CRY:
-            // [[c, -s], [s, c]]' = [[-s/2, -c/2], [c/2, -s/2]]
-            d[0] = -0.5 * s; d[2] = -0.5 * c; d[4] = 0.5 * c; d[6] = -0.5 * s;
-            return true;
-        case KT_OP_RZ: case KT_OP_CRZ:
-            // diag(c - i s, c + i s)' = diag(-s/2 - i c/2, -s/2 + i c/2)
-            d[0] = -0.5 * s; d[1] = -0.5 * c; d[6] = -0.5 * s; d[7] = 0.5 * c;
-            return true;
-        case KT_OP_P: case KT_OP_CP:
-            // diag(1, cos + i sin)' = diag(0, -sin + i cos)
-            d[6] = -std::sin(th); d[7] = std::cos(th);
-            return true;
-        default:
-            return false;
-    }
-}
-
 struct BGate
 {
     kt::LGate adj;   // U^dagger (kind preserved)
@@ -370,7 +343,7 @@ int32_t kt_adjoint_forward(kt_adjoint a, const kt_gate* gates, int64_t n_gates, 
             const kt_gate& g = gates[i];
             if (g.param >= 0) {
                 const double th = params[g.param];
-                if (derivative(g.op, th, b.d)) {
+                if (kt::gate_derivative(g.op, th, b.d)) {
                     b.slot = g.param;
                 }
             }
@@ -612,13 +585,6 @@ int32_t kt_adjoint_backward(kt_adjoint a, double* grad, int64_t n_params)
         kt::set_error(KT_ERR_INVALID, e.what());
         return KT_ERR_INVALID;
     }
-}
-
-int32_t kt_batch_run(const kt_batch_item*, int64_t, const kt_gate*, int64_t, const double*, int64_t, const kt_pauli*,
-                     const double*, int64_t, int32_t, double*, double*, void*)
-{
-    kt::set_error(KT_ERR_UNSUPPORTED, "batch not built yet");
-    return KT_ERR_UNSUPPORTED;
 }
 
 }  // extern "C"

@@ -26,357 +26,13 @@
 //    target that is a thread bit.  The kernel does no per-amplitude index math.
 //  * Loads and stores use a layout whose lane bits are the L lowest qubits:
 //    each warp instruction touches whole 128-byte lines.
-#include <algorithm>
-#include <cstring>
-#include <numeric>
-
-#include "kt_complex.cuh"
-#include "kt_internal.cuh"
+#include "kt_fused.cuh"
 
 namespace kt
 {
 
 namespace
 {
-
-constexpr int KMAX = 14;
-constexpr int RBMAX = 5;
-constexpr int TBMAX = 8;
-constexpr int MAX_OPS_PER_BLOCK = 256;
-constexpr int MAX_PHASES_PER_BLOCK = 64;
-
-enum OpKind : uint8_t
-{
-    OP_GEN = 0,    // general complex 2x2
-    OP_GENR = 1,   // real 2x2 (H, RY, real U)
-    OP_ANTI = 2,   // [[0, m01], [m10, 0]]
-    OP_SWAP = 3,   // X / CX
-    OP_DIAG = 4,   // diag(m00, m11)
-    OP_DIAG1 = 5,  // diag(1, m11)
-};
-
-constexpr uint8_t NO_SLOT = 0xFF;
-
-template <typename T>
-struct FOp
-{
-    uint8_t kind;
-    uint8_t tslot;    // register slot of the target (NO_SLOT: the target is not a register bit)
-    uint8_t cslot;    // register slot of the control (NO_SLOT: none, or not a register bit)
-    uint8_t pad0;
-    uint32_t pad2;
-    uint32_t pad3;
-    uint32_t cthr;    // control as thread-index bits (0: none)
-    uint32_t tthr;    // diagonal target as thread-index bits (0: none)
-    uint32_t pad1;
-    uint64_t cglob;   // control outside the tile (0: none)
-    uint64_t tglob;   // diagonal target outside the tile (0: none)
-    T m[8];
-    static constexpr bool HAS_D = false;
-};
-
-// an op of the adjoint sweep: m = U^dagger, d = dU/dtheta, row = gradient row (-1: none)
-template <typename T>
-struct FOpA
-{
-    uint8_t kind;
-    uint8_t tslot;
-    uint8_t cslot;
-    uint8_t pad0;
-    int32_t row;
-    uint32_t pad3;
-    uint32_t cthr;
-    uint32_t tthr;
-    uint32_t pad1;
-    uint64_t cglob;
-    uint64_t tglob;
-    T m[8];
-    T d[8];
-    static constexpr bool HAS_D = true;
-};
-
-struct FPhase
-{
-    uint64_t rstride[RBMAX];   // global stride of each register slot
-    uint64_t tstride[TBMAX];   // global stride of each thread-index bit
-    uint32_t rsw[RBMAX];       // swizzled shared-memory term of each register slot
-    uint32_t tsw[TBMAX];       // swizzled shared-memory term of each thread-index bit
-    int32_t op_begin;
-    int32_t op_end;
-};
-
-struct FBlock
-{
-    int32_t K;
-    int32_t nfree;
-    int32_t phase_begin;
-    int32_t phase_end;
-    int32_t op_begin;
-    int32_t op_end;
-    int32_t qubit[KMAX];    // tile bit -> qubit
-    int32_t freebit[64];    // qubits outside the tile, ascending
-};
-
-// tile configuration per amplitude type
-template <typename T>
-struct Cfg;
-template <>
-struct Cfg<double>
-{
-    static constexpr int RB = 4;     // 16 amplitudes per thread
-    static constexpr int L = 3;      // 8 x 16 B = 128 B runs
-    static constexpr int G = 3;      // swizzle group (16-byte elements: 8 per 128-byte bank row)
-};
-template <>
-struct Cfg<float>
-{
-    static constexpr int RB = 5;     // 32 amplitudes per thread
-    static constexpr int L = 4;      // 16 x 8 B = 128 B runs
-    static constexpr int G = 4;      // 8-byte elements: 16 per bank row
-};
-
-// XOR swizzle: the low G bits are XORed with a fold of the higher bits.  It is
-// linear over GF(2), so swz(a ^ b) = swz(a) ^ swz(b).
-__host__ __device__ inline uint32_t swz(uint32_t l, int G)
-{
-    uint32_t f = 0;
-    for (int s = G; s < 32; s += G) {
-        f ^= l >> s;
-    }
-    return l ^ (f & ((1u << G) - 1));
-}
-
-template <int RB, typename U>
-__device__ __forceinline__ U xor_terms(int i, const U (&terms)[RBMAX])
-{
-    U a = 0;
-#pragma unroll
-    for (int s = 0; s < RB; ++s) {
-        if (i & (1 << s)) {
-            a ^= terms[s];
-        }
-    }
-    return a;
-}
-
-// --- register-level gate bodies -------------------------------------------------
-// S: register slot of the target; CS: register slot of the control (-1: none).
-// Both are template arguments, so a body is straight-line code that touches
-// exactly the amplitudes its gate changes (no per-amplitude predicates).
-template <int S, int CS>
-__device__ __forceinline__ constexpr bool lower_of_pair(int i)
-{
-    return !(i & (1 << S)) && (CS < 0 || (i & (1 << CS)));
-}
-
-template <int CS>
-__device__ __forceinline__ constexpr bool ctrl_on(int i)
-{
-    return CS < 0 || (i & (1 << CS));
-}
-
-template <typename T, int RB>
-struct GenF
-{
-    using C = typename CxT<T>::type;
-    C (&v)[1 << RB];
-    C m00, m01, m10, m11;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (lower_of_pair<S, CS>(i)) {
-                const int j = i | (1 << S);
-                const C a = v[i];
-                const C b = v[j];
-                v[i] = cfma(m01, b, cmul(m00, a));
-                v[j] = cfma(m11, b, cmul(m10, a));
-            }
-        }
-    }
-};
-
-template <typename T, int RB>
-struct GenRF
-{
-    using C = typename CxT<T>::type;
-    C (&v)[1 << RB];
-    T m00, m01, m10, m11;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (lower_of_pair<S, CS>(i)) {
-                const int j = i | (1 << S);
-                const C a = v[i];
-                const C b = v[j];
-                C x, y;
-                x.x = fma(m01, b.x, m00 * a.x);
-                x.y = fma(m01, b.y, m00 * a.y);
-                y.x = fma(m11, b.x, m10 * a.x);
-                y.y = fma(m11, b.y, m10 * a.y);
-                v[i] = x;
-                v[j] = y;
-            }
-        }
-    }
-};
-
-template <typename T, int RB, bool PURE>
-struct AntiF
-{
-    using C = typename CxT<T>::type;
-    C (&v)[1 << RB];
-    C m01, m10;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (lower_of_pair<S, CS>(i)) {
-                const int j = i | (1 << S);
-                const C a = v[i];
-                const C b = v[j];
-                if (PURE) {
-                    v[i] = b;
-                    v[j] = a;
-                } else {
-                    v[i] = cmul(m01, b);
-                    v[j] = cmul(m10, a);
-                }
-            }
-        }
-    }
-};
-
-// diagonal gate whose target is register slot S
-template <typename T, int RB, bool ONE>
-struct DiagRegF
-{
-    using C = typename CxT<T>::type;
-    C (&v)[1 << RB];
-    C d0, d1;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (ctrl_on<CS>(i)) {
-                if (i & (1 << S)) {
-                    v[i] = cmul(d1, v[i]);
-                } else if (!ONE) {
-                    v[i] = cmul(d0, v[i]);
-                }
-            }
-        }
-    }
-};
-
-// one factor for every register of this thread (target is a thread bit or outside the tile)
-template <typename T, int RB>
-struct DiagAllF
-{
-    using C = typename CxT<T>::type;
-    C (&v)[1 << RB];
-    C d;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (ctrl_on<CS>(i)) {
-                v[i] = cmul(d, v[i]);
-            }
-        }
-    }
-};
-
-template <int RB, int S, typename F>
-__device__ __forceinline__ void dispatch_c(int cs, F& f)
-{
-    switch (cs) {
-        case 0: if constexpr (S != 0) { f.template run<S, 0>(); } break;
-        case 1: if constexpr (S != 1) { f.template run<S, 1>(); } break;
-        case 2: if constexpr (S != 2) { f.template run<S, 2>(); } break;
-        case 3: if constexpr (S != 3) { f.template run<S, 3>(); } break;
-        case 4: if constexpr (RB > 4 && S != 4) { f.template run<S, (RB > 4 ? 4 : 0)>(); } break;
-        default: f.template run<S, -1>(); break;
-    }
-}
-
-template <int RB, typename F>
-__device__ __forceinline__ void dispatch_sc(int s, int cs, F& f)
-{
-    switch (s) {
-        case 0: dispatch_c<RB, 0>(cs, f); break;
-        case 1: dispatch_c<RB, 1>(cs, f); break;
-        case 2: dispatch_c<RB, 2>(cs, f); break;
-        case 3: dispatch_c<RB, 3>(cs, f); break;
-        default: if constexpr (RB > 4) { dispatch_c<RB, (RB > 4 ? 4 : 0)>(cs, f); } break;
-    }
-}
-
-template <typename T, int RB>
-__device__ __forceinline__ void apply_op(typename CxT<T>::type (&v)[1 << RB], const FOp<T>& op, uint32_t t,
-                                         uint64_t base)
-{
-    using C = typename CxT<T>::type;
-    if ((base & op.cglob) != op.cglob) {
-        return;  // control outside the tile is 0 for the whole tile
-    }
-    if ((t & op.cthr) != op.cthr) {
-        return;  // control on a thread bit is 0 for this thread
-    }
-    const int kind = op.kind;
-    const int ts = op.tslot;
-    const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
-    switch (kind) {
-        case OP_GEN: {
-            GenF<T, RB> f {v, make_cx<T>(op.m[0], op.m[1]), make_cx<T>(op.m[2], op.m[3]),
-                           make_cx<T>(op.m[4], op.m[5]), make_cx<T>(op.m[6], op.m[7])};
-            dispatch_sc<RB>(ts, cs, f);
-            return;
-        }
-        case OP_GENR: {
-            GenRF<T, RB> f {v, op.m[0], op.m[2], op.m[4], op.m[6]};
-            dispatch_sc<RB>(ts, cs, f);
-            return;
-        }
-        case OP_ANTI: {
-            AntiF<T, RB, false> f {v, make_cx<T>(op.m[2], op.m[3]), make_cx<T>(op.m[4], op.m[5])};
-            dispatch_sc<RB>(ts, cs, f);
-            return;
-        }
-        case OP_SWAP: {
-            AntiF<T, RB, true> f {v, make_cx<T>(0, 0), make_cx<T>(0, 0)};
-            dispatch_sc<RB>(ts, cs, f);
-            return;
-        }
-        default:
-            break;
-    }
-    // diagonal
-    const C d1 = make_cx<T>(op.m[6], op.m[7]);
-    const C d0 = make_cx<T>(op.m[0], op.m[1]);
-    if (ts != NO_SLOT) {
-        if (kind == OP_DIAG1) {
-            DiagRegF<T, RB, true> f {v, d0, d1};
-            dispatch_sc<RB>(ts, cs, f);
-        } else {
-            DiagRegF<T, RB, false> f {v, d0, d1};
-            dispatch_sc<RB>(ts, cs, f);
-        }
-        return;
-    }
-    const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
-    if (!b && kind == OP_DIAG1) {
-        return;
-    }
-    DiagAllF<T, RB> f {v, b ? d1 : d0};
-    dispatch_c<RB, 99>(cs, f);
-}
 
 // MINB: CTAs per SM the register budget is sized for (2: <= 128 registers,
 // 1: the compiler's natural allocation); chosen per run by the tuning table.
@@ -387,9 +43,7 @@ __global__ void __launch_bounds__(256, MINB) k_fused(typename CxT<T>::type* __re
 {
     using C = typename CxT<T>::type;
     constexpr int RB = Cfg<T>::RB;
-    constexpr int R = 1 << RB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-
     __shared__ FBlock bk;
     __shared__ FPhase sph[MAX_PHASES_PER_BLOCK];
     const uint32_t t = threadIdx.x;
@@ -397,435 +51,13 @@ __global__ void __launch_bounds__(256, MINB) k_fused(typename CxT<T>::type* __re
         bk = *blk;
     }
     __syncthreads();
-    const int K = bk.K;
-    const int TB = K - RB;
-    const int np = bk.phase_end - bk.phase_begin;
-    const int no = bk.op_end - bk.op_begin;
     C* sm = reinterpret_cast<C*>(smem_raw);
-    FOp<T>* sops = reinterpret_cast<FOp<T>*>(smem_raw + (sizeof(C) << K));
-    {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(phases + bk.phase_begin);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(sph);
-        for (int w = t; w < np * static_cast<int>(sizeof(FPhase) / 4); w += blockDim.x) {
-            dst[w] = src[w];
-        }
-        const uint32_t* so = reinterpret_cast<const uint32_t*>(ops + bk.op_begin);
-        uint32_t* dop = reinterpret_cast<uint32_t*>(sops);
-        for (int w = t; w < no * static_cast<int>(sizeof(FOp<T>) / 4); w += blockDim.x) {
-            dop[w] = so[w];
-        }
-    }
+    FOp<T>* sops = reinterpret_cast<FOp<T>*>(smem_raw + (sizeof(C) << bk.K));
+    stage_block(bk, phases, ops, sph, sops, t);
     __syncthreads();
-    const int op0 = bk.op_begin;
-
     for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        uint64_t base = 0;
-        for (int k = 0; k < bk.nfree; ++k) {
-            if ((tile >> k) & 1) {
-                base |= uint64_t {1} << bk.freebit[k];
-            }
-        }
-        C v[R];
-        {
-            const FPhase& ph = sph[0];
-            uint64_t toff = 0;
-            for (int j = 0; j < TB; ++j) {
-                if ((t >> j) & 1) {
-                    toff += ph.tstride[j];
-                }
-            }
-            const C* src = a + base + toff;
-#pragma unroll
-            for (int i = 0; i < R; ++i) {
-                uint64_t o = 0;
-#pragma unroll
-                for (int s = 0; s < RB; ++s) {
-                    if (i & (1 << s)) {
-                        o += ph.rstride[s];
-                    }
-                }
-                v[i] = src[o];
-            }
-        }
-        uint32_t tsw_prev = 0;
-        for (int p = 0; p < np; ++p) {
-            const FPhase& ph = sph[p];
-            uint32_t tsw = 0;
-            for (int j = 0; j < TB; ++j) {
-                if ((t >> j) & 1) {
-                    tsw ^= ph.tsw[j];
-                }
-            }
-            if (p > 0) {
-                // transpose: registers (previous layout) -> smem -> registers (this layout)
-                const FPhase& pp = sph[p - 1];
-#pragma unroll
-                for (int i = 0; i < R; ++i) {
-                    sm[tsw_prev ^ xor_terms<RB>(i, pp.rsw)] = v[i];
-                }
-                __syncthreads();
-#pragma unroll
-                for (int i = 0; i < R; ++i) {
-                    v[i] = sm[tsw ^ xor_terms<RB>(i, ph.rsw)];
-                }
-                __syncthreads();
-            }
-            tsw_prev = tsw;
-            for (int o = ph.op_begin; o < ph.op_end; ++o) {
-                apply_op<T, RB>(v, sops[o - op0], t, base);
-            }
-        }
-        {
-            const FPhase& ph = sph[np - 1];
-            uint64_t toff = 0;
-            for (int j = 0; j < TB; ++j) {
-                if ((t >> j) & 1) {
-                    toff += ph.tstride[j];
-                }
-            }
-            C* dst = a + base + toff;
-#pragma unroll
-            for (int i = 0; i < R; ++i) {
-                uint64_t o = 0;
-#pragma unroll
-                for (int s = 0; s < RB; ++s) {
-                    if (i & (1 << s)) {
-                        o += ph.rstride[s];
-                    }
-                }
-                dst[o] = v[i];
-            }
-        }
+        fwd_tile<T, RB, false>(a, bk, sph, sops, tile, sm, t, false);
     }
-}
-
-// ---------------------------------------------------------------------------
-// host planner
-
-struct PlanBlock
-{
-    int K;
-    std::vector<int> qubits;     // tile bit -> qubit (ascending)
-    std::vector<int> gates;      // gate indices in execution order
-};
-
-uint64_t bit(int q)
-{
-    return uint64_t {1} << q;
-}
-
-// Greedy block formation: in circuit order, take each gate that does not
-// share a qubit with a gate skipped before it and whose target (when it must
-// be in the tile) fits in the K-qubit set.
-std::vector<PlanBlock> form_blocks(const std::vector<LGate>& g, int n, int K, int L, size_t max_ops)
-{
-    std::vector<PlanBlock> out;
-    std::vector<int> pend(g.size());
-    std::iota(pend.begin(), pend.end(), 0);
-    const uint64_t all = (n >= 64) ? ~uint64_t {0} : (bit(n) - 1);
-    while (!pend.empty()) {
-        uint64_t Q = bit(L) - 1;
-        uint64_t blocked = 0;
-        std::vector<int> take;
-        std::vector<int> rest;
-        rest.reserve(pend.size());
-        for (size_t k = 0; k < pend.size(); ++k) {
-            const int idx = pend[k];
-            const LGate& x = g[idx];
-            const uint64_t touch = bit(x.target) | (x.control >= 0 ? bit(x.control) : 0);
-            if ((touch & blocked) != 0 || take.size() >= max_ops) {
-                blocked |= touch;
-                rest.push_back(idx);
-            } else {
-                const uint64_t need = (x.kind == KIND_DIAG) ? 0 : bit(x.target);
-                if (__builtin_popcountll(Q | need) <= K) {
-                    Q |= need;
-                    take.push_back(idx);
-                } else {
-                    blocked |= touch;
-                    rest.push_back(idx);
-                }
-            }
-            if (blocked == all) {
-                rest.insert(rest.end(), pend.begin() + static_cast<long>(k) + 1, pend.end());
-                break;
-            }
-        }
-        // fill the tile up to K qubits with the lowest free qubits (longer contiguous runs)
-        for (int q = 0; q < n && __builtin_popcountll(Q) < K; ++q) {
-            Q |= bit(q);
-        }
-        PlanBlock b;
-        b.K = K;
-        for (int q = 0; q < n; ++q) {
-            if (Q & bit(q)) {
-                b.qubits.push_back(q);
-            }
-        }
-        b.gates = std::move(take);
-        out.push_back(std::move(b));
-        pend.swap(rest);
-    }
-    return out;
-}
-
-// Slot order of a layout: register bits, then the lane bits (distinct
-// residues mod G so a quarter/half warp hits distinct shared-memory banks;
-// the L lowest tile bits when none of them is a register bit, which also
-// makes global accesses coalesced), then the remaining thread bits.
-void make_slots(const std::vector<int>& regs, int K, int G, int8_t* slot_bit)
-{
-    std::vector<bool> is_reg(K, false);
-    for (int r : regs) {
-        is_reg[r] = true;
-    }
-    int s = 0;
-    for (int r : regs) {
-        slot_bit[s++] = static_cast<int8_t>(r);
-    }
-    std::vector<int> lanes;
-    std::vector<bool> used(K, false);
-    bool low_free = true;
-    for (int b = 0; b < G; ++b) {
-        low_free = low_free && !is_reg[b];
-    }
-    if (low_free) {
-        for (int b = 0; b < G; ++b) {
-            lanes.push_back(b);
-        }
-    } else {
-        std::vector<bool> res_used(G, false);
-        for (int b = 0; b < K && static_cast<int>(lanes.size()) < G; ++b) {
-            if (!is_reg[b] && !res_used[b % G]) {
-                res_used[b % G] = true;
-                lanes.push_back(b);
-            }
-        }
-        for (int b = 0; b < K && static_cast<int>(lanes.size()) < G; ++b) {
-            if (!is_reg[b] && std::find(lanes.begin(), lanes.end(), b) == lanes.end()) {
-                lanes.push_back(b);
-            }
-        }
-    }
-    for (int b : lanes) {
-        slot_bit[s++] = static_cast<int8_t>(b);
-        used[b] = true;
-    }
-    for (int b = 0; b < K; ++b) {
-        if (!is_reg[b] && !used[b]) {
-            slot_bit[s++] = static_cast<int8_t>(b);
-        }
-    }
-}
-
-template <typename T, typename OPT = FOp<T>>
-struct Plan
-{
-    std::vector<FBlock> blocks;
-    std::vector<FPhase> phases;
-    std::vector<OPT> ops;
-    int transposes {0};
-};
-
-// per-gate extras of the adjoint sweep: dU/dtheta and the gradient row (-1: none)
-struct AdjExtra
-{
-    double d[8];
-    int32_t row;
-};
-
-template <typename T, typename CFG = Cfg<T>, typename OPT = FOp<T>>
-void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T, OPT>& plan,
-                const AdjExtra* extra = nullptr)
-{
-    constexpr int RB = CFG::RB;
-    constexpr int L = CFG::L;
-    constexpr int G = CFG::G;
-    const int K = pb.K;
-    std::vector<int> loc(n, -1);
-    for (int j = 0; j < K; ++j) {
-        loc[pb.qubits[j]] = j;
-    }
-    FBlock fb {};
-    fb.K = K;
-    fb.nfree = n - K;
-    for (int j = 0; j < K; ++j) {
-        fb.qubit[j] = pb.qubits[j];
-    }
-    int nf = 0;
-    for (int q = 0; q < n; ++q) {
-        if (loc[q] < 0) {
-            fb.freebit[nf++] = q;
-        }
-    }
-    // the tile bit each gate needs as a register bit (-1 = none)
-    const size_t m = pb.gates.size();
-    std::vector<int> need(m, -1);
-    for (size_t k = 0; k < m; ++k) {
-        const LGate& x = g[pb.gates[k]];
-        if (x.kind != KIND_DIAG) {
-            need[k] = loc[x.target];
-        }
-    }
-    auto next_use = [&](int b, size_t from) -> size_t {
-        for (size_t k = from; k < m; ++k) {
-            if (need[k] == b) {
-                return k;
-            }
-        }
-        return SIZE_MAX;
-    };
-    // register set for a phase starting at `from`: the RB needed bits used
-    // soonest, then current bits by next use, then bits >= L (keeps the
-    // load/store layout coalesced)
-    auto choose = [&](size_t from, const std::vector<int>& keep) -> std::vector<int> {
-        std::vector<int> regs;
-        for (size_t k = from; k < m && static_cast<int>(regs.size()) < RB; ++k) {
-            if (need[k] >= 0 && std::find(regs.begin(), regs.end(), need[k]) == regs.end()) {
-                regs.push_back(need[k]);
-            }
-        }
-        for (int b : keep) {
-            if (static_cast<int>(regs.size()) >= RB) break;
-            if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
-        }
-        for (int b = K - 1; b >= L && static_cast<int>(regs.size()) < RB; --b) {
-            if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
-        }
-        for (int b = K - 1; b >= 0 && static_cast<int>(regs.size()) < RB; --b) {
-            if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
-        }
-        std::sort(regs.begin(), regs.end());
-        return regs;
-    };
-    auto has_low = [&](const std::vector<int>& regs) {
-        for (int r : regs) {
-            if (r < L) return true;
-        }
-        return false;
-    };
-    auto io_regs = [&]() {
-        std::vector<int> regs;
-        for (int b = K - 1; b >= L && static_cast<int>(regs.size()) < RB; --b) regs.push_back(b);
-        std::sort(regs.begin(), regs.end());
-        return regs;
-    };
-    struct PhaseSpec
-    {
-        std::vector<int> regs;
-        size_t begin, end;
-    };
-    std::vector<PhaseSpec> ph;
-    std::vector<int> cur = choose(0, {});
-    if (has_low(cur)) {
-        ph.push_back({io_regs(), 0, 0});
-    }
-    size_t start = 0;
-    for (size_t k = 0; k < m; ++k) {
-        if (need[k] >= 0 && std::find(cur.begin(), cur.end(), need[k]) == cur.end()) {
-            ph.push_back({cur, start, k});
-            std::vector<int> keep = cur;
-            std::sort(keep.begin(), keep.end(), [&](int x, int y) { return next_use(x, k) < next_use(y, k); });
-            cur = choose(k, keep);
-            start = k;
-        }
-    }
-    ph.push_back({cur, start, m});
-    if (has_low(cur)) {
-        ph.push_back({io_regs(), m, m});
-    }
-    // phases
-    const int TB = K - RB;
-    const size_t op_base = plan.ops.size();
-    fb.phase_begin = static_cast<int32_t>(plan.phases.size());
-    std::vector<std::vector<int8_t>> slots;
-    for (auto& spec : ph) {
-        int8_t sb[KMAX] = {};
-        make_slots(spec.regs, K, G, sb);
-        slots.emplace_back(sb, sb + K);
-        FPhase fp {};
-        for (int s = 0; s < RB; ++s) {
-            fp.rstride[s] = bit(pb.qubits[sb[s]]);
-            fp.rsw[s] = swz(1u << sb[s], G);
-        }
-        for (int j = 0; j < TB; ++j) {
-            fp.tstride[j] = bit(pb.qubits[sb[RB + j]]);
-            fp.tsw[j] = swz(1u << sb[RB + j], G);
-        }
-        fp.op_begin = static_cast<int32_t>(op_base + spec.begin);
-        fp.op_end = static_cast<int32_t>(op_base + spec.end);
-        plan.phases.push_back(fp);
-    }
-    fb.phase_end = static_cast<int32_t>(plan.phases.size());
-    plan.transposes += static_cast<int>(ph.size()) - 1;
-    // ops, resolved against the layout of their phase
-    size_t pi = 0;
-    for (size_t k = 0; k < m; ++k) {
-        while (!(k >= ph[pi].begin && k < ph[pi].end)) {
-            ++pi;
-        }
-        const auto& sb = slots[pi];
-        auto reg_slot = [&](int tilebit) -> int {
-            for (int s = 0; s < RB; ++s) {
-                if (sb[s] == tilebit) return s;
-            }
-            return -1;
-        };
-        auto thread_bit = [&](int tilebit) -> int {
-            for (int j = 0; j < TB; ++j) {
-                if (sb[RB + j] == tilebit) return j;
-            }
-            return -1;
-        };
-        const LGate& x = g[pb.gates[k]];
-        OPT op {};
-        op.tslot = NO_SLOT;
-        op.cslot = NO_SLOT;
-        if (x.control >= 0) {
-            const int lc = loc[x.control];
-            if (lc < 0) {
-                op.cglob = bit(x.control);
-            } else if (const int s = reg_slot(lc); s >= 0) {
-                op.cslot = static_cast<uint8_t>(s);
-            } else {
-                op.cthr = 1u << thread_bit(lc);
-            }
-        }
-        const bool real = x.m[1] == 0.0 && x.m[3] == 0.0 && x.m[5] == 0.0 && x.m[7] == 0.0;
-        if (x.kind == KIND_DIAG) {
-            op.kind = (x.flags & 1) ? OP_DIAG1 : OP_DIAG;
-            const int lt = loc[x.target];
-            if (lt < 0) {
-                op.tglob = bit(x.target);
-            } else if (const int s = reg_slot(lt); s >= 0) {
-                op.tslot = static_cast<uint8_t>(s);
-            } else {
-                op.tthr = 1u << thread_bit(lt);
-            }
-        } else {
-            op.tslot = static_cast<uint8_t>(reg_slot(loc[x.target]));
-            if (x.kind == KIND_ANTI) {
-                const bool pure = x.m[2] == 1.0 && x.m[3] == 0.0 && x.m[4] == 1.0 && x.m[5] == 0.0;
-                op.kind = pure ? OP_SWAP : OP_ANTI;
-            } else {
-                op.kind = real ? OP_GENR : OP_GEN;
-            }
-        }
-        for (int e = 0; e < 8; ++e) {
-            op.m[e] = static_cast<T>(x.m[e]);
-        }
-        if constexpr (OPT::HAS_D) {
-            const AdjExtra& ex = extra[pb.gates[k]];
-            op.row = ex.row;
-            for (int e = 0; e < 8; ++e) {
-                op.d[e] = static_cast<T>(ex.d[e]);
-            }
-        }
-        plan.ops.push_back(op);
-    }
-    fb.op_begin = static_cast<int32_t>(op_base);
-    fb.op_end = static_cast<int32_t>(plan.ops.size());
-    plan.blocks.push_back(fb);
 }
 
 template <typename T>
@@ -924,176 +156,6 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
 // forward planner's reordering is valid here too.
 
 template <typename T>
-struct CfgA;
-template <>
-struct CfgA<double>
-{
-    static constexpr int RB = 3;  // 8 amplitudes of psi and 8 of lambda per thread
-    static constexpr int L = 3;
-    static constexpr int G = 3;
-};
-template <>
-struct CfgA<float>
-{
-    static constexpr int RB = 4;
-    static constexpr int L = 4;
-    static constexpr int G = 4;
-};
-
-constexpr int ADJ_WARPS = 8;          // 256 threads
-constexpr int ADJ_MAX_ROWS = 256;     // parameterised gates per block
-
-template <typename T, int RB>
-struct GradGenF
-{
-    using C = typename CxT<T>::type;
-    const C (&l)[1 << RB];
-    const C (&p)[1 << RB];
-    C d00, d01, d10, d11;
-    double acc;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (lower_of_pair<S, CS>(i)) {
-                const int j = i | (1 << S);
-                const C e0 = cfma(d01, p[j], cmul(d00, p[i]));
-                const C e1 = cfma(d11, p[j], cmul(d10, p[i]));
-                const double2 a0 = to_d2(l[i]), a1 = to_d2(l[j]);
-                const double2 b0 = to_d2(e0), b1 = to_d2(e1);
-                acc += a0.x * b0.x + a0.y * b0.y + a1.x * b1.x + a1.y * b1.y;
-            }
-        }
-    }
-};
-
-template <typename T, int RB>
-struct GradDiagRegF
-{
-    using C = typename CxT<T>::type;
-    const C (&l)[1 << RB];
-    const C (&p)[1 << RB];
-    C d0, d1;
-    double acc;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (ctrl_on<CS>(i)) {
-                const C e = cmul((i & (1 << S)) ? d1 : d0, p[i]);
-                const double2 a = to_d2(l[i]), b = to_d2(e);
-                acc += a.x * b.x + a.y * b.y;
-            }
-        }
-    }
-};
-
-template <typename T, int RB>
-struct GradDiagAllF
-{
-    using C = typename CxT<T>::type;
-    const C (&l)[1 << RB];
-    const C (&p)[1 << RB];
-    C d;
-    double acc;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (ctrl_on<CS>(i)) {
-                const C e = cmul(d, p[i]);
-                const double2 a = to_d2(l[i]), b = to_d2(e);
-                acc += a.x * b.x + a.y * b.y;
-            }
-        }
-    }
-};
-
-// apply the op's U^dagger to one register array (the forward gate bodies)
-template <typename T, int RB, typename OPT>
-__device__ __forceinline__ void apply_u(typename CxT<T>::type (&v)[1 << RB], const OPT& op, uint32_t t, uint64_t base)
-{
-    using C = typename CxT<T>::type;
-    const int kind = op.kind;
-    const int ts = op.tslot;
-    const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
-    switch (kind) {
-        case OP_GEN: {
-            GenF<T, RB> f {v, make_cx<T>(op.m[0], op.m[1]), make_cx<T>(op.m[2], op.m[3]), make_cx<T>(op.m[4], op.m[5]),
-                           make_cx<T>(op.m[6], op.m[7])};
-            dispatch_sc<RB>(ts, cs, f);
-            return;
-        }
-        case OP_GENR: {
-            GenRF<T, RB> f {v, op.m[0], op.m[2], op.m[4], op.m[6]};
-            dispatch_sc<RB>(ts, cs, f);
-            return;
-        }
-        case OP_ANTI: {
-            AntiF<T, RB, false> f {v, make_cx<T>(op.m[2], op.m[3]), make_cx<T>(op.m[4], op.m[5])};
-            dispatch_sc<RB>(ts, cs, f);
-            return;
-        }
-        case OP_SWAP: {
-            AntiF<T, RB, true> f {v, make_cx<T>(0, 0), make_cx<T>(0, 0)};
-            dispatch_sc<RB>(ts, cs, f);
-            return;
-        }
-        default:
-            break;
-    }
-    const C d1 = make_cx<T>(op.m[6], op.m[7]);
-    const C d0 = make_cx<T>(op.m[0], op.m[1]);
-    if (ts != NO_SLOT) {
-        if (kind == OP_DIAG1) {
-            DiagRegF<T, RB, true> f {v, d0, d1};
-            dispatch_sc<RB>(ts, cs, f);
-        } else {
-            DiagRegF<T, RB, false> f {v, d0, d1};
-            dispatch_sc<RB>(ts, cs, f);
-        }
-        return;
-    }
-    const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
-    if (!b && kind == OP_DIAG1) {
-        return;
-    }
-    DiagAllF<T, RB> f {v, b ? d1 : d0};
-    dispatch_c<RB, 99>(cs, f);
-}
-
-// Re <lambda| D psi> over this thread's registers for a parameterised op
-template <typename T, int RB, typename OPT>
-__device__ __forceinline__ double grad_term(const typename CxT<T>::type (&l)[1 << RB],
-                                            const typename CxT<T>::type (&p)[1 << RB], const OPT& op, uint32_t t,
-                                            uint64_t base)
-{
-    const int kind = op.kind;
-    const int ts = op.tslot;
-    const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
-    if (kind < OP_DIAG) {
-        GradGenF<T, RB> f {l, p, make_cx<T>(op.d[0], op.d[1]), make_cx<T>(op.d[2], op.d[3]), make_cx<T>(op.d[4], op.d[5]),
-                           make_cx<T>(op.d[6], op.d[7]), 0.0};
-        dispatch_sc<RB>(ts, cs, f);
-        return f.acc;
-    }
-    const auto d0 = make_cx<T>(op.d[0], op.d[1]);
-    const auto d1 = make_cx<T>(op.d[6], op.d[7]);
-    if (ts != NO_SLOT) {
-        GradDiagRegF<T, RB> f {l, p, d0, d1, 0.0};
-        dispatch_sc<RB>(ts, cs, f);
-        return f.acc;
-    }
-    const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
-    GradDiagAllF<T, RB> f {l, p, b ? d1 : d0, 0.0};
-    dispatch_c<RB, 99>(cs, f);
-    return f.acc;
-}
-
-template <typename T>
 __global__ void __launch_bounds__(256, 2) k_fused_adj(typename CxT<T>::type* __restrict__ psi,
                                                       typename CxT<T>::type* __restrict__ lam,
                                                       const FBlock* __restrict__ blk, const FPhase* __restrict__ phases,
@@ -1102,7 +164,6 @@ __global__ void __launch_bounds__(256, 2) k_fused_adj(typename CxT<T>::type* __r
 {
     using C = typename CxT<T>::type;
     constexpr int RB = CfgA<T>::RB;
-    constexpr int R = 1 << RB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ FBlock bk;
     __shared__ FPhase sph[MAX_PHASES_PER_BLOCK];
@@ -1111,137 +172,19 @@ __global__ void __launch_bounds__(256, 2) k_fused_adj(typename CxT<T>::type* __r
         bk = *blk;
     }
     __syncthreads();
-    const int K = bk.K;
-    const int TB = K - RB;
-    const int np = bk.phase_end - bk.phase_begin;
     const int no = bk.op_end - bk.op_begin;
-    const size_t tile_bytes = sizeof(C) << K;
+    const size_t tile_bytes = sizeof(C) << bk.K;
     C* smp = reinterpret_cast<C*>(smem_raw);
     C* sml = reinterpret_cast<C*>(smem_raw + tile_bytes);
     FOpA<T>* sops = reinterpret_cast<FOpA<T>*>(smem_raw + 2 * tile_bytes);
     double* acc = reinterpret_cast<double*>(smem_raw + 2 * tile_bytes + static_cast<size_t>(no) * sizeof(FOpA<T>));
-    {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(phases + bk.phase_begin);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(sph);
-        for (int w = t; w < np * static_cast<int>(sizeof(FPhase) / 4); w += blockDim.x) {
-            dst[w] = src[w];
-        }
-        const uint32_t* so = reinterpret_cast<const uint32_t*>(ops + bk.op_begin);
-        uint32_t* dop = reinterpret_cast<uint32_t*>(sops);
-        for (int w = t; w < no * static_cast<int>(sizeof(FOpA<T>) / 4); w += blockDim.x) {
-            dop[w] = so[w];
-        }
-        for (int w = t; w < n_rows * ADJ_WARPS; w += blockDim.x) {
-            acc[w] = 0.0;
-        }
+    stage_block(bk, phases, ops, sph, sops, t);
+    for (int w = t; w < n_rows * ADJ_WARPS; w += blockDim.x) {
+        acc[w] = 0.0;
     }
     __syncthreads();
-    const int op0 = bk.op_begin;
-    const int lane = t & 31;
-    const int warp = t >> 5;
-
     for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        uint64_t base = 0;
-        for (int k = 0; k < bk.nfree; ++k) {
-            if ((tile >> k) & 1) {
-                base |= uint64_t {1} << bk.freebit[k];
-            }
-        }
-        C vp[R];
-        C vl[R];
-        {
-            const FPhase& ph = sph[0];
-            uint64_t toff = 0;
-            for (int j = 0; j < TB; ++j) {
-                if ((t >> j) & 1) {
-                    toff += ph.tstride[j];
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < R; ++i) {
-                uint64_t o = 0;
-#pragma unroll
-                for (int s = 0; s < RB; ++s) {
-                    if (i & (1 << s)) {
-                        o += ph.rstride[s];
-                    }
-                }
-                vp[i] = psi[base + toff + o];
-                vl[i] = lam[base + toff + o];
-            }
-        }
-        uint32_t tsw_prev = 0;
-        for (int p = 0; p < np; ++p) {
-            const FPhase& ph = sph[p];
-            uint32_t tsw = 0;
-            for (int j = 0; j < TB; ++j) {
-                if ((t >> j) & 1) {
-                    tsw ^= ph.tsw[j];
-                }
-            }
-            if (p > 0) {
-                const FPhase& pp = sph[p - 1];
-#pragma unroll
-                for (int i = 0; i < R; ++i) {
-                    const uint32_t a = tsw_prev ^ xor_terms<RB>(i, pp.rsw);
-                    smp[a] = vp[i];
-                    sml[a] = vl[i];
-                }
-                __syncthreads();
-#pragma unroll
-                for (int i = 0; i < R; ++i) {
-                    const uint32_t a = tsw ^ xor_terms<RB>(i, ph.rsw);
-                    vp[i] = smp[a];
-                    vl[i] = sml[a];
-                }
-                __syncthreads();
-            }
-            tsw_prev = tsw;
-            for (int o = ph.op_begin; o < ph.op_end; ++o) {
-                const FOpA<T>& op = sops[o - op0];
-                if ((base & op.cglob) != op.cglob) {
-                    continue;  // control outside the tile is 0: nothing changes, the derivative term is 0
-                }
-                const bool on = (t & op.cthr) == op.cthr;
-                if (on) {
-                    apply_u<T, RB>(vp, op, t, base);
-                }
-                if (op.row >= 0) {
-                    double g = on ? grad_term<T, RB>(vl, vp, op, t, base) : 0.0;
-#pragma unroll
-                    for (int s = 16; s > 0; s >>= 1) {
-                        g += __shfl_down_sync(0xffffffffU, g, s);
-                    }
-                    if (lane == 0) {
-                        acc[op.row * ADJ_WARPS + warp] += g;
-                    }
-                }
-                if (on) {
-                    apply_u<T, RB>(vl, op, t, base);
-                }
-            }
-        }
-        {
-            const FPhase& ph = sph[np - 1];
-            uint64_t toff = 0;
-            for (int j = 0; j < TB; ++j) {
-                if ((t >> j) & 1) {
-                    toff += ph.tstride[j];
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < R; ++i) {
-                uint64_t o = 0;
-#pragma unroll
-                for (int s = 0; s < RB; ++s) {
-                    if (i & (1 << s)) {
-                        o += ph.rstride[s];
-                    }
-                }
-                psi[base + toff + o] = vp[i];
-                lam[base + toff + o] = vl[i];
-            }
-        }
+        adj_tile<T, RB, false>(psi, lam, bk, sph, sops, tile, smp, sml, acc, t);
     }
     __syncthreads();
     for (int r = t; r < n_rows; r += blockDim.x) {
@@ -1289,7 +232,7 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
         ex.push_back(e);
     }
     // cap the ops of a block so its gradient rows fit the shared-memory slots
-    const auto pbs = form_blocks(lg, n, K, L, static_cast<size_t>(std::min(ADJ_MAX_ROWS, tuning().fused_max_ops)));
+    const auto pbs = form_blocks(lg, n, K, L, static_cast<size_t>(std::min(ADJ_MAX_OPS, tuning().fused_max_ops)));
     Plan<T, FOpA<T>> plan;
     std::vector<std::vector<int32_t>> rows_of_block;
     for (const auto& pb : pbs) {
@@ -1358,7 +301,9 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
     auto* d_part = reinterpret_cast<double*>(dev + off_part);
     static bool attr = false;
     if (!attr) {
-        KT_CUDA(cudaFuncSetAttribute(k_fused_adj<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024));
+        const int most = static_cast<int>(2 * (sizeof(C) << (CfgA<T>::RB + TBMAX)) + ADJ_MAX_OPS * sizeof(FOpA<T>) +
+                                          ADJ_MAX_OPS * ADJ_WARPS * sizeof(double));
+        KT_CUDA(cudaFuncSetAttribute(k_fused_adj<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         attr = true;
     }
     const int threads = 1 << (K - RB);

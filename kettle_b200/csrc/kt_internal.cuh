@@ -23,6 +23,10 @@ namespace kt
 // errors
 void set_error(int32_t code, const std::string& msg);
 int32_t cuda_fail(cudaError_t e, const char* where);
+const char* last_error_cstr();
+// replace this thread's error text with an already formatted message (one
+// captured on another thread)
+void set_error_text(const std::string& text);
 
 #define KT_CUDA(call)                                   \
     do {                                                \
@@ -94,6 +98,11 @@ int32_t lower_gates(const kt_gate* gates, int64_t n_gates, const double* params,
 
 // conj(U) on (t + shift, c + shift): the column half of U rho U^dagger.
 LGate conj_shifted(const LGate& g, int shift);
+
+// Analytic dU/dtheta (row-major interleaved, like LGate::m) of the rotation
+// gates RX/RY/RZ/P and their controlled forms at angle th; false (d = 0) for
+// every other op.
+bool gate_derivative(int op, double th, double* d);
 
 // ---------------------------------------------------------------------------
 // kernels (launchers return KT_OK or a CUDA error status)

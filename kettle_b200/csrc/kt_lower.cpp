@@ -27,6 +27,11 @@ const char* last_error_cstr()
     return g_last_error.c_str();
 }
 
+void set_error_text(const std::string& text)
+{
+    g_last_error = text;
+}
+
 int32_t cuda_fail(cudaError_t e, const char* where)
 {
     std::ostringstream os;
@@ -294,6 +299,32 @@ int32_t lower_gates(const kt_gate* gates, int64_t n_gates, const double* params,
         out.push_back(l);
     }
     return KT_OK;
+}
+
+bool gate_derivative(int op, double th, double* d)
+{
+    std::fill(d, d + 8, 0.0);
+    const double c = std::cos(th / 2.0), s = std::sin(th / 2.0);
+    switch (op) {
+        case KT_OP_RX: case KT_OP_CRX:
+            // [[c, -i s], [-i s, c]]' = [[-s/2, -i c/2], [-i c/2, -s/2]]
+            d[0] = -0.5 * s; d[3] = -0.5 * c; d[5] = -0.5 * c; d[6] = -0.5 * s;
+            return true;
+        case KT_OP_RY: case KT_OP_CRY:
+            // [[c, -s], [s, c]]' = [[-s/2, -c/2], [c/2, -s/2]]
+            d[0] = -0.5 * s; d[2] = -0.5 * c; d[4] = 0.5 * c; d[6] = -0.5 * s;
+            return true;
+        case KT_OP_RZ: case KT_OP_CRZ:
+            // diag(c - i s, c + i s)' = diag(-s/2 - i c/2, -s/2 + i c/2)
+            d[0] = -0.5 * s; d[1] = -0.5 * c; d[6] = -0.5 * s; d[7] = 0.5 * c;
+            return true;
+        case KT_OP_P: case KT_OP_CP:
+            // diag(1, cos + i sin)' = diag(0, -sin + i cos)
+            d[6] = -std::sin(th); d[7] = std::cos(th);
+            return true;
+        default:
+            return false;
+    }
 }
 
 LGate conj_shifted(const LGate& g, int shift)

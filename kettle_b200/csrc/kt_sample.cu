@@ -243,17 +243,28 @@ __global__ void k_sample_fast(const double* __restrict__ p, const double* __rest
 
 // exact tier -------------------------------------------------------------------
 // The sequential sum s_i = fl(s_{i-1} + p_i) of std::partial_sum, computed
-// exactly by one block.  While s stays in one binade [2^E, 2^(E+1)) every
-// representable value is a multiple of u = 2^(E-52), so (no tie, no binade
-// exit) fl(s + p) = s + rint(p / u) * u exactly: a run of additions is an
-// integer prefix sum, which the block computes in parallel (uint64 units).
-// An element whose p/u is an exact tie (.5), is large (>= 2^50 units), or
-// whose running sum leaves the binade is added with one IEEE add instead,
-// after which the block continues from the new (exact) s.  Each 8192-element
-// tile costs one block scan, plus one round per such element.
+// exactly.  While s stays in one binade [2^(E-1), 2^E) every representable
+// value is a multiple of u = 2^(E-53), so (no tie, no binade exit)
+// fl(s + p) = s + rint(p / u) * u exactly: a run of additions is an integer
+// prefix sum.  The array is cut into tiles of XS_TILE elements:
+//  1. tile sums (FP64, any order) and their exclusive scan give each tile an
+//     approximate start value, hence a guess of its binade (or "all zero");
+//  2. every tile with a guess sums rint(p / u) in uint64, flagging exact ties
+//     (.5) and huge terms (>= 2^50 units);
+//  3. one block walks the tiles in order with the exact running value s: a
+//     tile whose guess is s's binade, has no flag and does not reach 2^53
+//     units is passed over in O(1) (its start value is recorded); any other
+//     tile is computed element by element from the exact s (the same integer
+//     scan, with one IEEE add for each tie, huge term or binade exit);
+//  4. every recorded tile writes its CDF from its exact start value.
+// A wrong guess only sends a tile down the element-by-element path: the
+// result never depends on the approximate sums.
 constexpr int XS_THREADS = 1024;
 constexpr int XS_EPT = 16;
 constexpr int XS_TILE = XS_THREADS * XS_EPT;
+constexpr int TILE_ZERO = -100000;    // every p in the tile is +0: s passes unchanged
+constexpr int TILE_DIRTY = -200000;   // no binade guess, or a flagged term
+constexpr double TINY = 0x1p-900;     // below this the running value is summed with IEEE adds
 
 __device__ __forceinline__ unsigned long long block_excl_scan_u64(unsigned long long v, unsigned long long* sh,
                                                                   unsigned long long& total)
@@ -291,43 +302,51 @@ __device__ __forceinline__ unsigned long long block_excl_scan_u64(unsigned long 
     return r;
 }
 
-__global__ void __launch_bounds__(XS_THREADS) k_exact_cdf(const double* __restrict__ p, uint64_t N, double* __restrict__ cdf)
+// shared state of the element-by-element path
+struct XState
 {
-    __shared__ unsigned long long sh[32];
-    __shared__ double s_sh;
-    __shared__ unsigned long long i_sh;
-    __shared__ unsigned int viol_sh;
+    unsigned long long sh[32];
+    double s;
+    unsigned long long i;
+    unsigned int viol;
+};
+
+// cdf[beg, end) as the sequential sum continued from the exact value s_in, by
+// the whole block (XS_THREADS threads); returns the value after element end-1.
+__device__ double exact_range(const double* __restrict__ p, uint64_t beg, uint64_t end, double s_in,
+                              double* __restrict__ cdf, XState& X)
+{
     const int t = threadIdx.x;
+    __syncthreads();
     if (t == 0) {
-        s_sh = p[0];
-        cdf[0] = p[0];
-        i_sh = 1;
+        X.s = s_in;
+        X.i = beg;
     }
     __syncthreads();
     constexpr unsigned long long TWO53 = 1ULL << 53;
     while (true) {
-        const uint64_t i = i_sh;
-        const double s = s_sh;
-        if (i >= N) {
+        const uint64_t i = X.i;
+        const double s = X.s;
+        __syncthreads();  // every thread has read (i, s) before anyone moves them on
+        if (i >= end) {
             break;
         }
-        if (s < 0x1p-900) {
+        if (s < TINY) {
             // zero or tiny running value (subnormal spacing, huge 1/ulp): plain IEEE steps
             if (t == 0) {
                 const double nv = __dadd_rn(s, p[i]);
-                s_sh = nv;
+                X.s = nv;
                 cdf[i] = nv;
-                i_sh = i + 1;
+                X.i = i + 1;
             }
             __syncthreads();
             continue;
         }
         int E;
-        frexp(s, &E);                       // s in [2^(E-1), 2^E)
+        frexp(s, &E);                             // s in [2^(E-1), 2^E)
         const double inv_u = ldexp(1.0, 53 - E);  // 1 / ulp(s)
         const double u = ldexp(1.0, E - 53);
         const unsigned long long m = static_cast<unsigned long long>(s * inv_u);  // exact, in [2^52, 2^53)
-        // this thread's elements: i + t*EPT + k
         unsigned long long r[XS_EPT];
         unsigned int bad = XS_TILE;  // first flagged local index
         unsigned long long run = 0;
@@ -336,20 +355,20 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_cdf(const double* __restri
         for (int k = 0; k < XS_EPT; ++k) {
             const uint64_t g = b0 + k;
             double q = 0.0;
-            if (g < N) {
+            if (g < end) {
                 q = p[g] * inv_u;
             }
             const double f = floor(q);
             const bool tie = (q - f) == 0.5;
             const bool big = !(q < 1125899906842624.0);  // 2^50 (also catches inf)
-            if ((tie || big) && g < N && bad == XS_TILE) {
+            if ((tie || big) && g < end && bad == XS_TILE) {
                 bad = t * XS_EPT + k;
             }
             r[k] = big ? 0ULL : static_cast<unsigned long long>(rint(q));
             run += r[k];
         }
         unsigned long long total;
-        const unsigned long long excl = block_excl_scan_u64(run, sh, total);
+        const unsigned long long excl = block_excl_scan_u64(run, X.sh, total);
         // binade exit: first element whose running sum reaches 2^53 units
         unsigned long long acc = m + excl;
 #pragma unroll
@@ -361,13 +380,13 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_cdf(const double* __restri
             }
         }
         if (t == 0) {
-            viol_sh = XS_TILE;
+            X.viol = XS_TILE;
         }
         __syncthreads();
-        atomicMin(&viol_sh, bad);
+        atomicMin(&X.viol, bad);
         __syncthreads();
-        const uint64_t tile_len = (N - i) < XS_TILE ? (N - i) : XS_TILE;
-        const unsigned int v = viol_sh < tile_len ? viol_sh : static_cast<unsigned int>(tile_len);
+        const uint64_t tile_len = (end - i) < XS_TILE ? (end - i) : XS_TILE;
+        const unsigned int v = X.viol < tile_len ? X.viol : static_cast<unsigned int>(tile_len);
         // commit the elements before v
         acc = m + excl;
 #pragma unroll
@@ -378,40 +397,299 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_cdf(const double* __restri
                 cdf[i + li] = static_cast<double>(acc) * u;
             }
         }
-        // the value before element v, for thread 0's IEEE step
         if (v < tile_len) {
-            // running value just before v: the thread owning v - 1 knows it
-            const unsigned int last = v;  // element index to add with an IEEE add
-            if (last == 0) {
+            // element v gets one IEEE add onto the value just before it
+            if (v == 0) {
                 if (t == 0) {
                     const double nv = __dadd_rn(s, p[i]);
                     cdf[i] = nv;
-                    s_sh = nv;
-                    i_sh = i + 1;
+                    X.s = nv;
+                    X.i = i + 1;
                 }
             } else {
-                const unsigned int owner = (last - 1) / XS_EPT;
+                const unsigned int owner = (v - 1) / XS_EPT;
                 if (static_cast<unsigned int>(t) == owner) {
                     unsigned long long a2 = m + excl;
                     for (int k = 0; k < XS_EPT; ++k) {
-                        if (t * XS_EPT + k < last) {
+                        if (t * XS_EPT + k < v) {
                             a2 += r[k];
                         }
                     }
                     const double before = static_cast<double>(a2) * u;
-                    const double nv = __dadd_rn(before, p[i + last]);
-                    cdf[i + last] = nv;
-                    s_sh = nv;
-                    i_sh = i + last + 1;
+                    const double nv = __dadd_rn(before, p[i + v]);
+                    cdf[i + v] = nv;
+                    X.s = nv;
+                    X.i = i + v + 1;
                 }
             }
-        } else {
-            if (t == 0) {
-                s_sh = static_cast<double>(m + total) * u;
-                i_sh = i + tile_len;
+        } else if (t == 0) {
+            X.s = static_cast<double>(m + total) * u;
+            X.i = i + tile_len;
+        }
+        __syncthreads();
+    }
+    return X.s;
+}
+
+// 1. FP64 sum of each tile (any order)
+__global__ void __launch_bounds__(256) k_tile_sums(const double* __restrict__ p, uint64_t N, double* __restrict__ tsum)
+{
+    __shared__ double sh[8];
+    const uint64_t beg = static_cast<uint64_t>(blockIdx.x) * XS_TILE;
+    const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+    double acc = 0.0;
+    for (uint64_t i = beg + threadIdx.x; i < end; i += 256) {
+        acc += p[i];
+    }
+    acc = warp_sum_d(acc);
+    if ((threadIdx.x & 31) == 0) {
+        sh[threadIdx.x >> 5] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            s += sh[w];
+        }
+        tsum[blockIdx.x] = s;
+    }
+}
+
+// 1b. one block: approximate start value of every tile, and its binade guess
+__global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restrict__ tsum, uint64_t n_tiles,
+                                                           int* __restrict__ code)
+{
+    __shared__ double sh[32];
+    const int t = threadIdx.x;
+    const uint64_t per = (n_tiles + XS_THREADS - 1) / XS_THREADS;
+    const uint64_t b = static_cast<uint64_t>(t) * per;
+    const uint64_t e = b + per < n_tiles ? b + per : n_tiles;
+    double local = 0.0;
+    for (uint64_t k = b; k < e; ++k) {
+        local += tsum[k];
+    }
+    // exclusive block scan of the thread sums (FP64, approximate)
+    const int lane = t & 31, warp = t >> 5;
+    double x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffU, x, o);
+        if (lane >= o) {
+            x += y;
+        }
+    }
+    if (lane == 31) {
+        sh[warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double w = sh[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffU, w, o);
+            if (lane >= o) {
+                w += y;
+            }
+        }
+        sh[lane] = w;
+    }
+    __syncthreads();
+    double a0 = ((warp > 0) ? sh[warp - 1] : 0.0) + (x - local);
+    for (uint64_t k = b; k < e; ++k) {
+        const double ts = tsum[k];
+        const double a1 = a0 + ts;
+        int c = TILE_DIRTY;
+        if (ts == 0.0) {
+            c = TILE_ZERO;
+        } else if (a0 >= 2.0 * TINY) {
+            int e0, e1;
+            frexp(a0 * (1.0 - 0x1p-20), &e0);
+            frexp(a1 * (1.0 + 0x1p-20), &e1);
+            if (e0 == e1) {
+                c = e0;
+            }
+        }
+        code[k] = c;
+        a0 = a1;
+    }
+}
+
+// 2. integer sum of a tile in the units of its guessed binade; flags demote it
+__global__ void __launch_bounds__(256) k_tile_ints(const double* __restrict__ p, uint64_t N, int* __restrict__ code,
+                                                   unsigned long long* __restrict__ ints)
+{
+    __shared__ unsigned long long sh[8];
+    __shared__ int flag_sh;
+    const int c = code[blockIdx.x];
+    if (c == TILE_ZERO || c == TILE_DIRTY) {
+        return;
+    }
+    if (threadIdx.x == 0) {
+        flag_sh = 0;
+    }
+    __syncthreads();
+    const double inv_u = ldexp(1.0, 53 - c);
+    const uint64_t beg = static_cast<uint64_t>(blockIdx.x) * XS_TILE;
+    const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+    unsigned long long acc = 0;
+    bool flag = false;
+    for (uint64_t i = beg + threadIdx.x; i < end; i += 256) {
+        const double q = p[i] * inv_u;
+        const double f = floor(q);
+        flag = flag || ((q - f) == 0.5) || !(q < 1125899906842624.0);
+        acc += flag ? 0ULL : static_cast<unsigned long long>(rint(q));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        acc += __shfl_down_sync(0xffffffffU, acc, o);
+    }
+    if (flag) {
+        flag_sh = 1;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sh[threadIdx.x >> 5] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (int w = 0; w < 8; ++w) {
+            s += sh[w];
+        }
+        ints[blockIdx.x] = s;
+        if (flag_sh) {
+            code[blockIdx.x] = TILE_DIRTY;
+        }
+    }
+}
+
+// 3. one block: the exact running value through all tiles.  carry[t] gets the
+// exact value before tile t, or -1 when the tile's CDF was written here.
+__global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const double* __restrict__ p, uint64_t N, uint64_t n_tiles,
+                                                            const int* __restrict__ code,
+                                                            const unsigned long long* __restrict__ ints,
+                                                            double* __restrict__ carry, double* __restrict__ cdf)
+{
+    __shared__ XState X;
+    __shared__ unsigned long long t_sh;
+    __shared__ double s_sh;
+    __shared__ unsigned int first_sh;
+    __shared__ unsigned long long m_sh;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        t_sh = 0;
+        s_sh = 0.0;  // the value before element 0: cdf[0] = 0 + p[0] = p[0]
+    }
+    __syncthreads();
+    constexpr unsigned long long TWO53 = 1ULL << 53;
+    while (true) {
+        const uint64_t t0 = t_sh;
+        const double s = s_sh;
+        if (t == 0) {
+            first_sh = XS_THREADS;
+        }
+        __syncthreads();
+        if (t0 >= n_tiles) {
+            break;
+        }
+        // fast step over tiles t0 .. t0 + XS_THREADS - 1
+        const bool normal = s >= TINY;
+        int E = 0;
+        unsigned long long m = 0;
+        double u = 0.0;
+        if (normal) {
+            frexp(s, &E);
+            m = static_cast<unsigned long long>(s * ldexp(1.0, 53 - E));
+            u = ldexp(1.0, E - 53);
+        }
+        const uint64_t tile = t0 + static_cast<uint64_t>(t);
+        const int c = tile < n_tiles ? code[tile] : TILE_DIRTY;
+        const unsigned long long I = (tile < n_tiles && c != TILE_ZERO && c != TILE_DIRTY) ? ints[tile] : 0ULL;
+        unsigned long long total;
+        const unsigned long long excl = block_excl_scan_u64(I, X.sh, total);
+        bool ok = tile < n_tiles && (c == TILE_ZERO || (normal && c == E));
+        if (ok && normal && m + excl + I >= TWO53) {
+            ok = false;
+        }
+        if (!ok) {
+            atomicMin(&first_sh, static_cast<unsigned int>(t));
+        }
+        __syncthreads();
+        const unsigned int first = first_sh;
+        if (static_cast<unsigned int>(t) < first) {
+            carry[tile] = normal ? static_cast<double>(m + excl) * u : s;
+            if (static_cast<unsigned int>(t) + 1 == first) {
+                m_sh = m + excl + I;
             }
         }
         __syncthreads();
+        if (t == 0) {
+            if (first > 0) {
+                s_sh = normal ? static_cast<double>(m_sh) * u : s;
+            }
+            t_sh = t0 + first;
+        }
+        __syncthreads();
+        if (first == XS_THREADS) {
+            continue;
+        }
+        const uint64_t bad = t_sh;
+        if (bad >= n_tiles) {
+            break;
+        }
+        // tile `bad`, element by element from the exact value
+        const uint64_t beg = bad * XS_TILE;
+        const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+        const double s_out = exact_range(p, beg, end, s_sh, cdf, X);
+        __syncthreads();
+        if (t == 0) {
+            carry[bad] = -1.0;
+            s_sh = s_out;
+            t_sh = bad + 1;
+        }
+        __syncthreads();
+    }
+}
+
+// 4. the CDF of every tile passed over in step 3, from its exact start value
+__global__ void __launch_bounds__(XS_THREADS) k_tile_write(const double* __restrict__ p, uint64_t N,
+                                                           const int* __restrict__ code,
+                                                           const double* __restrict__ carry, double* __restrict__ cdf)
+{
+    __shared__ unsigned long long sh[32];
+    const double c0 = carry[blockIdx.x];
+    if (c0 < 0.0) {
+        return;
+    }
+    const uint64_t beg = static_cast<uint64_t>(blockIdx.x) * XS_TILE;
+    const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+    const uint64_t b0 = beg + static_cast<uint64_t>(threadIdx.x) * XS_EPT;
+    const int c = code[blockIdx.x];
+    if (c == TILE_ZERO) {
+        for (int k = 0; k < XS_EPT; ++k) {
+            if (b0 + k < end) {
+                cdf[b0 + k] = c0;
+            }
+        }
+        return;
+    }
+    const double inv_u = ldexp(1.0, 53 - c);
+    const double u = ldexp(1.0, c - 53);
+    const unsigned long long m = static_cast<unsigned long long>(c0 * inv_u);
+    unsigned long long r[XS_EPT];
+    unsigned long long run = 0;
+#pragma unroll
+    for (int k = 0; k < XS_EPT; ++k) {
+        r[k] = (b0 + k < end) ? static_cast<unsigned long long>(rint(p[b0 + k] * inv_u)) : 0ULL;
+        run += r[k];
+    }
+    unsigned long long total;
+    unsigned long long acc = m + block_excl_scan_u64(run, sh, total);
+#pragma unroll
+    for (int k = 0; k < XS_EPT; ++k) {
+        acc += r[k];
+        if (b0 + k < end) {
+            cdf[b0 + k] = static_cast<double>(acc) * u;
+        }
     }
 }
 
@@ -498,7 +776,12 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
     const size_t off_out = al(off_canon + ns * 8);
     const size_t off_unc = al(off_out + ns * 8);
     const size_t off_bound = al(off_unc + 8);
-    if (const int32_t rc = s.scratch.reserve(off_bound + 8); rc != KT_OK) {
+    const uint64_t n_xt = (N + XS_TILE - 1) / XS_TILE;
+    const size_t off_tsum = al(off_bound + 8);
+    const size_t off_code = al(off_tsum + n_xt * 8);
+    const size_t off_ints = al(off_code + n_xt * 4);
+    const size_t off_carry = al(off_ints + n_xt * 8);
+    if (const int32_t rc = s.scratch.reserve(off_carry + n_xt * 8); rc != KT_OK) {
         return rc;
     }
     double* dp = static_cast<double*>(s.scratch2.ptr);
@@ -512,6 +795,10 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
     auto* d_out = reinterpret_cast<uint64_t*>(base + off_out);
     auto* d_unc = reinterpret_cast<int*>(base + off_unc);
     auto* d_bound = reinterpret_cast<double*>(base + off_bound);
+    auto* d_tsum = reinterpret_cast<double*>(base + off_tsum);
+    auto* d_code = reinterpret_cast<int*>(base + off_code);
+    auto* d_ints = reinterpret_cast<unsigned long long*>(base + off_ints);
+    auto* d_carry = reinterpret_cast<double*>(base + off_carry);
 
     if (const int32_t rc = device_probabilities(s, noise, dp); rc != KT_OK) {
         return rc;
@@ -544,8 +831,17 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
         }
     }
     if (unc != 0) {
-        k_exact_cdf<<<1, XS_THREADS, 0, s.stream>>>(dp, N, dcdf);
-        KT_CHECK_LAUNCH("k_exact_cdf");
+        const uint64_t n_tiles = (N + XS_TILE - 1) / XS_TILE;
+        k_tile_sums<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_tsum);
+        KT_CHECK_LAUNCH("k_tile_sums");
+        k_tile_guess<<<1, XS_THREADS, 0, s.stream>>>(d_tsum, n_tiles, d_code);
+        KT_CHECK_LAUNCH("k_tile_guess");
+        k_tile_ints<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_code, d_ints);
+        KT_CHECK_LAUNCH("k_tile_ints");
+        k_exact_chain<<<1, XS_THREADS, 0, s.stream>>>(dp, N, n_tiles, d_code, d_ints, d_carry, dcdf);
+        KT_CHECK_LAUNCH("k_exact_chain");
+        k_tile_write<<<static_cast<unsigned>(n_tiles), XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf);
+        KT_CHECK_LAUNCH("k_tile_write");
         KT_CUDA(cudaMemsetAsync(d_nz, 0, 8, s.stream));
         const unsigned lb_blocks = static_cast<unsigned>(std::min<uint64_t>((N + 255) / 256, sm_count() * 8ULL));
         k_last_below<<<lb_blocks, 256, 0, s.stream>>>(dcdf, N, d_nz);

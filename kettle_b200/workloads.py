@@ -155,3 +155,25 @@ def xxz_chain(n: int, seed: int, delta: float = 0.5, j: float = 1.0):
         strs.append(pauli(n, {i: "Z"}))
         cs.append(h[i])
     return np.concatenate(strs), np.asarray(cs, dtype=np.complex128)
+
+
+def hea_batch(count: int, seed: int, qubits=(10, 22), layers=(2, 10), n_strings: int = 50):
+    """`count` hardware-efficient-ansatz instances with qubit counts uniform
+    over `qubits` and depths uniform over `layers` (inclusive), each with its
+    own parameters (uniform in [-pi, pi)) and its own Hamiltonian of
+    `n_strings` random Pauli strings with N(0,1) coefficients.
+
+    Returns (circuits, params): circuits is a list of
+    (n_qubits, gates, n_params, strings, coeffs) in the form
+    kettle_b200.capi.batch_items takes; params is the concatenated vector."""
+    rng = np.random.default_rng(seed)
+    circuits, params = [], []
+    for b in range(count):
+        n = int(rng.integers(qubits[0], qubits[1] + 1))
+        d = int(rng.integers(layers[0], layers[1] + 1))
+        sub = int(rng.integers(1 << 31))
+        gates, p = hea(n, d, seed=sub)
+        strings, coeffs = random_paulis(n, n_strings, seed=sub + 1)
+        circuits.append((n, gates, p.size, strings, coeffs))
+        params.append(p)
+    return circuits, np.concatenate(params)

@@ -55,3 +55,30 @@ def test_no_gpu_fails_loudly():
 def test_canonicals_helper_is_host_only():
     v = capi.canonicals_mt19937(5489, 10)
     assert np.all((v >= 0) & (v < 1))
+
+
+def test_batch_rejects_bad_items_on_the_host():
+    from kettle_b200 import workloads as W
+    g, p = W.hea(4, 1, seed=0)
+    s, c = W.random_paulis(4, 3, seed=0)
+    items, gates, strings, coeffs, n_params = capi.batch_items([(4, g, p.size, s, c)])
+    bad = items.copy()
+    bad["n_params"] = p.size + 1          # parameter range past the end of params
+    with pytest.raises(capi.KettleError) as e:
+        capi.Batch(bad, gates, strings, coeffs, n_params)
+    assert e.value.code == -1 and "out of range" in str(e.value)
+    wide = strings.copy()
+    wide["z"][0] = 1 << 6                  # a Pauli string on a qubit the item does not have
+    with pytest.raises(capi.KettleError) as e:
+        capi.Batch(items, gates, wide, coeffs, n_params)
+    assert "outside its qubits" in str(e.value)
+    slot = gates.copy()
+    slot["param"][0] = 99                  # a gate bound to a slot the item does not have
+    with pytest.raises(capi.KettleError) as e:
+        capi.Batch(items, slot, strings, coeffs, n_params)
+    assert "parameter slot 99" in str(e.value)
+    meas = np.concatenate([gates, W.gate("M", 0)])
+    items2, _, _, _, _ = capi.batch_items([(4, meas, p.size, s, c)])
+    with pytest.raises(capi.KettleError) as e:
+        capi.Batch(items2, meas, strings, coeffs, n_params)
+    assert "M gates" in str(e.value)

@@ -96,3 +96,14 @@ def test_fused_complex64(engine):
     _, g0, _ = _grad(n, gates, params, strings, coeffs, fused=True)
     _, g1, _ = _grad(n, gates, params, strings, coeffs, fused=True, dtype=capi.KT_C64)
     assert np.abs(g0 - g1).max() < 1e-3
+
+
+def test_fused_deep_blocks(engine):
+    """A deep ansatz whose adjoint blocks hit the per-block op cap (shared-memory budget)."""
+    n = 16
+    gates, params = W.hea(n, 10, seed=4)
+    strings, coeffs = W.xxz_chain(n, seed=4)
+    e0, g0, _ = _grad(n, gates, params, strings, coeffs, fused=False)
+    e1, g1, _ = _grad(n, gates, params, strings, coeffs, fused=True)
+    assert e0 == e1
+    assert np.abs(g0 - g1).max() < 1e-11

@@ -375,3 +375,60 @@ def test_sampling_large_state_exact(engine, port):
     idx, rescanned = sv.sample(can)
     assert rescanned == 1  # above 2^22 amplitudes the exact scan runs directly
     assert np.array_equal(idx, port.sample(n, port.probabilities(n, psi), can))
+
+
+def _exact_probes(probs, positions):
+    """Canonicals c whose drawn value u = c * bound lands exactly on the
+    sequential CDF value at `positions` or one ulp above it: a device CDF that
+    differs by one ulp at such an element changes the sampled index."""
+    cdf = np.cumsum(probs)  # sequential left-to-right, as std::partial_sum
+    last = cdf[-1]
+    below = cdf[cdf < last]
+    second = below[-1] if below.size else 0.0
+    bound = last - (last - second) * 1.0e-4
+    out = []
+    for i in positions:
+        for target in (cdf[i], np.nextafter(cdf[i], np.inf)):
+            if not (0.0 < target <= bound):
+                continue
+            c = target / bound
+            for cc in (c, np.nextafter(c, 0.0), np.nextafter(c, 1.0)):
+                if 0.0 <= cc < 1.0 and cc * bound + 0.0 == target:
+                    out.append(cc)
+                    break
+    return np.array(out)
+
+
+@pytest.mark.parametrize("case", ["random", "zero_prefix", "dyadic", "dominant", "uniform", "tiny_head"])
+def test_sampling_exact_tier_probes(engine, port, case):
+    """The tiled exact CDF (several 16384-element tiles) probed at tile
+    boundaries and random elements, against std::partial_sum semantics."""
+    n = 18
+    N = 1 << n
+    rng = np.random.default_rng(sum(map(ord, case)))
+    if case == "random":
+        v = random_state(n, 5)
+    elif case == "zero_prefix":
+        v = np.zeros(N, dtype=np.complex128)
+        v[40000:] = rng.standard_normal(N - 40000)
+    elif case == "dyadic":
+        v = np.zeros(N, dtype=np.complex128)
+        v[::3] = 2.0 ** (-rng.integers(3, 30, size=v[::3].size) / 2.0)
+    elif case == "dominant":
+        v = (rng.standard_normal(N) * 1e-4).astype(np.complex128)
+        v[100000] = 1.0
+    elif case == "uniform":
+        v = np.full(N, 2.0 ** (-n / 2), dtype=np.complex128)
+    else:
+        v = rng.standard_normal(N).astype(np.complex128)
+        v[:30000] *= 1e-170
+    sv = capi.Statevector(n)
+    sv.upload(v)
+    probs = port.probabilities(n, v)
+    tiles = np.arange(0, N, 16384)
+    pos = np.unique(np.clip(np.concatenate([tiles - 1, tiles, tiles + 1, rng.integers(0, N, 3000)]), 0, N - 1))
+    can = np.concatenate([_exact_probes(probs, pos), port.canonicals(9, 2000)])
+    assert can.size > 2000
+    idx, rescanned = sv.sample(can, mode=1)
+    assert rescanned == 1
+    assert np.array_equal(idx, port.sample(n, probs, can))
