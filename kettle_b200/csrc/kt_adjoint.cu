@@ -185,8 +185,9 @@ __global__ void k_grad_finalize(const double* __restrict__ partial, int n_blocks
 struct BGate
 {
     kt::LGate adj;   // U^dagger (kind preserved)
-    double d[8];     // dU/dtheta
+    double d[8];     // dU/dtheta (the one-kernel-per-gate sweep)
     int32_t slot;    // parameter slot, -1 = no gradient
+    int32_t gen;     // generator of the rotation (the fused sweep)
 };
 
 }  // namespace
@@ -345,6 +346,7 @@ int32_t kt_adjoint_forward(kt_adjoint a, const kt_gate* gates, int64_t n_gates, 
                 const double th = params[g.param];
                 if (kt::gate_derivative(g.op, th, b.d)) {
                     b.slot = g.param;
+                    b.gen = kt::gate_generator(g.op);
                 }
             }
             a->gates.push_back(b);
@@ -515,7 +517,7 @@ int32_t kt_adjoint_backward(kt_adjoint a, double* grad, int64_t n_params)
                 for (int64_t g = g1 - 1; g >= g0; --g) {
                     kt::AdjGate ag {};
                     ag.adj = a->gates[g].adj;
-                    std::copy(a->gates[g].d, a->gates[g].d + 8, ag.d);
+                    ag.gen = a->gates[g].gen;
                     ag.row = row_of[g];
                     sweep.push_back(ag);
                 }

@@ -249,7 +249,6 @@ __global__ void k_batch_patch(const double* __restrict__ params, const BPatch* _
     } else if (p.table == TAB_BWD) {
         for (int e = 0; e < 8; ++e) {
             bops[p.index].m[e] = static_cast<T>(ua[e]);
-            bops[p.index].d[e] = static_cast<T>(d[e]);
         }
     } else {
         for (int e = 0; e < 8; ++e) {
@@ -694,7 +693,10 @@ void plan_item(const kt_batch_item& it, const kt_gate* gates, bool with_grad, It
     }
     // forward blocks (an item without gates still gets one block: it writes |0...0>)
     const int K = Cfg<T>::RB + TBMAX;
-    auto pbs = form_blocks(lg, q, K, Cfg<T>::L, BATCH_FWD_MAX_OPS);
+    // fusion depth: the fused_max_ops knob (set by the autotuner), within the kernel's budgets
+    const size_t fwd_ops = static_cast<size_t>(std::min(BATCH_FWD_MAX_OPS, tuning().fused_max_ops));
+    const size_t bwd_ops = static_cast<size_t>(std::min(BATCH_BWD_MAX_OPS, tuning().fused_max_ops));
+    auto pbs = form_blocks(lg, q, K, Cfg<T>::L, fwd_ops);
     if (pbs.empty()) {
         PlanBlock b;
         b.K = K;
@@ -724,15 +726,14 @@ void plan_item(const kt_batch_item& it, const kt_gate* gates, bool with_grad, It
             const size_t gi = G - 1 - k;
             gate_of[k] = static_cast<int32_t>(gi);
             rl[k] = dagger(lg[gi]);
-            std::memset(&ex[k], 0, sizeof(AdjExtra));
             ex[k].row = -1;
-            double scratch[8];
-            if (ip.slot[gi] >= 0 && gate_derivative(ip.opcode[gi], 1.0, scratch)) {
+            ex[k].gen = gate_generator(ip.opcode[gi]);
+            if (ip.slot[gi] >= 0 && ex[k].gen >= 0) {
                 ex[k].row = n_rows++;
                 ip.row_slot.push_back(ip.slot[gi]);
             }
         }
-        const auto abs = form_blocks(rl, q, KA, CfgA<T>::L, BATCH_BWD_MAX_OPS);
+        const auto abs = form_blocks(rl, q, KA, CfgA<T>::L, bwd_ops);
         for (const auto& pb : abs) {
             std::vector<int32_t> rows;
             std::vector<AdjExtra> local(ex.size());

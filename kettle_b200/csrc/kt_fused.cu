@@ -227,8 +227,8 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
     for (const auto& g : gates) {
         lg.push_back(g.adj);
         AdjExtra e {};
-        std::memcpy(e.d, g.d, sizeof(e.d));
         e.row = g.row;
+        e.gen = g.gen;
         ex.push_back(e);
     }
     // cap the ops of a block so its gradient rows fit the shared-memory slots

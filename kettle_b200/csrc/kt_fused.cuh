@@ -81,14 +81,15 @@ struct FOp
     static constexpr bool HAS_D = false;
 };
 
-// an op of the adjoint sweep: m = U^dagger, d = dU/dtheta, row = gradient row (-1: none)
+// an op of the adjoint sweep: m = U^dagger; row = gradient row (-1: none);
+// gen = the generator of a parameterised rotation (GEN_X/Y/Z/P)
 template <typename T>
 struct FOpA
 {
     uint8_t kind;
     uint8_t tslot;
     uint8_t cslot;
-    uint8_t pad0;
+    uint8_t gen;
     int32_t row;
     uint32_t pad3;
     uint32_t cthr;
@@ -97,7 +98,6 @@ struct FOpA
     uint64_t cglob;
     uint64_t tglob;
     T m[8];
-    T d[8];
     static constexpr bool HAS_D = true;
 };
 
@@ -407,13 +407,31 @@ constexpr int ADJ_WARPS = 8;          // 256 threads
 // CTAs fit on an SM
 constexpr int ADJ_MAX_OPS = 128;
 
-template <typename T, int RB>
-struct GradGenF
+// Gradient terms.  A parameterised gate is U = exp(-i theta G / 2) with G a
+// Pauli (RX, RY, RZ and their controlled forms: G = X, Y, Z on the target,
+// times the control projector) or P(theta) = diag(1, e^(i theta)).  With
+// psi_g = U psi_(g-1) (the state before U^dagger is un-applied):
+//   dU/dtheta psi_(g-1) = -(i/2) G psi_g   =>  Re <lambda| dU psi_(g-1)> = Im <lambda| G psi_g> / 2
+//   dP/dtheta psi_(g-1) = i Pi_1 psi_g     =>  Re <lambda| dP psi_(g-1)> = -Im <lambda| Pi_1 psi_g>
+// so the term is a sign pattern over conj(lambda) * psi, no matrix products
+// (the rows are doubled when they are finalised).
+__device__ __forceinline__ double im_cj(double2 a, double2 b)
+{
+    return a.x * b.y - a.y * b.x;  // Im(conj(a) b)
+}
+
+__device__ __forceinline__ double re_cj(double2 a, double2 b)
+{
+    return a.x * b.x + a.y * b.y;  // Re(conj(a) b)
+}
+
+// generator on register slot S (control register slot CS)
+template <typename T, int RB, int GENK>
+struct GradRegF
 {
     using C = typename CxT<T>::type;
     const C (&l)[1 << RB];
     const C (&p)[1 << RB];
-    C d00, d01, d10, d11;
     double acc;
     template <int S, int CS>
     __device__ __forceinline__ void run()
@@ -422,23 +440,30 @@ struct GradGenF
         for (int i = 0; i < (1 << RB); ++i) {
             if (lower_of_pair<S, CS>(i)) {
                 const int j = i | (1 << S);
-                const C e0 = cfma(d01, p[j], cmul(d00, p[i]));
-                const C e1 = cfma(d11, p[j], cmul(d10, p[i]));
-                const double2 a0 = to_d2(l[i]), a1 = to_d2(l[j]);
-                const double2 b0 = to_d2(e0), b1 = to_d2(e1);
-                acc += a0.x * b0.x + a0.y * b0.y + a1.x * b1.x + a1.y * b1.y;
+                const double2 l0 = to_d2(l[i]), l1 = to_d2(l[j]);
+                const double2 p0 = to_d2(p[i]), p1 = to_d2(p[j]);
+                if constexpr (GENK == GEN_X) {
+                    acc += im_cj(l0, p1) + im_cj(l1, p0);
+                } else if constexpr (GENK == GEN_Y) {
+                    acc += re_cj(l1, p0) - re_cj(l0, p1);
+                } else if constexpr (GENK == GEN_Z) {
+                    acc += im_cj(l0, p0) - im_cj(l1, p1);
+                } else {
+                    acc -= im_cj(l1, p1);
+                }
             }
         }
     }
 };
 
+// sum of Im(conj(lambda) psi) over this thread's registers with the control on
+// (a diagonal generator whose target bit is fixed for the thread)
 template <typename T, int RB>
-struct GradDiagRegF
+struct GradAllF
 {
     using C = typename CxT<T>::type;
     const C (&l)[1 << RB];
     const C (&p)[1 << RB];
-    C d0, d1;
     double acc;
     template <int S, int CS>
     __device__ __forceinline__ void run()
@@ -446,31 +471,7 @@ struct GradDiagRegF
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
             if (ctrl_on<CS>(i)) {
-                const C e = cmul((i & (1 << S)) ? d1 : d0, p[i]);
-                const double2 a = to_d2(l[i]), b = to_d2(e);
-                acc += a.x * b.x + a.y * b.y;
-            }
-        }
-    }
-};
-
-template <typename T, int RB>
-struct GradDiagAllF
-{
-    using C = typename CxT<T>::type;
-    const C (&l)[1 << RB];
-    const C (&p)[1 << RB];
-    C d;
-    double acc;
-    template <int S, int CS>
-    __device__ __forceinline__ void run()
-    {
-#pragma unroll
-        for (int i = 0; i < (1 << RB); ++i) {
-            if (ctrl_on<CS>(i)) {
-                const C e = cmul(d, p[i]);
-                const double2 a = to_d2(l[i]), b = to_d2(e);
-                acc += a.x * b.x + a.y * b.y;
+                acc += im_cj(to_d2(l[i]), to_d2(p[i]));
             }
         }
     }
@@ -529,32 +530,47 @@ __device__ __forceinline__ void apply_u(typename CxT<T>::type (&v)[1 << RB], con
     dispatch_c<RB, 99>(cs, f);
 }
 
-// Re <lambda| D psi> over this thread's registers for a parameterised op
+// Re <lambda| dU/dtheta psi_(g-1)> over this thread's registers, from psi_g
 template <typename T, int RB, typename OPT>
 __device__ __forceinline__ double grad_term(const typename CxT<T>::type (&l)[1 << RB],
                                             const typename CxT<T>::type (&p)[1 << RB], const OPT& op, uint32_t t,
                                             uint64_t base)
 {
-    const int kind = op.kind;
     const int ts = op.tslot;
     const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
-    if (kind < OP_DIAG) {
-        GradGenF<T, RB> f {l, p, make_cx<T>(op.d[0], op.d[1]), make_cx<T>(op.d[2], op.d[3]), make_cx<T>(op.d[4], op.d[5]),
-                           make_cx<T>(op.d[6], op.d[7]), 0.0};
-        dispatch_sc<RB>(ts, cs, f);
-        return f.acc;
-    }
-    const auto d0 = make_cx<T>(op.d[0], op.d[1]);
-    const auto d1 = make_cx<T>(op.d[6], op.d[7]);
     if (ts != NO_SLOT) {
-        GradDiagRegF<T, RB> f {l, p, d0, d1, 0.0};
-        dispatch_sc<RB>(ts, cs, f);
-        return f.acc;
+        switch (op.gen) {
+            case GEN_X: {
+                GradRegF<T, RB, GEN_X> f {l, p, 0.0};
+                dispatch_sc<RB>(ts, cs, f);
+                return 0.5 * f.acc;
+            }
+            case GEN_Y: {
+                GradRegF<T, RB, GEN_Y> f {l, p, 0.0};
+                dispatch_sc<RB>(ts, cs, f);
+                return 0.5 * f.acc;
+            }
+            case GEN_Z: {
+                GradRegF<T, RB, GEN_Z> f {l, p, 0.0};
+                dispatch_sc<RB>(ts, cs, f);
+                return 0.5 * f.acc;
+            }
+            default: {
+                GradRegF<T, RB, GEN_P> f {l, p, 0.0};
+                dispatch_sc<RB>(ts, cs, f);
+                return f.acc;
+            }
+        }
     }
+    // Z or P whose target is a thread bit or outside the tile
     const bool b = ((t & op.tthr) != 0) || ((base & op.tglob) != 0);
-    GradDiagAllF<T, RB> f {l, p, b ? d1 : d0, 0.0};
+    const double w = (op.gen == GEN_Z) ? (b ? -0.5 : 0.5) : (b ? -1.0 : 0.0);
+    if (w == 0.0) {
+        return 0.0;
+    }
+    GradAllF<T, RB> f {l, p, 0.0};
     dispatch_c<RB, 99>(cs, f);
-    return f.acc;
+    return w * f.acc;
 }
 
 // --- per-tile bodies ------------------------------------------------------------
@@ -695,8 +711,8 @@ __device__ __forceinline__ void fwd_tile(typename CxT<T>::type* __restrict__ a, 
 }
 
 // One tile of an adjoint block: psi and lambda go through the block's ops
-// (U^dagger on both); each parameterised op adds this tile's
-// Re <lambda| D psi> into acc[row * ADJ_WARPS + warp].
+// (U^dagger on both); each parameterised op first adds this tile's share of
+// Re <lambda| dU/dtheta psi_(g-1)> into acc[row * ADJ_WARPS + warp].
 template <typename T, int RB, bool LDCG>
 __device__ __forceinline__ void adj_tile(typename CxT<T>::type* __restrict__ psi, typename CxT<T>::type* __restrict__ lam,
                                          const FBlock& bk, const FPhase* sph, const FOpA<T>* sops, uint64_t tile,
@@ -756,10 +772,8 @@ __device__ __forceinline__ void adj_tile(typename CxT<T>::type* __restrict__ psi
                 continue;  // control outside the tile is 0: nothing changes, the derivative term is 0
             }
             const bool on = (t & op.cthr) == op.cthr;
-            if (on) {
-                apply_u<T, RB>(vp, op, t, base);
-            }
             if (op.row >= 0) {
+                // the gradient term reads psi_g and lambda before U^dagger is applied to either
                 double g = on ? grad_term<T, RB>(vl, vp, op, t, base) : 0.0;
 #pragma unroll
                 for (int s = 16; s > 0; s >>= 1) {
@@ -770,6 +784,7 @@ __device__ __forceinline__ void adj_tile(typename CxT<T>::type* __restrict__ psi
                 }
             }
             if (on) {
+                apply_u<T, RB>(vp, op, t, base);
                 apply_u<T, RB>(vl, op, t, base);
             }
         }
@@ -914,11 +929,11 @@ struct Plan
     int transposes {0};
 };
 
-// per-gate extras of the adjoint sweep: dU/dtheta and the gradient row (-1: none)
+// per-gate extras of the adjoint sweep: the gradient row (-1: none) and the generator
 struct AdjExtra
 {
-    double d[8];
     int32_t row;
+    int32_t gen;
 };
 
 template <typename T, typename CFG = Cfg<T>, typename OPT = FOp<T>>
@@ -1104,9 +1119,7 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
         if constexpr (OPT::HAS_D) {
             const AdjExtra& ex = extra[pb.gates[k]];
             op.row = ex.row;
-            for (int e = 0; e < 8; ++e) {
-                op.d[e] = static_cast<T>(ex.d[e]);
-            }
+            op.gen = static_cast<uint8_t>(ex.gen < 0 ? 0 : ex.gen);
         }
         plan.ops.push_back(op);
     }

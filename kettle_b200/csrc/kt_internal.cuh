@@ -104,6 +104,18 @@ LGate conj_shifted(const LGate& g, int shift);
 // every other op.
 bool gate_derivative(int op, double th, double* d);
 
+// Generators of the parameterised gates: RX/RY/RZ (and CRX/CRY/CRZ) are
+// exp(-i theta G / 2) with G = X, Y, Z; P (and CP) is diag(1, e^(i theta)).
+enum Generator : int32_t
+{
+    GEN_X = 0,
+    GEN_Y = 1,
+    GEN_Z = 2,
+    GEN_P = 3,
+};
+// GEN_* of a gate op, or -1 when it has no angle
+int gate_generator(int op);
+
 // ---------------------------------------------------------------------------
 // kernels (launchers return KT_OK or a CUDA error status)
 int32_t launch_set_basis(State& s, uint64_t index);
@@ -117,11 +129,12 @@ int32_t launch_pairs(uint32_t n, uint32_t c, uint32_t t, int kind, uint64_t k0, 
 // fused blocks
 struct FusedPlan;
 int32_t apply_fused(State& s, const std::vector<LGate>& gates);
-// adjoint sweep gates, in backward order: U^dagger, dU/dtheta and the gradient row (-1: none)
+// adjoint sweep gates, in backward order: U^dagger, the generator of a
+// parameterised rotation (gate_generator) and the gradient row (-1: none)
 struct AdjGate
 {
     LGate adj;
-    double d[8];
+    int32_t gen;
     int32_t row;
 };
 // un-apply `gates` to psi and lambda with fused blocks; dev_grad[row] = 2 Re <lambda|D psi>

@@ -327,6 +327,17 @@ bool gate_derivative(int op, double th, double* d)
     }
 }
 
+int gate_generator(int op)
+{
+    switch (op) {
+        case KT_OP_RX: case KT_OP_CRX: return GEN_X;
+        case KT_OP_RY: case KT_OP_CRY: return GEN_Y;
+        case KT_OP_RZ: case KT_OP_CRZ: return GEN_Z;
+        case KT_OP_P: case KT_OP_CP: return GEN_P;
+        default: return -1;
+    }
+}
+
 LGate conj_shifted(const LGate& g, int shift)
 {
     LGate c = g;
