@@ -141,7 +141,10 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  * autotuner (kettle_b200/autotune.py) or from KT_TUNING="name=value,...":
  *   fused_ctas_per_sm  1 or 2   register budget of the fused block kernel
  *   fused_tile_bits    9..12    tile qubits per fused block (complex128)
- *   fused_max_ops      1..256   gates per fused block
+ *   fused_max_ops      1..256   gates per fused block (also the batch engine's fusion depth)
+ *   adjoint_fused      0 or 1   fused adjoint blocks (1) or one kernel per gate (0)
+ *   fold_permutations  0 or 1   X / CX with every qubit in a tile folded into a
+ *                               shared-memory transpose (1) or run as ops (0)
  * Unknown names return KT_ERR_INVALID. */
 int32_t kt_tuning_set(const char* name, int64_t value);
 int32_t kt_tuning_get(const char* name, int64_t* value);
@@ -175,8 +178,9 @@ int32_t kt_sv_apply(kt_sv sv, const kt_gate* gates, int64_t n_gates,
                     const double* params, int64_t n_params, int32_t mode);
 
 /* Host-only dry run of the fused planner (no device work, no reference
- * counterpart): the fused blocks, layout phases, gate ops and shared-memory
- * transposes kt_sv_apply would use for this gate stream on n_qubits. */
+ * counterpart): the fused blocks, layout phases, gates placed in blocks (X /
+ * CX folded into transposes included) and shared-memory transposes
+ * kt_sv_apply would use for this gate stream on n_qubits. */
 int32_t kt_plan_stats(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates,
                       const double* params, int64_t n_params, int64_t* blocks, int64_t* phases,
                       int64_t* ops, int64_t* transposes);

@@ -706,12 +706,12 @@ void plan_item(const kt_batch_item& it, const kt_gate* gates, bool with_grad, It
         pbs.push_back(b);
     }
     for (const auto& pb : pbs) {
-        const int64_t op0 = static_cast<int64_t>(ip.fwd.ops.size());
         plan_block<T>(pb, lg, q, ip.fwd);
-        for (size_t k = 0; k < pb.gates.size(); ++k) {
-            if (ip.slot[static_cast<size_t>(pb.gates[k])] >= 0) {
-                ip.fpatch.emplace_back(op0 + static_cast<int64_t>(k), pb.gates[k]);
-            }
+    }
+    for (size_t o = 0; o < ip.fwd.ops.size(); ++o) {
+        const int32_t gi = ip.fwd.op_gate[o];
+        if (ip.slot[static_cast<size_t>(gi)] >= 0) {
+            ip.fpatch.emplace_back(static_cast<int64_t>(o), gi);
         }
     }
     if (with_grad) {
@@ -744,15 +744,14 @@ void plan_item(const kt_batch_item& it, const kt_gate* gates, bool with_grad, It
                     rows.push_back(ex[gi].row);
                 }
             }
-            const int64_t op0 = static_cast<int64_t>(ip.bwd.ops.size());
             plan_block<T, CfgA<T>, FOpA<T>>(pb, rl, q, ip.bwd, local.data());
-            for (size_t k = 0; k < pb.gates.size(); ++k) {
-                const int32_t g = gate_of[static_cast<size_t>(pb.gates[k])];
-                if (ip.slot[static_cast<size_t>(g)] >= 0) {
-                    ip.bpatch.emplace_back(op0 + static_cast<int64_t>(k), g);
-                }
-            }
             ip.rows_of_block.push_back(std::move(rows));
+        }
+        for (size_t o = 0; o < ip.bwd.ops.size(); ++o) {
+            const int32_t g = gate_of[static_cast<size_t>(ip.bwd.op_gate[o])];
+            if (ip.slot[static_cast<size_t>(g)] >= 0) {
+                ip.bpatch.emplace_back(static_cast<int64_t>(o), g);
+            }
         }
     }
     if (!phases_fit(ip.fwd) || !phases_fit(ip.bwd)) {

@@ -369,7 +369,7 @@ void plan_only(int n, const std::vector<LGate>& gates, int64_t* blocks, int64_t*
     }
     *blocks = static_cast<int64_t>(plan.blocks.size());
     *phases = static_cast<int64_t>(plan.phases.size());
-    *ops = static_cast<int64_t>(plan.ops.size());
+    *ops = static_cast<int64_t>(plan.ops.size()) + plan.folded;  // every gate placed, folded ones included
     *transposes = plan.transposes;
 }
 

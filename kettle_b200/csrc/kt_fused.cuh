@@ -101,12 +101,20 @@ struct FOpA
     static constexpr bool HAS_D = true;
 };
 
+// A layout phase.  rsw/tsw address a register or thread bit's amplitude when
+// the phase is loaded from shared memory; rsw_out/tsw_out/xor_out when it is
+// stored at the next transpose.  They differ when X / CX gates were folded
+// into that transpose: an index permutation b -> M b + c over GF(2), stored
+// as the swizzled images M e_k (every term) and c (xor_out).
 struct FPhase
 {
     uint64_t rstride[RBMAX];   // global stride of each register slot
     uint64_t tstride[TBMAX];   // global stride of each thread-index bit
     uint32_t rsw[RBMAX];       // swizzled shared-memory term of each register slot
     uint32_t tsw[TBMAX];       // swizzled shared-memory term of each thread-index bit
+    uint32_t rsw_out[RBMAX];
+    uint32_t tsw_out[TBMAX];
+    uint32_t xor_out;
     int32_t op_begin;
     int32_t op_end;
 };
@@ -631,6 +639,18 @@ __device__ __forceinline__ void stage_block(const FBlock& bk, const FPhase* __re
     }
 }
 
+// this thread's part of a phase's store-side shared-memory address
+__device__ __forceinline__ uint32_t store_thread_term(const FPhase& ph, uint32_t t, int TB)
+{
+    uint32_t a = ph.xor_out;
+    for (int j = 0; j < TB; ++j) {
+        if ((t >> j) & 1) {
+            a ^= ph.tsw_out[j];
+        }
+    }
+    return a;
+}
+
 template <bool LDCG, typename C>
 __device__ __forceinline__ C load_amp(const C* p)
 {
@@ -672,7 +692,6 @@ __device__ __forceinline__ void fwd_tile(typename CxT<T>::type* __restrict__ a, 
             }
         }
     }
-    uint32_t tsw_prev = 0;
     for (int p = 0; p < np; ++p) {
         const FPhase& ph = sph[p];
         uint32_t tsw = 0;
@@ -682,11 +701,13 @@ __device__ __forceinline__ void fwd_tile(typename CxT<T>::type* __restrict__ a, 
             }
         }
         if (p > 0) {
-            // transpose: registers (previous layout) -> smem -> registers (this layout)
+            // transpose: registers (previous layout, through its folded
+            // permutation) -> smem -> registers (this layout)
             const FPhase& pp = sph[p - 1];
+            const uint32_t tso = store_thread_term(pp, t, TB);
 #pragma unroll
             for (int i = 0; i < R; ++i) {
-                sm[tsw_prev ^ xor_terms<RB>(i, pp.rsw)] = v[i];
+                sm[tso ^ xor_terms<RB>(i, pp.rsw_out)] = v[i];
             }
             __syncthreads();
 #pragma unroll
@@ -695,7 +716,6 @@ __device__ __forceinline__ void fwd_tile(typename CxT<T>::type* __restrict__ a, 
             }
             __syncthreads();
         }
-        tsw_prev = tsw;
         for (int o = ph.op_begin; o < ph.op_end; ++o) {
             apply_op<T, RB>(v, sops[o - op0], t, base);
         }
@@ -739,7 +759,6 @@ __device__ __forceinline__ void adj_tile(typename CxT<T>::type* __restrict__ psi
             vl[i] = load_amp<LDCG>(lam + o);
         }
     }
-    uint32_t tsw_prev = 0;
     for (int p = 0; p < np; ++p) {
         const FPhase& ph = sph[p];
         uint32_t tsw = 0;
@@ -750,9 +769,10 @@ __device__ __forceinline__ void adj_tile(typename CxT<T>::type* __restrict__ psi
         }
         if (p > 0) {
             const FPhase& pp = sph[p - 1];
+            const uint32_t tso = store_thread_term(pp, t, TB);
 #pragma unroll
             for (int i = 0; i < R; ++i) {
-                const uint32_t x = tsw_prev ^ xor_terms<RB>(i, pp.rsw);
+                const uint32_t x = tso ^ xor_terms<RB>(i, pp.rsw_out);
                 smp[x] = vp[i];
                 sml[x] = vl[i];
             }
@@ -765,7 +785,6 @@ __device__ __forceinline__ void adj_tile(typename CxT<T>::type* __restrict__ psi
             }
             __syncthreads();
         }
-        tsw_prev = tsw;
         for (int o = ph.op_begin; o < ph.op_end; ++o) {
             const FOpA<T>& op = sops[o - op0];
             if ((base & op.cglob) != op.cglob) {
@@ -926,7 +945,9 @@ struct Plan
     std::vector<FBlock> blocks;
     std::vector<FPhase> phases;
     std::vector<OPT> ops;
+    std::vector<int32_t> op_gate;  // the gate (index into the planned gate list) each op runs
     int transposes {0};
+    int folded {0};   // X / CX gates folded into transposes
 };
 
 // per-gate extras of the adjoint sweep: the gradient row (-1: none) and the generator
@@ -935,6 +956,12 @@ struct AdjExtra
     int32_t row;
     int32_t gen;
 };
+
+// Is this lowered gate X or CX (the matrix [[0, 1], [1, 0]] exactly)?
+inline bool is_pure_x(const LGate& x)
+{
+    return x.kind == KIND_ANTI && x.m[2] == 1.0 && x.m[3] == 0.0 && x.m[4] == 1.0 && x.m[5] == 0.0;
+}
 
 template <typename T, typename CFG = Cfg<T>, typename OPT = FOp<T>>
 void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T, OPT>& plan,
@@ -960,12 +987,18 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
             fb.freebit[nf++] = q;
         }
     }
-    // the tile bit each gate needs as a register bit (-1 = none)
+    // X and CX with every qubit in the tile are index permutations; with
+    // folding on they become part of the next transpose instead of ops.
+    // The tile bit every other non-diagonal gate needs as a register bit.
     const size_t m = pb.gates.size();
+    const bool folding = tuning().fold_permutations != 0;
+    std::vector<char> fold(m, 0);
     std::vector<int> need(m, -1);
     for (size_t k = 0; k < m; ++k) {
         const LGate& x = g[pb.gates[k]];
-        if (x.kind != KIND_DIAG) {
+        if (folding && is_pure_x(x) && loc[x.target] >= 0 && (x.control < 0 || loc[x.control] >= 0)) {
+            fold[k] = 1;
+        } else if (x.kind != KIND_DIAG) {
             need[k] = loc[x.target];
         }
     }
@@ -1012,64 +1045,130 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
         std::sort(regs.begin(), regs.end());
         return regs;
     };
+    auto tile_mask = [&](const LGate& x) -> uint64_t {
+        uint64_t mk = 0;
+        if (loc[x.target] >= 0) mk |= bit(loc[x.target]);
+        if (x.control >= 0 && loc[x.control] >= 0) mk |= bit(loc[x.control]);
+        return mk;
+    };
     struct PhaseSpec
     {
         std::vector<int> regs;
-        size_t begin, end;
+        std::vector<size_t> ops;    // gate positions run as ops in this phase
+        std::vector<size_t> folds;  // X / CX applied when this phase is stored
     };
     std::vector<PhaseSpec> ph;
     std::vector<int> cur = choose(0, {});
     if (has_low(cur)) {
-        ph.push_back({io_regs(), 0, 0});
+        ph.push_back({io_regs(), {}, {}});
     }
-    size_t start = 0;
-    for (size_t k = 0; k < m; ++k) {
-        if (need[k] >= 0 && std::find(cur.begin(), cur.end(), need[k]) == cur.end()) {
-            ph.push_back({cur, start, k});
-            std::vector<int> keep = cur;
-            std::sort(keep.begin(), keep.end(), [&](int x, int y) { return next_use(x, k) < next_use(y, k); });
-            cur = choose(k, keep);
-            start = k;
+    PhaseSpec open {cur, {}, {}};
+    uint64_t pending = 0;  // tile bits of the folded gates waiting in `open`
+    // Pending permutations wait for the next transpose.  A gate that touches
+    // their qubits before then runs them as ordinary ops first when their
+    // targets are register bits (they were only moved past gates on other
+    // qubits, which commute with them); otherwise that gate starts a new
+    // phase, as a gate on a missing register bit does.  So folding never adds
+    // a transpose.
+    auto targets_in_regs = [&](const PhaseSpec& sp) {
+        for (size_t f : sp.folds) {
+            if (std::find(cur.begin(), cur.end(), loc[g[pb.gates[f]].target]) == cur.end()) {
+                return false;
+            }
         }
+        return true;
+    };
+    for (size_t k = 0; k < m; ++k) {
+        const LGate& x = g[pb.gates[k]];
+        const uint64_t qm = tile_mask(x);
+        if (fold[k]) {
+            open.folds.push_back(k);
+            pending |= qm;
+            continue;
+        }
+        const bool miss = need[k] >= 0 && std::find(cur.begin(), cur.end(), need[k]) == cur.end();
+        if (!miss && (qm & pending) != 0 && targets_in_regs(open)) {
+            open.ops.insert(open.ops.end(), open.folds.begin(), open.folds.end());
+            open.folds.clear();
+            pending = 0;
+        }
+        if (miss || (qm & pending) != 0) {
+            // a transpose: it applies the pending permutations; the next
+            // register set is chosen by next use
+            ph.push_back(open);
+            std::vector<int> keep = cur;
+            std::sort(keep.begin(), keep.end(), [&](int a, int b2) { return next_use(a, k) < next_use(b2, k); });
+            cur = choose(k, keep);
+            open = PhaseSpec {cur, {}, {}};
+            pending = 0;
+        }
+        open.ops.push_back(k);
     }
-    ph.push_back({cur, start, m});
-    if (has_low(cur)) {
-        ph.push_back({io_regs(), m, m});
+    if (!open.folds.empty() && !has_low(cur) && targets_in_regs(open)) {
+        open.ops.insert(open.ops.end(), open.folds.begin(), open.folds.end());
+        open.folds.clear();
+    }
+    ph.push_back(open);
+    if (!open.folds.empty() || has_low(cur)) {
+        // one more transpose: it applies the last permutations and leaves a
+        // coalesced layout for the store
+        ph.push_back({io_regs(), {}, {}});
     }
     // phases
     const int TB = K - RB;
     const size_t op_base = plan.ops.size();
     fb.phase_begin = static_cast<int32_t>(plan.phases.size());
     std::vector<std::vector<int8_t>> slots;
+    size_t emitted = 0;
     for (auto& spec : ph) {
         int8_t sb[KMAX] = {};
         make_slots(spec.regs, K, G, sb);
         slots.emplace_back(sb, sb + K);
         FPhase fp {};
-        for (int s = 0; s < RB; ++s) {
-            fp.rstride[s] = bit(pb.qubits[sb[s]]);
-            fp.rsw[s] = swz(1u << sb[s], G);
+        // store side: the folded permutation M (columns M e_k) and offset c
+        uint32_t col[KMAX];
+        for (int k = 0; k < K; ++k) {
+            col[k] = 1u << k;
+        }
+        uint32_t xc = 0;
+        for (size_t f : spec.folds) {
+            const LGate& x = g[pb.gates[f]];
+            const int lt = loc[x.target];
+            if (x.control >= 0) {
+                const int lc = loc[x.control];
+                for (int k = 0; k < K; ++k) {
+                    col[k] ^= ((col[k] >> lc) & 1u) << lt;
+                }
+                xc ^= ((xc >> lc) & 1u) << lt;
+            } else {
+                xc ^= 1u << lt;
+            }
+        }
+        for (int s2 = 0; s2 < RB; ++s2) {
+            fp.rstride[s2] = bit(pb.qubits[sb[s2]]);
+            fp.rsw[s2] = swz(1u << sb[s2], G);
+            fp.rsw_out[s2] = swz(col[sb[s2]], G);
         }
         for (int j = 0; j < TB; ++j) {
             fp.tstride[j] = bit(pb.qubits[sb[RB + j]]);
             fp.tsw[j] = swz(1u << sb[RB + j], G);
+            fp.tsw_out[j] = swz(col[sb[RB + j]], G);
         }
-        fp.op_begin = static_cast<int32_t>(op_base + spec.begin);
-        fp.op_end = static_cast<int32_t>(op_base + spec.end);
+        fp.xor_out = swz(xc, G);
+        fp.op_begin = static_cast<int32_t>(op_base + emitted);
+        emitted += spec.ops.size();
+        fp.op_end = static_cast<int32_t>(op_base + emitted);
         plan.phases.push_back(fp);
+        plan.folded += static_cast<int>(spec.folds.size());
     }
     fb.phase_end = static_cast<int32_t>(plan.phases.size());
     plan.transposes += static_cast<int>(ph.size()) - 1;
     // ops, resolved against the layout of their phase
-    size_t pi = 0;
-    for (size_t k = 0; k < m; ++k) {
-        while (!(k >= ph[pi].begin && k < ph[pi].end)) {
-            ++pi;
-        }
+    for (size_t pi = 0; pi < ph.size(); ++pi) {
         const auto& sb = slots[pi];
         auto reg_slot = [&](int tilebit) -> int {
-            for (int s = 0; s < RB; ++s) {
-                if (sb[s] == tilebit) return s;
+            for (int s2 = 0; s2 < RB; ++s2) {
+                if (sb[s2] == tilebit) return s2;
             }
             return -1;
         };
@@ -1079,49 +1178,51 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
             }
             return -1;
         };
-        const LGate& x = g[pb.gates[k]];
-        OPT op {};
-        op.tslot = NO_SLOT;
-        op.cslot = NO_SLOT;
-        if (x.control >= 0) {
-            const int lc = loc[x.control];
-            if (lc < 0) {
-                op.cglob = bit(x.control);
-            } else if (const int s = reg_slot(lc); s >= 0) {
-                op.cslot = static_cast<uint8_t>(s);
-            } else {
-                op.cthr = 1u << thread_bit(lc);
+        for (size_t k : ph[pi].ops) {
+            const LGate& x = g[pb.gates[k]];
+            OPT op {};
+            op.tslot = NO_SLOT;
+            op.cslot = NO_SLOT;
+            if (x.control >= 0) {
+                const int lc = loc[x.control];
+                if (lc < 0) {
+                    op.cglob = bit(x.control);
+                } else if (const int s2 = reg_slot(lc); s2 >= 0) {
+                    op.cslot = static_cast<uint8_t>(s2);
+                } else {
+                    op.cthr = 1u << thread_bit(lc);
+                }
             }
-        }
-        const bool real = x.m[1] == 0.0 && x.m[3] == 0.0 && x.m[5] == 0.0 && x.m[7] == 0.0;
-        if (x.kind == KIND_DIAG) {
-            op.kind = (x.flags & 1) ? OP_DIAG1 : OP_DIAG;
-            const int lt = loc[x.target];
-            if (lt < 0) {
-                op.tglob = bit(x.target);
-            } else if (const int s = reg_slot(lt); s >= 0) {
-                op.tslot = static_cast<uint8_t>(s);
+            const bool real = x.m[1] == 0.0 && x.m[3] == 0.0 && x.m[5] == 0.0 && x.m[7] == 0.0;
+            if (x.kind == KIND_DIAG) {
+                op.kind = (x.flags & 1) ? OP_DIAG1 : OP_DIAG;
+                const int lt = loc[x.target];
+                if (lt < 0) {
+                    op.tglob = bit(x.target);
+                } else if (const int s2 = reg_slot(lt); s2 >= 0) {
+                    op.tslot = static_cast<uint8_t>(s2);
+                } else {
+                    op.tthr = 1u << thread_bit(lt);
+                }
             } else {
-                op.tthr = 1u << thread_bit(lt);
+                op.tslot = static_cast<uint8_t>(reg_slot(loc[x.target]));
+                if (x.kind == KIND_ANTI) {
+                    op.kind = is_pure_x(x) ? OP_SWAP : OP_ANTI;
+                } else {
+                    op.kind = real ? OP_GENR : OP_GEN;
+                }
             }
-        } else {
-            op.tslot = static_cast<uint8_t>(reg_slot(loc[x.target]));
-            if (x.kind == KIND_ANTI) {
-                const bool pure = x.m[2] == 1.0 && x.m[3] == 0.0 && x.m[4] == 1.0 && x.m[5] == 0.0;
-                op.kind = pure ? OP_SWAP : OP_ANTI;
-            } else {
-                op.kind = real ? OP_GENR : OP_GEN;
+            for (int e = 0; e < 8; ++e) {
+                op.m[e] = static_cast<T>(x.m[e]);
             }
+            if constexpr (OPT::HAS_D) {
+                const AdjExtra& ex = extra[pb.gates[k]];
+                op.row = ex.row;
+                op.gen = static_cast<uint8_t>(ex.gen < 0 ? 0 : ex.gen);
+            }
+            plan.ops.push_back(op);
+            plan.op_gate.push_back(pb.gates[k]);
         }
-        for (int e = 0; e < 8; ++e) {
-            op.m[e] = static_cast<T>(x.m[e]);
-        }
-        if constexpr (OPT::HAS_D) {
-            const AdjExtra& ex = extra[pb.gates[k]];
-            op.row = ex.row;
-            op.gen = static_cast<uint8_t>(ex.gen < 0 ? 0 : ex.gen);
-        }
-        plan.ops.push_back(op);
     }
     fb.op_begin = static_cast<int32_t>(op_base);
     fb.op_end = static_cast<int32_t>(plan.ops.size());

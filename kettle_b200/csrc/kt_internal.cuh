@@ -173,6 +173,7 @@ struct Tuning
     int fused_tile_bits {12};    // K for complex128 (complex64 uses K + 1), clamped to the kernel's range
     int fused_max_ops {256};     // gates per fused block
     int adjoint_fused {1};       // 1: fused backward blocks, 0: one kernel per gate
+    int fold_permutations {1};   // 1: X / CX inside a tile become part of a transpose, 0: ops
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);

@@ -94,6 +94,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.adjoint_fused = (v != 0) ? 1 : 0;
     } else if (name == "fused_max_ops") {
         t.fused_max_ops = static_cast<int>(std::max(1LL, std::min(256LL, v)));
+    } else if (name == "fold_permutations") {
+        t.fold_permutations = (v != 0) ? 1 : 0;
     } else {
         return false;
     }
@@ -147,6 +149,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.adjoint_fused;
     } else if (n == "fused_max_ops") {
         *value = t.fused_max_ops;
+    } else if (n == "fold_permutations") {
+        *value = t.fold_permutations;
     } else {
         return false;
     }

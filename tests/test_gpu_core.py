@@ -432,3 +432,54 @@ def test_sampling_exact_tier_probes(engine, port, case):
     idx, rescanned = sv.sample(can, mode=1)
     assert rescanned == 1
     assert np.array_equal(idx, port.sample(n, probs, can))
+
+
+def _perm_heavy(n, layers, seed):
+    """Layers of X / CX / CCX-free permutation gates mixed with rotations and
+    diagonal gates, with controls and targets spread over every qubit."""
+    rng = np.random.default_rng(seed)
+    recs = []
+    for _ in range(layers):
+        for q in range(n):
+            r = rng.integers(6)
+            if r == 0:
+                recs.append(W.gate("X", q))
+            elif r == 1:
+                recs.append(W.gate("RY", q, angle=float(rng.uniform(0, 6.28))))
+            elif r == 2:
+                recs.append(W.gate("RZ", q, angle=float(rng.uniform(0, 6.28))))
+            elif r == 3:
+                recs.append(W.gate("H", q))
+        for _ in range(n):
+            c, t = rng.choice(n, 2, replace=False)
+            recs.append(W.gate("CX", int(t), control=int(c)))
+        c, t = rng.choice(n, 2, replace=False)
+        recs.append(W.gate("CRX", int(t), control=int(c), angle=0.7))
+        recs.append(W.gate("CZ", int(t), control=int(c)))
+    return np.concatenate(recs)
+
+
+@pytest.mark.parametrize("n", [10, 14, 20])
+def test_permutation_folding(engine, port, n):
+    """X / CX folded into the transposes give the oracle's state, and the
+    same state as running them as ops (knob off) and as per-gate sweeps."""
+    g = _perm_heavy(n, 6, seed=n)
+    want = port.apply(n, basis(n), g)
+    old = capi.tuning_get("fold_permutations")
+    try:
+        states = []
+        for f in (1, 0):
+            capi.tuning_set("fold_permutations", f)
+            sv = capi.Statevector(n)
+            sv.apply(g)
+            states.append(sv.download())
+            sv.close()
+    finally:
+        capi.tuning_set("fold_permutations", old)
+    assert np.abs(states[0] - want).max() < TOL
+    assert np.abs(states[1] - want).max() < TOL
+    assert np.abs(states[0] - states[1]).max() < 1e-13
+    # complex64 with folding
+    sv = capi.Statevector(n, capi.KT_C64)
+    sv.apply(g)
+    assert np.abs(sv.download() - want).max() < 1e-4
