@@ -174,19 +174,34 @@ __device__ __forceinline__ U xor_terms(int i, const U (&terms)[RBMAX])
 }
 
 // --- register-level gate bodies -------------------------------------------------
-// S: register slot of the target; CS: register slot of the control (-1: none).
-// Both are template arguments, so a body is straight-line code that touches
-// exactly the amplitudes its gate changes (no per-amplitude predicates).
+// S: register slot of the target (a template argument, so the register pairs
+// are fixed at compile time); CS: -1 without a register control, CS_RT with a
+// control on register slot `crt`, read at run time (one predicated body per
+// target slot instead of one per target and control slot: the bodies are the
+// kernel's code size and register pressure).
+constexpr int CS_RT = -2;
+
 template <int S, int CS>
-__device__ __forceinline__ constexpr bool lower_of_pair(int i)
+__device__ __forceinline__ bool lower_of_pair(int i, int crt)
 {
-    return !(i & (1 << S)) && (CS < 0 || (i & (1 << CS)));
+    if (i & (1 << S)) {
+        return false;
+    }
+    if constexpr (CS == -1) {
+        return true;
+    } else {
+        return ((i >> crt) & 1) != 0;
+    }
 }
 
 template <int CS>
-__device__ __forceinline__ constexpr bool ctrl_on(int i)
+__device__ __forceinline__ bool ctrl_on(int i, int crt)
 {
-    return CS < 0 || (i & (1 << CS));
+    if constexpr (CS == -1) {
+        return true;
+    } else {
+        return ((i >> crt) & 1) != 0;
+    }
 }
 
 template <typename T, int RB>
@@ -195,12 +210,13 @@ struct GenF
     using C = typename CxT<T>::type;
     C (&v)[1 << RB];
     C m00, m01, m10, m11;
+    int crt = -1;
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
-            if (lower_of_pair<S, CS>(i)) {
+            if (lower_of_pair<S, CS>(i, crt)) {
                 const int j = i | (1 << S);
                 const C a = v[i];
                 const C b = v[j];
@@ -217,12 +233,13 @@ struct GenRF
     using C = typename CxT<T>::type;
     C (&v)[1 << RB];
     T m00, m01, m10, m11;
+    int crt = -1;
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
-            if (lower_of_pair<S, CS>(i)) {
+            if (lower_of_pair<S, CS>(i, crt)) {
                 const int j = i | (1 << S);
                 const C a = v[i];
                 const C b = v[j];
@@ -244,12 +261,13 @@ struct AntiF
     using C = typename CxT<T>::type;
     C (&v)[1 << RB];
     C m01, m10;
+    int crt = -1;
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
-            if (lower_of_pair<S, CS>(i)) {
+            if (lower_of_pair<S, CS>(i, crt)) {
                 const int j = i | (1 << S);
                 const C a = v[i];
                 const C b = v[j];
@@ -272,12 +290,13 @@ struct DiagRegF
     using C = typename CxT<T>::type;
     C (&v)[1 << RB];
     C d0, d1;
+    int crt = -1;
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
-            if (ctrl_on<CS>(i)) {
+            if (ctrl_on<CS>(i, crt)) {
                 if (i & (1 << S)) {
                     v[i] = cmul(d1, v[i]);
                 } else if (!ONE) {
@@ -295,12 +314,13 @@ struct DiagAllF
     using C = typename CxT<T>::type;
     C (&v)[1 << RB];
     C d;
+    int crt = -1;
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
-            if (ctrl_on<CS>(i)) {
+            if (ctrl_on<CS>(i, crt)) {
                 v[i] = cmul(d, v[i]);
             }
         }
@@ -310,13 +330,11 @@ struct DiagAllF
 template <int RB, int S, typename F>
 __device__ __forceinline__ void dispatch_c(int cs, F& f)
 {
-    switch (cs) {
-        case 0: if constexpr (S != 0) { f.template run<S, 0>(); } break;
-        case 1: if constexpr (S != 1) { f.template run<S, 1>(); } break;
-        case 2: if constexpr (S != 2) { f.template run<S, 2>(); } break;
-        case 3: if constexpr (S != 3) { f.template run<S, 3>(); } break;
-        case 4: if constexpr (RB > 4 && S != 4) { f.template run<S, (RB > 4 ? 4 : 0)>(); } break;
-        default: f.template run<S, -1>(); break;
+    if (cs < 0) {
+        f.template run<S, -1>();
+    } else {
+        f.crt = cs;
+        f.template run<S, CS_RT>();
     }
 }
 
@@ -364,7 +382,8 @@ __device__ __forceinline__ void apply_op(typename CxT<T>::type (&v)[1 << RB], co
             return;
         }
         case OP_SWAP: {
-            AntiF<T, RB, true> f {v, make_cx<T>(0, 0), make_cx<T>(0, 0)};
+            // through the multiply path: a register-move body needs temporaries that spill
+            AntiF<T, RB, false> f {v, make_cx<T>(1, 0), make_cx<T>(1, 0)};
             dispatch_sc<RB>(ts, cs, f);
             return;
         }
@@ -441,12 +460,13 @@ struct GradRegF
     const C (&l)[1 << RB];
     const C (&p)[1 << RB];
     double acc;
+    int crt = -1;
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
-            if (lower_of_pair<S, CS>(i)) {
+            if (lower_of_pair<S, CS>(i, crt)) {
                 const int j = i | (1 << S);
                 const double2 l0 = to_d2(l[i]), l1 = to_d2(l[j]);
                 const double2 p0 = to_d2(p[i]), p1 = to_d2(p[j]);
@@ -473,12 +493,13 @@ struct GradAllF
     const C (&l)[1 << RB];
     const C (&p)[1 << RB];
     double acc;
+    int crt = -1;
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
-            if (ctrl_on<CS>(i)) {
+            if (ctrl_on<CS>(i, crt)) {
                 acc += im_cj(to_d2(l[i]), to_d2(p[i]));
             }
         }
@@ -511,7 +532,8 @@ __device__ __forceinline__ void apply_u(typename CxT<T>::type (&v)[1 << RB], con
             return;
         }
         case OP_SWAP: {
-            AntiF<T, RB, true> f {v, make_cx<T>(0, 0), make_cx<T>(0, 0)};
+            // through the multiply path: a register-move body needs temporaries that spill
+            AntiF<T, RB, false> f {v, make_cx<T>(1, 0), make_cx<T>(1, 0)};
             dispatch_sc<RB>(ts, cs, f);
             return;
         }
