@@ -292,6 +292,150 @@ def batch_bench(stream, count=4096, reps=2, sample_every=32):
     return out
 
 
+def _timed(stream, fn, reps=1):
+    import torch
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps / 1e3, out
+
+
+class _DeviceArray:
+    """A raw device buffer seen by torch (__cuda_array_interface__), for error reports."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3}
+
+
+def config_legs(stream, cpu=True):
+    """The other configurations of the benchmark set, each timed on the device
+    (CUDA events; inputs from host buffers, results read back):
+      config1  20 q complex128, 100 layers of {H, RX, RY, RZ} + CX brickwork,
+               <H> of 200 random strings (N(0,1) coefficients), 4096 shots;
+               the reference's ket::simulate / expectation_value / sampler on the
+               first 10 layers for the CPU time (scaled x10 for the simulate
+               part) and for parity at this size (amplitudes, <H>, shots);
+      config2b 13 q complex128 density matrix through the same 100-layer circuit
+               family, then Tr(rho H) for 200 strings;
+      config3  33 q complex64 (64 GiB) through the 40-layer mixed circuit, FP64
+               norm and <H> over 500 strings; and the 30 q complex64 state
+               against complex128: max amplitude error, norm drift, |d<H>|."""
+    import torch
+    from kettle_b200 import capi
+    from kettle_b200 import workloads as W
+
+    out = {}
+    # ---- config 1
+    n = 20
+    gates = W.random_layers(n, 100, seed=SEED, mixed=False)
+    strings, coeffs = W.random_paulis(n, 200, seed=SEED)
+    canon = capi.canonicals_mt19937(SEED, 4096)
+    sv = capi.Statevector(n, capi.KT_C128, stream=stream.cuda_stream)
+
+    def pipeline(g=gates):
+        sv.set_basis(0)
+        sv.apply(g)
+        _, tot = sv.expect(strings, coeffs)
+        idx, _ = sv.sample(canon)
+        return tot, idx
+
+    pipeline()
+    t1, (tot, idx) = _timed(stream, pipeline, reps=3)
+    c1 = {"qubits": n, "layers": 100, "gates": int(gates.size), "strings": 200, "shots": 4096,
+          "seconds": t1, "layers_per_s": 100 / t1, "expectation": tot.real}
+    if cpu:
+        from oracle.oracle import ref, ref_available
+        if ref_available():
+            R = ref()
+            per_layer = gates.size / 100
+            pre = gates[: int(round(10 * per_layer))]
+            amp0 = np.zeros(1 << n, dtype=np.complex128)
+            amp0[0] = 1.0
+            t0 = time.perf_counter()
+            ra, _ = R.simulate_sv(n, amp0, pre)
+            t_sim = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            _, rtot = R.expect(n, ra, strings, coeffs)
+            t_exp = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            ridx = R.sample_memory(n, ra, 4096, SEED)  # the same mt19937(SEED) draws as `canon`
+            t_smp = time.perf_counter() - t0
+            ptot, pidx = pipeline(pre)
+            eng = sv.download()
+            t_ref = 10 * t_sim + t_exp + t_smp
+            c1["cpu_reference"] = {"seconds": t_ref, "layers_per_s": 100 / t_ref, "cores": 1,
+                                   "sample": f"ket::simulate on the first 10 layers ({t_sim:.2f} s, x10), "
+                                             f"expectation_value of 200 strings ({t_exp:.2f} s), "
+                                             f"4096 shots ({t_smp:.3f} s)"}
+            c1["parity_first_10_layers"] = {"max_abs_amplitude_diff": float(np.abs(eng - ra).max()),
+                                            "abs_expectation_diff": abs(ptot - rtot),
+                                            "shots_identical": bool(np.array_equal(pidx, ridx))}
+    sv.close()
+    out["config1"] = c1
+    # ---- config 2b
+    n = 13
+    gates = W.random_layers(n, 100, seed=SEED, mixed=False)
+    strings, coeffs = W.random_paulis(n, 200, seed=SEED)
+    dm = capi.DensityMatrix(n)
+    dm.set_stream(stream.cuda_stream)
+
+    def dm_pipeline():
+        dm.set_basis(0)
+        dm.apply(gates)
+        return dm.expect(strings, coeffs)[1]
+
+    dm_pipeline()
+    t2, tot = _timed(stream, dm_pipeline, reps=2)
+    out["config2b"] = {"qubits": n, "entries": 1 << (2 * n), "layers": 100, "gates": int(gates.size), "strings": 200,
+                       "seconds": t2, "layers_per_s": 100 / t2, "expectation": tot.real, "trace": dm.trace().real}
+    dm.close()
+    # ---- config 3: 33 q complex64
+    n = 33
+    gates = W.random_layers(n, 40, seed=SEED, mixed=True)
+    strings, coeffs = W.random_paulis(n, 500, seed=SEED)
+    sv = capi.Statevector(n, capi.KT_C64, stream=stream.cuda_stream)
+
+    def c64_pipeline():
+        sv.set_basis(0)
+        sv.apply(gates)
+        return sv.norm_sq(), sv.expect(strings, coeffs)[1]
+
+    t3, (nrm, tot) = _timed(stream, c64_pipeline, reps=1)
+    out["config3"] = {"qubits": n, "dtype": "c64 (FP64 norm and expectation)", "layers": 40, "gates": int(gates.size),
+                      "strings": 500, "seconds": t3, "layers_per_s": 40 / t3, "norm_drift": abs(nrm - 1.0),
+                      "expectation": tot.real}
+    sv.close()
+    # 30 q complex64 against complex128
+    n = 30
+    gates = W.random_layers(n, 40, seed=SEED, mixed=True)
+    strings, coeffs = W.random_paulis(n, 500, seed=SEED)
+    a = capi.Statevector(n, capi.KT_C128, stream=stream.cuda_stream)
+    b = capi.Statevector(n, capi.KT_C64, stream=stream.cuda_stream)
+    a.apply(gates)
+    b.apply(gates)
+    ea = a.expect(strings, coeffs)[1]
+    eb = b.expect(strings, coeffs)[1]
+    N2 = 2 << n
+    ta = torch.as_tensor(_DeviceArray(a.device_ptr(), N2, "<f8"), device="cuda")
+    tb = torch.as_tensor(_DeviceArray(b.device_ptr(), N2, "<f4"), device="cuda")
+    worst = 0.0
+    chunk = 1 << 26
+    with torch.cuda.stream(stream):
+        for i in range(0, N2, chunk):
+            worst = max(worst, float((ta[i:i + chunk] - tb[i:i + chunk].double()).abs().max()))
+    out["config3"]["c64_vs_c128_30q"] = {"max_abs_component_error": worst, "norm_drift_c64": abs(b.norm_sq() - 1.0),
+                                         "abs_expectation_diff": abs(ea - eb)}
+    del ta, tb
+    a.close()
+    b.close()
+    return out
+
+
 def run_reference(args):
     world, rank, _ = dist_setup(args.gpus)
     if rank != 0:
@@ -448,6 +592,8 @@ def run_engine(args):
         line["adjoint"] = adjoint_bench(stream)
     if args.batch > 0:
         line["batch"] = batch_bench(stream, count=args.batch)
+    if not args.no_configs and world == 1:
+        line["configs"] = config_legs(stream, cpu=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(n, gates, per_layer)
@@ -473,6 +619,8 @@ def main():
     ap.add_argument("--ref-gates", type=int, default=3, help="gates in the reference arm's sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the 24-qubit adjoint vs parameter-shift leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other benchmark configurations (20 q, 13 q density matrix, 33 q complex64)")
     ap.add_argument("--batch", type=int, default=4096,
                     help="instances in the batched energy+gradient leg (0 skips it)")
     args = ap.parse_args()

@@ -271,6 +271,12 @@ class Statevector:
         check(lib().kt_sv_norm_sq(self._h, C.byref(v)))
         return v.value
 
+    def device_ptr(self) -> int:
+        """Device address of the amplitudes (kt_sv_info)."""
+        n, dt, p = I32(), I32(), P()
+        check(lib().kt_sv_info(self._h, C.byref(n), C.byref(dt), C.byref(p)))
+        return int(p.value)
+
     def inner(self, ket: "Statevector") -> complex:
         out = np.empty(2, dtype=np.float64)
         check(lib().kt_sv_inner(self._h, ket._h, ptr(out)))
@@ -297,6 +303,9 @@ class DensityMatrix:
             self.close()
         except Exception:
             pass
+
+    def set_stream(self, stream: int | None):
+        check(lib().kt_dm_set_stream(self._h, stream))
 
     def set_basis(self, index: int = 0):
         check(lib().kt_dm_set_basis(self._h, index))
