@@ -145,6 +145,8 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *   adjoint_fused      0 or 1   fused adjoint blocks (1) or one kernel per gate (0)
  *   fold_permutations  0 or 1   X / CX with every qubit in a tile folded into a
  *                               shared-memory transpose (1) or run as ops (0)
+ *   c64_renormalize    0 or 1   complex64 applies rescale every fused block to the
+ *                               norm the state had when the apply began (1)
  * Unknown names return KT_ERR_INVALID. */
 int32_t kt_tuning_set(const char* name, int64_t value);
 int32_t kt_tuning_get(const char* name, int64_t* value);

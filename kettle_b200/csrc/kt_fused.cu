@@ -26,6 +26,8 @@
 //    target that is a thread bit.  The kernel does no per-amplitude index math.
 //  * Loads and stores use a layout whose lane bits are the L lowest qubits:
 //    each warp instruction touches whole 128-byte lines.
+#include <type_traits>
+
 #include "kt_fused.cuh"
 
 namespace kt
@@ -58,6 +60,154 @@ __global__ void __launch_bounds__(256, MINB) k_fused(typename CxT<T>::type* __re
     for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         fwd_tile<T, RB, false>(a, bk, sph, sops, tile, sm, t, false);
     }
+}
+
+// Renormalisation of a complex64 apply: the norm must not drift with the
+// FP32 rounding of thousands of gates, so every block rescales what it loads
+// to the norm the state had when the apply began (the target: FP64 sums of
+// |a|^2 that the first block takes over what it loads).  Each launch leaves,
+// per CTA, the FP64 sum of |a|^2 over what it stored; the next launch scales
+// its loads by sqrt(target / that), and a last short pass scales the result.
+struct NormArgs
+{
+    const double* target;  // per-CTA target sums (nullptr in the first block)
+    const double* prev;    // per-CTA sums left by the previous block (nullptr in the first block)
+    int n_parts;
+    double* in_parts;      // first block: per-CTA sums over the loads (the target)
+    double* out_parts;     // per-CTA sums over the stores
+};
+
+__device__ __forceinline__ double norm_scale(const double* target, const double* prev, int n)
+{
+    double num = 0.0, den = 0.0;
+    for (int i = 0; i < n; ++i) {
+        num += target[i];
+        den += prev[i];
+    }
+    return (num > 0.0 && den > 0.0) ? sqrt(num / den) : 1.0;
+}
+
+template <typename T, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_fused_norm(typename CxT<T>::type* __restrict__ a,
+                                                       const FBlock* __restrict__ blk,
+                                                       const FPhase* __restrict__ phases, const FOp<T>* __restrict__ ops,
+                                                       uint64_t n_tiles, NormArgs na)
+{
+    using C = typename CxT<T>::type;
+    constexpr int RB = Cfg<T>::RB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ FBlock bk;
+    __shared__ FPhase sph[MAX_PHASES_PER_BLOCK];
+    __shared__ double w_in[8], w_out[8];
+    __shared__ float scale_sh;
+    const uint32_t t = threadIdx.x;
+    if (t == 0) {
+        bk = *blk;
+        scale_sh = (na.prev != nullptr) ? static_cast<float>(norm_scale(na.target, na.prev, na.n_parts)) : 1.0f;
+    }
+    if (t < 8) {
+        w_in[t] = 0.0;
+        w_out[t] = 0.0;
+    }
+    __syncthreads();
+    C* sm = reinterpret_cast<C*>(smem_raw);
+    FOp<T>* sops = reinterpret_cast<FOp<T>*>(smem_raw + (sizeof(C) << bk.K));
+    stage_block(bk, phases, ops, sph, sops, t);
+    __syncthreads();
+    const NormCtx nc {na.in_parts != nullptr ? w_in : nullptr, w_out, scale_sh};
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        fwd_tile<T, RB, false, true>(a, bk, sph, sops, tile, sm, t, false, &nc);
+    }
+    __syncthreads();
+    if (t == 0) {
+        double so = 0.0, si = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            so += w_out[w];
+            si += w_in[w];
+        }
+        na.out_parts[blockIdx.x] = so;
+        if (na.in_parts != nullptr) {
+            na.in_parts[blockIdx.x] = si;
+        }
+    }
+}
+
+// the last step of a renormalising apply: a *= sqrt(target / last)
+template <typename C>
+__global__ void k_norm_final(C* __restrict__ a, uint64_t n, const double* __restrict__ target,
+                             const double* __restrict__ last, int n_parts)
+{
+    __shared__ float sc;
+    if (threadIdx.x == 0) {
+        sc = static_cast<float>(norm_scale(target, last, n_parts));
+    }
+    __syncthreads();
+    const float f = sc;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        C v = a[i];
+        v.x *= f;
+        v.y *= f;
+        a[i] = v;
+    }
+}
+
+// the renormalising launch sequence of a complex64 apply (see k_fused_norm)
+template <typename T>
+int32_t run_fused_norm(State& s, const Plan<T>& plan, const FBlock* d_blk, const FPhase* d_ph, const FOp<T>* d_ops,
+                       int K, int threads, int minb)
+{
+    using C = typename CxT<T>::type;
+    static bool attr_set[2] = {false, false};
+    if (!attr_set[minb - 1]) {
+        if (minb == 1) {
+            KT_CUDA(cudaFuncSetAttribute(k_fused_norm<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        } else {
+            KT_CUDA(cudaFuncSetAttribute(k_fused_norm<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        }
+        attr_set[minb - 1] = true;
+    }
+    const int n = s.n_bits;
+    const uint64_t n_tiles = uint64_t {1} << (n - K);
+    const int grid = static_cast<int>(std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * minb));
+    // per-CTA sums: target | out (even blocks) | out (odd blocks)
+    if (const int32_t rc = s.scratch2.reserve(3 * static_cast<size_t>(grid) * sizeof(double)); rc != KT_OK) {
+        return rc;
+    }
+    double* parts = static_cast<double*>(s.scratch2.ptr);
+    double* target = parts;
+    double* out[2] = {parts + grid, parts + 2 * grid};
+    const double pass_bytes = 2.0 * static_cast<double>(sizeof(C)) * static_cast<double>(s.n_amps());
+    for (size_t b = 0; b < plan.blocks.size(); ++b) {
+        const auto& fb = plan.blocks[b];
+        const size_t smem = (size_t {1} << K) * sizeof(C) + static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOp<T>);
+        NormArgs na {};
+        na.n_parts = grid;
+        na.target = (b == 0) ? nullptr : target;
+        na.prev = (b == 0) ? nullptr : out[(b - 1) & 1];
+        na.in_parts = (b == 0) ? target : nullptr;
+        na.out_parts = out[b & 1];
+        if (minb == 1) {
+            k_fused_norm<T, 1><<<grid, threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b, d_ph, d_ops,
+                                                                 n_tiles, na);
+        } else {
+            k_fused_norm<T, 2><<<grid, threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b, d_ph, d_ops,
+                                                                 n_tiles, na);
+        }
+        KT_CHECK_LAUNCH("k_fused_norm");
+        s.last_launches += 1;
+        s.last_alg_bytes += pass_bytes;
+    }
+    if (!plan.blocks.empty()) {
+        const unsigned fin_grid = static_cast<unsigned>(std::min<uint64_t>((s.n_amps() + 255) / 256,
+                                                                           static_cast<uint64_t>(sm_count()) * 8));
+        k_norm_final<C><<<fin_grid, 256, 0, s.stream>>>(static_cast<C*>(s.amps), s.n_amps(), target,
+                                                        out[(plan.blocks.size() - 1) & 1], grid);
+        KT_CHECK_LAUNCH("k_norm_final");
+        s.last_launches += 1;
+        s.last_alg_bytes += pass_bytes;
+    }
+    return KT_OK;
 }
 
 template <typename T>
@@ -116,6 +266,11 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     const auto* d_ops = reinterpret_cast<const FOp<T>*>(dev + off_o);
     const int threads = 1 << (K - RB);
     const int minb = tuning().fused_ctas_per_sm == 1 ? 1 : 2;
+    if constexpr (std::is_same<T, float>::value) {
+        if (tuning().c64_renormalize != 0) {
+            return run_fused_norm<T>(s, plan, d_blk, d_ph, d_ops, K, threads, minb);
+        }
+    }
     static bool attr_set[2] = {false, false};
     if (!attr_set[minb - 1]) {
         if (minb == 1) {

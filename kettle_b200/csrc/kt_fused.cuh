@@ -686,10 +686,47 @@ __device__ __forceinline__ C load_amp(const C* p)
 // One tile of a forward block: load it (or, with `init`, start from
 // |0...0>), run the block's phases with a shared-memory transpose between
 // them, store it.  The block, its phases and ops are already in shared memory.
-template <typename T, int RB, bool LDCG>
+// Norm bookkeeping of a renormalising apply (complex64): per-warp FP64 sums
+// of |a|^2 in shared memory, and the scale applied to every loaded amplitude.
+struct NormCtx
+{
+    double* warp_in;   // sums over the loaded amplitudes (nullptr: not wanted)
+    double* warp_out;  // sums over the stored amplitudes
+    float scale;
+};
+
+// sum of |v_i|^2 over this thread's registers (a pairwise tree in T), then
+// over the warp in FP64, added to slot[warp] by lane 0
+template <typename T, int R, typename C>
+__device__ __forceinline__ void warp_norm_add(const C (&v)[R], double* slot, uint32_t t)
+{
+    T q[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        q[i] = v[i].x * v[i].x + v[i].y * v[i].y;
+    }
+#pragma unroll
+    for (int w = 1; w < R; w <<= 1) {
+#pragma unroll
+        for (int i = 0; i < R; i += 2 * w) {
+            q[i] += q[i + w];
+        }
+    }
+    double d = static_cast<double>(q[0]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        d += __shfl_down_sync(0xffffffffU, d, o);
+    }
+    if ((t & 31) == 0) {
+        slot[t >> 5] += d;
+    }
+}
+
+template <typename T, int RB, bool LDCG, bool NORM = false>
 __device__ __forceinline__ void fwd_tile(typename CxT<T>::type* __restrict__ a, const FBlock& bk,
                                          const FPhase* sph, const FOp<T>* sops, uint64_t tile,
-                                         typename CxT<T>::type* sm, uint32_t t, bool init)
+                                         typename CxT<T>::type* sm, uint32_t t, bool init,
+                                         const NormCtx* nc = nullptr)
 {
     using C = typename CxT<T>::type;
     constexpr int R = 1 << RB;
@@ -711,6 +748,17 @@ __device__ __forceinline__ void fwd_tile(typename CxT<T>::type* __restrict__ a, 
 #pragma unroll
             for (int i = 0; i < R; ++i) {
                 v[i] = load_amp<LDCG>(src + reg_offset<RB>(ph, i));
+            }
+        }
+        if constexpr (NORM) {
+            if (nc->warp_in != nullptr) {
+                warp_norm_add<T>(v, nc->warp_in, t);
+            }
+            const T sc = static_cast<T>(nc->scale);
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                v[i].x *= sc;
+                v[i].y *= sc;
             }
         }
     }
@@ -749,6 +797,9 @@ __device__ __forceinline__ void fwd_tile(typename CxT<T>::type* __restrict__ a, 
         for (int i = 0; i < R; ++i) {
             dst[reg_offset<RB>(ph, i)] = v[i];
         }
+    }
+    if constexpr (NORM) {
+        warp_norm_add<T>(v, nc->warp_out, t);
     }
 }
 

@@ -174,6 +174,7 @@ struct Tuning
     int fused_max_ops {256};     // gates per fused block
     int adjoint_fused {1};       // 1: fused backward blocks, 0: one kernel per gate
     int fold_permutations {1};   // 1: X / CX inside a tile become part of a transpose, 0: ops
+    int c64_renormalize {1};     // 1: complex64 applies keep the state's norm (per-block rescaling)
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);

@@ -96,6 +96,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.fused_max_ops = static_cast<int>(std::max(1LL, std::min(256LL, v)));
     } else if (name == "fold_permutations") {
         t.fold_permutations = (v != 0) ? 1 : 0;
+    } else if (name == "c64_renormalize") {
+        t.c64_renormalize = (v != 0) ? 1 : 0;
     } else {
         return false;
     }
@@ -151,6 +153,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.fused_max_ops;
     } else if (n == "fold_permutations") {
         *value = t.fold_permutations;
+    } else if (n == "c64_renormalize") {
+        *value = t.c64_renormalize;
     } else {
         return false;
     }
