@@ -20,12 +20,13 @@
 // a memory wave).  Their work is cut into jobs — the item's fused forward
 // blocks, one Hamiltonian job (lambda = H psi and the energy), its fused
 // adjoint blocks — and each job into units (ranges of tiles).  One persistent
-// launch per wave runs a global list of (job, unit) in an order that keeps
-// many items in flight; before starting a unit a CTA waits until every unit
-// of the job's predecessor has finished (a completion counter per job).  A
-// unit is only taken after every unit listed before it has been taken by a
-// running CTA, and dependencies point backwards in the list, so the waits
-// always end; they are bounded anyway and set an error status on expiry.
+// launch per wave serves a device queue of ready jobs: it starts with every
+// item's first job (costliest chains first); a CTA takes the next unit of the
+// oldest queued job that still has one, and the CTA that finishes a job's last
+// unit appends the item's next job.  A CTA waits only while no job is ready
+// (then every job in flight is being run by some CTA, which will queue its
+// successor), so the waits end; they are bounded anyway and set an error
+// status on expiry.
 //
 // The whole evaluation — parameter upload, matrix patching, the two
 // persistent launches (on forked streams), FP64 finalisation, download — is
@@ -77,7 +78,7 @@ struct BJob
     int32_t block;           // block index in the forward or adjoint table (-1 for JOB_HAM)
     int32_t n_units;
     int32_t tiles_per_unit;  // tiles (or Hamiltonian chunks) per unit
-    int32_t dep;             // job whose units must all be finished first (-1: none)
+    int32_t succ;            // the item's next job, queued when this one's last unit is done (-1: none)
     int32_t n_rows;          // JOB_BWD: gradient rows of the block
     int32_t init;            // JOB_FWD: the item's first block starts from |0...0>
     int64_t part;            // JOB_BWD: part[part + r * n_units + u]; JOB_HAM: epart[part + u]
@@ -159,8 +160,8 @@ struct BArgs
     typename CxT<T>::type* arena;
     const BJob* jobs;
     const BInst* insts;
-    const int2* work;
-    long long n_work;
+    int* queue;               // ready jobs in the order they became ready (-1: slot not written yet)
+    int n_jobs;               // jobs of this wave: every one enters the queue exactly once
     const FBlock* fblk;
     const FPhase* fph;
     const FOp<T>* fops;
@@ -171,7 +172,9 @@ struct BArgs
     double* part;
     double* epart;
     int* done;
-    unsigned long long* next;
+    unsigned long long* qhead;  // first queue slot whose job may still have units to hand out
+    unsigned long long* qtail;  // queue slots reserved so far
+    int* taken;                 // per job: units handed out
     int* status;
     int with_grad;
 };
@@ -407,42 +410,54 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_batch_persist(BArgs<T> A)
     __shared__ FBlock bk;
     __shared__ FPhase sph[MAX_PHASES_PER_BLOCK];
     __shared__ double red[B_THREADS / 32];
-    __shared__ long long w_sh;
+    __shared__ int2 wu_sh;
     __shared__ int stop_sh;
     const uint32_t t = threadIdx.x;
     while (true) {
         if (t == 0) {
-            const long long w = static_cast<long long>(atomicAdd(A.next, 1ULL));
-            int stop = (w >= A.n_work) || (*reinterpret_cast<volatile int*>(A.status) != 0);
-            if (!stop) {
-                const int dep = A.jobs[A.work[w].x].dep;
-                if (dep >= 0) {
-                    const int need = A.jobs[dep].n_units;
-                    const volatile int* cnt = reinterpret_cast<volatile int*>(A.done + dep);
-                    long long spins = 0;
-                    while (*cnt < need) {
-                        if (++spins > SPIN_LIMIT) {
-                            atomicExch(A.status, 1);
-                            stop = 1;
-                            break;
-                        }
-                        if (*reinterpret_cast<volatile int*>(A.status) != 0) {
-                            stop = 1;
-                            break;
-                        }
-                        __nanosleep(256);
-                    }
-                    __threadfence();
+            // take a unit of the oldest ready job that still has one; wait only
+            // while nothing is ready (every job in flight has a running CTA)
+            int stop = 0;
+            int2 got = make_int2(-1, -1);
+            long long spins = 0;
+            while (true) {
+                if (*reinterpret_cast<volatile int*>(A.status) != 0) {
+                    stop = 1;
+                    break;
                 }
+                const unsigned long long h = *reinterpret_cast<volatile unsigned long long*>(A.qhead);
+                if (h >= static_cast<unsigned long long>(A.n_jobs)) {
+                    stop = 1;  // every job has been handed out
+                    break;
+                }
+                if (h < *reinterpret_cast<volatile unsigned long long*>(A.qtail)) {
+                    const int j = *reinterpret_cast<volatile int*>(A.queue + h);
+                    if (j >= 0) {
+                        const int u = atomicAdd(A.taken + j, 1);
+                        if (u < A.jobs[j].n_units) {
+                            got = make_int2(j, u);
+                            break;
+                        }
+                        atomicCAS(A.qhead, h, h + 1);  // job exhausted: move the head on
+                        continue;
+                    }
+                }
+                if (++spins > SPIN_LIMIT) {
+                    atomicExch(A.status, 1);
+                    stop = 1;
+                    break;
+                }
+                __nanosleep(128);
             }
-            w_sh = w;
+            __threadfence();  // the job's inputs were written by its predecessor's units
+            wu_sh = got;
             stop_sh = stop;
         }
         __syncthreads();
         if (stop_sh) {
             break;
         }
-        const int2 wu = A.work[w_sh];
+        const int2 wu = wu_sh;
         const BJob job = A.jobs[wu.x];
         const BInst inst = A.insts[job.inst];
         const uint64_t t0 = static_cast<uint64_t>(wu.y) * static_cast<uint64_t>(job.tiles_per_unit);
@@ -544,7 +559,13 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_batch_persist(BArgs<T> A)
         __syncthreads();
         if (t == 0) {
             __threadfence();
-            atomicAdd(A.done + wu.x, 1);
+            const int d = atomicAdd(A.done + wu.x, 1) + 1;
+            if (d == job.n_units && job.succ >= 0) {
+                // the last unit of the job: its successor is ready
+                __threadfence();
+                const unsigned long long pos = atomicAdd(A.qtail, 1ULL);
+                *reinterpret_cast<volatile int*>(A.queue + pos) = job.succ;
+            }
         }
     }
 }
@@ -1037,7 +1058,7 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
             j.n_tiles = int64_t {1} << (q - K);
             j.n_units = static_cast<int32_t>(units_for(j.n_tiles, &j.tiles_per_unit));
             j.init = (b == 0) ? 1 : 0;
-            j.dep = -1;
+            j.succ = -1;
             chain[k].push_back(static_cast<int32_t>(jobs.size()));
             jobs.push_back(j);
             alg += (b == 0 ? 1.0 : 2.0) * state_bytes;
@@ -1050,7 +1071,7 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
             j.n_tiles = int64_t {1} << (q - K);
             j.n_units = static_cast<int32_t>(units_for(j.n_tiles, &j.tiles_per_unit));
             j.part = epart_size;
-            j.dep = -1;
+            j.succ = -1;
             epart_size += j.n_units;
             esrc.push_back(ESrc {j.part, j.n_units, 0, large[k]});
             chain[k].push_back(static_cast<int32_t>(jobs.size()));
@@ -1078,7 +1099,7 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
                 j.n_units = static_cast<int32_t>(units_for(j.n_tiles, &j.tiles_per_unit));
                 j.n_rows = static_cast<int32_t>(ip.rows_of_block[b].size());
                 j.part = part_size;
-                j.dep = -1;
+                j.succ = -1;
                 for (int32_t r = 0; r < j.n_rows; ++r) {
                     const int64_t grow = row0 + ip.rows_of_block[b][static_cast<size_t>(r)];
                     row_src[static_cast<size_t>(grow - small_rows_end)] =
@@ -1091,41 +1112,40 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
             }
         }
         for (size_t c = 1; c < chain[k].size(); ++c) {
-            jobs[static_cast<size_t>(chain[k][c])].dep = chain[k][c - 1];
+            jobs[static_cast<size_t>(chain[k][c - 1])].succ = chain[k][c];
         }
         ip = ItemPlan<T>();  // free the item's copy
     }
 
-    // work lists per wave: chains aligned at their ends, items interleaved per level
-    std::vector<std::vector<int2>> work(static_cast<size_t>(B->n_waves));
+    // ready queues per wave: each item's first job, the costliest chains first;
+    // later jobs are appended on the device as their predecessors finish
+    std::vector<std::vector<int32_t>> queue0(static_cast<size_t>(B->n_waves));
+    std::vector<int32_t> wave_jobs(static_cast<size_t>(B->n_waves), 0);
     {
         std::vector<std::vector<size_t>> by_wave(static_cast<size_t>(B->n_waves));
         for (size_t k = 0; k < large.size(); ++k) {
             by_wave[static_cast<size_t>(wave_of[k])].push_back(k);
         }
         for (size_t w = 0; w < by_wave.size(); ++w) {
-            size_t lmax = 0;
-            for (size_t k : by_wave[w]) {
-                lmax = std::max(lmax, chain[k].size());
-            }
-            for (size_t level = 0; level < lmax; ++level) {
-                for (size_t k : by_wave[w]) {
-                    const size_t start = lmax - chain[k].size();
-                    if (level < start) {
-                        continue;
-                    }
-                    const int32_t jid = chain[k][level - start];
-                    for (int32_t u = 0; u < jobs[static_cast<size_t>(jid)].n_units; ++u) {
-                        work[w].push_back(make_int2(jid, u));
-                    }
+            auto chain_cost = [&](size_t k) {
+                double c = 0.0;
+                for (int32_t jid : chain[k]) {
+                    c += static_cast<double>(jobs[static_cast<size_t>(jid)].n_tiles);
                 }
+                return c;
+            };
+            std::vector<size_t> order = by_wave[w];
+            std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return chain_cost(x) > chain_cost(y); });
+            for (size_t k : order) {
+                queue0[w].push_back(chain[k].front());
+                wave_jobs[w] += static_cast<int32_t>(chain[k].size());
             }
         }
     }
     B->n_jobs = static_cast<int64_t>(jobs.size());
     B->n_units = 0;
-    for (const auto& w : work) {
-        B->n_units += static_cast<int64_t>(w.size());
+    for (const auto& j : jobs) {
+        B->n_units += j.n_units;
     }
 
     // parameter -> rows (CSR, rows in id order)
@@ -1151,10 +1171,18 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
     const size_t o_strs = lay.add(strs.size() * sizeof(BStr));
     const size_t o_insts = lay.add(insts.size() * sizeof(BInst));
     const size_t o_jobs = lay.add(jobs.size() * sizeof(BJob));
-    std::vector<size_t> o_work(work.size());
-    for (size_t w = 0; w < work.size(); ++w) {
-        o_work[w] = lay.add(work[w].size() * sizeof(int2));
+    // per wave: the queue's initial contents (static) and its head and tail
+    std::vector<size_t> o_q0(queue0.size());
+    std::vector<std::vector<int32_t>> q_init(queue0.size());
+    std::vector<unsigned long long> ht_init;
+    for (size_t w = 0; w < queue0.size(); ++w) {
+        q_init[w].assign(static_cast<size_t>(wave_jobs[w]), -1);
+        std::copy(queue0[w].begin(), queue0[w].end(), q_init[w].begin());
+        o_q0[w] = lay.add(q_init[w].size() * sizeof(int32_t));
+        ht_init.push_back(0ULL);
+        ht_init.push_back(static_cast<unsigned long long>(queue0[w].size()));
     }
+    const size_t o_ht0 = lay.add(ht_init.size() * sizeof(unsigned long long));
     const size_t o_fblk = lay.add(gf.blocks.size() * sizeof(FBlock));
     const size_t o_fph = lay.add(gf.phases.size() * sizeof(FPhase));
     const size_t o_fops = lay.add(gf.ops.size() * sizeof(FOp<T>));
@@ -1171,9 +1199,14 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
     const size_t o_part = lay.add(static_cast<size_t>(part_size) * sizeof(double));
     const size_t o_epart = lay.add(static_cast<size_t>(epart_size) * sizeof(double));
     const size_t o_rowval = lay.add(row_param.size() * sizeof(double));
-    // counters: small-item queue, status, one queue per wave, one completion count per job
-    const size_t count_bytes =
-        sizeof(unsigned int) * 2 + sizeof(unsigned long long) * work.size() + sizeof(int) * jobs.size();
+    // queues (rewritten from their initial contents by every evaluation)
+    std::vector<size_t> o_q(queue0.size());
+    for (size_t w = 0; w < queue0.size(); ++w) {
+        o_q[w] = lay.add(q_init[w].size() * sizeof(int32_t));
+    }
+    const size_t o_ht = lay.add(ht_init.size() * sizeof(unsigned long long));
+    // counters (zeroed by every evaluation): small-item queue, status, per job units done and taken
+    const size_t count_bytes = sizeof(unsigned int) * 2 + 2 * sizeof(int) * jobs.size();
     const size_t o_count = lay.add(count_bytes);
     B->out_bytes = static_cast<size_t>(n_items + n_params) * sizeof(double) + sizeof(double);
     const size_t o_out = lay.add(B->out_bytes);
@@ -1195,9 +1228,10 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         put(o_strs, strs.data(), strs.size() * sizeof(BStr));
         put(o_insts, insts.data(), insts.size() * sizeof(BInst));
         put(o_jobs, jobs.data(), jobs.size() * sizeof(BJob));
-        for (size_t w = 0; w < work.size(); ++w) {
-            put(o_work[w], work[w].data(), work[w].size() * sizeof(int2));
+        for (size_t w = 0; w < q_init.size(); ++w) {
+            put(o_q0[w], q_init[w].data(), q_init[w].size() * sizeof(int32_t));
         }
+        put(o_ht0, ht_init.data(), ht_init.size() * sizeof(unsigned long long));
         put(o_fblk, gf.blocks.data(), gf.blocks.size() * sizeof(FBlock));
         put(o_fph, gf.phases.data(), gf.phases.size() * sizeof(FPhase));
         put(o_fops, gf.ops.data(), gf.ops.size() * sizeof(FOp<T>));
@@ -1226,8 +1260,9 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
     int* d_status_out = reinterpret_cast<int*>(d_grads + n_params);
     unsigned int* d_small_counter = static_cast<unsigned int*>(at(o_count));
     int* d_status = reinterpret_cast<int*>(d_small_counter + 1);
-    unsigned long long* d_next = reinterpret_cast<unsigned long long*>(d_small_counter + 2);
-    int* d_done = reinterpret_cast<int*>(d_next + work.size());
+    int* d_done = reinterpret_cast<int*>(d_small_counter + 2);
+    int* d_taken = d_done + jobs.size();
+    unsigned long long* d_ht = static_cast<unsigned long long*>(at(o_ht));
 
     // launch shapes
     size_t small_smem = 0;
@@ -1280,6 +1315,13 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         ++launches;
     }
     chk(cudaMemsetAsync(at(o_count), 0, count_bytes, s0));
+    for (size_t w = 0; w < q_init.size(); ++w) {
+        chk(cudaMemcpyAsync(at(o_q[w]), at(o_q0[w]), q_init[w].size() * sizeof(int32_t), cudaMemcpyDeviceToDevice, s0));
+    }
+    if (!ht_init.empty()) {
+        chk(cudaMemcpyAsync(d_ht, at(o_ht0), ht_init.size() * sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                            s0));
+    }
     chk(cudaMemsetAsync(d_status_out, 0, sizeof(double), s0));
     chk(cudaEventRecord(B->ev_fork, s0));
     chk(cudaStreamWaitEvent(s1, B->ev_fork, 0));
@@ -1292,13 +1334,13 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         ++launches;
     }
     chk(cudaEventRecord(B->ev_join, s1));
-    for (size_t w = 0; w < work.size(); ++w) {
+    for (size_t w = 0; w < q_init.size(); ++w) {
         BArgs<T> a {};
         a.arena = static_cast<C*>(B->arena);
         a.jobs = static_cast<const BJob*>(at(o_jobs));
         a.insts = static_cast<const BInst*>(at(o_insts));
-        a.work = static_cast<const int2*>(at(o_work[w]));
-        a.n_work = static_cast<long long>(work[w].size());
+        a.queue = static_cast<int*>(at(o_q[w]));
+        a.n_jobs = wave_jobs[w];
         a.fblk = static_cast<const FBlock*>(at(o_fblk));
         a.fph = static_cast<const FPhase*>(at(o_fph));
         a.fops = static_cast<const FOp<T>*>(at(o_fops));
@@ -1309,7 +1351,9 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         a.part = static_cast<double*>(at(o_part));
         a.epart = static_cast<double*>(at(o_epart));
         a.done = d_done;
-        a.next = d_next + w;
+        a.taken = d_taken;
+        a.qhead = d_ht + 2 * w;
+        a.qtail = d_ht + 2 * w + 1;
         a.status = d_status;
         a.with_grad = with_grad;
         k_batch_persist<T><<<big_grid, B_THREADS, big_smem, s0>>>(a);
@@ -1440,7 +1484,7 @@ int32_t kt_batch_evaluate(kt_batch b, const double* params, double* energies, do
     int status = 0;
     std::memcpy(&status, o + b->n_items + b->n_params, sizeof(int));
     if (status != 0) {
-        return kt::fail(KT_ERR_TIMEOUT, "batch: a work unit waited too long for its predecessor block");
+        return kt::fail(KT_ERR_TIMEOUT, "batch: a CTA waited too long for a ready job");
     }
     std::memcpy(energies, o, static_cast<size_t>(b->n_items) * sizeof(double));
     if (grads != nullptr && b->n_params > 0) {
