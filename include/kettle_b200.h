@@ -140,7 +140,8 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
 /* Launch-shape knobs of the engine (no reference counterpart), set by the
  * autotuner (kettle_b200/autotune.py) or from KT_TUNING="name=value,...":
  *   fused_ctas_per_sm  1 or 2   register budget of the fused block kernel
- *   fused_tile_bits    9..12    tile qubits per fused block (complex128)
+ *   fused_tile_bits    9..13    tile qubits per fused block (complex128; complex64
+ *                               one more); 13 runs 512-thread CTAs, one per SM
  *   fused_max_ops      1..256   gates per fused block (also the batch engine's fusion depth)
  *   adjoint_fused      0 or 1   fused adjoint blocks (1) or one kernel per gate (0)
  *   fold_permutations  0 or 1   X / CX with every qubit in a tile folded into a

@@ -1,7 +1,7 @@
 """Autotuner for the fused-block launch shape (no reference counterpart).
 
 The fused kernels take three knobs (kt_tuning_set): the tile size
-(`fused_tile_bits`, 9..12 qubits for complex128, one more for complex64), the
+(`fused_tile_bits`, 9..13 qubits for complex128, one more for complex64), the
 number of gates a block may take (`fused_max_ops`, the fusion depth), and the
 register budget (`fused_ctas_per_sm`: 2 CTAs per SM at <= 128 registers, or 1
 with the compiler's natural allocation).  `autotune` times `kt_sv_apply` on a
@@ -25,7 +25,7 @@ from . import capi
 
 KNOBS = ("fused_tile_bits", "fused_max_ops", "fused_ctas_per_sm")
 DEFAULT_GRID = {
-    "fused_tile_bits": (10, 11, 12),
+    "fused_tile_bits": (10, 11, 12, 13),
     "fused_max_ops": (64, 128, 256),
     "fused_ctas_per_sm": (1, 2),
 }

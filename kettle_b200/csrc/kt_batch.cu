@@ -713,7 +713,7 @@ void plan_item(const kt_batch_item& it, const kt_gate* gates, bool with_grad, It
         ip.opcode[i] = gates[it.gate_offset + static_cast<int64_t>(i)].op;
     }
     // forward blocks (an item without gates still gets one block: it writes |0...0>)
-    const int K = Cfg<T>::RB + TBMAX;
+    const int K = Cfg<T>::RB + TB256;
     // fusion depth: the fused_max_ops knob (set by the autotuner), within the kernel's budgets
     const size_t fwd_ops = static_cast<size_t>(std::min(BATCH_FWD_MAX_OPS, tuning().fused_max_ops));
     const size_t bwd_ops = static_cast<size_t>(std::min(BATCH_BWD_MAX_OPS, tuning().fused_max_ops));
@@ -737,7 +737,7 @@ void plan_item(const kt_batch_item& it, const kt_gate* gates, bool with_grad, It
     }
     if (with_grad) {
         // adjoint blocks over the reversed gate list (U^dagger; rows in backward order)
-        const int KA = CfgA<T>::RB + TBMAX;
+        const int KA = CfgA<T>::RB + TB256;
         const size_t G = lg.size();
         std::vector<LGate> rl(G);
         std::vector<AdjExtra> ex(G);
@@ -1031,8 +1031,8 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
     std::vector<ESrc> esrc;
     int64_t part_size = 0, epart_size = 0;
     double alg = 0.0;
-    const int K = Cfg<T>::RB + TBMAX;
-    const int KA = CfgA<T>::RB + TBMAX;
+    const int K = Cfg<T>::RB + TB256;
+    const int KA = CfgA<T>::RB + TB256;
     for (size_t k = 0; k < large.size(); ++k) {
         const kt_batch_item& it = items[large[k]];
         ItemPlan<T>& ip = ips[k];

@@ -36,10 +36,24 @@ namespace kt
 namespace
 {
 
-// MINB: CTAs per SM the register budget is sized for (2: <= 128 registers,
-// 1: the compiler's natural allocation); chosen per run by the tuning table.
+// SHAPE: 2 = 256 threads, 2 CTAs per SM (<= 128 registers); 1 = 256 threads,
+// 1 CTA per SM (the compiler's natural allocation); 0 = 512 threads, 1 CTA
+// per SM (<= 128 registers: the tiles of 13 complex128 / 14 complex64 qubits).
+#define KT_FUSED_BOUNDS(SHAPE) __launch_bounds__((SHAPE) == 0 ? 512 : 256, (SHAPE) == 0 ? 1 : (SHAPE))
+
+inline int fused_ctas(int shape)
+{
+    return shape == 2 ? 2 : 1;
+}
+
+// dynamic shared memory a launch shape may use: the tile plus MAX_OPS_PER_BLOCK op records
+inline int fused_smem_limit(int shape)
+{
+    return shape == 0 ? 160 * 1024 : 96 * 1024;
+}
+
 template <typename T, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_fused(typename CxT<T>::type* __restrict__ a, const FBlock* __restrict__ blk,
+__global__ void KT_FUSED_BOUNDS(MINB) k_fused(typename CxT<T>::type* __restrict__ a, const FBlock* __restrict__ blk,
                                                   const FPhase* __restrict__ phases, const FOp<T>* __restrict__ ops,
                                                   uint64_t n_tiles)
 {
@@ -88,7 +102,7 @@ __device__ __forceinline__ double norm_scale(const double* target, const double*
 }
 
 template <typename T, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_fused_norm(typename CxT<T>::type* __restrict__ a,
+__global__ void KT_FUSED_BOUNDS(MINB) k_fused_norm(typename CxT<T>::type* __restrict__ a,
                                                        const FBlock* __restrict__ blk,
                                                        const FPhase* __restrict__ phases, const FOp<T>* __restrict__ ops,
                                                        uint64_t n_tiles, NormArgs na)
@@ -98,14 +112,14 @@ __global__ void __launch_bounds__(256, MINB) k_fused_norm(typename CxT<T>::type*
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ FBlock bk;
     __shared__ FPhase sph[MAX_PHASES_PER_BLOCK];
-    __shared__ double w_in[8], w_out[8];
+    __shared__ double w_in[16], w_out[16];
     __shared__ float scale_sh;
     const uint32_t t = threadIdx.x;
     if (t == 0) {
         bk = *blk;
         scale_sh = (na.prev != nullptr) ? static_cast<float>(norm_scale(na.target, na.prev, na.n_parts)) : 1.0f;
     }
-    if (t < 8) {
+    if (t < 16) {
         w_in[t] = 0.0;
         w_out[t] = 0.0;
     }
@@ -121,7 +135,7 @@ __global__ void __launch_bounds__(256, MINB) k_fused_norm(typename CxT<T>::type*
     __syncthreads();
     if (t == 0) {
         double so = 0.0, si = 0.0;
-        for (int w = 0; w < 8; ++w) {
+        for (int w = 0; w < 16; ++w) {
             so += w_out[w];
             si += w_in[w];
         }
@@ -155,21 +169,22 @@ __global__ void k_norm_final(C* __restrict__ a, uint64_t n, const double* __rest
 // the renormalising launch sequence of a complex64 apply (see k_fused_norm)
 template <typename T>
 int32_t run_fused_norm(State& s, const Plan<T>& plan, const FBlock* d_blk, const FPhase* d_ph, const FOp<T>* d_ops,
-                       int K, int threads, int minb)
+                       int K, int threads, int shape)
 {
     using C = typename CxT<T>::type;
-    static bool attr_set[2] = {false, false};
-    if (!attr_set[minb - 1]) {
-        if (minb == 1) {
-            KT_CUDA(cudaFuncSetAttribute(k_fused_norm<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-        } else {
-            KT_CUDA(cudaFuncSetAttribute(k_fused_norm<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    static bool attr_set[3] = {false, false, false};
+    if (!attr_set[shape]) {
+        const int bytes = fused_smem_limit(shape);
+        switch (shape) {
+            case 0: KT_CUDA(cudaFuncSetAttribute(k_fused_norm<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
+            case 1: KT_CUDA(cudaFuncSetAttribute(k_fused_norm<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
+            default: KT_CUDA(cudaFuncSetAttribute(k_fused_norm<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
         }
-        attr_set[minb - 1] = true;
+        attr_set[shape] = true;
     }
     const int n = s.n_bits;
     const uint64_t n_tiles = uint64_t {1} << (n - K);
-    const int grid = static_cast<int>(std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * minb));
+    const int grid = static_cast<int>(std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * fused_ctas(shape)));
     // per-CTA sums: target | out (even blocks) | out (odd blocks)
     if (const int32_t rc = s.scratch2.reserve(3 * static_cast<size_t>(grid) * sizeof(double)); rc != KT_OK) {
         return rc;
@@ -187,12 +202,11 @@ int32_t run_fused_norm(State& s, const Plan<T>& plan, const FBlock* d_blk, const
         na.prev = (b == 0) ? nullptr : out[(b - 1) & 1];
         na.in_parts = (b == 0) ? target : nullptr;
         na.out_parts = out[b & 1];
-        if (minb == 1) {
-            k_fused_norm<T, 1><<<grid, threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b, d_ph, d_ops,
-                                                                 n_tiles, na);
-        } else {
-            k_fused_norm<T, 2><<<grid, threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b, d_ph, d_ops,
-                                                                 n_tiles, na);
+        C* a = static_cast<C*>(s.amps);
+        switch (shape) {
+            case 0: k_fused_norm<T, 0><<<grid, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles, na); break;
+            case 1: k_fused_norm<T, 1><<<grid, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles, na); break;
+            default: k_fused_norm<T, 2><<<grid, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles, na); break;
         }
         KT_CHECK_LAUNCH("k_fused_norm");
         s.last_launches += 1;
@@ -265,33 +279,35 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     const auto* d_ph = reinterpret_cast<const FPhase*>(dev + off_p);
     const auto* d_ops = reinterpret_cast<const FOp<T>*>(dev + off_o);
     const int threads = 1 << (K - RB);
-    const int minb = tuning().fused_ctas_per_sm == 1 ? 1 : 2;
+    // 512-thread tiles run one CTA per SM; 256-thread tiles follow the register-budget knob
+    const int shape = threads > 256 ? 0 : (tuning().fused_ctas_per_sm == 1 ? 1 : 2);
     if constexpr (std::is_same<T, float>::value) {
         if (tuning().c64_renormalize != 0) {
-            return run_fused_norm<T>(s, plan, d_blk, d_ph, d_ops, K, threads, minb);
+            return run_fused_norm<T>(s, plan, d_blk, d_ph, d_ops, K, threads, shape);
         }
     }
-    static bool attr_set[2] = {false, false};
-    if (!attr_set[minb - 1]) {
-        if (minb == 1) {
-            KT_CUDA(cudaFuncSetAttribute(k_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-        } else {
-            KT_CUDA(cudaFuncSetAttribute(k_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    static bool attr_set[3] = {false, false, false};
+    if (!attr_set[shape]) {
+        const int bytes = fused_smem_limit(shape);
+        switch (shape) {
+            case 0: KT_CUDA(cudaFuncSetAttribute(k_fused<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
+            case 1: KT_CUDA(cudaFuncSetAttribute(k_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
+            default: KT_CUDA(cudaFuncSetAttribute(k_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
         }
-        attr_set[minb - 1] = true;
+        attr_set[shape] = true;
     }
     const uint64_t n_tiles = uint64_t {1} << (n - K);
-    const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * minb);
+    const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * fused_ctas(shape));
     const double pass_bytes = 2.0 * static_cast<double>(sizeof(C)) * static_cast<double>(s.n_amps());
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         const auto& fb = plan.blocks[b];
         const size_t smem = (size_t {1} << K) * sizeof(C) + static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOp<T>);
-        if (minb == 1) {
-            k_fused<T, 1><<<static_cast<unsigned>(grid), threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b,
-                                                                                   d_ph, d_ops, n_tiles);
-        } else {
-            k_fused<T, 2><<<static_cast<unsigned>(grid), threads, smem, s.stream>>>(static_cast<C*>(s.amps), d_blk + b,
-                                                                                   d_ph, d_ops, n_tiles);
+        C* a = static_cast<C*>(s.amps);
+        const unsigned g = static_cast<unsigned>(grid);
+        switch (shape) {
+            case 0: k_fused<T, 0><<<g, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles); break;
+            case 1: k_fused<T, 1><<<g, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles); break;
+            default: k_fused<T, 2><<<g, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles); break;
         }
         KT_CHECK_LAUNCH("k_fused");
         s.last_launches += 1;
@@ -374,7 +390,7 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
     constexpr int RB = CfgA<T>::RB;
     constexpr int L = CfgA<T>::L;
     const int n = psi.n_bits;
-    const int K = std::min(n, RB + TBMAX);
+    const int K = std::min(n, RB + TB256);
     std::vector<LGate> lg;
     std::vector<AdjExtra> ex;
     lg.reserve(gates.size());
@@ -456,7 +472,7 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
     auto* d_part = reinterpret_cast<double*>(dev + off_part);
     static bool attr = false;
     if (!attr) {
-        const int most = static_cast<int>(2 * (sizeof(C) << (CfgA<T>::RB + TBMAX)) + ADJ_MAX_OPS * sizeof(FOpA<T>) +
+        const int most = static_cast<int>(2 * (sizeof(C) << (CfgA<T>::RB + TB256)) + ADJ_MAX_OPS * sizeof(FOpA<T>) +
                                           ADJ_MAX_OPS * ADJ_WARPS * sizeof(double));
         KT_CUDA(cudaFuncSetAttribute(k_fused_adj<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         attr = true;

@@ -47,7 +47,8 @@ namespace
 
 constexpr int KMAX = 14;
 constexpr int RBMAX = 5;
-constexpr int TBMAX = 8;
+constexpr int TBMAX = 9;   // thread bits of a tile: up to 512 threads (the largest forward tiles)
+constexpr int TB256 = 8;   // thread bits of the 256-thread kernels (adjoint, batch)
 constexpr int MAX_OPS_PER_BLOCK = 256;
 constexpr int MAX_PHASES_PER_BLOCK = 64;
 

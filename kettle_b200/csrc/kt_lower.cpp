@@ -89,7 +89,7 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
     if (name == "fused_ctas_per_sm") {
         t.fused_ctas_per_sm = (v == 1) ? 1 : 2;
     } else if (name == "fused_tile_bits") {
-        t.fused_tile_bits = static_cast<int>(std::max(9LL, std::min(12LL, v)));
+        t.fused_tile_bits = static_cast<int>(std::max(9LL, std::min(13LL, v)));
     } else if (name == "adjoint_fused") {
         t.adjoint_fused = (v != 0) ? 1 : 0;
     } else if (name == "fused_max_ops") {

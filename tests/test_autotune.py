@@ -16,7 +16,7 @@ def test_candidates_cover_the_grid_in_order():
         {"fused_tile_bits": 12, "fused_max_ops": 128, "fused_ctas_per_sm": 1},
         {"fused_tile_bits": 12, "fused_max_ops": 128, "fused_ctas_per_sm": 2},
     ]
-    assert len(AT.candidates()) == 18
+    assert len(AT.candidates()) == 24
 
 
 def test_search_picks_fastest_and_keeps_first_on_ties():

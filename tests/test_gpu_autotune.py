@@ -11,7 +11,8 @@ from kettle_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def test_candidates_agree(engine, port):
+@pytest.mark.parametrize("dtype,tol", [(capi.KT_C128, 1e-12), (capi.KT_C64, 1e-4)])
+def test_candidates_agree(engine, port, dtype, tol):
     n = 16
     gates = W.random_layers(n, 6, seed=3, mixed=True)
     want = port.apply(n, basis(n), gates)
@@ -19,9 +20,9 @@ def test_candidates_agree(engine, port):
     try:
         for knobs in AT.candidates():
             AT.set_knobs(knobs)
-            sv = capi.Statevector(n)
+            sv = capi.Statevector(n, dtype)
             sv.apply(gates)
-            assert np.abs(sv.download() - want).max() < 1e-12, knobs
+            assert np.abs(sv.download() - want).max() < tol, knobs
             sv.close()
     finally:
         AT.set_knobs(before)
