@@ -206,6 +206,42 @@ def adjoint_bench(stream, n=24, layers=8, ps_params=24, reps=3):
                                   f"(every {params.size // idx.size}th parameter), time scaled to {2 * params.size}"}
 
 
+def batch_bench_sharded(stream, count, world, rank, dist, reps=2):
+    """The batch configuration over `world` GPUs: items sharded by cost
+    (kettle_b200.distributed), one kt_batch per rank, one SUM all-reduce of
+    the energies and gradients; the time is the max over ranks."""
+    import torch
+    from kettle_b200 import capi
+    from kettle_b200 import distributed as D
+    from kettle_b200 import workloads as W
+
+    circuits, params = W.hea_batch(count, seed=SEED)
+    items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
+    out = {"instances": count, "ranks": world, "scaling": "strong (the batch is fixed, sharded by item cost)"}
+    for name, dt in (("c128", capi.KT_C128), ("c64", capi.KT_C64)):
+        sb = D.ShardedBatch(items, gates, strings, coeffs, n_params, rank, world, dtype=dt, dist=dist,
+                            device=torch.device("cuda", torch.cuda.current_device()))
+        if sb.local is not None:
+            sb.local.set_stream(stream.cuda_stream)
+        for _ in range(2):
+            sb.evaluate(params)
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            e, g = sb.evaluate(params)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1) / reps], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        out[name] = {"ms": ms, "instances_per_s": count / (ms / 1e3), "items_on_rank0": len(sb.shards[0])}
+        sb.close()
+    return out
+
+
 def batch_bench(stream, count=4096, reps=2, sample_every=32):
     """Energies and adjoint gradients of `count` hardware-efficient-ansatz
     instances (qubits uniform over 10..22, 2..10 layers, 50 random Pauli
@@ -591,7 +627,10 @@ def run_engine(args):
     if not args.no_adjoint:
         line["adjoint"] = adjoint_bench(stream)
     if args.batch > 0:
-        line["batch"] = batch_bench(stream, count=args.batch)
+        if world > 1:
+            line["batch"] = batch_bench_sharded(stream, args.batch, world, rank, dist)
+        else:
+            line["batch"] = batch_bench(stream, count=args.batch)
     if not args.no_configs and world == 1:
         line["configs"] = config_legs(stream, cpu=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
