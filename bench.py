@@ -145,7 +145,7 @@ def cpu_baseline(n, gates, per_layer, sample_gates=3):
                       f"at {n} qubits, ket::simulate timed alone ({t:.2f} s); layers = gates / {per_layer:.1f}"}
 
 
-def adjoint_bench(stream, n=24, layers=8, ps_params=24, reps=3):
+def adjoint_bench(stream, n=24, layers=8, ps_params=24, reps=3, cpu_ref=True):
     """Adjoint gradient of the 24-qubit, 8-layer hardware-efficient ansatz (384
     parameters) for the XXZ chain, against the parameter-shift rule evaluated
     with the engine's own forward passes on the same GPU."""
@@ -197,13 +197,43 @@ def adjoint_bench(stream, n=24, layers=8, ps_params=24, reps=3):
     t_ps = t_eval * 2 * params.size
     adj.close()
     sv.close()
+    # 50 VQE iterations (L-BFGS-B on the adjoint gradient; the reference's loop uses nlopt, absent here)
+    from kettle_b200 import autograd as AG
+    prob = AG.Problem(n, gates, strings, coeffs)
+    t0 = time.perf_counter()
+    e_best, _, hist = AG.vqe(prob, params, iterations=50)
+    t_vqe = time.perf_counter() - t0
+    prob.close()
+    vqe = {"iterations": 50, "method": "L-BFGS-B (scipy) with adjoint gradients", "evaluations": len(hist),
+           "energy_start": hist[0] if hist else None, "energy_best": e_best, "seconds": t_vqe}
+    cpu = None
+    if cpu_ref:
+        from oracle.oracle import ref, ref_available
+        if ref_available():
+            R = ref()
+            per_layer = gates.size // layers
+            amp0 = np.zeros(1 << n, dtype=np.complex128)
+            amp0[0] = 1.0
+            t0 = time.perf_counter()
+            ra, _ = R.simulate_sv(n, amp0, gates[:per_layer], params)
+            t_layer = time.perf_counter() - t0
+            k = min(10, strings.size)
+            t0 = time.perf_counter()
+            R.expect(n, ra, strings[:k], coeffs[:k])
+            t_h = (time.perf_counter() - t0) * strings.size / k
+            t_fwd = layers * t_layer + t_h
+            cpu = {"forward_plus_energy_s": t_fwd, "param_shift_gradient_s": t_fwd * 2 * params.size, "cores": 1,
+                   "sample": f"ket::simulate of 1 of the {layers} layers ({t_layer:.2f} s, x{layers}) and "
+                             f"expectation_value of {k} of the {strings.size} terms (scaled: {t_h:.2f} s); the "
+                             f"parameter-shift gradient is {2 * params.size} such evaluations"}
     return {"qubits": n, "layers": layers, "params": int(params.size), "hamiltonian_terms": int(strings.size),
             "energy": e, "adjoint_ms": t_adj * 1e3, "adjoint_grads_per_s": params.size / t_adj,
             "param_shift_eval_ms": t_eval * 1e3, "param_shift_grads_per_s": params.size / t_ps,
             "speedup_vs_param_shift": t_ps / t_adj,
             "max_abs_dgrad_vs_param_shift": float(np.abs(g[idx] - ps).max()),
             "param_shift_sample": f"{2 * idx.size} of the {2 * params.size} shifted evaluations timed "
-                                  f"(every {params.size // idx.size}th parameter), time scaled to {2 * params.size}"}
+                                  f"(every {params.size // idx.size}th parameter), time scaled to {2 * params.size}",
+            "vqe": vqe, "cpu_reference": cpu}
 
 
 def batch_bench_sharded(stream, count, world, rank, dist, reps=2):
@@ -396,20 +426,21 @@ def config_legs(stream, cpu=True):
             ra, _ = R.simulate_sv(n, amp0, pre)
             t_sim = time.perf_counter() - t0
             t0 = time.perf_counter()
-            _, rtot = R.expect(n, ra, strings, coeffs)
-            t_exp = time.perf_counter() - t0
+            _, rtot20 = R.expect(n, ra, strings[:20], coeffs[:20])
+            t_exp = (time.perf_counter() - t0) * strings.size / 20
             t0 = time.perf_counter()
             ridx = R.sample_memory(n, ra, 4096, SEED)  # the same mt19937(SEED) draws as `canon`
             t_smp = time.perf_counter() - t0
             ptot, pidx = pipeline(pre)
+            _, ptot20 = sv.expect(strings[:20], coeffs[:20])
             eng = sv.download()
             t_ref = 10 * t_sim + t_exp + t_smp
             c1["cpu_reference"] = {"seconds": t_ref, "layers_per_s": 100 / t_ref, "cores": 1,
                                    "sample": f"ket::simulate on the first 10 layers ({t_sim:.2f} s, x10), "
-                                             f"expectation_value of 200 strings ({t_exp:.2f} s), "
+                                             f"expectation_value of 20 of the 200 strings (x10: {t_exp:.2f} s), "
                                              f"4096 shots ({t_smp:.3f} s)"}
             c1["parity_first_10_layers"] = {"max_abs_amplitude_diff": float(np.abs(eng - ra).max()),
-                                            "abs_expectation_diff": abs(ptot - rtot),
+                                            "abs_expectation_diff_20_strings": abs(ptot20 - rtot20),
                                             "shots_identical": bool(np.array_equal(pidx, ridx))}
     sv.close()
     out["config1"] = c1
@@ -430,6 +461,19 @@ def config_legs(stream, cpu=True):
     out["config2b"] = {"qubits": n, "entries": 1 << (2 * n), "layers": 100, "gates": int(gates.size), "strings": 200,
                        "seconds": t2, "layers_per_s": 100 / t2, "expectation": tot.real, "trace": dm.trace().real}
     dm.close()
+    if cpu:
+        from oracle.oracle import ref, ref_available
+        if ref_available():
+            rho0 = np.zeros((1 << n, 1 << n), dtype=np.complex128)
+            rho0[0, 0] = 1.0
+            sample = gates[n - 1:n + 1]  # a one-qubit gate and the first CX
+            t0 = time.perf_counter()
+            ref().simulate_dm(n, rho0, sample)
+            t_s = time.perf_counter() - t0
+            t_ref = t_s / sample.size * gates.size
+            out["config2b"]["cpu_reference"] = {"seconds": t_ref, "layers_per_s": 100 / t_ref, "cores": 1,
+                                                "sample": f"ket::simulate(circuit, DensityMatrix) of {sample.size} "
+                                                          f"gates ({t_s:.2f} s), scaled to {gates.size} gates"}
     # ---- config 3: 33 q complex64
     n = 33
     gates = W.random_layers(n, 40, seed=SEED, mixed=True)
@@ -625,7 +669,7 @@ def run_engine(args):
             "clocks": clk.summary()}
     sv.close()
     if not args.no_adjoint:
-        line["adjoint"] = adjoint_bench(stream)
+        line["adjoint"] = adjoint_bench(stream, cpu_ref=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     if args.batch > 0:
         if world > 1:
             line["batch"] = batch_bench_sharded(stream, args.batch, world, rank, dist)
