@@ -14,7 +14,11 @@
 //   ket::param::{ParameterID, parameterized, ParameterData}
 //                                        include/kettle/parameter/parameter.hpp:14-65
 //   ket::QuantumCircuit                  include/kettle/circuit/circuit.hpp:20-419 (primitive gates,
-//                                        parameters, M gates; no control flow or loggers)
+//                                        parameters, M gates, classical if / if-else statements,
+//                                        circuit loggers; no compound gates)
+//   ket::ControlFlowPredicate, Classical*Statement, CircuitLogger, CircuitElement
+//                                        include/kettle/circuit/control_flow*.hpp, circuit_element.hpp,
+//                                        include/kettle/circuit_loggers/*.hpp
 //   ket::ClassicalRegister               include/kettle/circuit/classical_register.hpp:14-42
 //   ket::Statevector                     include/kettle/state/statevector.hpp:14-96
 //   ket::DensityMatrix                   include/kettle/state/density_matrix.hpp:22-110 (matrix()
@@ -44,6 +48,7 @@
 #include <unordered_map>
 #include <utility>
 #include <vector>
+#include <variant>
 
 #include "kettle_b200.h"
 
@@ -147,6 +152,190 @@ struct GateInfo
     std::optional<param::ParameterID> parameter;  // angle bound to a circuit parameter
 };
 
+// ---- classical control flow and circuit loggers ---------------------------------------
+// include/kettle/circuit/control_flow_predicate.hpp:12-56, control_flow.hpp:28-157,
+// circuit_loggers/*.hpp, circuit/circuit_element.hpp: the same classes and accessors.
+// Sub-circuits and logged snapshots are immutable once stored and are held by
+// shared pointers (ClonePtr here), which dereference like the reference's ClonePtr.
+class QuantumCircuit;
+class ClassicalRegister;
+class Statevector;
+class DensityMatrix;
+
+template <typename T>
+using ClonePtr = std::shared_ptr<const T>;
+
+enum class ControlFlowBooleanKind : std::uint8_t
+{
+    IF,
+    IF_NOT
+};
+
+class ControlFlowPredicate
+{
+public:
+    ControlFlowPredicate(std::vector<std::size_t> bit_indices_to_check, std::vector<int> expected_bits,
+                         ControlFlowBooleanKind control_kind);
+    auto operator()(const ClassicalRegister& creg) const -> bool;
+    [[nodiscard]] auto bit_indices_to_check() const -> const std::vector<std::size_t>& { return bit_indices_to_check_; }
+    [[nodiscard]] auto expected_bits() const -> const std::vector<int>& { return expected_bits_; }
+    [[nodiscard]] auto control_kind() const -> ControlFlowBooleanKind { return control_kind_; }
+
+private:
+    std::vector<std::size_t> bit_indices_to_check_;
+    std::vector<int> expected_bits_;
+    ControlFlowBooleanKind control_kind_;
+};
+
+class ClassicalIfStatement
+{
+public:
+    ClassicalIfStatement(ControlFlowPredicate predicate, ClonePtr<QuantumCircuit> circuit)
+        : predicate_ {std::move(predicate)}, circuit_ {std::move(circuit)}
+    {}
+    auto operator()(const ClassicalRegister& c_register) const -> bool { return predicate_(c_register); }
+    [[nodiscard]] auto circuit() const -> const ClonePtr<QuantumCircuit>& { return circuit_; }
+    [[nodiscard]] auto predicate() const -> const ControlFlowPredicate& { return predicate_; }
+
+private:
+    ControlFlowPredicate predicate_;
+    ClonePtr<QuantumCircuit> circuit_;
+};
+
+class ClassicalIfElseStatement
+{
+public:
+    ClassicalIfElseStatement(ControlFlowPredicate predicate, ClonePtr<QuantumCircuit> if_circuit,
+                             ClonePtr<QuantumCircuit> else_circuit)
+        : predicate_ {std::move(predicate)}, if_circuit_ {std::move(if_circuit)}, else_circuit_ {std::move(else_circuit)}
+    {}
+    auto operator()(const ClassicalRegister& c_register) const -> bool { return predicate_(c_register); }
+    [[nodiscard]] auto if_circuit() const -> const ClonePtr<QuantumCircuit>& { return if_circuit_; }
+    [[nodiscard]] auto else_circuit() const -> const ClonePtr<QuantumCircuit>& { return else_circuit_; }
+    [[nodiscard]] auto predicate() const -> const ControlFlowPredicate& { return predicate_; }
+
+private:
+    ControlFlowPredicate predicate_;
+    ClonePtr<QuantumCircuit> if_circuit_;
+    ClonePtr<QuantumCircuit> else_circuit_;
+};
+
+class ClassicalControlFlowInstruction
+{
+public:
+    ClassicalControlFlowInstruction(ClassicalIfStatement instruction) : instruction_ {std::move(instruction)} {}  // NOLINT
+    ClassicalControlFlowInstruction(ClassicalIfElseStatement instruction) : instruction_ {std::move(instruction)} {}  // NOLINT
+    [[nodiscard]] auto is_if_statement() const -> bool { return std::holds_alternative<ClassicalIfStatement>(instruction_); }
+    [[nodiscard]] auto is_if_else_statement() const -> bool
+    {
+        return std::holds_alternative<ClassicalIfElseStatement>(instruction_);
+    }
+    [[nodiscard]] auto get_if_statement() const -> const ClassicalIfStatement&
+    {
+        return std::get<ClassicalIfStatement>(instruction_);
+    }
+    [[nodiscard]] auto get_if_else_statement() const -> const ClassicalIfElseStatement&
+    {
+        return std::get<ClassicalIfElseStatement>(instruction_);
+    }
+
+private:
+    std::variant<ClassicalIfStatement, ClassicalIfElseStatement> instruction_;
+};
+
+class ClassicalRegisterCircuitLogger
+{
+public:
+    void add_classical_register(ClassicalRegister cregister);
+    [[nodiscard]] auto classical_register() const -> const ClassicalRegister&;
+
+private:
+    ClonePtr<ClassicalRegister> cregister_;
+};
+
+class StatevectorCircuitLogger
+{
+public:
+    void add_statevector(Statevector statevector);
+    [[nodiscard]] auto statevector() const -> const Statevector&;
+
+private:
+    ClonePtr<Statevector> statevector_;
+};
+
+class DensityMatrixCircuitLogger
+{
+public:
+    void add_density_matrix(DensityMatrix density_matrix);
+    [[nodiscard]] auto density_matrix() const -> const DensityMatrix&;
+
+private:
+    ClonePtr<DensityMatrix> density_matrix_;
+};
+
+class CircuitLogger
+{
+public:
+    CircuitLogger(ClassicalRegisterCircuitLogger logger) : logger_ {std::move(logger)} {}  // NOLINT
+    CircuitLogger(StatevectorCircuitLogger logger) : logger_ {std::move(logger)} {}  // NOLINT
+    CircuitLogger(DensityMatrixCircuitLogger logger) : logger_ {std::move(logger)} {}  // NOLINT
+    [[nodiscard]] auto is_classical_register_circuit_logger() const -> bool
+    {
+        return std::holds_alternative<ClassicalRegisterCircuitLogger>(logger_);
+    }
+    [[nodiscard]] auto get_classical_register_circuit_logger() const -> const ClassicalRegisterCircuitLogger&
+    {
+        return std::get<ClassicalRegisterCircuitLogger>(logger_);
+    }
+    [[nodiscard]] auto is_statevector_circuit_logger() const -> bool
+    {
+        return std::holds_alternative<StatevectorCircuitLogger>(logger_);
+    }
+    [[nodiscard]] auto get_statevector_circuit_logger() const -> const StatevectorCircuitLogger&
+    {
+        return std::get<StatevectorCircuitLogger>(logger_);
+    }
+    [[nodiscard]] auto is_density_matrix_circuit_logger() const -> bool
+    {
+        return std::holds_alternative<DensityMatrixCircuitLogger>(logger_);
+    }
+    [[nodiscard]] auto get_density_matrix_circuit_logger() const -> const DensityMatrixCircuitLogger&
+    {
+        return std::get<DensityMatrixCircuitLogger>(logger_);
+    }
+
+private:
+    std::variant<ClassicalRegisterCircuitLogger, StatevectorCircuitLogger, DensityMatrixCircuitLogger> logger_;
+};
+
+struct CircuitElement
+{
+public:
+    CircuitElement(const GateInfo& ginfo) : element_ {ginfo} {}  // NOLINT
+    CircuitElement(ClassicalIfStatement instruction) : element_ {ClassicalControlFlowInstruction {std::move(instruction)}} {}  // NOLINT
+    CircuitElement(ClassicalIfElseStatement instruction)  // NOLINT
+        : element_ {ClassicalControlFlowInstruction {std::move(instruction)}}
+    {}
+    CircuitElement(CircuitLogger logger) : element_ {std::move(logger)} {}  // NOLINT
+    CircuitElement(ClassicalRegisterCircuitLogger logger) : element_ {CircuitLogger {std::move(logger)}} {}  // NOLINT
+    CircuitElement(StatevectorCircuitLogger logger) : element_ {CircuitLogger {std::move(logger)}} {}  // NOLINT
+    [[nodiscard]] auto is_gate() const -> bool { return std::holds_alternative<GateInfo>(element_); }
+    [[nodiscard]] auto is_control_flow() const -> bool
+    {
+        return std::holds_alternative<ClassicalControlFlowInstruction>(element_);
+    }
+    [[nodiscard]] auto is_circuit_logger() const -> bool { return std::holds_alternative<CircuitLogger>(element_); }
+    [[nodiscard]] auto get_gate() const -> const GateInfo& { return std::get<GateInfo>(element_); }
+    [[nodiscard]] auto get_control_flow() const -> const ClassicalControlFlowInstruction&
+    {
+        return std::get<ClassicalControlFlowInstruction>(element_);
+    }
+    [[nodiscard]] auto get_circuit_logger() const -> const CircuitLogger& { return std::get<CircuitLogger>(element_); }
+
+private:
+    std::variant<GateInfo, ClassicalControlFlowInstruction, CircuitLogger> element_;
+};
+
 // ---- circuit ------------------------------------------------------------------------
 class QuantumCircuit
 {
@@ -157,10 +346,10 @@ public:
     [[nodiscard]] auto n_qubits() const noexcept -> std::size_t { return n_qubits_; }
     [[nodiscard]] auto n_bits() const noexcept -> std::size_t { return n_bits_; }
     [[nodiscard]] auto n_circuit_elements() const noexcept -> std::size_t { return elements_.size(); }
-    [[nodiscard]] auto operator[](std::size_t index) const noexcept -> const GateInfo& { return elements_[index]; }
+    [[nodiscard]] auto operator[](std::size_t index) const noexcept -> const CircuitElement& { return elements_[index]; }
     [[nodiscard]] auto begin() const noexcept { return elements_.begin(); }
     [[nodiscard]] auto end() const noexcept { return elements_.end(); }
-    [[nodiscard]] auto circuit_elements() const noexcept -> const std::vector<GateInfo>& { return elements_; }
+    [[nodiscard]] auto circuit_elements() const noexcept -> const std::vector<CircuitElement>& { return elements_; }
     [[nodiscard]] auto parameter_data_map() const noexcept -> const param::ParameterDataMap& { return parameter_data_; }
     void pop_back();
 
@@ -233,15 +422,29 @@ public:
     void add_m_gate(std::initializer_list<std::size_t> indices) { add_m_gate(std::vector<std::size_t>(indices)); }
     void add_m_gate(std::size_t target_index, std::size_t bit_index);
 
+    // non-gate elements (circuit.hpp:280-362 of the reference)
+    void add_if_statement(ControlFlowPredicate predicate, QuantumCircuit circuit,
+                          double tolerance = MATCHING_PARAMETER_VALUE_TOLERANCE);
+    void add_if_statement(std::size_t bit_index, QuantumCircuit subcircuit);
+    void add_if_not_statement(std::size_t bit_index, QuantumCircuit subcircuit);
+    void add_if_else_statement(ControlFlowPredicate predicate, QuantumCircuit if_subcircuit,
+                               QuantumCircuit else_subcircuit);
+    void add_if_else_statement(std::size_t bit_index, QuantumCircuit if_subcircuit, QuantumCircuit else_subcircuit);
+    void add_if_not_else_statement(std::size_t bit_index, QuantumCircuit if_subcircuit, QuantumCircuit else_subcircuit);
+    void add_classical_register_circuit_logger();
+    void add_statevector_circuit_logger();
+    void add_circuit_logger(CircuitLogger circuit_logger);
+
 private:
     std::size_t n_qubits_;
     std::size_t n_bits_;
-    std::vector<GateInfo> elements_;
+    std::vector<CircuitElement> elements_;
     param::ParameterDataMap parameter_data_;
     std::size_t parameter_count_ {0};
 
     void check_qubit_range_(std::size_t index, const char* qubit_name, const char* gate_name) const;
     void check_bit_range_(std::size_t bit_index) const;
+    void merge_subcircuit_parameters_(const QuantumCircuit& subcircuit, double tolerance);
     void add_one_(Gate g, std::size_t target);
     void add_one_angle_(Gate g, std::size_t target, double angle);
     auto add_one_param_(Gate g, std::size_t target, double angle) -> param::ParameterID;
@@ -385,10 +588,12 @@ public:
     [[nodiscard]] auto has_been_run() const -> bool { return has_been_run_; }
     [[nodiscard]] auto classical_register() const -> const ClassicalRegister&;
     auto classical_register() -> ClassicalRegister&;
+    [[nodiscard]] auto circuit_loggers() const -> const std::vector<CircuitLogger>& { return circuit_loggers_; }
 
 private:
     std::optional<ClassicalRegister> cregister_;
     bool has_been_run_ {false};
+    std::vector<CircuitLogger> circuit_loggers_;
 };
 
 class DensityMatrixSimulator

@@ -181,6 +181,167 @@ void QuantumCircuit::pop_back()
     elements_.pop_back();
 }
 
+// ---- control flow and loggers (circuit.cpp:905-1000, control_flow_predicate.cpp:13-69) ------------
+
+ControlFlowPredicate::ControlFlowPredicate(std::vector<std::size_t> bit_indices_to_check, std::vector<int> expected_bits,
+                                           ControlFlowBooleanKind control_kind)
+    : bit_indices_to_check_ {std::move(bit_indices_to_check)}
+    , expected_bits_ {std::move(expected_bits)}
+    , control_kind_ {control_kind}
+{
+    if (bit_indices_to_check_.size() != expected_bits_.size()) {
+        std::ostringstream err;
+        err << "There is a mismatch in the number of bits to check, and the number of expected bits:\n";
+        err << "bit_indices_to_check.size() = " << bit_indices_to_check_.size() << '\n';
+        err << "expected_bits.size() = " << expected_bits_.size() << '\n';
+        throw std::runtime_error {err.str()};
+    }
+    if (bit_indices_to_check_.empty()) {
+        throw std::runtime_error {"The control flow predicate must depend on at least one bit.\n"};
+    }
+    for (int b : expected_bits_) {
+        if (b != 0 && b != 1) {
+            throw std::runtime_error {"The expected bits must all be 0 or 1.\n"};
+        }
+    }
+}
+
+auto ControlFlowPredicate::operator()(const ClassicalRegister& creg) const -> bool
+{
+    bool all_match = true;
+    for (std::size_t i = 0; i < bit_indices_to_check_.size(); ++i) {
+        const auto bit_index = bit_indices_to_check_[i];
+        if (!creg.is_measured(bit_index)) {
+            std::ostringstream err;
+            err << "There is no measured bit at classical register " << bit_index << '\n';
+            throw std::runtime_error {err.str()};
+        }
+        if (creg.get(bit_index) != expected_bits_[i]) {
+            all_match = false;
+            break;
+        }
+    }
+    return (control_kind_ == ControlFlowBooleanKind::IF) ? all_match : !all_match;
+}
+
+void ClassicalRegisterCircuitLogger::add_classical_register(ClassicalRegister cregister)
+{
+    cregister_ = std::make_shared<const ClassicalRegister>(std::move(cregister));
+}
+
+auto ClassicalRegisterCircuitLogger::classical_register() const -> const ClassicalRegister&
+{
+    if (!cregister_) {
+        throw std::runtime_error {"ERROR: Cannot access classical register; it is not in the logger\n"};
+    }
+    return *cregister_;
+}
+
+void StatevectorCircuitLogger::add_statevector(Statevector statevector)
+{
+    statevector_ = std::make_shared<const Statevector>(std::move(statevector));
+}
+
+auto StatevectorCircuitLogger::statevector() const -> const Statevector&
+{
+    if (!statevector_) {
+        throw std::runtime_error {"ERROR: Cannot access statevector; it is not in the logger\n"};
+    }
+    return *statevector_;
+}
+
+void DensityMatrixCircuitLogger::add_density_matrix(DensityMatrix density_matrix)
+{
+    density_matrix_ = std::make_shared<const DensityMatrix>(std::move(density_matrix));
+}
+
+auto DensityMatrixCircuitLogger::density_matrix() const -> const DensityMatrix&
+{
+    if (!density_matrix_) {
+        throw std::runtime_error {"ERROR: Cannot access density matrix; it is not in the logger\n"};
+    }
+    return *density_matrix_;
+}
+
+void QuantumCircuit::add_if_statement(ControlFlowPredicate predicate, QuantumCircuit circuit, double tolerance)
+{
+    for (auto bit_index : predicate.bit_indices_to_check()) {
+        check_bit_range_(bit_index);
+    }
+    merge_subcircuit_parameters_(circuit, tolerance);
+    elements_.emplace_back(ClassicalIfStatement {std::move(predicate), std::make_shared<const QuantumCircuit>(std::move(circuit))});
+}
+
+void QuantumCircuit::add_if_statement(std::size_t bit_index, QuantumCircuit subcircuit)
+{
+    add_if_statement(ControlFlowPredicate {{bit_index}, {1}, ControlFlowBooleanKind::IF}, std::move(subcircuit));
+}
+
+void QuantumCircuit::add_if_not_statement(std::size_t bit_index, QuantumCircuit subcircuit)
+{
+    add_if_statement(ControlFlowPredicate {{bit_index}, {0}, ControlFlowBooleanKind::IF}, std::move(subcircuit));
+}
+
+void QuantumCircuit::add_if_else_statement(ControlFlowPredicate predicate, QuantumCircuit if_subcircuit,
+                                           QuantumCircuit else_subcircuit)
+{
+    // as in the reference, the branches' parameters are not merged into this circuit's
+    for (auto bit_index : predicate.bit_indices_to_check()) {
+        check_bit_range_(bit_index);
+    }
+    elements_.emplace_back(ClassicalIfElseStatement {std::move(predicate),
+                                                     std::make_shared<const QuantumCircuit>(std::move(if_subcircuit)),
+                                                     std::make_shared<const QuantumCircuit>(std::move(else_subcircuit))});
+}
+
+void QuantumCircuit::add_if_else_statement(std::size_t bit_index, QuantumCircuit if_subcircuit, QuantumCircuit else_subcircuit)
+{
+    add_if_else_statement(ControlFlowPredicate {{bit_index}, {1}, ControlFlowBooleanKind::IF}, std::move(if_subcircuit),
+                          std::move(else_subcircuit));
+}
+
+void QuantumCircuit::add_if_not_else_statement(std::size_t bit_index, QuantumCircuit if_subcircuit,
+                                               QuantumCircuit else_subcircuit)
+{
+    add_if_else_statement(ControlFlowPredicate {{bit_index}, {0}, ControlFlowBooleanKind::IF}, std::move(if_subcircuit),
+                          std::move(else_subcircuit));
+}
+
+void QuantumCircuit::add_classical_register_circuit_logger()
+{
+    elements_.emplace_back(ClassicalRegisterCircuitLogger {});
+}
+
+void QuantumCircuit::add_statevector_circuit_logger()
+{
+    elements_.emplace_back(StatevectorCircuitLogger {});
+}
+
+void QuantumCircuit::add_circuit_logger(CircuitLogger circuit_logger)
+{
+    elements_.emplace_back(std::move(circuit_logger));
+}
+
+// circuit.cpp:1158-1197: parameters of an if-statement's sub-circuit join this circuit's
+void QuantumCircuit::merge_subcircuit_parameters_(const QuantumCircuit& subcircuit, double tolerance)
+{
+    for (const auto& [id, sub_data] : subcircuit.parameter_data_) {
+        const auto [it, inserted] = parameter_data_.insert({id, sub_data});
+        if (inserted) {
+            continue;
+        }
+        auto& cur = it->second;
+        cur.count += sub_data.count;
+        if (!cur.value && sub_data.value) {
+            cur.value = sub_data.value;
+            continue;
+        }
+        if (cur.value && sub_data.value && std::fabs(*cur.value - *sub_data.value) > tolerance) {
+            throw std::runtime_error {"ERROR: found two parameter instances with same id but different non-optional values\n"};
+        }
+    }
+}
+
 void QuantumCircuit::set_parameter_value(const param::ParameterID& id, double angle)
 {
     if (!parameter_data_.contains(id)) {
@@ -837,25 +998,67 @@ void check_valid_number_of_qubits(std::size_t circuit_n, std::size_t state_n)
     }
 }
 
-// the circuit's gates as records, split at M gates
-template <typename ApplyFn, typename MeasureFn>
-void run_segments(const QuantumCircuit& circuit, ApplyFn&& apply, MeasureFn&& measure)
+// The circuit as the reference's simulate loop walks it (simulate.cpp:418-507):
+// a stack of element lists with instruction pointers, if / if-else statements
+// evaluated against the classical register on the host, loggers taking
+// snapshots.  Consecutive gates (across statement boundaries) are collected
+// and handed to the engine as one fused apply; anything that needs the state
+// (M, a logger) or the classical register (a predicate) flushes them first.
+// Gate parameters come from the top circuit's parameter map, as in the reference.
+template <typename ApplyFn, typename MeasureFn, typename LogFn>
+void run_elements(const QuantumCircuit& circuit, const ClassicalRegister& creg, ApplyFn&& apply, MeasureFn&& measure,
+                  LogFn&& log)
 {
+    const auto& pmap = circuit.parameter_data_map();
     std::vector<kt_gate> seg;
-    for (const auto& gi : circuit.circuit_elements()) {
-        if (gi.gate == Gate::M) {
-            if (!seg.empty()) {
-                apply(seg);
-                seg.clear();
-            }
-            measure(gi.arg0, gi.arg1);
+    auto flush = [&]() {
+        if (!seg.empty()) {
+            apply(seg);
+            seg.clear();
+        }
+    };
+    std::vector<const std::vector<CircuitElement>*> stack {&circuit.circuit_elements()};
+    std::vector<std::size_t> ip {0};
+    while (!stack.empty()) {
+        const auto& elems = *stack.back();
+        const std::size_t i = ip.back()++;
+        if (i >= elems.size()) {
+            stack.pop_back();
+            ip.pop_back();
             continue;
         }
-        seg.push_back(to_record(gi, circuit.parameter_data_map()));
+        const auto& el = elems[i];
+        if (el.is_gate()) {
+            const auto& gi = el.get_gate();
+            if (gi.gate == Gate::M) {
+                flush();
+                measure(gi.arg0, gi.arg1);
+            } else {
+                seg.push_back(to_record(gi, pmap));
+            }
+        } else if (el.is_control_flow()) {
+            flush();
+            const auto& cf = el.get_control_flow();
+            const QuantumCircuit* sub = nullptr;
+            if (cf.is_if_statement()) {
+                const auto& st = cf.get_if_statement();
+                if (st(creg)) {
+                    sub = st.circuit().get();
+                }
+            } else {
+                const auto& st = cf.get_if_else_statement();
+                sub = st(creg) ? st.if_circuit().get() : st.else_circuit().get();
+            }
+            if (sub != nullptr) {
+                stack.push_back(&sub->circuit_elements());
+                ip.push_back(0);
+            }
+        } else {
+            flush();
+            log(el.get_circuit_logger());
+        }
     }
-    if (!seg.empty()) {
-        apply(seg);
-    }
+    flush();
 }
 
 }  // namespace
@@ -864,9 +1067,10 @@ void StatevectorSimulator::run(const QuantumCircuit& circuit, Statevector& state
 {
     check_valid_number_of_qubits(circuit.n_qubits(), state.n_qubits());
     cregister_.emplace(circuit.n_bits());
+    circuit_loggers_.clear();
     kt_sv h = state.device();
-    run_segments(
-        circuit,
+    run_elements(
+        circuit, *cregister_,
         [&](const std::vector<kt_gate>& seg) {
             check(kt_sv_apply(h, seg.data(), static_cast<int64_t>(seg.size()), nullptr, 0, KT_APPLY_FUSED));
         },
@@ -880,6 +1084,20 @@ void StatevectorSimulator::run(const QuantumCircuit& circuit, Statevector& state
             const double norm = std::sqrt(1.0 / (outcome == 0 ? p0 : p1));
             check(kt_sv_collapse(h, static_cast<uint32_t>(qubit), outcome, norm));
             cregister_->set(bit, outcome);
+        },
+        [&](const CircuitLogger& logger) {
+            if (logger.is_classical_register_circuit_logger()) {
+                auto l = logger.get_classical_register_circuit_logger();
+                l.add_classical_register(*cregister_);
+                circuit_loggers_.emplace_back(std::move(l));
+            } else if (logger.is_statevector_circuit_logger()) {
+                state.mark_device_modified();
+                auto l = logger.get_statevector_circuit_logger();
+                l.add_statevector(state);
+                circuit_loggers_.emplace_back(std::move(l));
+            } else {
+                throw std::runtime_error {"DEV ERROR: unimplemented circuit logger in `simulate_loop_body_iterative_()`\n"};
+            }
         });
     state.mark_device_modified();
     has_been_run_ = true;
@@ -909,13 +1127,17 @@ void DensityMatrixSimulator::run(const QuantumCircuit& circuit, DensityMatrix& s
     }
     cregister_.emplace(circuit.n_bits());
     kt_dm h = state.device();
-    run_segments(
-        circuit,
+    run_elements(
+        circuit, *cregister_,
         [&](const std::vector<kt_gate>& seg) {
             check(kt_dm_apply(h, seg.data(), static_cast<int64_t>(seg.size()), nullptr, 0, KT_APPLY_FUSED));
         },
         [&](std::size_t, std::size_t) {
             throw std::runtime_error {"ERROR: M gates on a DensityMatrix are not supported by the B200 engine.\n"};
+        },
+        [&](const CircuitLogger&) {
+            // simulate_density_matrix.cpp:391-392
+            throw std::runtime_error {"DEV ERROR: loggers haven't been implemented yet for the density matrix simulator.\n"};
         });
     state.mark_device_modified();
     has_been_run_ = true;
@@ -1296,7 +1518,11 @@ auto adjoint_gradient(const QuantumCircuit& circuit, const Statevector& initial,
     std::vector<kt_gate> recs;
     std::vector<double> values;
     std::vector<param::ParameterID> slot_id;
-    for (const auto& gi : circuit.circuit_elements()) {
+    for (const auto& el : circuit.circuit_elements()) {
+        if (!el.is_gate()) {
+            throw std::runtime_error {"ERROR: the adjoint gradient needs a circuit of gates only (no control flow or loggers).\n"};
+        }
+        const auto& gi = el.get_gate();
         if (gi.gate == Gate::M) {
             throw std::runtime_error {"ERROR: the adjoint gradient needs a circuit without M gates.\n"};
         }

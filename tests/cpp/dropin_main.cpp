@@ -142,6 +142,53 @@ int main(int argc, char** argv)
         std::printf("mamp %zu %.17g %.17g\n", i, msv[i].real(), msv[i].imag());
     }
 
+    // 5b. classical control flow and circuit loggers
+    auto cf = ket::QuantumCircuit {n};
+    build(cf, n, 1, r);
+    cf.add_m_gate(0);
+    cf.add_classical_register_circuit_logger();
+    auto sub_x = ket::QuantumCircuit {n};
+    sub_x.add_x_gate(1);
+    sub_x.add_h_gate(n - 1);
+    cf.add_if_statement(0, sub_x);
+    cf.add_m_gate(1);
+    auto sub_ry = ket::QuantumCircuit {n};
+    sub_ry.add_ry_gate(0, 0.3);
+    sub_ry.add_cx_gate(0, n - 1);
+    auto sub_rz = ket::QuantumCircuit {n};
+    sub_rz.add_rz_gate(0, 0.7);
+    sub_rz.add_h_gate(1);
+    cf.add_if_else_statement(1, sub_ry, sub_rz);
+    cf.add_if_not_statement(0, sub_ry);
+    cf.add_statevector_circuit_logger();
+    cf.add_if_statement(ket::ControlFlowPredicate {{0, 1}, {1, 0}, ket::ControlFlowBooleanKind::IF_NOT}, sub_rz);
+    cf.add_if_not_else_statement(1, sub_x, sub_ry);
+    cf.add_m_gate(n - 1);
+    cf.add_classical_register_circuit_logger();
+    auto csv = ket::Statevector {n};
+    auto csim = ket::StatevectorSimulator {};
+    csim.run(cf, csv, seed + 7);
+    std::printf("cfbits %d %d %d\n", csim.classical_register().get(0), csim.classical_register().get(1),
+                csim.classical_register().get(n - 1));
+    int k = 0;
+    for (const auto& logger : csim.circuit_loggers()) {
+        if (logger.is_classical_register_circuit_logger()) {
+            const auto& creg = logger.get_classical_register_circuit_logger().classical_register();
+            for (std::size_t b = 0; b < n; ++b) {
+                std::printf("logbit %d %zu %d\n", k, b, creg.is_measured(b) ? creg.get(b) : -1);
+            }
+        } else if (logger.is_statevector_circuit_logger()) {
+            const auto& lsv = logger.get_statevector_circuit_logger().statevector();
+            for (std::size_t i = 0; i < lsv.n_states(); ++i) {
+                std::printf("logamp %d %zu %.17g %.17g\n", k, i, lsv[i].real(), lsv[i].imag());
+            }
+        }
+        ++k;
+    }
+    for (std::size_t i = 0; i < csv.n_states(); ++i) {
+        std::printf("cfamp %zu %.17g %.17g\n", i, csv[i].real(), csv[i].imag());
+    }
+
     // 5. density matrix propagation
     const std::size_t nd = n < 5 ? n : 5;
     auto dc = ket::QuantumCircuit {nd};

@@ -2,7 +2,9 @@
 Built against the reference (oracle/_ref/dropin_ref, from the reference's own
 sources) and against this engine's ket:: front end (kettle_b200/lib/dropin_b200),
 both binaries must print the same results: amplitudes, expectation value and
-density matrix within 1e-12, sampled counts and measured bits identical."""
+density matrix within 1e-12, sampled counts and measured bits identical, and
+for a circuit with mid-circuit measurements, if / if-else statements and
+circuit loggers: the same measured bits, logged registers and states."""
 import pathlib
 import subprocess
 
@@ -19,11 +21,18 @@ pytestmark = pytest.mark.gpu
 def _run(exe, *args):
     out = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr
-    rec = {"amp": {}, "mamp": {}, "rho": {}, "count": {}, "expect": None, "cbits": None}
+    rec = {"amp": {}, "mamp": {}, "cfamp": {}, "rho": {}, "count": {}, "expect": None, "cbits": None, "cfbits": None,
+           "logbit": {}, "logamp": {}}
     for line in out.stdout.splitlines():
         f = line.split()
-        if f[0] in ("amp", "mamp"):
+        if f[0] in ("amp", "mamp", "cfamp"):
             rec[f[0]][int(f[1])] = complex(float(f[2]), float(f[3]))
+        elif f[0] == "cfbits":
+            rec["cfbits"] = tuple(int(x) for x in f[1:])
+        elif f[0] == "logbit":
+            rec["logbit"][(int(f[1]), int(f[2]))] = int(f[3])
+        elif f[0] == "logamp":
+            rec["logamp"][(int(f[1]), int(f[2]))] = complex(float(f[3]), float(f[4]))
         elif f[0] == "rho":
             rec["rho"][(int(f[1]), int(f[2]))] = complex(float(f[3]), float(f[4]))
         elif f[0] == "count":
@@ -51,6 +60,16 @@ def test_dropin_same_results(engine, n, layers, seed):
     ma = np.array([ref["mamp"][i] for i in sorted(ref["mamp"])])
     mb = np.array([our["mamp"][i] for i in sorted(our["mamp"])])
     assert np.abs(ma - mb).max() < 1e-12
+    # classical control flow and circuit loggers
+    assert ref["cfbits"] == our["cfbits"]
+    assert ref["logbit"] == our["logbit"] and len(ref["logbit"]) == 2 * n
+    assert sorted(ref["logamp"]) == sorted(our["logamp"]) and len(ref["logamp"]) == 1 << n
+    la = np.array([ref["logamp"][k] for k in sorted(ref["logamp"])])
+    lb = np.array([our["logamp"][k] for k in sorted(our["logamp"])])
+    assert np.abs(la - lb).max() < 1e-12
+    ca = np.array([ref["cfamp"][i] for i in sorted(ref["cfamp"])])
+    cb = np.array([our["cfamp"][i] for i in sorted(our["cfamp"])])
+    assert np.abs(ca - cb).max() < 1e-12
     ra = np.array([ref["rho"][k] for k in sorted(ref["rho"])])
     rb = np.array([our["rho"][k] for k in sorted(our["rho"])])
     assert np.abs(ra - rb).max() < 1e-12
