@@ -4,3 +4,4 @@
 #pragma once
 
 #include "kettle/ket_b200.hpp"
+#include "kettle/ket_b200_io.hpp"

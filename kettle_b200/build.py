@@ -98,7 +98,7 @@ def build_front_end(verbose: bool = False, force: bool = False) -> pathlib.Path:
     demo = LIB / "dropin_b200"
     if demo_src.exists() and (force or _stale(demo, [demo_src, out] + headers)):
         cxx = shutil.which("g++") or "g++"
-        _run([cxx, "-std=c++20", "-O2", f"-I{INCLUDE}", str(demo_src), f"-L{LIB}", "-lket_b200", "-lkettle_b200",
+        _run([cxx, "-std=c++20", "-O2", "-ffp-contract=off", f"-I{INCLUDE}", str(demo_src), f"-L{LIB}", "-lket_b200", "-lkettle_b200",
               "-Wl,-rpath,$ORIGIN", "-o", str(demo)])
     return out
 

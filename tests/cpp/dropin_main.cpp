@@ -6,12 +6,19 @@
 // runs both and compares what they print.
 //
 //   dropin <n_qubits> <layers> <seed>
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <filesystem>
+#include <fstream>
+#include <sstream>
+#include <string>
 #include <vector>
+
+#include <unistd.h>
 
 #include <kettle/kettle.hpp>
 
@@ -89,6 +96,15 @@ auto hamiltonian(std::size_t n, SplitMix& r) -> ket::PauliOperator
         terms.push_back(ket::WeightedPauliString {{r.uniform() - 0.5, r.uniform() - 0.5}, s});
     }
     return ket::PauliOperator {terms};
+}
+
+auto fnv1a(const std::string& text) -> unsigned long long
+{
+    unsigned long long h = 0xcbf29ce484222325ULL;
+    for (const unsigned char ch : text) {
+        h = (h ^ ch) * 0x100000001b3ULL;
+    }
+    return h;
 }
 
 }  // namespace
@@ -200,6 +216,132 @@ int main(int argc, char** argv)
         for (long cc = 0; cc < static_cast<long>(dm.n_states()); ++cc) {
             std::printf("rho %ld %ld %.17g %.17g\n", rr, cc, m(rr, cc).real(), m(rr, cc).imag());
         }
+    }
+    // 6. on-disk formats
+    // 6a. the statevector text, bit for bit, on a state both builds hold
+    //     exactly: amplitudes made here, with zeros, negative zeros and values
+    //     that print as -0.00000000000000
+    std::vector<std::complex<double>> coeffs(std::size_t {1} << n);
+    double norm2 = 0.0;
+    for (std::size_t i = 0; i < coeffs.size(); ++i) {
+        double re = r.uniform() - 0.5;
+        double im = r.uniform() - 0.5;
+        switch (i % 7) {
+            case 1: re = 0.0; break;
+            case 2: im = -0.0; break;
+            case 3: re = -1e-17; break;
+            case 4: im = 4e-15; break;
+            default: break;
+        }
+        coeffs[i] = {re, im};
+        norm2 += re * re + im * im;
+    }
+    const double inv_norm = 1.0 / std::sqrt(norm2);
+    for (auto& c : coeffs) {
+        c *= inv_norm;
+    }
+    const auto hsv = ket::Statevector {coeffs};
+    for (const auto endian : {ket::Endian::LITTLE, ket::Endian::BIG}) {
+        std::ostringstream text;
+        ket::save_statevector(text, hsv, endian);
+        const auto str = text.str();
+        std::printf("svtext %d %zu %016llx\n", static_cast<int>(endian == ket::Endian::BIG), str.size(), fnv1a(str));
+        std::istringstream in {str};
+        const auto back = ket::load_statevector(in);
+        double dev = 0.0;
+        for (std::size_t i = 0; i < hsv.n_states(); ++i) {
+            dev = std::max(dev, std::abs(back[i] - hsv[i]));
+        }
+        std::printf("svload %d %zu %.3g\n", static_cast<int>(endian == ket::Endian::BIG), back.n_qubits(), dev);
+    }
+
+    // 6b. the simulated state through a file, big-endian, and back
+    const auto tmp = std::filesystem::temp_directory_path();
+    const auto tag = std::to_string(static_cast<long>(getpid()));
+    const auto sv_path = tmp / ("kt_dropin_sv_" + tag + ".txt");
+    ket::save_statevector(sv_path, sv, ket::Endian::BIG);
+    const auto sv_back = ket::load_statevector(sv_path);
+    for (std::size_t i = 0; i < sv_back.n_states(); ++i) {
+        std::printf("ioamp %zu %.17g %.17g\n", i, sv_back[i].real(), sv_back[i].imag());
+    }
+
+    // 6c. numpy's complex text, read as big-endian and, from a file, as little-endian
+    std::ostringstream np_text;
+    np_text << n << '\n';
+    char buf[96];
+    for (std::size_t i = 0; i < sv.n_states(); ++i) {
+        const auto v = sv[i];
+        std::snprintf(buf, sizeof(buf), (i % 3 == 0) ? "(%.17g%+.17gj)\n" : "(%.8e%+.8ej)\n", v.real(), v.imag());
+        np_text << buf;
+    }
+    std::istringstream np_in {np_text.str()};
+    const auto np_sv = ket::read_numpy_statevector(np_in, ket::Endian::BIG);
+    for (std::size_t i = 0; i < np_sv.n_states(); ++i) {
+        std::printf("npamp %zu %.17g %.17g\n", i, np_sv[i].real(), np_sv[i].imag());
+    }
+    const auto np_path = tmp / ("kt_dropin_np_" + tag + ".txt");
+    {
+        auto out = std::ofstream {np_path};
+        out << np_text.str();
+    }
+    const auto np_file = ket::read_numpy_statevector(np_path);
+    double np_dev = 0.0;
+    for (std::size_t i = 0; i < np_file.n_states(); ++i) {
+        np_dev = std::max(np_dev, std::abs(np_file[i] - sv[i]));
+    }
+    std::printf("npfile %.3g\n", np_dev);
+
+    // 6d. a Hamiltonian in the "re im : (q, P) ..." text, then its expectation value
+    std::ostringstream ham_text;
+    for (int k = 0; k < 30; ++k) {
+        std::snprintf(buf, sizeof(buf), "%.17g %.17g :", r.uniform() - 0.5, (k % 4 == 0) ? 0.0 : r.uniform() - 0.5);
+        ham_text << buf;
+        for (std::size_t q = 0; q < n; ++q) {
+            const auto t = r.below(4);
+            if (t != 0) {
+                ham_text << " (" << q << ", " << "XYZ"[t - 1] << ')';
+            }
+        }
+        ham_text << '\n';
+    }
+    std::istringstream ham_in {ham_text.str()};
+    const auto ham = ket::read_pauli_operator(ham_in, n);
+    const auto he = ket::expectation_value(ham, sv);
+    std::printf("pauliop %zu %.17g %.17g\n", ham.weighted_pauli_strings().size(), he.real(), he.imag());
+    const auto ham_path = tmp / ("kt_dropin_ham_" + tag + ".txt");
+    {
+        auto out = std::ofstream {ham_path};
+        out << ham_text.str();
+    }
+    const auto he_file = ket::expectation_value(ket::read_pauli_operator(ham_path, n), sv);
+    std::printf("pauliopfile %.17g %.17g\n", he_file.real(), he_file.imag());
+    std::filesystem::remove(sv_path);
+    std::filesystem::remove(np_path);
+    std::filesystem::remove(ham_path);
+
+    // 6e. the readers' errors
+    const auto missing = tmp / ("kt_dropin_missing_" + tag + ".txt");
+    try {
+        (void) ket::load_statevector(missing);
+    } catch (const std::exception& err) {
+        std::printf("ioerr load %d\n", static_cast<int>(std::string {err.what()}.find("unable to open file to load statevector") != std::string::npos));
+    }
+    try {
+        (void) ket::read_numpy_statevector(missing);
+    } catch (const std::exception& err) {
+        std::printf("ioerr numpy %d\n", static_cast<int>(std::string {err.what()}.find("unable to open file for statevector") != std::string::npos));
+    }
+    try {
+        (void) ket::read_pauli_operator(missing, n);
+    } catch (const std::exception& err) {
+        std::printf("ioerr pauli %d\n", static_cast<int>(std::string {err.what()}.find("ERROR: unable to open: ") != std::string::npos));
+    }
+    try {
+        std::istringstream bad {"0.5 0.0 : (0, W)\n"};
+        (void) ket::read_pauli_operator(bad, n);
+        std::printf("ioerr badterm none\n");
+    } catch (const std::out_of_range&) {
+        std::printf("ioerr badterm out_of_range\n");
     }
     return 0;
 }

@@ -4,7 +4,10 @@ sources) and against this engine's ket:: front end (kettle_b200/lib/dropin_b200)
 both binaries must print the same results: amplitudes, expectation value and
 density matrix within 1e-12, sampled counts and measured bits identical, and
 for a circuit with mid-circuit measurements, if / if-else statements and
-circuit loggers: the same measured bits, logged registers and states."""
+circuit loggers: the same measured bits, logged registers and states; and
+for the on-disk formats: the same statevector text byte for byte, the same
+states read back from statevector and numpy text, the same Hamiltonian read
+from Pauli-operator text, and the same reader errors."""
 import pathlib
 import subprocess
 
@@ -21,11 +24,11 @@ pytestmark = pytest.mark.gpu
 def _run(exe, *args):
     out = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr
-    rec = {"amp": {}, "mamp": {}, "cfamp": {}, "rho": {}, "count": {}, "expect": None, "cbits": None, "cfbits": None,
-           "logbit": {}, "logamp": {}}
+    rec = {"amp": {}, "mamp": {}, "cfamp": {}, "ioamp": {}, "npamp": {}, "rho": {}, "count": {}, "expect": None,
+           "cbits": None, "cfbits": None, "logbit": {}, "logamp": {}, "svtext": {}, "svload": {}, "ioerr": {}}
     for line in out.stdout.splitlines():
         f = line.split()
-        if f[0] in ("amp", "mamp", "cfamp"):
+        if f[0] in ("amp", "mamp", "cfamp", "ioamp", "npamp"):
             rec[f[0]][int(f[1])] = complex(float(f[2]), float(f[3]))
         elif f[0] == "cfbits":
             rec["cfbits"] = tuple(int(x) for x in f[1:])
@@ -39,6 +42,18 @@ def _run(exe, *args):
             rec["count"][f[1]] = int(f[2])
         elif f[0] == "expect":
             rec["expect"] = complex(float(f[1]), float(f[2]))
+        elif f[0] == "svtext":
+            rec["svtext"][int(f[1])] = (int(f[2]), f[3])
+        elif f[0] == "svload":
+            rec["svload"][int(f[1])] = (int(f[2]), float(f[3]))
+        elif f[0] in ("npfile",):
+            rec[f[0]] = float(f[1])
+        elif f[0] in ("pauliop",):
+            rec[f[0]] = (int(f[1]), complex(float(f[2]), float(f[3])))
+        elif f[0] in ("pauliopfile",):
+            rec[f[0]] = complex(float(f[1]), float(f[2]))
+        elif f[0] == "ioerr":
+            rec["ioerr"][f[1]] = f[2]
         elif f[0] == "cbit0":
             rec["cbits"] = (int(f[1]), int(f[3]))
     return rec
@@ -73,3 +88,21 @@ def test_dropin_same_results(engine, n, layers, seed):
     ra = np.array([ref["rho"][k] for k in sorted(ref["rho"])])
     rb = np.array([our["rho"][k] for k in sorted(our["rho"])])
     assert np.abs(ra - rb).max() < 1e-12
+    # on-disk formats: the statevector text is the same bytes in both endians
+    assert ref["svtext"] == our["svtext"] and len(our["svtext"]) == 2
+    for endian in (0, 1):
+        assert our["svload"][endian][0] == n and our["svload"][endian][1] < 1e-14
+    ia = np.array([ref["ioamp"][i] for i in sorted(ref["ioamp"])])
+    ib = np.array([our["ioamp"][i] for i in sorted(our["ioamp"])])
+    assert ia.size == b.size and np.abs(ia - ib).max() < 1e-12
+    assert np.abs(ib - b).max() < 1e-13    # 14 printed digits
+    na = np.array([ref["npamp"][i] for i in sorted(ref["npamp"])])
+    nb = np.array([our["npamp"][i] for i in sorted(our["npamp"])])
+    flip = [int(format(i, f"0{n}b")[::-1], 2) for i in range(1 << n)]
+    assert np.abs(na - nb).max() < 1e-12
+    assert np.abs(nb - b[flip]).max() < 1e-7   # every third value has 9 significant digits
+    assert our["npfile"] < 1e-7
+    assert ref["pauliop"][0] == our["pauliop"][0] == 30
+    assert abs(ref["pauliop"][1] - our["pauliop"][1]) < 1e-12
+    assert abs(our["pauliopfile"] - our["pauliop"][1]) == 0.0
+    assert ref["ioerr"] == our["ioerr"] == {"load": "1", "numpy": "1", "pauli": "1", "badterm": "out_of_range"}
