@@ -59,6 +59,7 @@ namespace ket
 constexpr inline auto PROJECTION_NORMALIZATION_TOLERANCE = double {1.0e-8};
 constexpr inline auto CONSTRUCTION_NORMALIZATION_TOLERANCE = double {1.0e-6};
 constexpr inline auto COMPLEX_ALMOST_EQ_TOLERANCE_SQ = double {1.0e-6};
+constexpr inline auto MATRIX_2X2_SQRT_TOLERANCE = double {1.0e-6};
 constexpr inline auto MATCHING_PARAMETER_VALUE_TOLERANCE = double {1.0e-6};
 constexpr inline auto DENSITY_MATRIX_TRACE_TOLERANCE = double {1.0e-8};
 
@@ -88,10 +89,49 @@ struct Matrix2X2
     std::complex<double> elem01;
     std::complex<double> elem10;
     std::complex<double> elem11;
+
+    // common/matrix2x2.hpp:19-25: in-place sum, product (this * other) and scaling
+    auto operator+=(const Matrix2X2& other) noexcept -> Matrix2X2
+    {
+        elem00 += other.elem00;
+        elem01 += other.elem01;
+        elem10 += other.elem10;
+        elem11 += other.elem11;
+        return *this;
+    }
+    auto operator*=(const Matrix2X2& other) noexcept -> Matrix2X2
+    {
+        const auto n00 = elem00 * other.elem00 + elem01 * other.elem10;
+        const auto n01 = elem00 * other.elem01 + elem01 * other.elem11;
+        const auto n10 = elem10 * other.elem00 + elem11 * other.elem10;
+        const auto n11 = elem10 * other.elem01 + elem11 * other.elem11;
+        elem00 = n00;
+        elem01 = n01;
+        elem10 = n10;
+        elem11 = n11;
+        return *this;
+    }
+    template <typename Number>
+    auto operator*=(Number scalar) noexcept -> Matrix2X2
+    {
+        elem00 *= scalar;
+        elem01 *= scalar;
+        elem10 *= scalar;
+        elem11 *= scalar;
+        return *this;
+    }
 };
 
 auto conjugate_transpose(const Matrix2X2& mat) -> Matrix2X2;
 auto operator*(const Matrix2X2& lhs, const Matrix2X2& rhs) -> Matrix2X2;
+auto operator+(const Matrix2X2& lhs, const Matrix2X2& rhs) -> Matrix2X2;
+auto operator*(const Matrix2X2& lhs, std::complex<double> scalar) -> Matrix2X2;
+auto operator*(std::complex<double> scalar, const Matrix2X2& rhs) -> Matrix2X2;
+auto determinant(const Matrix2X2& mat) -> std::complex<double>;
+auto trace(const Matrix2X2& mat) -> std::complex<double>;
+// common/matrix2x2.cpp:117-135: the square root with the positive roots s, t of
+// the general 2x2 formula, switching to -s when |tr + 2s|^2 <= tolerance
+auto matrix_square_root(const Matrix2X2& mat, double matrix_sqrt_tolerance = MATRIX_2X2_SQRT_TOLERANCE) -> Matrix2X2;
 auto almost_eq(const Matrix2X2& left, const Matrix2X2& right,
                double tolerance_sq = COMPLEX_ALMOST_EQ_TOLERANCE_SQ) noexcept -> bool;
 auto almost_eq(const std::complex<double>& left, const std::complex<double>& right,
@@ -148,7 +188,7 @@ struct GateInfo
     std::size_t arg0;   // target (one-target gates), control (controlled gates), qubit (M)
     std::size_t arg1;   // target (controlled gates), classical bit (M)
     double arg2;        // angle
-    std::optional<Matrix2X2> unitary;
+    std::optional<Matrix2X2> unitary_ptr;  // the reference's field name; dereferences the same way
     std::optional<param::ParameterID> parameter;  // angle bound to a circuit parameter
 };
 
@@ -417,6 +457,34 @@ public:
     void add_cu_gate(const Matrix2X2& gate, std::size_t control_index, std::size_t target_index);
     void add_cu_gate(const Matrix2X2& gate, const std::vector<std::pair<std::size_t, std::size_t>>& pairs);
 
+    // compound gates: the same primitive gates the reference appends
+    // (circuit/circuit.cpp:723-900), which the engine fuses like any others
+    using Triplets = std::vector<std::tuple<std::size_t, std::size_t, std::size_t>>;
+    using TripletsIList = std::initializer_list<std::tuple<std::size_t, std::size_t, std::size_t>>;
+    void add_ccx_gate(std::size_t control_index0, std::size_t control_index1, std::size_t target_index);
+    void add_ccx_gate(const Triplets& triplets);
+    void add_ccx_gate(TripletsIList triplets) { add_ccx_gate(Triplets(triplets)); }
+    void add_ccy_gate(std::size_t control_index0, std::size_t control_index1, std::size_t target_index);
+    void add_ccy_gate(const Triplets& triplets);
+    void add_ccy_gate(TripletsIList triplets) { add_ccy_gate(Triplets(triplets)); }
+    void add_ccz_gate(std::size_t control_index0, std::size_t control_index1, std::size_t target_index);
+    void add_ccz_gate(const Triplets& triplets);
+    void add_ccz_gate(TripletsIList triplets) { add_ccz_gate(Triplets(triplets)); }
+    void add_ccu_gate(const Matrix2X2& unitary, std::size_t control_index0, std::size_t control_index1,
+                      std::size_t target_index);
+    void add_ccu_gate(const Matrix2X2& unitary, const Triplets& triplets);
+    void add_ccu_gate(const Matrix2X2& unitary, TripletsIList triplets) { add_ccu_gate(unitary, Triplets(triplets)); }
+    void add_swap_gate(std::size_t target_index0, std::size_t target_index1);
+    void add_swap_gate(const std::vector<std::pair<std::size_t, std::size_t>>& target_index_pairs);
+    void add_swap_gate(std::initializer_list<std::pair<std::size_t, std::size_t>> pairs) { add_swap_gate(std::vector<std::pair<std::size_t, std::size_t>>(pairs)); }
+    void add_cswap_gate(std::size_t control_qubit, std::size_t target_index0, std::size_t target_index1);
+    void add_cswap_gate(const Triplets& triplets);
+    void add_cswap_gate(TripletsIList triplets) { add_cswap_gate(Triplets(triplets)); }
+    void add_qft_gate(const std::vector<std::size_t>& indices);
+    void add_qft_gate(std::initializer_list<std::size_t> indices) { add_qft_gate(std::vector<std::size_t>(indices)); }
+    void add_iqft_gate(const std::vector<std::size_t>& indices);
+    void add_iqft_gate(std::initializer_list<std::size_t> indices) { add_iqft_gate(std::vector<std::size_t>(indices)); }
+
     void add_m_gate(std::size_t target_index);
     void add_m_gate(const std::vector<std::size_t>& indices);
     void add_m_gate(std::initializer_list<std::size_t> indices) { add_m_gate(std::vector<std::size_t>(indices)); }
@@ -436,6 +504,9 @@ public:
     void add_circuit_logger(CircuitLogger circuit_logger);
 
 private:
+    friend void extend_circuit(QuantumCircuit& left, const QuantumCircuit& right);
+    friend auto transpile_to_primitive(const QuantumCircuit& circuit, double tolerance_sq) -> QuantumCircuit;
+
     std::size_t n_qubits_;
     std::size_t n_bits_;
     std::vector<CircuitElement> elements_;
@@ -563,11 +634,19 @@ public:
     [[nodiscard]] auto n_states() const noexcept -> std::size_t { return n_states_; }
     [[nodiscard]] auto n_qubits() const noexcept -> std::size_t { return n_qubits_; }
     [[nodiscard]] auto trace() const -> std::complex<double>;
+    // |Tr(rho^2) - 1|^2 <= tolerance (state/density_matrix.cpp, is_pure)
+    [[nodiscard]] auto is_pure(double tolerance = DENSITY_MATRIX_TRACE_TOLERANCE) const -> bool;
+    [[nodiscard]] auto trace_of_square() const -> std::complex<double>;
 
     [[nodiscard]] auto device() const -> kt_dm;
     void mark_device_modified() const;
 
 private:
+    // adopts a device matrix made by the engine (partial trace, tensor product)
+    DensityMatrix(kt_dm handle, std::size_t n_qubits, DType dtype);
+    friend auto partial_trace(const DensityMatrix& density_matrix, std::vector<std::size_t> qubit_indices) -> DensityMatrix;
+    friend auto tensor_product(const DensityMatrix& left, const DensityMatrix& right) -> DensityMatrix;
+
     std::size_t n_qubits_ {0};
     std::size_t n_states_ {0};
     DType dtype_ {DType::C128};
@@ -579,6 +658,12 @@ private:
 };
 
 auto statevector_to_density_matrix(const Statevector& statevector) -> DensityMatrix;
+
+// state/density_matrix.hpp:115-132.  The left factor's qubits are the low ones.
+auto tensor_product(const DensityMatrix& left, const DensityMatrix& right) -> DensityMatrix;
+auto tensor_product(const std::vector<DensityMatrix>& density_matrices) -> DensityMatrix;
+// Trace over `qubit_indices`; tracing every qubit leaves the trace as a 1 x 1 matrix.
+auto partial_trace(const DensityMatrix& density_matrix, std::vector<std::size_t> qubit_indices) -> DensityMatrix;
 
 // ---- simulation ----------------------------------------------------------------------
 class StatevectorSimulator

@@ -277,6 +277,19 @@ int32_t kt_dm_expect(kt_dm dm, const kt_pauli* strings, int64_t n_strings,
 int32_t kt_dm_trace(kt_dm dm, double* out_re_im);
 /* diagonal of rho as probabilities (for sampling a density matrix) */
 int32_t kt_dm_probabilities(kt_dm dm, double* host_out);
+/* Partial trace over `n_traced` distinct qubits of `src` into `dst`, which
+ * has n - n_traced qubits and src's dtype (n_traced == n leaves the trace in
+ * a 0-qubit, 1 x 1 matrix).  `qubits` lists the traced qubits in the order
+ * they are traced out; sums are grouped like tracing them one at a time in
+ * that order.  Replaces ket::partial_trace (state/density_matrix.hpp:127,
+ * state/density_matrix.cpp:231-278), whose front end traces the highest index
+ * first. */
+int32_t kt_dm_partial_trace(kt_dm src, const int32_t* qubits, int32_t n_traced, kt_dm dst);
+/* rho_left (low qubits) (x) rho_right (high qubits) into dst of
+ * n_left + n_right qubits: ket::tensor_product (state/density_matrix.cpp:187-214). */
+int32_t kt_dm_tensor_product(kt_dm left, kt_dm right, kt_dm dst);
+/* Tr(rho^2), FP64: ket::DensityMatrix::trace_of_square (state/density_matrix.hpp:98-104). */
+int32_t kt_dm_trace_of_square(kt_dm dm, double* out_re_im);
 
 /* ---- adjoint differentiation (new) -------------------------------------------
  * E(theta) = <psi(theta)| H |psi(theta)>, psi = U_G ... U_1 |psi0>.

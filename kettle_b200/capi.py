@@ -91,6 +91,9 @@ _SIGS = {
     "kt_dm_expect": ([P, P, I64, P, P, P], I32),
     "kt_dm_trace": ([P, P], I32),
     "kt_dm_probabilities": ([P, P], I32),
+    "kt_dm_partial_trace": ([P, P, I32, P], I32),
+    "kt_dm_tensor_product": ([P, P, P], I32),
+    "kt_dm_trace_of_square": ([P, P], I32),
     "kt_adjoint_create": ([P, I32, C.POINTER(P)], I32),
     "kt_adjoint_destroy": ([P], I32),
     "kt_adjoint_forward": ([P, P, I64, P, I64, P, I64, P, DP], I32),
@@ -343,6 +346,25 @@ class DensityMatrix:
         out = np.empty(1 << self.n_qubits, dtype=np.float64)
         check(lib().kt_dm_probabilities(self._h, ptr(out)))
         return out
+
+    def partial_trace(self, qubits) -> "DensityMatrix":
+        """A new density matrix: this one traced over `qubits` (distinct), in
+        the order given (sums grouped like tracing one qubit at a time)."""
+        q = np.ascontiguousarray(list(qubits), dtype=np.int32)
+        out = DensityMatrix(self.n_qubits - q.size, self.dtype)
+        check(lib().kt_dm_partial_trace(self._h, ptr(q), q.size, out._h))
+        return out
+
+    def tensor_product(self, right: "DensityMatrix") -> "DensityMatrix":
+        """self (low qubits) (x) right (high qubits)."""
+        out = DensityMatrix(self.n_qubits + right.n_qubits, self.dtype)
+        check(lib().kt_dm_tensor_product(self._h, right._h, out._h))
+        return out
+
+    def trace_of_square(self) -> complex:
+        out = np.empty(2, dtype=np.float64)
+        check(lib().kt_dm_trace_of_square(self._h, ptr(out)))
+        return complex(out[0], out[1])
 
 
 def pairs_single(n: int, t: int, k0: int = 0, count: int | None = None) -> np.ndarray:

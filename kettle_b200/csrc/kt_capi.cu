@@ -489,8 +489,8 @@ int32_t kt_dm_create(int32_t n_qubits, int32_t dtype, kt_dm* out)
         if (const int32_t rc = check_dtype(dtype); rc != KT_OK) {
             return rc;
         }
-        if (n_qubits < 1 || n_qubits > 17) {
-            return invalid("density matrix qubit count out of range (1..17)");
+        if (n_qubits < 0 || n_qubits > 17) {
+            return invalid("density matrix qubit count out of range (0..17)");
         }
         auto* h = new kt_dm_s {};
         h->n = n_qubits;
@@ -585,6 +585,9 @@ int32_t kt_dm_expect(kt_dm dm, const kt_pauli* strings, int64_t n_strings, const
         if (n_strings < 0 || (n_strings > 0 && strings == nullptr)) {
             return invalid("bad Pauli string array");
         }
+        if (dm->n == 0) {
+            return invalid("a density matrix of 0 qubits has no Pauli expectation value");
+        }
         return kt::dm_expect_paulis(dm->st, dm->n, strings, n_strings, coeffs, out_terms, out_total);
     });
 }
@@ -597,6 +600,57 @@ int32_t kt_dm_trace(kt_dm dm, double* out_re_im)
 int32_t kt_dm_probabilities(kt_dm dm, double* host_out)
 {
     return guard([&]() -> int32_t { return (dm && host_out) ? kt::dm_diagonal(dm->st, dm->n, host_out) : invalid("null pointer"); });
+}
+
+int32_t kt_dm_partial_trace(kt_dm src, const int32_t* qubits, int32_t n_traced, kt_dm dst)
+{
+    return guard([&]() -> int32_t {
+        if (src == nullptr || dst == nullptr || src == dst) {
+            return invalid("partial trace needs two distinct density matrices");
+        }
+        if (n_traced < 0 || n_traced > src->n || (n_traced > 0 && qubits == nullptr)) {
+            return invalid("bad traced-qubit array");
+        }
+        uint32_t seen = 0;
+        for (int32_t j = 0; j < n_traced; ++j) {
+            if (qubits[j] < 0 || qubits[j] >= src->n) {
+                return invalid("ERROR: Cannot take partial trace; found qubit index out of bounds\n");
+            }
+            if (((seen >> qubits[j]) & 1U) != 0U) {
+                return invalid("traced qubits must be distinct");
+            }
+            seen |= 1U << qubits[j];
+        }
+        if (dst->n != src->n - n_traced || dst->st.dtype != src->st.dtype) {
+            return invalid("the output density matrix needs n - n_traced qubits and the input's dtype");
+        }
+        if (n_traced == 0) {
+            KT_CUDA(cudaMemcpyAsync(dst->st.amps, src->st.amps, src->st.n_amps() * src->st.amp_bytes(),
+                                    cudaMemcpyDeviceToDevice, dst->st.stream));
+            return KT_OK;
+        }
+        return kt::dm_partial_trace(src->st, src->n, qubits, n_traced, dst->st);
+    });
+}
+
+int32_t kt_dm_tensor_product(kt_dm left, kt_dm right, kt_dm dst)
+{
+    return guard([&]() -> int32_t {
+        if (left == nullptr || right == nullptr || dst == nullptr || dst == left || dst == right) {
+            return invalid("tensor product needs two inputs and a distinct output");
+        }
+        if (dst->n != left->n + right->n || left->st.dtype != dst->st.dtype || right->st.dtype != dst->st.dtype) {
+            return invalid("the output density matrix needs n_left + n_right qubits and the inputs' dtype");
+        }
+        return kt::dm_tensor_product(left->st, left->n, right->st, right->n, dst->st);
+    });
+}
+
+int32_t kt_dm_trace_of_square(kt_dm dm, double* out_re_im)
+{
+    return guard([&]() -> int32_t {
+        return (dm && out_re_im) ? kt::dm_trace_of_square(dm->st, dm->n, out_re_im) : invalid("null pointer");
+    });
 }
 
 }  // extern "C"

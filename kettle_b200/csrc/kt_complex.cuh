@@ -85,4 +85,18 @@ __device__ __forceinline__ double2 to_d2(float2 v)
     return make_double2(static_cast<double>(v.x), static_cast<double>(v.y));
 }
 
+// FP64 value -> the storage type (round to nearest for complex64)
+template <typename C>
+__device__ __forceinline__ C from_d2(double2 v);
+template <>
+__device__ __forceinline__ double2 from_d2<double2>(double2 v)
+{
+    return v;
+}
+template <>
+__device__ __forceinline__ float2 from_d2<float2>(double2 v)
+{
+    return make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+}
+
 }  // namespace kt

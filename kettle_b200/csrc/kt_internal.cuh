@@ -157,6 +157,10 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
                int32_t* n_rescanned);
 int32_t dm_trace(State& s, int n_qubits, double* out);
 int32_t dm_diagonal(State& s, int n_qubits, double* host_out);
+// density-matrix operations (kt_dm_ops.cu); `traced` in trace order, distinct
+int32_t dm_partial_trace(const State& src, int n_qubits, const int32_t* traced, int n_traced, State& dst);
+int32_t dm_tensor_product(const State& left, int n_left, const State& right, int n_right, State& dst);
+int32_t dm_trace_of_square(State& s, int n_qubits, double* out);
 
 // pin-memory staging helper for host <-> device copies
 int32_t copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t st);

@@ -69,8 +69,8 @@ auto to_record(const GateInfo& gi, const param::ParameterDataMap& pmap) -> kt_ga
         }
         r.angle = *it->second.value;
     }
-    if (gi.unitary) {
-        const Matrix2X2& m = *gi.unitary;
+    if (gi.unitary_ptr) {
+        const Matrix2X2& m = *gi.unitary_ptr;
         const std::complex<double> e[4] = {m.elem00, m.elem01, m.elem10, m.elem11};
         for (int i = 0; i < 4; ++i) {
             r.u[2 * i] = e[i].real();
@@ -103,6 +103,48 @@ auto operator*(const Matrix2X2& a, const Matrix2X2& b) -> Matrix2X2
 {
     return {a.elem00 * b.elem00 + a.elem01 * b.elem10, a.elem00 * b.elem01 + a.elem01 * b.elem11,
             a.elem10 * b.elem00 + a.elem11 * b.elem10, a.elem10 * b.elem01 + a.elem11 * b.elem11};
+}
+
+auto operator+(const Matrix2X2& a, const Matrix2X2& b) -> Matrix2X2
+{
+    return {a.elem00 + b.elem00, a.elem01 + b.elem01, a.elem10 + b.elem10, a.elem11 + b.elem11};
+}
+
+auto operator*(const Matrix2X2& a, std::complex<double> k) -> Matrix2X2
+{
+    return {a.elem00 * k, a.elem01 * k, a.elem10 * k, a.elem11 * k};
+}
+
+auto operator*(std::complex<double> k, const Matrix2X2& a) -> Matrix2X2
+{
+    return a * k;
+}
+
+auto determinant(const Matrix2X2& m) -> std::complex<double>
+{
+    return m.elem00 * m.elem11 - m.elem10 * m.elem01;
+}
+
+auto trace(const Matrix2X2& m) -> std::complex<double>
+{
+    return m.elem00 + m.elem11;
+}
+
+auto matrix_square_root(const Matrix2X2& m, double tolerance) -> Matrix2X2
+{
+    // sqrt(M) = (M + s I) / t with s = sqrt(det M), t = sqrt(tr M + 2 s); the
+    // other sign of s where tr M + 2 s vanishes (within the tolerance)
+    const auto tr = m.elem00 + m.elem11;
+    const auto det = m.elem00 * m.elem11 - m.elem01 * m.elem10;
+    auto s = std::sqrt(det);
+    std::complex<double> t;
+    if (std::norm(tr + 2.0 * s) > tolerance) {
+        t = std::sqrt(tr + 2.0 * s);
+    } else {
+        t = std::sqrt(tr - 2.0 * s);
+        s = -s;
+    }
+    return {(m.elem00 + s) / t, m.elem01 / t, m.elem10 / t, (m.elem11 + s) / t};
 }
 
 auto almost_eq(const std::complex<double>& l, const std::complex<double>& r, double tol_sq) noexcept -> bool
@@ -562,6 +604,161 @@ void QuantumCircuit::add_cu_gate(const Matrix2X2& gate, const std::vector<std::p
     }
 }
 
+// ---- compound gates (circuit/circuit.cpp:723-900) ------------------------------------------
+
+void QuantumCircuit::add_ccx_gate(std::size_t c0, std::size_t c1, std::size_t target)
+{
+    // sqrt(X) on the target under c1, c1 XOR c0, and c0: X exactly when both are set
+    add_csx_gate(c1, target);
+    add_cx_gate(c0, c1);
+    add_cx_gate(c1, target);
+    add_csx_gate(c1, target);
+    add_cx_gate(c0, c1);
+    add_csx_gate(c0, target);
+}
+
+void QuantumCircuit::add_ccx_gate(const Triplets& triplets)
+{
+    for (const auto& [c0, c1, t] : triplets) {
+        add_ccx_gate(c0, c1, t);
+    }
+}
+
+void QuantumCircuit::add_ccy_gate(std::size_t c0, std::size_t c1, std::size_t target)
+{
+    add_sdag_gate(target);
+    add_ccx_gate(c0, c1, target);
+    add_s_gate(target);
+}
+
+void QuantumCircuit::add_ccy_gate(const Triplets& triplets)
+{
+    for (const auto& [c0, c1, t] : triplets) {
+        add_ccy_gate(c0, c1, t);
+    }
+}
+
+void QuantumCircuit::add_ccz_gate(std::size_t c0, std::size_t c1, std::size_t target)
+{
+    add_h_gate(target);
+    add_ccx_gate(c0, c1, target);
+    add_h_gate(target);
+}
+
+void QuantumCircuit::add_ccz_gate(const Triplets& triplets)
+{
+    for (const auto& [c0, c1, t] : triplets) {
+        add_ccz_gate(c0, c1, t);
+    }
+}
+
+void QuantumCircuit::add_ccu_gate(const Matrix2X2& unitary, std::size_t c0, std::size_t c1, std::size_t target)
+{
+    const auto root = matrix_square_root(unitary);
+    const auto root_adj = conjugate_transpose(root);
+    add_cu_gate(root, c1, target);
+    add_cx_gate(c0, c1);
+    add_cu_gate(root_adj, c1, target);
+    add_cx_gate(c0, c1);
+    add_cu_gate(root, c0, target);
+}
+
+void QuantumCircuit::add_ccu_gate(const Matrix2X2& unitary, const Triplets& triplets)
+{
+    for (const auto& [c0, c1, t] : triplets) {
+        add_ccu_gate(unitary, c0, c1, t);
+    }
+}
+
+void QuantumCircuit::add_swap_gate(std::size_t t0, std::size_t t1)
+{
+    if (t0 == t1) {
+        throw std::runtime_error {"Cannot swap a index with itself"};
+    }
+    add_cx_gate(t0, t1);
+    add_cx_gate(t1, t0);
+    add_cx_gate(t0, t1);
+}
+
+void QuantumCircuit::add_swap_gate(const std::vector<std::pair<std::size_t, std::size_t>>& target_index_pairs)
+{
+    for (const auto& [t0, t1] : target_index_pairs) {
+        add_swap_gate(t0, t1);
+    }
+}
+
+void QuantumCircuit::add_cswap_gate(std::size_t control, std::size_t t0, std::size_t t1)
+{
+    if (t0 == t1) {
+        throw std::runtime_error {"Cannot swap a qubit with itself"};
+    }
+    if (control == t0 || control == t1) {
+        throw std::runtime_error {"Cannot use the control qubit as one of the qubits to be swapped"};
+    }
+    add_cx_gate(t1, t0);
+    add_ccx_gate(control, t0, t1);
+    add_cx_gate(t1, t0);
+}
+
+void QuantumCircuit::add_cswap_gate(const Triplets& triplets)
+{
+    for (const auto& [c, t0, t1] : triplets) {
+        add_cswap_gate(c, t0, t1);
+    }
+}
+
+namespace
+{
+
+// reverse the order of `indices` with swaps, outermost pair first
+void fourier_swaps(QuantumCircuit& circuit, const std::vector<std::size_t>& indices)
+{
+    if (indices.empty()) {
+        return;
+    }
+    std::size_t left = 0;
+    std::size_t right = indices.size() - 1;
+    while (right > left) {
+        circuit.add_swap_gate(indices[left], indices[right]);
+        ++left;
+        --right;
+    }
+}
+
+}  // namespace
+
+void QuantumCircuit::add_qft_gate(const std::vector<std::size_t>& indices)
+{
+    // H on each target, then CP(2 pi / 2^d) from every later index at distance d - 1
+    const auto size = indices.size();
+    for (std::size_t i = 0; i < size; ++i) {
+        add_h_gate(indices[i]);
+        std::size_t denom_bits = 2;
+        for (std::size_t j = i + 1; j < size; ++j) {
+            const double angle = 2.0 * M_PI / static_cast<double>(std::size_t {1} << denom_bits);
+            add_cp_gate(indices[j], indices[i], angle);
+            ++denom_bits;
+        }
+    }
+    fourier_swaps(*this, indices);
+}
+
+void QuantumCircuit::add_iqft_gate(const std::vector<std::size_t>& indices)
+{
+    // the adjoint: the swaps, then the forward sequence reversed with negated angles
+    fourier_swaps(*this, indices);
+    const auto size = indices.size();
+    for (std::size_t ii = size; ii-- > 0;) {
+        std::size_t denom_bits = size - ii;
+        for (std::size_t jj = size; jj-- > ii + 1;) {
+            const double angle = 2.0 * M_PI / static_cast<double>(std::size_t {1} << denom_bits);
+            add_cp_gate(indices[jj], indices[ii], -angle);
+            --denom_bits;
+        }
+        add_h_gate(indices[ii]);
+    }
+}
+
 void QuantumCircuit::add_m_gate(std::size_t target)
 {
     add_m_gate(target, target);
@@ -843,7 +1040,7 @@ DensityMatrix::DensityMatrix(HostMatrix matrix, const density_matrix_nocheck&, D
     : n_states_ {static_cast<std::size_t>(matrix.cols())}
     , dtype_ {dtype}
 {
-    if (matrix.rows() != matrix.cols() || !is_power_of_2(n_states_) || n_states_ < 2) {
+    if (matrix.rows() != matrix.cols() || !is_power_of_2(n_states_) || n_states_ < 1) {
         throw std::runtime_error {"The provided coefficients must have a size equal to a power of 2.\n"};
     }
     n_qubits_ = static_cast<std::size_t>(__builtin_ctzll(n_states_));
@@ -967,6 +1164,85 @@ auto DensityMatrix::trace() const -> std::complex<double>
     double out[2];
     check(kt_dm_trace(device(), out));
     return {out[0], out[1]};
+}
+
+DensityMatrix::DensityMatrix(kt_dm handle, std::size_t n_qubits, DType dtype)
+    : n_qubits_ {n_qubits}
+    , n_states_ {std::size_t {1} << n_qubits}
+    , dtype_ {dtype}
+    , handle_ {handle}
+{}
+
+auto DensityMatrix::trace_of_square() const -> std::complex<double>
+{
+    double out[2];
+    check(kt_dm_trace_of_square(device(), out));
+    return {out[0], out[1]};
+}
+
+auto DensityMatrix::is_pure(double tolerance) const -> bool
+{
+    return std::norm(trace_of_square() - std::complex<double> {1.0, 0.0}) <= tolerance;
+}
+
+auto tensor_product(const DensityMatrix& left, const DensityMatrix& right) -> DensityMatrix
+{
+    const auto n = left.n_qubits() + right.n_qubits();
+    const auto dtype = (left.dtype_ == DType::C64 && right.dtype_ == DType::C64) ? DType::C64 : DType::C128;
+    if (left.dtype_ != dtype || right.dtype_ != dtype) {
+        // mixed storage: the complex64 factor is widened first
+        const DensityMatrix wide_left = (left.dtype_ == dtype) ? left : DensityMatrix {left.matrix(), density_matrix_nocheck {}, dtype};
+        const DensityMatrix wide_right = (right.dtype_ == dtype) ? right : DensityMatrix {right.matrix(), density_matrix_nocheck {}, dtype};
+        return tensor_product(wide_left, wide_right);
+    }
+    kt_dm out = nullptr;
+    check(kt_dm_create(static_cast<int32_t>(n), static_cast<int32_t>(dtype), &out));
+    auto result = DensityMatrix {out, n, dtype};
+    check(kt_dm_tensor_product(left.device(), right.device(), out));
+    return result;
+}
+
+auto tensor_product(const std::vector<DensityMatrix>& density_matrices) -> DensityMatrix
+{
+    if (density_matrices.size() < 2) {
+        throw std::runtime_error {"Cannot take tensor product of 0 or 1 matrices.\n"};
+    }
+    auto output = tensor_product(density_matrices[0], density_matrices[1]);
+    for (std::size_t i = 2; i < density_matrices.size(); ++i) {
+        output = tensor_product(output, density_matrices[i]);
+    }
+    return output;
+}
+
+auto partial_trace(const DensityMatrix& density_matrix, std::vector<std::size_t> qubit_indices) -> DensityMatrix
+{
+    // state/density_matrix.cpp:231-278: indices sorted high to low, each one an
+    // index into the matrix left by the traces before it
+    const auto n = density_matrix.n_qubits();
+    const auto out_of_range = [n](std::size_t index) { return index >= n; };
+    if (std::any_of(qubit_indices.begin(), qubit_indices.end(), out_of_range) || qubit_indices.size() > n) {
+        throw std::runtime_error {"ERROR: Cannot take partial trace; found qubit index out of bounds\n"};
+    }
+    std::sort(qubit_indices.begin(), qubit_indices.end(), [](auto x, auto y) { return x > y; });
+    std::vector<std::size_t> remaining(n);
+    for (std::size_t q = 0; q < n; ++q) {
+        remaining[q] = q;
+    }
+    std::vector<int32_t> traced;
+    traced.reserve(qubit_indices.size());
+    for (const auto position : qubit_indices) {
+        if (position >= remaining.size()) {
+            throw std::runtime_error {"ERROR: Cannot take partial trace; found qubit index out of bounds\n"};
+        }
+        traced.push_back(static_cast<int32_t>(remaining[position]));
+        remaining.erase(remaining.begin() + static_cast<std::ptrdiff_t>(position));
+    }
+    const auto m = remaining.size();
+    kt_dm out = nullptr;
+    check(kt_dm_create(static_cast<int32_t>(m), static_cast<int32_t>(density_matrix.dtype_), &out));
+    auto result = DensityMatrix {out, m, density_matrix.dtype_};
+    check(kt_dm_partial_trace(density_matrix.device(), traced.data(), static_cast<int32_t>(traced.size()), out));
+    return result;
 }
 
 auto statevector_to_density_matrix(const Statevector& sv) -> DensityMatrix

@@ -565,3 +565,100 @@ int32_t kto_dm_expect(int32_t n, const double* rho_d, const kt_pauli* strings, i
     if (out_total) { out_total[0] = total.re; out_total[1] = total.im; }
     return 0;
 }
+
+/*
+ * Partial trace, restated from state/density_matrix.cpp:231-278: the indices
+ * are sorted high to low and traced one at a time; tracing (current-matrix)
+ * qubit q keeps, for every reduced row r' and column c' (column-major), the
+ * sum current(r, c) + current(r + 2^q, c + 2^q) with r, c = r', c' with a 0
+ * inserted at bit q (PartialTraceIndexGenerator_ order: blocks of 2^(q+1),
+ * steps of 1 inside the low half).  `qubits` holds k indices, each < n
+ * (duplicates allowed: each is an index into the matrix left by the traces
+ * before it, as the reference reads them).  rho_out has 4^(n-k) entries.
+ */
+static int cmp_desc_size(const void* a, const void* b)
+{
+    const int64_t x = *(const int64_t*)a, y = *(const int64_t*)b;
+    return (x < y) - (x > y);
+}
+
+int32_t kto_dm_partial_trace(int32_t n, const double* rho_d, const int64_t* qubits, int32_t k, double* out_d)
+{
+    if (n < 0 || k < 0 || k > n) {
+        return KT_ERR_INVALID;
+    }
+    int64_t* q = (int64_t*)malloc(sizeof(int64_t) * (size_t)(k > 0 ? k : 1));
+    for (int32_t i = 0; i < k; ++i) {
+        if (qubits[i] < 0 || qubits[i] >= n) {
+            free(q);
+            return KT_ERR_INVALID;
+        }
+        q[i] = qubits[i];
+    }
+    qsort(q, (size_t)k, sizeof(int64_t), cmp_desc_size);
+    uint64_t N = (uint64_t)1 << n;
+    cplx* cur = (cplx*)malloc(sizeof(cplx) * N * N);
+    memcpy(cur, rho_d, sizeof(cplx) * N * N);
+    for (int32_t i = 0; i < k; ++i) {
+        const int64_t n_cur = n - i;
+        if (q[i] >= n_cur) {
+            free(cur);
+            free(q);
+            return KT_ERR_INVALID;
+        }
+        const uint64_t step = (uint64_t)1 << q[i];
+        const uint64_t Nc = (uint64_t)1 << n_cur;
+        const uint64_t Nr = Nc >> 1;
+        cplx* red = (cplx*)malloc(sizeof(cplx) * (Nr > 0 ? Nr * Nr : 1));
+        for (uint64_t ic = 0; ic < Nr; ++ic) {
+            const uint64_t c = ((ic / step) * 2 * step) + (ic % step);
+            for (uint64_t ir = 0; ir < Nr; ++ir) {
+                const uint64_t r = ((ir / step) * 2 * step) + (ir % step);
+                red[ir + ic * Nr] = cadd(cur[r + c * Nc], cur[(r + step) + (c + step) * Nc]);
+            }
+        }
+        free(cur);
+        cur = red;
+        N = Nr;
+    }
+    memcpy(out_d, cur, sizeof(cplx) * N * N);
+    free(cur);
+    free(q);
+    return KT_OK;
+}
+
+/* state/density_matrix.cpp:187-214: result(rR * A + rL, cR * A + cL) = L(rL, cL) R(rR, cR) */
+int32_t kto_dm_tensor_product(int32_t nl, const double* left_d, int32_t nr, const double* right_d, double* out_d)
+{
+    const uint64_t A = (uint64_t)1 << nl, B = (uint64_t)1 << nr, D = A * B;
+    const cplx* L = (const cplx*)left_d;
+    const cplx* R = (const cplx*)right_d;
+    cplx* out = (cplx*)out_d;
+    for (uint64_t cl = 0; cl < A; ++cl) {
+        for (uint64_t rl = 0; rl < A; ++rl) {
+            const cplx lv = L[rl + cl * A];
+            for (uint64_t cr = 0; cr < B; ++cr) {
+                for (uint64_t rr = 0; rr < B; ++rr) {
+                    out[(rr * A + rl) + (cr * A + cl) * D] = cmul(lv, R[rr + cr * B]);
+                }
+            }
+        }
+    }
+    return KT_OK;
+}
+
+/* Tr(rho^2) = sum_i sum_j rho(i, j) rho(j, i), row by row */
+int32_t kto_dm_trace_of_square(int32_t n, const double* rho_d, double* out)
+{
+    const uint64_t N = (uint64_t)1 << n;
+    const cplx* rho = (const cplx*)rho_d;
+    cplx s = {0.0, 0.0};
+    for (uint64_t i = 0; i < N; ++i) {
+        for (uint64_t j = 0; j < N; ++j) {
+            s = cadd(s, cmul(rho[i + j * N], rho[j + i * N]));
+        }
+    }
+    out[0] = s.re;
+    out[1] = s.im;
+    return KT_OK;
+}

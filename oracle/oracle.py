@@ -66,6 +66,12 @@ class Port:
         L.kto_dm_expect.argtypes = [I32, P, P, I64, P, P, P]
         L.kto_dm_expect.restype = I32
         L.kto_gate_matrix.argtypes = [P, P, P]
+        L.kto_dm_partial_trace.argtypes = [I32, P, P, I32, P]
+        L.kto_dm_partial_trace.restype = I32
+        L.kto_dm_tensor_product.argtypes = [I32, P, I32, P, P]
+        L.kto_dm_tensor_product.restype = I32
+        L.kto_dm_trace_of_square.argtypes = [I32, P, P]
+        L.kto_dm_trace_of_square.restype = I32
         self.L = L
 
     def pairs_single(self, n, t, k0=0, count=None):
@@ -147,6 +153,34 @@ class Port:
         self.L.kto_dm_expect(n, _p(flat), _p(s), s.size, _p(c), _p(terms), _p(total))
         return terms, complex(total[0])
 
+    def dm_partial_trace(self, n, rho, qubits):
+        """rho (N, N) -> the reduced (M, M), qubits read as the reference reads them."""
+        flat = np.ascontiguousarray(np.asarray(rho, dtype=np.complex128).T).reshape(-1)
+        q = np.ascontiguousarray(list(qubits), dtype=np.int64)
+        m = n - q.size
+        out = np.empty((1 << m) * (1 << m), dtype=np.complex128)
+        self._chk_dm(self.L.kto_dm_partial_trace(n, _p(flat), _p(q), q.size, _p(out)))
+        return out.reshape(1 << m, 1 << m).T.copy()
+
+    def dm_tensor_product(self, nl, left, nr, right):
+        l = np.ascontiguousarray(np.asarray(left, dtype=np.complex128).T).reshape(-1)
+        r = np.ascontiguousarray(np.asarray(right, dtype=np.complex128).T).reshape(-1)
+        D = 1 << (nl + nr)
+        out = np.empty(D * D, dtype=np.complex128)
+        self._chk_dm(self.L.kto_dm_tensor_product(nl, _p(l), nr, _p(r), _p(out)))
+        return out.reshape(D, D).T.copy()
+
+    def dm_trace_of_square(self, n, rho):
+        flat = np.ascontiguousarray(np.asarray(rho, dtype=np.complex128).T).reshape(-1)
+        out = np.empty(2, dtype=np.float64)
+        self._chk_dm(self.L.kto_dm_trace_of_square(n, _p(flat), _p(out)))
+        return complex(out[0], out[1])
+
+    @staticmethod
+    def _chk_dm(rc):
+        if rc != 0:
+            raise ValueError("oracle rejected the density-matrix operation")
+
     def gate_matrix(self, gate_rec, params=None):
         g = np.ascontiguousarray(gate_rec, dtype=GATE_DTYPE).reshape(1)
         p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
@@ -190,6 +224,12 @@ class Ref:
         L.ref_sv_free.argtypes = [P]
         L.ref_sv_time.argtypes = [P, P, I64, P, C.POINTER(C.c_double)]
         L.ref_sv_time.restype = I32
+        L.ref_dm_partial_trace.argtypes = [I32, P, P, I32, P]
+        L.ref_dm_partial_trace.restype = I32
+        L.ref_dm_tensor_product.argtypes = [I32, P, I32, P, P]
+        L.ref_dm_tensor_product.restype = I32
+        L.ref_dm_trace_of_square.argtypes = [I32, P, P]
+        L.ref_dm_trace_of_square.restype = I32
         self.L = L
 
     def time_sv(self, n, gates, params=None):
@@ -244,6 +284,32 @@ class Ref:
         self._chk(self.L.ref_simulate_dm(n, _p(g), g.size, _p(p), _p(flat), seed))
         N = 1 << n
         return flat.reshape(N, N).T.copy()
+
+    def dm_partial_trace(self, n, rho, qubits):
+        """rho (N, N) -> the reduced (M, M), qubits read as the reference reads them."""
+        flat = np.ascontiguousarray(np.asarray(rho, dtype=np.complex128).T).reshape(-1)
+        q = np.ascontiguousarray(list(qubits), dtype=np.int64)
+        m = n - q.size
+        out = np.empty((1 << m) * (1 << m), dtype=np.complex128)
+        self._chk_dm(self.L.ref_dm_partial_trace(n, _p(flat), _p(q), q.size, _p(out)))
+        return out.reshape(1 << m, 1 << m).T.copy()
+
+    def dm_tensor_product(self, nl, left, nr, right):
+        l = np.ascontiguousarray(np.asarray(left, dtype=np.complex128).T).reshape(-1)
+        r = np.ascontiguousarray(np.asarray(right, dtype=np.complex128).T).reshape(-1)
+        D = 1 << (nl + nr)
+        out = np.empty(D * D, dtype=np.complex128)
+        self._chk_dm(self.L.ref_dm_tensor_product(nl, _p(l), nr, _p(r), _p(out)))
+        return out.reshape(D, D).T.copy()
+
+    def dm_trace_of_square(self, n, rho):
+        flat = np.ascontiguousarray(np.asarray(rho, dtype=np.complex128).T).reshape(-1)
+        out = np.empty(2, dtype=np.float64)
+        self._chk_dm(self.L.ref_dm_trace_of_square(n, _p(flat), _p(out)))
+        return complex(out[0], out[1])
+
+    def _chk_dm(self, rc):
+        self._chk(rc)
 
     def sv_to_dm(self, n, amps):
         a = np.ascontiguousarray(amps, dtype=np.complex128)

@@ -276,6 +276,51 @@ int32_t ref_simulate_dm(int32_t n, const kt_gate* gates, int64_t n_gates, const 
     });
 }
 
+// ket::partial_trace (density_matrix.cpp:231-278), column-major in and out.
+int32_t ref_dm_partial_trace(int32_t n, const double* rho, const int64_t* qubits, int32_t k, double* out)
+{
+    return guarded([&] {
+        const auto N = static_cast<Eigen::Index>(std::size_t {1} << n);
+        Eigen::MatrixXcd m(N, N);
+        std::memcpy(m.data(), rho, static_cast<std::size_t>(N * N) * sizeof(std::complex<double>));
+        const auto dm = ket::DensityMatrix {std::move(m), ket::density_matrix_nocheck {}};
+        std::vector<std::size_t> idx(qubits, qubits + k);
+        const auto red = ket::partial_trace(dm, idx);
+        const auto M = static_cast<std::size_t>(red.n_states());
+        std::memcpy(out, red.matrix().data(), M * M * sizeof(std::complex<double>));
+    });
+}
+
+// ket::tensor_product (density_matrix.cpp:187-214)
+int32_t ref_dm_tensor_product(int32_t nl, const double* left, int32_t nr, const double* right, double* out)
+{
+    return guarded([&] {
+        const auto A = static_cast<Eigen::Index>(std::size_t {1} << nl);
+        const auto B = static_cast<Eigen::Index>(std::size_t {1} << nr);
+        Eigen::MatrixXcd l(A, A);
+        Eigen::MatrixXcd r(B, B);
+        std::memcpy(l.data(), left, static_cast<std::size_t>(A * A) * sizeof(std::complex<double>));
+        std::memcpy(r.data(), right, static_cast<std::size_t>(B * B) * sizeof(std::complex<double>));
+        const auto t = ket::tensor_product(ket::DensityMatrix {std::move(l), ket::density_matrix_nocheck {}},
+                                           ket::DensityMatrix {std::move(r), ket::density_matrix_nocheck {}});
+        const auto D = static_cast<std::size_t>(t.n_states());
+        std::memcpy(out, t.matrix().data(), D * D * sizeof(std::complex<double>));
+    });
+}
+
+// DensityMatrix::trace_of_square
+int32_t ref_dm_trace_of_square(int32_t n, const double* rho, double* out)
+{
+    return guarded([&] {
+        const auto N = static_cast<Eigen::Index>(std::size_t {1} << n);
+        Eigen::MatrixXcd m(N, N);
+        std::memcpy(m.data(), rho, static_cast<std::size_t>(N * N) * sizeof(std::complex<double>));
+        const auto v = ket::DensityMatrix {std::move(m), ket::density_matrix_nocheck {}}.trace_of_square();
+        out[0] = v.real();
+        out[1] = v.imag();
+    });
+}
+
 // statevector_to_density_matrix (density_matrix.cpp:170-185), column-major out.
 int32_t ref_sv_to_dm(int32_t n, const double* amps, double* rho)
 {

@@ -16,6 +16,7 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include <unistd.h>
@@ -342,6 +343,130 @@ int main(int argc, char** argv)
         std::printf("ioerr badterm none\n");
     } catch (const std::out_of_range&) {
         std::printf("ioerr badterm out_of_range\n");
+    }
+    // 7. compound gates (Toffoli family, CCU, SWAP, CSWAP, QFT / inverse QFT)
+    if (n >= 4) {
+        auto cg = ket::QuantumCircuit {n};
+        build(cg, n, 1, r);
+        const auto pick3 = [&]() {
+            std::size_t a = r.below(n), b = r.below(n), c = r.below(n);
+            while (b == a) b = r.below(n);
+            while (c == a || c == b) c = r.below(n);
+            return std::tuple<std::size_t, std::size_t, std::size_t> {a, b, c};
+        };
+        const auto [a0, b0, c0] = pick3();
+        cg.add_ccx_gate(a0, b0, c0);
+        const auto [a1, b1, c1] = pick3();
+        cg.add_ccy_gate({{a1, b1, c1}});
+        const auto [a2, b2, c2] = pick3();
+        cg.add_ccz_gate(a2, b2, c2);
+        const auto [a3, b3, c3] = pick3();
+        cg.add_ccu_gate(unitary(r), a3, b3, c3);
+        const auto [a4, b4, c4] = pick3();
+        cg.add_swap_gate(a4, b4);
+        cg.add_cswap_gate(c4, a4, b4);
+        std::vector<std::size_t> fourier;
+        for (std::size_t q = 0; q < n; q += 2) {
+            fourier.push_back(q);
+        }
+        std::vector<std::size_t> all(n);
+        for (std::size_t q = 0; q < n; ++q) {
+            all[q] = n - 1 - q;
+        }
+        cg.add_qft_gate(fourier);
+        cg.add_iqft_gate(all);
+        auto cgs = ket::Statevector {n};
+        ket::simulate(cg, cgs);
+        std::printf("cgelems %zu\n", cg.n_circuit_elements());
+        for (std::size_t i = 0; i < cgs.n_states(); ++i) {
+            std::printf("cgamp %zu %.17g %.17g\n", i, cgs[i].real(), cgs[i].imag());
+        }
+        const auto root = ket::matrix_square_root(unitary(r));
+        std::printf("sqrtu %.17g %.17g %.17g %.17g\n", root.elem00.real(), root.elem01.imag(), root.elem10.real(),
+                    root.elem11.imag());
+    }
+
+    // 8. density-matrix partial traces, tensor products and purity
+    {
+        const std::size_t nt = n < 6 ? n : 6;
+        auto tc = ket::QuantumCircuit {nt};
+        build(tc, nt, 2, r);
+        auto tdm = ket::DensityMatrix {std::string(nt, '0')};
+        ket::simulate(tc, tdm);
+        const auto print_dm = [](const char* tag, int id, const ket::DensityMatrix& d) {
+            const auto& mm = d.matrix();
+            std::printf("%s %d nq %zu\n", tag, id, d.n_qubits());
+            for (long rr = 0; rr < static_cast<long>(d.n_states()); ++rr) {
+                for (long cc = 0; cc < static_cast<long>(d.n_states()); ++cc) {
+                    std::printf("%s %d %ld %ld %.17g %.17g\n", tag, id, rr, cc, mm(rr, cc).real(), mm(rr, cc).imag());
+                }
+            }
+        };
+        std::vector<std::vector<std::size_t>> cases {{0}, {nt - 1}};
+        if (nt >= 3) {
+            cases.push_back({nt - 1, 0, 1});
+            cases.push_back({1, 1});
+            cases.push_back({2, 0});
+        }
+        std::vector<std::size_t> every(nt);
+        for (std::size_t q = 0; q < nt; ++q) {
+            every[q] = q;
+        }
+        cases.push_back(every);
+        for (std::size_t j = 0; j < cases.size(); ++j) {
+            print_dm("ptrace", static_cast<int>(j), ket::partial_trace(tdm, cases[j]));
+        }
+        try {
+            (void) ket::partial_trace(tdm, {nt});
+        } catch (const std::runtime_error& err) {
+            std::printf("pterr %d\n", static_cast<int>(std::string {err.what()}.find("out of bounds") != std::string::npos));
+        }
+        auto lc = ket::QuantumCircuit {2};
+        build(lc, 2, 2, r);
+        auto ldm = ket::DensityMatrix {"00"};
+        ket::simulate(lc, ldm);
+        const auto tp = ket::tensor_product(ldm, tdm);
+        print_dm("tensor", 0, ket::partial_trace(tp, {1}));
+        const auto tp3 = ket::tensor_product({ldm, ket::DensityMatrix {"1"}, ldm});
+        print_dm("tensor", 1, tp3);
+        const auto t2 = tdm.trace_of_square();
+        const auto mixed = ket::partial_trace(tdm, {0});
+        const auto m2 = mixed.trace_of_square();
+        std::printf("purity %.17g %.17g %d %.17g %.17g %d\n", t2.real(), t2.imag(), static_cast<int>(tdm.is_pure()),
+                    m2.real(), m2.imag(), static_cast<int>(mixed.is_pure()));
+    }
+    // 9. circuit transforms: U / CU gates lowered to primitive gates, circuits appended
+    if (n >= 2) {
+        auto uc = ket::QuantumCircuit {n};
+        build(uc, n, 1, r);
+        uc.add_u_gate(ket::h_gate(), 0);
+        uc.add_u_gate(ket::rx_gate(0.3), n - 1);
+        uc.add_u_gate(ket::p_gate(-1.1), 1);
+        uc.add_u_gate(unitary(r), 0);
+        uc.add_cu_gate(unitary(r), 0, n - 1);
+        uc.add_cu_gate(ket::sx_gate(), n - 1, 0);
+        auto prod = ket::rz_gate(2.0);
+        prod *= ket::ry_gate(0.4);
+        uc.add_u_gate(prod, 1);
+        uc.add_cu_gate(ket::x_gate() * std::complex<double> {0.0, 1.0}, 1, 0);
+        const auto tr = ket::transpile_to_primitive(uc);
+        int k = 0;
+        for (const auto& el : tr) {
+            const auto& gi = el.get_gate();
+            std::printf("tpgate %d %d %zu %zu %.17g\n", k++, static_cast<int>(gi.gate), gi.arg0, gi.arg1, gi.arg2);
+        }
+        const auto joined = ket::append_circuits(tr, uc);
+        std::printf("tpelems %zu %zu %zu\n", uc.n_circuit_elements(), tr.n_circuit_elements(), joined.n_circuit_elements());
+        auto js = ket::Statevector {n};
+        ket::simulate(joined, js);
+        for (std::size_t i = 0; i < js.n_states(); ++i) {
+            std::printf("tpamp %zu %.17g %.17g\n", i, js[i].real(), js[i].imag());
+        }
+        try {
+            (void) ket::append_circuits(tr, ket::QuantumCircuit {n + 1});
+        } catch (const std::runtime_error& err) {
+            std::printf("tperr %s\n", std::string {err.what()}.find("different numbers of qubits") != std::string::npos ? "qubits" : "other");
+        }
     }
     return 0;
 }

@@ -3,6 +3,8 @@ the reference has been compiled into oracle/_ref by `make -C oracle ref`):
 
     python tests/golden/make_golden.py
 
+    python tests/golden/make_golden.py dm_ops     # golden_dm_ops.npz only
+
 Writes
   * ref_kats.json   known-answer cases restated from the reference's own tests
                     (file:line cited per case), expected values as the tests
@@ -10,7 +12,9 @@ Writes
   * golden_ref.npz  outputs of the reference library itself (oracle/_ref) on
                     seeded small workloads: pair sequences, final amplitudes,
                     expectation values, sampled indices, M-gate outcomes and
-                    density matrices.
+                    density matrices;
+  * golden_dm_ops.npz partial traces, tensor products and Tr(rho^2) of the
+                    reference library on seeded random density matrices.
 The fixtures are committed; tests read them without needing the reference.
 """
 from __future__ import annotations
@@ -191,10 +195,50 @@ def golden_ref():
     return out
 
 
+def random_rho(n, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((1 << n, 1 << n)) + 1j * rng.standard_normal((1 << n, 1 << n))
+    rho = a @ a.conj().T
+    return rho / np.trace(rho)
+
+
+# traced-qubit lists per size: single qubits, several in either order, a
+# repeated index (read as the reference reads it) and every qubit
+DM_TRACE_CASES = {
+    3: [[0], [1], [2], [0, 2], [2, 0], [1, 1], [0, 1, 2]],
+    4: [[3], [0, 3], [3, 1, 0], [2, 2], [0, 1, 2, 3]],
+    5: [[2], [4, 0], [1, 3], [0, 2, 4], [3, 3, 1]],
+}
+
+
+def golden_dm_ops():
+    """Partial traces, tensor products and Tr(rho^2) of the reference library
+    (state/density_matrix.cpp:187-278) on seeded random density matrices."""
+    R = ref()
+    out = {}
+    for n, cases in DM_TRACE_CASES.items():
+        rho = random_rho(n, 100 + n)
+        out[f"dmop_{n}_rho"] = rho
+        out[f"dmop_{n}_tsq"] = np.array([R.dm_trace_of_square(n, rho)])
+        for j, qs in enumerate(cases):
+            out[f"dmop_{n}_pt_{j}_q"] = np.array(qs, dtype=np.int64)
+            out[f"dmop_{n}_pt_{j}_out"] = R.dm_partial_trace(n, rho, qs)
+    left, right = random_rho(2, 7), random_rho(3, 8)
+    out["dmop_tp_left"] = left
+    out["dmop_tp_right"] = right
+    out["dmop_tp_out"] = R.dm_tensor_product(2, left, 3, right)
+    return out
+
+
 def main():
-    (HERE / "ref_kats.json").write_text(json.dumps(kats(), indent=1))
-    np.savez_compressed(HERE / "golden_ref.npz", **golden_ref())
-    print("wrote", HERE / "ref_kats.json", HERE / "golden_ref.npz")
+    which = sys.argv[1:] or ["all"]
+    if "all" in which:
+        (HERE / "ref_kats.json").write_text(json.dumps(kats(), indent=1))
+        np.savez_compressed(HERE / "golden_ref.npz", **golden_ref())
+        print("wrote", HERE / "ref_kats.json", HERE / "golden_ref.npz")
+    if "all" in which or "dm_ops" in which:
+        np.savez_compressed(HERE / "golden_dm_ops.npz", **golden_dm_ops())
+        print("wrote", HERE / "golden_dm_ops.npz")
 
 
 if __name__ == "__main__":

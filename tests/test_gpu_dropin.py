@@ -25,10 +25,11 @@ def _run(exe, *args):
     out = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr
     rec = {"amp": {}, "mamp": {}, "cfamp": {}, "ioamp": {}, "npamp": {}, "rho": {}, "count": {}, "expect": None,
-           "cbits": None, "cfbits": None, "logbit": {}, "logamp": {}, "svtext": {}, "svload": {}, "ioerr": {}}
+           "cbits": None, "cfbits": None, "logbit": {}, "logamp": {}, "svtext": {}, "svload": {}, "ioerr": {},
+           "cgamp": {}, "ptrace": {}, "tensor": {}, "nq": {}, "tpamp": {}}
     for line in out.stdout.splitlines():
         f = line.split()
-        if f[0] in ("amp", "mamp", "cfamp", "ioamp", "npamp"):
+        if f[0] in ("amp", "mamp", "cfamp", "ioamp", "npamp", "cgamp", "tpamp"):
             rec[f[0]][int(f[1])] = complex(float(f[2]), float(f[3]))
         elif f[0] == "cfbits":
             rec["cfbits"] = tuple(int(x) for x in f[1:])
@@ -52,6 +53,22 @@ def _run(exe, *args):
             rec[f[0]] = (int(f[1]), complex(float(f[2]), float(f[3])))
         elif f[0] in ("pauliopfile",):
             rec[f[0]] = complex(float(f[1]), float(f[2]))
+        elif f[0] in ("ptrace", "tensor") and f[2] == "nq":
+            rec["nq"][(f[0], int(f[1]))] = int(f[3])
+        elif f[0] in ("ptrace", "tensor"):
+            rec[f[0]][(int(f[1]), int(f[2]), int(f[3]))] = complex(float(f[4]), float(f[5]))
+        elif f[0] == "tpgate":
+            rec.setdefault("tpgate", []).append((int(f[2]), int(f[3]), int(f[4]), float(f[5])))
+        elif f[0] == "tpelems":
+            rec[f[0]] = tuple(int(x) for x in f[1:])
+        elif f[0] == "tperr":
+            rec[f[0]] = f[1]
+        elif f[0] in ("cgelems", "pterr"):
+            rec[f[0]] = int(f[1])
+        elif f[0] == "sqrtu":
+            rec[f[0]] = np.array([float(x) for x in f[1:]])
+        elif f[0] == "purity":
+            rec[f[0]] = (complex(float(f[1]), float(f[2])), int(f[3]), complex(float(f[4]), float(f[5])), int(f[6]))
         elif f[0] == "ioerr":
             rec["ioerr"][f[1]] = f[2]
         elif f[0] == "cbit0":
@@ -106,3 +123,31 @@ def test_dropin_same_results(engine, n, layers, seed):
     assert abs(ref["pauliop"][1] - our["pauliop"][1]) < 1e-12
     assert abs(our["pauliopfile"] - our["pauliop"][1]) == 0.0
     assert ref["ioerr"] == our["ioerr"] == {"load": "1", "numpy": "1", "pauli": "1", "badterm": "out_of_range"}
+    # compound gates
+    if n >= 4:
+        assert ref["cgelems"] == our["cgelems"]
+        ga = np.array([ref["cgamp"][i] for i in sorted(ref["cgamp"])])
+        gb = np.array([our["cgamp"][i] for i in sorted(our["cgamp"])])
+        assert ga.size == 1 << n and np.abs(ga - gb).max() < 1e-12
+        assert np.abs(ref["sqrtu"] - our["sqrtu"]).max() < 1e-14
+    # density-matrix partial traces, tensor products, purity
+    assert ref["nq"] == our["nq"]
+    for key in ("ptrace", "tensor"):
+        assert sorted(ref[key]) == sorted(our[key]) and len(ref[key]) > 0
+        pa = np.array([ref[key][k] for k in sorted(ref[key])])
+        pb = np.array([our[key][k] for k in sorted(our[key])])
+        assert np.abs(pa - pb).max() < 1e-12
+    assert ref["pterr"] == our["pterr"] == 1
+    rp, op = ref["purity"], our["purity"]
+    assert abs(rp[0] - op[0]) < 1e-12 and abs(rp[2] - op[2]) < 1e-12
+    assert rp[1] == op[1] and rp[3] == op[3]
+    # circuit transforms
+    ta, tb = ref["tpgate"], our["tpgate"]
+    assert len(ta) == len(tb) == our["tpelems"][1]
+    for x, y in zip(ta, tb):
+        assert x[:3] == y[:3] and abs(x[3] - y[3]) < 1e-12
+    assert ref["tpelems"] == our["tpelems"]
+    pa = np.array([ref["tpamp"][i] for i in sorted(ref["tpamp"])])
+    pb = np.array([our["tpamp"][i] for i in sorted(our["tpamp"])])
+    assert pa.size == 1 << n and np.abs(pa - pb).max() < 1e-12
+    assert ref["tperr"] == our["tperr"] == "qubits"

@@ -200,3 +200,53 @@ def test_live_reference_dm(port, ref):
     rho0 = np.zeros((8, 8), dtype=np.complex128)
     rho0[0, 0] = 1
     np.testing.assert_allclose(port.simulate_dm(n, rho0, g), ref.simulate_dm(n, rho0, g), atol=1e-15)
+
+
+# --- density-matrix operations -----------------------------------------------------
+
+def _dm_golden():
+    from conftest import GOLDEN
+    return dict(np.load(GOLDEN / "golden_dm_ops.npz"))
+
+
+def test_golden_partial_trace_tensor_purity(port):
+    g = _dm_golden()
+    sizes = sorted({int(k.split("_")[1]) for k in g if k.startswith("dmop_") and k.endswith("_rho")})
+    assert sizes == [3, 4, 5]
+    for n in sizes:
+        rho = g[f"dmop_{n}_rho"]
+        j = 0
+        while f"dmop_{n}_pt_{j}_q" in g:
+            got = port.dm_partial_trace(n, rho, g[f"dmop_{n}_pt_{j}_q"].tolist())
+            assert np.array_equal(got, g[f"dmop_{n}_pt_{j}_out"]), (n, j)
+            j += 1
+        assert abs(port.dm_trace_of_square(n, rho) - g[f"dmop_{n}_tsq"][0]) < 1e-15
+    got = port.dm_tensor_product(2, g["dmop_tp_left"], 3, g["dmop_tp_right"])
+    assert np.array_equal(got, g["dmop_tp_out"])
+
+
+def test_kat_partial_trace_of_product_states(port):
+    # test/source/state/density_matrix_test.cpp:270-410: tracing one factor
+    # of a tensor product out leaves the other factor
+    rng = np.random.default_rng(3)
+    states = []
+    for _ in range(3):
+        v = rng.standard_normal(2) + 1j * rng.standard_normal(2)
+        v /= np.linalg.norm(v)
+        states.append(np.outer(v, v.conj()))
+    t01 = port.dm_tensor_product(1, states[0], 1, states[1])
+    t012 = port.dm_tensor_product(2, t01, 1, states[2])
+    np.testing.assert_allclose(port.dm_partial_trace(3, t012, [0]), port.dm_tensor_product(1, states[1], 1, states[2]), atol=1e-15)
+    np.testing.assert_allclose(port.dm_partial_trace(3, t012, [1]), port.dm_tensor_product(1, states[0], 1, states[2]), atol=1e-15)
+    np.testing.assert_allclose(port.dm_partial_trace(3, t012, [2]), t01, atol=1e-15)
+    for qs, keep in (([0, 1], 2), ([1, 0], 2), ([0, 2], 1), ([2, 0], 1), ([1, 2], 0), ([2, 1], 0)):
+        np.testing.assert_allclose(port.dm_partial_trace(3, t012, qs), states[keep], atol=1e-15)
+    assert abs(port.dm_trace_of_square(3, t012) - 1.0) < 1e-14
+
+
+def test_live_reference_dm_ops(port, ref):
+    from tests.golden.make_golden import random_rho
+    for n in (1, 2, 6):
+        rho = random_rho(n, 40 + n)
+        for qs in ([0], [n - 1], list(range(n))[::-1], [0] * (n // 2 + 1) if n > 1 else [0]):
+            assert np.array_equal(port.dm_partial_trace(n, rho, qs), ref.dm_partial_trace(n, rho, qs))
