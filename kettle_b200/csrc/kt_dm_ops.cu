@@ -11,9 +11,10 @@
 // r, c = r', c' with a 0 inserted at bit q.  Over k traced qubits the result
 // is a sum of 2^k diagonal blocks, grouped as that sequence of pairwise sums:
 // the innermost pairs differ in the first qubit traced, the outermost in the
-// last.  One thread per output element adds its 2^k leaves in that same
-// tree order (a pairwise stack indexed by the leaf counter), so the sums
-// round like the reference's sequence of reduced matrices.  Each leaf is one
+// last.  Each output element's 2^k leaves are added in that same tree order
+// (pairwise stacks over aligned subtrees, then the subtrees pairwise), so the
+// sums round like the reference's sequence of reduced matrices.  When few
+// outputs remain, up to 32 warps share one warp of outputs, one subtree each.  Each leaf is one
 // gathered element; rows and columns share the traced bits, so a launch reads
 // 4^m 2^k elements and writes 4^m (m = n - k).
 //
@@ -38,6 +39,7 @@ namespace
 {
 
 constexpr int DM_THREADS = 256;
+constexpr int DM_PT_MAX_THREADS = 1024;
 constexpr int DM_MAX_QUBITS = 17;
 
 // bit positions handed to the partial-trace kernel
@@ -62,12 +64,45 @@ __device__ __forceinline__ uint32_t spread8(uint32_t x, const int8_t* pos, int b
     return v;
 }
 
+// Sum of the leaves lo .. lo + count - 1 (count a power of 2, lo a multiple
+// of it): one subtree of the reference's grouping, by a pairwise stack.
 template <typename C>
-__global__ void __launch_bounds__(DM_THREADS)
-    k_partial_trace(const C* __restrict__ rho, int n, TraceMap map, C* __restrict__ out)
+__device__ __forceinline__ double2 trace_subtree(const C* __restrict__ rho, int n, uint64_t base, uint32_t lo,
+                                                 uint32_t count, int levels, const uint32_t (*tr_tab)[256])
+{
+    double2 stack[DM_MAX_QUBITS + 1];
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t t = lo + i;
+        const uint64_t off = tr_tab[0][t & 255U] | tr_tab[1][(t >> 8) & 255U] | tr_tab[2][t >> 16];
+        double2 v = to_d2(rho[base + off + (off << n)]);
+        int j = 0;
+        while (((i >> j) & 1U) != 0U) {
+            v.x = stack[j].x + v.x;
+            v.y = stack[j].y + v.y;
+            ++j;
+        }
+        if (j < levels) {
+            stack[j] = v;
+        } else {
+            acc = v;
+        }
+    }
+    return acc;
+}
+
+// Thread layout: lanes = 32 consecutive output elements; a block holds
+// `out_warps` such warps of outputs times G = 2^g leaf groups (warp w: group
+// w % G, output warp w / G).  Group j sums the leaves j 2^(k-g) .. (j+1) 2^(k-g) - 1
+// (the subtrees under the top g tree levels), and the G partials are then
+// added pairwise in tree order, so the grouping stays the reference's.
+template <typename C>
+__global__ void __launch_bounds__(DM_PT_MAX_THREADS)
+    k_partial_trace(const C* __restrict__ rho, int n, TraceMap map, int g, C* __restrict__ out)
 {
     __shared__ uint32_t keep_tab[2][256];
     __shared__ uint32_t tr_tab[3][256];
+    __shared__ double2 part[DM_PT_MAX_THREADS];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         keep_tab[0][i] = spread8(static_cast<uint32_t>(i), map.keep, 0, map.m);
         keep_tab[1][i] = spread8(static_cast<uint32_t>(i), map.keep, 8, map.m);
@@ -79,34 +114,50 @@ __global__ void __launch_bounds__(DM_THREADS)
 
     const int m = map.m;
     const int k = map.k;
+    const int G = 1 << g;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int group = warp & (G - 1);
+    const int out_warp = warp >> g;
+    const int out_warps = (blockDim.x >> 5) >> g;
     const uint64_t n_out = uint64_t {1} << (2 * m);
     const uint64_t M = uint64_t {1} << m;
-    const uint32_t n_leaves = 1U << k;
-    for (uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; o < n_out; o += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t rr = static_cast<uint32_t>(o & (M - 1));
-        const uint32_t cc = static_cast<uint32_t>(o >> m);
-        const uint64_t row = keep_tab[0][rr & 255U] | keep_tab[1][rr >> 8];
-        const uint64_t col = keep_tab[0][cc & 255U] | keep_tab[1][cc >> 8];
-        const uint64_t base = row + (col << n);
-        // pairwise stack: stack[j] holds the left sibling at tree level j
-        double2 stack[DM_MAX_QUBITS + 1];
-        double2 acc = make_double2(0.0, 0.0);
-        for (uint32_t t = 0; t < n_leaves; ++t) {
-            const uint64_t off = tr_tab[0][t & 255U] | tr_tab[1][(t >> 8) & 255U] | tr_tab[2][t >> 16];
-            double2 v = to_d2(rho[base + off + (off << n)]);
-            int j = 0;
-            while (((t >> j) & 1U) != 0U) {
-                v.x = stack[j].x + v.x;
-                v.y = stack[j].y + v.y;
-                ++j;
-            }
-            if (j < k) {
-                stack[j] = v;
-            } else {
-                acc = v;
-            }
+    const uint32_t per_group = 1U << (k - g);
+    const uint64_t chunk = 32ULL * out_warps;
+    for (uint64_t o0 = (uint64_t)blockIdx.x * chunk; o0 < n_out; o0 += (uint64_t)gridDim.x * chunk) {
+        const uint64_t o = o0 + (uint64_t)out_warp * 32 + lane;
+        double2 v = make_double2(0.0, 0.0);
+        if (o < n_out) {
+            const uint32_t rr = static_cast<uint32_t>(o & (M - 1));
+            const uint32_t cc = static_cast<uint32_t>(o >> m);
+            const uint64_t row = keep_tab[0][rr & 255U] | keep_tab[1][rr >> 8];
+            const uint64_t col = keep_tab[0][cc & 255U] | keep_tab[1][cc >> 8];
+            v = trace_subtree(rho, n, row + (col << n), static_cast<uint32_t>(group) * per_group, per_group, k - g,
+                              tr_tab);
         }
-        out[o] = from_d2<C>(acc);
+        if (G == 1) {
+            if (o < n_out) {
+                out[o] = from_d2<C>(v);
+            }
+            continue;
+        }
+        part[threadIdx.x] = v;
+        __syncthreads();
+        if (group == 0 && o < n_out) {
+            // partial of group j sits at warp (out_warp * G + j)
+            double2 vals[32];
+            for (int j = 0; j < G; ++j) {
+                vals[j] = part[((out_warp << g) + j) * 32 + lane];
+            }
+            for (int step = 1; step < G; step <<= 1) {
+                for (int j = 0; j < G; j += 2 * step) {
+                    vals[j].x = vals[j].x + vals[j + step].x;
+                    vals[j].y = vals[j].y + vals[j + step].y;
+                }
+            }
+            out[o] = from_d2<C>(vals[0]);
+        }
+        __syncthreads();
     }
 }
 
@@ -218,14 +269,27 @@ int32_t dm_partial_trace(const State& src, int n, const int32_t* traced, int k, 
             map.keep[jm++] = static_cast<int8_t>(q);
         }
     }
+    // leaf groups per output: enough threads to fill the GPU when few outputs
+    // remain (G = 2^g <= 32, at most 2^k), 256-thread blocks up to G = 8
     const uint64_t n_out = uint64_t {1} << (2 * map.m);
-    const int blocks = dm_blocks(n_out);
+    const uint64_t want_threads = static_cast<uint64_t>(sm_count()) * 2048;
+    int g = 0;
+    while (g < 5 && g < k && n_out * (uint64_t {1} << g) < want_threads) {
+        ++g;
+    }
+    const int G = 1 << g;
+    const int out_warps = G <= 8 ? 8 / G : 1;
+    const int threads = 32 * out_warps * G;
+    const uint64_t chunk = 32ULL * out_warps;
+    const uint64_t want_blocks = (n_out + chunk - 1) / chunk;
+    const int blocks = static_cast<int>(std::max<uint64_t>(
+        1, std::min<uint64_t>(want_blocks, static_cast<uint64_t>(sm_count()) * (2048 / threads))));
     if (src.dtype == KT_C128) {
-        k_partial_trace<double2><<<blocks, DM_THREADS, 0, dst.stream>>>(static_cast<const double2*>(src.amps), n, map,
-                                                                        static_cast<double2*>(dst.amps));
+        k_partial_trace<double2><<<blocks, threads, 0, dst.stream>>>(static_cast<const double2*>(src.amps), n, map, g,
+                                                                     static_cast<double2*>(dst.amps));
     } else {
-        k_partial_trace<float2><<<blocks, DM_THREADS, 0, dst.stream>>>(static_cast<const float2*>(src.amps), n, map,
-                                                                       static_cast<float2*>(dst.amps));
+        k_partial_trace<float2><<<blocks, threads, 0, dst.stream>>>(static_cast<const float2*>(src.amps), n, map, g,
+                                                                    static_cast<float2*>(dst.amps));
     }
     KT_CHECK_LAUNCH("k_partial_trace");
     return KT_OK;
