@@ -60,6 +60,7 @@ enum OpKind : uint8_t
     OP_SWAP = 3,   // X / CX
     OP_DIAG = 4,   // diag(m00, m11)
     OP_DIAG1 = 5,  // diag(1, m11)
+    OP_RXL = 6,    // [[c, i s], [i s, c]] with c, s real (RX, CRX): m[0] = c, m[3] = s
 };
 
 constexpr uint8_t NO_SLOT = 0xFF;
@@ -256,6 +257,35 @@ struct GenRF
     }
 };
 
+// [[c, i s], [i s, c]]: 8 FP64 operations per pair instead of the general 16
+template <typename T, int RB>
+struct RxF
+{
+    using C = typename CxT<T>::type;
+    C (&v)[1 << RB];
+    T c, s;
+    int crt = -1;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (lower_of_pair<S, CS>(i, crt)) {
+                const int j = i | (1 << S);
+                const C a = v[i];
+                const C b = v[j];
+                C x, y;
+                x.x = fma(-s, b.y, c * a.x);
+                x.y = fma(s, b.x, c * a.y);
+                y.x = fma(-s, a.y, c * b.x);
+                y.y = fma(s, a.x, c * b.y);
+                v[i] = x;
+                v[j] = y;
+            }
+        }
+    }
+};
+
 template <typename T, int RB, bool PURE>
 struct AntiF
 {
@@ -374,6 +404,11 @@ __device__ __forceinline__ void apply_op(typename CxT<T>::type (&v)[1 << RB], co
         }
         case OP_GENR: {
             GenRF<T, RB> f {v, op.m[0], op.m[2], op.m[4], op.m[6]};
+            dispatch_sc<RB>(ts, cs, f);
+            return;
+        }
+        case OP_RXL: {
+            RxF<T, RB> f {v, op.m[0], op.m[3]};
             dispatch_sc<RB>(ts, cs, f);
             return;
         }
@@ -524,6 +559,11 @@ __device__ __forceinline__ void apply_u(typename CxT<T>::type (&v)[1 << RB], con
         }
         case OP_GENR: {
             GenRF<T, RB> f {v, op.m[0], op.m[2], op.m[4], op.m[6]};
+            dispatch_sc<RB>(ts, cs, f);
+            return;
+        }
+        case OP_RXL: {
+            RxF<T, RB> f {v, op.m[0], op.m[3]};
             dispatch_sc<RB>(ts, cs, f);
             return;
         }
@@ -1282,8 +1322,13 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
                 op.tslot = static_cast<uint8_t>(reg_slot(loc[x.target]));
                 if (x.kind == KIND_ANTI) {
                     op.kind = is_pure_x(x) ? OP_SWAP : OP_ANTI;
+                } else if (real) {
+                    op.kind = OP_GENR;
+                } else if (x.m[1] == 0.0 && x.m[7] == 0.0 && x.m[0] == x.m[6] && x.m[2] == 0.0 && x.m[4] == 0.0 &&
+                           x.m[3] == x.m[5]) {
+                    op.kind = OP_RXL;
                 } else {
-                    op.kind = real ? OP_GENR : OP_GEN;
+                    op.kind = OP_GEN;
                 }
             }
             for (int e = 0; e < 8; ++e) {
