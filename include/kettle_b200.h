@@ -148,9 +148,28 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               shared-memory transpose (1) or run as ops (0)
  *   c64_renormalize    0 or 1   complex64 applies rescale every fused block to the
  *                               norm the state had when the apply began (1)
+ *   fused_jit          0, 1, 2  complex128 fused blocks as kernels compiled at run
+ *                               time (NVRTC, cached per block structure: gate bodies
+ *                               as straight-line code, every slot and mask a
+ *                               constant): 0 never, 1 always, 2 (default) from the
+ *                               second apply of the same circuit structure on states
+ *                               of >= jit_min_qubits qubits; without NVRTC, or if a
+ *                               compile fails, the precompiled kernels run (kt_jit_stats)
+ *   jit_min_qubits     1..64    (26) the state size from which fused_jit = 2 compiles
+ *   fused_reg_bits     3 or 4   complex128 amplitudes per thread in fused blocks
+ *                               (2^4; or 2^3 with twice the warps: 12-qubit tiles of
+ *                               512 threads, 2 CTAs per SM, or 11-qubit tiles of 256
+ *                               threads, 3 CTAs per SM, by fused_tile_bits)
  * Unknown names return KT_ERR_INVALID. */
 int32_t kt_tuning_set(const char* name, int64_t value);
 int32_t kt_tuning_get(const char* name, int64_t* value);
+/* Run-time compiled block kernels so far, fused-block launches through them,
+ * and 1 if run-time compilation was unavailable or failed (new). */
+int32_t kt_jit_stats(int64_t* kernels_compiled, int64_t* block_launches, int32_t* failed);
+/* Host-only: plan a complex128 apply of n_qubits and compile its block kernels
+ * with NVRTC without loading them (no GPU needed); n_kernels = blocks compiled. */
+int32_t kt_jit_compile_only(int32_t n_qubits, const kt_gate* gates, int64_t n_gates, const double* params,
+                            int64_t n_params, int64_t* n_kernels);
 
 /* ---- statevector handle --------------------------------------------------
  * A statevector of n qubits lives on the current CUDA device as 2^n amplitudes,

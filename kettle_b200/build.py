@@ -54,10 +54,34 @@ def _stale(out: pathlib.Path, deps: list[pathlib.Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
+# headers the run-time compiled block kernels include (kt_jit.cpp embeds their text)
+JIT_HEADERS = ("kt_complex.cuh", "kt_fused_dev.cuh")
+
+
+def write_jit_headers() -> pathlib.Path:
+    """BUILD/kt_jit_headers.inc: the text of JIT_HEADERS as C++ raw strings."""
+    out = BUILD / "kt_jit_headers.inc"
+    parts = ["// generated by kettle_b200/build.py from kettle_b200/csrc: do not edit",
+             f"#define KT_JIT_N_HEADERS {len(JIT_HEADERS)}",
+             "static const char* const KT_JIT_HEADER_NAMES[] = {" + ", ".join(f'"{h}"' for h in JIT_HEADERS) + "};",
+             "static const char* const KT_JIT_HEADER_TEXT[] = {"]
+    for h in JIT_HEADERS:
+        text = (CSRC / h).read_text()
+        if ")KTJIT\"" in text:
+            raise RuntimeError(f"{h} contains the raw-string delimiter")
+        parts.append('R"KTJIT(' + text + ')KTJIT",')
+    parts.append("};")
+    content = "\n".join(parts) + "\n"
+    if not out.exists() or out.read_text() != content:
+        out.write_text(content)
+    return out
+
+
 def build_library(verbose: bool = False, force: bool = False) -> pathlib.Path:
     """Compile every .cu/.cpp under csrc/ for sm_100a and link libkettle_b200.so."""
     BUILD.mkdir(exist_ok=True)
     LIB.mkdir(exist_ok=True)
+    write_jit_headers()
     headers = sorted(CSRC.glob("*.cuh")) + [INCLUDE / "kettle_b200.h"]
     sources = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
     jobs = []
@@ -66,7 +90,7 @@ def build_library(verbose: bool = False, force: bool = False) -> pathlib.Path:
         obj = BUILD / (src.name + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", f"-I{BUILD}", "-c", str(src), "-o", str(obj)]
             jobs.append(cmd)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         for out in ex.map(_run, jobs):
@@ -74,7 +98,7 @@ def build_library(verbose: bool = False, force: bool = False) -> pathlib.Path:
                 print(out)
     lib = LIB / LIB_NAME
     if force or jobs or _stale(lib, objs):
-        _run([nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(lib), *map(str, objs)])
+        _run([nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(lib), *map(str, objs), "-ldl"])
     return lib
 
 

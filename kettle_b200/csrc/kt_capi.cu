@@ -180,6 +180,30 @@ int32_t kt_tuning_get(const char* name, int64_t* value)
     return KT_OK;
 }
 
+int32_t kt_jit_compile_only(int32_t n_qubits, const kt_gate* gates, int64_t n_gates, const double* params,
+                            int64_t n_params, int64_t* n_kernels)
+{
+    return guard([&]() -> int32_t {
+        if (n_kernels == nullptr || n_gates < 0 || (n_gates > 0 && gates == nullptr)) {
+            return invalid("bad arguments");
+        }
+        std::vector<kt::LGate> lg;
+        if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, n_qubits, lg); rc != KT_OK) {
+            return rc;
+        }
+        return kt::jit_compile_only(n_qubits, lg, n_kernels);
+    });
+}
+
+int32_t kt_jit_stats(int64_t* kernels_compiled, int64_t* block_launches, int32_t* failed)
+{
+    if (kernels_compiled == nullptr || block_launches == nullptr || failed == nullptr) {
+        return invalid("null pointer");
+    }
+    kt::jit_stats(kernels_compiled, block_launches, failed);
+    return KT_OK;
+}
+
 // ---- statevector --------------------------------------------------------------
 
 int32_t kt_sv_create(int32_t n_qubits, int32_t dtype, kt_sv* out)

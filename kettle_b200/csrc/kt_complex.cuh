@@ -2,12 +2,34 @@
 // index bit helpers used by every kernel.
 #pragma once
 
+#ifdef __CUDACC_RTC__
+// compiled at run time (generated block kernels): no host headers
+typedef signed char int8_t;
+typedef unsigned char uint8_t;
+typedef short int16_t;
+typedef unsigned short uint16_t;
+typedef int int32_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+#else
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#endif
 
 namespace kt
 {
+
+// Generators of the parameterised gates: RX/RY/RZ (and CRX/CRY/CRZ) are
+// exp(-i theta G / 2) with G = X, Y, Z; P (and CP) is diag(1, e^(i theta)).
+enum Generator : int32_t
+{
+    GEN_X = 0,
+    GEN_Y = 1,
+    GEN_Z = 2,
+    GEN_P = 3,
+};
 
 template <typename T>
 struct CxT;

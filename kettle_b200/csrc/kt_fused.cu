@@ -26,7 +26,12 @@
 //    target that is a thread bit.  The kernel does no per-amplitude index math.
 //  * Loads and stores use a layout whose lane bits are the L lowest qubits:
 //    each warp instruction touches whole 128-byte lines.
+#include <cstdio>
+#include <mutex>
+#include <string>
 #include <type_traits>
+#include <unordered_map>
+#include <unordered_set>
 
 #include "kt_fused.cuh"
 
@@ -39,17 +44,39 @@ namespace
 // SHAPE: 2 = 256 threads, 2 CTAs per SM (<= 128 registers); 1 = 256 threads,
 // 1 CTA per SM (the compiler's natural allocation); 0 = 512 threads, 1 CTA
 // per SM (<= 128 registers: the tiles of 13 complex128 / 14 complex64 qubits).
-#define KT_FUSED_BOUNDS(SHAPE) __launch_bounds__((SHAPE) == 0 ? 512 : 256, (SHAPE) == 0 ? 1 : (SHAPE))
+// Complex128 with 8 amplitudes per thread (fused_reg_bits = 3): 3 = 512
+// threads, 2 CTAs per SM (12-qubit tiles, <= 64 registers); 4 = 256 threads,
+// 3 CTAs per SM (11-qubit tiles, <= 80 registers).
+#define KT_FUSED_BOUNDS(SHAPE)                                                                 \
+    __launch_bounds__(((SHAPE) == 0 || (SHAPE) == 3) ? 512 : 256,                               \
+                      (SHAPE) == 0 ? 1 : ((SHAPE) == 3 ? 2 : ((SHAPE) == 4 ? 3 : (SHAPE))))
+
+// register bits (amplitudes per thread = 2^RB) of a launch shape
+template <typename T, int SHAPE>
+struct ShapeCfg
+{
+    using type = Cfg<T>;
+};
+template <typename T>
+struct ShapeCfg<T, 3>
+{
+    using type = Cfg3;
+};
+template <typename T>
+struct ShapeCfg<T, 4>
+{
+    using type = Cfg3;
+};
 
 inline int fused_ctas(int shape)
 {
-    return shape == 2 ? 2 : 1;
+    return shape == 2 ? 2 : (shape == 3 ? 2 : (shape == 4 ? 3 : 1));
 }
 
 // dynamic shared memory a launch shape may use: the tile plus MAX_OPS_PER_BLOCK op records
 inline int fused_smem_limit(int shape)
 {
-    return shape == 0 ? 160 * 1024 : 96 * 1024;
+    return shape == 0 ? 160 * 1024 : (shape == 4 ? 72 * 1024 : 96 * 1024);
 }
 
 template <typename T, int MINB>
@@ -58,7 +85,7 @@ __global__ void KT_FUSED_BOUNDS(MINB) k_fused(typename CxT<T>::type* __restrict_
                                                   uint64_t n_tiles)
 {
     using C = typename CxT<T>::type;
-    constexpr int RB = Cfg<T>::RB;
+    constexpr int RB = ShapeCfg<T, MINB>::type::RB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ FBlock bk;
     __shared__ FPhase sph[MAX_PHASES_PER_BLOCK];
@@ -224,16 +251,265 @@ int32_t run_fused_norm(State& s, const Plan<T>& plan, const FBlock* d_blk, const
     return KT_OK;
 }
 
+// Block formation and planning of a forward apply (n >= Cfg<T>::RB + 5):
+// tile size from fused_tile_bits, 8 amplitudes per thread for complex128
+// when fused_reg_bits is 3 (12- or 11-qubit tiles).  A block whose phases
+// overflow the kernel's table is re-formed with half the ops per block.
+template <typename T>
+int32_t fused_plan(int n, const std::vector<LGate>& gates, Plan<T>& plan, int* K_out, bool* rb3_out)
+{
+    constexpr int RB = Cfg<T>::RB;
+    constexpr int L = Cfg<T>::L;
+    const bool rb3 = std::is_same<T, double>::value && tuning().fused_reg_bits == 3 && n >= 12;
+    int K = 0;
+    if (rb3) {
+        K = std::max(11, std::min(12, tuning().fused_tile_bits));
+    } else {
+        K = std::min(n, std::min(RB + TBMAX, tuning().fused_tile_bits + (RB - 4)));
+    }
+    size_t max_ops = static_cast<size_t>(std::min(MAX_OPS_PER_BLOCK, tuning().fused_max_ops));
+    for (;;) {
+        plan = Plan<T> {};
+        const auto blocks = form_blocks(gates, n, K, L, max_ops);
+        for (const auto& b : blocks) {
+            if (rb3) {
+                plan_block<T, Cfg3>(b, gates, n, plan);
+            } else {
+                plan_block<T>(b, gates, n, plan);
+            }
+        }
+        bool fits = true;
+        for (const auto& fb : plan.blocks) {
+            if (fb.phase_end - fb.phase_begin > MAX_PHASES_PER_BLOCK) {
+                fits = false;
+            }
+        }
+        if (fits) {
+            break;
+        }
+        if (max_ops <= 8) {
+            set_error(KT_ERR_INVALID, "fused block planner produced too many phases");
+            return KT_ERR_INVALID;
+        }
+        max_ops /= 2;
+    }
+    *K_out = K;
+    *rb3_out = rb3;
+    return KT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Run-time compiled block kernels (fused_jit = 1, complex128).  A block's
+// kernel is the k_fused tile loop with the block's gate bodies written out as
+// straight-line code: the target and control register slots, the thread and
+// tile masks are literals, so there is no op dispatch, the control predicates
+// fold away (a controlled gate computes only its active pairs) and the
+// register allocator sees the whole block.  Matrices are still read from the
+// op records, so one compiled kernel serves every angle.  Kernels are cached
+// by their source text for the life of the process.
+
+std::string jit_hex(uint64_t v)
+{
+    char b[40];
+    std::snprintf(b, sizeof(b), "0x%llxULL", static_cast<unsigned long long>(v));
+    return b;
+}
+
+void jit_emit_op(std::string& s, const FOp<double>& op, int j)
+{
+    const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
+    auto run = [&](int ts) {
+        return std::string("f.crt = ") + std::to_string(cs) + "; f.template run<" + std::to_string(ts) + ", " +
+               (cs < 0 ? "-1" : "CS_RT") + ">();";
+    };
+    std::string guard;
+    if (op.cglob != 0) {
+        guard += "if ((base & " + jit_hex(op.cglob) + ") == " + jit_hex(op.cglob) + ") ";
+    }
+    if (op.cthr != 0) {
+        guard += "if ((t & " + std::to_string(op.cthr) + "u) == " + std::to_string(op.cthr) + "u) ";
+    }
+    s += "        " + guard + "{\n            const FOp<double>& o = sops[" + std::to_string(j) + "];\n            ";
+    switch (op.kind) {
+        case OP_GEN:
+            s += "GenF<double, RB> f {v, make_cx<double>(o.m[0], o.m[1]), make_cx<double>(o.m[2], o.m[3]), "
+                 "make_cx<double>(o.m[4], o.m[5]), make_cx<double>(o.m[6], o.m[7])}; " + run(op.tslot);
+            break;
+        case OP_GENR:
+            s += "GenRF<double, RB> f {v, o.m[0], o.m[2], o.m[4], o.m[6]}; " + run(op.tslot);
+            break;
+        case OP_RXL:
+            s += "RxF<double, RB> f {v, o.m[0], o.m[3]}; " + run(op.tslot);
+            break;
+        case OP_ANTI:
+            s += "AntiF<double, RB, false> f {v, make_cx<double>(o.m[2], o.m[3]), make_cx<double>(o.m[4], o.m[5])}; " +
+                 run(op.tslot);
+            break;
+        case OP_SWAP:
+            s += "AntiF<double, RB, true> f {v, make_cx<double>(1, 0), make_cx<double>(1, 0)}; " + run(op.tslot);
+            break;
+        default: {
+            const bool one = (op.kind == OP_DIAG1);
+            if (op.tslot != NO_SLOT) {
+                s += std::string("DiagRegF<double, RB, ") + (one ? "true" : "false") +
+                     "> f {v, make_cx<double>(o.m[0], o.m[1]), make_cx<double>(o.m[6], o.m[7])}; " + run(op.tslot);
+            } else {
+                std::string b = "false";
+                if (op.tthr != 0 && op.tglob != 0) {
+                    b = "((t & " + std::to_string(op.tthr) + "u) != 0u) || ((base & " + jit_hex(op.tglob) + ") != 0ULL)";
+                } else if (op.tthr != 0) {
+                    b = "(t & " + std::to_string(op.tthr) + "u) != 0u";
+                } else if (op.tglob != 0) {
+                    b = "(base & " + jit_hex(op.tglob) + ") != 0ULL";
+                }
+                s += "const bool b = " + b + "; ";
+                s += one ? "if (b) " : "";
+                s += "{ DiagAllF<double, RB> f {v, b ? make_cx<double>(o.m[6], o.m[7]) : make_cx<double>(o.m[0], o.m[1])}; " +
+                     run(0) + " }";
+            }
+            break;
+        }
+    }
+    s += "\n        }\n";
+}
+
+// the body of block b's kernel (everything after its name)
+std::string jit_block_body(const Plan<double>& plan, size_t b, int RB, int threads, int minb)
+{
+    const FBlock& fb = plan.blocks[b];
+    const int TB = fb.K - RB;
+    const int np = fb.phase_end - fb.phase_begin;
+    std::string s;
+    s.reserve(16384);
+    s += "(void* a_, const void* blk_, const void* ph_, const void* ops_, unsigned long long n_tiles)\n{\n";
+    s += "    using namespace kt;\n    using C = double2;\n";
+    s += "    constexpr int RB = " + std::to_string(RB) + ";\n";
+    s += "    constexpr int TB = " + std::to_string(TB) + ";\n";
+    s += "    C* __restrict__ a = static_cast<C*>(a_);\n";
+    s += "    extern __shared__ __align__(16) unsigned char smem_raw[];\n";
+    s += "    __shared__ FBlock bk;\n    __shared__ FPhase sph[" + std::to_string(np) + "];\n";
+    s += "    const uint32_t t = threadIdx.x;\n";
+    s += "    if (t == 0) {\n        bk = *static_cast<const FBlock*>(blk_);\n    }\n    __syncthreads();\n";
+    s += "    C* sm = reinterpret_cast<C*>(smem_raw);\n";
+    s += "    FOp<double>* sops = reinterpret_cast<FOp<double>*>(smem_raw + (sizeof(C) << " + std::to_string(fb.K) + "));\n";
+    s += "    stage_block(bk, static_cast<const FPhase*>(ph_), static_cast<const FOp<double>*>(ops_), sph, sops, t);\n";
+    s += "    __syncthreads();\n";
+    s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
+    s += "        C v[1 << RB];\n        const uint64_t base = tile_base(bk, tile);\n";
+    s += "        tile_load<double, RB, false>(v, a, sph[0], base, t, TB, false);\n";
+    for (int p = 0; p < np; ++p) {
+        const FPhase& ph = plan.phases[static_cast<size_t>(fb.phase_begin + p)];
+        if (p > 0) {
+            s += "        tile_transpose<double, RB>(v, sm, sph[" + std::to_string(p - 1) + "], sph[" + std::to_string(p) +
+                 "], t, TB);\n";
+        }
+        for (int o = ph.op_begin; o < ph.op_end; ++o) {
+            jit_emit_op(s, plan.ops[static_cast<size_t>(o)], o - fb.op_begin);
+        }
+    }
+    s += "        tile_store<double, RB>(v, a, sph[" + std::to_string(np - 1) + "], base, t, TB);\n    }\n}\n";
+    (void)threads;
+    (void)minb;
+    return s;
+}
+
+struct JitCache
+{
+    std::mutex m;
+    std::unordered_map<std::string, const void*> kernels;  // launch-bounds prefix + body -> kernel
+    std::unordered_set<size_t> seen;                       // plans applied once with the precompiled kernels
+    int64_t compiled {0};
+    int64_t launches {0};
+    bool failed {false};
+};
+
+JitCache& jit_cache()
+{
+    static JitCache c;
+    return c;
+}
+
+// The kernels of every block of `plan` (compiling the ones not cached yet);
+// false when the precompiled kernels should run instead: run-time compilation
+// is unavailable or failed, or (`on_repeat`) the plan is new to this process,
+// so compiling waits for its second apply.
+bool jit_kernels(const Plan<double>& plan, int RB, int threads, int minb, int smem_bytes, bool on_repeat,
+                 std::vector<const void*>& out)
+{
+    JitCache& jc = jit_cache();
+    std::lock_guard<std::mutex> lock(jc.m);
+    if (jc.failed) {
+        return false;
+    }
+    const std::string bounds =
+        "__launch_bounds__(" + std::to_string(threads) + ", " + std::to_string(minb) + ")";
+    const size_t nb = plan.blocks.size();
+    std::vector<std::string> keys(nb);
+    std::vector<size_t> missing;
+    std::unordered_map<std::string, size_t> first_of;
+    for (size_t b = 0; b < nb; ++b) {
+        keys[b] = bounds + jit_block_body(plan, b, RB, threads, minb);
+        if (jc.kernels.count(keys[b]) == 0 && first_of.count(keys[b]) == 0) {
+            first_of[keys[b]] = b;
+            missing.push_back(b);
+        }
+    }
+    if (!missing.empty() && on_repeat) {
+        std::string all;
+        for (const auto& k : keys) {
+            all += k;
+        }
+        if (jc.seen.insert(std::hash<std::string> {}(all)).second) {
+            return false;
+        }
+    }
+    if (!missing.empty()) {
+        // a handful of programs, compiled on parallel host threads
+        const size_t workers = std::max<size_t>(1, std::min<size_t>(missing.size(), 32));
+        std::vector<std::string> sources(workers, "#include \"kt_fused_dev.cuh\"\n\n");
+        std::vector<std::vector<std::string>> names(workers);
+        std::vector<std::vector<size_t>> owner(workers);
+        for (size_t i = 0; i < missing.size(); ++i) {
+            const size_t w = i % workers;
+            const std::string name = "kt_jb" + std::to_string(jc.compiled + static_cast<int64_t>(i));
+            sources[w] += "extern \"C\" __global__ void " + bounds + " " + name + keys[missing[i]].substr(bounds.size()) + "\n";
+            names[w].push_back(name);
+            owner[w].push_back(missing[i]);
+        }
+        std::vector<std::vector<const void*>> got;
+        if (jit_compile(sources, names, got, true) != KT_OK) {
+            jc.failed = true;
+            return false;
+        }
+        for (size_t w = 0; w < workers; ++w) {
+            for (size_t k = 0; k < names[w].size(); ++k) {
+                const void* fn = got[w][k];
+                if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes) != cudaSuccess) {
+                    set_error(KT_ERR_CUDA, "cudaFuncSetAttribute on a run-time compiled block kernel failed");
+                    jc.failed = true;
+                    return false;
+                }
+                jc.kernels[keys[owner[w][k]]] = fn;
+            }
+        }
+        jc.compiled += static_cast<int64_t>(missing.size());
+    }
+    out.resize(nb);
+    for (size_t b = 0; b < nb; ++b) {
+        out[b] = jc.kernels[keys[b]];
+    }
+    return true;
+}
+
 template <typename T>
 int32_t run_fused(State& s, const std::vector<LGate>& gates)
 {
     using C = typename CxT<T>::type;
-    constexpr int RB = Cfg<T>::RB;
-    constexpr int L = Cfg<T>::L;
     const int n = s.n_bits;
-    const int k_pref = std::min(RB + TBMAX, tuning().fused_tile_bits + (RB - 4));
-    const int K = std::min(n, k_pref);
-    if (n < RB + 5 || gates.empty()) {
+    Plan<T> plan;
+    int K = 0;
+    bool rb3 = false;
+    if (n < Cfg<T>::RB + 5 || gates.empty()) {
         for (const auto& g : gates) {
             if (const int32_t rc = launch_gate_sweep(s, g); rc != KT_OK) {
                 return rc;
@@ -241,19 +517,8 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
         }
         return KT_OK;
     }
-    auto blocks = form_blocks(gates, n, K, L,
-                              static_cast<size_t>(std::min(MAX_OPS_PER_BLOCK, tuning().fused_max_ops)));
-    Plan<T> plan;
-    for (const auto& b : blocks) {
-        plan_block<T>(b, gates, n, plan);
-    }
-    // a block with more phases than the kernel's table holds is split in two
-    // (never happens with MAX_OPS_PER_BLOCK ops and RB >= 4, checked here)
-    for (const auto& fb : plan.blocks) {
-        if (fb.phase_end - fb.phase_begin > MAX_PHASES_PER_BLOCK) {
-            set_error(KT_ERR_INVALID, "fused block planner produced too many phases");
-            return KT_ERR_INVALID;
-        }
+    if (const int32_t rc = fused_plan<T>(n, gates, plan, &K, &rb3); rc != KT_OK) {
+        return rc;
     }
     // upload the plan: blocks | phases | ops
     auto al = [](size_t v) { return (v + 255) & ~size_t {255}; };
@@ -278,20 +543,33 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     const auto* d_blk = reinterpret_cast<const FBlock*>(dev);
     const auto* d_ph = reinterpret_cast<const FPhase*>(dev + off_p);
     const auto* d_ops = reinterpret_cast<const FOp<T>*>(dev + off_o);
-    const int threads = 1 << (K - RB);
+    const int threads = 1 << (K - (rb3 ? Cfg3::RB : Cfg<T>::RB));
     // 512-thread tiles run one CTA per SM; 256-thread tiles follow the register-budget knob
-    const int shape = threads > 256 ? 0 : (tuning().fused_ctas_per_sm == 1 ? 1 : 2);
+    int shape = threads > 256 ? 0 : (tuning().fused_ctas_per_sm == 1 ? 1 : 2);
+    if (rb3) {
+        shape = threads > 256 ? 3 : 4;
+    }
     if constexpr (std::is_same<T, float>::value) {
         if (tuning().c64_renormalize != 0) {
             return run_fused_norm<T>(s, plan, d_blk, d_ph, d_ops, K, threads, shape);
         }
     }
-    static bool attr_set[3] = {false, false, false};
+    static bool attr_set[5] = {false, false, false, false, false};
     if (!attr_set[shape]) {
         const int bytes = fused_smem_limit(shape);
         switch (shape) {
             case 0: KT_CUDA(cudaFuncSetAttribute(k_fused<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
             case 1: KT_CUDA(cudaFuncSetAttribute(k_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
+            case 3:
+            case 4:
+                if constexpr (std::is_same<T, double>::value) {
+                    if (shape == 3) {
+                        KT_CUDA(cudaFuncSetAttribute(k_fused<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+                    } else {
+                        KT_CUDA(cudaFuncSetAttribute(k_fused<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+                    }
+                }
+                break;
             default: KT_CUDA(cudaFuncSetAttribute(k_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)); break;
         }
         attr_set[shape] = true;
@@ -299,6 +577,35 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     const uint64_t n_tiles = uint64_t {1} << (n - K);
     const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * fused_ctas(shape));
     const double pass_bytes = 2.0 * static_cast<double>(sizeof(C)) * static_cast<double>(s.n_amps());
+    if constexpr (std::is_same<T, double>::value) {
+        // fused_jit: 1 = always; 2 = from the second apply of a plan, on states of
+        // at least jit_min_qubits qubits (where a pass is long enough to repay
+        // the compile, about half a second per block kernel on one host thread)
+        const int mode = tuning().fused_jit;
+        const bool want = mode == 1 || (mode == 2 && n >= tuning().jit_min_qubits);
+        std::vector<const void*> jk;
+        if (want && !rb3 &&
+            jit_kernels(plan, Cfg<T>::RB, threads, shape == 0 ? 1 : fused_ctas(shape), fused_smem_limit(shape),
+                        mode == 2, jk)) {
+            void* a = s.amps;
+            unsigned long long nt = n_tiles;
+            for (size_t b = 0; b < plan.blocks.size(); ++b) {
+                const auto& fb = plan.blocks[b];
+                const size_t smem =
+                    (size_t {1} << K) * sizeof(C) + static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOp<T>);
+                const void* blkp = d_blk + b;
+                const void* php = d_ph;
+                const void* opsp = d_ops;
+                void* args[] = {&a, &blkp, &php, &opsp, &nt};
+                KT_CUDA(cudaLaunchKernel(jk[b], dim3(static_cast<unsigned>(grid)), dim3(static_cast<unsigned>(threads)),
+                                         args, smem, s.stream));
+                s.last_launches += 1;
+                s.last_alg_bytes += pass_bytes;
+            }
+            jit_cache().launches += static_cast<int64_t>(plan.blocks.size());
+            return KT_OK;
+        }
+    }
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         const auto& fb = plan.blocks[b];
         const size_t smem = (size_t {1} << K) * sizeof(C) + static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOp<T>);
@@ -307,6 +614,16 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
         switch (shape) {
             case 0: k_fused<T, 0><<<g, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles); break;
             case 1: k_fused<T, 1><<<g, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles); break;
+            case 3:
+            case 4:
+                if constexpr (std::is_same<T, double>::value) {
+                    if (shape == 3) {
+                        k_fused<T, 3><<<g, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles);
+                    } else {
+                        k_fused<T, 4><<<g, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles);
+                    }
+                }
+                break;
             default: k_fused<T, 2><<<g, threads, smem, s.stream>>>(a, d_blk + b, d_ph, d_ops, n_tiles); break;
         }
         KT_CHECK_LAUNCH("k_fused");
@@ -511,6 +828,45 @@ int32_t adjoint_sweep_fused(State& psi, State& lam, const std::vector<AdjGate>& 
                                 : run_adjoint_sweep<float>(psi, lam, gates, dev_grad, work);
 }
 
+int32_t jit_compile_only(int n, const std::vector<LGate>& gates, int64_t* n_kernels)
+{
+    *n_kernels = 0;
+    if (n < Cfg<double>::RB + 5 || gates.empty()) {
+        return KT_OK;
+    }
+    Plan<double> plan;
+    int K = 0;
+    bool rb3 = false;
+    if (const int32_t rc = fused_plan<double>(n, gates, plan, &K, &rb3); rc != KT_OK) {
+        return rc;
+    }
+    const int RB = rb3 ? Cfg3::RB : Cfg<double>::RB;
+    const int threads = 1 << (K - RB);
+    std::vector<std::string> sources(1, "#include \"kt_fused_dev.cuh\"\n\n");
+    std::vector<std::vector<std::string>> names(1);
+    for (size_t b = 0; b < plan.blocks.size(); ++b) {
+        const std::string name = "kt_jc" + std::to_string(b);
+        sources[0] += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(threads) + ", 1) " + name +
+                      jit_block_body(plan, b, RB, threads, 1) + "\n";
+        names[0].push_back(name);
+    }
+    std::vector<std::vector<const void*>> got;
+    if (const int32_t rc = jit_compile(sources, names, got, false); rc != KT_OK) {
+        return rc;
+    }
+    *n_kernels = static_cast<int64_t>(plan.blocks.size());
+    return KT_OK;
+}
+
+void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed)
+{
+    JitCache& jc = jit_cache();
+    std::lock_guard<std::mutex> lock(jc.m);
+    *compiled = jc.compiled;
+    *launches = jc.launches;
+    *failed = jc.failed ? 1 : 0;
+}
+
 int32_t apply_fused(State& s, const std::vector<LGate>& gates)
 {
     return s.dtype == KT_C128 ? run_fused<double>(s, gates) : run_fused<float>(s, gates);
@@ -522,21 +878,18 @@ namespace
 template <typename T>
 void plan_only(int n, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases, int64_t* ops, int64_t* transposes)
 {
-    constexpr int RB = Cfg<T>::RB;
-    constexpr int L = Cfg<T>::L;
-    const int k_pref = std::min(RB + TBMAX, tuning().fused_tile_bits + (RB - 4));
-    const int K = std::min(n, k_pref);
-    if (n < RB + 5) {
-        *blocks = 0;
-        *phases = 0;
-        *ops = 0;
-        *transposes = 0;
+    *blocks = 0;
+    *phases = 0;
+    *ops = 0;
+    *transposes = 0;
+    if (n < Cfg<T>::RB + 5 || gates.empty()) {
         return;
     }
-    const auto pbs = form_blocks(gates, n, K, L, static_cast<size_t>(std::min(MAX_OPS_PER_BLOCK, tuning().fused_max_ops)));
     Plan<T> plan;
-    for (const auto& b : pbs) {
-        plan_block<T>(b, gates, n, plan);
+    int K = 0;
+    bool rb3 = false;
+    if (fused_plan<T>(n, gates, plan, &K, &rb3) != KT_OK) {
+        return;
     }
     *blocks = static_cast<int64_t>(plan.blocks.size());
     *phases = static_cast<int64_t>(plan.phases.size());

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "kettle_b200.h"
+#include "kt_complex.cuh"
 
 namespace kt
 {
@@ -104,16 +105,7 @@ LGate conj_shifted(const LGate& g, int shift);
 // every other op.
 bool gate_derivative(int op, double th, double* d);
 
-// Generators of the parameterised gates: RX/RY/RZ (and CRX/CRY/CRZ) are
-// exp(-i theta G / 2) with G = X, Y, Z; P (and CP) is diag(1, e^(i theta)).
-enum Generator : int32_t
-{
-    GEN_X = 0,
-    GEN_Y = 1,
-    GEN_Z = 2,
-    GEN_P = 3,
-};
-// GEN_* of a gate op, or -1 when it has no angle
+// GEN_* (kt_complex.cuh) of a gate op, or -1 when it has no angle
 int gate_generator(int op);
 
 // ---------------------------------------------------------------------------
@@ -139,6 +131,16 @@ struct AdjGate
 };
 // un-apply `gates` to psi and lambda with fused blocks; dev_grad[row] = 2 Re <lambda|D psi>
 int32_t adjoint_sweep_fused(State& psi, State& lam, const std::vector<AdjGate>& gates, double* dev_grad, DevBuf& work);
+// run-time compiled block kernels (kt_jit.cpp): compile each source (which may
+// include "kt_fused_dev.cuh") for sm_100a and return its kernels `names[i]`
+bool jit_available(std::string* why);
+// (load = false: compile only, no device needed)
+int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<std::vector<std::string>>& names,
+                    std::vector<std::vector<const void*>>& kernels, bool load = true);
+// host-only: plan a complex128 apply and compile its block kernels without loading them
+int32_t jit_compile_only(int n, const std::vector<LGate>& gates, int64_t* n_kernels);
+// kernels compiled so far, block launches through them, and whether compiling failed
+void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed);
 // host-only: what the fused planner makes of a gate stream
 int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases,
                    int64_t* ops, int64_t* transposes);
@@ -179,6 +181,10 @@ struct Tuning
     int adjoint_fused {1};       // 1: fused backward blocks, 0: one kernel per gate
     int fold_permutations {1};   // 1: X / CX inside a tile become part of a transpose, 0: ops
     int c64_renormalize {1};     // 1: complex64 applies keep the state's norm (per-block rescaling)
+    int fused_reg_bits {4};      // complex128 amplitudes per thread in fused blocks: 2^4, or 2^3 (more warps)
+    int fused_jit {2};           // complex128 blocks as run-time compiled kernels: 0 never, 1 always,
+                                 // 2 from a plan's second apply on >= jit_min_qubits qubits
+    int jit_min_qubits {26};
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);

@@ -1,0 +1,183 @@
+// kt_jit.cpp — run-time compilation of generated block kernels (NVRTC).
+//
+// The fused-block planner can emit, for each block, CUDA C++ whose gate
+// bodies are straight-line code with every register slot, control slot and
+// thread / tile mask a compile-time constant (kt_fused.cu, jit_block_body).
+// This file compiles such sources for sm_100a with NVRTC, loads the cubins
+// with cudaLibraryLoadData and hands back launchable kernels.  NVRTC is
+// opened with dlopen at first use, so the library itself has no link-time
+// dependency on it; when it cannot be opened, or a compile fails, the caller
+// keeps using the precompiled kernels.
+//
+// The generated sources include the fused device header; its text (and that
+// of the header it includes) is embedded at build time (kt_jit_headers.inc,
+// written by kettle_b200/build.py into the build directory).
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <nvrtc.h>
+
+#include "kt_internal.cuh"
+#include "kt_jit_headers.inc"
+
+namespace kt
+{
+
+namespace
+{
+
+struct Nvrtc
+{
+    void* handle {nullptr};
+    decltype(&nvrtcCreateProgram) create {nullptr};
+    decltype(&nvrtcCompileProgram) compile {nullptr};
+    decltype(&nvrtcGetProgramLogSize) log_size {nullptr};
+    decltype(&nvrtcGetProgramLog) log {nullptr};
+    decltype(&nvrtcGetCUBINSize) cubin_size {nullptr};
+    decltype(&nvrtcGetCUBIN) cubin {nullptr};
+    decltype(&nvrtcDestroyProgram) destroy {nullptr};
+    decltype(&nvrtcGetErrorString) error_string {nullptr};
+    bool ok {false};
+    std::string why;
+};
+
+Nvrtc& nvrtc()
+{
+    static Nvrtc lib;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const char* names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"};
+        for (const char* n : names) {
+            lib.handle = dlopen(n, RTLD_NOW | RTLD_LOCAL);
+            if (lib.handle != nullptr) {
+                break;
+            }
+        }
+        if (lib.handle == nullptr) {
+            lib.why = "NVRTC (libnvrtc.so.12) could not be opened";
+            return;
+        }
+        auto sym = [&](const char* s) { return dlsym(lib.handle, s); };
+        lib.create = reinterpret_cast<decltype(lib.create)>(sym("nvrtcCreateProgram"));
+        lib.compile = reinterpret_cast<decltype(lib.compile)>(sym("nvrtcCompileProgram"));
+        lib.log_size = reinterpret_cast<decltype(lib.log_size)>(sym("nvrtcGetProgramLogSize"));
+        lib.log = reinterpret_cast<decltype(lib.log)>(sym("nvrtcGetProgramLog"));
+        lib.cubin_size = reinterpret_cast<decltype(lib.cubin_size)>(sym("nvrtcGetCUBINSize"));
+        lib.cubin = reinterpret_cast<decltype(lib.cubin)>(sym("nvrtcGetCUBIN"));
+        lib.destroy = reinterpret_cast<decltype(lib.destroy)>(sym("nvrtcDestroyProgram"));
+        lib.error_string = reinterpret_cast<decltype(lib.error_string)>(sym("nvrtcGetErrorString"));
+        lib.ok = lib.create && lib.compile && lib.log_size && lib.log && lib.cubin_size && lib.cubin && lib.destroy &&
+                 lib.error_string;
+        if (!lib.ok) {
+            lib.why = "NVRTC is missing an entry point";
+        }
+    });
+    return lib;
+}
+
+// one source -> one cubin (empty on failure, with the reason in `err`)
+std::vector<char> compile_one(const std::string& source, std::string& err)
+{
+    Nvrtc& L = nvrtc();
+    nvrtcProgram prog = nullptr;
+    nvrtcResult r = L.create(&prog, source.c_str(), "kt_jit_blocks.cu", KT_JIT_N_HEADERS, KT_JIT_HEADER_TEXT,
+                             KT_JIT_HEADER_NAMES);
+    if (r != NVRTC_SUCCESS) {
+        err = std::string("nvrtcCreateProgram: ") + L.error_string(r);
+        return {};
+    }
+    const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device", "--fmad=true",
+                          "--extra-device-vectorization"};
+    r = L.compile(prog, static_cast<int>(sizeof(opts) / sizeof(opts[0])), opts);
+    if (r != NVRTC_SUCCESS) {
+        size_t n = 0;
+        L.log_size(prog, &n);
+        std::string log(n, '\0');
+        if (n > 0) {
+            L.log(prog, &log[0]);
+        }
+        err = std::string("nvrtcCompileProgram: ") + L.error_string(r) + "\n" + log.substr(0, 2000);
+        L.destroy(&prog);
+        return {};
+    }
+    size_t n = 0;
+    L.cubin_size(prog, &n);
+    std::vector<char> out(n);
+    if (n > 0) {
+        L.cubin(prog, out.data());
+    }
+    L.destroy(&prog);
+    return out;
+}
+
+}  // namespace
+
+bool jit_available(std::string* why)
+{
+    Nvrtc& L = nvrtc();
+    if (!L.ok && why != nullptr) {
+        *why = L.why;
+    }
+    return L.ok;
+}
+
+int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<std::vector<std::string>>& names,
+                    std::vector<std::vector<const void*>>& kernels, bool load)
+{
+    std::string why;
+    if (!jit_available(&why)) {
+        set_error(KT_ERR_CUDA, why);
+        return KT_ERR_CUDA;
+    }
+    const size_t n = sources.size();
+    std::vector<std::vector<char>> cubins(n);
+    std::vector<std::string> errs(n);
+    const size_t workers = std::max<size_t>(1, std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency())));
+    std::vector<std::thread> pool;
+    std::mutex m;
+    size_t next = 0;
+    for (size_t w = 0; w < workers; ++w) {
+        pool.emplace_back([&] {
+            for (;;) {
+                size_t i = 0;
+                {
+                    std::lock_guard<std::mutex> g(m);
+                    if (next >= n) {
+                        return;
+                    }
+                    i = next++;
+                }
+                cubins[i] = compile_one(sources[i], errs[i]);
+            }
+        });
+    }
+    for (auto& th : pool) {
+        th.join();
+    }
+    kernels.assign(n, {});
+    for (size_t i = 0; i < n; ++i) {
+        if (cubins[i].empty()) {
+            set_error(KT_ERR_CUDA, "run-time compile of a block kernel failed: " + errs[i]);
+            return KT_ERR_CUDA;
+        }
+        if (!load) {
+            continue;
+        }
+        cudaLibrary_t lib = nullptr;
+        KT_CUDA(cudaLibraryLoadData(&lib, cubins[i].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+        for (const auto& name : names[i]) {
+            cudaKernel_t k = nullptr;
+            KT_CUDA(cudaLibraryGetKernel(&k, lib, name.c_str()));
+            kernels[i].push_back(reinterpret_cast<const void*>(k));
+        }
+        // the library stays loaded for the life of the process (its kernels are cached)
+    }
+    return KT_OK;
+}
+
+}  // namespace kt

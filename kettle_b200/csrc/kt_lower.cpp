@@ -98,6 +98,12 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.fold_permutations = (v != 0) ? 1 : 0;
     } else if (name == "c64_renormalize") {
         t.c64_renormalize = (v != 0) ? 1 : 0;
+    } else if (name == "fused_reg_bits") {
+        t.fused_reg_bits = (v == 3) ? 3 : 4;
+    } else if (name == "fused_jit") {
+        t.fused_jit = static_cast<int>(std::max(0LL, std::min(2LL, v)));
+    } else if (name == "jit_min_qubits") {
+        t.jit_min_qubits = static_cast<int>(std::max(1LL, std::min(64LL, v)));
     } else {
         return false;
     }
@@ -155,6 +161,12 @@ bool tuning_get(const char* name, long long* value)
         *value = t.fold_permutations;
     } else if (n == "c64_renormalize") {
         *value = t.c64_renormalize;
+    } else if (n == "fused_reg_bits") {
+        *value = t.fused_reg_bits;
+    } else if (n == "fused_jit") {
+        *value = t.fused_jit;
+    } else if (n == "jit_min_qubits") {
+        *value = t.jit_min_qubits;
     } else {
         return false;
     }

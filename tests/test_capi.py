@@ -82,3 +82,13 @@ def test_batch_rejects_bad_items_on_the_host():
     with pytest.raises(capi.KettleError) as e:
         capi.Batch(items2, meas, strings, coeffs, n_params)
     assert "M gates" in str(e.value)
+
+
+def test_run_time_block_kernels_compile_on_the_host():
+    # the generated straight-line block kernels compile for sm_100a with NVRTC
+    # (no GPU needed: compile only, nothing is loaded)
+    from kettle_b200 import workloads as W
+    g = W.random_layers(14, 3, seed=1, mixed=True)
+    assert capi.jit_compile_only(14, g) >= 1
+    gates, params = W.hea(13, 2, seed=2)
+    assert capi.jit_compile_only(13, gates, params) >= 1

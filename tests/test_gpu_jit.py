@@ -1,0 +1,125 @@
+"""Run-time compiled block kernels (fused_jit = 1): the same amplitudes as the
+oracle (1e-12) and as the precompiled fused kernels (1e-13) on circuits that
+exercise every op kind (general, real, RX-like, anti-diagonal, swap, diagonal
+on register / thread / tile-external bits) with controls on register, thread
+and tile-external bits and folded permutations; kernels are reused for a new
+set of angles; parameterised circuits bind their angles at run time."""
+import numpy as np
+import pytest
+
+from conftest import basis, random_state
+from kettle_b200 import capi
+from kettle_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture()
+def jit(engine):
+    old = capi.tuning_get("fused_jit")
+    capi.tuning_set("fused_jit", 1)
+    yield capi
+    capi.tuning_set("fused_jit", old)
+
+
+def _apply(n, init, gates, params=None):
+    sv = capi.Statevector(n)
+    sv.upload(init)
+    sv.apply(gates, params)
+    out = sv.download()
+    sv.close()
+    return out
+
+
+@pytest.mark.parametrize("n,layers,seed", [(10, 6, 1), (14, 5, 2), (17, 4, 3), (20, 3, 4)])
+def test_jit_matches_oracle(jit, port, n, layers, seed):
+    g = W.random_layers(n, layers, seed=seed, mixed=True)
+    init = random_state(n, seed)
+    before = capi.jit_stats()
+    got = _apply(n, init, g)
+    after = capi.jit_stats()
+    assert not after["failed"]
+    assert after["launches"] > before["launches"]
+    assert np.abs(got - port.apply(n, init, g)).max() < 1e-12
+
+
+def test_jit_matches_precompiled_and_reuses_kernels(jit):
+    n = 24
+    g = W.random_layers(n, 4, seed=11, mixed=True)
+    a = _apply(n, basis(n), g)
+    capi.tuning_set("fused_jit", 0)
+    b = _apply(n, basis(n), g)
+    capi.tuning_set("fused_jit", 1)
+    assert np.abs(a - b).max() < 1e-13
+    # new angles, same structure: no new kernels
+    g2 = g.copy()
+    rng = np.random.default_rng(5)
+    has_angle = np.isin(g2["op"], [capi.OP[x] for x in capi.ANGLE_GATES])
+    g2["angle"][has_angle] = rng.uniform(0, 2 * np.pi, int(has_angle.sum()))
+    k0 = capi.jit_stats()["kernels"]
+    c = _apply(n, basis(n), g2)
+    assert capi.jit_stats()["kernels"] == k0
+    capi.tuning_set("fused_jit", 0)
+    d = _apply(n, basis(n), g2)
+    capi.tuning_set("fused_jit", 1)
+    assert np.abs(c - d).max() < 1e-13
+
+
+def test_jit_parameterised(jit, port):
+    n = 16
+    gates, params = W.hea(n, 3, seed=4)
+    got = _apply(n, basis(n), gates, params)
+    assert np.abs(got - port.apply(n, basis(n), gates, params)).max() < 1e-12
+    k0 = capi.jit_stats()["kernels"]
+    p2 = params + 0.37
+    got2 = _apply(n, basis(n), gates, p2)
+    assert capi.jit_stats()["kernels"] == k0
+    assert np.abs(got2 - port.apply(n, basis(n), gates, p2)).max() < 1e-12
+
+
+def test_jit_every_gate_kind(jit, port):
+    # every gate on low (register / lane), middle (thread) and high (outside the tile) qubits
+    n = 18
+    rng = np.random.default_rng(7)
+    names = [x for x in capi.GATES if x != "M"]
+    parts = []
+    for name in names:
+        for t, c in ((0, 5), (5, 0), (9, 16), (16, 2), (3, 17)):
+            if name in ("U", "CU"):
+                parts.append(W.gate(name, t, control=c, u=W.haar_unitary2(rng)))
+            elif name in capi.ANGLE_GATES:
+                parts.append(W.gate(name, t, control=c, angle=float(rng.uniform(0, 2 * np.pi))))
+            else:
+                parts.append(W.gate(name, t, control=c))
+        parts.append(W.gate("H", int(rng.integers(0, n))))
+    g = np.concatenate(parts)
+    init = random_state(n, 3)
+    assert np.abs(_apply(n, init, g) - port.apply(n, init, g)).max() < 1e-12
+
+
+def test_auto_mode_compiles_on_the_second_apply(engine, port):
+    # fused_jit = 2: a circuit structure new to the process runs on the
+    # precompiled kernels; its second apply compiles and runs the block kernels
+    old = {k: capi.tuning_get(k) for k in ("fused_jit", "jit_min_qubits")}
+    try:
+        capi.tuning_set("fused_jit", 2)
+        capi.tuning_set("jit_min_qubits", 19)
+        n = 19
+        g = W.random_layers(n, 3, seed=99, mixed=True)
+        s0 = capi.jit_stats()
+        a = _apply(n, basis(n), g)
+        s1 = capi.jit_stats()
+        assert s1["launches"] == s0["launches"] and s1["kernels"] == s0["kernels"]
+        b = _apply(n, basis(n), g)
+        s2 = capi.jit_stats()
+        assert s2["kernels"] > s1["kernels"] and s2["launches"] > s1["launches"]
+        want = port.apply(n, basis(n), g)
+        assert np.abs(a - want).max() < 1e-12 and np.abs(b - want).max() < 1e-12
+        # below jit_min_qubits nothing is compiled
+        small = W.random_layers(12, 3, seed=98, mixed=True)
+        _apply(12, basis(12), small)
+        _apply(12, basis(12), small)
+        assert capi.jit_stats()["kernels"] == s2["kernels"]
+    finally:
+        for k, v in old.items():
+            capi.tuning_set(k, v)
