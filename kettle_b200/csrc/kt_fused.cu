@@ -322,6 +322,9 @@ void jit_emit_op(std::string& s, const FOp<double>& op, int j)
         return std::string("f.crt = ") + std::to_string(cs) + "; f.template run<" + std::to_string(ts) + ", " +
                (cs < 0 ? "-1" : "CS_RT") + ">();";
     };
+    // the op's matrix entries: the kernel's constant-bank parameter
+    auto m = [&](int e) { return "M.m[" + std::to_string(8 * j + e) + "]"; };
+    auto cx = [&](int e) { return "make_cx<double>(" + m(e) + ", " + m(e + 1) + ")"; };
     std::string guard;
     if (op.cglob != 0) {
         guard += "if ((base & " + jit_hex(op.cglob) + ") == " + jit_hex(op.cglob) + ") ";
@@ -329,21 +332,19 @@ void jit_emit_op(std::string& s, const FOp<double>& op, int j)
     if (op.cthr != 0) {
         guard += "if ((t & " + std::to_string(op.cthr) + "u) == " + std::to_string(op.cthr) + "u) ";
     }
-    s += "        " + guard + "{\n            const FOp<double>& o = sops[" + std::to_string(j) + "];\n            ";
+    s += "        " + guard + "{\n            ";
     switch (op.kind) {
         case OP_GEN:
-            s += "GenF<double, RB> f {v, make_cx<double>(o.m[0], o.m[1]), make_cx<double>(o.m[2], o.m[3]), "
-                 "make_cx<double>(o.m[4], o.m[5]), make_cx<double>(o.m[6], o.m[7])}; " + run(op.tslot);
+            s += "GenF<double, RB> f {v, " + cx(0) + ", " + cx(2) + ", " + cx(4) + ", " + cx(6) + "}; " + run(op.tslot);
             break;
         case OP_GENR:
-            s += "GenRF<double, RB> f {v, o.m[0], o.m[2], o.m[4], o.m[6]}; " + run(op.tslot);
+            s += "GenRF<double, RB> f {v, " + m(0) + ", " + m(2) + ", " + m(4) + ", " + m(6) + "}; " + run(op.tslot);
             break;
         case OP_RXL:
-            s += "RxF<double, RB> f {v, o.m[0], o.m[3]}; " + run(op.tslot);
+            s += "RxF<double, RB> f {v, " + m(0) + ", " + m(3) + "}; " + run(op.tslot);
             break;
         case OP_ANTI:
-            s += "AntiF<double, RB, false> f {v, make_cx<double>(o.m[2], o.m[3]), make_cx<double>(o.m[4], o.m[5])}; " +
-                 run(op.tslot);
+            s += "AntiF<double, RB, false> f {v, " + cx(2) + ", " + cx(4) + "}; " + run(op.tslot);
             break;
         case OP_SWAP:
             s += "AntiF<double, RB, true> f {v, make_cx<double>(1, 0), make_cx<double>(1, 0)}; " + run(op.tslot);
@@ -351,8 +352,8 @@ void jit_emit_op(std::string& s, const FOp<double>& op, int j)
         default: {
             const bool one = (op.kind == OP_DIAG1);
             if (op.tslot != NO_SLOT) {
-                s += std::string("DiagRegF<double, RB, ") + (one ? "true" : "false") +
-                     "> f {v, make_cx<double>(o.m[0], o.m[1]), make_cx<double>(o.m[6], o.m[7])}; " + run(op.tslot);
+                s += std::string("DiagRegF<double, RB, ") + (one ? "true" : "false") + "> f {v, " + cx(0) + ", " + cx(6) +
+                     "}; " + run(op.tslot);
             } else {
                 std::string b = "false";
                 if (op.tthr != 0 && op.tglob != 0) {
@@ -364,8 +365,7 @@ void jit_emit_op(std::string& s, const FOp<double>& op, int j)
                 }
                 s += "const bool b = " + b + "; ";
                 s += one ? "if (b) " : "";
-                s += "{ DiagAllF<double, RB> f {v, b ? make_cx<double>(o.m[6], o.m[7]) : make_cx<double>(o.m[0], o.m[1])}; " +
-                     run(0) + " }";
+                s += "{ DiagAllF<double, RB> f {v, b ? " + cx(6) + " : " + cx(0) + "}; " + run(0) + " }";
             }
             break;
         }
@@ -373,45 +373,141 @@ void jit_emit_op(std::string& s, const FOp<double>& op, int j)
     s += "\n        }\n";
 }
 
-// the body of block b's kernel (everything after its name)
-std::string jit_block_body(const Plan<double>& plan, size_t b, int RB, int threads, int minb)
+// sum over the bits j of `var` of bit_j * strides[j], strides powers of two:
+// shift-and-mask runs of consecutive target bits
+std::string jit_deposit(const std::string& var, const uint64_t* strides, int nbits)
+{
+    std::string e;
+    int j = 0;
+    while (j < nbits) {
+        if (strides[j] == 0) {
+            ++j;
+            continue;
+        }
+        const int q = __builtin_ctzll(strides[j]);
+        int len = 1;
+        while (j + len < nbits && strides[j + len] == (uint64_t {1} << (q + len))) {
+            ++len;
+        }
+        const uint64_t mask = (len >= 64) ? ~uint64_t {0} : ((uint64_t {1} << len) - 1);
+        if (!e.empty()) {
+            e += " | ";
+        }
+        e += "(((static_cast<uint64_t>(" + var + ") >> " + std::to_string(j) + ") & " + jit_hex(mask) + ") << " +
+             std::to_string(q) + ")";
+        j += len;
+    }
+    return e.empty() ? std::string("0ULL") : "(" + e + ")";
+}
+
+// XOR over the bits j of t of terms[j] (32-bit shared-memory address terms)
+std::string jit_xor_terms(const uint32_t* terms, int nbits, uint32_t start)
+{
+    std::string e = std::to_string(start) + "u";
+    for (int j = 0; j < nbits; ++j) {
+        if (terms[j] != 0) {
+            e += " ^ ((0u - ((t >> " + std::to_string(j) + ") & 1u)) & " + std::to_string(terms[j]) + "u)";
+        }
+    }
+    return "(" + e + ")";
+}
+
+// The body of block b's kernel (everything after its name): the tile loop
+// with the layout of every phase written out as constants (tile base, thread
+// and register offsets, swizzled shared-memory terms) and the gate bodies as
+// straight-line code; matrices arrive in the constant-bank parameter M.
+std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
 {
     const FBlock& fb = plan.blocks[b];
     const int TB = fb.K - RB;
+    const int R = 1 << RB;
     const int np = fb.phase_end - fb.phase_begin;
+    const int nops = std::max(1, fb.op_end - fb.op_begin);
+    const FPhase* ph = plan.phases.data() + fb.phase_begin;
+    std::vector<uint64_t> free_strides(static_cast<size_t>(std::max(1, fb.nfree)));
+    for (int k = 0; k < fb.nfree; ++k) {
+        free_strides[static_cast<size_t>(k)] = uint64_t {1} << fb.freebit[k];
+    }
+    auto reg_off = [&](const FPhase& f, int i) {
+        uint64_t o = 0;
+        for (int sl = 0; sl < RB; ++sl) {
+            if (i & (1 << sl)) {
+                o += f.rstride[sl];
+            }
+        }
+        return o;
+    };
+    auto reg_xor = [&](const uint32_t* terms, int i) {
+        uint32_t x = 0;
+        for (int sl = 0; sl < RB; ++sl) {
+            if (i & (1 << sl)) {
+                x ^= terms[sl];
+            }
+        }
+        return x;
+    };
     std::string s;
-    s.reserve(16384);
-    s += "(void* a_, const void* blk_, const void* ph_, const void* ops_, unsigned long long n_tiles)\n{\n";
+    s.reserve(32768);
+    s += "(void* a_, unsigned long long n_tiles, const __grid_constant__ KtMats<" + std::to_string(8 * nops) + "> M)\n{\n";
     s += "    using namespace kt;\n    using C = double2;\n";
     s += "    constexpr int RB = " + std::to_string(RB) + ";\n";
-    s += "    constexpr int TB = " + std::to_string(TB) + ";\n";
     s += "    C* __restrict__ a = static_cast<C*>(a_);\n";
     s += "    extern __shared__ __align__(16) unsigned char smem_raw[];\n";
-    s += "    __shared__ FBlock bk;\n    __shared__ FPhase sph[" + std::to_string(np) + "];\n";
-    s += "    const uint32_t t = threadIdx.x;\n";
-    s += "    if (t == 0) {\n        bk = *static_cast<const FBlock*>(blk_);\n    }\n    __syncthreads();\n";
     s += "    C* sm = reinterpret_cast<C*>(smem_raw);\n";
-    s += "    FOp<double>* sops = reinterpret_cast<FOp<double>*>(smem_raw + (sizeof(C) << " + std::to_string(fb.K) + "));\n";
-    s += "    stage_block(bk, static_cast<const FPhase*>(ph_), static_cast<const FOp<double>*>(ops_), sph, sops, t);\n";
-    s += "    __syncthreads();\n";
+    s += "    const uint32_t t = threadIdx.x;\n";
     s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
-    s += "        C v[1 << RB];\n        const uint64_t base = tile_base(bk, tile);\n";
-    s += "        tile_load<double, RB, false>(v, a, sph[0], base, t, TB, false);\n";
+    s += "        C v[1 << RB];\n";
+    s += "        const uint64_t base = " + jit_deposit("tile", free_strides.data(), fb.nfree) + ";\n";
+    s += "        {\n            const C* src = a + base + " + jit_deposit("t", ph[0].tstride, TB) + ";\n";
+    for (int i = 0; i < R; ++i) {
+        s += "            v[" + std::to_string(i) + "] = src[" + std::to_string(reg_off(ph[0], i)) + "ULL];\n";
+    }
+    s += "        }\n";
     for (int p = 0; p < np; ++p) {
-        const FPhase& ph = plan.phases[static_cast<size_t>(fb.phase_begin + p)];
+        const FPhase& cur = ph[p];
         if (p > 0) {
-            s += "        tile_transpose<double, RB>(v, sm, sph[" + std::to_string(p - 1) + "], sph[" + std::to_string(p) +
-                 "], t, TB);\n";
+            const FPhase& prev = ph[p - 1];
+            s += "        {\n            const uint32_t so = " + jit_xor_terms(prev.tsw_out, TB, prev.xor_out) + ";\n";
+            for (int i = 0; i < R; ++i) {
+                s += "            sm[so ^ " + std::to_string(reg_xor(prev.rsw_out, i)) + "u] = v[" + std::to_string(i) + "];\n";
+            }
+            s += "            __syncthreads();\n";
+            s += "            const uint32_t lo = " + jit_xor_terms(cur.tsw, TB, 0) + ";\n";
+            for (int i = 0; i < R; ++i) {
+                s += "            v[" + std::to_string(i) + "] = sm[lo ^ " + std::to_string(reg_xor(cur.rsw, i)) + "u];\n";
+            }
+            s += "            __syncthreads();\n        }\n";
         }
-        for (int o = ph.op_begin; o < ph.op_end; ++o) {
+        for (int o = cur.op_begin; o < cur.op_end; ++o) {
             jit_emit_op(s, plan.ops[static_cast<size_t>(o)], o - fb.op_begin);
         }
     }
-    s += "        tile_store<double, RB>(v, a, sph[" + std::to_string(np - 1) + "], base, t, TB);\n    }\n}\n";
-    (void)threads;
-    (void)minb;
+    s += "        {\n            C* dst = a + base + " + jit_deposit("t", ph[np - 1].tstride, TB) + ";\n";
+    for (int i = 0; i < R; ++i) {
+        s += "            dst[" + std::to_string(reg_off(ph[np - 1], i)) + "ULL] = v[" + std::to_string(i) + "];\n";
+    }
+    s += "        }\n    }\n}\n";
     return s;
 }
+
+// the matrices of block b's ops, in the layout of its kernel's parameter M
+std::vector<double> jit_block_mats(const Plan<double>& plan, size_t b)
+{
+    const FBlock& fb = plan.blocks[b];
+    const int nops = std::max(1, fb.op_end - fb.op_begin);
+    std::vector<double> m(static_cast<size_t>(8 * nops), 0.0);
+    for (int j = 0; j < fb.op_end - fb.op_begin; ++j) {
+        const FOp<double>& op = plan.ops[static_cast<size_t>(fb.op_begin + j)];
+        for (int e = 0; e < 8; ++e) {
+            m[static_cast<size_t>(8 * j + e)] = op.m[e];
+        }
+    }
+    return m;
+}
+
+constexpr const char* JIT_PRELUDE =
+    "#include \"kt_fused_dev.cuh\"\n\n"
+    "template <int N>\nstruct KtMats\n{\n    double m[N];\n};\n\n";
 
 struct JitCache
 {
@@ -448,7 +544,7 @@ bool jit_kernels(const Plan<double>& plan, int RB, int threads, int minb, int sm
     std::vector<size_t> missing;
     std::unordered_map<std::string, size_t> first_of;
     for (size_t b = 0; b < nb; ++b) {
-        keys[b] = bounds + jit_block_body(plan, b, RB, threads, minb);
+        keys[b] = bounds + jit_block_body(plan, b, RB);
         if (jc.kernels.count(keys[b]) == 0 && first_of.count(keys[b]) == 0) {
             first_of[keys[b]] = b;
             missing.push_back(b);
@@ -466,7 +562,7 @@ bool jit_kernels(const Plan<double>& plan, int RB, int threads, int minb, int sm
     if (!missing.empty()) {
         // a handful of programs, compiled on parallel host threads
         const size_t workers = std::max<size_t>(1, std::min<size_t>(missing.size(), 32));
-        std::vector<std::string> sources(workers, "#include \"kt_fused_dev.cuh\"\n\n");
+        std::vector<std::string> sources(workers, JIT_PRELUDE);
         std::vector<std::vector<std::string>> names(workers);
         std::vector<std::vector<size_t>> owner(workers);
         for (size_t i = 0; i < missing.size(); ++i) {
@@ -589,14 +685,10 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
                         mode == 2, jk)) {
             void* a = s.amps;
             unsigned long long nt = n_tiles;
+            const size_t smem = (size_t {1} << K) * sizeof(C);
             for (size_t b = 0; b < plan.blocks.size(); ++b) {
-                const auto& fb = plan.blocks[b];
-                const size_t smem =
-                    (size_t {1} << K) * sizeof(C) + static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOp<T>);
-                const void* blkp = d_blk + b;
-                const void* php = d_ph;
-                const void* opsp = d_ops;
-                void* args[] = {&a, &blkp, &php, &opsp, &nt};
+                std::vector<double> mats = jit_block_mats(plan, b);
+                void* args[] = {&a, &nt, mats.data()};
                 KT_CUDA(cudaLaunchKernel(jk[b], dim3(static_cast<unsigned>(grid)), dim3(static_cast<unsigned>(threads)),
                                          args, smem, s.stream));
                 s.last_launches += 1;
@@ -842,12 +934,12 @@ int32_t jit_compile_only(int n, const std::vector<LGate>& gates, int64_t* n_kern
     }
     const int RB = rb3 ? Cfg3::RB : Cfg<double>::RB;
     const int threads = 1 << (K - RB);
-    std::vector<std::string> sources(1, "#include \"kt_fused_dev.cuh\"\n\n");
+    std::vector<std::string> sources(1, JIT_PRELUDE);
     std::vector<std::vector<std::string>> names(1);
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         const std::string name = "kt_jc" + std::to_string(b);
         sources[0] += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(threads) + ", 1) " + name +
-                      jit_block_body(plan, b, RB, threads, 1) + "\n";
+                      jit_block_body(plan, b, RB) + "\n";
         names[0].push_back(name);
     }
     std::vector<std::vector<const void*>> got;
