@@ -26,6 +26,7 @@
 //    target that is a thread bit.  The kernel does no per-amplitude index math.
 //  * Loads and stores use a layout whose lane bits are the L lowest qubits:
 //    each warp instruction touches whole 128-byte lines.
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -463,6 +464,18 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
         s += "            v[" + std::to_string(i) + "] = src[" + std::to_string(reg_off(ph[0], i)) + "ULL];\n";
     }
     s += "        }\n";
+    if (tuning().jit_prefetch != 0) {
+        // the next tile of this CTA into L2 while this one computes: one
+        // prefetch per 128-byte line (lanes whose low L bits are 0)
+        s += "        if ((t & 7u) == 0u && tile + gridDim.x < n_tiles) {\n";
+        s += "            const C* nxt = a + " + jit_deposit("(tile + gridDim.x)", free_strides.data(), fb.nfree) + " + " +
+             jit_deposit("t", ph[0].tstride, TB) + ";\n";
+        for (int i = 0; i < R; ++i) {
+            s += "            asm volatile(\"prefetch.global.L2 [%0];\" :: \"l\"(nxt + " + std::to_string(reg_off(ph[0], i)) +
+                 "ULL));\n";
+        }
+        s += "        }\n";
+    }
     for (int p = 0; p < np; ++p) {
         const FPhase& cur = ph[p];
         if (p > 0) {
@@ -478,8 +491,61 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
             }
             s += "            __syncthreads();\n        }\n";
         }
+        // Diagonal ops whose target (and controls, if any) are thread or
+        // tile-external bits scale all of a thread's amplitudes by one factor;
+        // they commute with every other op of the phase (those target register
+        // bits), so a phase's several such ops become one product of factors
+        // applied once, at the phase's end.
+        std::vector<int> scal;
         for (int o = cur.op_begin; o < cur.op_end; ++o) {
+            const FOp<double>& op = plan.ops[static_cast<size_t>(o)];
+            if ((op.kind == OP_DIAG || op.kind == OP_DIAG1) && op.tslot == NO_SLOT && op.cslot == NO_SLOT) {
+                scal.push_back(o);
+            }
+        }
+        const bool merge = tuning().jit_merge_diag != 0 && scal.size() >= 2;
+        for (int o = cur.op_begin; o < cur.op_end; ++o) {
+            if (merge && std::find(scal.begin(), scal.end(), o) != scal.end()) {
+                continue;
+            }
             jit_emit_op(s, plan.ops[static_cast<size_t>(o)], o - fb.op_begin);
+        }
+        if (merge) {
+            s += "        {\n            C fac = make_cx<double>(1, 0);\n";
+            for (const int o : scal) {
+                const FOp<double>& op = plan.ops[static_cast<size_t>(o)];
+                const int j = o - fb.op_begin;
+                auto cx = [&](int e) {
+                    return "make_cx<double>(M.m[" + std::to_string(8 * j + e) + "], M.m[" + std::to_string(8 * j + e + 1) + "])";
+                };
+                std::string cond;
+                if (op.cglob != 0) {
+                    cond += "((base & " + jit_hex(op.cglob) + ") == " + jit_hex(op.cglob) + ")";
+                }
+                if (op.cthr != 0) {
+                    cond += std::string(cond.empty() ? "" : " && ") + "((t & " + std::to_string(op.cthr) + "u) == " +
+                            std::to_string(op.cthr) + "u)";
+                }
+                std::string b = "false";
+                if (op.tthr != 0 && op.tglob != 0) {
+                    b = "(((t & " + std::to_string(op.tthr) + "u) != 0u) || ((base & " + jit_hex(op.tglob) + ") != 0ULL))";
+                } else if (op.tthr != 0) {
+                    b = "((t & " + std::to_string(op.tthr) + "u) != 0u)";
+                } else if (op.tglob != 0) {
+                    b = "((base & " + jit_hex(op.tglob) + ") != 0ULL)";
+                }
+                s += "            ";
+                if (!cond.empty()) {
+                    s += "if (" + cond + ") ";
+                }
+                s += "{ const bool b = " + b + "; ";
+                if (op.kind == OP_DIAG1) {
+                    s += "if (b) { fac = cmul(fac, " + cx(6) + "); } }\n";
+                } else {
+                    s += "fac = cmul(fac, b ? " + cx(6) + " : " + cx(0) + "); }\n";
+                }
+            }
+            s += "            DiagAllF<double, RB> f {v, fac}; f.template run<0, -1>();\n        }\n";
         }
     }
     s += "        {\n            C* dst = a + base + " + jit_deposit("t", ph[np - 1].tstride, TB) + ";\n";
@@ -680,12 +746,16 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
         const int mode = tuning().fused_jit;
         const bool want = mode == 1 || (mode == 2 && n >= tuning().jit_min_qubits);
         std::vector<const void*> jk;
+        // the generated kernels keep only the tile in shared memory, so 256-thread
+        // tiles may run jit_ctas_per_sm CTAs per SM (register budget 65536 / (256 * CTAs))
+        const int jit_minb = (shape == 0) ? 1 : (shape == 1 ? 1 : std::max(2, std::min(3, tuning().jit_ctas_per_sm)));
+        const uint64_t jit_grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * jit_minb);
         if (want && !rb3 &&
-            jit_kernels(plan, Cfg<T>::RB, threads, shape == 0 ? 1 : fused_ctas(shape), fused_smem_limit(shape),
-                        mode == 2, jk)) {
+            jit_kernels(plan, Cfg<T>::RB, threads, jit_minb, fused_smem_limit(shape), mode == 2, jk)) {
             void* a = s.amps;
             unsigned long long nt = n_tiles;
             const size_t smem = (size_t {1} << K) * sizeof(C);
+            const uint64_t grid = jit_grid;
             for (size_t b = 0; b < plan.blocks.size(); ++b) {
                 std::vector<double> mats = jit_block_mats(plan, b);
                 void* args[] = {&a, &nt, mats.data()};

@@ -102,6 +102,12 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.fused_reg_bits = (v == 3) ? 3 : 4;
     } else if (name == "fused_jit") {
         t.fused_jit = static_cast<int>(std::max(0LL, std::min(2LL, v)));
+    } else if (name == "jit_ctas_per_sm") {
+        t.jit_ctas_per_sm = (v >= 3) ? 3 : 2;
+    } else if (name == "jit_merge_diag") {
+        t.jit_merge_diag = (v != 0) ? 1 : 0;
+    } else if (name == "jit_prefetch") {
+        t.jit_prefetch = (v != 0) ? 1 : 0;
     } else if (name == "jit_min_qubits") {
         t.jit_min_qubits = static_cast<int>(std::max(1LL, std::min(64LL, v)));
     } else {
@@ -165,6 +171,12 @@ bool tuning_get(const char* name, long long* value)
         *value = t.fused_reg_bits;
     } else if (n == "fused_jit") {
         *value = t.fused_jit;
+    } else if (n == "jit_ctas_per_sm") {
+        *value = t.jit_ctas_per_sm;
+    } else if (n == "jit_merge_diag") {
+        *value = t.jit_merge_diag;
+    } else if (n == "jit_prefetch") {
+        *value = t.jit_prefetch;
     } else if (n == "jit_min_qubits") {
         *value = t.jit_min_qubits;
     } else {
