@@ -459,26 +459,54 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
     s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
     s += "        C v[1 << RB];\n";
     s += "        const uint64_t base = " + jit_deposit("tile", free_strides.data(), fb.nfree) + ";\n";
-    s += "        {\n            const C* src = a + base + " + jit_deposit("t", ph[0].tstride, TB) + ";\n";
+    // A block's first phase may only set up the coalesced load layout (no ops,
+    // no permutation to apply) and its last one only the store layout; then
+    // the tile is loaded straight into the second phase's layout, or stored
+    // from the one before last, and that transpose goes away (the accesses
+    // of a warp still cover whole 128-byte lines across its instructions).
+    auto identity_store = [&](const FPhase& f) {
+        if (f.xor_out != 0) {
+            return false;
+        }
+        for (int sl = 0; sl < RB; ++sl) {
+            if (f.rsw_out[sl] != f.rsw[sl]) {
+                return false;
+            }
+        }
+        for (int j = 0; j < TB; ++j) {
+            if (f.tsw_out[j] != f.tsw[j]) {
+                return false;
+            }
+        }
+        return true;
+    };
+    const bool skip_io = tuning().jit_skip_io != 0;
+    const int first = (skip_io && np > 1 && ph[0].op_begin == ph[0].op_end && identity_store(ph[0])) ? 1 : 0;
+    const int last = (skip_io && np - 1 > first && ph[np - 1].op_begin == ph[np - 1].op_end && identity_store(ph[np - 2]))
+                         ? np - 2
+                         : np - 1;
+    s += "        {\n            const C* src = a + base + " + jit_deposit("t", ph[first].tstride, TB) + ";\n";
     for (int i = 0; i < R; ++i) {
-        s += "            v[" + std::to_string(i) + "] = src[" + std::to_string(reg_off(ph[0], i)) + "ULL];\n";
+        s += "            v[" + std::to_string(i) + "] = src[" + std::to_string(reg_off(ph[first], i)) + "ULL];\n";
     }
     s += "        }\n";
     if (tuning().jit_prefetch != 0) {
         // the next tile of this CTA into L2 while this one computes: one
-        // prefetch per 128-byte line (lanes whose low L bits are 0)
-        s += "        if ((t & 7u) == 0u && tile + gridDim.x < n_tiles) {\n";
+        // prefetch per 128-byte line when the lowest qubits are the low lanes
+        const bool lines_on_lanes = TB >= 3 && ph[first].tstride[0] == 1 && ph[first].tstride[1] == 2 &&
+                                    ph[first].tstride[2] == 4;
+        s += std::string("        if (") + (lines_on_lanes ? "(t & 7u) == 0u && " : "") + "tile + gridDim.x < n_tiles) {\n";
         s += "            const C* nxt = a + " + jit_deposit("(tile + gridDim.x)", free_strides.data(), fb.nfree) + " + " +
-             jit_deposit("t", ph[0].tstride, TB) + ";\n";
+             jit_deposit("t", ph[first].tstride, TB) + ";\n";
         for (int i = 0; i < R; ++i) {
-            s += "            asm volatile(\"prefetch.global.L2 [%0];\" :: \"l\"(nxt + " + std::to_string(reg_off(ph[0], i)) +
+            s += "            asm volatile(\"prefetch.global.L2 [%0];\" :: \"l\"(nxt + " + std::to_string(reg_off(ph[first], i)) +
                  "ULL));\n";
         }
         s += "        }\n";
     }
-    for (int p = 0; p < np; ++p) {
+    for (int p = first; p <= last; ++p) {
         const FPhase& cur = ph[p];
-        if (p > 0) {
+        if (p > first) {
             const FPhase& prev = ph[p - 1];
             s += "        {\n            const uint32_t so = " + jit_xor_terms(prev.tsw_out, TB, prev.xor_out) + ";\n";
             for (int i = 0; i < R; ++i) {
@@ -548,9 +576,9 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
             s += "            DiagAllF<double, RB> f {v, fac}; f.template run<0, -1>();\n        }\n";
         }
     }
-    s += "        {\n            C* dst = a + base + " + jit_deposit("t", ph[np - 1].tstride, TB) + ";\n";
+    s += "        {\n            C* dst = a + base + " + jit_deposit("t", ph[last].tstride, TB) + ";\n";
     for (int i = 0; i < R; ++i) {
-        s += "            dst[" + std::to_string(reg_off(ph[np - 1], i)) + "ULL] = v[" + std::to_string(i) + "];\n";
+        s += "            dst[" + std::to_string(reg_off(ph[last], i)) + "ULL] = v[" + std::to_string(i) + "];\n";
     }
     s += "        }\n    }\n}\n";
     return s;
@@ -746,9 +774,9 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
         const int mode = tuning().fused_jit;
         const bool want = mode == 1 || (mode == 2 && n >= tuning().jit_min_qubits);
         std::vector<const void*> jk;
-        // the generated kernels keep only the tile in shared memory, so 256-thread
-        // tiles may run jit_ctas_per_sm CTAs per SM (register budget 65536 / (256 * CTAs))
-        const int jit_minb = (shape == 0) ? 1 : (shape == 1 ? 1 : std::max(2, std::min(3, tuning().jit_ctas_per_sm)));
+        // the generated kernels keep only the tile in shared memory, so they may
+        // run jit_ctas_per_sm CTAs per SM (register budget 65536 / (threads * CTAs))
+        const int jit_minb = (shape == 0) ? 1 : (shape == 1 ? 1 : std::max(2, std::min(4, tuning().jit_ctas_per_sm)));
         const uint64_t jit_grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * jit_minb);
         if (want && !rb3 &&
             jit_kernels(plan, Cfg<T>::RB, threads, jit_minb, fused_smem_limit(shape), mode == 2, jk)) {

@@ -186,8 +186,9 @@ struct Tuning
                                  // 2 from a plan's second apply on >= jit_min_qubits qubits
     int jit_min_qubits {26};
     int jit_prefetch {1};        // 1: run-time compiled blocks prefetch their CTA's next tile into L2
-    int jit_ctas_per_sm {2};     // CTAs per SM of run-time compiled 256-thread blocks: 2 or 3
-    int jit_merge_diag {1};      // 1: a phase's diagonal ops on thread / tile-external bits as one factor
+    int jit_ctas_per_sm {2};     // CTAs per SM of run-time compiled blocks: 2..4
+    int jit_merge_diag {1};
+    int jit_skip_io {1};         // 1: no transpose into a block's load layout or out of its store layout      // 1: a phase's diagonal ops on thread / tile-external bits as one factor
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);
