@@ -481,6 +481,9 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
         return true;
     };
     const bool skip_io = tuning().jit_skip_io != 0;
+    // jit_fence = k: every k ops the amplitudes pass through an empty asm, so
+    // the scheduler cannot interleave more than k ops (bounds the live registers)
+    const int fence_every = tuning().jit_fence;
     const int first = (skip_io && np > 1 && ph[0].op_begin == ph[0].op_end && identity_store(ph[0])) ? 1 : 0;
     const int last = (skip_io && np - 1 > first && ph[np - 1].op_begin == ph[np - 1].op_end && identity_store(ph[np - 2]))
                          ? np - 2
@@ -532,11 +535,16 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
             }
         }
         const bool merge = tuning().jit_merge_diag != 0 && scal.size() >= 2;
+        int emitted = 0;
         for (int o = cur.op_begin; o < cur.op_end; ++o) {
             if (merge && std::find(scal.begin(), scal.end(), o) != scal.end()) {
                 continue;
             }
+            if (fence_every > 0 && emitted > 0 && emitted % fence_every == 0) {
+                s += "        kt_jit_fence(v);\n";
+            }
             jit_emit_op(s, plan.ops[static_cast<size_t>(o)], o - fb.op_begin);
+            ++emitted;
         }
         if (merge) {
             s += "        {\n            C fac = make_cx<double>(1, 0);\n";
@@ -601,7 +609,15 @@ std::vector<double> jit_block_mats(const Plan<double>& plan, size_t b)
 
 constexpr const char* JIT_PRELUDE =
     "#include \"kt_fused_dev.cuh\"\n\n"
-    "template <int N>\nstruct KtMats\n{\n    double m[N];\n};\n\n";
+    "template <int N>\nstruct KtMats\n{\n    double m[N];\n};\n\n"
+    "__device__ __forceinline__ void kt_jit_fence(double2 (&v)[16])\n{\n"
+    "    asm volatile(\"\" : \"+d\"(v[0].x), \"+d\"(v[0].y), \"+d\"(v[1].x), \"+d\"(v[1].y), \"+d\"(v[2].x), \"+d\"(v[2].y),\n"
+    "                 \"+d\"(v[3].x), \"+d\"(v[3].y), \"+d\"(v[4].x), \"+d\"(v[4].y), \"+d\"(v[5].x), \"+d\"(v[5].y),\n"
+    "                 \"+d\"(v[6].x), \"+d\"(v[6].y), \"+d\"(v[7].x), \"+d\"(v[7].y));\n"
+    "    asm volatile(\"\" : \"+d\"(v[8].x), \"+d\"(v[8].y), \"+d\"(v[9].x), \"+d\"(v[9].y), \"+d\"(v[10].x), \"+d\"(v[10].y),\n"
+    "                 \"+d\"(v[11].x), \"+d\"(v[11].y), \"+d\"(v[12].x), \"+d\"(v[12].y), \"+d\"(v[13].x), \"+d\"(v[13].y),\n"
+    "                 \"+d\"(v[14].x), \"+d\"(v[14].y), \"+d\"(v[15].x), \"+d\"(v[15].y));\n"
+    "}\n\n";
 
 struct JitCache
 {
@@ -1036,7 +1052,8 @@ int32_t jit_compile_only(int n, const std::vector<LGate>& gates, int64_t* n_kern
     std::vector<std::vector<std::string>> names(1);
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         const std::string name = "kt_jc" + std::to_string(b);
-        sources[0] += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(threads) + ", 1) " + name +
+        sources[0] += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(threads) + ", " +
+                      std::to_string(threads > 256 ? 1 : 2) + ") " + name +
                       jit_block_body(plan, b, RB) + "\n";
         names[0].push_back(name);
     }

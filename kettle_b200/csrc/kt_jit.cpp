@@ -15,6 +15,8 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -135,6 +137,16 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
         return KT_ERR_CUDA;
     }
     const size_t n = sources.size();
+    // KT_JIT_DUMP_DIR: also write each generated program's source there (for inspection)
+    if (const char* dir = std::getenv("KT_JIT_DUMP_DIR"); dir != nullptr && *dir != '\0') {
+        for (size_t i = 0; i < n; ++i) {
+            const std::string path = std::string(dir) + "/kt_jit_" + std::to_string(i) + ".cu";
+            if (FILE* f = std::fopen(path.c_str(), "w")) {
+                std::fwrite(sources[i].data(), 1, sources[i].size(), f);
+                std::fclose(f);
+            }
+        }
+    }
     std::vector<std::vector<char>> cubins(n);
     std::vector<std::string> errs(n);
     const size_t workers = std::max<size_t>(1, std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency())));

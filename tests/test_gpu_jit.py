@@ -123,3 +123,22 @@ def test_auto_mode_compiles_on_the_second_apply(engine, port):
     finally:
         for k, v in old.items():
             capi.tuning_set(k, v)
+
+
+@pytest.mark.parametrize("knobs", [
+    {"jit_merge_diag": 0}, {"jit_prefetch": 0}, {"jit_skip_io": 0}, {"jit_fence": 2},
+    {"fused_tile_bits": 11, "jit_ctas_per_sm": 3}, {"fused_tile_bits": 13},
+])
+def test_jit_variants_agree(jit, port, knobs):
+    # every generated-kernel variant computes the same state
+    old = {k: capi.tuning_get(k) for k in knobs}
+    try:
+        for k, v in knobs.items():
+            capi.tuning_set(k, v)
+        n = 18
+        g = W.random_layers(n, 4, seed=31, mixed=True)
+        init = random_state(n, 31)
+        assert np.abs(_apply(n, init, g) - port.apply(n, init, g)).max() < 1e-12
+    finally:
+        for k, v in old.items():
+            capi.tuning_set(k, v)
