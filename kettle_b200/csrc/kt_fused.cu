@@ -610,13 +610,11 @@ std::vector<double> jit_block_mats(const Plan<double>& plan, size_t b)
 constexpr const char* JIT_PRELUDE =
     "#include \"kt_fused_dev.cuh\"\n\n"
     "template <int N>\nstruct KtMats\n{\n    double m[N];\n};\n\n"
-    "__device__ __forceinline__ void kt_jit_fence(double2 (&v)[16])\n{\n"
-    "    asm volatile(\"\" : \"+d\"(v[0].x), \"+d\"(v[0].y), \"+d\"(v[1].x), \"+d\"(v[1].y), \"+d\"(v[2].x), \"+d\"(v[2].y),\n"
-    "                 \"+d\"(v[3].x), \"+d\"(v[3].y), \"+d\"(v[4].x), \"+d\"(v[4].y), \"+d\"(v[5].x), \"+d\"(v[5].y),\n"
-    "                 \"+d\"(v[6].x), \"+d\"(v[6].y), \"+d\"(v[7].x), \"+d\"(v[7].y));\n"
-    "    asm volatile(\"\" : \"+d\"(v[8].x), \"+d\"(v[8].y), \"+d\"(v[9].x), \"+d\"(v[9].y), \"+d\"(v[10].x), \"+d\"(v[10].y),\n"
-    "                 \"+d\"(v[11].x), \"+d\"(v[11].y), \"+d\"(v[12].x), \"+d\"(v[12].y), \"+d\"(v[13].x), \"+d\"(v[13].y),\n"
-    "                 \"+d\"(v[14].x), \"+d\"(v[14].y), \"+d\"(v[15].x), \"+d\"(v[15].y));\n"
+    "template <int N>\n__device__ __forceinline__ void kt_jit_fence(double2 (&v)[N])\n{\n"
+    "#pragma unroll\n"
+    "    for (int i = 0; i < N; ++i) {\n"
+    "        asm volatile(\"\" : \"+d\"(v[i].x), \"+d\"(v[i].y));\n"
+    "    }\n"
     "}\n\n";
 
 struct JitCache
@@ -792,10 +790,14 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
         std::vector<const void*> jk;
         // the generated kernels keep only the tile in shared memory, so they may
         // run jit_ctas_per_sm CTAs per SM (register budget 65536 / (threads * CTAs))
-        const int jit_minb = (shape == 0) ? 1 : (shape == 1 ? 1 : std::max(2, std::min(4, tuning().jit_ctas_per_sm)));
+        int jit_minb = 1;
+        if (shape == 2) {
+            jit_minb = std::max(2, std::min(4, tuning().jit_ctas_per_sm));
+        } else if (shape == 3 || shape == 4) {
+            jit_minb = fused_ctas(shape);
+        }
         const uint64_t jit_grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * jit_minb);
-        if (want && !rb3 &&
-            jit_kernels(plan, Cfg<T>::RB, threads, jit_minb, fused_smem_limit(shape), mode == 2, jk)) {
+        if (want && jit_kernels(plan, rb3 ? Cfg3::RB : Cfg<T>::RB, threads, jit_minb, fused_smem_limit(shape), mode == 2, jk)) {
             void* a = s.amps;
             unsigned long long nt = n_tiles;
             const size_t smem = (size_t {1} << K) * sizeof(C);
