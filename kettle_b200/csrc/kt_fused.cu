@@ -617,6 +617,9 @@ constexpr const char* JIT_PRELUDE =
     "    }\n"
     "}\n\n";
 
+constexpr size_t JIT_MAX_KERNELS = 4096;
+constexpr size_t JIT_MAX_SEEN = 65536;
+
 struct JitCache
 {
     std::mutex m;
@@ -657,6 +660,25 @@ bool jit_kernels(const Plan<double>& plan, int RB, int threads, int minb, int sm
             first_of[keys[b]] = b;
             missing.push_back(b);
         }
+    }
+    // bounded memory: past JIT_MAX_KERNELS cached kernels (or JIT_MAX_SEEN plans
+    // remembered), start over; the launches of this stream that used the old
+    // kernels are ordered before the unload, which waits for the device
+    if (jc.kernels.size() + missing.size() > JIT_MAX_KERNELS) {
+        cudaDeviceSynchronize();
+        jit_unload_all();
+        jc.kernels.clear();
+        missing.clear();
+        first_of.clear();
+        for (size_t b = 0; b < nb; ++b) {
+            if (first_of.count(keys[b]) == 0) {
+                first_of[keys[b]] = b;
+                missing.push_back(b);
+            }
+        }
+    }
+    if (jc.seen.size() > JIT_MAX_SEEN) {
+        jc.seen.clear();
     }
     if (!missing.empty() && on_repeat) {
         std::string all;

@@ -139,6 +139,8 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
                     std::vector<std::vector<const void*>>& kernels, bool load = true);
 // host-only: plan a complex128 apply and compile its block kernels without loading them
 int32_t jit_compile_only(int n, const std::vector<LGate>& gates, int64_t* n_kernels);
+// unload every program jit_compile loaded (their kernels become invalid)
+void jit_unload_all();
 // kernels compiled so far, block launches through them, and whether compiling failed
 void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed);
 // host-only: what the fused planner makes of a gate stream

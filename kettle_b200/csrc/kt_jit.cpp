@@ -128,6 +128,21 @@ bool jit_available(std::string* why)
     return L.ok;
 }
 
+namespace
+{
+std::mutex g_libs_mutex;
+std::vector<cudaLibrary_t> g_libs;  // every loaded program, until jit_unload_all
+}  // namespace
+
+void jit_unload_all()
+{
+    std::lock_guard<std::mutex> lock(g_libs_mutex);
+    for (cudaLibrary_t lib : g_libs) {
+        cudaLibraryUnload(lib);
+    }
+    g_libs.clear();
+}
+
 int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<std::vector<std::string>>& names,
                     std::vector<std::vector<const void*>>& kernels, bool load)
 {
@@ -182,12 +197,15 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
         }
         cudaLibrary_t lib = nullptr;
         KT_CUDA(cudaLibraryLoadData(&lib, cubins[i].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+        {
+            std::lock_guard<std::mutex> lock(g_libs_mutex);
+            g_libs.push_back(lib);
+        }
         for (const auto& name : names[i]) {
             cudaKernel_t k = nullptr;
             KT_CUDA(cudaLibraryGetKernel(&k, lib, name.c_str()));
             kernels[i].push_back(reinterpret_cast<const void*>(k));
         }
-        // the library stays loaded for the life of the process (its kernels are cached)
     }
     return KT_OK;
 }
