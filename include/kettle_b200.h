@@ -148,7 +148,7 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               shared-memory transpose (1) or run as ops (0)
  *   c64_renormalize    0 or 1   complex64 applies rescale every fused block to the
  *                               norm the state had when the apply began (1)
- *   fused_jit          0, 1, 2  complex128 fused blocks as kernels compiled at run
+ *   fused_jit          0, 1, 2  fused blocks as kernels compiled at run
  *                               time (NVRTC, cached per block structure: gate bodies
  *                               as straight-line code, every slot and mask a
  *                               constant): 0 never, 1 always, 2 (default) from the
@@ -166,10 +166,10 @@ int32_t kt_tuning_get(const char* name, int64_t* value);
 /* Run-time compiled block kernels so far, fused-block launches through them,
  * and 1 if run-time compilation was unavailable or failed (new). */
 int32_t kt_jit_stats(int64_t* kernels_compiled, int64_t* block_launches, int32_t* failed);
-/* Host-only: plan a complex128 apply of n_qubits and compile its block kernels
+/* Host-only: plan an apply of n_qubits in `dtype` and compile its block kernels
  * with NVRTC without loading them (no GPU needed); n_kernels = blocks compiled. */
-int32_t kt_jit_compile_only(int32_t n_qubits, const kt_gate* gates, int64_t n_gates, const double* params,
-                            int64_t n_params, int64_t* n_kernels);
+int32_t kt_jit_compile_only(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates,
+                            const double* params, int64_t n_params, int64_t* n_kernels);
 
 /* ---- statevector handle --------------------------------------------------
  * A statevector of n qubits lives on the current CUDA device as 2^n amplitudes,

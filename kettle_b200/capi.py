@@ -60,7 +60,7 @@ _SIGS = {
     "kt_tuning_set": ([C.c_char_p, I64], I32),
     "kt_tuning_get": ([C.c_char_p, C.POINTER(I64)], I32),
     "kt_jit_stats": ([P, P, P], I32),
-    "kt_jit_compile_only": ([I32, P, I64, P, I64, P], I32),
+    "kt_jit_compile_only": ([I32, I32, P, I64, P, I64, P], I32),
     "kt_sv_create": ([I32, I32, C.POINTER(P)], I32),
     "kt_sv_wrap": ([P, I32, I32, C.POINTER(P)], I32),
     "kt_sv_destroy": ([P], I32),
@@ -166,12 +166,12 @@ def jit_stats() -> dict:
     return {"kernels": int(k.value), "launches": int(l.value), "failed": bool(f.value)}
 
 
-def jit_compile_only(n_qubits: int, gates: np.ndarray, params: np.ndarray | None = None) -> int:
-    """Host-only: compile the run-time block kernels of a complex128 apply (no GPU); returns the block count."""
+def jit_compile_only(n_qubits: int, gates: np.ndarray, params: np.ndarray | None = None, dtype: int = KT_C128) -> int:
+    """Host-only: compile the run-time block kernels of an apply (no GPU); returns the block count."""
     g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
     p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
     k = I64(0)
-    check(lib().kt_jit_compile_only(n_qubits, ptr(g), g.size, ptr(p), 0 if p is None else p.size, C.byref(k)))
+    check(lib().kt_jit_compile_only(n_qubits, dtype, ptr(g), g.size, ptr(p), 0 if p is None else p.size, C.byref(k)))
     return int(k.value)
 
 

@@ -180,18 +180,21 @@ int32_t kt_tuning_get(const char* name, int64_t* value)
     return KT_OK;
 }
 
-int32_t kt_jit_compile_only(int32_t n_qubits, const kt_gate* gates, int64_t n_gates, const double* params,
-                            int64_t n_params, int64_t* n_kernels)
+int32_t kt_jit_compile_only(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates,
+                            const double* params, int64_t n_params, int64_t* n_kernels)
 {
     return guard([&]() -> int32_t {
         if (n_kernels == nullptr || n_gates < 0 || (n_gates > 0 && gates == nullptr)) {
             return invalid("bad arguments");
         }
+        if (const int32_t rc = check_dtype(dtype); rc != KT_OK) {
+            return rc;
+        }
         std::vector<kt::LGate> lg;
         if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, n_qubits, lg); rc != KT_OK) {
             return rc;
         }
-        return kt::jit_compile_only(n_qubits, lg, n_kernels);
+        return kt::jit_compile_only(n_qubits, dtype, lg, n_kernels);
     });
 }
 

@@ -28,6 +28,7 @@
 //    each warp instruction touches whole 128-byte lines.
 #include <algorithm>
 #include <cstdio>
+#include <map>
 #include <mutex>
 #include <string>
 #include <type_traits>
@@ -110,25 +111,6 @@ __global__ void KT_FUSED_BOUNDS(MINB) k_fused(typename CxT<T>::type* __restrict_
 // |a|^2 that the first block takes over what it loads).  Each launch leaves,
 // per CTA, the FP64 sum of |a|^2 over what it stored; the next launch scales
 // its loads by sqrt(target / that), and a last short pass scales the result.
-struct NormArgs
-{
-    const double* target;  // per-CTA target sums (nullptr in the first block)
-    const double* prev;    // per-CTA sums left by the previous block (nullptr in the first block)
-    int n_parts;
-    double* in_parts;      // first block: per-CTA sums over the loads (the target)
-    double* out_parts;     // per-CTA sums over the stores
-};
-
-__device__ __forceinline__ double norm_scale(const double* target, const double* prev, int n)
-{
-    double num = 0.0, den = 0.0;
-    for (int i = 0; i < n; ++i) {
-        num += target[i];
-        den += prev[i];
-    }
-    return (num > 0.0 && den > 0.0) ? sqrt(num / den) : 1.0;
-}
-
 template <typename T, int MINB>
 __global__ void KT_FUSED_BOUNDS(MINB) k_fused_norm(typename CxT<T>::type* __restrict__ a,
                                                        const FBlock* __restrict__ blk,
@@ -316,7 +298,14 @@ std::string jit_hex(uint64_t v)
     return b;
 }
 
-void jit_emit_op(std::string& s, const FOp<double>& op, int j)
+// asynchronous tile loads need a second tile buffer; only where both fit a CTA
+inline bool jit_async(int K, size_t elem_bytes)
+{
+    return tuning().jit_async_load != 0 && 2 * (size_t {1} << K) * elem_bytes <= 227 * 1024;
+}
+
+template <typename T>
+void jit_emit_op(std::string& s, const FOp<T>& op, int j)
 {
     const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
     auto run = [&](int ts) {
@@ -325,7 +314,7 @@ void jit_emit_op(std::string& s, const FOp<double>& op, int j)
     };
     // the op's matrix entries: the kernel's constant-bank parameter
     auto m = [&](int e) { return "M.m[" + std::to_string(8 * j + e) + "]"; };
-    auto cx = [&](int e) { return "make_cx<double>(" + m(e) + ", " + m(e + 1) + ")"; };
+    auto cx = [&](int e) { return "make_cx<$T>(" + m(e) + ", " + m(e + 1) + ")"; };
     std::string guard;
     if (op.cglob != 0) {
         guard += "if ((base & " + jit_hex(op.cglob) + ") == " + jit_hex(op.cglob) + ") ";
@@ -336,24 +325,24 @@ void jit_emit_op(std::string& s, const FOp<double>& op, int j)
     s += "        " + guard + "{\n            ";
     switch (op.kind) {
         case OP_GEN:
-            s += "GenF<double, RB> f {v, " + cx(0) + ", " + cx(2) + ", " + cx(4) + ", " + cx(6) + "}; " + run(op.tslot);
+            s += "GenF<$T, RB> f {v, " + cx(0) + ", " + cx(2) + ", " + cx(4) + ", " + cx(6) + "}; " + run(op.tslot);
             break;
         case OP_GENR:
-            s += "GenRF<double, RB> f {v, " + m(0) + ", " + m(2) + ", " + m(4) + ", " + m(6) + "}; " + run(op.tslot);
+            s += "GenRF<$T, RB> f {v, " + m(0) + ", " + m(2) + ", " + m(4) + ", " + m(6) + "}; " + run(op.tslot);
             break;
         case OP_RXL:
-            s += "RxF<double, RB> f {v, " + m(0) + ", " + m(3) + "}; " + run(op.tslot);
+            s += "RxF<$T, RB> f {v, " + m(0) + ", " + m(3) + "}; " + run(op.tslot);
             break;
         case OP_ANTI:
-            s += "AntiF<double, RB, false> f {v, " + cx(2) + ", " + cx(4) + "}; " + run(op.tslot);
+            s += "AntiF<$T, RB, false> f {v, " + cx(2) + ", " + cx(4) + "}; " + run(op.tslot);
             break;
         case OP_SWAP:
-            s += "AntiF<double, RB, true> f {v, make_cx<double>(1, 0), make_cx<double>(1, 0)}; " + run(op.tslot);
+            s += "AntiF<$T, RB, true> f {v, make_cx<$T>(1, 0), make_cx<$T>(1, 0)}; " + run(op.tslot);
             break;
         default: {
             const bool one = (op.kind == OP_DIAG1);
             if (op.tslot != NO_SLOT) {
-                s += std::string("DiagRegF<double, RB, ") + (one ? "true" : "false") + "> f {v, " + cx(0) + ", " + cx(6) +
+                s += std::string("DiagRegF<$T, RB, ") + (one ? "true" : "false") + "> f {v, " + cx(0) + ", " + cx(6) +
                      "}; " + run(op.tslot);
             } else {
                 std::string b = "false";
@@ -366,7 +355,7 @@ void jit_emit_op(std::string& s, const FOp<double>& op, int j)
                 }
                 s += "const bool b = " + b + "; ";
                 s += one ? "if (b) " : "";
-                s += "{ DiagAllF<double, RB> f {v, b ? " + cx(6) + " : " + cx(0) + "}; " + run(0) + " }";
+                s += "{ DiagAllF<$T, RB> f {v, b ? " + cx(6) + " : " + cx(0) + "}; " + run(0) + " }";
             }
             break;
         }
@@ -417,7 +406,8 @@ std::string jit_xor_terms(const uint32_t* terms, int nbits, uint32_t start)
 // with the layout of every phase written out as constants (tile base, thread
 // and register offsets, swizzled shared-memory terms) and the gate bodies as
 // straight-line code; matrices arrive in the constant-bank parameter M.
-std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
+template <typename T>
+std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
 {
     const FBlock& fb = plan.blocks[b];
     const int TB = fb.K - RB;
@@ -449,16 +439,24 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
     };
     std::string s;
     s.reserve(32768);
-    s += "(void* a_, unsigned long long n_tiles, const __grid_constant__ KtMats<" + std::to_string(8 * nops) + "> M)\n{\n";
-    s += "    using namespace kt;\n    using C = double2;\n";
+    s += std::string("(void* a_, unsigned long long n_tiles, ") + (norm ? "kt::NormArgs na, " : "") +
+         "const __grid_constant__ $M<" + std::to_string(8 * nops) + "> M)\n{\n";
+    s += "    using namespace kt;\n    using C = $C;\n";
     s += "    constexpr int RB = " + std::to_string(RB) + ";\n";
     s += "    C* __restrict__ a = static_cast<C*>(a_);\n";
     s += "    extern __shared__ __align__(16) unsigned char smem_raw[];\n";
     s += "    C* sm = reinterpret_cast<C*>(smem_raw);\n";
     s += "    const uint32_t t = threadIdx.x;\n";
-    s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
-    s += "        C v[1 << RB];\n";
-    s += "        const uint64_t base = " + jit_deposit("tile", free_strides.data(), fb.nfree) + ";\n";
+    if (norm) {
+        // renormalisation (complex64): per-warp FP64 sums of |a|^2 over the
+        // loads (first block: the target) and the stores, loads scaled by
+        // sqrt(target / what the previous block stored)
+        s += "    __shared__ double w_in[16], w_out[16];\n    __shared__ float scale_sh;\n";
+        s += "    if (t == 0) {\n        scale_sh = (na.prev != nullptr) ? static_cast<float>(norm_scale(na.target, na.prev, "
+             "na.n_parts)) : 1.0f;\n    }\n";
+        s += "    if (t < 16) {\n        w_in[t] = 0.0;\n        w_out[t] = 0.0;\n    }\n    __syncthreads();\n";
+        s += "    const float sc = scale_sh;\n";
+    }
     // A block's first phase may only set up the coalesced load layout (no ops,
     // no permutation to apply) and its last one only the store layout; then
     // the tile is loaded straight into the second phase's layout, or stored
@@ -488,12 +486,50 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
     const int last = (skip_io && np - 1 > first && ph[np - 1].op_begin == ph[np - 1].op_end && identity_store(ph[np - 2]))
                          ? np - 2
                          : np - 1;
-    s += "        {\n            const C* src = a + base + " + jit_deposit("t", ph[first].tstride, TB) + ";\n";
-    for (int i = 0; i < R; ++i) {
-        s += "            v[" + std::to_string(i) + "] = src[" + std::to_string(reg_off(ph[first], i)) + "ULL];\n";
+    // jit_async_load: each thread copies its next tile's amplitudes (in the
+    // first layout) into its own slots of a second shared-memory buffer with
+    // cp.async while the current tile computes; no other thread touches those
+    // slots, so a wait_group is the only synchronisation.
+    const bool async_load = jit_async(fb.K, sizeof(typename CxT<T>::type));
+    const int n_thr = 1 << TB;
+    auto issue_async = [&](const std::string& tile_expr, const std::string& indent) {
+        std::string e;
+        e += indent + "{\n" + indent + "    const C* src = a + " + jit_deposit(tile_expr, free_strides.data(), fb.nfree) +
+             " + " + jit_deposit("t", ph[first].tstride, TB) + ";\n";
+        e += indent + "    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sb + t));\n";
+        for (int i = 0; i < R; ++i) {
+            e += indent + "    asm volatile(\"cp.async.cg.shared.global [%0], [%1], 16;\" :: \"r\"(dst + " +
+                 std::to_string(16 * i * n_thr) + "u), \"l\"(src + " + std::to_string(reg_off(ph[first], i)) + "ULL) : \"memory\");\n";
+        }
+        e += indent + "}\n";
+        return e;
+    };
+    if (async_load) {
+        s += "    C* sb = sm + " + std::to_string(1 << fb.K) + ";\n";
+        s += "    if (static_cast<unsigned long long>(blockIdx.x) < n_tiles) {\n";
+        s += issue_async("static_cast<unsigned long long>(blockIdx.x)", "        ");
+        s += "    }\n    asm volatile(\"cp.async.commit_group;\" ::: \"memory\");\n";
     }
-    s += "        }\n";
-    if (tuning().jit_prefetch != 0) {
+    s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
+    s += "        C v[1 << RB];\n";
+    s += "        const uint64_t base = " + jit_deposit("tile", free_strides.data(), fb.nfree) + ";\n";
+    if (async_load) {
+        s += "        asm volatile(\"cp.async.wait_group 0;\" ::: \"memory\");\n";
+        for (int i = 0; i < R; ++i) {
+            s += "        v[" + std::to_string(i) + "] = sb[" + std::to_string(i * n_thr) + "u + t];\n";
+        }
+    } else {
+        s += "        {\n            const C* src = a + base + " + jit_deposit("t", ph[first].tstride, TB) + ";\n";
+        for (int i = 0; i < R; ++i) {
+            s += "            v[" + std::to_string(i) + "] = src[" + std::to_string(reg_off(ph[first], i)) + "ULL];\n";
+        }
+        s += "        }\n";
+    }
+    if (norm) {
+        s += "        if (na.in_parts != nullptr) {\n            warp_norm_add<float>(v, w_in, t);\n        }\n";
+        s += "#pragma unroll\n        for (int i = 0; i < (1 << RB); ++i) {\n            v[i].x *= sc;\n            v[i].y *= sc;\n        }\n";
+    }
+    if (tuning().jit_prefetch != 0 && !async_load) {
         // the next tile of this CTA into L2 while this one computes: one
         // prefetch per 128-byte line when the lowest qubits are the low lanes
         const bool lines_on_lanes = TB >= 3 && ph[first].tstride[0] == 1 && ph[first].tstride[1] == 2 &&
@@ -529,7 +565,7 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
         // applied once, at the phase's end.
         std::vector<int> scal;
         for (int o = cur.op_begin; o < cur.op_end; ++o) {
-            const FOp<double>& op = plan.ops[static_cast<size_t>(o)];
+            const FOp<T>& op = plan.ops[static_cast<size_t>(o)];
             if ((op.kind == OP_DIAG || op.kind == OP_DIAG1) && op.tslot == NO_SLOT && op.cslot == NO_SLOT) {
                 scal.push_back(o);
             }
@@ -547,12 +583,12 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
             ++emitted;
         }
         if (merge) {
-            s += "        {\n            C fac = make_cx<double>(1, 0);\n";
+            s += "        {\n            C fac = make_cx<$T>(1, 0);\n";
             for (const int o : scal) {
-                const FOp<double>& op = plan.ops[static_cast<size_t>(o)];
+                const FOp<T>& op = plan.ops[static_cast<size_t>(o)];
                 const int j = o - fb.op_begin;
                 auto cx = [&](int e) {
-                    return "make_cx<double>(M.m[" + std::to_string(8 * j + e) + "], M.m[" + std::to_string(8 * j + e + 1) + "])";
+                    return "make_cx<$T>(M.m[" + std::to_string(8 * j + e) + "], M.m[" + std::to_string(8 * j + e + 1) + "])";
                 };
                 std::string cond;
                 if (op.cglob != 0) {
@@ -581,25 +617,52 @@ std::string jit_block_body(const Plan<double>& plan, size_t b, int RB)
                     s += "fac = cmul(fac, b ? " + cx(6) + " : " + cx(0) + "); }\n";
                 }
             }
-            s += "            DiagAllF<double, RB> f {v, fac}; f.template run<0, -1>();\n        }\n";
+            s += "            DiagAllF<$T, RB> f {v, fac}; f.template run<0, -1>();\n        }\n";
+        }
+        if (async_load && p == first) {
+            // this thread's slots were read at the top of the tile; refill them
+            s += "        if (tile + gridDim.x < n_tiles) {\n";
+            s += issue_async("(tile + gridDim.x)", "            ");
+            s += "        }\n        asm volatile(\"cp.async.commit_group;\" ::: \"memory\");\n";
         }
     }
     s += "        {\n            C* dst = a + base + " + jit_deposit("t", ph[last].tstride, TB) + ";\n";
     for (int i = 0; i < R; ++i) {
         s += "            dst[" + std::to_string(reg_off(ph[last], i)) + "ULL] = v[" + std::to_string(i) + "];\n";
     }
-    s += "        }\n    }\n}\n";
+    s += "        }\n";
+    if (norm) {
+        s += "        warp_norm_add<float>(v, w_out, t);\n";
+    }
+    s += "    }\n";
+    if (norm) {
+        s += "    __syncthreads();\n    if (t == 0) {\n        double so = 0.0, si = 0.0;\n";
+        s += "        for (int w = 0; w < 16; ++w) {\n            so += w_out[w];\n            si += w_in[w];\n        }\n";
+        s += "        na.out_parts[blockIdx.x] = so;\n        if (na.in_parts != nullptr) {\n            na.in_parts[blockIdx.x] = si;\n        }\n    }\n";
+    }
+    s += "}\n";
+    // the precision's type names
+    const bool f32 = std::is_same<T, float>::value;
+    auto subst = [&](const std::string& from, const std::string& to) {
+        for (size_t at = s.find(from); at != std::string::npos; at = s.find(from, at + to.size())) {
+            s.replace(at, from.size(), to);
+        }
+    };
+    subst("$T", f32 ? "float" : "double");
+    subst("$C", f32 ? "float2" : "double2");
+    subst("$M", f32 ? "KtMatsF" : "KtMats");
     return s;
 }
 
 // the matrices of block b's ops, in the layout of its kernel's parameter M
-std::vector<double> jit_block_mats(const Plan<double>& plan, size_t b)
+template <typename T>
+std::vector<T> jit_block_mats(const Plan<T>& plan, size_t b)
 {
     const FBlock& fb = plan.blocks[b];
     const int nops = std::max(1, fb.op_end - fb.op_begin);
-    std::vector<double> m(static_cast<size_t>(8 * nops), 0.0);
+    std::vector<T> m(static_cast<size_t>(8 * nops), T(0));
     for (int j = 0; j < fb.op_end - fb.op_begin; ++j) {
-        const FOp<double>& op = plan.ops[static_cast<size_t>(fb.op_begin + j)];
+        const FOp<T>& op = plan.ops[static_cast<size_t>(fb.op_begin + j)];
         for (int e = 0; e < 8; ++e) {
             m[static_cast<size_t>(8 * j + e)] = op.m[e];
         }
@@ -610,10 +673,17 @@ std::vector<double> jit_block_mats(const Plan<double>& plan, size_t b)
 constexpr const char* JIT_PRELUDE =
     "#include \"kt_fused_dev.cuh\"\n\n"
     "template <int N>\nstruct KtMats\n{\n    double m[N];\n};\n\n"
+    "template <int N>\nstruct KtMatsF\n{\n    float m[N];\n};\n\n"
     "template <int N>\n__device__ __forceinline__ void kt_jit_fence(double2 (&v)[N])\n{\n"
     "#pragma unroll\n"
     "    for (int i = 0; i < N; ++i) {\n"
     "        asm volatile(\"\" : \"+d\"(v[i].x), \"+d\"(v[i].y));\n"
+    "    }\n"
+    "}\n\n"
+    "template <int N>\n__device__ __forceinline__ void kt_jit_fence(float2 (&v)[N])\n{\n"
+    "#pragma unroll\n"
+    "    for (int i = 0; i < N; ++i) {\n"
+    "        asm volatile(\"\" : \"+f\"(v[i].x), \"+f\"(v[i].y));\n"
     "    }\n"
     "}\n\n";
 
@@ -625,6 +695,7 @@ struct JitCache
     std::mutex m;
     std::unordered_map<std::string, const void*> kernels;  // launch-bounds prefix + body -> kernel
     std::unordered_set<size_t> seen;                       // plans applied once with the precompiled kernels
+    std::map<std::pair<const void*, int>, int> smem_set;   // (kernel, device) -> shared-memory limit set
     int64_t compiled {0};
     int64_t launches {0};
     bool failed {false};
@@ -640,7 +711,8 @@ JitCache& jit_cache()
 // false when the precompiled kernels should run instead: run-time compilation
 // is unavailable or failed, or (`on_repeat`) the plan is new to this process,
 // so compiling waits for its second apply.
-bool jit_kernels(const Plan<double>& plan, int RB, int threads, int minb, int smem_bytes, bool on_repeat,
+template <typename T>
+bool jit_kernels(const Plan<T>& plan, int RB, int threads, int minb, int smem_bytes, bool on_repeat, bool norm,
                  std::vector<const void*>& out)
 {
     JitCache& jc = jit_cache();
@@ -655,7 +727,7 @@ bool jit_kernels(const Plan<double>& plan, int RB, int threads, int minb, int sm
     std::vector<size_t> missing;
     std::unordered_map<std::string, size_t> first_of;
     for (size_t b = 0; b < nb; ++b) {
-        keys[b] = bounds + jit_block_body(plan, b, RB);
+        keys[b] = bounds + jit_block_body<T>(plan, b, RB, norm);
         if (jc.kernels.count(keys[b]) == 0 && first_of.count(keys[b]) == 0) {
             first_of[keys[b]] = b;
             missing.push_back(b);
@@ -668,6 +740,7 @@ bool jit_kernels(const Plan<double>& plan, int RB, int threads, int minb, int sm
         cudaDeviceSynchronize();
         jit_unload_all();
         jc.kernels.clear();
+        jc.smem_set.clear();
         missing.clear();
         first_of.clear();
         for (size_t b = 0; b < nb; ++b) {
@@ -705,25 +778,116 @@ bool jit_kernels(const Plan<double>& plan, int RB, int threads, int minb, int sm
         std::vector<std::vector<const void*>> got;
         if (jit_compile(sources, names, got, true) != KT_OK) {
             jc.failed = true;
+            cudaGetLastError();  // the precompiled kernels' launch check must not see this failure
             return false;
         }
         for (size_t w = 0; w < workers; ++w) {
             for (size_t k = 0; k < names[w].size(); ++k) {
-                const void* fn = got[w][k];
-                if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes) != cudaSuccess) {
-                    set_error(KT_ERR_CUDA, "cudaFuncSetAttribute on a run-time compiled block kernel failed");
-                    jc.failed = true;
-                    return false;
-                }
-                jc.kernels[keys[owner[w][k]]] = fn;
+                jc.kernels[keys[owner[w][k]]] = got[w][k];
             }
         }
         jc.compiled += static_cast<int64_t>(missing.size());
     }
+    // the libraries load for every device, but a kernel's shared-memory limit is
+    // per device: set it on the current one the first time a kernel runs there
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        dev = 0;
+    }
     out.resize(nb);
     for (size_t b = 0; b < nb; ++b) {
-        out[b] = jc.kernels[keys[b]];
+        const void* fn = jc.kernels[keys[b]];
+        const auto key = std::make_pair(fn, dev);
+        auto it = jc.smem_set.find(key);
+        if (it == jc.smem_set.end() || it->second < smem_bytes) {
+            if (cudaKernelSetAttributeForDevice(reinterpret_cast<cudaKernel_t>(const_cast<void*>(fn)),
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes,
+                                                dev) != cudaSuccess) {
+                // this configuration does not fit: the precompiled kernels run it
+                // (and the runtime's last-error slot is cleared for their launch check)
+                cudaGetLastError();
+                return false;
+            }
+            jc.smem_set[key] = smem_bytes;
+        }
+        out[b] = fn;
     }
+    return true;
+}
+
+// The launch of a plan's blocks as run-time compiled kernels, or false when
+// the caller should run the precompiled ones: fused_jit = 1 always; 2 from
+// the second apply of a plan on states of at least jit_min_qubits qubits
+// (where a pass is long enough to repay the compile, about half a second per
+// block kernel on one host thread).  With `parts` (complex64
+// renormalisation: target | out even | out odd, n_parts per-CTA sums each)
+// every block gets its NormArgs and the caller finishes with k_norm_final.
+template <typename T>
+bool jit_launch(State& s, const Plan<T>& plan, int K, bool rb3, int threads, int shape, double* parts, int32_t* rc,
+                int* n_parts_out)
+{
+    using C = typename CxT<T>::type;
+    *rc = KT_OK;
+    const int n = s.n_bits;
+    const int mode = tuning().fused_jit;
+    const bool want = mode == 1 || (mode == 2 && n >= tuning().jit_min_qubits);
+    if (!want) {
+        return false;
+    }
+    // the generated kernels keep only the tile in shared memory, so they may
+    // run jit_ctas_per_sm CTAs per SM (register budget 65536 / (threads * CTAs))
+    int minb = 1;
+    if (shape == 2) {
+        minb = std::max(2, std::min(4, tuning().jit_ctas_per_sm));
+    } else if (shape == 3 || shape == 4) {
+        minb = fused_ctas(shape);
+    }
+    const uint64_t n_tiles = uint64_t {1} << (n - K);
+    const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * minb);
+    const size_t smem = (size_t {1} << K) * sizeof(C) * (jit_async(K, sizeof(C)) ? 2 : 1);
+    const int smem_attr = std::max(fused_smem_limit(shape), static_cast<int>(smem));
+    const int RB = rb3 ? Cfg3::RB : Cfg<T>::RB;
+    const bool norm = parts != nullptr;
+    if (norm && grid > static_cast<uint64_t>(*n_parts_out)) {
+        return false;  // the caller reserved per-CTA sums for fewer CTAs
+    }
+    std::vector<const void*> jk;
+    if (!jit_kernels<T>(plan, RB, threads, minb, smem_attr, mode == 2, norm, jk)) {
+        return false;
+    }
+    void* a = s.amps;
+    unsigned long long nt = n_tiles;
+    const int np = static_cast<int>(grid);
+    double* target = parts;
+    double* out[2] = {norm ? parts + np : nullptr, norm ? parts + 2 * np : nullptr};
+    const double pass_bytes = 2.0 * static_cast<double>(sizeof(C)) * static_cast<double>(s.n_amps());
+    for (size_t b = 0; b < plan.blocks.size(); ++b) {
+        std::vector<T> mats = jit_block_mats<T>(plan, b);
+        cudaError_t e = cudaSuccess;
+        if (norm) {
+            NormArgs na {};
+            na.n_parts = np;
+            na.target = (b == 0) ? nullptr : target;
+            na.prev = (b == 0) ? nullptr : out[(b - 1) & 1];
+            na.in_parts = (b == 0) ? target : nullptr;
+            na.out_parts = out[b & 1];
+            void* args[] = {&a, &nt, &na, mats.data()};
+            e = cudaLaunchKernel(jk[b], dim3(static_cast<unsigned>(grid)), dim3(static_cast<unsigned>(threads)), args,
+                                 smem, s.stream);
+        } else {
+            void* args[] = {&a, &nt, mats.data()};
+            e = cudaLaunchKernel(jk[b], dim3(static_cast<unsigned>(grid)), dim3(static_cast<unsigned>(threads)), args,
+                                 smem, s.stream);
+        }
+        if (e != cudaSuccess) {
+            *rc = cuda_fail(e, "cudaLaunchKernel(run-time compiled block)");
+            return true;
+        }
+        s.last_launches += 1;
+        s.last_alg_bytes += pass_bytes;
+    }
+    *n_parts_out = np;
+    jit_cache().launches += static_cast<int64_t>(plan.blocks.size());
     return true;
 }
 
@@ -777,6 +941,29 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     }
     if constexpr (std::is_same<T, float>::value) {
         if (tuning().c64_renormalize != 0) {
+            // compiled blocks keep the renormalisation: per-CTA sums for up to
+            // 4 CTAs per SM, then the closing rescale
+            const int max_parts = sm_count() * 4;
+            if (const int32_t rc = s.scratch2.reserve(3 * static_cast<size_t>(max_parts) * sizeof(double)); rc != KT_OK) {
+                return rc;
+            }
+            double* parts = static_cast<double*>(s.scratch2.ptr);
+            int32_t rc = KT_OK;
+            int n_parts = max_parts;
+            if (jit_launch<T>(s, plan, K, rb3, threads, shape, parts, &rc, &n_parts)) {
+                if (rc != KT_OK || plan.blocks.empty()) {
+                    return rc;
+                }
+                const unsigned fin_grid = static_cast<unsigned>(
+                    std::min<uint64_t>((s.n_amps() + 255) / 256, static_cast<uint64_t>(sm_count()) * 8));
+                k_norm_final<C><<<fin_grid, 256, 0, s.stream>>>(static_cast<C*>(s.amps), s.n_amps(), parts,
+                                                                parts + n_parts * (1 + ((plan.blocks.size() - 1) & 1)),
+                                                                n_parts);
+                KT_CHECK_LAUNCH("k_norm_final");
+                s.last_launches += 1;
+                s.last_alg_bytes += 2.0 * static_cast<double>(sizeof(C)) * static_cast<double>(s.n_amps());
+                return KT_OK;
+            }
             return run_fused_norm<T>(s, plan, d_blk, d_ph, d_ops, K, threads, shape);
         }
     }
@@ -803,37 +990,11 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     const uint64_t n_tiles = uint64_t {1} << (n - K);
     const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * fused_ctas(shape));
     const double pass_bytes = 2.0 * static_cast<double>(sizeof(C)) * static_cast<double>(s.n_amps());
-    if constexpr (std::is_same<T, double>::value) {
-        // fused_jit: 1 = always; 2 = from the second apply of a plan, on states of
-        // at least jit_min_qubits qubits (where a pass is long enough to repay
-        // the compile, about half a second per block kernel on one host thread)
-        const int mode = tuning().fused_jit;
-        const bool want = mode == 1 || (mode == 2 && n >= tuning().jit_min_qubits);
-        std::vector<const void*> jk;
-        // the generated kernels keep only the tile in shared memory, so they may
-        // run jit_ctas_per_sm CTAs per SM (register budget 65536 / (threads * CTAs))
-        int jit_minb = 1;
-        if (shape == 2) {
-            jit_minb = std::max(2, std::min(4, tuning().jit_ctas_per_sm));
-        } else if (shape == 3 || shape == 4) {
-            jit_minb = fused_ctas(shape);
-        }
-        const uint64_t jit_grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * jit_minb);
-        if (want && jit_kernels(plan, rb3 ? Cfg3::RB : Cfg<T>::RB, threads, jit_minb, fused_smem_limit(shape), mode == 2, jk)) {
-            void* a = s.amps;
-            unsigned long long nt = n_tiles;
-            const size_t smem = (size_t {1} << K) * sizeof(C);
-            const uint64_t grid = jit_grid;
-            for (size_t b = 0; b < plan.blocks.size(); ++b) {
-                std::vector<double> mats = jit_block_mats(plan, b);
-                void* args[] = {&a, &nt, mats.data()};
-                KT_CUDA(cudaLaunchKernel(jk[b], dim3(static_cast<unsigned>(grid)), dim3(static_cast<unsigned>(threads)),
-                                         args, smem, s.stream));
-                s.last_launches += 1;
-                s.last_alg_bytes += pass_bytes;
-            }
-            jit_cache().launches += static_cast<int64_t>(plan.blocks.size());
-            return KT_OK;
+    {
+        int32_t rc = KT_OK;
+        int n_parts = 0;
+        if (jit_launch<T>(s, plan, K, rb3, threads, shape, nullptr, &rc, &n_parts)) {
+            return rc;
         }
     }
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
@@ -1058,27 +1219,32 @@ int32_t adjoint_sweep_fused(State& psi, State& lam, const std::vector<AdjGate>& 
                                 : run_adjoint_sweep<float>(psi, lam, gates, dev_grad, work);
 }
 
-int32_t jit_compile_only(int n, const std::vector<LGate>& gates, int64_t* n_kernels)
+namespace
+{
+
+template <typename T>
+int32_t jit_compile_only_t(int n, const std::vector<LGate>& gates, int64_t* n_kernels)
 {
     *n_kernels = 0;
-    if (n < Cfg<double>::RB + 5 || gates.empty()) {
+    if (n < Cfg<T>::RB + 5 || gates.empty()) {
         return KT_OK;
     }
-    Plan<double> plan;
+    Plan<T> plan;
     int K = 0;
     bool rb3 = false;
-    if (const int32_t rc = fused_plan<double>(n, gates, plan, &K, &rb3); rc != KT_OK) {
+    if (const int32_t rc = fused_plan<T>(n, gates, plan, &K, &rb3); rc != KT_OK) {
         return rc;
     }
-    const int RB = rb3 ? Cfg3::RB : Cfg<double>::RB;
+    const int RB = rb3 ? Cfg3::RB : Cfg<T>::RB;
     const int threads = 1 << (K - RB);
+    // complex64 applies renormalise by default
+    const bool norm = std::is_same<T, float>::value && tuning().c64_renormalize != 0;
     std::vector<std::string> sources(1, JIT_PRELUDE);
     std::vector<std::vector<std::string>> names(1);
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         const std::string name = "kt_jc" + std::to_string(b);
         sources[0] += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(threads) + ", " +
-                      std::to_string(threads > 256 ? 1 : 2) + ") " + name +
-                      jit_block_body(plan, b, RB) + "\n";
+                      std::to_string(threads > 256 ? 1 : 2) + ") " + name + jit_block_body<T>(plan, b, RB, norm) + "\n";
         names[0].push_back(name);
     }
     std::vector<std::vector<const void*>> got;
@@ -1087,6 +1253,14 @@ int32_t jit_compile_only(int n, const std::vector<LGate>& gates, int64_t* n_kern
     }
     *n_kernels = static_cast<int64_t>(plan.blocks.size());
     return KT_OK;
+}
+
+}  // namespace
+
+int32_t jit_compile_only(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* n_kernels)
+{
+    return dtype == KT_C64 ? jit_compile_only_t<float>(n, gates, n_kernels)
+                           : jit_compile_only_t<double>(n, gates, n_kernels);
 }
 
 void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed)

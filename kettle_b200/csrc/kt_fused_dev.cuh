@@ -702,6 +702,25 @@ __device__ __forceinline__ C load_amp(const C* p)
 // One tile of a forward block: load it (or, with `init`, start from
 // |0...0>), run the block's phases with a shared-memory transpose between
 // them, store it.  The block, its phases and ops are already in shared memory.
+struct NormArgs
+{
+    const double* target;  // per-CTA target sums (nullptr in the first block)
+    const double* prev;    // per-CTA sums left by the previous block (nullptr in the first block)
+    int n_parts;
+    double* in_parts;      // first block: per-CTA sums over the loads (the target)
+    double* out_parts;     // per-CTA sums over the stores
+};
+
+__device__ __forceinline__ double norm_scale(const double* target, const double* prev, int n)
+{
+    double num = 0.0, den = 0.0;
+    for (int i = 0; i < n; ++i) {
+        num += target[i];
+        den += prev[i];
+    }
+    return (num > 0.0 && den > 0.0) ? sqrt(num / den) : 1.0;
+}
+
 // Norm bookkeeping of a renormalising apply (complex64): per-warp FP64 sums
 // of |a|^2 in shared memory, and the scale applied to every loaded amplitude.
 struct NormCtx

@@ -137,8 +137,8 @@ bool jit_available(std::string* why);
 // (load = false: compile only, no device needed)
 int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<std::vector<std::string>>& names,
                     std::vector<std::vector<const void*>>& kernels, bool load = true);
-// host-only: plan a complex128 apply and compile its block kernels without loading them
-int32_t jit_compile_only(int n, const std::vector<LGate>& gates, int64_t* n_kernels);
+// host-only: plan an apply and compile its block kernels without loading them
+int32_t jit_compile_only(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* n_kernels);
 // unload every program jit_compile loaded (their kernels become invalid)
 void jit_unload_all();
 // kernels compiled so far, block launches through them, and whether compiling failed
@@ -191,6 +191,7 @@ struct Tuning
     int jit_ctas_per_sm {2};     // CTAs per SM of run-time compiled blocks: 2..4
     int jit_merge_diag {1};
     int jit_skip_io {1};
+    int jit_async_load {0};      // 1: run-time compiled blocks load the next tile with cp.async into a second buffer
     int jit_fence {0};           // k > 0: run-time compiled blocks fence the amplitudes every k ops         // 1: no transpose into a block's load layout or out of its store layout      // 1: a phase's diagonal ops on thread / tile-external bits as one factor
 };
 Tuning& tuning();

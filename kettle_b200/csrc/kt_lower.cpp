@@ -104,6 +104,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.fused_jit = static_cast<int>(std::max(0LL, std::min(2LL, v)));
     } else if (name == "jit_ctas_per_sm") {
         t.jit_ctas_per_sm = static_cast<int>(std::max(2LL, std::min(4LL, v)));
+    } else if (name == "jit_async_load") {
+        t.jit_async_load = (v != 0) ? 1 : 0;
     } else if (name == "jit_fence") {
         t.jit_fence = static_cast<int>(std::max(0LL, std::min(64LL, v)));
     } else if (name == "jit_skip_io") {
@@ -177,6 +179,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.fused_jit;
     } else if (n == "jit_ctas_per_sm") {
         *value = t.jit_ctas_per_sm;
+    } else if (n == "jit_async_load") {
+        *value = t.jit_async_load;
     } else if (n == "jit_fence") {
         *value = t.jit_fence;
     } else if (n == "jit_skip_io") {

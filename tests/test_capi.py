@@ -92,3 +92,5 @@ def test_run_time_block_kernels_compile_on_the_host():
     assert capi.jit_compile_only(14, g) >= 1
     gates, params = W.hea(13, 2, seed=2)
     assert capi.jit_compile_only(13, gates, params) >= 1
+    assert capi.jit_compile_only(15, W.random_layers(15, 2, seed=3, mixed=True),
+                                 dtype=capi.KT_C64) >= 1

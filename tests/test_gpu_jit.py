@@ -142,3 +142,29 @@ def test_jit_variants_agree(jit, port, knobs):
     finally:
         for k, v in old.items():
             capi.tuning_set(k, v)
+
+
+@pytest.mark.parametrize("renorm", [1, 0])
+def test_jit_complex64(jit, port, renorm):
+    # complex64 blocks compile too, with the per-block renormalisation by default
+    old = capi.tuning_get("c64_renormalize")
+    try:
+        capi.tuning_set("c64_renormalize", renorm)
+        n = 20
+        g = W.random_layers(n, 6, seed=41, mixed=True)
+        want = port.apply(n, basis(n), g)
+        s0 = capi.jit_stats()
+        sv = capi.Statevector(n, capi.KT_C64)
+        sv.apply(g)
+        got = sv.download()
+        assert capi.jit_stats()["launches"] > s0["launches"]
+        assert np.abs(got - want).max() < 1e-4
+        assert abs(sv.norm_sq() - 1.0) < 1e-5
+        sv.close()
+        capi.tuning_set("fused_jit", 0)
+        ref = capi.Statevector(n, capi.KT_C64)
+        ref.apply(g)
+        assert np.abs(ref.download() - got).max() < 1e-5
+        ref.close()
+    finally:
+        capi.tuning_set("c64_renormalize", old)
