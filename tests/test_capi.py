@@ -94,3 +94,21 @@ def test_run_time_block_kernels_compile_on_the_host():
     assert capi.jit_compile_only(13, gates, params) >= 1
     assert capi.jit_compile_only(15, W.random_layers(15, 2, seed=3, mixed=True),
                                  dtype=capi.KT_C64) >= 1
+
+
+@pytest.mark.parametrize("knobs", [
+    {"jit_async_load": 1}, {"fused_reg_bits": 3}, {"jit_fence": 2, "jit_merge_diag": 0},
+    {"jit_skip_io": 0, "jit_prefetch": 0, "fused_tile_bits": 11},
+])
+def test_generated_kernel_variants_compile_on_the_host(knobs):
+    from kettle_b200 import workloads as W
+    old = {k: capi.tuning_get(k) for k in knobs}
+    try:
+        for k, v in knobs.items():
+            capi.tuning_set(k, v)
+        g = W.random_layers(14, 2, seed=5, mixed=True)
+        assert capi.jit_compile_only(14, g) >= 1
+        assert capi.jit_compile_only(15, g, dtype=capi.KT_C64) >= 1
+    finally:
+        for k, v in old.items():
+            capi.tuning_set(k, v)
