@@ -156,6 +156,14 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               of >= jit_min_qubits qubits; without NVRTC, or if a
  *                               compile fails, the precompiled kernels run (kt_jit_stats)
  *   jit_min_qubits     1..64    (26) the state size from which fused_jit = 2 compiles
+ *   jit_ctas_per_sm    2..4     (2) CTAs per SM of compiled 256- or 128-thread blocks
+ *   jit_prefetch       0 or 1   (1) each CTA prefetches its next tile into L2
+ *   jit_merge_diag     0 or 1   (1) a phase's diagonal gates on thread / tile-external
+ *                               qubits applied as one per-thread factor
+ *   jit_skip_io        0 or 1   (1) load / store in the first / last compute layout
+ *   jit_async_load     0 or 1   (0) next tile copied with cp.async into a second
+ *                               shared-memory buffer (where two tiles fit a CTA)
+ *   jit_fence          0..64    (0) every k gates, an empty asm pins the amplitudes
  *   fused_reg_bits     3 or 4   complex128 amplitudes per thread in fused blocks
  *                               (2^4; or 2^3 with twice the warps: 12-qubit tiles of
  *                               512 threads, 2 CTAs per SM, or 11-qubit tiles of 256
