@@ -497,9 +497,16 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
         e += indent + "{\n" + indent + "    const C* src = a + " + jit_deposit(tile_expr, free_strides.data(), fb.nfree) +
              " + " + jit_deposit("t", ph[first].tstride, TB) + ";\n";
         e += indent + "    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sb + t));\n";
+        // one amplitude per copy: 16 bytes (.cg, L2 only) for complex128, 8 bytes
+        // (.ca, the only form for sizes below 16) for complex64; both addresses
+        // are aligned to the amplitude size
+        const size_t amp = sizeof(typename CxT<T>::type);
+        const std::string op = (amp == 16) ? "cp.async.cg.shared.global [%0], [%1], 16;"
+                                           : "cp.async.ca.shared.global [%0], [%1], 8;";
         for (int i = 0; i < R; ++i) {
-            e += indent + "    asm volatile(\"cp.async.cg.shared.global [%0], [%1], 16;\" :: \"r\"(dst + " +
-                 std::to_string(16 * i * n_thr) + "u), \"l\"(src + " + std::to_string(reg_off(ph[first], i)) + "ULL) : \"memory\");\n";
+            e += indent + "    asm volatile(\"" + op + "\" :: \"r\"(dst + " +
+                 std::to_string(amp * static_cast<size_t>(i) * static_cast<size_t>(n_thr)) + "u), \"l\"(src + " +
+                 std::to_string(reg_off(ph[first], i)) + "ULL) : \"memory\");\n";
         }
         e += indent + "}\n";
         return e;
