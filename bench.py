@@ -584,6 +584,13 @@ def run_engine(args):
         sv.set_basis(0)
         sv.apply(gates, mode=mode)
 
+    # warm-up: the circuit is applied every step, so its fused blocks are
+    # compiled up front (kt_sv_prepare) as a repeated workload would have them
+    if mode == capi.KT_APPLY_FUSED:
+        try:
+            sv.prepare(gates)
+        except capi.KettleError as e:
+            print(f"note: block kernels not compiled ({e}); the precompiled kernels run", file=sys.stderr)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()

@@ -148,13 +148,20 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               shared-memory transpose (1) or run as ops (0)
  *   c64_renormalize    0 or 1   complex64 applies rescale every fused block to the
  *                               norm the state had when the apply began (1)
+ *   plan_lookahead     0 or 1   (1) each fused block's tile qubits chosen among the
+ *                               greedy tile and tiles pinned to the qubits the next
+ *                               gates need most, by the gates it and the next block take
  *   fused_jit          0, 1, 2  fused blocks as kernels compiled at run
  *                               time (NVRTC, cached per block structure: gate bodies
  *                               as straight-line code, every slot and mask a
- *                               constant): 0 never, 1 always, 2 (default) from the
- *                               second apply of the same circuit structure on states
- *                               of >= jit_min_qubits qubits; without NVRTC, or if a
- *                               compile fails, the precompiled kernels run (kt_jit_stats)
+ *                               constant): 0 never, 1 always, 2 (default) once a
+ *                               circuit structure has been applied often enough to
+ *                               repay the compile (jit_after) on states of
+ *                               >= jit_min_qubits qubits, or after kt_sv_prepare;
+ *                               without NVRTC, or if a compile fails, the
+ *                               precompiled kernels run (kt_jit_stats)
+ *   jit_after          0..1e6   (0) the apply at which fused_jit = 2 compiles; 0 estimates
+ *                               it from the state size and the host's threads (>= 2)
  *   jit_min_qubits     1..64    (26) the state size from which fused_jit = 2 compiles
  *   jit_ctas_per_sm    2..4     (2) CTAs per SM of compiled 256- or 128-thread blocks
  *   jit_prefetch       0 or 1   (1) each CTA prefetches its next tile into L2
@@ -206,6 +213,13 @@ int32_t kt_sv_copy(kt_sv dst, kt_sv src);
 #define KT_APPLY_PER_GATE 1
 int32_t kt_sv_apply(kt_sv sv, const kt_gate* gates, int64_t n_gates,
                     const double* params, int64_t n_params, int32_t mode);
+/* Compile the fused block kernels of this circuit for `sv` now (new), so that
+ * every later kt_sv_apply of a circuit with the same structure (any parameter
+ * values) on a state of this size and dtype runs them from its first apply;
+ * without it they are compiled once a circuit has been applied often enough to
+ * repay the compile (fused_jit = 2).  Returns KT_ERR_CUDA when run-time
+ * compilation is unavailable (applies then use the precompiled kernels). */
+int32_t kt_sv_prepare(kt_sv sv, const kt_gate* gates, int64_t n_gates, const double* params, int64_t n_params);
 
 /* Host-only dry run of the fused planner (no device work, no reference
  * counterpart): the fused blocks, layout phases, gates placed in blocks (X /

@@ -60,6 +60,7 @@ _SIGS = {
     "kt_tuning_set": ([C.c_char_p, I64], I32),
     "kt_tuning_get": ([C.c_char_p, C.POINTER(I64)], I32),
     "kt_jit_stats": ([P, P, P], I32),
+    "kt_sv_prepare": ([P, P, I64, P, I64], I32),
     "kt_jit_compile_only": ([I32, I32, P, I64, P, I64, P], I32),
     "kt_sv_create": ([I32, I32, C.POINTER(P)], I32),
     "kt_sv_wrap": ([P, I32, I32, C.POINTER(P)], I32),
@@ -291,6 +292,12 @@ class Statevector:
         v = C.c_double()
         check(lib().kt_sv_norm_sq(self._h, C.byref(v)))
         return v.value
+
+    def prepare(self, gates: np.ndarray, params: np.ndarray | None = None):
+        """Compile the fused block kernels of this circuit now (kt_sv_prepare)."""
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        check(lib().kt_sv_prepare(self._h, ptr(g), g.size, ptr(p), 0 if p is None else p.size))
 
     def device_ptr(self) -> int:
         """Device address of the amplitudes (kt_sv_info)."""

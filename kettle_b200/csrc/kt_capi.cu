@@ -198,6 +198,23 @@ int32_t kt_jit_compile_only(int32_t n_qubits, int32_t dtype, const kt_gate* gate
     });
 }
 
+int32_t kt_sv_prepare(kt_sv sv, const kt_gate* gates, int64_t n_gates, const double* params, int64_t n_params)
+{
+    return guard([&]() -> int32_t {
+        if (sv == nullptr) {
+            return invalid("null handle");
+        }
+        if (n_gates < 0 || (n_gates > 0 && gates == nullptr)) {
+            return invalid("bad gate array");
+        }
+        std::vector<kt::LGate> lg;
+        if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, sv->st.n_bits, lg); rc != KT_OK) {
+            return rc;
+        }
+        return kt::jit_prepare(sv->st, lg);
+    });
+}
+
 int32_t kt_jit_stats(int64_t* kernels_compiled, int64_t* block_launches, int32_t* failed)
 {
     if (kernels_compiled == nullptr || block_launches == nullptr || failed == nullptr) {

@@ -27,9 +27,11 @@
 //  * Loads and stores use a layout whose lane bits are the L lowest qubits:
 //    each warp instruction touches whole 128-byte lines.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <type_traits>
 #include <unordered_map>
@@ -278,6 +280,101 @@ int32_t fused_plan(int n, const std::vector<LGate>& gates, Plan<T>& plan, int* K
     }
     *K_out = K;
     *rb3_out = rb3;
+    return KT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Plan cache.  Planning depends on the gates' kinds, qubits and a few value
+// classes (real, RX-like, pure X, diag(1, .)), not on the angles, so a
+// circuit applied again with new parameters reuses its plan: the op records
+// take the new matrices and nothing else changes.  Entries are keyed by that
+// structure (and the planning knobs), checked in full on a hit.
+
+uint32_t gate_class(const LGate& x)
+{
+    const double* m = x.m;
+    const bool real = m[1] == 0.0 && m[3] == 0.0 && m[5] == 0.0 && m[7] == 0.0;
+    const bool rxl = m[1] == 0.0 && m[7] == 0.0 && m[0] == m[6] && m[2] == 0.0 && m[4] == 0.0 && m[3] == m[5];
+    return static_cast<uint32_t>(x.kind) | (static_cast<uint32_t>(x.flags & 1) << 4) | (real ? 1u << 5 : 0u) |
+           (rxl ? 1u << 6 : 0u) | (is_pure_x(x) ? 1u << 7 : 0u);
+}
+
+template <typename T>
+struct PlanEntry
+{
+    std::vector<uint64_t> signature;
+    Plan<T> plan;
+    int K {0};
+    bool rb3 {false};
+};
+
+template <typename T>
+struct PlanCache
+{
+    std::mutex m;
+    std::unordered_map<uint64_t, PlanEntry<T>> entries;
+};
+
+template <typename T>
+PlanCache<T>& plan_cache()
+{
+    static PlanCache<T> c;
+    return c;
+}
+
+constexpr size_t PLAN_CACHE_MAX = 64;
+
+// fused_plan through the cache; *key identifies the plan's structure
+template <typename T>
+int32_t fused_plan_cached(int n, const std::vector<LGate>& gates, Plan<T>& plan, int* K_out, bool* rb3_out,
+                          uint64_t* key)
+{
+    const Tuning& tu = tuning();
+    std::vector<uint64_t> sig;
+    sig.reserve(gates.size() + 2);
+    sig.push_back(static_cast<uint64_t>(n) | (static_cast<uint64_t>(sizeof(T)) << 8) |
+                  (static_cast<uint64_t>(tu.fused_tile_bits) << 16) | (static_cast<uint64_t>(tu.fold_permutations) << 24) |
+                  (static_cast<uint64_t>(tu.fused_reg_bits) << 28) | (static_cast<uint64_t>(tu.plan_lookahead) << 32) |
+                  (static_cast<uint64_t>(tu.fused_max_ops) << 40));
+    for (const LGate& x : gates) {
+        sig.push_back(static_cast<uint64_t>(gate_class(x)) | (static_cast<uint64_t>(x.target & 0xFFFF) << 8) |
+                      (static_cast<uint64_t>(x.control & 0xFFFF) << 24));
+    }
+    uint64_t h = 0xcbf29ce484222325ULL;
+    for (const uint64_t v : sig) {
+        h = (h ^ v) * 0x100000001b3ULL;
+        h ^= h >> 29;
+    }
+    *key = h;
+    PlanCache<T>& pc = plan_cache<T>();
+    {
+        std::lock_guard<std::mutex> lock(pc.m);
+        auto it = pc.entries.find(h);
+        if (it != pc.entries.end() && it->second.signature == sig) {
+            plan = it->second.plan;
+            *K_out = it->second.K;
+            *rb3_out = it->second.rb3;
+            for (size_t i = 0; i < plan.ops.size(); ++i) {
+                const LGate& x = gates[static_cast<size_t>(plan.op_gate[i])];
+                for (int e = 0; e < 8; ++e) {
+                    plan.ops[i].m[e] = static_cast<T>(x.m[e]);
+                }
+            }
+            return KT_OK;
+        }
+    }
+    if (const int32_t rc = fused_plan<T>(n, gates, plan, K_out, rb3_out); rc != KT_OK) {
+        return rc;
+    }
+    std::lock_guard<std::mutex> lock(pc.m);
+    if (pc.entries.size() >= PLAN_CACHE_MAX) {
+        pc.entries.clear();
+    }
+    PlanEntry<T>& e = pc.entries[h];
+    e.signature = std::move(sig);
+    e.plan = plan;
+    e.K = *K_out;
+    e.rb3 = *rb3_out;
     return KT_OK;
 }
 
@@ -702,6 +799,17 @@ struct JitCache
     std::mutex m;
     std::unordered_map<std::string, const void*> kernels;  // launch-bounds prefix + body -> kernel
     std::unordered_set<size_t> seen;                       // plans applied once with the precompiled kernels
+    struct PlanState
+    {
+        int64_t applies {0};
+        bool prepared {false};
+        int64_t generation {-1};
+        int device {-1};
+        std::string config;                 // launch bounds, shared memory, renormalisation
+        std::vector<const void*> kernels;   // one per block, once compiled
+    };
+    std::unordered_map<uint64_t, PlanState> plans;        // by plan structure (fused_plan_cached)
+    int64_t generation {0};                                // bumped when every program is unloaded
     std::map<std::pair<const void*, int>, int> smem_set;   // (kernel, device) -> shared-memory limit set
     int64_t compiled {0};
     int64_t launches {0};
@@ -748,6 +856,7 @@ bool jit_kernels(const Plan<T>& plan, int RB, int threads, int minb, int smem_by
         jit_unload_all();
         jc.kernels.clear();
         jc.smem_set.clear();
+        ++jc.generation;
         missing.clear();
         first_of.clear();
         for (size_t b = 0; b < nb; ++b) {
@@ -759,6 +868,9 @@ bool jit_kernels(const Plan<T>& plan, int RB, int threads, int minb, int smem_by
     }
     if (jc.seen.size() > JIT_MAX_SEEN) {
         jc.seen.clear();
+    }
+    if (jc.plans.size() > JIT_MAX_SEEN) {
+        jc.plans.clear();
     }
     if (!missing.empty() && on_repeat) {
         std::string all;
@@ -822,22 +934,38 @@ bool jit_kernels(const Plan<T>& plan, int RB, int threads, int minb, int smem_by
     return true;
 }
 
+// The apply of a plan from which its compiled kernels pay for themselves:
+// compiling takes about 0.6 s per block kernel on one host thread (the
+// blocks compile in parallel), and a compiled pass saves about half of a
+// precompiled one, ~2^n * 2 * amplitude bytes at 1.5 TB/s; jit_after
+// (>= 1) fixes the count instead.  At least the second apply.
+int64_t jit_after_applies(int n, size_t amp_bytes)
+{
+    if (tuning().jit_after > 0) {
+        return tuning().jit_after;
+    }
+    const double pass = std::ldexp(1.0, n) * 2.0 * static_cast<double>(amp_bytes) / 1.5e12;
+    const double threads = std::max(1u, std::thread::hardware_concurrency());
+    const double k = std::ceil(0.6 / threads / (0.5 * pass));
+    return static_cast<int64_t>(std::max(2.0, std::min(k, 1.0e9)));
+}
+
 // The launch of a plan's blocks as run-time compiled kernels, or false when
-// the caller should run the precompiled ones: fused_jit = 1 always; 2 from
-// the second apply of a plan on states of at least jit_min_qubits qubits
-// (where a pass is long enough to repay the compile, about half a second per
-// block kernel on one host thread).  With `parts` (complex64
+// the caller should run the precompiled ones: fused_jit = 1 always; 2 on
+// states of at least jit_min_qubits index bits once the plan has been applied
+// jit_after_applies times, or after kt_sv_prepare (`compile_only`: compile,
+// launch nothing).  With `parts` (complex64
 // renormalisation: target | out even | out odd, n_parts per-CTA sums each)
 // every block gets its NormArgs and the caller finishes with k_norm_final.
 template <typename T>
-bool jit_launch(State& s, const Plan<T>& plan, int K, bool rb3, int threads, int shape, double* parts, int32_t* rc,
-                int* n_parts_out)
+bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb3, int threads, int shape, double* parts,
+                int32_t* rc, int* n_parts_out, bool compile_only = false)
 {
     using C = typename CxT<T>::type;
     *rc = KT_OK;
     const int n = s.n_bits;
     const int mode = tuning().fused_jit;
-    const bool want = mode == 1 || (mode == 2 && n >= tuning().jit_min_qubits);
+    const bool want = compile_only || mode == 1 || (mode == 2 && n >= tuning().jit_min_qubits);
     if (!want) {
         return false;
     }
@@ -858,9 +986,50 @@ bool jit_launch(State& s, const Plan<T>& plan, int K, bool rb3, int threads, int
     if (norm && grid > static_cast<uint64_t>(*n_parts_out)) {
         return false;  // the caller reserved per-CTA sums for fewer CTAs
     }
+    // this plan's kernels: resolved once, compiled once the plan has been
+    // applied often enough to repay the compile (jit_after_applies)
     std::vector<const void*> jk;
-    if (!jit_kernels<T>(plan, RB, threads, minb, smem_attr, mode == 2, norm, jk)) {
-        return false;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        dev = 0;
+    }
+    const std::string config = std::to_string(RB) + "/" + std::to_string(threads) + "/" + std::to_string(minb) + "/" +
+                               std::to_string(smem_attr) + "/" + (norm ? "n" : "-") + "/" +
+                               std::to_string(jit_async(K, sizeof(C)) ? 1 : 0) + "/" +
+                               std::to_string(tuning().jit_prefetch) + std::to_string(tuning().jit_merge_diag) +
+                               std::to_string(tuning().jit_skip_io) + std::to_string(tuning().jit_fence);
+    bool ready = false;
+    bool compile = compile_only || mode == 1;
+    {
+        JitCache& jc = jit_cache();
+        std::lock_guard<std::mutex> lock(jc.m);
+        if (jc.failed) {
+            return false;
+        }
+        JitCache::PlanState& st = jc.plans[plan_key];
+        st.applies += compile_only ? 0 : 1;
+        st.prepared = st.prepared || compile_only;
+        ready = st.generation == jc.generation && st.device == dev && st.config == config &&
+                st.kernels.size() == plan.blocks.size();
+        if (ready) {
+            jk = st.kernels;
+        }
+        compile = compile || st.prepared || st.applies >= jit_after_applies(n, sizeof(C));
+    }
+    if (!ready) {
+        if (!compile || !jit_kernels<T>(plan, RB, threads, minb, smem_attr, false, norm, jk)) {
+            return false;
+        }
+        JitCache& jc = jit_cache();
+        std::lock_guard<std::mutex> lock(jc.m);
+        JitCache::PlanState& st = jc.plans[plan_key];
+        st.generation = jc.generation;
+        st.device = dev;
+        st.config = config;
+        st.kernels = jk;
+    }
+    if (compile_only) {
+        return true;
     }
     void* a = s.amps;
     unsigned long long nt = n_tiles;
@@ -906,6 +1075,7 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     Plan<T> plan;
     int K = 0;
     bool rb3 = false;
+    uint64_t plan_key = 0;
     if (n < Cfg<T>::RB + 5 || gates.empty()) {
         for (const auto& g : gates) {
             if (const int32_t rc = launch_gate_sweep(s, g); rc != KT_OK) {
@@ -914,7 +1084,7 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
         }
         return KT_OK;
     }
-    if (const int32_t rc = fused_plan<T>(n, gates, plan, &K, &rb3); rc != KT_OK) {
+    if (const int32_t rc = fused_plan_cached<T>(n, gates, plan, &K, &rb3, &plan_key); rc != KT_OK) {
         return rc;
     }
     // upload the plan: blocks | phases | ops
@@ -957,7 +1127,7 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
             double* parts = static_cast<double*>(s.scratch2.ptr);
             int32_t rc = KT_OK;
             int n_parts = max_parts;
-            if (jit_launch<T>(s, plan, K, rb3, threads, shape, parts, &rc, &n_parts)) {
+            if (jit_launch<T>(s, plan, plan_key, K, rb3, threads, shape, parts, &rc, &n_parts)) {
                 if (rc != KT_OK || plan.blocks.empty()) {
                     return rc;
                 }
@@ -1000,7 +1170,7 @@ int32_t run_fused(State& s, const std::vector<LGate>& gates)
     {
         int32_t rc = KT_OK;
         int n_parts = 0;
-        if (jit_launch<T>(s, plan, K, rb3, threads, shape, nullptr, &rc, &n_parts)) {
+        if (jit_launch<T>(s, plan, plan_key, K, rb3, threads, shape, nullptr, &rc, &n_parts)) {
             return rc;
         }
     }
@@ -1277,6 +1447,58 @@ void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed)
     *compiled = jc.compiled;
     *launches = jc.launches;
     *failed = jc.failed ? 1 : 0;
+}
+
+namespace
+{
+
+template <typename T>
+int32_t jit_prepare_t(State& s, const std::vector<LGate>& gates)
+{
+    const int n = s.n_bits;
+    if (n < Cfg<T>::RB + 5 || gates.empty()) {
+        return KT_OK;  // applied one gate at a time: nothing to compile
+    }
+    Plan<T> plan;
+    int K = 0;
+    bool rb3 = false;
+    uint64_t key = 0;
+    if (const int32_t rc = fused_plan_cached<T>(n, gates, plan, &K, &rb3, &key); rc != KT_OK) {
+        return rc;
+    }
+    const int threads = 1 << (K - (rb3 ? Cfg3::RB : Cfg<T>::RB));
+    int shape = threads > 256 ? 0 : (tuning().fused_ctas_per_sm == 1 ? 1 : 2);
+    if (rb3) {
+        shape = threads > 256 ? 3 : 4;
+    }
+    double* parts = nullptr;
+    int n_parts = 0;
+    if (std::is_same<T, float>::value && tuning().c64_renormalize != 0) {
+        n_parts = sm_count() * 4;
+        if (const int32_t rc = s.scratch2.reserve(3 * static_cast<size_t>(n_parts) * sizeof(double)); rc != KT_OK) {
+            return rc;
+        }
+        parts = static_cast<double*>(s.scratch2.ptr);
+    }
+    int32_t rc = KT_OK;
+    if (!jit_launch<T>(s, plan, key, K, rb3, threads, shape, parts, &rc, &n_parts, true)) {
+        std::string why;
+        if (!jit_available(&why)) {
+            set_error(KT_ERR_CUDA, why);
+        } else {
+            set_error(KT_ERR_CUDA, "the block kernels of this circuit could not be compiled; applies use the "
+                                   "precompiled kernels");
+        }
+        return KT_ERR_CUDA;
+    }
+    return rc;
+}
+
+}  // namespace
+
+int32_t jit_prepare(State& s, const std::vector<LGate>& gates)
+{
+    return s.dtype == KT_C128 ? jit_prepare_t<double>(s, gates) : jit_prepare_t<float>(s, gates);
 }
 
 int32_t apply_fused(State& s, const std::vector<LGate>& gates)

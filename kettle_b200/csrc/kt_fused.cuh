@@ -63,52 +63,178 @@ uint64_t bit(int q)
 // Greedy block formation: in circuit order, take each gate that does not
 // share a qubit with a gate skipped before it and whose target (when it must
 // be in the tile) fits in the K-qubit set.
+// One block from the pending gates: every gate that can move ahead of the
+// gates not taken (no shared qubit with them) and whose non-diagonal target
+// fits the tile.  `fixed` (0: grow the tile as gates arrive) pins the tile's
+// qubit set up front.  Gates with mark[idx] == skip are treated as gone (taken
+// by a block planned before this one); the scan stops once every qubit is
+// blocked.  Returns the number of gates taken; `take` (if not null) gets them.
+size_t scan_block(const std::vector<LGate>& g, const std::vector<int>& pend, const std::vector<uint32_t>& mark,
+                  uint32_t skip, int n, int K, int L, size_t max_ops, uint64_t fixed, uint64_t* Q_out,
+                  std::vector<int>* take)
+{
+    const uint64_t all = (n >= 64) ? ~uint64_t {0} : (bit(n) - 1);
+    uint64_t Q = fixed != 0 ? fixed : (bit(L) - 1);
+    uint64_t blocked = 0;
+    size_t taken = 0;
+    if (take != nullptr) {
+        take->clear();
+    }
+    for (const int idx : pend) {
+        if (skip != 0 && mark[static_cast<size_t>(idx)] == skip) {
+            continue;
+        }
+        const LGate& x = g[idx];
+        const uint64_t touch = bit(x.target) | (x.control >= 0 ? bit(x.control) : 0);
+        if ((touch & blocked) != 0 || taken >= max_ops) {
+            blocked |= touch;
+        } else {
+            const uint64_t need = (x.kind == KIND_DIAG) ? 0 : bit(x.target);
+            const bool fits = fixed != 0 ? ((need & ~Q) == 0) : (__builtin_popcountll(Q | need) <= K);
+            if (fits) {
+                Q |= need;
+                ++taken;
+                if (take != nullptr) {
+                    take->push_back(idx);
+                }
+            } else {
+                blocked |= touch;
+            }
+        }
+        if (blocked == all) {
+            break;
+        }
+    }
+    if (Q_out != nullptr) {
+        *Q_out = Q;
+    }
+    return taken;
+}
+
+// The tile qubits a lookahead prefers: the L lowest, then the qubits that the
+// first `window` pending non-diagonal gates (not marked `skip`) target most
+// often (earliest first among equals).
+uint64_t lookahead_tile(const std::vector<LGate>& g, const std::vector<int>& pend, const std::vector<uint32_t>& mark,
+                        uint32_t skip, int n, int K, int L, size_t window)
+{
+    int count[64] = {};
+    size_t first[64];
+    for (int q = 0; q < 64; ++q) {
+        first[q] = SIZE_MAX;
+    }
+    size_t seen = 0;
+    for (const int idx : pend) {
+        if (seen >= window) {
+            break;
+        }
+        if (skip != 0 && mark[static_cast<size_t>(idx)] == skip) {
+            continue;
+        }
+        const LGate& x = g[idx];
+        if (x.kind != KIND_DIAG) {
+            ++count[x.target];
+            first[x.target] = std::min(first[x.target], seen);
+        }
+        ++seen;
+    }
+    int order[64];
+    int no = 0;
+    for (int q = L; q < n; ++q) {
+        order[no++] = q;
+    }
+    std::stable_sort(order, order + no, [&](int a, int b) {
+        if (count[a] != count[b]) {
+            return count[a] > count[b];
+        }
+        return first[a] < first[b];
+    });
+    uint64_t Q = bit(L) - 1;
+    for (int i = 0; i < no && __builtin_popcountll(Q) < K; ++i) {
+        Q |= bit(order[i]);
+    }
+    return Q;
+}
+
+// Candidate tiles for a block: 0 (the tile grows as gates arrive) and the
+// lookahead tiles of several windows.
+void tile_candidates(const std::vector<LGate>& g, const std::vector<int>& pend, const std::vector<uint32_t>& mark,
+                     uint32_t skip, int n, int K, int L, std::vector<uint64_t>& c)
+{
+    c.assign(1, 0);
+    for (int w : {1, 2, 3, 4, 6, 8, 12, 16, 32, 64}) {
+        const uint64_t q = lookahead_tile(g, pend, mark, skip, n, K, L, static_cast<size_t>(w) * static_cast<size_t>(K));
+        if (std::find(c.begin(), c.end(), q) == c.end()) {
+            c.push_back(q);
+        }
+    }
+}
+
 std::vector<PlanBlock> form_blocks(const std::vector<LGate>& g, int n, int K, int L, size_t max_ops)
 {
     std::vector<PlanBlock> out;
     std::vector<int> pend(g.size());
     std::iota(pend.begin(), pend.end(), 0);
-    const uint64_t all = (n >= 64) ? ~uint64_t {0} : (bit(n) - 1);
+    const bool look = tuning().plan_lookahead != 0 && K < n && n <= 64;
+    std::vector<uint32_t> mark(g.size(), 0);
+    uint32_t stamp = 0;
+    std::vector<int> take, best_take;
+    std::vector<uint64_t> cand1, cand2;
     while (!pend.empty()) {
-        uint64_t Q = bit(L) - 1;
-        uint64_t blocked = 0;
-        std::vector<int> take;
-        std::vector<int> rest;
-        rest.reserve(pend.size());
-        for (size_t k = 0; k < pend.size(); ++k) {
-            const int idx = pend[k];
-            const LGate& x = g[idx];
-            const uint64_t touch = bit(x.target) | (x.control >= 0 ? bit(x.control) : 0);
-            if ((touch & blocked) != 0 || take.size() >= max_ops) {
-                blocked |= touch;
-                rest.push_back(idx);
-            } else {
-                const uint64_t need = (x.kind == KIND_DIAG) ? 0 : bit(x.target);
-                if (__builtin_popcountll(Q | need) <= K) {
-                    Q |= need;
-                    take.push_back(idx);
-                } else {
-                    blocked |= touch;
-                    rest.push_back(idx);
+        uint64_t Q = 0;
+        uint64_t bestQ = 0;
+        scan_block(g, pend, mark, 0, n, K, L, max_ops, 0, &bestQ, &best_take);
+        if (look) {
+            // plan_lookahead: of the candidate tiles, the one whose block and the
+            // best next block together take the most gates (ties: the greedy one)
+            size_t best_score = 0;
+            bool first = true;
+            tile_candidates(g, pend, mark, 0, n, K, L, cand1);
+            for (const uint64_t c1 : cand1) {
+                scan_block(g, pend, mark, 0, n, K, L, max_ops, c1, &Q, &take);
+                ++stamp;
+                for (const int idx : take) {
+                    mark[static_cast<size_t>(idx)] = stamp;
+                }
+                size_t next = 0;
+                if (take.size() < pend.size()) {
+                    tile_candidates(g, pend, mark, stamp, n, K, L, cand2);
+                    for (const uint64_t c2 : cand2) {
+                        next = std::max(next, scan_block(g, pend, mark, stamp, n, K, L, max_ops, c2, nullptr, nullptr));
+                    }
+                }
+                const size_t score = take.size() + next;
+                if (first || score > best_score) {
+                    first = false;
+                    best_score = score;
+                    best_take.swap(take);
+                    bestQ = Q;
                 }
             }
-            if (blocked == all) {
-                rest.insert(rest.end(), pend.begin() + static_cast<long>(k) + 1, pend.end());
-                break;
+        }
+        // the chosen block's gates leave the pending list
+        ++stamp;
+        for (const int idx : best_take) {
+            mark[static_cast<size_t>(idx)] = stamp;
+        }
+        std::vector<int> rest;
+        rest.reserve(pend.size() - best_take.size());
+        for (const int idx : pend) {
+            if (mark[static_cast<size_t>(idx)] != stamp) {
+                rest.push_back(idx);
             }
         }
         // fill the tile up to K qubits with the lowest free qubits (longer contiguous runs)
-        for (int q = 0; q < n && __builtin_popcountll(Q) < K; ++q) {
-            Q |= bit(q);
+        for (int q = 0; q < n && __builtin_popcountll(bestQ) < K; ++q) {
+            bestQ |= bit(q);
         }
         PlanBlock b;
         b.K = K;
         for (int q = 0; q < n; ++q) {
-            if (Q & bit(q)) {
+            if (bestQ & bit(q)) {
                 b.qubits.push_back(q);
             }
         }
-        b.gates = std::move(take);
+        b.gates = best_take;
         out.push_back(std::move(b));
         pend.swap(rest);
     }

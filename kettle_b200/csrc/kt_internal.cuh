@@ -141,6 +141,8 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
 int32_t jit_compile_only(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* n_kernels);
 // unload every program jit_compile loaded (their kernels become invalid)
 void jit_unload_all();
+// compile the fused block kernels of `gates` on this state now (kt_sv_prepare)
+int32_t jit_prepare(State& s, const std::vector<LGate>& gates);
 // kernels compiled so far, block launches through them, and whether compiling failed
 void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed);
 // host-only: what the fused planner makes of a gate stream
@@ -184,9 +186,11 @@ struct Tuning
     int fold_permutations {1};   // 1: X / CX inside a tile become part of a transpose, 0: ops
     int c64_renormalize {1};     // 1: complex64 applies keep the state's norm (per-block rescaling)
     int fused_reg_bits {4};      // complex128 amplitudes per thread in fused blocks: 2^4, or 2^3 (more warps)
+    int plan_lookahead {1};      // 1: a block's tile may be pinned to the qubits the next gates need most
     int fused_jit {2};           // complex128 blocks as run-time compiled kernels: 0 never, 1 always,
                                  // 2 from a plan's second apply on >= jit_min_qubits qubits
     int jit_min_qubits {26};
+    int jit_after {0};           // fused_jit = 2 compiles at this apply of a plan (0: estimated, >= 2)
     int jit_prefetch {1};        // 1: run-time compiled blocks prefetch their CTA's next tile into L2
     int jit_ctas_per_sm {2};     // CTAs per SM of run-time compiled blocks: 2..4
     int jit_merge_diag {1};

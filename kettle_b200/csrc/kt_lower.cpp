@@ -100,6 +100,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.c64_renormalize = (v != 0) ? 1 : 0;
     } else if (name == "fused_reg_bits") {
         t.fused_reg_bits = (v == 3) ? 3 : 4;
+    } else if (name == "plan_lookahead") {
+        t.plan_lookahead = (v != 0) ? 1 : 0;
     } else if (name == "fused_jit") {
         t.fused_jit = static_cast<int>(std::max(0LL, std::min(2LL, v)));
     } else if (name == "jit_ctas_per_sm") {
@@ -114,6 +116,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.jit_merge_diag = (v != 0) ? 1 : 0;
     } else if (name == "jit_prefetch") {
         t.jit_prefetch = (v != 0) ? 1 : 0;
+    } else if (name == "jit_after") {
+        t.jit_after = static_cast<int>(std::max(0LL, std::min(1000000LL, v)));
     } else if (name == "jit_min_qubits") {
         t.jit_min_qubits = static_cast<int>(std::max(1LL, std::min(64LL, v)));
     } else {
@@ -175,6 +179,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.c64_renormalize;
     } else if (n == "fused_reg_bits") {
         *value = t.fused_reg_bits;
+    } else if (n == "plan_lookahead") {
+        *value = t.plan_lookahead;
     } else if (n == "fused_jit") {
         *value = t.fused_jit;
     } else if (n == "jit_ctas_per_sm") {
@@ -189,6 +195,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.jit_merge_diag;
     } else if (n == "jit_prefetch") {
         *value = t.jit_prefetch;
+    } else if (n == "jit_after") {
+        *value = t.jit_after;
     } else if (n == "jit_min_qubits") {
         *value = t.jit_min_qubits;
     } else {

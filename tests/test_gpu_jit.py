@@ -98,12 +98,14 @@ def test_jit_every_gate_kind(jit, port):
 
 
 def test_auto_mode_compiles_on_the_second_apply(engine, port):
-    # fused_jit = 2: a circuit structure new to the process runs on the
-    # precompiled kernels; its second apply compiles and runs the block kernels
-    old = {k: capi.tuning_get(k) for k in ("fused_jit", "jit_min_qubits")}
+    # fused_jit = 2 with jit_after = 2: a circuit structure new to the process
+    # runs on the precompiled kernels; its second apply compiles and runs the
+    # block kernels
+    old = {k: capi.tuning_get(k) for k in ("fused_jit", "jit_min_qubits", "jit_after")}
     try:
         capi.tuning_set("fused_jit", 2)
         capi.tuning_set("jit_min_qubits", 19)
+        capi.tuning_set("jit_after", 2)
         n = 19
         g = W.random_layers(n, 3, seed=99, mixed=True)
         s0 = capi.jit_stats()
@@ -186,3 +188,32 @@ def test_jit_density_matrix(jit):
     capi.tuning_set("fused_jit", 1)
     assert np.abs(a - b).max() < 1e-13
     assert abs(np.trace(a) - 1.0) < 1e-12
+
+
+def test_prepare_compiles_before_the_first_apply(engine, port):
+    # kt_sv_prepare compiles a circuit's block kernels up front; an apply of the
+    # same structure with other angles then runs them at once, and a plan
+    # served from the plan cache takes the new angles
+    old = {k: capi.tuning_get(k) for k in ("fused_jit", "jit_min_qubits", "jit_after")}
+    try:
+        capi.tuning_set("fused_jit", 2)
+        capi.tuning_set("jit_min_qubits", 17)
+        capi.tuning_set("jit_after", 0)
+        n = 17
+        gates, params = W.hea(n, 3, seed=61)
+        sv = capi.Statevector(n)
+        k0 = capi.jit_stats()["kernels"]
+        sv.prepare(gates, params)
+        s1 = capi.jit_stats()
+        assert s1["kernels"] > k0
+        for shift in (0.0, 0.41, -1.3):
+            p = params + shift
+            sv.set_basis(0)
+            sv.apply(gates, p)
+            assert np.abs(sv.download() - port.apply(n, basis(n), gates, p)).max() < 1e-12
+        s2 = capi.jit_stats()
+        assert s2["kernels"] == s1["kernels"] and s2["launches"] > s1["launches"]
+        sv.close()
+    finally:
+        for k, v in old.items():
+            capi.tuning_set(k, v)

@@ -55,3 +55,24 @@ def test_diagonal_gates_cost_no_tile_qubit():
     recs = [W.gate("RZ", q, angle=0.1 * q) for q in range(n)] + [W.gate("CZ", (q + 1) % n, control=q) for q in range(n)]
     st = capi.plan_stats(n, np.concatenate(recs))
     assert st["blocks"] == 1
+
+
+def test_lookahead_takes_fewer_passes():
+    # pinning a block's tile to the qubits the next gates need most (with a
+    # two-block lookahead) never costs passes on these circuits and saves some
+    cases = [(30, W.random_layers(30, 40, seed=2024, mixed=True)), (26, W.random_layers(26, 20, seed=5, mixed=False)),
+             (28, W.random_layers(28, 30, seed=7, mixed=True))]
+    old = capi.tuning_get("plan_lookahead")
+    try:
+        saved = 0
+        for n, g in cases:
+            capi.tuning_set("plan_lookahead", 0)
+            greedy = capi.plan_stats(n, g)
+            capi.tuning_set("plan_lookahead", 1)
+            look = capi.plan_stats(n, g)
+            assert look["ops"] == greedy["ops"] == len(g)
+            assert look["blocks"] <= greedy["blocks"]
+            saved += greedy["blocks"] - look["blocks"]
+        assert saved > 0
+    finally:
+        capi.tuning_set("plan_lookahead", old)
