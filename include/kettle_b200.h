@@ -148,9 +148,12 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               shared-memory transpose (1) or run as ops (0)
  *   c64_renormalize    0 or 1   complex64 applies rescale every fused block to the
  *                               norm the state had when the apply began (1)
- *   plan_lookahead     0 or 1   (1) each fused block's tile qubits chosen among the
+ *   plan_lookahead     0, 1, 2  (1) each fused block's tile qubits chosen among the
  *                               greedy tile and tiles pinned to the qubits the next
- *                               gates need most, by the gates it and the next block take
+ *                               gates need most, by the gates it and the next block
+ *                               (2, or states of >= plan_deep_qubits index bits: the
+ *                               next two blocks) take
+ *   plan_deep_qubits   1..64    (28) see plan_lookahead
  *   fused_jit          0, 1, 2  fused blocks as kernels compiled at run
  *                               time (NVRTC, cached per block structure: gate bodies
  *                               as straight-line code, every slot and mask a

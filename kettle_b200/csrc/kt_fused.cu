@@ -335,7 +335,8 @@ int32_t fused_plan_cached(int n, const std::vector<LGate>& gates, Plan<T>& plan,
     sig.push_back(static_cast<uint64_t>(n) | (static_cast<uint64_t>(sizeof(T)) << 8) |
                   (static_cast<uint64_t>(tu.fused_tile_bits) << 16) | (static_cast<uint64_t>(tu.fold_permutations) << 24) |
                   (static_cast<uint64_t>(tu.fused_reg_bits) << 28) | (static_cast<uint64_t>(tu.plan_lookahead) << 32) |
-                  (static_cast<uint64_t>(tu.fused_max_ops) << 40));
+                  (static_cast<uint64_t>(tu.plan_deep_qubits) << 34) |
+                  (static_cast<uint64_t>(tu.fused_max_ops) << 48));
     for (const LGate& x : gates) {
         sig.push_back(static_cast<uint64_t>(gate_class(x)) | (static_cast<uint64_t>(x.target & 0xFFFF) << 8) |
                       (static_cast<uint64_t>(x.control & 0xFFFF) << 24));

@@ -71,7 +71,7 @@ uint64_t bit(int q)
 // blocked.  Returns the number of gates taken; `take` (if not null) gets them.
 size_t scan_block(const std::vector<LGate>& g, const std::vector<int>& pend, const std::vector<uint32_t>& mark,
                   uint32_t skip, int n, int K, int L, size_t max_ops, uint64_t fixed, uint64_t* Q_out,
-                  std::vector<int>* take)
+                  std::vector<int>* take, const std::vector<uint32_t>* mark2 = nullptr, uint32_t skip2 = 0)
 {
     const uint64_t all = (n >= 64) ? ~uint64_t {0} : (bit(n) - 1);
     uint64_t Q = fixed != 0 ? fixed : (bit(L) - 1);
@@ -82,6 +82,9 @@ size_t scan_block(const std::vector<LGate>& g, const std::vector<int>& pend, con
     }
     for (const int idx : pend) {
         if (skip != 0 && mark[static_cast<size_t>(idx)] == skip) {
+            continue;
+        }
+        if (mark2 != nullptr && skip2 != 0 && (*mark2)[static_cast<size_t>(idx)] == skip2) {
             continue;
         }
         const LGate& x = g[idx];
@@ -115,7 +118,8 @@ size_t scan_block(const std::vector<LGate>& g, const std::vector<int>& pend, con
 // first `window` pending non-diagonal gates (not marked `skip`) target most
 // often (earliest first among equals).
 uint64_t lookahead_tile(const std::vector<LGate>& g, const std::vector<int>& pend, const std::vector<uint32_t>& mark,
-                        uint32_t skip, int n, int K, int L, size_t window)
+                        uint32_t skip, int n, int K, int L, size_t window, const std::vector<uint32_t>* mark2 = nullptr,
+                        uint32_t skip2 = 0)
 {
     int count[64] = {};
     size_t first[64];
@@ -128,6 +132,9 @@ uint64_t lookahead_tile(const std::vector<LGate>& g, const std::vector<int>& pen
             break;
         }
         if (skip != 0 && mark[static_cast<size_t>(idx)] == skip) {
+            continue;
+        }
+        if (mark2 != nullptr && skip2 != 0 && (*mark2)[static_cast<size_t>(idx)] == skip2) {
             continue;
         }
         const LGate& x = g[idx];
@@ -158,11 +165,13 @@ uint64_t lookahead_tile(const std::vector<LGate>& g, const std::vector<int>& pen
 // Candidate tiles for a block: 0 (the tile grows as gates arrive) and the
 // lookahead tiles of several windows.
 void tile_candidates(const std::vector<LGate>& g, const std::vector<int>& pend, const std::vector<uint32_t>& mark,
-                     uint32_t skip, int n, int K, int L, std::vector<uint64_t>& c)
+                     uint32_t skip, int n, int K, int L, std::vector<uint64_t>& c,
+                     const std::vector<uint32_t>* mark2 = nullptr, uint32_t skip2 = 0)
 {
     c.assign(1, 0);
     for (int w : {1, 2, 3, 4, 6, 8, 12, 16, 32, 64}) {
-        const uint64_t q = lookahead_tile(g, pend, mark, skip, n, K, L, static_cast<size_t>(w) * static_cast<size_t>(K));
+        const uint64_t q = lookahead_tile(g, pend, mark, skip, n, K, L, static_cast<size_t>(w) * static_cast<size_t>(K),
+                                          mark2, skip2);
         if (std::find(c.begin(), c.end(), q) == c.end()) {
             c.push_back(q);
         }
@@ -176,9 +185,14 @@ std::vector<PlanBlock> form_blocks(const std::vector<LGate>& g, int n, int K, in
     std::iota(pend.begin(), pend.end(), 0);
     const bool look = tuning().plan_lookahead != 0 && K < n && n <= 64;
     std::vector<uint32_t> mark(g.size(), 0);
+    std::vector<uint32_t> mark2(g.size(), 0);
     uint32_t stamp = 0;
-    std::vector<int> take, best_take;
-    std::vector<uint64_t> cand1, cand2;
+    uint32_t stamp2 = 0;
+    // three blocks deep on large states (a pass there costs milliseconds, a
+    // deeper plan ~0.1 s once, the plan cache keeps it), two otherwise
+    const int depth = (tuning().plan_lookahead >= 2 || n >= tuning().plan_deep_qubits) ? 3 : 2;
+    std::vector<int> take, take2, best_take;
+    std::vector<uint64_t> cand1, cand2, cand3;
     while (!pend.empty()) {
         uint64_t Q = 0;
         uint64_t bestQ = 0;
@@ -199,7 +213,23 @@ std::vector<PlanBlock> form_blocks(const std::vector<LGate>& g, int n, int K, in
                 if (take.size() < pend.size()) {
                     tile_candidates(g, pend, mark, stamp, n, K, L, cand2);
                     for (const uint64_t c2 : cand2) {
-                        next = std::max(next, scan_block(g, pend, mark, stamp, n, K, L, max_ops, c2, nullptr, nullptr));
+                        if (depth < 3) {
+                            next = std::max(next, scan_block(g, pend, mark, stamp, n, K, L, max_ops, c2, nullptr, nullptr));
+                            continue;
+                        }
+                        // three blocks deep: this second block, then the best third
+                        const size_t t2 = scan_block(g, pend, mark, stamp, n, K, L, max_ops, c2, nullptr, &take2);
+                        ++stamp2;
+                        for (const int idx : take2) {
+                            mark2[static_cast<size_t>(idx)] = stamp2;
+                        }
+                        size_t third = 0;
+                        tile_candidates(g, pend, mark, stamp, n, K, L, cand3, &mark2, stamp2);
+                        for (const uint64_t c3 : cand3) {
+                            third = std::max(third, scan_block(g, pend, mark, stamp, n, K, L, max_ops, c3, nullptr,
+                                                               nullptr, &mark2, stamp2));
+                        }
+                        next = std::max(next, t2 + third);
                     }
                 }
                 const size_t score = take.size() + next;

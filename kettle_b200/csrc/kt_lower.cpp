@@ -100,8 +100,10 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.c64_renormalize = (v != 0) ? 1 : 0;
     } else if (name == "fused_reg_bits") {
         t.fused_reg_bits = (v == 3) ? 3 : 4;
+    } else if (name == "plan_deep_qubits") {
+        t.plan_deep_qubits = static_cast<int>(std::max(1LL, std::min(64LL, v)));
     } else if (name == "plan_lookahead") {
-        t.plan_lookahead = (v != 0) ? 1 : 0;
+        t.plan_lookahead = static_cast<int>(std::max(0LL, std::min(2LL, v)));
     } else if (name == "fused_jit") {
         t.fused_jit = static_cast<int>(std::max(0LL, std::min(2LL, v)));
     } else if (name == "jit_ctas_per_sm") {
@@ -179,6 +181,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.c64_renormalize;
     } else if (n == "fused_reg_bits") {
         *value = t.fused_reg_bits;
+    } else if (n == "plan_deep_qubits") {
+        *value = t.plan_deep_qubits;
     } else if (n == "plan_lookahead") {
         *value = t.plan_lookahead;
     } else if (n == "fused_jit") {
