@@ -946,7 +946,7 @@ int64_t jit_after_applies(int n, size_t amp_bytes)
         return tuning().jit_after;
     }
     const double pass = std::ldexp(1.0, n) * 2.0 * static_cast<double>(amp_bytes) / 1.5e12;
-    const double threads = std::max(1u, std::thread::hardware_concurrency());
+    const double threads = jit_threads();
     const double k = std::ceil(0.6 / threads / (0.5 * pass));
     return static_cast<int64_t>(std::max(2.0, std::min(k, 1.0e9)));
 }

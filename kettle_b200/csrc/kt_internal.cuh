@@ -134,6 +134,8 @@ int32_t adjoint_sweep_fused(State& psi, State& lam, const std::vector<AdjGate>& 
 // run-time compiled block kernels (kt_jit.cpp): compile each source (which may
 // include "kt_fused_dev.cuh") for sm_100a and return its kernels `names[i]`
 bool jit_available(std::string* why);
+// host threads a run-time compile uses
+int jit_threads();
 // (load = false: compile only, no device needed)
 int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<std::vector<std::string>>& names,
                     std::vector<std::vector<const void*>>& kernels, bool load = true);

@@ -119,6 +119,21 @@ std::vector<char> compile_one(const std::string& source, std::string& err)
 
 }  // namespace
 
+int jit_threads()
+{
+    // the host threads one process compiles with: its share of the machine
+    // when several ranks run on it (LOCAL_WORLD_SIZE, as torchrun sets), at
+    // most 16 (each NVRTC instance holds a few hundred MB while it compiles)
+    unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    if (const char* lws = std::getenv("LOCAL_WORLD_SIZE")) {
+        const int ranks = std::atoi(lws);
+        if (ranks > 1) {
+            hw = std::max(1u, hw / static_cast<unsigned>(ranks));
+        }
+    }
+    return static_cast<int>(std::min(16u, hw));
+}
+
 bool jit_available(std::string* why)
 {
     Nvrtc& L = nvrtc();
@@ -164,7 +179,7 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
     }
     std::vector<std::vector<char>> cubins(n);
     std::vector<std::string> errs(n);
-    const size_t workers = std::max<size_t>(1, std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency())));
+    const size_t workers = std::max<size_t>(1, std::min<size_t>(n, static_cast<size_t>(jit_threads())));
     std::vector<std::thread> pool;
     std::mutex m;
     size_t next = 0;
