@@ -154,6 +154,11 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               (2, or states of >= plan_deep_qubits index bits: the
  *                               next two blocks) take
  *   plan_deep_qubits   1..64    (28) see plan_lookahead
+ *   plan_schedule      0 or 1   (1) inside a fused block, a gate whose qubits are
+ *                               free of unplaced earlier gates runs as soon as its
+ *                               target is a register bit of the current layout
+ *                               phase, so a shared-memory transpose comes only when
+ *                               no such gate is left (0: the gates' given order)
  *   fused_jit          0, 1, 2  fused blocks as kernels compiled at run
  *                               time (NVRTC, cached per block structure: gate bodies
  *                               as straight-line code, every slot and mask a
@@ -231,6 +236,16 @@ int32_t kt_sv_prepare(kt_sv sv, const kt_gate* gates, int64_t n_gates, const dou
 int32_t kt_plan_stats(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates,
                       const double* params, int64_t n_params, int64_t* blocks, int64_t* phases,
                       int64_t* ops, int64_t* transposes);
+
+/* Host-only, like kt_plan_stats: the fused planner's gates in the order they
+ * take effect (blocks in order; in a block, each layout phase's gates, then
+ * the X / CX folded into its transpose).  Entries index `gates` (M is not
+ * accepted, as in kt_plan_stats).  *count receives the length; KT_ERR_INVALID
+ * if it exceeds capacity.  Empty when the state is too small for fused
+ * blocks.  No reference counterpart. */
+int32_t kt_plan_order(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates,
+                      const double* params, int64_t n_params, int64_t* order, int64_t capacity,
+                      int64_t* count);
 
 /* What the most recent kt_sv_apply / kt_dm_apply on this handle launched:
  * kernel launches and the algorithmic HBM bytes they move (read + write of

@@ -74,6 +74,7 @@ _SIGS = {
     "kt_sv_apply": ([P, P, I64, P, I64, I32], I32),
     "kt_sv_apply_stats": ([P, C.POINTER(I64), DP], I32),
     "kt_plan_stats": ([I32, I32, P, I64, P, I64, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)], I32),
+    "kt_plan_order": ([I32, I32, P, I64, P, I64, P, I64, C.POINTER(I64)], I32),
     "kt_sv_expect": ([P, P, I64, P, P, P], I32),
     "kt_sv_expect_noalloc": ([P, I32, I32, P, I64, P, P, P, P], I32),
     "kt_sv_probabilities": ([P, P, P], I32),
@@ -158,6 +159,17 @@ def plan_stats(n_qubits: int, gates: np.ndarray, params: np.ndarray | None = Non
     check(lib().kt_plan_stats(n_qubits, dtype, ptr(g), g.size, ptr(p), 0 if p is None else p.size,
                               *[C.byref(o) for o in out]))
     return dict(zip(("blocks", "phases", "ops", "transposes"), (int(o.value) for o in out)))
+
+
+def plan_order(n_qubits: int, gates: np.ndarray, params: np.ndarray | None = None, dtype: int = KT_C128) -> np.ndarray:
+    """Host-only: the fused planner's gates (lowered-stream indices) in the order they take effect."""
+    g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+    p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+    out = np.zeros(max(1, 2 * g.size), dtype=np.int64)
+    cnt = I64(0)
+    check(lib().kt_plan_order(n_qubits, dtype, ptr(g), g.size, ptr(p), 0 if p is None else p.size,
+                              ptr(out), out.size, C.byref(cnt)))
+    return out[:cnt.value].copy()
 
 
 def jit_stats() -> dict:

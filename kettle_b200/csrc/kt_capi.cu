@@ -382,6 +382,40 @@ int32_t kt_plan_stats(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int
     });
 }
 
+int32_t kt_plan_order(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates, const double* params,
+                      int64_t n_params, int64_t* order, int64_t capacity, int64_t* count)
+{
+    return guard([&]() -> int32_t {
+        if (count == nullptr || capacity < 0 || (capacity > 0 && order == nullptr)) {
+            return invalid("bad output array");
+        }
+        if (const int32_t rc = check_dtype(dtype); rc != KT_OK) {
+            return rc;
+        }
+        if (n_qubits < 1 || n_qubits > 40 || n_gates < 0 || (n_gates > 0 && gates == nullptr)) {
+            return invalid("bad qubit count or gate array");
+        }
+        std::vector<kt::LGate> lg;
+        if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, n_qubits, lg); rc != KT_OK) {
+            return rc;
+        }
+        int64_t blocks = 0, phases = 0, ops = 0, transposes = 0;
+        std::vector<int32_t> run;
+        if (const int32_t rc = kt::plan_stats(n_qubits, dtype, lg, &blocks, &phases, &ops, &transposes, &run);
+            rc != KT_OK) {
+            return rc;
+        }
+        *count = static_cast<int64_t>(run.size());
+        if (*count > capacity) {
+            return invalid("order array too small");
+        }
+        for (size_t i = 0; i < run.size(); ++i) {
+            order[i] = run[i];
+        }
+        return KT_OK;
+    });
+}
+
 int32_t kt_sv_apply_stats(kt_sv sv, int64_t* launches, double* alg_bytes)
 {
     if (sv == nullptr) {

@@ -335,7 +335,7 @@ int32_t fused_plan_cached(int n, const std::vector<LGate>& gates, Plan<T>& plan,
     sig.push_back(static_cast<uint64_t>(n) | (static_cast<uint64_t>(sizeof(T)) << 8) |
                   (static_cast<uint64_t>(tu.fused_tile_bits) << 16) | (static_cast<uint64_t>(tu.fold_permutations) << 24) |
                   (static_cast<uint64_t>(tu.fused_reg_bits) << 28) | (static_cast<uint64_t>(tu.plan_lookahead) << 32) |
-                  (static_cast<uint64_t>(tu.plan_deep_qubits) << 34) |
+                  (static_cast<uint64_t>(tu.plan_deep_qubits) << 34) | (static_cast<uint64_t>(tu.plan_schedule) << 42) |
                   (static_cast<uint64_t>(tu.fused_max_ops) << 48));
     for (const LGate& x : gates) {
         sig.push_back(static_cast<uint64_t>(gate_class(x)) | (static_cast<uint64_t>(x.target & 0xFFFF) << 8) |
@@ -1511,7 +1511,8 @@ namespace
 {
 
 template <typename T>
-void plan_only(int n, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases, int64_t* ops, int64_t* transposes)
+void plan_only(int n, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases, int64_t* ops, int64_t* transposes,
+               std::vector<int32_t>* order)
 {
     *blocks = 0;
     *phases = 0;
@@ -1530,17 +1531,23 @@ void plan_only(int n, const std::vector<LGate>& gates, int64_t* blocks, int64_t*
     *phases = static_cast<int64_t>(plan.phases.size());
     *ops = static_cast<int64_t>(plan.ops.size()) + plan.folded;  // every gate placed, folded ones included
     *transposes = plan.transposes;
+    if (order != nullptr) {
+        *order = plan.run_order;
+    }
 }
 
 }  // namespace
 
 int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases,
-                   int64_t* ops, int64_t* transposes)
+                   int64_t* ops, int64_t* transposes, std::vector<int32_t>* order)
 {
+    if (order != nullptr) {
+        order->clear();
+    }
     if (dtype == KT_C128) {
-        plan_only<double>(n, gates, blocks, phases, ops, transposes);
+        plan_only<double>(n, gates, blocks, phases, ops, transposes, order);
     } else {
-        plan_only<float>(n, gates, blocks, phases, ops, transposes);
+        plan_only<float>(n, gates, blocks, phases, ops, transposes, order);
     }
     return KT_OK;
 }

@@ -327,6 +327,7 @@ struct Plan
     std::vector<FPhase> phases;
     std::vector<OPT> ops;
     std::vector<int32_t> op_gate;  // the gate (index into the planned gate list) each op runs
+    std::vector<int32_t> run_order;  // every planned gate in the order it takes effect (folded ones included)
     int transposes {0};
     int folded {0};   // X / CX gates folded into transposes
 };
@@ -383,9 +384,11 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
             need[k] = loc[x.target];
         }
     }
+    // gates already placed in a phase (list scheduling may run them out of order)
+    std::vector<char> done(m, 0);
     auto next_use = [&](int b, size_t from) -> size_t {
         for (size_t k = from; k < m; ++k) {
-            if (need[k] == b) {
+            if (!done[k] && need[k] == b) {
                 return k;
             }
         }
@@ -397,7 +400,7 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
     auto choose = [&](size_t from, const std::vector<int>& keep) -> std::vector<int> {
         std::vector<int> regs;
         for (size_t k = from; k < m && static_cast<int>(regs.size()) < RB; ++k) {
-            if (need[k] >= 0 && std::find(regs.begin(), regs.end(), need[k]) == regs.end()) {
+            if (!done[k] && need[k] >= 0 && std::find(regs.begin(), regs.end(), need[k]) == regs.end()) {
                 regs.push_back(need[k]);
             }
         }
@@ -459,13 +462,15 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
         }
         return true;
     };
-    for (size_t k = 0; k < m; ++k) {
+    // place gate k in the open phase, or start a new phase for it
+    auto place = [&](size_t k) {
         const LGate& x = g[pb.gates[k]];
         const uint64_t qm = tile_mask(x);
+        done[k] = 1;
         if (fold[k]) {
             open.folds.push_back(k);
             pending |= qm;
-            continue;
+            return;
         }
         const bool miss = need[k] >= 0 && std::find(cur.begin(), cur.end(), need[k]) == cur.end();
         if (!miss && (qm & pending) != 0 && targets_in_regs(open)) {
@@ -478,12 +483,62 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
             // register set is chosen by next use
             ph.push_back(open);
             std::vector<int> keep = cur;
-            std::sort(keep.begin(), keep.end(), [&](int a, int b2) { return next_use(a, k) < next_use(b2, k); });
-            cur = choose(k, keep);
+            done[k] = 0;
+            std::sort(keep.begin(), keep.end(), [&](int a, int b2) { return next_use(a, 0) < next_use(b2, 0); });
+            cur = choose(0, keep);
+            done[k] = 1;
             open = PhaseSpec {cur, {}, {}};
             pending = 0;
         }
         open.ops.push_back(k);
+    };
+    if (tuning().plan_schedule == 0) {
+        for (size_t k = 0; k < m; ++k) {
+            place(k);
+        }
+    } else {
+        // List scheduling: a gate is ready once every earlier gate sharing a
+        // qubit with it is placed (gates on disjoint qubits commute, so any
+        // such order gives the same state).  The earliest ready gate that fits
+        // the open phase goes next: a folded permutation always fits (the
+        // store composes them in order); another gate fits when its target is
+        // a register bit (or it is diagonal) and no pending permutation is on
+        // its qubits.  Only when no ready gate fits does the earliest ready
+        // one go, through place(), which may start a phase.  That gate is the
+        // earliest unplaced one, so the next register set serves it first.
+        std::vector<uint64_t> qmask(m);
+        for (size_t k = 0; k < m; ++k) {
+            const LGate& x = g[pb.gates[k]];
+            qmask[k] = bit(x.target) | (x.control >= 0 ? bit(x.control) : 0);
+        }
+        size_t placed = 0;
+        while (placed < m) {
+            size_t pick = SIZE_MAX;
+            size_t first_ready = SIZE_MAX;
+            uint64_t blocked = 0;  // qubits of unplaced gates seen so far (in gate order)
+            for (size_t k = 0; k < m; ++k) {
+                if (done[k]) {
+                    continue;
+                }
+                const bool rdy = (blocked & qmask[k]) == 0;
+                blocked |= qmask[k];
+                if (!rdy) {
+                    continue;
+                }
+                if (first_ready == SIZE_MAX) {
+                    first_ready = k;
+                }
+                const uint64_t qm = tile_mask(g[pb.gates[k]]);
+                const bool fits = fold[k] || ((need[k] < 0 || std::find(cur.begin(), cur.end(), need[k]) != cur.end()) &&
+                                              (qm & pending) == 0);
+                if (fits) {
+                    pick = k;
+                    break;
+                }
+            }
+            place(pick != SIZE_MAX ? pick : first_ready);
+            ++placed;
+        }
     }
     if (!open.folds.empty() && !has_low(cur) && targets_in_regs(open)) {
         open.ops.insert(open.ops.end(), open.folds.begin(), open.folds.end());
@@ -544,6 +599,15 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
     }
     fb.phase_end = static_cast<int32_t>(plan.phases.size());
     plan.transposes += static_cast<int>(ph.size()) - 1;
+    // a phase's ops run first, its folded permutations at its store
+    for (const auto& spec : ph) {
+        for (size_t k : spec.ops) {
+            plan.run_order.push_back(pb.gates[k]);
+        }
+        for (size_t f : spec.folds) {
+            plan.run_order.push_back(pb.gates[f]);
+        }
+    }
     // ops, resolved against the layout of their phase
     for (size_t pi = 0; pi < ph.size(); ++pi) {
         const auto& sb = slots[pi];

@@ -147,9 +147,10 @@ void jit_unload_all();
 int32_t jit_prepare(State& s, const std::vector<LGate>& gates);
 // kernels compiled so far, block launches through them, and whether compiling failed
 void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed);
-// host-only: what the fused planner makes of a gate stream
+// host-only: what the fused planner makes of a gate stream; *order (if given)
+// receives the planned gates in the order they take effect
 int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases,
-                   int64_t* ops, int64_t* transposes);
+                   int64_t* ops, int64_t* transposes, std::vector<int32_t>* order = nullptr);
 
 // reductions
 int32_t expect_paulis(State& s, const kt_pauli* strings, int64_t n_strings, const double* coeffs,
@@ -188,6 +189,7 @@ struct Tuning
     int fold_permutations {1};   // 1: X / CX inside a tile become part of a transpose, 0: ops
     int c64_renormalize {1};     // 1: complex64 applies keep the state's norm (per-block rescaling)
     int fused_reg_bits {4};      // complex128 amplitudes per thread in fused blocks: 2^4, or 2^3 (more warps)
+    int plan_schedule {1};       // 1: a block's gates run in the dependency order that saves transposes; 0: as given
     int plan_deep_qubits {28};   // states of at least this many index bits plan three blocks deep
     int plan_lookahead {1};      // 1: a block's tile may be pinned to the qubits the next gates need most
     int fused_jit {2};           // complex128 blocks as run-time compiled kernels: 0 never, 1 always,

@@ -108,7 +108,9 @@ def test_adjoint_checkpoints_match(engine):
     strings, coeffs = W.xxz_chain(n, seed=8)
     e0, g0, _ = adjoint(n, gates, params, strings, coeffs, checkpoint=0)
     e1, g1, _ = adjoint(n, gates, params, strings, coeffs, checkpoint=16)
-    assert e0 == e1
+    # each checkpoint segment is planned on its own, so gates on disjoint
+    # qubits may run in another (equally valid) order: equal to rounding
+    assert abs(e0 - e1) < 1e-13
     assert np.abs(g0 - g1).max() < 1e-12
 
 
