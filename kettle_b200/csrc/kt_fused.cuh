@@ -386,6 +386,14 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
     }
     // gates already placed in a phase (list scheduling may run them out of order)
     std::vector<char> done(m, 0);
+    // every qubit of each gate (dependencies) and its tile bits (pending permutations)
+    std::vector<uint64_t> qmask(m), tmask(m);
+    for (size_t k = 0; k < m; ++k) {
+        const LGate& x = g[pb.gates[k]];
+        qmask[k] = bit(x.target) | (x.control >= 0 ? bit(x.control) : 0);
+        tmask[k] = (loc[x.target] >= 0 ? bit(loc[x.target]) : 0) |
+                   (x.control >= 0 && loc[x.control] >= 0 ? bit(loc[x.control]) : 0);
+    }
     auto next_use = [&](int b, size_t from) -> size_t {
         for (size_t k = from; k < m; ++k) {
             if (!done[k] && need[k] == b) {
@@ -416,6 +424,72 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
         }
         std::sort(regs.begin(), regs.end());
         return regs;
+    };
+    // The gates a phase with register set R would take from the unplaced ones
+    // under list scheduling, in one pass: a gate is taken when no earlier
+    // untaken gate shares a qubit with it and it fits (a later gate never
+    // makes an earlier one ready, and pending permutations only grow).
+    auto phase_gain = [&](const std::vector<int>& R) -> int {
+        uint64_t blocked = 0;
+        uint64_t pend = 0;
+        int taken = 0;
+        for (size_t i = 0; i < m; ++i) {
+            if (done[i]) {
+                continue;
+            }
+            bool ok = (blocked & qmask[i]) == 0;
+            if (ok && fold[i]) {
+                pend |= tmask[i];
+            } else if (ok) {
+                ok = (need[i] < 0 || std::find(R.begin(), R.end(), need[i]) != R.end()) && (tmask[i] & pend) == 0;
+            }
+            if (ok) {
+                ++taken;
+            } else {
+                blocked |= qmask[i];
+            }
+        }
+        return taken;
+    };
+    // register set for a phase that starts with gate k: need[k], then one bit
+    // at a time the one that lets the phase take the most gates (ties: the
+    // order choose() would use)
+    auto choose_gain = [&](size_t k, const std::vector<int>& keep) -> std::vector<int> {
+        std::vector<int> pref;
+        for (size_t i = 0; i < m; ++i) {
+            if (!done[i] && need[i] >= 0 && std::find(pref.begin(), pref.end(), need[i]) == pref.end()) {
+                pref.push_back(need[i]);
+            }
+        }
+        for (int b : keep) {
+            if (std::find(pref.begin(), pref.end(), b) == pref.end()) pref.push_back(b);
+        }
+        for (int b = K - 1; b >= 0; --b) {
+            if (std::find(pref.begin(), pref.end(), b) == pref.end()) pref.push_back(b);
+        }
+        std::vector<int> R;
+        if (need[k] >= 0) {
+            R.push_back(need[k]);
+        }
+        while (static_cast<int>(R.size()) < RB) {
+            int best = -1;
+            int best_gain = -1;
+            for (int b : pref) {
+                if (std::find(R.begin(), R.end(), b) != R.end()) {
+                    continue;
+                }
+                R.push_back(b);
+                const int gn = phase_gain(R);
+                R.pop_back();
+                if (gn > best_gain) {
+                    best_gain = gn;
+                    best = b;
+                }
+            }
+            R.push_back(best);
+        }
+        std::sort(R.begin(), R.end());
+        return R;
     };
     auto has_low = [&](const std::vector<int>& regs) {
         for (int r : regs) {
@@ -485,7 +559,7 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
             std::vector<int> keep = cur;
             done[k] = 0;
             std::sort(keep.begin(), keep.end(), [&](int a, int b2) { return next_use(a, 0) < next_use(b2, 0); });
-            cur = choose(0, keep);
+            cur = tuning().plan_schedule >= 2 ? choose_gain(k, keep) : choose(0, keep);
             done[k] = 1;
             open = PhaseSpec {cur, {}, {}};
             pending = 0;
@@ -506,11 +580,6 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
         // its qubits.  Only when no ready gate fits does the earliest ready
         // one go, through place(), which may start a phase.  That gate is the
         // earliest unplaced one, so the next register set serves it first.
-        std::vector<uint64_t> qmask(m);
-        for (size_t k = 0; k < m; ++k) {
-            const LGate& x = g[pb.gates[k]];
-            qmask[k] = bit(x.target) | (x.control >= 0 ? bit(x.control) : 0);
-        }
         size_t placed = 0;
         while (placed < m) {
             size_t pick = SIZE_MAX;

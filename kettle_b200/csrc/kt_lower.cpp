@@ -101,7 +101,7 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
     } else if (name == "fused_reg_bits") {
         t.fused_reg_bits = (v == 3) ? 3 : 4;
     } else if (name == "plan_schedule") {
-        t.plan_schedule = (v != 0) ? 1 : 0;
+        t.plan_schedule = static_cast<int>(std::max(0LL, std::min(2LL, v)));
     } else if (name == "plan_deep_qubits") {
         t.plan_deep_qubits = static_cast<int>(std::max(1LL, std::min(64LL, v)));
     } else if (name == "plan_lookahead") {
