@@ -295,8 +295,11 @@ uint32_t gate_class(const LGate& x)
     const double* m = x.m;
     const bool real = m[1] == 0.0 && m[3] == 0.0 && m[5] == 0.0 && m[7] == 0.0;
     const bool rxl = m[1] == 0.0 && m[7] == 0.0 && m[0] == m[6] && m[2] == 0.0 && m[4] == 0.0 && m[3] == m[5];
+    // m00 != 0 and m11 = +-m00: the run-time compiled blocks may divide the
+    // gate by m00 (jit_scaled), so these are part of the structure
     return static_cast<uint32_t>(x.kind) | (static_cast<uint32_t>(x.flags & 1) << 4) | (real ? 1u << 5 : 0u) |
-           (rxl ? 1u << 6 : 0u) | (is_pure_x(x) ? 1u << 7 : 0u);
+           (rxl ? 1u << 6 : 0u) | (is_pure_x(x) ? 1u << 7 : 0u) | (m[0] != 0.0 ? 1u << 8 : 0u) |
+           (m[6] == m[0] ? 1u << 9 : 0u) | (m[6] == -m[0] ? 1u << 10 : 0u);
 }
 
 template <typename T>
@@ -402,6 +405,60 @@ inline bool jit_async(int K, size_t elem_bytes)
     return tuning().jit_async_load != 0 && 2 * (size_t {1} << K) * elem_bytes <= 227 * 1024;
 }
 
+// Scaled forms of the run-time compiled blocks (complex128, jit_scale_ops):
+// an uncontrolled real op with m11 = +-m00 != 0 runs as [[1, p], [q, +-1]]
+// (1: +, 2: -) and an uncontrolled RX-like op with c != 0 as [[1, i t],
+// [i t, 1]] (3); the block's product of the m00 they drop multiplies one
+// other uncontrolled op of the block whose matrix scales every amplitude it
+// touches by the same factor (jit_sink), or, if there is none, every
+// amplitude before the store (an extra matrix slot).
+template <typename T>
+int jit_scaled(const FOp<T>& op)
+{
+    if constexpr (!std::is_same<T, double>::value) {
+        return 0;
+    } else {
+        if (tuning().jit_scale_ops == 0 || op.cslot != NO_SLOT || op.cthr != 0 || op.cglob != 0 || op.m[0] == 0.0) {
+            return 0;
+        }
+        if (op.kind == OP_GENR && op.m[6] == op.m[0]) {
+            return 1;
+        }
+        if (op.kind == OP_GENR && op.m[6] == -op.m[0]) {
+            return 2;
+        }
+        return op.kind == OP_RXL ? 3 : 0;
+    }
+}
+
+// the op (index within block b) that takes the block's scale factor, or -1
+template <typename T>
+int jit_sink(const Plan<T>& plan, size_t b)
+{
+    const FBlock& fb = plan.blocks[b];
+    for (int j = 0; j < fb.op_end - fb.op_begin; ++j) {
+        const FOp<T>& op = plan.ops[static_cast<size_t>(fb.op_begin + j)];
+        const bool unctl = op.cslot == NO_SLOT && op.cthr == 0 && op.cglob == 0;
+        if (unctl && jit_scaled(op) == 0 &&
+            (op.kind == OP_GEN || op.kind == OP_GENR || op.kind == OP_RXL || op.kind == OP_ANTI || op.kind == OP_DIAG)) {
+            return j;
+        }
+    }
+    return -1;
+}
+
+// does block b hold scaled ops, and does their factor need its own slot?
+template <typename T>
+void jit_scale_info(const Plan<T>& plan, size_t b, bool* any, bool* own_slot)
+{
+    const FBlock& fb = plan.blocks[b];
+    *any = false;
+    for (int j = fb.op_begin; j < fb.op_end && !*any; ++j) {
+        *any = jit_scaled(plan.ops[static_cast<size_t>(j)]) != 0;
+    }
+    *own_slot = *any && jit_sink(plan, b) < 0;
+}
+
 template <typename T>
 void jit_emit_op(std::string& s, const FOp<T>& op, int j)
 {
@@ -426,10 +483,19 @@ void jit_emit_op(std::string& s, const FOp<T>& op, int j)
             s += "GenF<$T, RB> f {v, " + cx(0) + ", " + cx(2) + ", " + cx(4) + ", " + cx(6) + "}; " + run(op.tslot);
             break;
         case OP_GENR:
-            s += "GenRF<$T, RB> f {v, " + m(0) + ", " + m(2) + ", " + m(4) + ", " + m(6) + "}; " + run(op.tslot);
+            if (const int sc = jit_scaled(op); sc != 0) {
+                s += std::string("GenRSF<$T, RB, ") + (sc == 2 ? "true" : "false") + "> f {v, " + m(2) + ", " + m(4) +
+                     "}; " + run(op.tslot);
+            } else {
+                s += "GenRF<$T, RB> f {v, " + m(0) + ", " + m(2) + ", " + m(4) + ", " + m(6) + "}; " + run(op.tslot);
+            }
             break;
         case OP_RXL:
-            s += "RxF<$T, RB> f {v, " + m(0) + ", " + m(3) + "}; " + run(op.tslot);
+            if (jit_scaled(op) != 0) {
+                s += "RxSF<$T, RB> f {v, " + m(3) + "}; " + run(op.tslot);
+            } else {
+                s += "RxF<$T, RB> f {v, " + m(0) + ", " + m(3) + "}; " + run(op.tslot);
+            }
             break;
         case OP_ANTI:
             s += "AntiF<$T, RB, false> f {v, " + cx(2) + ", " + cx(4) + "}; " + run(op.tslot);
@@ -512,6 +578,9 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     const int R = 1 << RB;
     const int np = fb.phase_end - fb.phase_begin;
     const int nops = std::max(1, fb.op_end - fb.op_begin);
+    bool scaled_any = false;
+    bool scale_slot = false;
+    jit_scale_info(plan, b, &scaled_any, &scale_slot);
     const FPhase* ph = plan.phases.data() + fb.phase_begin;
     std::vector<uint64_t> free_strides(static_cast<size_t>(std::max(1, fb.nfree)));
     for (int k = 0; k < fb.nfree; ++k) {
@@ -538,7 +607,7 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     std::string s;
     s.reserve(32768);
     s += std::string("(void* a_, unsigned long long n_tiles, ") + (norm ? "kt::NormArgs na, " : "") +
-         "const __grid_constant__ $M<" + std::to_string(8 * nops) + "> M)\n{\n";
+         "const __grid_constant__ $M<" + std::to_string(8 * (nops + (scale_slot ? 1 : 0))) + "> M)\n{\n";
     s += "    using namespace kt;\n    using C = $C;\n";
     s += "    constexpr int RB = " + std::to_string(RB) + ";\n";
     s += "    C* __restrict__ a = static_cast<C*>(a_);\n";
@@ -731,6 +800,14 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
             s += "        }\n        asm volatile(\"cp.async.commit_group;\" ::: \"memory\");\n";
         }
     }
+    if (scale_slot) {
+        // the factor the scaled ops dropped, with no other op to take it
+        s += "        {\n            const $T sc = M.m[" + std::to_string(8 * nops) + "];\n";
+        for (int i = 0; i < R; ++i) {
+            s += "            v[" + std::to_string(i) + "].x *= sc;\n            v[" + std::to_string(i) + "].y *= sc;\n";
+        }
+        s += "        }\n";
+    }
     s += "        {\n            C* dst = a + base + " + jit_deposit("t", ph[last].tstride, TB) + ";\n";
     for (int i = 0; i < R; ++i) {
         s += "            dst[" + std::to_string(reg_off(ph[last], i)) + "ULL] = v[" + std::to_string(i) + "];\n";
@@ -760,16 +837,45 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
 }
 
 // the matrices of block b's ops, in the layout of its kernel's parameter M
+// Block b's matrix parameter.  Scaled ops carry p = m01 / m00, q = m10 / m00
+// (or t = s / c); the product of their m00 multiplies the sink op's entries
+// or fills the extra slot.  *ok is false when that product is below 1e-150
+// (amplitudes inside the block would grow past 1e150): the block kernels
+// then do not run this apply.
 template <typename T>
-std::vector<T> jit_block_mats(const Plan<T>& plan, size_t b)
+std::vector<T> jit_block_mats(const Plan<T>& plan, size_t b, bool* ok)
 {
     const FBlock& fb = plan.blocks[b];
     const int nops = std::max(1, fb.op_end - fb.op_begin);
-    std::vector<T> m(static_cast<size_t>(8 * nops), T(0));
+    bool any = false;
+    bool own_slot = false;
+    jit_scale_info(plan, b, &any, &own_slot);
+    std::vector<T> m(static_cast<size_t>(8 * (nops + (own_slot ? 1 : 0))), T(0));
+    double factor = 1.0;
     for (int j = 0; j < fb.op_end - fb.op_begin; ++j) {
         const FOp<T>& op = plan.ops[static_cast<size_t>(fb.op_begin + j)];
         for (int e = 0; e < 8; ++e) {
             m[static_cast<size_t>(8 * j + e)] = op.m[e];
+        }
+        const int sc = jit_scaled(op);
+        if (sc == 1 || sc == 2) {
+            m[static_cast<size_t>(8 * j + 2)] = static_cast<T>(static_cast<double>(op.m[2]) / static_cast<double>(op.m[0]));
+            m[static_cast<size_t>(8 * j + 4)] = static_cast<T>(static_cast<double>(op.m[4]) / static_cast<double>(op.m[0]));
+            factor *= static_cast<double>(op.m[0]);
+        } else if (sc == 3) {
+            m[static_cast<size_t>(8 * j + 3)] = static_cast<T>(static_cast<double>(op.m[3]) / static_cast<double>(op.m[0]));
+            factor *= static_cast<double>(op.m[0]);
+        }
+    }
+    *ok = !any || std::fabs(factor) >= 1e-150;
+    if (any) {
+        if (own_slot) {
+            m[static_cast<size_t>(8 * nops)] = static_cast<T>(factor);
+        } else {
+            const int j = jit_sink(plan, b);
+            for (int e = 0; e < 8; ++e) {
+                m[static_cast<size_t>(8 * j + e)] *= static_cast<T>(factor);
+            }
         }
     }
     return m;
@@ -998,7 +1104,8 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
                                std::to_string(smem_attr) + "/" + (norm ? "n" : "-") + "/" +
                                std::to_string(jit_async(K, sizeof(C)) ? 1 : 0) + "/" +
                                std::to_string(tuning().jit_prefetch) + std::to_string(tuning().jit_merge_diag) +
-                               std::to_string(tuning().jit_skip_io) + std::to_string(tuning().jit_fence);
+                               std::to_string(tuning().jit_skip_io) + std::to_string(tuning().jit_fence) +
+                               std::to_string(tuning().jit_scale_ops);
     bool ready = false;
     bool compile = compile_only || mode == 1;
     {
@@ -1038,8 +1145,16 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
     double* target = parts;
     double* out[2] = {norm ? parts + np : nullptr, norm ? parts + 2 * np : nullptr};
     const double pass_bytes = 2.0 * static_cast<double>(sizeof(C)) * static_cast<double>(s.n_amps());
+    std::vector<std::vector<T>> all_mats(plan.blocks.size());
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
-        std::vector<T> mats = jit_block_mats<T>(plan, b);
+        bool ok = true;
+        all_mats[b] = jit_block_mats<T>(plan, b, &ok);
+        if (!ok) {
+            return false;  // scale factors out of range: the precompiled kernels run this apply
+        }
+    }
+    for (size_t b = 0; b < plan.blocks.size(); ++b) {
+        std::vector<T>& mats = all_mats[b];
         cudaError_t e = cudaSuccess;
         if (norm) {
             NormArgs na {};

@@ -261,6 +261,67 @@ struct RxF
     }
 };
 
+// A real gate with m11 = +-m00 != 0 divided by m00, [[1, p], [q, +-1]]; its
+// factor m00 is applied once per block elsewhere (run-time compiled blocks):
+// one FMA per component instead of a multiply and an FMA.
+template <typename T, int RB, bool NEG>
+struct GenRSF
+{
+    using C = typename CxT<T>::type;
+    C (&v)[1 << RB];
+    T p, q;
+    int crt = -1;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (lower_of_pair<S, CS>(i, crt)) {
+                const int j = i | (1 << S);
+                const C a = v[i];
+                const C b = v[j];
+                C x, y;
+                x.x = fma(p, b.x, a.x);
+                x.y = fma(p, b.y, a.y);
+                y.x = fma(q, a.x, NEG ? -b.x : b.x);
+                y.y = fma(q, a.y, NEG ? -b.y : b.y);
+                v[i] = x;
+                v[j] = y;
+            }
+        }
+    }
+};
+
+// [[1, i t], [i t, 1]]: an RX-like gate [[c, i s], [i s, c]] divided by c != 0
+// (t = s / c), its factor c applied once per block elsewhere
+template <typename T, int RB>
+struct RxSF
+{
+    using C = typename CxT<T>::type;
+    C (&v)[1 << RB];
+    T t;
+    int crt = -1;
+    template <int S, int CS>
+    __device__ __forceinline__ void run()
+    {
+#pragma unroll
+        for (int i = 0; i < (1 << RB); ++i) {
+            if (lower_of_pair<S, CS>(i, crt)) {
+                const int j = i | (1 << S);
+                const C a = v[i];
+                const C b = v[j];
+                C x, y;
+                x.x = fma(-t, b.y, a.x);
+                x.y = fma(t, b.x, a.y);
+                y.x = fma(-t, a.y, b.x);
+                y.y = fma(t, a.x, b.y);
+                v[i] = x;
+                v[j] = y;
+            }
+        }
+    }
+};
+
 template <typename T, int RB, bool PURE>
 struct AntiF
 {

@@ -128,7 +128,7 @@ def test_auto_mode_compiles_on_the_second_apply(engine, port):
 
 
 @pytest.mark.parametrize("knobs", [
-    {"jit_merge_diag": 0}, {"jit_prefetch": 0}, {"jit_skip_io": 0}, {"jit_fence": 2},
+    {"jit_merge_diag": 0}, {"jit_prefetch": 0}, {"jit_skip_io": 0}, {"jit_fence": 2}, {"jit_scale_ops": 0},
     {"fused_tile_bits": 11, "jit_ctas_per_sm": 3}, {"fused_tile_bits": 13},
 ])
 def test_jit_variants_agree(jit, port, knobs):
@@ -217,3 +217,48 @@ def test_prepare_compiles_before_the_first_apply(engine, port):
     finally:
         for k, v in old.items():
             capi.tuning_set(k, v)
+
+
+def test_scaled_ops(jit, port):
+    # jit_scale_ops: uncontrolled H / RY / RX run divided by their m00, the
+    # block's product of those factors applied once (by another gate of the
+    # block, or before the store); the same state as the unscaled kernels
+    n = 18
+    init = random_state(n, 71)
+    g = W.random_layers(n, 4, seed=71, mixed=True)
+    a = _apply(n, init, g)
+    capi.tuning_set("jit_scale_ops", 0)
+    b = _apply(n, init, g)
+    capi.tuning_set("jit_scale_ops", 1)
+    assert np.abs(a - b).max() < 1e-13
+    assert np.abs(a - port.apply(n, init, g)).max() < 1e-12
+    # only H, RY and CX: no gate of a block takes the factor, it has its own slot
+    recs = []
+    for layer in range(6):
+        recs += [W.gate("H" if (q + layer) % 2 else "RY", q, angle=0.3 + q) for q in range(n)]
+        recs += [W.gate("CX", q + 1, control=q) for q in range(layer % 2, n - 1, 2)]
+    g2 = np.concatenate(recs)
+    s0 = capi.jit_stats()
+    got = _apply(n, init, g2)
+    assert capi.jit_stats()["launches"] > s0["launches"]
+    assert np.abs(got - port.apply(n, init, g2)).max() < 1e-12
+
+
+def test_scaled_ops_out_of_range_fall_back(jit, port):
+    # RY(pi) has m00 = cos(pi / 2) ~ 6e-17: twelve in one block take the
+    # factor below 1e-150, so that apply runs on the precompiled kernels
+    n = 16
+    rng = np.random.default_rng(72)
+    recs = [W.gate("RY", q % 6, angle=np.pi) for q in range(12)] + [W.gate("U", 2, u=W.haar_unitary2(rng))]
+    g = np.concatenate(recs)
+    init = random_state(n, 72)
+    assert capi.plan_stats(n, g)["blocks"] == 1
+    s0 = capi.jit_stats()
+    got = _apply(n, init, g)
+    assert capi.jit_stats()["launches"] == s0["launches"]
+    assert np.abs(got - port.apply(n, init, g)).max() < 1e-12
+    # the same structure with ordinary angles runs the compiled blocks
+    g["angle"][:12] = rng.uniform(0.2, 2.0, 12)
+    got = _apply(n, init, g)
+    assert capi.jit_stats()["launches"] > s0["launches"]
+    assert np.abs(got - port.apply(n, init, g)).max() < 1e-12
