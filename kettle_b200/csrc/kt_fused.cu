@@ -27,6 +27,7 @@
 //  * Loads and stores use a layout whose lane bits are the L lowest qubits:
 //    each warp instruction touches whole 128-byte lines.
 #include <algorithm>
+#include <complex>
 #include <cmath>
 #include <cstdio>
 #include <map>
@@ -405,62 +406,94 @@ inline bool jit_async(int K, size_t elem_bytes)
     return tuning().jit_async_load != 0 && 2 * (size_t {1} << K) * elem_bytes <= 227 * 1024;
 }
 
-// Scaled forms of the run-time compiled blocks (complex128, jit_scale_ops):
-// an uncontrolled real op with m11 = +-m00 != 0 runs as [[1, p], [q, +-1]]
-// (1: +, 2: -) and an uncontrolled RX-like op with c != 0 as [[1, i t],
-// [i t, 1]] (3); the block's product of the m00 they drop multiplies one
-// other uncontrolled op of the block whose matrix scales every amplitude it
-// touches by the same factor (jit_sink), or, if there is none, every
-// amplitude before the store (an extra matrix slot).
+// Scaled forms of the run-time compiled blocks (complex128, jit_scale_ops).
+// An uncontrolled op may run divided by its m00 != 0:
+//   1 / 2  real with m11 = +m00 / -m00:  [[1, p], [q, +-1]]
+//   3      RX-like [[c, i s], [i s, c]]: [[1, i t], [i t, 1]]
+//   4      general complex:              [[1, p], [q, r]]
+//   5      diagonal [d0, d1]:            [1, d1 / d0]
+// The block's product of the m00 they drop multiplies one uncontrolled op
+// that is not scaled and scales every amplitude it touches by the same
+// factor (the sink: a general, anti-diagonal or diagonal op; a real one
+// only when every factor is real), or, with no such op, every amplitude
+// before the store (an extra matrix slot).
 template <typename T>
 int jit_scaled(const FOp<T>& op)
 {
     if constexpr (!std::is_same<T, double>::value) {
         return 0;
     } else {
-        if (tuning().jit_scale_ops == 0 || op.cslot != NO_SLOT || op.cthr != 0 || op.cglob != 0 || op.m[0] == 0.0) {
+        if (tuning().jit_scale_ops == 0 || op.cslot != NO_SLOT || op.cthr != 0 || op.cglob != 0) {
             return 0;
         }
-        if (op.kind == OP_GENR && op.m[6] == op.m[0]) {
-            return 1;
+        const bool nz = op.m[0] != 0.0 || op.m[1] != 0.0;
+        switch (op.kind) {
+            case OP_GENR:
+                return op.m[0] == 0.0 ? 0 : (op.m[6] == op.m[0] ? 1 : (op.m[6] == -op.m[0] ? 2 : 0));
+            case OP_RXL:
+                return op.m[0] != 0.0 ? 3 : 0;
+            case OP_GEN:
+                return nz ? 4 : 0;
+            case OP_DIAG:
+                return nz ? 5 : 0;
+            default:
+                return 0;
         }
-        if (op.kind == OP_GENR && op.m[6] == -op.m[0]) {
-            return 2;
-        }
-        return op.kind == OP_RXL ? 3 : 0;
     }
 }
 
-// the op (index within block b) that takes the block's scale factor, or -1
+struct JitScale
+{
+    int sink {-1};         // op index within the block taking the factor (-1: none)
+    bool any {false};      // some op of the block is scaled
+    bool own_slot {false}; // the factor has its own matrix slot, applied before the store
+};
+
 template <typename T>
-int jit_sink(const Plan<T>& plan, size_t b)
+JitScale jit_scale_plan(const Plan<T>& plan, size_t b)
 {
     const FBlock& fb = plan.blocks[b];
-    for (int j = 0; j < fb.op_end - fb.op_begin; ++j) {
-        const FOp<T>& op = plan.ops[static_cast<size_t>(fb.op_begin + j)];
-        const bool unctl = op.cslot == NO_SLOT && op.cthr == 0 && op.cglob == 0;
-        if (unctl && jit_scaled(op) == 0 &&
-            (op.kind == OP_GEN || op.kind == OP_GENR || op.kind == OP_RXL || op.kind == OP_ANTI || op.kind == OP_DIAG)) {
-            return j;
+    const int nops = fb.op_end - fb.op_begin;
+    auto op_at = [&](int j) -> const FOp<T>& { return plan.ops[static_cast<size_t>(fb.op_begin + j)]; };
+    auto unctl = [](const FOp<T>& op) { return op.cslot == NO_SLOT && op.cthr == 0 && op.cglob == 0; };
+    JitScale js;
+    if constexpr (!std::is_same<T, double>::value) {
+        return js;
+    }
+    if (tuning().jit_scale_ops == 0) {
+        return js;
+    }
+    for (int j = 0; j < nops && js.sink < 0; ++j) {
+        const FOp<T>& op = op_at(j);
+        if (unctl(op) && (op.kind == OP_GEN || op.kind == OP_ANTI || op.kind == OP_DIAG)) {
+            js.sink = j;
         }
     }
-    return -1;
-}
-
-// does block b hold scaled ops, and does their factor need its own slot?
-template <typename T>
-void jit_scale_info(const Plan<T>& plan, size_t b, bool* any, bool* own_slot)
-{
-    const FBlock& fb = plan.blocks[b];
-    *any = false;
-    for (int j = fb.op_begin; j < fb.op_end && !*any; ++j) {
-        *any = jit_scaled(plan.ops[static_cast<size_t>(j)]) != 0;
+    bool cplx = false;
+    for (int j = 0; j < nops; ++j) {
+        const int sc = (j == js.sink) ? 0 : jit_scaled(op_at(j));
+        js.any = js.any || sc != 0;
+        cplx = cplx || sc >= 4;
     }
-    *own_slot = *any && jit_sink(plan, b) < 0;
+    for (int j = 0; j < nops && js.sink < 0 && !cplx; ++j) {
+        const FOp<T>& op = op_at(j);
+        if (unctl(op) && (op.kind == OP_GENR || op.kind == OP_RXL) && jit_scaled(op) == 0) {
+            js.sink = j;
+        }
+    }
+    js.own_slot = js.any && js.sink < 0;
+    return js;
+}
+
+// the scaled form op j of block b runs in (0: none)
+template <typename T>
+int jit_scale_code(const Plan<T>& plan, size_t b, int j, const JitScale& js)
+{
+    return j == js.sink ? 0 : jit_scaled(plan.ops[static_cast<size_t>(plan.blocks[b].op_begin + j)]);
 }
 
 template <typename T>
-void jit_emit_op(std::string& s, const FOp<T>& op, int j)
+void jit_emit_op(std::string& s, const FOp<T>& op, int j, int sc)
 {
     const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
     auto run = [&](int ts) {
@@ -480,10 +513,14 @@ void jit_emit_op(std::string& s, const FOp<T>& op, int j)
     s += "        " + guard + "{\n            ";
     switch (op.kind) {
         case OP_GEN:
-            s += "GenF<$T, RB> f {v, " + cx(0) + ", " + cx(2) + ", " + cx(4) + ", " + cx(6) + "}; " + run(op.tslot);
+            if (sc == 4) {
+                s += "GenSF<$T, RB> f {v, " + cx(2) + ", " + cx(4) + ", " + cx(6) + "}; " + run(op.tslot);
+            } else {
+                s += "GenF<$T, RB> f {v, " + cx(0) + ", " + cx(2) + ", " + cx(4) + ", " + cx(6) + "}; " + run(op.tslot);
+            }
             break;
         case OP_GENR:
-            if (const int sc = jit_scaled(op); sc != 0) {
+            if (sc == 1 || sc == 2) {
                 s += std::string("GenRSF<$T, RB, ") + (sc == 2 ? "true" : "false") + "> f {v, " + m(2) + ", " + m(4) +
                      "}; " + run(op.tslot);
             } else {
@@ -491,7 +528,7 @@ void jit_emit_op(std::string& s, const FOp<T>& op, int j)
             }
             break;
         case OP_RXL:
-            if (jit_scaled(op) != 0) {
+            if (sc == 3) {
                 s += "RxSF<$T, RB> f {v, " + m(3) + "}; " + run(op.tslot);
             } else {
                 s += "RxF<$T, RB> f {v, " + m(0) + ", " + m(3) + "}; " + run(op.tslot);
@@ -504,7 +541,7 @@ void jit_emit_op(std::string& s, const FOp<T>& op, int j)
             s += "AntiF<$T, RB, true> f {v, make_cx<$T>(1, 0), make_cx<$T>(1, 0)}; " + run(op.tslot);
             break;
         default: {
-            const bool one = (op.kind == OP_DIAG1);
+            const bool one = (op.kind == OP_DIAG1) || sc == 5;
             if (op.tslot != NO_SLOT) {
                 s += std::string("DiagRegF<$T, RB, ") + (one ? "true" : "false") + "> f {v, " + cx(0) + ", " + cx(6) +
                      "}; " + run(op.tslot);
@@ -578,9 +615,8 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     const int R = 1 << RB;
     const int np = fb.phase_end - fb.phase_begin;
     const int nops = std::max(1, fb.op_end - fb.op_begin);
-    bool scaled_any = false;
-    bool scale_slot = false;
-    jit_scale_info(plan, b, &scaled_any, &scale_slot);
+    const JitScale js = jit_scale_plan(plan, b);
+    const bool scale_slot = js.own_slot;
     const FPhase* ph = plan.phases.data() + fb.phase_begin;
     std::vector<uint64_t> free_strides(static_cast<size_t>(std::max(1, fb.nfree)));
     for (int k = 0; k < fb.nfree; ++k) {
@@ -753,7 +789,7 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
             if (fence_every > 0 && emitted > 0 && emitted % fence_every == 0) {
                 s += "        kt_jit_fence(v);\n";
             }
-            jit_emit_op(s, plan.ops[static_cast<size_t>(o)], o - fb.op_begin);
+            jit_emit_op(s, plan.ops[static_cast<size_t>(o)], o - fb.op_begin, jit_scale_code(plan, b, o - fb.op_begin, js));
             ++emitted;
         }
         if (merge) {
@@ -761,6 +797,7 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
             for (const int o : scal) {
                 const FOp<T>& op = plan.ops[static_cast<size_t>(o)];
                 const int j = o - fb.op_begin;
+                const bool one_sided = op.kind == OP_DIAG1 || jit_scale_code(plan, b, j, js) == 5;
                 auto cx = [&](int e) {
                     return "make_cx<$T>(M.m[" + std::to_string(8 * j + e) + "], M.m[" + std::to_string(8 * j + e + 1) + "])";
                 };
@@ -785,7 +822,7 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
                     s += "if (" + cond + ") ";
                 }
                 s += "{ const bool b = " + b + "; ";
-                if (op.kind == OP_DIAG1) {
+                if (one_sided) {
                     s += "if (b) { fac = cmul(fac, " + cx(6) + "); } }\n";
                 } else {
                     s += "fac = cmul(fac, b ? " + cx(6) + " : " + cx(0) + "); }\n";
@@ -802,9 +839,10 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     }
     if (scale_slot) {
         // the factor the scaled ops dropped, with no other op to take it
-        s += "        {\n            const $T sc = M.m[" + std::to_string(8 * nops) + "];\n";
+        s += "        {\n            const C sc = make_cx<$T>(M.m[" + std::to_string(8 * nops) + "], M.m[" +
+             std::to_string(8 * nops + 1) + "]);\n";
         for (int i = 0; i < R; ++i) {
-            s += "            v[" + std::to_string(i) + "].x *= sc;\n            v[" + std::to_string(i) + "].y *= sc;\n";
+            s += "            v[" + std::to_string(i) + "] = cmul(sc, v[" + std::to_string(i) + "]);\n";
         }
         s += "        }\n";
     }
@@ -837,44 +875,73 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
 }
 
 // the matrices of block b's ops, in the layout of its kernel's parameter M
-// Block b's matrix parameter.  Scaled ops carry p = m01 / m00, q = m10 / m00
-// (or t = s / c); the product of their m00 multiplies the sink op's entries
-// or fills the extra slot.  *ok is false when that product is below 1e-150
-// (amplitudes inside the block would grow past 1e150): the block kernels
-// then do not run this apply.
+// Block b's matrix parameter.  Scaled ops carry their entries divided by
+// m00 (p = m01 / m00, ...); the product of those m00 multiplies the sink's
+// entries or fills the extra slot.  *ok is false when its magnitude is below
+// 1e-150 (amplitudes inside the block would grow past 1e150): the block
+// kernels then do not run this apply.
 template <typename T>
 std::vector<T> jit_block_mats(const Plan<T>& plan, size_t b, bool* ok)
 {
+    using Z = std::complex<double>;
     const FBlock& fb = plan.blocks[b];
     const int nops = std::max(1, fb.op_end - fb.op_begin);
-    bool any = false;
-    bool own_slot = false;
-    jit_scale_info(plan, b, &any, &own_slot);
-    std::vector<T> m(static_cast<size_t>(8 * (nops + (own_slot ? 1 : 0))), T(0));
-    double factor = 1.0;
+    const JitScale js = jit_scale_plan(plan, b);
+    std::vector<T> m(static_cast<size_t>(8 * (nops + (js.own_slot ? 1 : 0))), T(0));
+    auto put = [&](int j, int e, Z z) {
+        m[static_cast<size_t>(8 * j + e)] = static_cast<T>(z.real());
+        m[static_cast<size_t>(8 * j + e + 1)] = static_cast<T>(z.imag());
+    };
+    Z factor(1.0, 0.0);
     for (int j = 0; j < fb.op_end - fb.op_begin; ++j) {
         const FOp<T>& op = plan.ops[static_cast<size_t>(fb.op_begin + j)];
         for (int e = 0; e < 8; ++e) {
             m[static_cast<size_t>(8 * j + e)] = op.m[e];
         }
-        const int sc = jit_scaled(op);
-        if (sc == 1 || sc == 2) {
-            m[static_cast<size_t>(8 * j + 2)] = static_cast<T>(static_cast<double>(op.m[2]) / static_cast<double>(op.m[0]));
-            m[static_cast<size_t>(8 * j + 4)] = static_cast<T>(static_cast<double>(op.m[4]) / static_cast<double>(op.m[0]));
-            factor *= static_cast<double>(op.m[0]);
-        } else if (sc == 3) {
-            m[static_cast<size_t>(8 * j + 3)] = static_cast<T>(static_cast<double>(op.m[3]) / static_cast<double>(op.m[0]));
-            factor *= static_cast<double>(op.m[0]);
+        auto at = [&](int e) { return Z(static_cast<double>(op.m[e]), static_cast<double>(op.m[e + 1])); };
+        const Z m00 = at(0);
+        switch (jit_scale_code(plan, b, j, js)) {
+            case 1:
+            case 2:
+                m[static_cast<size_t>(8 * j + 2)] = static_cast<T>(static_cast<double>(op.m[2]) / m00.real());
+                m[static_cast<size_t>(8 * j + 4)] = static_cast<T>(static_cast<double>(op.m[4]) / m00.real());
+                factor *= m00.real();
+                break;
+            case 3:
+                m[static_cast<size_t>(8 * j + 3)] = static_cast<T>(static_cast<double>(op.m[3]) / m00.real());
+                factor *= m00.real();
+                break;
+            case 4:
+                put(j, 2, at(2) / m00);
+                put(j, 4, at(4) / m00);
+                put(j, 6, at(6) / m00);
+                factor *= m00;
+                break;
+            case 5:
+                put(j, 6, at(6) / m00);
+                factor *= m00;
+                break;
+            default:
+                break;
         }
     }
-    *ok = !any || std::fabs(factor) >= 1e-150;
-    if (any) {
-        if (own_slot) {
-            m[static_cast<size_t>(8 * nops)] = static_cast<T>(factor);
+    *ok = !js.any || std::abs(factor) >= 1e-150;
+    if (js.any) {
+        if (js.own_slot) {
+            put(nops, 0, factor);
         } else {
-            const int j = jit_sink(plan, b);
-            for (int e = 0; e < 8; ++e) {
-                m[static_cast<size_t>(8 * j + e)] *= static_cast<T>(factor);
+            const FOp<T>& op = plan.ops[static_cast<size_t>(fb.op_begin + js.sink)];
+            if (op.kind == OP_GENR || op.kind == OP_RXL) {
+                // a real sink takes only real factors
+                for (int e = 0; e < 8; ++e) {
+                    m[static_cast<size_t>(8 * js.sink + e)] *= static_cast<T>(factor.real());
+                }
+            } else {
+                for (int e = 0; e < 8; e += 2) {
+                    const Z z(static_cast<double>(m[static_cast<size_t>(8 * js.sink + e)]),
+                              static_cast<double>(m[static_cast<size_t>(8 * js.sink + e + 1)]));
+                    put(js.sink, e, z * factor);
+                }
             }
         }
     }
