@@ -182,13 +182,15 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *   jit_async_load     0 or 1   (0) next tile copied with cp.async into a second
  *                               shared-memory buffer (where two tiles fit a CTA)
  *   jit_fence          0..64    (0) every k gates, an empty asm pins the amplitudes
- *   jit_scale_ops      0 or 1   (1) complex128 compiled blocks run an uncontrolled
- *                               real gate with m11 = +-m00 != 0 (H, RY) or RX-like
- *                               gate divided by m00 (one FMA per component); the
- *                               block's product of those m00 scales one other
- *                               uncontrolled gate of the block (or every amplitude
- *                               before the store); below 1e-150 the apply runs on
- *                               the precompiled kernels
+ *   jit_scale_ops      0 or 1   (1) complex128 compiled blocks run uncontrolled
+ *                               gates divided by m00 != 0: real ones with
+ *                               m11 = +-m00 (H, RY) and RX-like ones at one FMA per
+ *                               component, general ones at 12 FP64 operations per
+ *                               pair instead of 16, two-sided diagonals (RZ) as
+ *                               one-sided; the block's product of those m00 scales
+ *                               one unscaled uncontrolled gate of the block (or
+ *                               every amplitude before the store); below 1e-150 the
+ *                               apply runs on the precompiled kernels
  *   fused_reg_bits     3 or 4   complex128 amplitudes per thread in fused blocks
  *                               (2^4; or 2^3 with twice the warps: 12-qubit tiles of
  *                               512 threads, 2 CTAs per SM, or 11-qubit tiles of 256
