@@ -98,7 +98,7 @@ def test_run_time_block_kernels_compile_on_the_host():
 
 @pytest.mark.parametrize("knobs", [
     {"jit_async_load": 1}, {"fused_reg_bits": 3}, {"jit_fence": 2, "jit_merge_diag": 0},
-    {"jit_skip_io": 0, "jit_prefetch": 0, "fused_tile_bits": 11},
+    {"jit_skip_io": 0, "jit_prefetch": 0, "fused_tile_bits": 11}, {"jit_scale_ops": 0},
 ])
 def test_generated_kernel_variants_compile_on_the_host(knobs):
     from kettle_b200 import workloads as W
@@ -112,3 +112,15 @@ def test_generated_kernel_variants_compile_on_the_host(knobs):
     finally:
         for k, v in old.items():
             capi.tuning_set(k, v)
+
+
+def test_scaled_block_without_a_sink_compiles_on_the_host():
+    # a block of only H, RY and CX has scaled gates and no unscaled gate to
+    # take their factor: the generated kernel applies it before the store
+    from kettle_b200 import workloads as W
+    n = 14
+    recs = []
+    for layer in range(3):
+        recs += [W.gate("H" if (q + layer) % 2 else "RY", q, angle=0.4 + q) for q in range(n)]
+        recs += [W.gate("CX", q + 1, control=q) for q in range(layer % 2, n - 1, 2)]
+    assert capi.jit_compile_only(n, np.concatenate(recs)) >= 1
