@@ -178,7 +178,11 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *   jit_prefetch       0 or 1   (1) each CTA prefetches its next tile into L2
  *   jit_merge_diag     0 or 1   (1) a phase's diagonal gates on thread / tile-external
  *                               qubits applied as one per-thread factor
- *   jit_skip_io        0 or 1   (1) load / store in the first / last compute layout
+ *   jit_skip_io        0, 1, 2  (2) load / store in the first / last compute layout
+ *                               instead of through a transpose: 1 always, 2 only
+ *                               where that layout keeps the lowest tile qubits on
+ *                               the lowest thread bits (whole 128-byte runs per
+ *                               group of lanes), 0 never
  *   jit_async_load     0 or 1   (0) next tile copied with cp.async into a second
  *                               shared-memory buffer (where two tiles fit a CTA)
  *   jit_fence          0..64    (0) every k gates, an empty asm pins the amplitudes

@@ -681,12 +681,31 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
         }
         return true;
     };
-    const bool skip_io = tuning().jit_skip_io != 0;
+    // jit_skip_io: 1 always loads (stores) the tile straight in the layout of
+    // the first (last) compute phase; 2 only where that layout keeps the
+    // lowest tile qubits on the lowest thread bits, so each group of lanes
+    // still moves whole 128-byte runs (otherwise the io transpose stays)
+    const int skip_mode = tuning().jit_skip_io;
+    const bool skip_io = skip_mode != 0;
+    const int L_run = (sizeof(typename CxT<T>::type) == 16) ? 3 : 4;
+    auto coalesced = [&](const FPhase& f) {
+        if (skip_mode != 2) {
+            return true;
+        }
+        for (int j = 0; j < L_run && j < TB; ++j) {
+            if (f.tstride[j] != bit(fb.qubit[j])) {
+                return false;
+            }
+        }
+        return true;
+    };
     // jit_fence = k: every k ops the amplitudes pass through an empty asm, so
     // the scheduler cannot interleave more than k ops (bounds the live registers)
     const int fence_every = tuning().jit_fence;
-    const int first = (skip_io && np > 1 && ph[0].op_begin == ph[0].op_end && identity_store(ph[0])) ? 1 : 0;
-    const int last = (skip_io && np - 1 > first && ph[np - 1].op_begin == ph[np - 1].op_end && identity_store(ph[np - 2]))
+    const int first =
+        (skip_io && np > 1 && ph[0].op_begin == ph[0].op_end && identity_store(ph[0]) && coalesced(ph[1])) ? 1 : 0;
+    const int last = (skip_io && np - 1 > first && ph[np - 1].op_begin == ph[np - 1].op_end &&
+                      identity_store(ph[np - 2]) && coalesced(ph[np - 2]))
                          ? np - 2
                          : np - 1;
     // jit_async_load: each thread copies its next tile's amplitudes (in the

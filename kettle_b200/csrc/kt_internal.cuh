@@ -200,7 +200,8 @@ struct Tuning
     int jit_prefetch {1};        // 1: run-time compiled blocks prefetch their CTA's next tile into L2
     int jit_ctas_per_sm {2};     // CTAs per SM of run-time compiled blocks: 2..4
     int jit_merge_diag {1};      // 1: a phase's diagonal ops on thread / tile-external bits as one factor
-    int jit_skip_io {1};         // 1: no transpose into a block's load layout or out of its store layout
+    int jit_skip_io {2};         // 1: no transpose into a block's load layout or out of its store layout;
+                                 // 2: only where that layout still moves whole 128-byte runs
     int jit_async_load {0};      // 1: run-time compiled blocks load the next tile with cp.async into a second buffer
     int jit_fence {0};           // k > 0: run-time compiled blocks fence the amplitudes every k ops
     int jit_scale_ops {1};       // complex128 blocks: uncontrolled real / RX-like ops divided by m00 (one FMA per component)

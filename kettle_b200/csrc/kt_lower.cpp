@@ -117,7 +117,7 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
     } else if (name == "jit_fence") {
         t.jit_fence = static_cast<int>(std::max(0LL, std::min(64LL, v)));
     } else if (name == "jit_skip_io") {
-        t.jit_skip_io = (v != 0) ? 1 : 0;
+        t.jit_skip_io = static_cast<int>(std::max(0LL, std::min(2LL, v)));
     } else if (name == "jit_merge_diag") {
         t.jit_merge_diag = (v != 0) ? 1 : 0;
     } else if (name == "jit_prefetch") {
