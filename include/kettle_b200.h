@@ -154,14 +154,17 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               (2, or states of >= plan_deep_qubits index bits: the
  *                               next two blocks) take
  *   plan_deep_qubits   1..64    (28) see plan_lookahead
- *   plan_schedule      0, 1, 2  (2) inside a fused block, a gate whose qubits are
+ *   plan_schedule      0..3     (3) inside a fused block, a gate whose qubits are
  *                               free of unplaced earlier gates runs as soon as its
  *                               target is a register bit of the current layout
  *                               phase, so a shared-memory transpose comes only when
- *                               no such gate is left (1, 2; 0: the gates' given
+ *                               no such gate is left (1..3; 0: the gates' given
  *                               order); at a transpose the next register set holds
  *                               the bits used soonest (1) or is built bit by bit to
- *                               take the most gates before the next one (2)
+ *                               take the most gates before the next one (2, 3); with
+ *                               3 a block's first set is built from the bits above
+ *                               the 128-byte runs when that takes any gate, so the
+ *                               tile loads without a transpose
  *   fused_jit          0, 1, 2  fused blocks as kernels compiled at run
  *                               time (NVRTC, cached per block structure: gate bodies
  *                               as straight-line code, every slot and mask a

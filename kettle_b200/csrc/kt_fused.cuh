@@ -517,6 +517,35 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
     };
     std::vector<PhaseSpec> ph;
     std::vector<int> cur = choose(0, {});
+    if (tuning().plan_schedule >= 3 && has_low(cur)) {
+        // a first register set of bits >= L only (built bit by bit by the
+        // gates it takes): the tile loads straight into it, with no transpose
+        std::vector<int> hi;
+        while (static_cast<int>(hi.size()) < RB) {
+            int best = -1;
+            int best_gain = -1;
+            for (int b = K - 1; b >= L; --b) {
+                if (std::find(hi.begin(), hi.end(), b) != hi.end()) {
+                    continue;
+                }
+                hi.push_back(b);
+                const int gn = phase_gain(hi);
+                hi.pop_back();
+                if (gn > best_gain) {
+                    best_gain = gn;
+                    best = b;
+                }
+            }
+            if (best < 0) {
+                break;
+            }
+            hi.push_back(best);
+        }
+        std::sort(hi.begin(), hi.end());
+        if (static_cast<int>(hi.size()) == RB && phase_gain(hi) > 0) {
+            cur = hi;
+        }
+    }
     if (has_low(cur)) {
         ph.push_back({io_regs(), {}, {}});
     }

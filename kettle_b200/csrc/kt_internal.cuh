@@ -189,8 +189,9 @@ struct Tuning
     int fold_permutations {1};   // 1: X / CX inside a tile become part of a transpose, 0: ops
     int c64_renormalize {1};     // 1: complex64 applies keep the state's norm (per-block rescaling)
     int fused_reg_bits {4};      // complex128 amplitudes per thread in fused blocks: 2^4, or 2^3 (more warps)
-    int plan_schedule {2};       // 1: a block's gates run in the dependency order that saves transposes; 2: and each
-                                 // new register set is the one that takes the most gates; 0: the given order
+    int plan_schedule {3};       // 1: a block's gates run in the dependency order that saves transposes; 2: and each
+                                 // new register set is the one that takes the most gates; 3: and the first set
+                                 // avoids the 128-byte run bits when it takes gates; 0: the given order
     int plan_deep_qubits {28};   // states of at least this many index bits plan three blocks deep
     int plan_lookahead {1};      // 1: a block's tile may be pinned to the qubits the next gates need most
     int fused_jit {2};           // complex128 blocks as run-time compiled kernels: 0 never, 1 always,

@@ -103,7 +103,7 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
     } else if (name == "jit_scale_ops") {
         t.jit_scale_ops = (v != 0) ? 1 : 0;
     } else if (name == "plan_schedule") {
-        t.plan_schedule = static_cast<int>(std::max(0LL, std::min(2LL, v)));
+        t.plan_schedule = static_cast<int>(std::max(0LL, std::min(3LL, v)));
     } else if (name == "plan_deep_qubits") {
         t.plan_deep_qubits = static_cast<int>(std::max(1LL, std::min(64LL, v)));
     } else if (name == "plan_lookahead") {

@@ -100,7 +100,7 @@ PLAN_CASES = [(30, W.random_layers(30, 40, seed=2024, mixed=True), None),
               (30, *W.hea(30, 8, seed=1)), (24, *W.hea(24, 6, seed=3))]
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3])
 def test_plan_order_is_a_dependency_order(schedule):
     # blocks take gates ahead of earlier gates on disjoint qubits, and with
     # plan_schedule = 1 a block's gates run in any order that saves
@@ -142,7 +142,12 @@ def test_list_scheduling_takes_fewer_transposes():
             gain = capi.plan_stats(n, g, p)
             assert gain["blocks"] == given["blocks"] and gain["ops"] == len(g)
             assert gain["transposes"] <= sched["transposes"]
-        # the 30-qubit bench circuit: 379 -> 251 -> 243
+            # a first register set above the 128-byte run bits: no more here either
+            capi.tuning_set("plan_schedule", 3)
+            high = capi.plan_stats(n, g, p)
+            assert high["blocks"] == given["blocks"] and high["ops"] == len(g)
+            assert high["transposes"] <= gain["transposes"]
+        # the 30-qubit bench circuit: 379 -> 251 -> 243 -> 239
         assert capi.plan_stats(*PLAN_CASES[0][:2])["transposes"] <= 0.65 * 379
     finally:
         capi.tuning_set("plan_schedule", old)
