@@ -82,8 +82,9 @@ Nvrtc& nvrtc()
     return lib;
 }
 
-// one source -> one cubin (empty on failure, with the reason in `err`)
-std::vector<char> compile_one(const std::string& source, std::string& err)
+// one source -> one cubin (empty on failure, with the reason in `err`); with
+// `info`, ptxas also reports each kernel's registers and spill bytes there
+std::vector<char> compile_one(const std::string& source, std::string& err, std::string* info = nullptr)
 {
     Nvrtc& L = nvrtc();
     nvrtcProgram prog = nullptr;
@@ -94,8 +95,9 @@ std::vector<char> compile_one(const std::string& source, std::string& err)
         return {};
     }
     const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device", "--fmad=true",
-                          "--extra-device-vectorization"};
-    r = L.compile(prog, static_cast<int>(sizeof(opts) / sizeof(opts[0])), opts);
+                          "--extra-device-vectorization", "--ptxas-options=-v"};
+    const int n_opts = static_cast<int>(sizeof(opts) / sizeof(opts[0])) - (info != nullptr ? 0 : 1);
+    r = L.compile(prog, n_opts, opts);
     if (r != NVRTC_SUCCESS) {
         size_t n = 0;
         L.log_size(prog, &n);
@@ -106,6 +108,14 @@ std::vector<char> compile_one(const std::string& source, std::string& err)
         err = std::string("nvrtcCompileProgram: ") + L.error_string(r) + "\n" + log.substr(0, 2000);
         L.destroy(&prog);
         return {};
+    }
+    if (info != nullptr) {
+        size_t m = 0;
+        L.log_size(prog, &m);
+        info->assign(m, '\0');
+        if (m > 0) {
+            L.log(prog, &(*info)[0]);
+        }
     }
     size_t n = 0;
     L.cubin_size(prog, &n);
@@ -167,8 +177,13 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
         return KT_ERR_CUDA;
     }
     const size_t n = sources.size();
-    // KT_JIT_DUMP_DIR: also write each generated program's source there (for inspection)
-    if (const char* dir = std::getenv("KT_JIT_DUMP_DIR"); dir != nullptr && *dir != '\0') {
+    // KT_JIT_DUMP_DIR: also write each generated program's source there, and
+    // ptxas's register / spill summary of its kernels beside it (for inspection)
+    const char* dump_dir = std::getenv("KT_JIT_DUMP_DIR");
+    const bool dump = dump_dir != nullptr && *dump_dir != '\0';
+    std::vector<std::string> infos(n);
+    if (dump) {
+        const char* dir = dump_dir;
         for (size_t i = 0; i < n; ++i) {
             const std::string path = std::string(dir) + "/kt_jit_" + std::to_string(i) + ".cu";
             if (FILE* f = std::fopen(path.c_str(), "w")) {
@@ -194,12 +209,21 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
                     }
                     i = next++;
                 }
-                cubins[i] = compile_one(sources[i], errs[i]);
+                cubins[i] = compile_one(sources[i], errs[i], dump ? &infos[i] : nullptr);
             }
         });
     }
     for (auto& th : pool) {
         th.join();
+    }
+    if (dump) {
+        for (size_t i = 0; i < n; ++i) {
+            const std::string path = std::string(dump_dir) + "/kt_jit_" + std::to_string(i) + ".log";
+            if (FILE* f = std::fopen(path.c_str(), "w")) {
+                std::fwrite(infos[i].data(), 1, infos[i].size(), f);
+                std::fclose(f);
+            }
+        }
     }
     kernels.assign(n, {});
     for (size_t i = 0; i < n; ++i) {

@@ -124,3 +124,15 @@ def test_scaled_block_without_a_sink_compiles_on_the_host():
         recs += [W.gate("H" if (q + layer) % 2 else "RY", q, angle=0.4 + q) for q in range(n)]
         recs += [W.gate("CX", q + 1, control=q) for q in range(layer % 2, n - 1, 2)]
     assert capi.jit_compile_only(n, np.concatenate(recs)) >= 1
+
+
+def test_jit_dump_writes_source_and_register_summary(tmp_path, monkeypatch):
+    # KT_JIT_DUMP_DIR (inspection): each generated program's source and
+    # ptxas's register / spill summary of its kernels
+    from kettle_b200 import workloads as W
+    monkeypatch.setenv("KT_JIT_DUMP_DIR", str(tmp_path))
+    assert capi.jit_compile_only(14, W.random_layers(14, 2, seed=9, mixed=True)) >= 1
+    src = (tmp_path / "kt_jit_0.cu").read_text()
+    log = (tmp_path / "kt_jit_0.log").read_text()
+    assert "__global__" in src
+    assert re.search(r"Used \d+ registers", log) and "spill" in log
