@@ -189,6 +189,10 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *   jit_async_load     0 or 1   (0) next tile copied with cp.async into a second
  *                               shared-memory buffer (where two tiles fit a CTA)
  *   jit_fence          0..64    (0) every k gates, an empty asm pins the amplitudes
+ *   jit_remat          0 or 1   (1) the thread index passes through an empty asm at
+ *                               the top of every tile, so the terms derived from it
+ *                               are recomputed per tile rather than held in
+ *                               registers across the tile loop (fewer spills)
  *   jit_scale_ops      0 or 1   (1) complex128 compiled blocks run uncontrolled
  *                               gates divided by m00 != 0: real ones with
  *                               m11 = +-m00 (H, RY) and RX-like ones at one FMA per

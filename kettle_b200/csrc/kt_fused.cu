@@ -739,7 +739,20 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
         s += issue_async("static_cast<unsigned long long>(blockIdx.x)", "        ");
         s += "    }\n    asm volatile(\"cp.async.commit_group;\" ::: \"memory\");\n";
     }
+    // jit_remat: the thread index passes through an empty asm at the top of
+    // every tile, so the terms derived from it (swizzled shared-memory
+    // offsets, thread masks, thread-bit deposits) are recomputed per tile
+    // instead of being hoisted out of the loop and held in registers (which
+    // made ptxas spill)
+    const bool remat = tuning().jit_remat != 0;
+    if (remat) {
+        s += "    const uint32_t t_outer = t;\n";
+    }
     s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
+    if (remat) {
+        s += "        uint32_t t_l;\n        asm volatile(\"mov.u32 %0, %1;\" : \"=r\"(t_l) : \"r\"(t_outer));\n";
+        s += "        const uint32_t t = t_l;\n";
+    }
     s += "        C v[1 << RB];\n";
     s += "        const uint64_t base = " + jit_deposit("tile", free_strides.data(), fb.nfree) + ";\n";
     if (async_load) {
@@ -1191,7 +1204,7 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
                                std::to_string(jit_async(K, sizeof(C)) ? 1 : 0) + "/" +
                                std::to_string(tuning().jit_prefetch) + std::to_string(tuning().jit_merge_diag) +
                                std::to_string(tuning().jit_skip_io) + std::to_string(tuning().jit_fence) +
-                               std::to_string(tuning().jit_scale_ops);
+                               std::to_string(tuning().jit_scale_ops) + std::to_string(tuning().jit_remat);
     bool ready = false;
     bool compile = compile_only || mode == 1;
     {

@@ -206,6 +206,7 @@ struct Tuning
     int jit_async_load {0};      // 1: run-time compiled blocks load the next tile with cp.async into a second buffer
     int jit_fence {0};           // k > 0: run-time compiled blocks fence the amplitudes every k ops
     int jit_scale_ops {1};       // complex128 blocks: uncontrolled real / RX-like ops divided by m00 (one FMA per component)
+    int jit_remat {1};           // 1: thread-index terms recomputed every tile, not held across the tile loop
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);

@@ -100,6 +100,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.c64_renormalize = (v != 0) ? 1 : 0;
     } else if (name == "fused_reg_bits") {
         t.fused_reg_bits = (v == 3) ? 3 : 4;
+    } else if (name == "jit_remat") {
+        t.jit_remat = (v != 0) ? 1 : 0;
     } else if (name == "jit_scale_ops") {
         t.jit_scale_ops = (v != 0) ? 1 : 0;
     } else if (name == "plan_schedule") {
@@ -185,6 +187,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.c64_renormalize;
     } else if (n == "fused_reg_bits") {
         *value = t.fused_reg_bits;
+    } else if (n == "jit_remat") {
+        *value = t.jit_remat;
     } else if (n == "jit_scale_ops") {
         *value = t.jit_scale_ops;
     } else if (n == "plan_schedule") {

@@ -98,7 +98,7 @@ def test_run_time_block_kernels_compile_on_the_host():
 
 @pytest.mark.parametrize("knobs", [
     {"jit_async_load": 1}, {"fused_reg_bits": 3}, {"jit_fence": 2, "jit_merge_diag": 0},
-    {"jit_skip_io": 0, "jit_prefetch": 0, "fused_tile_bits": 11}, {"jit_scale_ops": 0},
+    {"jit_skip_io": 0, "jit_prefetch": 0, "fused_tile_bits": 11}, {"jit_scale_ops": 0}, {"jit_remat": 0},
 ])
 def test_generated_kernel_variants_compile_on_the_host(knobs):
     from kettle_b200 import workloads as W

@@ -129,7 +129,7 @@ def test_auto_mode_compiles_on_the_second_apply(engine, port):
 
 @pytest.mark.parametrize("knobs", [
     {"jit_merge_diag": 0}, {"jit_prefetch": 0}, {"jit_skip_io": 0}, {"jit_skip_io": 1}, {"jit_fence": 2},
-    {"jit_scale_ops": 0},
+    {"jit_scale_ops": 0}, {"jit_remat": 0},
     {"fused_tile_bits": 11, "jit_ctas_per_sm": 3}, {"fused_tile_bits": 13},
 ])
 def test_jit_variants_agree(jit, port, knobs):
