@@ -503,12 +503,6 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
         std::sort(regs.begin(), regs.end());
         return regs;
     };
-    auto tile_mask = [&](const LGate& x) -> uint64_t {
-        uint64_t mk = 0;
-        if (loc[x.target] >= 0) mk |= bit(loc[x.target]);
-        if (x.control >= 0 && loc[x.control] >= 0) mk |= bit(loc[x.control]);
-        return mk;
-    };
     struct PhaseSpec
     {
         std::vector<int> regs;
@@ -567,8 +561,7 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
     };
     // place gate k in the open phase, or start a new phase for it
     auto place = [&](size_t k) {
-        const LGate& x = g[pb.gates[k]];
-        const uint64_t qm = tile_mask(x);
+        const uint64_t qm = tmask[k];
         done[k] = 1;
         if (fold[k]) {
             open.folds.push_back(k);
@@ -626,7 +619,7 @@ void plan_block(const PlanBlock& pb, const std::vector<LGate>& g, int n, Plan<T,
                 if (first_ready == SIZE_MAX) {
                     first_ready = k;
                 }
-                const uint64_t qm = tile_mask(g[pb.gates[k]]);
+                const uint64_t qm = tmask[k];
                 const bool fits = fold[k] || ((need[k] < 0 || std::find(cur.begin(), cur.end(), need[k]) != cur.end()) &&
                                               (qm & pending) == 0);
                 if (fits) {
