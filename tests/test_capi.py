@@ -136,3 +136,24 @@ def test_jit_dump_writes_source_and_register_summary(tmp_path, monkeypatch):
     log = (tmp_path / "kt_jit_0.log").read_text()
     assert "__global__" in src
     assert re.search(r"Used \d+ registers", log) and "spill" in log
+
+
+def test_every_documented_knob_is_known_with_its_documented_default():
+    # the knob list in include/kettle_b200.h against the library, in a fresh
+    # process (no KT_TUNING): every name is accepted, and where the comment
+    # states a default "(v)" after the range, kt_tuning_get returns it
+    import subprocess
+    import sys
+    head = (ROOT / "include" / "kettle_b200.h").read_text()
+    block = head[head.index("Launch-shape knobs of the engine"):head.index("Unknown names return")]
+    rows = re.findall(r"^ \*   ([a-z_0-9]+) +(\d+(?:\.\.[0-9e]+| or \d+|, \d+, \d+)?) +(?:\((\d+)\))?", block, re.M)
+    assert len(rows) >= 20 and sum(1 for r in rows if r[2]) >= 13
+    names = [r[0] for r in rows]
+    code = ("import json, sys\nsys.path.insert(0, %r)\nfrom kettle_b200 import capi\n"
+            "print(json.dumps({n: capi.tuning_get(n) for n in %r}))" % (str(ROOT), names))
+    env = {k: v for k, v in __import__("os").environ.items() if k != "KT_TUNING"}
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, check=True)
+    got = __import__("json").loads(out.stdout.strip().splitlines()[-1])
+    for name, _, default in rows:
+        if default:
+            assert got[name] == int(default), (name, got[name], default)
