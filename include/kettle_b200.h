@@ -139,14 +139,14 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
 
 /* Launch-shape knobs of the engine (no reference counterpart), set by the
  * autotuner (kettle_b200/autotune.py) or from KT_TUNING="name=value,...":
- *   fused_ctas_per_sm  1 or 2   register budget of the fused block kernel
- *   fused_tile_bits    9..13    tile qubits per fused block (complex128; complex64
+ *   fused_ctas_per_sm  1 or 2   (2) register budget of the fused block kernel
+ *   fused_tile_bits    9..13    (12) tile qubits per fused block (complex128; complex64
  *                               one more); 13 runs 512-thread CTAs, one per SM
- *   fused_max_ops      1..256   gates per fused block (also the batch engine's fusion depth)
- *   adjoint_fused      0 or 1   fused adjoint blocks (1) or one kernel per gate (0)
- *   fold_permutations  0 or 1   X / CX with every qubit in a tile folded into a
+ *   fused_max_ops      1..256   (256) gates per fused block (also the batch engine's fusion depth)
+ *   adjoint_fused      0 or 1   (1) fused adjoint blocks (1) or one kernel per gate (0)
+ *   fold_permutations  0 or 1   (1) X / CX with every qubit in a tile folded into a
  *                               shared-memory transpose (1) or run as ops (0)
- *   c64_renormalize    0 or 1   complex64 applies rescale every fused block to the
+ *   c64_renormalize    0 or 1   (1) complex64 applies rescale every fused block to the
  *                               norm the state had when the apply began (1)
  *   plan_lookahead     0, 1, 2  (1) each fused block's tile qubits chosen among the
  *                               greedy tile and tiles pinned to the qubits the next
@@ -165,7 +165,7 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               3 a block's first set is built from the bits above
  *                               the 128-byte runs when that takes any gate, so the
  *                               tile loads without a transpose
- *   fused_jit          0, 1, 2  fused blocks as kernels compiled at run
+ *   fused_jit          0, 1, 2  (2) fused blocks as kernels compiled at run
  *                               time (NVRTC, cached per block structure: gate bodies
  *                               as straight-line code, every slot and mask a
  *                               constant): 0 never, 1 always, 2 (default) once a
@@ -202,7 +202,7 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               one unscaled uncontrolled gate of the block (or
  *                               every amplitude before the store); below 1e-150 the
  *                               apply runs on the precompiled kernels
- *   fused_reg_bits     3 or 4   complex128 amplitudes per thread in fused blocks
+ *   fused_reg_bits     3 or 4   (4) complex128 amplitudes per thread in fused blocks
  *                               (2^4; or 2^3 with twice the warps: 12-qubit tiles of
  *                               512 threads, 2 CTAs per SM, or 11-qubit tiles of 256
  *                               threads, 3 CTAs per SM, by fused_tile_bits)
