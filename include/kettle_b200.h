@@ -202,6 +202,11 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               one unscaled uncontrolled gate of the block (or
  *                               every amplitude before the store); below 1e-150 the
  *                               apply runs on the precompiled kernels
+ *   batch_spin_limit   1..1e12  (33554432) polls of an empty job queue after which a
+ *                               CTA of a batch's persistent kernel gives up (about
+ *                               10 s): the evaluation then stops and
+ *                               kt_batch_evaluate returns KT_ERR_TIMEOUT; the value
+ *                               is taken when the batch is created (its graph)
  *   fused_reg_bits     3 or 4   (4) complex128 amplitudes per thread in fused blocks
  *                               (2^4; or 2^3 with twice the warps: 12-qubit tiles of
  *                               512 threads, 2 CTAs per SM, or 11-qubit tiles of 256
@@ -286,11 +291,13 @@ int32_t kt_sv_expect(kt_sv sv, const kt_pauli* strings, int64_t n_strings,
  * For callers that cannot let the library call cudaMalloc: a host that keeps
  * all device memory in its own pool or arena, or a loop that must not
  * allocate once running.  It takes the amplitudes as a raw device pointer
- * (2^n_qubits elements of `dtype`, on the current device), computes the same
- * per-string values and weighted total as kt_sv_expect, and keeps its scratch
- * in one fixed device array inside the library (about 1.3 MB, held by every
- * GPU that loads the library until the process exits), so it calls no
- * cudaMalloc or cudaFree.  At most KT_NOALLOC_MAX_STRINGS strings per call;
+ * (2^n_qubits elements of `dtype`, on the current device), computes the
+ * per-string values and weighted total of kt_sv_expect (bit for bit on GPUs
+ * of up to 148 SMs, such as a B200, where both add the same 4-per-SM block
+ * partials in the same order; within FP64 rounding on larger ones), and keeps
+ * its scratch in one fixed device array inside the library (about 2.5 MB,
+ * held by every GPU that loads the library until the process exits), so it
+ * calls no cudaMalloc or cudaFree.  At most KT_NOALLOC_MAX_STRINGS strings per call;
  * more is rejected with KT_ERR_INVALID.  The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress) with that device current;
  * make that first call before any stream capture.  All calls share the one

@@ -132,9 +132,10 @@ def build_oracle(verbose: bool = False) -> None:
     reference library from its sources when they are present on this machine."""
     make = shutil.which("make") or "make"
     _run([make, "-C", str(ROOT / "oracle"), "port"])
-    ref = pathlib.Path(os.environ.get("KETTLE_REFERENCE", "/root/reference"))
-    if (ref / "CMakeLists.txt").exists():
-        _run([make, "-C", str(ROOT / "oracle"), "ref", "dropin", f"REF={ref}", f"-j{min(8, os.cpu_count() or 4)}"])
+    # oracle/Makefile knows where the kettle sources lie (KETTLE_REFERENCE
+    # overrides it) and builds the reference only when they are there
+    extra = [f"REF={os.environ['KETTLE_REFERENCE']}"] if os.environ.get("KETTLE_REFERENCE") else []
+    _run([make, "-C", str(ROOT / "oracle"), "ref-if-present", *extra, f"-j{min(8, os.cpu_count() or 4)}"])
 
 
 def ptxas_report() -> str:

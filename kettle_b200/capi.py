@@ -14,6 +14,12 @@ import numpy as np
 LIB_PATH = pathlib.Path(__file__).resolve().parent / "lib" / "libkettle_b200.so"
 
 KT_OK = 0
+KT_ERR_INVALID = -1
+KT_ERR_CUDA = -2
+KT_ERR_NOMEM = -3
+KT_ERR_QUBITS = -4
+KT_ERR_TIMEOUT = -5
+KT_ERR_UNSUPPORTED = -6
 KT_C128 = 0
 KT_C64 = 1
 KT_APPLY_FUSED = 0

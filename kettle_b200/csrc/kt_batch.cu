@@ -55,7 +55,6 @@ constexpr int UNITS_PER_JOB = 64;        // a job's tiles are cut into at most t
 constexpr int HAM_SMEM_STRINGS = 512;    // strings staged in shared memory by a Hamiltonian unit
 constexpr int HJ = 8;                    // amplitudes per thread per step of a Hamiltonian unit (B_THREADS * HJ
                                          // divides every chunk: 2^12 or 2^13 amplitudes)
-constexpr long long SPIN_LIMIT = 1LL << 25;  // polls of a completion counter (~10 s) before giving up
 
 enum : int32_t
 {
@@ -177,6 +176,7 @@ struct BArgs
     int* taken;                 // per job: units handed out
     int* status;
     int with_grad;
+    long long spin_limit;       // polls of an empty queue before the CTA gives up (batch_spin_limit)
 };
 
 // ---------------------------------------------------------------------------
@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_batch_persist(BArgs<T> A)
                         continue;
                     }
                 }
-                if (++spins > SPIN_LIMIT) {
+                if (++spins > A.spin_limit) {
                     atomicExch(A.status, 1);
                     stop = 1;
                     break;
@@ -1356,6 +1356,7 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         a.qtail = d_ht + 2 * w + 1;
         a.status = d_status;
         a.with_grad = with_grad;
+        a.spin_limit = tuning().batch_spin_limit;
         k_batch_persist<T><<<big_grid, B_THREADS, big_smem, s0>>>(a);
         chk(cudaGetLastError());
         ++launches;

@@ -207,6 +207,7 @@ struct Tuning
     int jit_fence {0};           // k > 0: run-time compiled blocks fence the amplitudes every k ops
     int jit_scale_ops {1};       // complex128 blocks: uncontrolled real / RX-like ops divided by m00 (one FMA per component)
     int jit_remat {1};           // 1: thread-index terms recomputed every tile, not held across the tile loop
+    long long batch_spin_limit {1LL << 25};  // polls of the batch queue before a CTA gives up (~10 s)
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);

@@ -102,6 +102,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.fused_reg_bits = (v == 3) ? 3 : 4;
     } else if (name == "jit_remat") {
         t.jit_remat = (v != 0) ? 1 : 0;
+    } else if (name == "batch_spin_limit") {
+        t.batch_spin_limit = std::max(1LL, std::min(1000000000000LL, v));
     } else if (name == "jit_scale_ops") {
         t.jit_scale_ops = (v != 0) ? 1 : 0;
     } else if (name == "plan_schedule") {
@@ -189,6 +191,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.fused_reg_bits;
     } else if (n == "jit_remat") {
         *value = t.jit_remat;
+    } else if (n == "batch_spin_limit") {
+        *value = t.batch_spin_limit;
     } else if (n == "jit_scale_ops") {
         *value = t.jit_scale_ops;
     } else if (n == "plan_schedule") {

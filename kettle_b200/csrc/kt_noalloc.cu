@@ -10,7 +10,7 @@
 // launches the same kernels as kt_sv_expect.
 //
 // The array lives in every GPU that loads the library, from module load until
-// the process exits (about 1.3 MB).  Host code never passes the array's name
+// the process exits (about 2.5 MB).  Host code never passes the array's name
 // to a kernel (in host code that name is only a stand-in for the device
 // symbol): the device address is looked up once per device with
 // cudaGetSymbolAddress, with that device current, on the first call made on
@@ -29,13 +29,14 @@ int32_t pauli_terms_launch(const void* amps, int n, int32_t dtype, const void* s
 int32_t weighted_total_launch(const double* terms, const double* coeffs, int64_t n, double* total, cudaStream_t stream);
 int pauli_slot_bytes();
 int pauli_slot_width();
+int pauli_blocks(int n_bits);
 }  // namespace kt
 
 namespace
 {
 
 constexpr int NA_MAX_STRINGS = KT_NOALLOC_MAX_STRINGS;
-constexpr int NA_BLOCKS = 296;            // reduction blocks per string (2 per SM of a B200)
+constexpr int NA_BLOCKS = 592;            // reduction blocks per string: kt_sv_expect's 4 per SM of a B200
 constexpr int NA_SLOT_WIDTH = 16;         // strings per slot, as kt_sv_expect groups them
 
 // layout-identical to the slot record the reduction kernels read
@@ -77,6 +78,21 @@ int32_t fail(int32_t code, const std::string& msg)
     return code;
 }
 
+// An exception (std::bad_alloc from std::to_string, say) must not cross the C interface.
+template <typename F>
+int32_t guarded(F&& f)
+{
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return fail(KT_ERR_NOMEM, "kt_sv_expect_noalloc: host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(KT_ERR_INVALID, std::string("kt_sv_expect_noalloc: ") + e.what());
+    } catch (...) {
+        return fail(KT_ERR_INVALID, "kt_sv_expect_noalloc: unknown exception");
+    }
+}
+
 // Once per device, with that device current: the device address of the array.
 int32_t scratch_address(char** out)
 {
@@ -98,11 +114,8 @@ int32_t scratch_address(char** out)
     return KT_OK;
 }
 
-}  // namespace
-
-extern "C" int32_t kt_sv_expect_noalloc(const void* device_amps, int32_t n_qubits, int32_t dtype,
-                                        const kt_pauli* strings, int64_t n_strings, const double* coeffs,
-                                        double* out_terms, double* out_total, void* stream)
+int32_t expect_noalloc(const void* device_amps, int32_t n_qubits, int32_t dtype, const kt_pauli* strings,
+                       int64_t n_strings, const double* coeffs, double* out_terms, double* out_total, void* stream)
 {
     if (device_amps == nullptr) {
         return fail(KT_ERR_INVALID, "kt_sv_expect_noalloc: null device amplitude pointer");
@@ -178,8 +191,9 @@ extern "C" int32_t kt_sv_expect_noalloc(const void* device_amps, int32_t n_qubit
     KT_CUDA(cudaMemcpyAsync(dev + OFF_X, hx.data(), ns * 8, cudaMemcpyHostToDevice, st));
     KT_CUDA(cudaMemcpyAsync(dev + OFF_Z, hz.data(), ns * 8, cudaMemcpyHostToDevice, st));
     KT_CUDA(cudaMemcpyAsync(dev + OFF_P, hp.data(), ns * 4, cudaMemcpyHostToDevice, st));
-    const uint64_t half = uint64_t {1} << (n_qubits - 1);
-    const int blocks = static_cast<int>(std::min<uint64_t>(NA_BLOCKS, std::max<uint64_t>(1, (half + 255) / 256)));
+    // kt_sv_expect's block count where it fits the array (every GPU of up to
+    // 148 SMs): the partial sums are then added in the same order, bit for bit
+    const int blocks = std::min(NA_BLOCKS, kt::pauli_blocks(n_qubits));
     auto* d_terms = reinterpret_cast<double*>(dev + OFF_TERMS);
     if (const int32_t rc = kt::pauli_terms_launch(device_amps, n_qubits, dtype, dev + OFF_SLOTS, n_slots,
                                                   reinterpret_cast<const uint64_t*>(dev + OFF_X),
@@ -217,4 +231,15 @@ extern "C" int32_t kt_sv_expect_noalloc(const void* device_amps, int32_t n_qubit
         KT_CUDA(cudaStreamSynchronize(st));
     }
     return KT_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t kt_sv_expect_noalloc(const void* device_amps, int32_t n_qubits, int32_t dtype,
+                                        const kt_pauli* strings, int64_t n_strings, const double* coeffs,
+                                        double* out_terms, double* out_total, void* stream)
+{
+    return guarded([&] {
+        return expect_noalloc(device_amps, n_qubits, dtype, strings, n_strings, coeffs, out_terms, out_total, stream);
+    });
 }

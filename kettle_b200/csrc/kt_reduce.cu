@@ -518,6 +518,12 @@ int pauli_slot_width()
     return PAULI_MAXG;
 }
 
+// reduction blocks per string of kt_sv_expect on a state of n_bits index bits
+int pauli_blocks(int n_bits)
+{
+    return reduce_blocks((uint64_t {1} << n_bits) / 2 + 1);
+}
+
 int32_t norm_sq(State& s, double* out)
 {
     double r[2];

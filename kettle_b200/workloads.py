@@ -1,8 +1,10 @@
 """Seeded synthetic workloads: random brickwork circuits, hardware-efficient
 ansatz circuits, random Pauli Hamiltonians and the XXZ chain.
 
-All draws come from numpy's PCG64 generator with an explicit seed, so the
-engine, the oracle and the reference arm see identical gate records.
+Draws come from numpy's PCG64 generator with an explicit seed, except the
+random U matrices of `random_layers`, which come from kettle's own
+generate_random_unitary2x2 construction on a std::mt19937 stream; the engine,
+the oracle and the reference arm see identical gate records.
 """
 from __future__ import annotations
 
@@ -49,16 +51,50 @@ def haar_unitary2(rng: np.random.Generator) -> np.ndarray:
     return np.array([[g * c * ep, g * s * ec], [-g * s / ec, g * c / ep]], dtype=np.complex128)
 
 
+def random_unitaries(seed: int, count: int) -> list[np.ndarray]:
+    """`count` Haar-random 2x2 unitaries drawn one after another from one
+    std::mt19937(seed) stream, as kettle's
+    generate_random_unitary2x2(std::mt19937&) draws them
+    (gates/random_u_gates.cpp:13-36): four uniform_real_distribution{0, 1}
+    values per matrix (alpha, phi, chi, then psi = asin(sqrt(u))), each one
+    std::generate_canonical<double, 53> of the engine (two 32-bit outputs),
+    and the same products and quotients:
+        U = [[g cos(psi) e^{i phi},  g sin(psi) e^{i chi}],
+             [-g sin(psi) / e^{i chi}, g cos(psi) / e^{i phi}]],  g = e^{i alpha}.
+    The canonicals come from the library's host code (kt_canonicals_mt19937)."""
+    from .capi import canonicals_mt19937
+
+    u = canonicals_mt19937(seed, 4 * count)
+    out = []
+    for k in range(count):
+        alpha = 2.0 * math.pi * float(u[4 * k])
+        phi = 2.0 * math.pi * float(u[4 * k + 1])
+        chi = 2.0 * math.pi * float(u[4 * k + 2])
+        psi = math.asin(math.sqrt(float(u[4 * k + 3])))
+        cp, sp = math.cos(psi), math.sin(psi)
+        g = complex(math.cos(alpha), math.sin(alpha))
+        ep = complex(math.cos(phi), math.sin(phi))
+        ec = complex(math.cos(chi), math.sin(chi))
+        out.append(np.array([[g * cp * ep, g * sp * ec], [-g * sp / ec, g * cp / ep]], dtype=np.complex128))
+    return out
+
+
 def random_layers(n: int, layers: int, seed: int, mixed: bool = False) -> np.ndarray:
     """The random-circuit family of the benchmark configurations.
 
     Each layer: one gate per qubit drawn uniformly from {H, RX, RY, RZ}
-    (plus U, Haar-random, when `mixed`), angles uniform in [0, 2pi); then CX
-    on (0,1),(2,3),... on even layers and (1,2),(3,4),... on odd layers; when
+    (plus U when `mixed`), angles uniform in [0, 2pi); then CX on
+    (0,1),(2,3),... on even layers and (1,2),(3,4),... on odd layers; when
     `mixed`, then n//2 controlled rotations drawn from {CRX, CRY, CRZ, CP} on
     random distinct (control, target) pairs with angles uniform in [0, 2pi).
+    Gate choices, qubits and angles come from numpy's PCG64(seed); the U
+    matrices, in circuit order, from kettle's own generator on one
+    std::mt19937(seed) stream (`random_unitaries`), so a kettle program
+    seeding std::mt19937 with the same value draws the same matrices.
     """
     rng = np.random.default_rng(seed)
+    # at most one U per one-qubit slot: the stream's first layers * n matrices
+    u_stream = iter(random_unitaries(seed, layers * n)) if mixed else iter(())
     one_q = ["H", "RX", "RY", "RZ"] + (["U"] if mixed else [])
     ctl = ["CRX", "CRY", "CRZ", "CP"]
     recs = []
@@ -68,7 +104,7 @@ def random_layers(n: int, layers: int, seed: int, mixed: bool = False) -> np.nda
             if name == "H":
                 recs.append(gate("H", q))
             elif name == "U":
-                recs.append(gate("U", q, u=haar_unitary2(rng)))
+                recs.append(gate("U", q, u=next(u_stream)))
             else:
                 recs.append(gate(name, q, angle=float(TWO_PI * rng.random())))
         for q in range(layer % 2, n - 1, 2):

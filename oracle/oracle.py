@@ -217,6 +217,8 @@ class Ref:
         L.ref_pairs_double.restype = I32
         L.ref_random_unitary.argtypes = [I32, P]
         L.ref_random_unitary.restype = I32
+        L.ref_random_unitaries.argtypes = [I32, I64, P]
+        L.ref_random_unitaries.restype = I32
         L.ref_time_sv.argtypes = [I32, P, I64, P, C.POINTER(C.c_double)]
         L.ref_time_sv.restype = I32
         L.ref_sv_alloc.argtypes = [I32]
@@ -367,6 +369,13 @@ class Ref:
         u = np.empty(8, dtype=np.float64)
         self._chk(self.L.ref_random_unitary(seed, _p(u)))
         return np.array([[u[0] + 1j * u[1], u[2] + 1j * u[3]], [u[4] + 1j * u[5], u[6] + 1j * u[7]]])
+
+    def random_unitaries(self, seed, count):
+        """`count` matrices of generate_random_unitary2x2 on one std::mt19937(seed) stream."""
+        u = np.empty(8 * count, dtype=np.float64)
+        self._chk(self.L.ref_random_unitaries(seed, count, _p(u)))
+        return [np.array([[u[8 * k] + 1j * u[8 * k + 1], u[8 * k + 2] + 1j * u[8 * k + 3]],
+                          [u[8 * k + 4] + 1j * u[8 * k + 5], u[8 * k + 6] + 1j * u[8 * k + 7]]]) for k in range(count)]
 
 
 _port = None

@@ -463,4 +463,22 @@ int32_t ref_random_unitary(int32_t seed, double* u)
     });
 }
 
+// `count` matrices from one std::mt19937(seed) stream, one
+// generate_random_unitary2x2(std::mt19937&) call after another
+// (gates/random_u_gates.cpp:13-36); 8 doubles per matrix
+int32_t ref_random_unitaries(int32_t seed, int64_t count, double* u)
+{
+    return guarded([&] {
+        auto prng = std::mt19937 {static_cast<std::mt19937::result_type>(seed)};
+        for (int64_t k = 0; k < count; ++k) {
+            const auto m = ket::generate_random_unitary2x2(prng);
+            const std::complex<double> e[4] = {m.elem00, m.elem01, m.elem10, m.elem11};
+            for (int i = 0; i < 4; ++i) {
+                u[8 * k + 2 * i] = e[i].real();
+                u[8 * k + 2 * i + 1] = e[i].imag();
+            }
+        }
+    });
+}
+
 }  // extern "C"

@@ -4,6 +4,7 @@ the reference has been compiled into oracle/_ref by `make -C oracle ref`):
     python tests/golden/make_golden.py
 
     python tests/golden/make_golden.py dm_ops     # golden_dm_ops.npz only
+    python tests/golden/make_golden.py size       # golden_size.npz only (~1 min)
 
 Writes
   * ref_kats.json   known-answer cases restated from the reference's own tests
@@ -14,7 +15,10 @@ Writes
                     expectation values, sampled indices, M-gate outcomes and
                     density matrices;
   * golden_dm_ops.npz partial traces, tensor products and Tr(rho^2) of the
-                    reference library on seeded random density matrices.
+                    reference library on seeded random density matrices;
+  * golden_size.npz the 20-qubit, 100-layer benchmark configuration in full
+                    (probe amplitudes, state sums, all 200 <P_k>, 4096 shots)
+                    and a stream of generate_random_unitary2x2 matrices.
 The fixtures are committed; tests read them without needing the reference.
 """
 from __future__ import annotations
@@ -195,6 +199,53 @@ def golden_ref():
     return out
 
 
+CONFIG1_SEED = 2024          # the seed the benchmark draws its workloads with
+CONFIG1_PROBES = 4096        # amplitudes kept per state (the full 20-qubit state is 16 MiB)
+
+
+def golden_size():
+    """Full-size fixtures of the reference library:
+      * config 1 in full: the 20-qubit complex128 state after all 100 layers
+        (2950 gates) of the benchmark circuit, then <P_k> of all 200 strings,
+        the weighted total and 4096 sampled indices (std::mt19937(2024)
+        through perform_measurements_as_memory); the state is kept as
+        amplitudes at CONFIG1_PROBES seeded indices plus two sums over every
+        amplitude (sum |a_i|^2 i and sum a_i e^{-2 pi i i / 2^20 * 7}), so a
+        tile placed at the wrong address changes them;
+      * generate_random_unitary2x2 on one std::mt19937 stream (the source of
+        the benchmark circuits' U gates)."""
+    R = ref()
+    out = {}
+    n = 20
+    gates = W.random_layers(n, 100, seed=CONFIG1_SEED, mixed=False)
+    strings, coeffs = W.random_paulis(n, 200, seed=CONFIG1_SEED)
+    amps, _ = R.simulate_sv(n, basis(n, "0" * n), gates)
+    terms, total = R.expect(n, amps, strings, coeffs)
+    out["c1_gates"] = gates
+    out["c1_strings"] = strings
+    out["c1_coeffs"] = coeffs
+    out["c1_terms"] = terms
+    out["c1_total"] = np.array([total])
+    out["c1_samples"] = R.sample_memory(n, amps, 4096, CONFIG1_SEED)
+    idx = np.random.default_rng(7).choice(1 << n, size=CONFIG1_PROBES, replace=False).astype(np.int64)
+    out["c1_probe_index"] = idx
+    out["c1_probe_amps"] = amps[idx]
+    out["c1_sums"] = np.array(state_sums(amps))
+    for seed in (0, 2024):
+        out[f"ru_{seed}"] = np.array(R.random_unitaries(seed, 64))
+    return out
+
+
+def state_sums(amps):
+    """Two sums over every amplitude: sum |a_i|^2 i and sum a_i w^(7 i) with
+    w = e^{-2 pi i / N} (a single Fourier coefficient)."""
+    N = amps.size
+    i = np.arange(N, dtype=np.float64)
+    s1 = float(np.sum(np.abs(amps) ** 2 * i))
+    s2 = complex(np.sum(amps * np.exp(-2j * np.pi * 7.0 * i / N)))
+    return [s1, s2.real, s2.imag]
+
+
 def random_rho(n, seed):
     rng = np.random.default_rng(seed)
     a = rng.standard_normal((1 << n, 1 << n)) + 1j * rng.standard_normal((1 << n, 1 << n))
@@ -239,6 +290,9 @@ def main():
     if "all" in which or "dm_ops" in which:
         np.savez_compressed(HERE / "golden_dm_ops.npz", **golden_dm_ops())
         print("wrote", HERE / "golden_dm_ops.npz")
+    if "all" in which or "size" in which:
+        np.savez_compressed(HERE / "golden_size.npz", **golden_size())
+        print("wrote", HERE / "golden_size.npz")
 
 
 if __name__ == "__main__":

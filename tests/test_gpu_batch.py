@@ -176,3 +176,36 @@ def test_batch_many_items_work_queue(engine):
         assert abs(e[k] - e1[0]) < 1e-10
         assert np.abs(g[off[k]:off[k + 1]] - g1).max() < 1e-10
     b.close()
+
+
+def test_batch_wait_limit_returns_timeout_and_the_context_stays_usable(engine):
+    """The persistent kernel's bounded wait: with batch_spin_limit at a few
+    polls, CTAs that find no ready job (most of them, while the first forward
+    blocks run) give up at once; the evaluation stops with KT_ERR_TIMEOUT, the
+    kernel returns, and a batch created afterwards with the default limit
+    evaluates normally on the same context."""
+    circuits = []
+    params = []
+    for k, n in enumerate((16, 17, 16)):
+        g, p = W.hea(n, 6, seed=70 + k)
+        s, c = W.random_paulis(n, 20, seed=80 + k)
+        circuits.append((n, g, p.size, s, c))
+        params.append(p)
+    params = np.concatenate(params)
+    items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
+    old = capi.tuning_get("batch_spin_limit")
+    capi.tuning_set("batch_spin_limit", 2)
+    try:
+        b = capi.Batch(items, gates, strings, coeffs, n_params)
+    finally:
+        capi.tuning_set("batch_spin_limit", old)
+    with pytest.raises(capi.KettleError) as e:
+        b.evaluate(params)
+    assert e.value.code == capi.KT_ERR_TIMEOUT
+    b.close()
+    b2 = capi.Batch(items, gates, strings, coeffs, n_params)
+    energies, grads = b2.evaluate(params)
+    b2.close()
+    want_e, want_g = _one_by_one(circuits, params)
+    assert np.abs(energies - want_e).max() < 1e-10
+    assert np.abs(grads - want_g).max() < 1e-10

@@ -250,3 +250,40 @@ def test_live_reference_dm_ops(port, ref):
         rho = random_rho(n, 40 + n)
         for qs in ([0], [n - 1], list(range(n))[::-1], [0] * (n // 2 + 1) if n > 1 else [0]):
             assert np.array_equal(port.dm_partial_trace(n, rho, qs), ref.dm_partial_trace(n, rho, qs))
+
+
+# --- full-size fixtures (tests/golden/golden_size.npz) ----------------------
+
+@pytest.fixture(scope="module")
+def golden_size():
+    from conftest import GOLDEN
+    return dict(np.load(GOLDEN / "golden_size.npz"))
+
+
+def test_golden_config1_full_size(port, golden_size):
+    """The oracle on the whole 20-qubit, 100-layer benchmark configuration:
+    bit-exact with the reference's final amplitudes (at the stored probes),
+    <P_k> of 40 of its 200 strings and its 4096 sampled indices."""
+    g = golden_size
+    n = 20
+    amps = port.apply(n, basis(n), g["c1_gates"])
+    assert np.array_equal(amps[g["c1_probe_index"]], g["c1_probe_amps"])
+    terms, _ = port.expect(n, amps, g["c1_strings"][:40], g["c1_coeffs"][:40])
+    assert np.array_equal(terms, g["c1_terms"][:40])
+    idx = port.sample(n, port.probabilities(n, amps), port.canonicals(2024, 4096))
+    assert np.array_equal(idx, g["c1_samples"])
+
+
+def test_random_unitaries_are_the_reference_generator(golden_size):
+    """The benchmark circuits' U gates: generate_random_unitary2x2 on one
+    std::mt19937 stream (random_u_gates.cpp:13-36), bit for bit."""
+    for seed in (0, 2024):
+        got = np.array(W.random_unitaries(seed, 64))
+        assert np.array_equal(got, golden_size[f"ru_{seed}"]), seed
+
+
+def test_random_unitaries_live_reference(ref):
+    for seed in (1, 99, 123456):
+        got = W.random_unitaries(seed, 40)
+        want = ref.random_unitaries(seed, 40)
+        assert all(np.array_equal(a, b) for a, b in zip(got, want)), seed
