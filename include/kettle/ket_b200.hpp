@@ -593,6 +593,10 @@ auto almost_eq(const Statevector& left, const Statevector& right,
                double tolerance_sq = COMPLEX_ALMOST_EQ_TOLERANCE_SQ) noexcept -> bool;
 auto inner_product(const Statevector& bra_state, const Statevector& ket_state) -> std::complex<double>;
 auto inner_product_norm_squared(const Statevector& left, const Statevector& right) -> double;
+// state/statevector.hpp:115,119: the left state's qubits are the low ones
+auto tensor_product(const Statevector& left, const Statevector& right) -> Statevector;
+auto diagonal_expectation_value(const std::vector<std::complex<double>>& eigenvalues, const Statevector& state)
+    -> std::complex<double>;
 
 // Column-major N x N host matrix (element (r, c) at r + c * N), the element
 // order of the reference's Eigen::MatrixXcd.
@@ -699,6 +703,7 @@ void simulate(const QuantumCircuit& circuit, Statevector& state, std::optional<i
 void simulate(const QuantumCircuit& circuit, DensityMatrix& state, std::optional<int> prng_seed = std::nullopt);
 
 // ---- Pauli operators -------------------------------------------------------------------
+class SparsePauliString;
 enum class PauliTerm : std::uint8_t
 {
     I,
@@ -774,6 +779,20 @@ private:
     std::vector<WeightedPauliString> strings_;
 };
 
+// simulation/simulate_pauli.hpp:11-23: the string's X / Y / Z gates applied to
+// the state in term order (its phase is not applied)
+class StatevectorPauliStringSimulator
+{
+public:
+    void run(const SparsePauliString& pauli_string, Statevector& state);
+    [[nodiscard]] auto has_been_run() const -> bool { return has_been_run_; }
+
+private:
+    bool has_been_run_ {false};
+};
+
+void simulate(const SparsePauliString& pauli_string, Statevector& state);
+
 auto expectation_value(const PauliOperator& pauli_op, const Statevector& state) -> std::complex<double>;
 auto expectation_value(const SparsePauliString& sparse_pauli_string, const Statevector& state) -> std::complex<double>;
 auto expectation_value(const PauliOperator& pauli_op, const DensityMatrix& state) -> std::complex<double>;
@@ -796,6 +815,23 @@ auto calculate_probabilities_raw(const Statevector& state, const QuantumNoise* n
 auto calculate_probabilities(const Statevector& state, const QuantumNoise* noise = nullptr)
     -> std::map<std::string, double>;
 
+// calculations/measurements.hpp:40-97: the overloads on a probability vector
+// sample it on the device with the same sampler as the state overloads
+auto perform_measurements_as_memory(const std::vector<double>& probabilities_raw, std::size_t n_shots,
+                                    std::optional<int> seed = std::nullopt) -> std::vector<std::size_t>;
+auto perform_measurements_as_counts_raw(const std::vector<double>& probabilities_raw, std::size_t n_shots,
+                                        std::optional<int> seed = std::nullopt) -> std::map<std::size_t, std::size_t>;
+auto perform_measurements_as_counts_marginal(const std::vector<double>& probabilities_raw, std::size_t n_shots,
+                                             const std::vector<std::size_t>& marginal_qubits = {},
+                                             std::optional<int> seed = std::nullopt)
+    -> std::map<std::string, std::size_t>;
+// every shot simulates the circuit on a copy of the state and draws one
+// index with a sampler seeded anew (calculations/measurements.cpp:179-207)
+auto perform_measurements_as_counts_marginal(const QuantumCircuit& circuit, const Statevector& original_state,
+                                             std::size_t n_shots, const std::vector<std::size_t>& marginal_qubits = {},
+                                             const QuantumNoise* noise = nullptr,
+                                             std::optional<int> seed = std::nullopt)
+    -> std::map<std::string, std::size_t>;
 auto perform_measurements_as_memory(const Statevector& state, std::size_t n_shots, const QuantumNoise* noise = nullptr,
                                     std::optional<int> seed = std::nullopt) -> std::vector<std::size_t>;
 auto perform_measurements_as_counts_raw(const Statevector& state, std::size_t n_shots,

@@ -29,6 +29,10 @@
  *                        ket::internal::SingleQubitGatePairGenerator / DoubleQubitGatePairGenerator
  *                        source/kettle_internal/simulation/gate_pair_generator.hpp:25-160
  *   kt_sv_inner          ket::inner_product, source/kettle_internal/state/state.cpp:159-172
+ *   kt_sv_tensor_product ket::tensor_product(Statevector, Statevector), state/state.cpp:144-157
+ *   kt_sv_diagonal_expectation  ket::diagonal_expectation_value, state/state.cpp:174-188
+ *   kt_sample_probabilities     perform_measurements_as_* on a probability vector, measurements.cpp:58-159
+ *   kt_dm_measure_probs / kt_dm_collapse  M on a DensityMatrix, measure_density_matrix.cpp:22-105
  *   kt_adjoint_*         no reference counterpart (new capability; the consumer is the
  *                        VQE cost function of example/algorithms/vqe_basic.cpp:61-96)
  *   kt_batch_*           no reference counterpart (new capability)
@@ -331,6 +335,24 @@ int32_t kt_sv_collapse(kt_sv sv, uint32_t qubit, int32_t outcome, double scale);
 
 int32_t kt_sv_norm_sq(kt_sv sv, double* out);
 int32_t kt_sv_inner(kt_sv bra, kt_sv ket, double* out_re_im);
+/* |left> (x) |right> into `out` (n_left + n_right qubits, the same dtype): the
+ * left state's qubits are the low ones, out[i_l + i_r 2^n_left] =
+ * left[i_l] right[i_r].  Replaces ket::tensor_product(const Statevector&,
+ * const Statevector&) (state/statevector.hpp:115, state/state.cpp:144-157). */
+int32_t kt_sv_tensor_product(kt_sv left, kt_sv right, kt_sv out);
+/* sum_i conj(psi_i) lambda_i psi_i in FP64 for a diagonal operator given by its
+ * 2^n complex eigenvalues (interleaved doubles, host).  Replaces
+ * ket::diagonal_expectation_value (state/statevector.hpp:119,
+ * state/state.cpp:174-188); the sum is taken in another order, so the result
+ * agrees within FP64 rounding. */
+int32_t kt_sv_diagonal_expectation(kt_sv sv, const double* eigenvalues, double* out_re_im);
+/* Shots from a caller's probability vector (n doubles, host): the sampler of
+ * kt_sv_sample on those values, bit-exact to the reference's sequential CDF
+ * and lower_bound (calculations/measurements.cpp:58-159, the
+ * perform_measurements_as_* overloads taking std::vector<double>).  `stream`
+ * may be NULL; device scratch is allocated for the call and freed after it. */
+int32_t kt_sample_probabilities(const double* probabilities, uint64_t n, const double* canonicals,
+                                int64_t n_shots, uint64_t* out_indices, int32_t mode, void* stream);
 
 /* ---- pair enumeration (reference order, bit-exact) --------------------------
  * Pairs k0 .. k0+count-1 of SingleQubitGatePairGenerator(t, n).next() and of
@@ -379,6 +401,13 @@ int32_t kt_dm_partial_trace(kt_dm src, const int32_t* qubits, int32_t n_traced, 
 int32_t kt_dm_tensor_product(kt_dm left, kt_dm right, kt_dm dst);
 /* Tr(rho^2), FP64: ket::DensityMatrix::trace_of_square (state/density_matrix.hpp:98-104). */
 int32_t kt_dm_trace_of_square(kt_dm dm, double* out_re_im);
+/* M gate on a density matrix, split at the host coin like the statevector's:
+ * P(b) = sum |rho(r, c)|^2 over the rows r and columns c whose bit `qubit` is
+ * b (the reference's definition); then keep outcome o: the (o, o) block
+ * scaled by `scale` (the reference uses sqrt(1 / P(o))), the other three
+ * blocks cleared.  Replaces simulation/measure_density_matrix.cpp:22-105. */
+int32_t kt_dm_measure_probs(kt_dm dm, uint32_t qubit, double* p0, double* p1);
+int32_t kt_dm_collapse(kt_dm dm, uint32_t qubit, int32_t outcome, double scale);
 
 /* ---- adjoint differentiation (new) -------------------------------------------
  * E(theta) = <psi(theta)| H |psi(theta)>, psi = U_G ... U_1 |psi0>.

@@ -55,7 +55,7 @@ def _stale(out: pathlib.Path, deps: list[pathlib.Path]) -> bool:
 
 
 # headers the run-time compiled block kernels include (kt_jit.cpp embeds their text)
-JIT_HEADERS = ("kt_complex.cuh", "kt_fused_dev.cuh")
+JIT_HEADERS = ("kt_complex.cuh", "kt_fused_dev.cuh", "kt_tma_dev.cuh")
 
 
 def write_jit_headers() -> pathlib.Path:

@@ -18,7 +18,8 @@ template <typename F>
 int32_t guard(F&& f)
 {
     try {
-        return f();
+        const int32_t rc = f();
+        return rc == KT_OK ? kt::jit_async_error() : rc;
     } catch (const std::bad_alloc&) {
         kt::set_error(KT_ERR_NOMEM, "host allocation failed");
         return KT_ERR_NOMEM;

@@ -38,6 +38,8 @@
 #include <unordered_map>
 #include <unordered_set>
 
+#include <cuda.h>
+
 #include "kt_fused.cuh"
 
 namespace kt
@@ -603,12 +605,113 @@ std::string jit_xor_terms(const uint32_t* terms, int nbits, uint32_t start)
     return "(" + e + ")";
 }
 
+// ---------------------------------------------------------------------------
+// TMA-pipelined block kernels (jit_tma, complex128).  The state is seen as a
+// tensor of float64 whose dimensions follow the runs of consecutive qubits of a
+// block's tile: dimension 0 is (re, im) x qubits 0..2 (one 128-byte row), each
+// further dimension starts at the first qubit of a run and reaches the next
+// run (the last one the top of the state), so one box of the tensor map is
+// the tile, or, when the tile has more than four runs above qubit 2, the part
+// of it with the highest runs' bits fixed (those copies differ only in the
+// last dimension's coordinate).  Boxes land in shared memory with the 128-byte
+// swizzle: amplitude l of the tile (bit j of l = the tile's j-th qubit) sits
+// at slot l ^ ((l >> 3) & 7).
+struct TmaGeom
+{
+    bool ok {false};
+    int rank {0};
+    uint64_t dim[5] {};        // extents (float64 elements for dimension 0)
+    uint64_t stride[5] {};     // byte strides of dimensions 1..rank-1
+    uint32_t box[5] {};        // box extents
+    int start[5] {};           // first qubit of each dimension (0 for dimension 0)
+    int copies {1};
+    std::vector<uint32_t> copy_add;  // per copy: added to the last dimension's coordinate
+    uint32_t box_bytes {0};
+};
+
+TmaGeom tma_geom(const FBlock& fb, int n)
+{
+    TmaGeom g;
+    const int K = fb.K;
+    if (K < 4 || fb.qubit[0] != 0 || fb.qubit[1] != 1 || fb.qubit[2] != 2) {
+        return g;
+    }
+    std::vector<std::pair<int, int>> runs;  // (first qubit, length <= 8: a box extent <= 256)
+    for (int j = 3; j < K;) {
+        int len = 1;
+        while (j + len < K && fb.qubit[j + len] == fb.qubit[j] + len && len < 8) {
+            ++len;
+        }
+        runs.emplace_back(fb.qubit[j], len);
+        j += len;
+    }
+    const int D = std::min<int>(4, static_cast<int>(runs.size()));
+    g.rank = 1 + D;
+    for (int r = 1; r <= D; ++r) {
+        g.start[r] = runs[static_cast<size_t>(r - 1)].first;
+    }
+    auto end_of = [&](int r) { return r < D ? g.start[r + 1] : n; };
+    g.dim[0] = uint64_t {2} << g.start[1];
+    g.box[0] = 16;
+    for (int r = 1; r <= D; ++r) {
+        g.dim[r] = uint64_t {1} << (end_of(r) - g.start[r]);
+        g.stride[r] = uint64_t {16} << g.start[r];
+        g.box[r] = 1u << runs[static_cast<size_t>(r - 1)].second;
+    }
+    std::vector<int> extra;  // qubits of the runs above the fourth, ascending
+    for (size_t r = static_cast<size_t>(D); r < runs.size(); ++r) {
+        for (int k = 0; k < runs[r].second; ++k) {
+            extra.push_back(runs[r].first + k);
+        }
+    }
+    g.copies = 1 << extra.size();
+    g.copy_add.assign(static_cast<size_t>(g.copies), 0u);
+    for (int c = 0; c < g.copies; ++c) {
+        for (size_t k = 0; k < extra.size(); ++k) {
+            if ((c >> k) & 1) {
+                g.copy_add[static_cast<size_t>(c)] |= 1u << (extra[k] - g.start[D]);
+            }
+        }
+    }
+    g.box_bytes = 128u << (K - 3 - static_cast<int>(extra.size()));
+    g.ok = true;
+    return g;
+}
+
+// slot of tile amplitude l in a stage buffer (the 128-byte swizzle, 16-byte amplitudes)
+inline uint32_t tma_swz(uint32_t l)
+{
+    return l ^ ((l >> 3) & 7u);
+}
+
+struct TmaCfg
+{
+    int groups {1};
+    int stages {3};
+    TmaGeom geom;
+};
+
+// The tile's coordinates in the tensor map: c[0] = 2 (base mod 2^start[1]),
+// c[r] = the base's bits from start[r] up to the next dimension.
+std::string tma_coord_code(const TmaGeom& g, const std::string& base, const std::string& out)
+{
+    std::string e;
+    for (int r = 0; r < g.rank; ++r) {
+        const int lo = g.start[r];
+        const int hi = (r == 0) ? g.start[1] : lo + __builtin_ctzll(g.dim[r]);
+        const uint64_t mask = (hi - lo >= 64) ? ~uint64_t {0} : ((uint64_t {1} << (hi - lo)) - 1);
+        e += out + "[" + std::to_string(r) + "] = static_cast<int32_t>(((" + base + " >> " + std::to_string(lo) + ") & " +
+             jit_hex(mask) + ")" + (r == 0 ? " << 1" : "") + ");\n";
+    }
+    return e;
+}
+
 // The body of block b's kernel (everything after its name): the tile loop
 // with the layout of every phase written out as constants (tile base, thread
 // and register offsets, swizzled shared-memory terms) and the gate bodies as
 // straight-line code; matrices arrive in the constant-bank parameter M.
 template <typename T>
-std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
+std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm, const TmaCfg* tma = nullptr)
 {
     const FBlock& fb = plan.blocks[b];
     const int TB = fb.K - RB;
@@ -642,14 +745,120 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     };
     std::string s;
     s.reserve(32768);
-    s += std::string("(void* a_, unsigned long long n_tiles, ") + (norm ? "kt::NormArgs na, " : "") +
-         "const __grid_constant__ $M<" + std::to_string(8 * (nops + (scale_slot ? 1 : 0))) + "> M)\n{\n";
+    // TMA variant: tile index bit of a phase's register slot / thread bit, and
+    // its term in a stage buffer's (128-byte swizzled) slot index
+    auto tile_bit = [&](uint64_t stride) {
+        for (int k = 0; k < fb.K; ++k) {
+            if (bit(fb.qubit[k]) == stride) {
+                return k;
+            }
+        }
+        return 0;
+    };
+    auto tma_reg_term = [&](const FPhase& f, int i) {
+        uint32_t x = 0;
+        for (int sl = 0; sl < RB; ++sl) {
+            if (i & (1 << sl)) {
+                x ^= tma_swz(1u << tile_bit(f.rstride[sl]));
+            }
+        }
+        return x;
+    };
+    auto tma_thr_terms = [&](const FPhase& f) {
+        std::vector<uint32_t> tt(static_cast<size_t>(std::max(1, TB)), 0u);
+        for (int j = 0; j < TB; ++j) {
+            tt[static_cast<size_t>(j)] = tma_swz(1u << tile_bit(f.tstride[j]));
+        }
+        return tt;
+    };
+    const int NG = tma ? tma->groups : 1;
+    const int NS = tma ? tma->stages : 1;
+    const int GT = 1 << TB;  // threads of one tile
+    const size_t tile_bytes = (size_t {1} << fb.K) * sizeof(typename CxT<T>::type);
+    if (tma) {
+        s += "(const __grid_constant__ kt::KtTmap tm, void* a_, unsigned long long n_tiles, unsigned int* err_, "
+             "const __grid_constant__ $M<" + std::to_string(8 * (nops + (scale_slot ? 1 : 0))) + "> M)\n{\n";
+    } else {
+        s += std::string("(void* a_, unsigned long long n_tiles, ") + (norm ? "kt::NormArgs na, " : "") +
+             "const __grid_constant__ $M<" + std::to_string(8 * (nops + (scale_slot ? 1 : 0))) + "> M)\n{\n";
+    }
     s += "    using namespace kt;\n    using C = $C;\n";
     s += "    constexpr int RB = " + std::to_string(RB) + ";\n";
-    s += "    C* __restrict__ a = static_cast<C*>(a_);\n";
-    s += "    extern __shared__ __align__(16) unsigned char smem_raw[];\n";
-    s += "    C* sm = reinterpret_cast<C*>(smem_raw);\n";
-    s += "    const uint32_t t = threadIdx.x;\n";
+    if (tma) {
+        const TmaGeom& g = tma->geom;
+        const std::string NSs = std::to_string(NS) + "ull";
+        const std::string TBYTES = std::to_string(tile_bytes) + "u";
+        // stage buffers (1024-byte aligned for the swizzle), then the mbarriers:
+        // full[s] (the tile's copies landed) and done[s] (its group finished it)
+        s += "    (void)a_;\n";
+        s += "    extern __shared__ __align__(1024) unsigned char smem_raw[];\n";
+        s += "    unsigned char* stage0 = reinterpret_cast<unsigned char*>((reinterpret_cast<unsigned long long>(smem_raw) + "
+             "1023ull) & ~1023ull);\n";
+        s += "    uint64_t* full = reinterpret_cast<uint64_t*>(stage0 + " + std::to_string(NS * tile_bytes) + "u);\n";
+        s += "    uint64_t* done = full + " + std::to_string(NS) + ";\n";
+        s += "    if (threadIdx.x == 0) {\n        for (int k = 0; k < " + std::to_string(NS) +
+             "; ++k) {\n            kt_mbar_init(full + k, 1);\n            kt_mbar_init(done + k, " + std::to_string(GT) +
+             ");\n        }\n        kt_fence_mbar_init();\n    }\n    __syncthreads();\n";
+        // the producer: one thread of the last warp issues every copy
+        auto copies = [&](const std::string& tile_expr, const std::string& buf, bool load) {
+            std::string e = "            {\n                const uint64_t pb = " +
+                            jit_deposit(tile_expr, free_strides.data(), fb.nfree) + ";\n                int32_t c[" +
+                            std::to_string(g.rank) + "];\n";
+            std::string cc = tma_coord_code(g, "pb", "c");
+            for (size_t at = 0; at < cc.size();) {
+                const size_t nl = cc.find('\n', at);
+                e += "                " + cc.substr(at, nl - at + 1);
+                at = nl + 1;
+            }
+            const std::string last = "c[" + std::to_string(g.rank - 1) + "]";
+            e += "                const int32_t c_last = " + last + ";\n";
+            for (int k = 0; k < g.copies; ++k) {
+                e += "                " + last + " = c_last + " + std::to_string(g.copy_add[static_cast<size_t>(k)]) + ";\n";
+                const std::string dst = buf + " + " + std::to_string(static_cast<size_t>(k) * g.box_bytes) + "u";
+                if (load) {
+                    e += "                KtTma<" + std::to_string(g.rank) + ">::load(&tm, " + dst + ", full + st, c);\n";
+                } else {
+                    e += "                KtTma<" + std::to_string(g.rank) + ">::store(&tm, " + dst + ", c);\n";
+                }
+            }
+            e += "            }\n";
+            return e;
+        };
+        s += "    if (threadIdx.x >= " + std::to_string(NG * GT) + "u) {\n";
+        s += "        if (threadIdx.x == " + std::to_string(NG * GT) + "u) {\n";
+        s += "            unsigned long long i = 0;\n";
+        s += "            for (;; ++i) {\n";
+        s += "            const unsigned long long tile = blockIdx.x + i * gridDim.x;\n";
+        s += "            if (tile >= n_tiles) {\n                break;\n            }\n";
+        s += "            const uint32_t st = static_cast<uint32_t>(i % " + NSs + ");\n";
+        s += "            unsigned char* buf = stage0 + st * " + TBYTES + ";\n";
+        s += "            if (i >= " + NSs + ") {\n";
+        s += "            // the buffer's previous tile: finished by its group, stored, read out of shared memory\n";
+        s += "            kt_mbar_wait(done + st, static_cast<uint32_t>(((i / " + NSs + ") - 1ull) & 1ull), err_);\n";
+        s += copies("(tile - " + NSs + " * gridDim.x)", "buf", false);
+        s += "            kt_bulk_commit();\n            kt_bulk_wait_read0();\n            }\n";
+        s += "            kt_mbar_arrive_expect_tx(full + st, " + TBYTES + ");\n";
+        s += copies("tile", "buf", true);
+        s += "            }\n";
+        // the last tiles of each buffer: stored once finished; every load has landed
+        s += "            for (unsigned long long j = (i > " + NSs + " ? i - " + NSs + " : 0ull); j < i; ++j) {\n";
+        s += "            const uint32_t st = static_cast<uint32_t>(j % " + NSs + ");\n";
+        s += "            unsigned char* buf = stage0 + st * " + TBYTES + ";\n";
+        s += "            kt_mbar_wait(full + st, static_cast<uint32_t>((j / " + NSs + ") & 1ull), err_);\n";
+        s += "            kt_mbar_wait(done + st, static_cast<uint32_t>((j / " + NSs + ") & 1ull), err_);\n";
+        s += copies("(blockIdx.x + j * gridDim.x)", "buf", false);
+        s += "            kt_bulk_commit();\n            }\n";
+        s += "            kt_bulk_wait0();\n";
+        s += "        }\n        return;\n    }\n";
+        s += "    const uint32_t grp = threadIdx.x >> " + std::to_string(TB) + ";\n";
+        s += "    const uint32_t t = threadIdx.x & " + std::to_string(GT - 1) + "u;\n";
+        s += "    C* sm = nullptr;\n";
+    } else {
+        s += "    C* __restrict__ a = static_cast<C*>(a_);\n";
+        s += "    extern __shared__ __align__(16) unsigned char smem_raw[];\n";
+        s += "    C* sm = reinterpret_cast<C*>(smem_raw);\n";
+        s += "    const uint32_t t = threadIdx.x;\n";
+    }
     if (norm) {
         // renormalisation (complex64): per-warp FP64 sums of |a|^2 over the
         // loads (first block: the target) and the stores, loads scaled by
@@ -689,6 +898,17 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     const bool skip_io = skip_mode != 0;
     const int L_run = (sizeof(typename CxT<T>::type) == 16) ? 3 : 4;
     auto coalesced = [&](const FPhase& f) {
+        if (tma) {
+            // read from / written to a stage buffer: free of bank conflicts when
+            // the three lowest thread bits land on independent 16-byte slots
+            // of a 128-byte row under the swizzle
+            uint32_t g3[3] = {0, 0, 0};
+            for (int j = 0; j < 3 && j < TB; ++j) {
+                g3[j] = tma_swz(1u << tile_bit(f.tstride[j])) & 7u;
+            }
+            return g3[0] != 0 && g3[1] != 0 && g3[2] != 0 && g3[0] != g3[1] && g3[0] != g3[2] && g3[1] != g3[2] &&
+                   (g3[0] ^ g3[1]) != g3[2];
+        }
         if (skip_mode != 2) {
             return true;
         }
@@ -702,9 +922,11 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     // jit_fence = k: every k ops the amplitudes pass through an empty asm, so
     // the scheduler cannot interleave more than k ops (bounds the live registers)
     const int fence_every = tuning().jit_fence;
-    const int first =
-        (skip_io && np > 1 && ph[0].op_begin == ph[0].op_end && identity_store(ph[0]) && coalesced(ph[1])) ? 1 : 0;
-    const int last = (skip_io && np - 1 > first && ph[np - 1].op_begin == ph[np - 1].op_end &&
+    const int first = ((skip_io || tma) && np > 1 && ph[0].op_begin == ph[0].op_end && identity_store(ph[0]) &&
+                       coalesced(ph[1]))
+                          ? 1
+                          : 0;
+    const int last = ((skip_io || tma) && np - 1 > first && ph[np - 1].op_begin == ph[np - 1].op_end &&
                       identity_store(ph[np - 2]) && coalesced(ph[np - 2]))
                          ? np - 2
                          : np - 1;
@@ -712,7 +934,7 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     // first layout) into its own slots of a second shared-memory buffer with
     // cp.async while the current tile computes; no other thread touches those
     // slots, so a wait_group is the only synchronisation.
-    const bool async_load = jit_async(fb.K, sizeof(typename CxT<T>::type));
+    const bool async_load = !tma && jit_async(fb.K, sizeof(typename CxT<T>::type));
     const int n_thr = 1 << TB;
     auto issue_async = [&](const std::string& tile_expr, const std::string& indent) {
         std::string e;
@@ -748,14 +970,34 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
     if (remat) {
         s += "    const uint32_t t_outer = t;\n";
     }
-    s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
+    if (tma) {
+        // group grp takes the CTA's tiles grp, grp + NG, ...; tile it sits in stage it % NS
+        s += "    for (unsigned long long it = grp;; it += " + std::to_string(NG) + "ull) {\n";
+        s += "        const unsigned long long tile = blockIdx.x + it * gridDim.x;\n";
+        s += "        if (tile >= n_tiles) {\n            break;\n        }\n";
+        s += "        const uint32_t st = static_cast<uint32_t>(it % " + std::to_string(NS) + "ull);\n";
+    } else {
+        s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
+    }
     if (remat) {
         s += "        uint32_t t_l;\n        asm volatile(\"mov.u32 %0, %1;\" : \"=r\"(t_l) : \"r\"(t_outer));\n";
         s += "        const uint32_t t = t_l;\n";
     }
     s += "        C v[1 << RB];\n";
     s += "        const uint64_t base = " + jit_deposit("tile", free_strides.data(), fb.nfree) + ";\n";
-    if (async_load) {
+    if (tma) {
+        // the tile's copies landed in stage st: read it in the first layout, then
+        // the group's barrier before any thread writes the buffer again
+        s += "        kt_mbar_wait(full + st, static_cast<uint32_t>((it / " + std::to_string(NS) + "ull) & 1ull), err_);\n";
+        s += "        sm = reinterpret_cast<C*>(stage0 + st * " + std::to_string(tile_bytes) + "u);\n";
+        const std::vector<uint32_t> tt = tma_thr_terms(ph[first]);
+        s += "        {\n            const uint32_t lt = " + jit_xor_terms(tt.data(), TB, 0) + ";\n";
+        for (int i = 0; i < R; ++i) {
+            s += "            v[" + std::to_string(i) + "] = sm[lt ^ " + std::to_string(tma_reg_term(ph[first], i)) + "u];\n";
+        }
+        s += "        }\n";
+        s += "        kt_bar_sync(1u + grp, " + std::to_string(GT) + "u);\n";
+    } else if (async_load) {
         s += "        asm volatile(\"cp.async.wait_group 0;\" ::: \"memory\");\n";
         for (int i = 0; i < R; ++i) {
             s += "        v[" + std::to_string(i) + "] = sb[" + std::to_string(i * n_thr) + "u + t];\n";
@@ -771,7 +1013,7 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
         s += "        if (na.in_parts != nullptr) {\n            warp_norm_add<float>(v, w_in, t);\n        }\n";
         s += "#pragma unroll\n        for (int i = 0; i < (1 << RB); ++i) {\n            v[i].x *= sc;\n            v[i].y *= sc;\n        }\n";
     }
-    if (tuning().jit_prefetch != 0 && !async_load) {
+    if (tuning().jit_prefetch != 0 && !async_load && !tma) {
         // the next tile of this CTA into L2 while this one computes: one
         // prefetch per 128-byte line when the lowest qubits are the low lanes
         const bool lines_on_lanes = TB >= 3 && ph[first].tstride[0] == 1 && ph[first].tstride[1] == 2 &&
@@ -785,6 +1027,9 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
         }
         s += "        }\n";
     }
+    // the barrier of a transpose: the whole CTA, or (TMA) the tile's own thread group
+    const std::string tbar = tma ? "            kt_bar_sync(1u + grp, " + std::to_string(GT) + "u);\n"
+                                 : "            __syncthreads();\n";
     for (int p = first; p <= last; ++p) {
         const FPhase& cur = ph[p];
         if (p > first) {
@@ -793,12 +1038,12 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
             for (int i = 0; i < R; ++i) {
                 s += "            sm[so ^ " + std::to_string(reg_xor(prev.rsw_out, i)) + "u] = v[" + std::to_string(i) + "];\n";
             }
-            s += "            __syncthreads();\n";
+            s += tbar;
             s += "            const uint32_t lo = " + jit_xor_terms(cur.tsw, TB, 0) + ";\n";
             for (int i = 0; i < R; ++i) {
                 s += "            v[" + std::to_string(i) + "] = sm[lo ^ " + std::to_string(reg_xor(cur.rsw, i)) + "u];\n";
             }
-            s += "            __syncthreads();\n        }\n";
+            s += tbar + "        }\n";
         }
         // Diagonal ops whose target (and controls, if any) are thread or
         // tile-external bits scale all of a thread's amplitudes by one factor;
@@ -878,11 +1123,22 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm)
         }
         s += "        }\n";
     }
-    s += "        {\n            C* dst = a + base + " + jit_deposit("t", ph[last].tstride, TB) + ";\n";
-    for (int i = 0; i < R; ++i) {
-        s += "            dst[" + std::to_string(reg_off(ph[last], i)) + "ULL] = v[" + std::to_string(i) + "];\n";
+    if (tma) {
+        // the tile into its stage buffer in the tensor map's order, visible to
+        // the TMA store the producer issues once the whole group has arrived
+        const std::vector<uint32_t> tt = tma_thr_terms(ph[last]);
+        s += "        {\n            const uint32_t lt = " + jit_xor_terms(tt.data(), TB, 0) + ";\n";
+        for (int i = 0; i < R; ++i) {
+            s += "            sm[lt ^ " + std::to_string(tma_reg_term(ph[last], i)) + "u] = v[" + std::to_string(i) + "];\n";
+        }
+        s += "        }\n        kt_fence_proxy_async_smem();\n        kt_mbar_arrive(done + st);\n";
+    } else {
+        s += "        {\n            C* dst = a + base + " + jit_deposit("t", ph[last].tstride, TB) + ";\n";
+        for (int i = 0; i < R; ++i) {
+            s += "            dst[" + std::to_string(reg_off(ph[last], i)) + "ULL] = v[" + std::to_string(i) + "];\n";
+        }
+        s += "        }\n";
     }
-    s += "        }\n";
     if (norm) {
         s += "        warp_norm_add<float>(v, w_out, t);\n";
     }
@@ -981,7 +1237,7 @@ std::vector<T> jit_block_mats(const Plan<T>& plan, size_t b, bool* ok)
 }
 
 constexpr const char* JIT_PRELUDE =
-    "#include \"kt_fused_dev.cuh\"\n\n"
+    "#include \"kt_fused_dev.cuh\"\n#include \"kt_tma_dev.cuh\"\n\n"
     "template <int N>\nstruct KtMats\n{\n    double m[N];\n};\n\n"
     "template <int N>\nstruct KtMatsF\n{\n    float m[N];\n};\n\n"
     "template <int N>\n__device__ __forceinline__ void kt_jit_fence(double2 (&v)[N])\n{\n"
@@ -1034,7 +1290,7 @@ JitCache& jit_cache()
 // so compiling waits for its second apply.
 template <typename T>
 bool jit_kernels(const Plan<T>& plan, int RB, int threads, int minb, int smem_bytes, bool on_repeat, bool norm,
-                 std::vector<const void*>& out)
+                 std::vector<const void*>& out, const std::vector<TmaCfg>* tma = nullptr)
 {
     JitCache& jc = jit_cache();
     std::lock_guard<std::mutex> lock(jc.m);
@@ -1048,7 +1304,7 @@ bool jit_kernels(const Plan<T>& plan, int RB, int threads, int minb, int smem_by
     std::vector<size_t> missing;
     std::unordered_map<std::string, size_t> first_of;
     for (size_t b = 0; b < nb; ++b) {
-        keys[b] = bounds + jit_block_body<T>(plan, b, RB, norm);
+        keys[b] = bounds + jit_block_body<T>(plan, b, RB, norm, tma ? &(*tma)[b] : nullptr);
         if (jc.kernels.count(keys[b]) == 0 && first_of.count(keys[b]) == 0) {
             first_of[keys[b]] = b;
             missing.push_back(b);
@@ -1140,6 +1396,98 @@ bool jit_kernels(const Plan<T>& plan, int RB, int threads, int minb, int smem_by
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// Host side of the TMA block kernels: the tensor map of a block over the
+// state (cuTensorMapEncodeTiled, reached through the runtime so the library
+// keeps no link-time dependency on the driver library), and the error word
+// their bounded waits set.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q {};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<EncodeTiledFn>(nullptr);
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+bool tma_encode(const TmaGeom& g, void* amps, CUtensorMap* out)
+{
+    EncodeTiledFn fn = encode_tiled();
+    if (fn == nullptr || !g.ok) {
+        return false;
+    }
+    cuuint64_t dims[5];
+    cuuint64_t strides[4];
+    cuuint32_t box[5];
+    cuuint32_t estr[5];
+    for (int r = 0; r < g.rank; ++r) {
+        dims[r] = g.dim[r];
+        box[r] = g.box[r];
+        estr[r] = 1;
+        if (r > 0) {
+            strides[r - 1] = g.stride[r];
+        }
+    }
+    return fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, static_cast<cuuint32_t>(g.rank), amps, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// One error word per device (set by a TMA block kernel whose bounded wait ran
+// out) and a pinned host copy of it, refreshed after every apply that ran
+// such kernels; the C entry points report it once the copy has landed.
+struct TmaErr
+{
+    std::mutex m;
+    std::map<int, unsigned int*> dev;
+    unsigned int* host {nullptr};  // pinned, one word per device ordinal (up to 64)
+};
+
+TmaErr& tma_err()
+{
+    static TmaErr e;
+    return e;
+}
+
+unsigned int* tma_err_word(int dev, unsigned int** host)
+{
+    TmaErr& e = tma_err();
+    std::lock_guard<std::mutex> lock(e.m);
+    if (e.host == nullptr) {
+        void* h = nullptr;
+        if (cudaMallocHost(&h, 64 * sizeof(unsigned int)) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        std::memset(h, 0, 64 * sizeof(unsigned int));
+        e.host = static_cast<unsigned int*>(h);
+    }
+    if (dev < 0 || dev >= 64) {
+        return nullptr;
+    }
+    auto it = e.dev.find(dev);
+    if (it == e.dev.end()) {
+        void* d = nullptr;
+        if (cudaMalloc(&d, 256) != cudaSuccess || cudaMemset(d, 0, 256) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        it = e.dev.emplace(dev, static_cast<unsigned int*>(d)).first;
+    }
+    *host = e.host + dev;
+    return it->second;
+}
+
 // The apply of a plan from which its compiled kernels pay for themselves:
 // compiling takes about 0.6 s per block kernel on one host thread (the
 // blocks compile in parallel), and a compiled pass saves about half of a
@@ -1184,14 +1532,45 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
         minb = fused_ctas(shape);
     }
     const uint64_t n_tiles = uint64_t {1} << (n - K);
-    const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * minb);
-    const size_t smem = (size_t {1} << K) * sizeof(C) * (jit_async(K, sizeof(C)) ? 2 : 1);
-    const int smem_attr = std::max(fused_smem_limit(shape), static_cast<int>(smem));
+    uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * minb);
+    size_t smem = (size_t {1} << K) * sizeof(C) * (jit_async(K, sizeof(C)) ? 2 : 1);
+    int smem_attr = std::max(fused_smem_limit(shape), static_cast<int>(smem));
     const int RB = rb3 ? Cfg3::RB : Cfg<T>::RB;
     const bool norm = parts != nullptr;
     if (norm && grid > static_cast<uint64_t>(*n_parts_out)) {
         return false;  // the caller reserved per-CTA sums for fewer CTAs
     }
+    // TMA-pipelined kernels (complex128, no renormalisation): one persistent
+    // CTA per SM of jit_tma_groups tile-sized thread groups and a producer
+    // warp, jit_tma_stages tile buffers; every block's tile must have the
+    // three lowest qubits (one 128-byte row per box line)
+    std::vector<TmaCfg> tma_cfg;
+    if (tuning().jit_tma != 0 && std::is_same<T, double>::value && !norm && encode_tiled() != nullptr) {
+        const int groups = tuning().jit_tma_groups;
+        const int stages = std::max(tuning().jit_tma_stages, groups + 1);
+        const size_t tile_bytes = (size_t {1} << K) * sizeof(C);
+        const size_t need = static_cast<size_t>(stages) * tile_bytes + 1024 + 16 * static_cast<size_t>(stages);
+        const int tthreads = groups * threads + 32;
+        bool ok = need <= 227 * 1024 && tthreads <= 1024 && (groups * threads) % 32 == 0;
+        for (size_t b = 0; ok && b < plan.blocks.size(); ++b) {
+            TmaCfg c;
+            c.groups = groups;
+            c.stages = stages;
+            c.geom = tma_geom(plan.blocks[b], n);
+            ok = c.geom.ok;
+            tma_cfg.push_back(std::move(c));
+        }
+        if (ok) {
+            threads = tthreads;
+            minb = 1;
+            grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()));
+            smem = need;
+            smem_attr = static_cast<int>(need);
+        } else {
+            tma_cfg.clear();
+        }
+    }
+    const bool use_tma = !tma_cfg.empty();
     // this plan's kernels: resolved once, compiled once the plan has been
     // applied often enough to repay the compile (jit_after_applies)
     std::vector<const void*> jk;
@@ -1204,7 +1583,10 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
                                std::to_string(jit_async(K, sizeof(C)) ? 1 : 0) + "/" +
                                std::to_string(tuning().jit_prefetch) + std::to_string(tuning().jit_merge_diag) +
                                std::to_string(tuning().jit_skip_io) + std::to_string(tuning().jit_fence) +
-                               std::to_string(tuning().jit_scale_ops) + std::to_string(tuning().jit_remat);
+                               std::to_string(tuning().jit_scale_ops) + std::to_string(tuning().jit_remat) +
+                               (use_tma ? "/tma" + std::to_string(tma_cfg[0].groups) + "x" +
+                                              std::to_string(tma_cfg[0].stages)
+                                        : std::string());
     bool ready = false;
     bool compile = compile_only || mode == 1;
     {
@@ -1224,7 +1606,8 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
         compile = compile || st.prepared || st.applies >= jit_after_applies(n, sizeof(C));
     }
     if (!ready) {
-        if (!compile || !jit_kernels<T>(plan, RB, threads, minb, smem_attr, false, norm, jk)) {
+        if (!compile ||
+            !jit_kernels<T>(plan, RB, threads, minb, smem_attr, false, norm, jk, use_tma ? &tma_cfg : nullptr)) {
             return false;
         }
         JitCache& jc = jit_cache();
@@ -1252,10 +1635,25 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
             return false;  // scale factors out of range: the precompiled kernels run this apply
         }
     }
+    unsigned int* err_host = nullptr;
+    unsigned int* err_dev = use_tma ? tma_err_word(dev, &err_host) : nullptr;
+    if (use_tma && err_dev == nullptr) {
+        return false;
+    }
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         std::vector<T>& mats = all_mats[b];
         cudaError_t e = cudaSuccess;
-        if (norm) {
+        if (use_tma) {
+            CUtensorMap tm;
+            if (!tma_encode(tma_cfg[b].geom, a, &tm)) {
+                *rc = KT_ERR_CUDA;
+                set_error(KT_ERR_CUDA, "cuTensorMapEncodeTiled failed for a block's tile");
+                return true;
+            }
+            void* args[] = {&tm, &a, &nt, &err_dev, mats.data()};
+            e = cudaLaunchKernel(jk[b], dim3(static_cast<unsigned>(grid)), dim3(static_cast<unsigned>(threads)), args,
+                                 smem, s.stream);
+        } else if (norm) {
             NormArgs na {};
             na.n_parts = np;
             na.target = (b == 0) ? nullptr : target;
@@ -1276,6 +1674,14 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
         }
         s.last_launches += 1;
         s.last_alg_bytes += pass_bytes;
+    }
+    if (use_tma) {
+        // the error word to the host once these blocks are done (read by the C entry points)
+        const cudaError_t e = cudaMemcpyAsync(err_host, err_dev, sizeof(unsigned int), cudaMemcpyDeviceToHost, s.stream);
+        if (e != cudaSuccess) {
+            *rc = cuda_fail(e, "cudaMemcpyAsync(block kernel error word)");
+            return true;
+        }
     }
     *n_parts_out = np;
     jit_cache().launches += static_cast<int64_t>(plan.blocks.size());
@@ -1631,12 +2037,20 @@ int32_t jit_compile_only_t(int n, const std::vector<LGate>& gates, int64_t* n_ke
     const int threads = 1 << (K - RB);
     // complex64 applies renormalise by default
     const bool norm = std::is_same<T, float>::value && tuning().c64_renormalize != 0;
+    const bool tma = tuning().jit_tma != 0 && std::is_same<T, double>::value && !norm;
     std::vector<std::string> sources(1, JIT_PRELUDE);
     std::vector<std::vector<std::string>> names(1);
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         const std::string name = "kt_jc" + std::to_string(b);
-        sources[0] += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(threads) + ", " +
-                      std::to_string(threads > 256 ? 1 : 2) + ") " + name + jit_block_body<T>(plan, b, RB, norm) + "\n";
+        TmaCfg c;
+        c.groups = tuning().jit_tma_groups;
+        c.stages = std::max(tuning().jit_tma_stages, c.groups + 1);
+        c.geom = tma_geom(plan.blocks[b], n);
+        const bool bt = tma && c.geom.ok;
+        const int bthreads = bt ? c.groups * threads + 32 : threads;
+        sources[0] += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(bthreads) + ", " +
+                      std::to_string(bt || threads > 256 ? 1 : 2) + ") " + name +
+                      jit_block_body<T>(plan, b, RB, norm, bt ? &c : nullptr) + "\n";
         names[0].push_back(name);
     }
     std::vector<std::vector<const void*>> got;
@@ -1648,6 +2062,32 @@ int32_t jit_compile_only_t(int n, const std::vector<LGate>& gates, int64_t* n_ke
 }
 
 }  // namespace
+
+int32_t jit_async_error()
+{
+    TmaErr& e = tma_err();
+    std::lock_guard<std::mutex> lock(e.m);
+    if (e.host == nullptr) {
+        return KT_OK;
+    }
+    for (const auto& kv : e.dev) {
+        volatile unsigned int* h = e.host + kv.first;
+        if (*h != 0u) {
+            // clear it on the device (the next launches must start clean) and here
+            int cur = 0;
+            cudaGetDevice(&cur);
+            cudaSetDevice(kv.first);
+            cudaMemset(kv.second, 0, sizeof(unsigned int));
+            cudaDeviceSynchronize();
+            cudaSetDevice(cur);
+            *h = 0u;
+            set_error(KT_ERR_TIMEOUT, "a TMA block kernel's bounded wait ran out on device " + std::to_string(kv.first) +
+                                          ": the results of the applies since the last check are void");
+            return KT_ERR_TIMEOUT;
+        }
+    }
+    return KT_OK;
+}
 
 int32_t jit_compile_only(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* n_kernels)
 {

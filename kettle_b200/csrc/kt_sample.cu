@@ -751,8 +751,13 @@ __global__ void k_seq_search(const double* __restrict__ cdf, uint64_t N, const d
 
 }  // namespace
 
-int32_t sample(State& s, const double* noise, const double* canonicals, int64_t n_shots, uint64_t* out, int32_t mode,
-               int32_t* n_rescanned)
+namespace
+{
+
+// The sampler over N probabilities: the state's own (|a_i|^2 with its noise)
+// or, with host_probs, a caller's vector uploaded as it is.
+int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double* noise, const double* canonicals,
+                    int64_t n_shots, uint64_t* out, int32_t mode, int32_t* n_rescanned)
 {
     if (n_rescanned) {
         *n_rescanned = 0;
@@ -760,7 +765,6 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
     if (n_shots <= 0) {
         return KT_OK;
     }
-    const uint64_t N = s.n_amps();
     const uint64_t n_chunks = (N + CHUNK - 1) / CHUNK;
     auto al = [](size_t v) { return (v + 255) & ~size_t {255}; };
     const size_t ns = static_cast<size_t>(n_shots);
@@ -800,7 +804,11 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
     auto* d_ints = reinterpret_cast<unsigned long long*>(base + off_ints);
     auto* d_carry = reinterpret_cast<double*>(base + off_carry);
 
-    if (const int32_t rc = device_probabilities(s, noise, dp); rc != KT_OK) {
+    if (host_probs != nullptr) {
+        if (const int32_t rc = copy_h2d(dp, host_probs, N * 8, s.stream); rc != KT_OK) {
+            return rc;
+        }
+    } else if (const int32_t rc = device_probabilities(s, noise, dp); rc != KT_OK) {
         return rc;
     }
     if (const int32_t rc = copy_h2d(d_canon, canonicals, ns * 8, s.stream); rc != KT_OK) {
@@ -856,6 +864,20 @@ int32_t sample(State& s, const double* noise, const double* canonicals, int64_t 
         }
     }
     return copy_d2h(out, d_out, ns * 8, s.stream);
+}
+
+}  // namespace
+
+int32_t sample(State& s, const double* noise, const double* canonicals, int64_t n_shots, uint64_t* out, int32_t mode,
+               int32_t* n_rescanned)
+{
+    return sample_core(s, s.n_amps(), nullptr, noise, canonicals, n_shots, out, mode, n_rescanned);
+}
+
+int32_t sample_from_probabilities(State& s, const double* host_probs, uint64_t n, const double* canonicals,
+                                  int64_t n_shots, uint64_t* out, int32_t mode, int32_t* n_rescanned)
+{
+    return sample_core(s, n, host_probs, nullptr, canonicals, n_shots, out, mode, n_rescanned);
 }
 
 }  // namespace kt

@@ -1034,6 +1034,38 @@ auto inner_product_norm_squared(const Statevector& left, const Statevector& righ
     return std::norm(inner_product(left, right));
 }
 
+auto tensor_product(const Statevector& left, const Statevector& right) -> Statevector
+{
+    // state/state.cpp:144-157: the product is built as a new Statevector from its
+    // coefficients, whose constructor checks the normalisation
+    if (left.dtype() != right.dtype()) {
+        throw std::runtime_error {"ERROR: cannot take the tensor product of states of different precision.\n"};
+    }
+    Statevector out {left.n_qubits() + right.n_qubits(), left.dtype()};
+    check(kt_sv_tensor_product(left.device(), right.device(), out.device()));
+    out.mark_device_modified();
+    double sum = 0.0;
+    check(kt_sv_norm_sq(out.device(), &sum));
+    if (!(std::fabs(sum - 1.0) < CONSTRUCTION_NORMALIZATION_TOLERANCE)) {
+        std::stringstream err;
+        err << "The provided coefficients are not properly normalized.\n";
+        err << "Found sum of squared norms : " << std::fixed << std::setprecision(14) << sum;
+        throw std::runtime_error {err.str()};
+    }
+    return out;
+}
+
+auto diagonal_expectation_value(const std::vector<std::complex<double>>& eigenvalues, const Statevector& state)
+    -> std::complex<double>
+{
+    if (eigenvalues.size() != state.n_states()) {
+        throw std::runtime_error {"ERROR: mismatch in sizes when taking expectation value of diagonal operator.\n"};
+    }
+    double out[2] = {0.0, 0.0};
+    check(kt_sv_diagonal_expectation(state.device(), reinterpret_cast<const double*>(eigenvalues.data()), out));
+    return {out[0], out[1]};
+}
+
 // ---- DensityMatrix ------------------------------------------------------------------------------
 
 DensityMatrix::DensityMatrix(HostMatrix matrix, const density_matrix_nocheck&, DType dtype)
@@ -1395,7 +1427,7 @@ auto StatevectorSimulator::classical_register() -> ClassicalRegister&
     return *cregister_;
 }
 
-void DensityMatrixSimulator::run(const QuantumCircuit& circuit, DensityMatrix& state, std::optional<int>)
+void DensityMatrixSimulator::run(const QuantumCircuit& circuit, DensityMatrix& state, std::optional<int> prng_seed)
 {
     check_valid_number_of_qubits(circuit.n_qubits(), state.n_qubits());
     if (circuit.n_qubits() != n_qubits_) {
@@ -1408,8 +1440,17 @@ void DensityMatrixSimulator::run(const QuantumCircuit& circuit, DensityMatrix& s
         [&](const std::vector<kt_gate>& seg) {
             check(kt_dm_apply(h, seg.data(), static_cast<int64_t>(seg.size()), nullptr, 0, KT_APPLY_FUSED));
         },
-        [&](std::size_t, std::size_t) {
-            throw std::runtime_error {"ERROR: M gates on a DensityMatrix are not supported by the B200 engine.\n"};
+        [&](std::size_t qubit, std::size_t bit) {
+            // simulation/measure_density_matrix.hpp:33-56: P(0), P(1); a fresh prng per
+            // M gate; discrete draw; the surviving block scaled by sqrt(1 / P)
+            double p0 = 0.0, p1 = 0.0;
+            check(kt_dm_measure_probs(h, static_cast<uint32_t>(qubit), &p0, &p1));
+            auto prng = make_prng(prng_seed);
+            auto coin = std::discrete_distribution<int> {{p0, p1}};
+            const int outcome = coin(prng);
+            const double norm = std::sqrt(1.0 / (outcome == 0 ? p0 : p1));
+            check(kt_dm_collapse(h, static_cast<uint32_t>(qubit), outcome, norm));
+            cregister_->set(bit, outcome);
         },
         [&](const CircuitLogger&) {
             // simulate_density_matrix.cpp:391-392
@@ -1437,6 +1478,45 @@ void simulate(const QuantumCircuit& circuit, DensityMatrix& state, std::optional
 {
     auto sim = DensityMatrixSimulator {state.n_qubits()};
     sim.run(circuit, state, prng_seed);
+}
+
+void StatevectorPauliStringSimulator::run(const SparsePauliString& pauli_string, Statevector& state)
+{
+    // simulation/simulate_pauli.cpp:91-122: the string's X / Y / Z gates in term
+    // order, one fused apply; the string's phase is not applied
+    if (pauli_string.n_qubits() != state.n_qubits()) {
+        throw std::runtime_error {"Invalid simulation; SparsePauliString and state have different number of qubits."};
+    }
+    if (pauli_string.n_qubits() == 0) {
+        throw std::runtime_error {"Cannot simulate a SparsePauliString or state with zero qubits."};
+    }
+    std::vector<kt_gate> gates;
+    for (const auto& [q, t] : pauli_string.terms()) {
+        kt_gate g {};
+        g.param = -1;
+        g.target = static_cast<uint32_t>(q);
+        if (t == PauliTerm::X) {
+            g.op = static_cast<uint8_t>(Gate::X);
+        } else if (t == PauliTerm::Y) {
+            g.op = static_cast<uint8_t>(Gate::Y);
+        } else if (t == PauliTerm::Z) {
+            g.op = static_cast<uint8_t>(Gate::Z);
+        } else {
+            continue;
+        }
+        gates.push_back(g);
+    }
+    if (!gates.empty()) {
+        check(kt_sv_apply(state.device(), gates.data(), static_cast<int64_t>(gates.size()), nullptr, 0, KT_APPLY_FUSED));
+        state.mark_device_modified();
+    }
+    has_been_run_ = true;
+}
+
+void simulate(const SparsePauliString& pauli_string, Statevector& state)
+{
+    auto simulator = StatevectorPauliStringSimulator {};
+    simulator.run(pauli_string, state);
 }
 
 // ---- Pauli ---------------------------------------------------------------------------------------
@@ -1723,6 +1803,98 @@ auto perform_measurements_as_memory(const Statevector& state, std::size_t n_shot
     check(kt_sv_sample(state.device(), noise ? noise->values().data() : nullptr, canon.data(),
                        static_cast<int64_t>(n_shots), idx.data(), 0, &rescanned));
     return {idx.begin(), idx.end()};
+}
+
+namespace
+{
+
+// ProbabilitySampler_ (measurements.cpp:288-311) on a probability vector: one
+// mt19937 for all shots, one generate_canonical draw per shot, scaled by the
+// CDF bound and searched on the device
+auto sample_probabilities(const std::vector<double>& probabilities_raw, std::size_t n_shots, std::optional<int> seed)
+    -> std::vector<std::size_t>
+{
+    auto prng = make_prng(seed);
+    std::vector<double> canon(n_shots);
+    for (auto& c : canon) {
+        c = std::generate_canonical<double, std::numeric_limits<double>::digits>(prng);
+    }
+    std::vector<uint64_t> idx(n_shots);
+    check(kt_sample_probabilities(probabilities_raw.data(), probabilities_raw.size(), canon.data(),
+                                  static_cast<int64_t>(n_shots), idx.data(), 0, nullptr));
+    return {idx.begin(), idx.end()};
+}
+
+auto marginal_mask(const std::vector<std::size_t>& marginal_qubits, std::size_t n) -> std::vector<char>
+{
+    // build_marginal_bitmask_ (measurements.cpp:269-286)
+    std::vector<char> marginal(n, 0);
+    for (auto q : marginal_qubits) {
+        if (q >= n) {
+            throw std::runtime_error {"ERROR: marginal qubit index out of range."};
+        }
+    }
+    for (auto q : marginal_qubits) {
+        marginal[q] = 1;
+    }
+    return marginal;
+}
+
+// state_index_to_bitstring_marginal_ (state/marginal.cpp:19-45): character q = qubit q, 'x' if marginal
+auto marginal_bitstring(std::size_t i, const std::vector<char>& marginal) -> std::string
+{
+    const auto n = marginal.size();
+    std::string s(n, '0');
+    for (std::size_t q = 0; q < n; ++q) {
+        s[q] = marginal[q] ? 'x' : (((i >> q) & 1U) ? '1' : '0');
+    }
+    return s;
+}
+
+}  // namespace
+
+auto perform_measurements_as_memory(const std::vector<double>& probabilities_raw, std::size_t n_shots,
+                                    std::optional<int> seed) -> std::vector<std::size_t>
+{
+    return sample_probabilities(probabilities_raw, n_shots, seed);
+}
+
+auto perform_measurements_as_counts_raw(const std::vector<double>& probabilities_raw, std::size_t n_shots,
+                                        std::optional<int> seed) -> std::map<std::size_t, std::size_t>
+{
+    return memory_to_counts(sample_probabilities(probabilities_raw, n_shots, seed));
+}
+
+auto perform_measurements_as_counts_marginal(const std::vector<double>& probabilities_raw, std::size_t n_shots,
+                                             const std::vector<std::size_t>& marginal_qubits, std::optional<int> seed)
+    -> std::map<std::string, std::size_t>
+{
+    if (!is_power_of_2(probabilities_raw.size())) {
+        throw std::runtime_error {"The number of probabilities must be a power of 2.\n"};
+    }
+    const auto n = static_cast<std::size_t>(__builtin_ctzll(probabilities_raw.size()));
+    const auto marginal = marginal_mask(marginal_qubits, n);
+    std::map<std::string, std::size_t> out;
+    for (auto i : sample_probabilities(probabilities_raw, n_shots, seed)) {
+        ++out[marginal_bitstring(i, marginal)];
+    }
+    return out;
+}
+
+auto perform_measurements_as_counts_marginal(const QuantumCircuit& circuit, const Statevector& original_state,
+                                             std::size_t n_shots, const std::vector<std::size_t>& marginal_qubits,
+                                             const QuantumNoise* noise, std::optional<int> seed)
+    -> std::map<std::string, std::size_t>
+{
+    const auto marginal = marginal_mask(marginal_qubits, circuit.n_qubits());
+    std::map<std::string, std::size_t> out;
+    for (std::size_t shot = 0; shot < n_shots; ++shot) {
+        auto state = original_state;
+        simulate(circuit, state);
+        const auto idx = perform_measurements_as_memory(state, 1, noise, seed);
+        ++out[marginal_bitstring(idx[0], marginal)];
+    }
+    return out;
 }
 
 auto perform_measurements_as_counts_raw(const Statevector& state, std::size_t n_shots, const QuantumNoise* noise,

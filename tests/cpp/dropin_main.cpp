@@ -468,5 +468,92 @@ int main(int argc, char** argv)
             std::printf("tperr %s\n", std::string {err.what()}.find("different numbers of qubits") != std::string::npos ? "qubits" : "other");
         }
     }
+    // 10. a Pauli string applied to a state, statevector tensor products, a
+    //     diagonal expectation value, sampling from a probability vector, the
+    //     circuit-and-state marginal counts, and M gates on a density matrix
+    {
+        auto pc = ket::QuantumCircuit {n};
+        build(pc, n, 2, r);
+        auto ps = ket::Statevector {n};
+        ket::simulate(pc, ps);
+        auto terms = std::vector<std::pair<std::size_t, ket::PauliTerm>> {};
+        const ket::PauliTerm kinds[3] = {ket::PauliTerm::X, ket::PauliTerm::Y, ket::PauliTerm::Z};
+        for (std::size_t q = 0; q < n; ++q) {
+            if (r.below(4) != 0) {
+                terms.emplace_back(q, kinds[r.below(3)]);
+            }
+        }
+        ket::simulate(ket::SparsePauliString {terms, n, ket::PauliPhase::MINUS_EYE}, ps);
+        for (std::size_t i = 0; i < ps.n_states(); ++i) {
+            std::printf("psamp %zu %.17g %.17g\n", i, ps[i].real(), ps[i].imag());
+        }
+        try {
+            ket::simulate(ket::SparsePauliString {n + 1}, ps);
+        } catch (const std::runtime_error& err) {
+            std::printf("pserr %d\n", static_cast<int>(std::string {err.what()}.find("different number of qubits") != std::string::npos));
+        }
+        const std::size_t na = (n + 1) / 2;
+        auto ca = ket::QuantumCircuit {na};
+        build(ca, na, 2, r);
+        auto cb = ket::QuantumCircuit {n - na + 1};
+        build(cb, n - na + 1, 2, r);
+        auto sa = ket::Statevector {na};
+        auto sb = ket::Statevector {n - na + 1};
+        ket::simulate(ca, sa);
+        ket::simulate(cb, sb);
+        const auto tp = ket::tensor_product(sa, sb);
+        for (std::size_t i = 0; i < tp.n_states(); ++i) {
+            std::printf("svtp %zu %.17g %.17g\n", i, tp[i].real(), tp[i].imag());
+        }
+        auto eig = std::vector<std::complex<double>> {};
+        for (std::size_t i = 0; i < ps.n_states(); ++i) {
+            eig.emplace_back(2.0 * r.uniform() - 1.0, 2.0 * r.uniform() - 1.0);
+        }
+        const auto de = ket::diagonal_expectation_value(eig, ps);
+        std::printf("diagexp %.17g %.17g\n", de.real(), de.imag());
+        const auto probs = ket::calculate_probabilities_raw(ps);
+        const auto mem = ket::perform_measurements_as_memory(probs, 64, 17);
+        for (std::size_t k = 0; k < mem.size(); ++k) {
+            std::printf("pmem %zu %zu\n", k, mem[k]);
+        }
+        for (const auto& [idx, cnt] : ket::perform_measurements_as_counts_raw(probs, 256, 23)) {
+            std::printf("pcraw %zu %zu\n", idx, cnt);
+        }
+        for (const auto& [bits, cnt] : ket::perform_measurements_as_counts_marginal(probs, 256, {0, n - 1}, 29)) {
+            std::printf("pcmarg %s %zu\n", bits.c_str(), cnt);
+        }
+        auto odd = std::vector<double> {0.25, 0.5, 0.25};
+        for (const auto& [idx, cnt] : ket::perform_measurements_as_counts_raw(odd, 64, 31)) {
+            std::printf("pcodd %zu %zu\n", idx, cnt);
+        }
+        try {
+            (void) ket::perform_measurements_as_counts_marginal(odd, 8, {}, 31);
+        } catch (const std::runtime_error& err) {
+            std::printf("pmerr %d\n", static_cast<int>(std::string {err.what()}.find("power of 2") != std::string::npos));
+        }
+        for (const auto& [bits, cnt] : ket::perform_measurements_as_counts_marginal(pc, ket::Statevector {n}, 6, {1}, nullptr, 37)) {
+            std::printf("ccmarg %s %zu\n", bits.c_str(), cnt);
+        }
+        // M gates on a density matrix (fewer qubits: the reference's density
+        // matrix passes are slow)
+        const std::size_t nd = std::min<std::size_t>(n, 5);
+        auto mc = ket::QuantumCircuit {nd, nd};
+        build(mc, nd, 1, r);
+        mc.add_m_gate(0, 0);
+        build(mc, nd, 1, r);
+        mc.add_m_gate(nd - 1, nd - 1);
+        mc.add_m_gate(1 % nd, 1 % nd);
+        auto mdm = ket::DensityMatrix {std::string(nd, '0')};
+        auto dsim = ket::DensityMatrixSimulator {nd};
+        dsim.run(mc, mdm, 43);
+        std::printf("dmmbits %d %d %d\n", dsim.classical_register().get(0), dsim.classical_register().get(nd - 1),
+                    dsim.classical_register().get(1 % nd));
+        const auto& dm2 = mdm.matrix();
+        for (long rr = 0; rr < dm2.rows(); ++rr) {
+            for (long cc = 0; cc < dm2.cols(); ++cc) {
+                std::printf("dmmrho %ld %ld %.17g %.17g\n", rr, cc, dm2(rr, cc).real(), dm2(rr, cc).imag());
+            }
+        }
+    }
     return 0;
 }

@@ -26,10 +26,11 @@ def _run(exe, *args):
     assert out.returncode == 0, out.stderr
     rec = {"amp": {}, "mamp": {}, "cfamp": {}, "ioamp": {}, "npamp": {}, "rho": {}, "count": {}, "expect": None,
            "cbits": None, "cfbits": None, "logbit": {}, "logamp": {}, "svtext": {}, "svload": {}, "ioerr": {},
-           "cgamp": {}, "ptrace": {}, "tensor": {}, "nq": {}, "tpamp": {}}
+           "cgamp": {}, "ptrace": {}, "tensor": {}, "nq": {}, "tpamp": {}, "psamp": {}, "svtp": {}, "pmem": {},
+           "pcraw": {}, "pcmarg": {}, "pcodd": {}, "ccmarg": {}, "dmmrho": {}}
     for line in out.stdout.splitlines():
         f = line.split()
-        if f[0] in ("amp", "mamp", "cfamp", "ioamp", "npamp", "cgamp", "tpamp"):
+        if f[0] in ("amp", "mamp", "cfamp", "ioamp", "npamp", "cgamp", "tpamp", "psamp", "svtp"):
             rec[f[0]][int(f[1])] = complex(float(f[2]), float(f[3]))
         elif f[0] == "cfbits":
             rec["cfbits"] = tuple(int(x) for x in f[1:])
@@ -73,6 +74,18 @@ def _run(exe, *args):
             rec["ioerr"][f[1]] = f[2]
         elif f[0] == "cbit0":
             rec["cbits"] = (int(f[1]), int(f[3]))
+        elif f[0] in ("pmem", "pcraw", "pcodd"):
+            rec[f[0]][int(f[1])] = int(f[2])
+        elif f[0] in ("pcmarg", "ccmarg"):
+            rec[f[0]][f[1]] = int(f[2])
+        elif f[0] == "diagexp":
+            rec[f[0]] = complex(float(f[1]), float(f[2]))
+        elif f[0] in ("pserr", "pmerr"):
+            rec[f[0]] = int(f[1])
+        elif f[0] == "dmmbits":
+            rec[f[0]] = tuple(int(x) for x in f[1:])
+        elif f[0] == "dmmrho":
+            rec[f[0]][(int(f[1]), int(f[2]))] = complex(float(f[3]), float(f[4]))
     return rec
 
 
@@ -151,3 +164,18 @@ def test_dropin_same_results(engine, n, layers, seed):
     pb = np.array([our["tpamp"][i] for i in sorted(our["tpamp"])])
     assert pa.size == 1 << n and np.abs(pa - pb).max() < 1e-12
     assert ref["tperr"] == our["tperr"] == "qubits"
+    # Pauli string on a state, statevector tensor product, diagonal expectation,
+    # probability-vector sampling, circuit-and-state marginal counts, M on a density matrix
+    for key, size in (("psamp", 1 << n), ("svtp", 1 << (n + 1))):
+        pa = np.array([ref[key][i] for i in sorted(ref[key])])
+        pb = np.array([our[key][i] for i in sorted(our[key])])
+        assert pa.size == size and np.abs(pa - pb).max() < 1e-12, key
+    assert ref["pserr"] == our["pserr"] == 1
+    assert abs(ref["diagexp"] - our["diagexp"]) < 1e-12
+    for key in ("pmem", "pcraw", "pcmarg", "pcodd", "ccmarg"):
+        assert ref[key] == our[key] and len(ref[key]) > 0, key
+    assert ref["pmerr"] == our["pmerr"] == 1
+    assert ref["dmmbits"] == our["dmmbits"]
+    da = np.array([ref["dmmrho"][k] for k in sorted(ref["dmmrho"])])
+    db = np.array([our["dmmrho"][k] for k in sorted(our["dmmrho"])])
+    assert da.size == 4 ** min(n, 5) and np.abs(da - db).max() < 1e-12

@@ -263,3 +263,51 @@ def test_scaled_ops_out_of_range_fall_back(jit, port):
     got = _apply(n, init, g)
     assert capi.jit_stats()["launches"] > s0["launches"]
     assert np.abs(got - port.apply(n, init, g)).max() < 1e-12
+
+
+@pytest.mark.parametrize("knobs", [
+    {"jit_tma": 1},
+    {"jit_tma": 1, "jit_tma_groups": 2},
+    {"jit_tma": 1, "jit_tma_stages": 2},
+    {"jit_tma": 1, "jit_tma_groups": 2, "jit_tma_stages": 6, "fused_tile_bits": 11},
+    {"jit_tma": 1, "fused_reg_bits": 3},
+])
+@pytest.mark.parametrize("n,layers,seed", [(13, 4, 81), (18, 4, 82), (22, 3, 83)])
+def test_tma_blocks_match_oracle(jit, port, knobs, n, layers, seed):
+    """TMA-pipelined compiled blocks (tiles moved by tensor copies into
+    swizzled stage buffers, a producer warp, one or two tile groups per CTA):
+    the oracle's amplitudes; from 13 qubits (two tiles) to 22 (every tile
+    shape the planner makes, including tiles with more than four runs)."""
+    old = {k: capi.tuning_get(k) for k in knobs}
+    try:
+        for k, v in knobs.items():
+            capi.tuning_set(k, v)
+        g = W.random_layers(n, layers, seed=seed, mixed=True)
+        init = random_state(n, seed)
+        s0 = capi.jit_stats()
+        got = _apply(n, init, g)
+        s1 = capi.jit_stats()
+        assert not s1["failed"] and s1["launches"] > s0["launches"]
+        assert np.abs(got - port.apply(n, init, g)).max() < 1e-12
+        capi.tuning_set("jit_tma", 0)
+        ref = _apply(n, init, g)
+        assert np.abs(got - ref).max() < 1e-13
+    finally:
+        for k, v in old.items():
+            capi.tuning_set(k, v)
+
+
+def test_tma_blocks_at_26_qubits(jit):
+    """The bench circuit family at 26 qubits (1 GiB): TMA blocks equal the
+    classic compiled blocks."""
+    n = 26
+    g = W.random_layers(n, 4, seed=84, mixed=True)
+    old = capi.tuning_get("jit_tma")
+    try:
+        capi.tuning_set("jit_tma", 1)
+        a = _apply(n, basis(n), g)
+        capi.tuning_set("jit_tma", 0)
+        b = _apply(n, basis(n), g)
+    finally:
+        capi.tuning_set("jit_tma", old)
+    assert np.abs(a - b).max() < 1e-13

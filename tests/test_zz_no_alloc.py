@@ -86,13 +86,28 @@ def test_noalloc_on_a_caller_stream(engine):
 
 
 _ALLOC_PROBE = textwrap.dedent(r"""
-    import ctypes as C, json, sys
+    import ctypes as C, glob, json, os, sys
     import numpy as np
-    import torch
     sys.path.insert(0, sys.argv[1])
     from kettle_b200 import capi
     from kettle_b200 import workloads as W
-    torch.cuda.init()
+    # the CUDA runtime as a shared library, for cudaMemGetInfo on the same
+    # (primary) context the engine uses; torch is not loaded
+    cands = glob.glob(os.path.join(sys.prefix, "lib", "python3*", "site-packages", "nvidia", "cuda_runtime", "lib",
+                                   "libcudart.so.*")) + ["/usr/local/cuda/lib64/libcudart.so.12", "libcudart.so.12"]
+    rt = None
+    for c in cands:
+        try:
+            rt = C.CDLL(c)
+            break
+        except OSError:
+            continue
+    assert rt is not None, "no CUDA runtime library"
+    def free_bytes():
+        assert rt.cudaDeviceSynchronize() == 0
+        f, t = C.c_size_t(), C.c_size_t()
+        assert rt.cudaMemGetInfo(C.byref(f), C.byref(t)) == 0
+        return f.value
     n = 20
     sv = capi.Statevector(n)
     sv.set_basis(3)
@@ -104,23 +119,21 @@ _ALLOC_PROBE = textwrap.dedent(r"""
     c = np.ascontiguousarray(coeffs, dtype=np.complex128)
     terms = np.empty(s.size, dtype=np.complex128)
     total = np.empty(1, dtype=np.complex128)
-    torch.cuda.synchronize()
-    free = [torch.cuda.mem_get_info()[0]]
+    free = [free_bytes()]
     for _ in range(2):
         capi.check(capi.lib().kt_sv_expect_noalloc(ptr, nq.value, dt.value, capi.ptr(s), s.size, capi.ptr(c),
                                                    capi.ptr(terms), capi.ptr(total), None))
-        torch.cuda.synchronize()
-        free.append(torch.cuda.mem_get_info()[0])
+        free.append(free_bytes())
     sv.expect(many, many_c)  # the allocating path grows the handle's scratch (~5.7 MB)
-    torch.cuda.synchronize()
-    free.append(torch.cuda.mem_get_info()[0])
+    free.append(free_bytes())
     print(json.dumps(free))
 """)
 
 
 def test_noalloc_allocates_no_device_memory(engine):
     """In a fresh process whose modules load eagerly (so the library's fixed
-    array is in place before anything is measured), the free device memory is
+    array is in place before anything is measured; torch is not imported, so
+    only the engine and the CUDA runtime load), the free device memory is
     the same before and after the first and second call; the allocating
     kt_sv_expect afterwards lowers it, which shows the measurement sees an
     allocation of this size."""
