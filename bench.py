@@ -108,11 +108,11 @@ def dist_setup(n_gpus: int):
 
 
 def reference_gate_sample(gates, k):
-    """A representative bounded sample: first one-qubit gate, first CX, first controlled rotation,
+    """A representative bounded sample: first one-qubit rotation, first CX, first controlled rotation,
     then further gates in circuit order until k are taken."""
     from kettle_b200.capi import OP
     picks = []
-    for want in ({OP["H"], OP["RX"], OP["RY"], OP["RZ"], OP["U"]}, {OP["CX"]}, {OP["CRX"], OP["CRY"], OP["CRZ"], OP["CP"]}):
+    for want in ({OP["RX"], OP["RY"], OP["RZ"]}, {OP["CX"]}, {OP["CRX"], OP["CRY"], OP["CRZ"], OP["CP"]}):
         for i, g in enumerate(gates):
             if int(g["op"]) in want and i not in picks:
                 picks.append(i)
@@ -125,24 +125,63 @@ def reference_gate_sample(gates, k):
     return gates[sorted(picks[:k])]
 
 
-def cpu_baseline(n, gates, per_layer, sample_gates=3):
-    """The reference's CPU path (oracle/_ref: ket::simulate, 1 thread) on a bounded sample."""
+def host_cpu():
+    """The host's logical CPU count and model (the CPU baseline's machine)."""
+    model = None
+    try:
+        for line in pathlib.Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
+
+
+def gate_classes(gates):
+    """Counts of the three gate classes of the circuit: one-qubit, CX, controlled rotation."""
+    from kettle_b200.capi import OP
+    one = {OP[x] for x in ("H", "RX", "RY", "RZ", "U")}
+    ops = gates["op"].astype(int)
+    return {"one_qubit": int(np.isin(ops, list(one)).sum()), "cx": int((ops == OP["CX"]).sum()),
+            "controlled": int(np.isin(ops, [OP[x] for x in ("CRX", "CRY", "CRZ", "CP")]).sum())}
+
+
+def cpu_baseline(n, gates, layers):
+    """The reference's CPU path (oracle/_ref: ket::simulate, 1 thread, as kettle
+    has no threaded path) on a bounded sample: one gate of each class (the first
+    one-qubit rotation, the first CX, the first controlled rotation) timed
+    alone, combined with the circuit's own class counts per layer."""
+    from kettle_b200.capi import OP
     from oracle.oracle import port, ref, ref_available
-    sample = reference_gate_sample(gates, sample_gates)
+    ops = gates["op"].astype(int)
+    picks = {"one_qubit": int(np.flatnonzero(np.isin(ops, [OP["RX"], OP["RY"], OP["RZ"]]))[0]),
+             "cx": int(np.flatnonzero(ops == OP["CX"])[0]),
+             "controlled": int(np.flatnonzero(np.isin(ops, [OP[x] for x in ("CRX", "CRY", "CRZ", "CP")]))[0])}
+    times = {}
     if ref_available():
-        t = ref().time_sv(n, sample)
+        held = ref().held_state(n)
+        for k, i in picks.items():
+            times[k] = held.time(gates[i:i + 1])
+        held.close()
         kind = "reference"
     else:
         st = np.zeros(1 << n, dtype=np.complex128)
         st[0] = 1.0
-        t0 = time.perf_counter()
-        port().apply(n, st, sample)
-        t = time.perf_counter() - t0
+        for k, i in picks.items():
+            t0 = time.perf_counter()
+            port().apply(n, st, gates[i:i + 1])
+            times[k] = time.perf_counter() - t0
         kind = "port"
-    layers = len(sample) / per_layer
-    return {"value": layers / t, "unit": "layers/s", "cores": 1, "kind": kind,
-            "sample": f"{len(sample)} of the {len(gates)} gates (a one-qubit gate, a CX, a controlled rotation) "
-                      f"at {n} qubits, ket::simulate timed alone ({t:.2f} s); layers = gates / {per_layer:.1f}"}
+    counts = gate_classes(gates)
+    per_layer = {k: counts[k] / layers for k in counts}
+    t_layer = sum(per_layer[k] * times[k] for k in times)
+    return {"value": 1.0 / t_layer, "unit": "layers/s", "cores": 1, "kind": kind, "host": host_cpu(),
+            "sample": f"one gate per class at {n} qubits, ket::simulate timed alone "
+                      f"(one-qubit rotation {times['one_qubit']:.2f} s, CX {times['cx']:.2f} s, controlled "
+                      f"rotation {times['controlled']:.2f} s), weighted by the circuit's "
+                      f"{per_layer['one_qubit']:g} : {per_layer['cx']:g} : {per_layer['controlled']:g} per layer",
+            "seconds_per_gate": times}
 
 
 def adjoint_bench(stream, n=24, layers=8, ps_params=24, reps=3, cpu_ref=True):
@@ -396,7 +435,27 @@ def config_legs(stream, cpu=True):
     from kettle_b200 import workloads as W
 
     out = {}
-    # ---- config 1
+    peak, peak_kind = hbm_peak()
+    # ---- config 1 (a 16 MiB state: its sweeps run from L2, so their bandwidth is
+    # set against an L2-resident copy measured here: 16 MiB -> 16 MiB, best of 20)
+    a_l2 = torch.empty(1 << 21, dtype=torch.float64, device="cuda")
+    b_l2 = torch.empty_like(a_l2)
+    best = None
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            b_l2.copy_(a_l2)
+        for _ in range(20):
+            c0 = torch.cuda.Event(enable_timing=True)
+            c1 = torch.cuda.Event(enable_timing=True)
+            c0.record(stream)
+            for _ in range(10):
+                b_l2.copy_(a_l2)
+            c1.record(stream)
+            c1.synchronize()
+            t = c0.elapsed_time(c1) / 10 / 1e3
+            best = t if best is None else min(best, t)
+    l2_copy_gbs = 2 * a_l2.numel() * 8 / best / 1e9
+    del a_l2, b_l2
     n = 20
     gates = W.random_layers(n, 100, seed=SEED, mixed=False)
     strings, coeffs = W.random_paulis(n, 200, seed=SEED)
@@ -412,8 +471,20 @@ def config_legs(stream, cpu=True):
 
     pipeline()
     t1, (tot, idx) = _timed(stream, pipeline, reps=3)
+
+    def apply_only():
+        sv.set_basis(0)
+        sv.apply(gates)
+
+    ta, _ = _timed(stream, apply_only, reps=3)
+    _, alg = sv.apply_stats()
+    alg += 16.0 * (1 << n)
     c1 = {"qubits": n, "layers": 100, "gates": int(gates.size), "strings": 200, "shots": 4096,
-          "seconds": t1, "layers_per_s": 100 / t1, "expectation": tot.real}
+          "seconds": t1, "layers_per_s": 100 / t1, "expectation": tot.real,
+          "roofline": {"bound": "l2", "kernel": "gate sweeps of the 100 layers (the state stays in L2)",
+                       "seconds": ta, "alg_bytes": alg, "achieved": alg / ta / 1e9,
+                       "peak": l2_copy_gbs, "unit": "GB/s", "frac": alg / ta / 1e9 / l2_copy_gbs,
+                       "peak_source": "L2-resident device copy (16 MiB -> 16 MiB) measured in this run"}}
     if cpu:
         from oracle.oracle import ref, ref_available
         if ref_available():
@@ -458,8 +529,19 @@ def config_legs(stream, cpu=True):
 
     dm_pipeline()
     t2, tot = _timed(stream, dm_pipeline, reps=2)
+
+    def dm_apply_only():
+        dm.set_basis(0)
+        dm.apply(gates)
+
+    tda, _ = _timed(stream, dm_apply_only, reps=2)
+    launches, dm_alg = dm.apply_stats()
     out["config2b"] = {"qubits": n, "entries": 1 << (2 * n), "layers": 100, "gates": int(gates.size), "strings": 200,
                        "seconds": t2, "layers_per_s": 100 / t2, "expectation": tot.real, "trace": dm.trace().real}
+    if dm_alg:
+        out["config2b"]["roofline"] = {"bound": "hbm", "kernel": f"{launches} fused passes over the 1 GiB density matrix",
+                                       "seconds": tda, "alg_bytes": dm_alg, "achieved": dm_alg / tda / 1e9,
+                                       "peak": peak, "unit": "GB/s", "frac": dm_alg / tda / 1e9 / peak}
     dm.close()
     if cpu:
         from oracle.oracle import ref, ref_available
@@ -485,10 +567,34 @@ def config_legs(stream, cpu=True):
         sv.apply(gates)
         return sv.norm_sq(), sv.expect(strings, coeffs)[1]
 
-    t3, (nrm, tot) = _timed(stream, c64_pipeline, reps=1)
+    # warm-up: the circuit's block kernels compiled (as a repeated workload has
+    # them) and one untimed run; then two timed runs
+    try:
+        sv.prepare(gates)
+    except capi.KettleError:
+        pass
+    c64_pipeline()
+    t3, (nrm, tot) = _timed(stream, c64_pipeline, reps=2)
+
+    def c64_apply():
+        sv.set_basis(0)
+        sv.apply(gates)
+
+    t3a, _ = _timed(stream, c64_apply, reps=1)
+    _, alg3 = sv.apply_stats()
+    t3e, _ = _timed(stream, lambda: sv.expect(strings, coeffs), reps=1)
+    masks = np.unique(strings["x"]).size
+    pauli_bytes = float(masks) * 8.0 * (1 << n)
     out["config3"] = {"qubits": n, "dtype": "c64 (FP64 norm and expectation)", "layers": 40, "gates": int(gates.size),
                       "strings": 500, "seconds": t3, "layers_per_s": 40 / t3, "norm_drift": abs(nrm - 1.0),
-                      "expectation": tot.real}
+                      "expectation": tot.real, "timing": "2 runs after a warm-up run (block kernels compiled)",
+                      "roofline": {
+                          "gates": {"bound": "hbm", "seconds": t3a, "alg_bytes": alg3, "achieved": alg3 / t3a / 1e9,
+                                    "peak": peak, "unit": "GB/s", "frac": alg3 / t3a / 1e9 / peak},
+                          "pauli": {"bound": "hbm", "seconds": t3e, "distinct_x_masks": int(masks),
+                                    "alg_bytes": pauli_bytes, "achieved": pauli_bytes / t3e / 1e9, "peak": peak,
+                                    "unit": "GB/s", "frac": pauli_bytes / t3e / 1e9 / peak,
+                                    "note": "one read of the state per distinct X/Y mask"}}}
     sv.close()
     # 30 q complex64 against complex128
     n = 30
@@ -526,6 +632,15 @@ def run_reference(args):
     gates = W.random_layers(n, layers, seed=SEED, mixed=True)
     per_layer = len(gates) / layers
     sample = reference_gate_sample(gates, max(1, args.ref_gates))
+    # the sample's classes weighted by the circuit's own mix: each class's mean
+    # time times its gates per layer
+    from kettle_b200.capi import OP
+    cls_of = {}
+    for k, g in enumerate(sample):
+        o = int(g["op"])
+        cls_of[k] = ("cx" if o == OP["CX"] else "controlled" if o in (OP["CRX"], OP["CRY"], OP["CRZ"], OP["CP"])
+                     else "one_qubit")
+    counts = gate_classes(gates)
     if ref_available():
         held = ref().held_state(n)
         timer = held.time
@@ -543,7 +658,13 @@ def run_reference(args):
         timer(sample[w % len(sample): w % len(sample) + 1])
     ts = [timer(sample[s % len(sample): s % len(sample) + 1]) for s in range(args.steps)]
     per_step = float(np.mean(ts))
-    value = (1.0 / per_layer) / per_step
+    by_cls = {}
+    for s, t in enumerate(ts):
+        by_cls.setdefault(cls_of[s % len(sample)], []).append(t)
+    mean_cls = {k: float(np.mean(v)) for k, v in by_cls.items()}
+    fill = float(np.mean(ts))
+    t_layer = sum(counts[k] / layers * mean_cls.get(k, fill) for k in counts)
+    value = 1.0 / t_layer
     line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "layers/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -551,9 +672,11 @@ def run_reference(args):
                                    "(1q from H/RX/RY/RZ/U, CX brickwork, n/2 CRX/CRY/CRZ/CP)",
                        "qubits": n, "layers": layers, "gates": int(len(gates)), "seed": SEED,
                        "step": "one gate of the circuit per step (bounded sample), layers = gates / gates-per-layer"},
-            "cpu_baseline": {"value": value, "unit": "layers/s", "cores": 1, "kind": kind,
-                             "sample": f"one gate per step from a {len(sample)}-gate sample at {n} qubits, "
-                                       "ket::simulate single-threaded (the reference has no threaded path)"},
+            "cpu_baseline": {"value": value, "unit": "layers/s", "cores": 1, "kind": kind, "host": host_cpu(),
+                             "sample": f"one gate per step from a {len(sample)}-gate sample at {n} qubits (a "
+                                       "one-qubit gate, a CX, a controlled rotation), ket::simulate "
+                                       "single-threaded (the reference has no threaded path); each class's mean "
+                                       "time weighted by the circuit's gates of that class per layer"},
             "e2e": {"value": value, "unit": "layers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -644,6 +767,16 @@ def run_engine(args):
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
+    # sampling alone on the final state: 4096 shots, probabilities + CDF + searches
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(3):
+        sv.sample(canon)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    sample_s = s0.elapsed_time(s1) / 3 / 1e3
+    sample_bytes = 16.0 * (1 << n) + 2 * 8.0 * (1 << n)
 
     traffic = None
     tf = ROOT / "profiles" / "roofline_traffic.json"
@@ -680,6 +813,10 @@ def run_engine(args):
                     "h2d_bytes_per_step": int(gates.nbytes + canon.nbytes), "d2h_bytes_per_step": 4096 * 8,
                     "path": "kt_sv_set_basis + kt_sv_apply(host gate records) + kt_sv_sample(4096 host uniforms)"},
             "gpu_launches": int((launches + 1) * args.steps),
+            "sampling": {"shots": 4096, "seconds": sample_s, "alg_bytes": sample_bytes,
+                         "achieved": sample_bytes / sample_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": sample_bytes / sample_s / 1e9 / peak,
+                         "alg_bytes_rule": "16 B x 2^n amplitudes read + 2 x 8 B x 2^n CDF written and read"},
             "clocks": clk.summary()}
     sv.close()
     if not args.no_adjoint:
@@ -693,7 +830,7 @@ def run_engine(args):
         line["configs"] = config_legs(stream, cpu=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(n, gates, per_layer)
+            line["cpu_baseline"] = cpu_baseline(n, gates, layers)
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(exc)}
     if rank == 0:

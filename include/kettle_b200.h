@@ -206,6 +206,18 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               one unscaled uncontrolled gate of the block (or
  *                               every amplitude before the store); below 1e-150 the
  *                               apply runs on the precompiled kernels
+ *   jit_tma            0 or 1   (0) complex128 compiled blocks (no renormalisation) as
+ *                               persistent kernels of one CTA per SM: a producer
+ *                               warp moves every tile between HBM and shared
+ *                               memory with tensor copies (cp.async.bulk.tensor,
+ *                               128-byte swizzle, mbarrier completion, bulk-group
+ *                               stores), jit_tma_stages tile buffers in flight, and
+ *                               jit_tma_groups thread groups compute one tile each;
+ *                               a bounded wait that runs out makes the next C call
+ *                               return KT_ERR_TIMEOUT
+ *   jit_tma_groups     1 or 2   (1) tiles computed at once per CTA (see jit_tma)
+ *   jit_tma_stages     2..6     (3) tile buffers per CTA (at least groups + 1; the
+ *                               kernel must fit 227 KB of shared memory)
  *   batch_spin_limit   1..1e12  (33554432) polls of an empty job queue after which a
  *                               CTA of a batch's persistent kernel gives up (about
  *                               10 s): the evaluation then stops and
@@ -401,6 +413,8 @@ int32_t kt_dm_partial_trace(kt_dm src, const int32_t* qubits, int32_t n_traced, 
 int32_t kt_dm_tensor_product(kt_dm left, kt_dm right, kt_dm dst);
 /* Tr(rho^2), FP64: ket::DensityMatrix::trace_of_square (state/density_matrix.hpp:98-104). */
 int32_t kt_dm_trace_of_square(kt_dm dm, double* out_re_im);
+/* kt_sv_apply_stats for a density matrix's most recent kt_dm_apply (instrumentation). */
+int32_t kt_dm_apply_stats(kt_dm dm, int64_t* launches, double* alg_bytes);
 /* M gate on a density matrix, split at the host coin like the statevector's:
  * P(b) = sum |rho(r, c)|^2 over the rows r and columns c whose bit `qubit` is
  * b (the reference's definition); then keep outcome o: the (o, o) block

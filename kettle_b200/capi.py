@@ -79,6 +79,12 @@ _SIGS = {
     "kt_sv_copy": ([P, P], I32),
     "kt_sv_apply": ([P, P, I64, P, I64, I32], I32),
     "kt_sv_apply_stats": ([P, C.POINTER(I64), DP], I32),
+    "kt_dm_apply_stats": ([P, C.POINTER(I64), DP], I32),
+    "kt_sv_tensor_product": ([P, P, P], I32),
+    "kt_sv_diagonal_expectation": ([P, P, P], I32),
+    "kt_sample_probabilities": ([P, U64, P, I64, P, I32, P], I32),
+    "kt_dm_measure_probs": ([P, U32, DP, DP], I32),
+    "kt_dm_collapse": ([P, U32, I32, C.c_double], I32),
     "kt_plan_stats": ([I32, I32, P, I64, P, I64, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)], I32),
     "kt_plan_order": ([I32, I32, P, I64, P, I64, P, I64, C.POINTER(I64)], I32),
     "kt_sv_expect": ([P, P, I64, P, P, P], I32),
@@ -329,6 +335,31 @@ class Statevector:
         return complex(out[0], out[1])
 
 
+    def tensor_product(self, right: "Statevector") -> "Statevector":
+        """|self> (x) |right>, this state's qubits the low ones (kt_sv_tensor_product)."""
+        out = Statevector(self.n_qubits + right.n_qubits, self.dtype)
+        check(lib().kt_sv_tensor_product(self._h, right._h, out._h))
+        return out
+
+    def diagonal_expectation(self, eigenvalues) -> complex:
+        """sum_i conj(psi_i) lambda_i psi_i (kt_sv_diagonal_expectation)."""
+        lam = np.ascontiguousarray(eigenvalues, dtype=np.complex128)
+        if lam.size != 1 << self.n_qubits:
+            raise ValueError("one eigenvalue per basis state")
+        out = np.empty(2, dtype=np.float64)
+        check(lib().kt_sv_diagonal_expectation(self._h, ptr(lam), ptr(out)))
+        return complex(out[0], out[1])
+
+
+def sample_probabilities(probabilities, canonicals, mode: int = 0, stream: int | None = None) -> np.ndarray:
+    """Shots from a probability vector through the device sampler (kt_sample_probabilities)."""
+    p = np.ascontiguousarray(probabilities, dtype=np.float64)
+    c = np.ascontiguousarray(canonicals, dtype=np.float64)
+    out = np.empty(c.size, dtype=np.uint64)
+    check(lib().kt_sample_probabilities(ptr(p), p.size, ptr(c), c.size, ptr(out), mode, stream))
+    return out
+
+
 class DensityMatrix:
     """Device density-matrix handle (kt_dm): column-major N x N."""
 
@@ -371,6 +402,22 @@ class DensityMatrix:
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
         p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
         check(lib().kt_dm_apply(self._h, ptr(g), g.size, ptr(p), 0 if p is None else p.size, mode))
+
+    def measure_probs(self, qubit: int):
+        """P(0), P(1) of an M gate on `qubit` as the reference defines them (kt_dm_measure_probs)."""
+        p0 = C.c_double()
+        p1 = C.c_double()
+        check(lib().kt_dm_measure_probs(self._h, qubit, C.byref(p0), C.byref(p1)))
+        return p0.value, p1.value
+
+    def collapse(self, qubit: int, outcome: int, scale: float):
+        check(lib().kt_dm_collapse(self._h, qubit, outcome, scale))
+
+    def apply_stats(self):
+        n = I64(0)
+        b = C.c_double(0.0)
+        check(lib().kt_dm_apply_stats(self._h, C.byref(n), C.byref(b)))
+        return int(n.value), float(b.value)
 
     def expect(self, strings: np.ndarray, coeffs: np.ndarray | None = None):
         s = np.ascontiguousarray(strings, dtype=PAULI_DTYPE)

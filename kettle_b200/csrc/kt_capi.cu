@@ -427,6 +427,16 @@ int32_t kt_sv_apply_stats(kt_sv sv, int64_t* launches, double* alg_bytes)
     return KT_OK;
 }
 
+int32_t kt_dm_apply_stats(kt_dm dm, int64_t* launches, double* alg_bytes)
+{
+    if (dm == nullptr) {
+        return invalid("null handle");
+    }
+    if (launches) *launches = dm->st.last_launches;
+    if (alg_bytes) *alg_bytes = dm->st.last_alg_bytes;
+    return KT_OK;
+}
+
 int32_t kt_sv_expect(kt_sv sv, const kt_pauli* strings, int64_t n_strings, const double* coeffs, double* out_terms,
                      double* out_total)
 {

@@ -408,9 +408,9 @@ int32_t kto_canonicals_mt19937(uint32_t seed, int64_t count, double* out)
  * sum; offset = (last - last strictly smaller cdf value) * 1e-4; a draw is
  * u = canonical * (last - offset) (+ 0.0, the distribution's lower bound) and
  * the outcome is lower_bound(cdf, u). */
-int32_t kto_sample(int32_t n, const double* probs, const double* canonicals, int64_t n_shots, uint64_t* out)
+int32_t kto_sample_raw(const double* probs, uint64_t N, const double* canonicals, int64_t n_shots, uint64_t* out)
 {
-    const uint64_t N = (uint64_t)1 << n;
+    if (N == 0) return -1;
     double* cdf = (double*)malloc(N * sizeof(double));
     if (!cdf) return -1;
     double acc = 0.0;
@@ -438,6 +438,12 @@ int32_t kto_sample(int32_t n, const double* probs, const double* canonicals, int
     }
     free(cdf);
     return 0;
+}
+
+/* the same on a state's 2^n probabilities */
+int32_t kto_sample(int32_t n, const double* probs, const double* canonicals, int64_t n_shots, uint64_t* out)
+{
+    return kto_sample_raw(probs, (uint64_t)1 << n, canonicals, n_shots, out);
 }
 
 /* ---------------------------------------------------------------------------

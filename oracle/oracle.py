@@ -58,6 +58,8 @@ class Port:
         L.kto_canonicals_mt19937.restype = I32
         L.kto_sample.argtypes = [I32, P, P, I64, P]
         L.kto_sample.restype = I32
+        L.kto_sample_raw.argtypes = [P, U64, P, I64, P]
+        L.kto_sample_raw.restype = I32
         L.kto_measure.argtypes = [I32, P, U32, C.c_double, C.POINTER(I32), C.POINTER(C.c_double),
                                   C.POINTER(C.c_double)]
         L.kto_measure.restype = I32
@@ -122,6 +124,15 @@ class Port:
         out = np.empty(c.size, dtype=np.uint64)
         rc = self.L.kto_sample(n, _p(pr), _p(c), c.size, _p(out))
         if rc != 0:
+            raise ValueError("oracle sampling failed")
+        return out
+
+    def sample_raw(self, probs, canonicals):
+        """Sampling from any probability vector (the std::vector<double> overloads)."""
+        pr = np.ascontiguousarray(probs, dtype=np.float64)
+        c = np.ascontiguousarray(canonicals, dtype=np.float64)
+        out = np.empty(c.size, dtype=np.uint64)
+        if self.L.kto_sample_raw(_p(pr), pr.size, _p(c), c.size, _p(out)) != 0:
             raise ValueError("oracle sampling failed")
         return out
 
@@ -219,6 +230,8 @@ class Ref:
         L.ref_random_unitary.restype = I32
         L.ref_random_unitaries.argtypes = [I32, I64, P]
         L.ref_random_unitaries.restype = I32
+        L.ref_sample_probabilities.argtypes = [P, I64, I64, I64, P]
+        L.ref_sample_probabilities.restype = I32
         L.ref_time_sv.argtypes = [I32, P, I64, P, C.POINTER(C.c_double)]
         L.ref_time_sv.restype = I32
         L.ref_sv_alloc.argtypes = [I32]
@@ -369,6 +382,12 @@ class Ref:
         u = np.empty(8, dtype=np.float64)
         self._chk(self.L.ref_random_unitary(seed, _p(u)))
         return np.array([[u[0] + 1j * u[1], u[2] + 1j * u[3]], [u[4] + 1j * u[5], u[6] + 1j * u[7]]])
+
+    def sample_probabilities(self, probs, n_shots, seed):
+        p = np.ascontiguousarray(probs, dtype=np.float64)
+        out = np.empty(n_shots, dtype=np.uint64)
+        self._chk(self.L.ref_sample_probabilities(_p(p), p.size, n_shots, seed, _p(out)))
+        return out
 
     def random_unitaries(self, seed, count):
         """`count` matrices of generate_random_unitary2x2 on one std::mt19937(seed) stream."""

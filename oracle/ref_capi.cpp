@@ -463,6 +463,19 @@ int32_t ref_random_unitary(int32_t seed, double* u)
     });
 }
 
+// perform_measurements_as_memory(const std::vector<double>&, n_shots, seed)
+// (calculations/measurements.cpp:73-94)
+int32_t ref_sample_probabilities(const double* probs, int64_t n, int64_t n_shots, int64_t seed, uint64_t* out)
+{
+    return guarded([&] {
+        const auto p = std::vector<double>(probs, probs + n);
+        const auto m = ket::perform_measurements_as_memory(p, static_cast<std::size_t>(n_shots), static_cast<int>(seed));
+        for (int64_t k = 0; k < n_shots; ++k) {
+            out[k] = m[static_cast<std::size_t>(k)];
+        }
+    });
+}
+
 // `count` matrices from one std::mt19937(seed) stream, one
 // generate_random_unitary2x2(std::mt19937&) call after another
 // (gates/random_u_gates.cpp:13-36); 8 doubles per matrix

@@ -483,3 +483,62 @@ def test_permutation_folding(engine, port, n):
     sv = capi.Statevector(n, capi.KT_C64)
     sv.apply(g)
     assert np.abs(sv.download() - want).max() < 1e-4
+
+
+def test_statevector_tensor_product_and_diagonal_expectation(engine, port):
+    """kt_sv_tensor_product (state/state.cpp:144-157: left qubits low) and
+    kt_sv_diagonal_expectation (state/state.cpp:174-188) against numpy."""
+    nl, nr = 7, 6
+    a = random_state(nl, 1)
+    b = random_state(nr, 2)
+    L = capi.Statevector(nl)
+    R = capi.Statevector(nr)
+    L.upload(a)
+    R.upload(b)
+    out = L.tensor_product(R)
+    want = np.kron(b, a)  # index i_l + i_r 2^nl
+    assert np.abs(out.download() - want).max() < 1e-15
+    lam = np.random.default_rng(3).standard_normal(1 << (nl + nr)) + 1j * np.random.default_rng(4).standard_normal(1 << (nl + nr))
+    got = out.diagonal_expectation(lam)
+    assert abs(got - np.sum(np.conj(want) * lam * want)) < 1e-12
+    for h in (L, R, out):
+        h.close()
+
+
+def test_sampling_from_a_probability_vector(engine, port):
+    """kt_sample_probabilities: the sampler of kt_sv_sample on a caller's vector,
+    bit-exact with the oracle's sequential CDF and lower_bound, also for a
+    length that is not a power of two."""
+    rng = np.random.default_rng(9)
+    for size in (3, 1000, 1 << 14):
+        p = rng.random(size) ** 3
+        p /= p.sum()
+        can = port.canonicals(11, 2048)
+        got = capi.sample_probabilities(p, can)
+        assert np.array_equal(got, port.sample_raw(p, can)), size
+
+
+def test_density_matrix_measurement(engine, port):
+    """M on a density matrix (measure_density_matrix.cpp:22-105): P(b) is the
+    sum of |rho(r, c)|^2 over rows and columns with bit b; the outcome's block
+    is kept and scaled, the other three cleared."""
+    n = 5
+    g = W.random_layers(n, 3, seed=12, mixed=True)
+    dm = capi.DensityMatrix(n)
+    dm.apply(g)
+    rho = dm.download()
+    for q in range(n):
+        bits = (np.arange(1 << n) >> q) & 1
+        same0 = np.outer(bits == 0, bits == 0)
+        same1 = np.outer(bits == 1, bits == 1)
+        p0, p1 = dm.measure_probs(q)
+        assert abs(p0 - np.sum(np.abs(rho[same0]) ** 2)) < 1e-13
+        assert abs(p1 - np.sum(np.abs(rho[same1]) ** 2)) < 1e-13
+    q, o = 2, 1
+    p0, p1 = dm.measure_probs(q)
+    s = np.sqrt(1.0 / p1)
+    dm.collapse(q, o, s)
+    bits = (np.arange(1 << n) >> q) & 1
+    want = np.where(np.outer(bits == o, bits == o), rho * s, 0.0)
+    assert np.abs(dm.download() - want).max() < 1e-14
+    dm.close()

@@ -287,3 +287,19 @@ def test_random_unitaries_live_reference(ref):
         got = W.random_unitaries(seed, 40)
         want = ref.random_unitaries(seed, 40)
         assert all(np.array_equal(a, b) for a, b in zip(got, want)), seed
+
+
+def test_sampling_from_probability_vectors(port, ref):
+    """The oracle's sampler on any probability vector (the std::vector<double>
+    overloads of perform_measurements_as_*) against the reference's own,
+    including lengths that are not powers of two and zero entries."""
+    rng = np.random.default_rng(5)
+    for size in (1, 2, 3, 7, 100, 4096):
+        p = rng.random(size) ** 2
+        p[rng.random(size) < 0.2] = 0.0
+        if p.sum() == 0.0:
+            p[0] = 1.0
+        for seed in (0, 77):
+            want = ref.sample_probabilities(p, 300, seed)
+            got = port.sample_raw(p, port.canonicals(seed, 300))
+            assert np.array_equal(got, want), (size, seed)
