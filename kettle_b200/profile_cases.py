@@ -1,0 +1,192 @@
+"""Small, self-contained workloads that run one family of the engine's kernels
+a few times, for profiling them one at a time (for example under Nsight
+Compute with a kernel-name filter and a launch count):
+
+    python -m kettle_b200.profile_cases <case> [--qubits N] [--reps R]
+
+Every case first runs its operation once (warm-up: plans, compiled kernels,
+scratch buffers), then `reps` more times, so a profiler can skip the first
+launch of the kernel it captures.  The states are sized past the 126 MB L2
+(1 GiB by default) so DRAM figures mean something, and stay a few GB at most.
+
+Cases and the kernels they run:
+  pauli        k_pauli, k_pauli_finalize          (kt_sv_expect, 32 strings)
+  sample       k_probs, k_tile_*, k_exact_chain, k_last_below, k_seq_*  (kt_sv_sample, exact tier)
+  sample_fast  k_probs, k_chunk_sums, k_chunk_offsets, k_sample_bound, k_sample_fast  (2^22 amplitudes)
+  dm_pauli     k_dm_pauli, k_dm_pauli_finalize    (kt_dm_expect on a 13-qubit density matrix)
+  hpsi         k_hsum                              (lambda = H psi of the adjoint forward pass)
+  adjoint      k_fused_adj, k_adj_rows             (fused adjoint backward blocks)
+  dm_ops       k_partial_trace, k_tensor_product, k_trace_square
+  norm         k_fused_norm or compiled blocks, k_norm_final  (complex64 renormalising apply)
+  blocks       kt_jb* (run-time compiled blocks of the benchmark circuit family)
+  fused        k_fused (the precompiled fused-block interpreter)
+  sweep        k_sweep (one pass per gate)
+  state_ops    k_sv_tensor_product, k_sv_diag_expect, k_dm_block_norms, k_dm_collapse
+  batch        k_batch_persist, k_batch_small, k_batch_patch
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+
+import numpy as np
+
+from . import capi
+from . import workloads as W
+
+
+def _random_state(n, seed, dtype=capi.KT_C128):
+    sv = capi.Statevector(n, dtype)
+    sv.set_basis(0)
+    sv.apply(W.random_layers(n, 1, seed=seed, mixed=True))
+    return sv
+
+
+def case_pauli(n, reps):
+    sv = _random_state(n, 1)
+    strings, coeffs = W.random_paulis(n, 32, seed=2)
+    for _ in range(1 + reps):
+        sv.expect(strings, coeffs)
+    sv.close()
+
+
+def case_sample(n, reps):
+    sv = _random_state(n, 3)
+    can = capi.canonicals_mt19937(4, 4096)
+    for _ in range(1 + reps):
+        sv.sample(can)
+    sv.close()
+
+
+def case_sample_fast(n, reps):
+    case_sample(min(n, 22), reps)
+
+
+def case_dm_pauli(n, reps):
+    m = max(2, n // 2)
+    dm = capi.DensityMatrix(m)
+    dm.apply(W.random_layers(m, 2, seed=5, mixed=True))
+    strings, coeffs = W.random_paulis(m, 32, seed=6)
+    for _ in range(1 + reps):
+        dm.expect(strings, coeffs)
+    dm.close()
+
+
+def case_hpsi(n, reps):
+    gates, params = W.hea(n, 1, seed=7)
+    strings, coeffs = W.xxz_chain(n, seed=7)
+    sv = capi.Statevector(n)
+    adj = capi.Adjoint(sv)
+    for _ in range(1 + reps):
+        sv.set_basis(0)
+        adj.forward(gates, params, strings, coeffs)
+    adj.close()
+    sv.close()
+
+
+def case_adjoint(n, reps):
+    gates, params = W.hea(n, 2, seed=8)
+    strings, coeffs = W.xxz_chain(n, seed=8)
+    sv = capi.Statevector(n)
+    adj = capi.Adjoint(sv)
+    for _ in range(1 + reps):
+        sv.set_basis(0)
+        adj.forward(gates, params, strings, coeffs)
+        adj.backward()
+    adj.close()
+    sv.close()
+
+
+def case_dm_ops(n, reps):
+    m = max(2, n // 2)
+    dm = capi.DensityMatrix(m)
+    dm.apply(W.random_layers(m, 2, seed=9, mixed=True))
+    left = capi.DensityMatrix(m // 2)
+    right = capi.DensityMatrix(m - m // 2)
+    for _ in range(1 + reps):
+        dm.partial_trace([0]).close()
+        left.tensor_product(right).close()
+        dm.trace_of_square()
+    for h in (dm, left, right):
+        h.close()
+
+
+def case_norm(n, reps):
+    g = W.random_layers(n, 2, seed=10, mixed=True)
+    sv = capi.Statevector(n, capi.KT_C64)
+    for _ in range(1 + reps):
+        sv.set_basis(0)
+        sv.apply(g)
+    sv.close()
+
+
+def case_blocks(n, reps):
+    g = W.random_layers(n, 2, seed=2024, mixed=True)
+    sv = capi.Statevector(n)
+    sv.prepare(g)
+    for _ in range(1 + reps):
+        sv.set_basis(0)
+        sv.apply(g)
+    sv.close()
+
+
+def case_fused(n, reps):
+    old = capi.tuning_get("fused_jit")
+    capi.tuning_set("fused_jit", 0)
+    try:
+        case_blocks(n, reps)
+    finally:
+        capi.tuning_set("fused_jit", old)
+
+
+def case_sweep(n, reps):
+    g = W.random_layers(n, 1, seed=11, mixed=True)[: 2 * n]
+    sv = capi.Statevector(n)
+    for _ in range(1 + reps):
+        sv.set_basis(0)
+        sv.apply(g, mode=capi.KT_APPLY_PER_GATE)
+    sv.close()
+
+
+def case_state_ops(n, reps):
+    a = _random_state(n // 2, 12)
+    b = _random_state(n - n // 2, 13)
+    lam = np.linspace(-1.0, 1.0, 1 << n).astype(np.complex128)
+    m = max(2, n // 2)
+    dm = capi.DensityMatrix(m)
+    dm.apply(W.random_layers(m, 1, seed=14, mixed=True))
+    for _ in range(1 + reps):
+        out = a.tensor_product(b)
+        out.diagonal_expectation(lam)
+        out.close()
+        dm.measure_probs(1)
+    dm.collapse(1, 0, 1.0)
+    for h in (a, b, dm):
+        h.close()
+
+
+def case_batch(n, reps):
+    circuits, params = W.hea_batch(64, seed=15, qubits=(10, min(n, 20)), layers=(2, 6), n_strings=20)
+    items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
+    b = capi.Batch(items, gates, strings, coeffs, n_params)
+    for _ in range(1 + reps):
+        b.evaluate(params)
+    b.close()
+
+
+CASES = {k[5:]: v for k, v in globals().items() if k.startswith("case_")}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("case", choices=sorted(CASES))
+    ap.add_argument("--qubits", type=int, default=26, help="state size (density matrices use half)")
+    ap.add_argument("--reps", type=int, default=2, help="runs after the warm-up run")
+    args = ap.parse_args(argv)
+    CASES[args.case](args.qubits, args.reps)
+    print(f"profile case {args.case} done ({args.qubits} qubits, 1 + {args.reps} runs)")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
