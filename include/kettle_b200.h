@@ -206,18 +206,22 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               one unscaled uncontrolled gate of the block (or
  *                               every amplitude before the store); below 1e-150 the
  *                               apply runs on the precompiled kernels
+ *   adjoint_jit        0, 1, 2  (2) fused adjoint blocks as kernels compiled at run
+ *                               time (NVRTC: gradient terms and U^dagger bodies as
+ *                               straight-line code): 0 never, 1 always, 2 from the
+ *                               second backward sweep of a circuit structure;
+ *                               adjoint plans are cached by structure
  *   jit_tma            0 or 1   (0) complex128 compiled blocks (no renormalisation) as
  *                               persistent kernels of one CTA per SM: a producer
  *                               warp moves every tile between HBM and shared
  *                               memory with tensor copies (cp.async.bulk.tensor,
  *                               128-byte swizzle, mbarrier completion, bulk-group
- *                               stores), jit_tma_stages tile buffers in flight, and
- *                               jit_tma_groups thread groups compute one tile each;
- *                               a bounded wait that runs out makes the next C call
- *                               return KT_ERR_TIMEOUT
- *   jit_tma_groups     1 or 2   (1) tiles computed at once per CTA (see jit_tma)
- *   jit_tma_stages     2..6     (3) tile buffers per CTA (at least groups + 1; the
- *                               kernel must fit 227 KB of shared memory)
+ *                               stores) and jit_tma_stages tile buffers in flight,
+ *                               while one thread group computes a tile; a bounded
+ *                               wait that runs out makes the next C call return
+ *                               KT_ERR_TIMEOUT
+ *   jit_tma_stages     2..4     (3) tile buffers per CTA (the kernel must fit 227 KB
+ *                               of shared memory)
  *   batch_spin_limit   1..1e12  (33554432) polls of an empty job queue after which a
  *                               CTA of a batch's persistent kernel gives up (about
  *                               10 s): the evaluation then stops and
@@ -234,7 +238,10 @@ int32_t kt_tuning_get(const char* name, int64_t* value);
  * and 1 if run-time compilation was unavailable or failed (new). */
 int32_t kt_jit_stats(int64_t* kernels_compiled, int64_t* block_launches, int32_t* failed);
 /* Host-only: plan an apply of n_qubits in `dtype` and compile its block kernels
- * with NVRTC without loading them (no GPU needed); n_kernels = blocks compiled. */
+ * with NVRTC without loading them (no GPU needed); n_kernels = blocks compiled.
+ * With adjoint_jit = 1 it compiles instead the fused adjoint blocks of the
+ * circuit's backward sweep (gates reversed, every parameterised rotation a
+ * gradient row). */
 int32_t kt_jit_compile_only(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates,
                             const double* params, int64_t n_params, int64_t* n_kernels);
 

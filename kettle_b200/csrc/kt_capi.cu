@@ -195,6 +195,30 @@ int32_t kt_jit_compile_only(int32_t n_qubits, int32_t dtype, const kt_gate* gate
         if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, n_qubits, lg); rc != KT_OK) {
             return rc;
         }
+        if (kt::tuning().adjoint_jit == 1) {
+            // the backward sweep of the circuit read as an ansatz: the gates in
+            // reverse order (their matrices do not change the kernels), every
+            // parameterised rotation a gradient row
+            std::vector<kt::AdjGate> sweep;
+            int32_t rows = 0;
+            for (int64_t i = 0; i < n_gates; ++i) {
+                if (gates[i].param >= 0 && kt::gate_generator(gates[i].op) >= 0) {
+                    ++rows;
+                }
+            }
+            for (int64_t i = n_gates - 1; i >= 0; --i) {
+                kt::AdjGate ag {};
+                ag.adj = lg[static_cast<size_t>(i)];
+                ag.row = -1;
+                ag.gen = 0;
+                if (gates[i].param >= 0 && kt::gate_generator(gates[i].op) >= 0) {
+                    ag.gen = kt::gate_generator(gates[i].op);
+                    ag.row = --rows;
+                }
+                sweep.push_back(ag);
+            }
+            return kt::jit_adjoint_compile_only(n_qubits, dtype, sweep, n_kernels);
+        }
         return kt::jit_compile_only(n_qubits, dtype, lg, n_kernels);
     });
 }

@@ -684,6 +684,10 @@ inline uint32_t tma_swz(uint32_t l)
     return l ^ ((l >> 3) & 7u);
 }
 
+// groups: thread groups computing a tile each per CTA.  Only 1 is used: a
+// 544-thread form with two groups over three 12-qubit stage buffers failed
+// with an unspecified launch failure on the 30-qubit benchmark (its cause was
+// not found by reading the code), so it is not offered.
 struct TmaCfg
 {
     int groups {1};
@@ -1541,13 +1545,13 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
         return false;  // the caller reserved per-CTA sums for fewer CTAs
     }
     // TMA-pipelined kernels (complex128, no renormalisation): one persistent
-    // CTA per SM of jit_tma_groups tile-sized thread groups and a producer
-    // warp, jit_tma_stages tile buffers; every block's tile must have the
-    // three lowest qubits (one 128-byte row per box line)
+    // CTA per SM of one tile-sized thread group and a producer warp,
+    // jit_tma_stages tile buffers; every block's tile must have the three
+    // lowest qubits (one 128-byte row per box line)
     std::vector<TmaCfg> tma_cfg;
     if (tuning().jit_tma != 0 && std::is_same<T, double>::value && !norm && encode_tiled() != nullptr) {
-        const int groups = tuning().jit_tma_groups;
-        const int stages = std::max(tuning().jit_tma_stages, groups + 1);
+        const int groups = 1;
+        const int stages = std::max(tuning().jit_tma_stages, 2);
         const size_t tile_bytes = (size_t {1} << K) * sizeof(C);
         const size_t need = static_cast<size_t>(stages) * tile_bytes + 1024 + 16 * static_cast<size_t>(stages);
         const int tthreads = groups * threads + 32;
@@ -1888,6 +1892,275 @@ __global__ void k_adj_rows(const double* __restrict__ partial, int n_blocks, con
     grad[rows[r]] = 2.0 * s;
 }
 
+// ---------------------------------------------------------------------------
+// Run-time compiled adjoint blocks (adjoint_jit).  The k_fused_adj tile loop
+// for one block with its ops written out: every gradient term a literal
+// generator form on literal register / thread slots, every U^dagger a
+// straight-line body on psi and then on lambda, control predicates folded;
+// the matrices arrive in the constant-bank parameter M (8 entries per op).
+template <typename T>
+std::string jit_adj_body(const Plan<T, FOpA<T>>& plan, size_t b, int RB)
+{
+    const FBlock& fb = plan.blocks[b];
+    const int TB = fb.K - RB;
+    const int R = 1 << RB;
+    const int np = fb.phase_end - fb.phase_begin;
+    const int nops = std::max(1, fb.op_end - fb.op_begin);
+    const FPhase* ph = plan.phases.data() + fb.phase_begin;
+    std::vector<uint64_t> free_strides(static_cast<size_t>(std::max(1, fb.nfree)));
+    for (int k = 0; k < fb.nfree; ++k) {
+        free_strides[static_cast<size_t>(k)] = uint64_t {1} << fb.freebit[k];
+    }
+    auto reg_off = [&](const FPhase& f, int i) {
+        uint64_t o = 0;
+        for (int sl = 0; sl < RB; ++sl) {
+            if (i & (1 << sl)) {
+                o += f.rstride[sl];
+            }
+        }
+        return o;
+    };
+    auto reg_xor = [&](const uint32_t* terms, int i) {
+        uint32_t x = 0;
+        for (int sl = 0; sl < RB; ++sl) {
+            if (i & (1 << sl)) {
+                x ^= terms[sl];
+            }
+        }
+        return x;
+    };
+    auto replace_all = [](std::string str, const std::string& from, const std::string& to) {
+        for (size_t at = str.find(from); at != std::string::npos; at = str.find(from, at + to.size())) {
+            str.replace(at, from.size(), to);
+        }
+        return str;
+    };
+    std::string s;
+    s.reserve(32768);
+    s += "(void* psi_, void* lam_, unsigned long long n_tiles, double* partial, int n_rows, const __grid_constant__ $M<" +
+         std::to_string(8 * nops) + "> M)\n{\n";
+    s += "    using namespace kt;\n    using C = $C;\n";
+    s += "    constexpr int RB = " + std::to_string(RB) + ";\n";
+    s += "    C* __restrict__ psi = static_cast<C*>(psi_);\n    C* __restrict__ lam = static_cast<C*>(lam_);\n";
+    s += "    extern __shared__ __align__(16) unsigned char smem_raw[];\n";
+    s += "    C* smp = reinterpret_cast<C*>(smem_raw);\n";
+    s += "    C* sml = smp + " + std::to_string(1 << fb.K) + ";\n";
+    s += "    double* acc = reinterpret_cast<double*>(sml + " + std::to_string(1 << fb.K) + ");\n";
+    s += "    const uint32_t t_outer = threadIdx.x;\n";
+    s += "    for (int w = threadIdx.x; w < n_rows * " + std::to_string(ADJ_WARPS) + "; w += blockDim.x) {\n"
+         "        acc[w] = 0.0;\n    }\n    __syncthreads();\n";
+    s += "    for (unsigned long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {\n";
+    s += "        uint32_t t_l;\n        asm volatile(\"mov.u32 %0, %1;\" : \"=r\"(t_l) : \"r\"(t_outer));\n";
+    s += "        const uint32_t t = t_l;\n        const int lane = static_cast<int>(t & 31u);\n"
+         "        const int warp = static_cast<int>(t >> 5);\n";
+    s += "        C vp[1 << RB];\n        C vl[1 << RB];\n";
+    s += "        const uint64_t base = " + jit_deposit("tile", free_strides.data(), fb.nfree) + ";\n";
+    s += "        {\n            const uint64_t off = base + " + jit_deposit("t", ph[0].tstride, TB) + ";\n";
+    for (int i = 0; i < R; ++i) {
+        s += "            vp[" + std::to_string(i) + "] = psi[off + " + std::to_string(reg_off(ph[0], i)) + "ULL];\n";
+        s += "            vl[" + std::to_string(i) + "] = lam[off + " + std::to_string(reg_off(ph[0], i)) + "ULL];\n";
+    }
+    s += "        }\n";
+    for (int p = 0; p < np; ++p) {
+        const FPhase& cur = ph[p];
+        if (p > 0) {
+            const FPhase& prev = ph[p - 1];
+            s += "        {\n            const uint32_t so = " + jit_xor_terms(prev.tsw_out, TB, prev.xor_out) + ";\n";
+            for (int i = 0; i < R; ++i) {
+                const std::string x = std::to_string(reg_xor(prev.rsw_out, i));
+                s += "            smp[so ^ " + x + "u] = vp[" + std::to_string(i) + "];\n";
+                s += "            sml[so ^ " + x + "u] = vl[" + std::to_string(i) + "];\n";
+            }
+            s += "            __syncthreads();\n";
+            s += "            const uint32_t lo = " + jit_xor_terms(cur.tsw, TB, 0) + ";\n";
+            for (int i = 0; i < R; ++i) {
+                const std::string x = std::to_string(reg_xor(cur.rsw, i));
+                s += "            vp[" + std::to_string(i) + "] = smp[lo ^ " + x + "u];\n";
+                s += "            vl[" + std::to_string(i) + "] = sml[lo ^ " + x + "u];\n";
+            }
+            s += "            __syncthreads();\n        }\n";
+        }
+        for (int o = cur.op_begin; o < cur.op_end; ++o) {
+            const FOpA<T>& op = plan.ops[static_cast<size_t>(o)];
+            const int j = o - fb.op_begin;
+            const int cs = (op.cslot == NO_SLOT) ? -1 : op.cslot;
+            const std::string csf = cs < 0 ? "-1" : "CS_RT";
+            s += "        ";
+            if (op.cglob != 0) {
+                s += "if ((base & " + jit_hex(op.cglob) + ") == " + jit_hex(op.cglob) + ") ";
+            }
+            s += "{\n";
+            const std::string on =
+                op.cthr != 0 ? "((t & " + std::to_string(op.cthr) + "u) == " + std::to_string(op.cthr) + "u)" : "true";
+            s += "            const bool on = " + on + ";\n";
+            if (op.row >= 0) {
+                // Re <lambda| dU psi_(g-1)> from psi_g and lambda, before U^dagger touches either
+                s += "            double g = 0.0;\n            if (on) {\n                ";
+                if (op.tslot != NO_SLOT) {
+                    const char* gk = op.gen == GEN_X ? "GEN_X" : op.gen == GEN_Y ? "GEN_Y" : op.gen == GEN_Z ? "GEN_Z" : "GEN_P";
+                    s += std::string("GradRegF<$T, RB, ") + gk + "> f {vl, vp, 0.0}; f.crt = " + std::to_string(cs) +
+                         "; f.template run<" + std::to_string(op.tslot) + ", " + csf + ">(); g = " +
+                         (op.gen == GEN_P ? "" : "0.5 * ") + "f.acc;\n";
+                } else {
+                    std::string bexpr = "false";
+                    if (op.tthr != 0 && op.tglob != 0) {
+                        bexpr = "(((t & " + std::to_string(op.tthr) + "u) != 0u) || ((base & " + jit_hex(op.tglob) + ") != 0ULL))";
+                    } else if (op.tthr != 0) {
+                        bexpr = "((t & " + std::to_string(op.tthr) + "u) != 0u)";
+                    } else if (op.tglob != 0) {
+                        bexpr = "((base & " + jit_hex(op.tglob) + ") != 0ULL)";
+                    }
+                    const std::string w = op.gen == GEN_Z ? "(" + bexpr + " ? -0.5 : 0.5)" : "(" + bexpr + " ? -1.0 : 0.0)";
+                    s += "GradAllF<$T, RB> f {vl, vp, 0.0}; f.crt = " + std::to_string(cs) + "; f.template run<0, " + csf +
+                         ">(); g = " + w + " * f.acc;\n";
+                }
+                s += "            }\n";
+                s += "#pragma unroll\n            for (int s_ = 16; s_ > 0; s_ >>= 1) {\n"
+                     "                g += __shfl_down_sync(0xffffffffU, g, s_);\n            }\n";
+                s += "            if (lane == 0) {\n                acc[" + std::to_string(op.row) + " * " +
+                     std::to_string(ADJ_WARPS) + " + warp] += g;\n            }\n";
+            }
+            // U^dagger on psi, then on lambda (the forward emitter with its guards folded in here)
+            FOp<T> fo {};
+            fo.kind = op.kind;
+            fo.tslot = op.tslot;
+            fo.cslot = op.cslot;
+            fo.tthr = op.tthr;
+            fo.tglob = op.tglob;
+            for (int e = 0; e < 8; ++e) {
+                fo.m[e] = op.m[e];
+            }
+            std::string body;
+            jit_emit_op(body, fo, j, 0);
+            s += "            if (on) {\n";
+            s += replace_all(body, "{v, ", "{vp, ");
+            s += replace_all(body, "{v, ", "{vl, ");
+            s += "            }\n        }\n";
+        }
+    }
+    {
+        const FPhase& last = ph[np - 1];
+        s += "        {\n            const uint64_t off = base + " + jit_deposit("t", last.tstride, TB) + ";\n";
+        for (int i = 0; i < R; ++i) {
+            s += "            psi[off + " + std::to_string(reg_off(last, i)) + "ULL] = vp[" + std::to_string(i) + "];\n";
+            s += "            lam[off + " + std::to_string(reg_off(last, i)) + "ULL] = vl[" + std::to_string(i) + "];\n";
+        }
+        s += "        }\n";
+    }
+    s += "    }\n    __syncthreads();\n";
+    s += "    for (int r = threadIdx.x; r < n_rows; r += blockDim.x) {\n        double sum = 0.0;\n"
+         "        for (int w = 0; w < " + std::to_string(ADJ_WARPS) + "; ++w) {\n"
+         "            sum += acc[r * " + std::to_string(ADJ_WARPS) + " + w];\n        }\n"
+         "        partial[static_cast<size_t>(r) * gridDim.x + blockIdx.x] = sum;\n    }\n}\n";
+    const bool f32 = std::is_same<T, float>::value;
+    s = replace_all(s, "$T", f32 ? "float" : "double");
+    s = replace_all(s, "$C", f32 ? "float2" : "double2");
+    s = replace_all(s, "$M", f32 ? "KtMatsF" : "KtMats");
+    return s;
+}
+
+// The compiled kernels of an adjoint plan's blocks (compiling the ones not
+// cached yet); false when run-time compilation is unavailable or failed.
+template <typename T>
+bool jit_adj_kernels(const Plan<T, FOpA<T>>& plan, int RB, int smem_bytes, std::vector<const void*>& out)
+{
+    JitCache& jc = jit_cache();
+    std::lock_guard<std::mutex> lock(jc.m);
+    if (jc.failed) {
+        return false;
+    }
+    const std::string bounds = "__launch_bounds__(256, 2)";
+    const size_t nb = plan.blocks.size();
+    std::vector<std::string> keys(nb);
+    std::vector<size_t> missing;
+    std::unordered_map<std::string, size_t> first_of;
+    for (size_t b = 0; b < nb; ++b) {
+        keys[b] = bounds + jit_adj_body<T>(plan, b, RB);
+        if (jc.kernels.count(keys[b]) == 0 && first_of.count(keys[b]) == 0) {
+            first_of[keys[b]] = b;
+            missing.push_back(b);
+        }
+    }
+    if (jc.kernels.size() + missing.size() > JIT_MAX_KERNELS) {
+        return false;
+    }
+    if (!missing.empty()) {
+        const size_t workers = std::max<size_t>(1, std::min<size_t>(missing.size(), 32));
+        std::vector<std::string> sources(workers, JIT_PRELUDE);
+        std::vector<std::vector<std::string>> names(workers);
+        std::vector<std::vector<size_t>> owner(workers);
+        for (size_t i = 0; i < missing.size(); ++i) {
+            const size_t w = i % workers;
+            const std::string name = "kt_ja" + std::to_string(jc.compiled + static_cast<int64_t>(i));
+            sources[w] += "extern \"C\" __global__ void " + bounds + " " + name + keys[missing[i]].substr(bounds.size()) + "\n";
+            names[w].push_back(name);
+            owner[w].push_back(missing[i]);
+        }
+        std::vector<std::vector<const void*>> got;
+        if (jit_compile(sources, names, got, true) != KT_OK) {
+            jc.failed = true;
+            cudaGetLastError();
+            return false;
+        }
+        for (size_t w = 0; w < workers; ++w) {
+            for (size_t k = 0; k < names[w].size(); ++k) {
+                jc.kernels[keys[owner[w][k]]] = got[w][k];
+            }
+        }
+        jc.compiled += static_cast<int64_t>(missing.size());
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        dev = 0;
+    }
+    out.resize(nb);
+    for (size_t b = 0; b < nb; ++b) {
+        const void* fn = jc.kernels[keys[b]];
+        const auto key = std::make_pair(fn, dev);
+        auto it = jc.smem_set.find(key);
+        if (it == jc.smem_set.end() || it->second < smem_bytes) {
+            if (cudaKernelSetAttributeForDevice(reinterpret_cast<cudaKernel_t>(const_cast<void*>(fn)),
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes,
+                                                dev) != cudaSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+            jc.smem_set[key] = smem_bytes;
+        }
+        out[b] = fn;
+    }
+    return true;
+}
+
+// Adjoint plans cached by circuit structure (gate kinds, qubits, value
+// classes, gradient rows and generators): a repeated gradient with new
+// parameters takes the new matrices and reuses the plan (and its kernels).
+template <typename T>
+struct AdjPlanEntry
+{
+    std::vector<uint64_t> signature;
+    Plan<T, FOpA<T>> plan;
+    std::vector<std::vector<int32_t>> rows_of_block;
+    int64_t sweeps {0};
+    std::vector<const void*> kernels;  // compiled blocks (adjoint_jit), once compiled
+    int64_t generation {-1};
+    int device {-1};
+};
+
+template <typename T>
+struct AdjPlanCache
+{
+    std::mutex m;
+    std::unordered_map<uint64_t, AdjPlanEntry<T>> entries;
+};
+
+template <typename T>
+AdjPlanCache<T>& adj_plan_cache()
+{
+    static AdjPlanCache<T> c;
+    return c;
+}
+
 template <typename T>
 int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& gates, double* dev_grad,
                           DevBuf& work)
@@ -1908,10 +2181,45 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
         e.gen = g.gen;
         ex.push_back(e);
     }
-    // cap the ops of a block so its gradient rows fit the shared-memory slots
-    const auto pbs = form_blocks(lg, n, K, L, static_cast<size_t>(std::min(ADJ_MAX_OPS, tuning().fused_max_ops)));
+    // the plan of this structure: from the cache (new matrices), or planned now
+    const size_t max_ops = static_cast<size_t>(std::min(ADJ_MAX_OPS, tuning().fused_max_ops));
+    std::vector<uint64_t> sig;
+    sig.reserve(2 * lg.size() + 1);
+    sig.push_back(static_cast<uint64_t>(n) | (static_cast<uint64_t>(sizeof(T)) << 8) | (static_cast<uint64_t>(K) << 16) |
+                  (static_cast<uint64_t>(tuning().fold_permutations) << 24) | (static_cast<uint64_t>(max_ops) << 32));
+    for (size_t i = 0; i < lg.size(); ++i) {
+        sig.push_back(static_cast<uint64_t>(gate_class(lg[i])) | (static_cast<uint64_t>(lg[i].target & 0xFFFF) << 16) |
+                      (static_cast<uint64_t>(lg[i].control & 0xFFFF) << 32) |
+                      (static_cast<uint64_t>(ex[i].gen & 0xFF) << 48));
+        sig.push_back(static_cast<uint64_t>(static_cast<uint32_t>(ex[i].row)));
+    }
+    uint64_t key = 0xcbf29ce484222325ULL;
+    for (const uint64_t v : sig) {
+        key = (key ^ v) * 0x100000001b3ULL;
+        key ^= key >> 29;
+    }
     Plan<T, FOpA<T>> plan;
     std::vector<std::vector<int32_t>> rows_of_block;
+    int64_t sweeps_before = 0;
+    bool cached = false;
+    {
+        AdjPlanCache<T>& pc = adj_plan_cache<T>();
+        std::lock_guard<std::mutex> lock(pc.m);
+        auto it = pc.entries.find(key);
+        if (it != pc.entries.end() && it->second.signature == sig) {
+            plan = it->second.plan;
+            rows_of_block = it->second.rows_of_block;
+            sweeps_before = it->second.sweeps++;
+            for (size_t i = 0; i < plan.ops.size(); ++i) {
+                const LGate& x = lg[static_cast<size_t>(plan.op_gate[i])];
+                for (int e = 0; e < 8; ++e) {
+                    plan.ops[i].m[e] = static_cast<T>(x.m[e]);
+                }
+            }
+            cached = true;
+        }
+    }
+    const auto pbs = cached ? std::vector<PlanBlock> {} : form_blocks(lg, n, K, L, max_ops);
     for (const auto& pb : pbs) {
         // local row numbers inside the block
         std::vector<int32_t> rows;
@@ -1934,6 +2242,19 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
             set_error(KT_ERR_INVALID, "fused adjoint planner produced too many phases");
             return KT_ERR_INVALID;
         }
+    }
+    if (!cached) {
+        AdjPlanCache<T>& pc = adj_plan_cache<T>();
+        std::lock_guard<std::mutex> lock(pc.m);
+        if (pc.entries.size() >= 64) {
+            pc.entries.clear();
+        }
+        AdjPlanEntry<T>& e = pc.entries[key];
+        e = AdjPlanEntry<T> {};
+        e.signature = sig;
+        e.plan = plan;
+        e.rows_of_block = rows_of_block;
+        e.sweeps = 1;
     }
     const uint64_t n_tiles = uint64_t {1} << (n - K);
     const int grid = static_cast<int>(std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * 2));
@@ -1984,15 +2305,71 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
         attr = true;
     }
     const int threads = 1 << (K - RB);
+    // compiled blocks: adjoint_jit = 1 always, 2 from a structure's second sweep
+    std::vector<const void*> jk;
+    const int jmode = tuning().adjoint_jit;
+    if (threads == 256 && (jmode == 1 || (jmode == 2 && sweeps_before >= 1))) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            dev = 0;
+        }
+        bool have = false;
+        {
+            AdjPlanCache<T>& pc = adj_plan_cache<T>();
+            std::lock_guard<std::mutex> lock(pc.m);
+            auto it = pc.entries.find(key);
+            if (it != pc.entries.end() && it->second.device == dev && it->second.generation == jit_cache().generation &&
+                it->second.kernels.size() == plan.blocks.size()) {
+                jk = it->second.kernels;
+                have = true;
+            }
+        }
+        if (!have) {
+            const int most = static_cast<int>(2 * (sizeof(C) << K) + max_rows * ADJ_WARPS * sizeof(double));
+            if (jit_adj_kernels<T>(plan, RB, most, jk)) {
+                AdjPlanCache<T>& pc = adj_plan_cache<T>();
+                std::lock_guard<std::mutex> lock(pc.m);
+                auto it = pc.entries.find(key);
+                if (it != pc.entries.end()) {
+                    it->second.kernels = jk;
+                    it->second.device = dev;
+                    it->second.generation = jit_cache().generation;
+                }
+            } else {
+                jk.clear();
+            }
+        }
+    }
     size_t row_off = 0;
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         const auto& fb = plan.blocks[b];
         const int nr = static_cast<int>(rows_of_block[b].size());
-        const size_t smem = 2 * (size_t {1} << K) * sizeof(C) + static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOpA<T>) +
-                            static_cast<size_t>(nr) * ADJ_WARPS * sizeof(double);
-        k_fused_adj<T><<<grid, threads, smem, psi.stream>>>(static_cast<C*>(psi.amps), static_cast<C*>(lam.amps), d_blk + b,
-                                                            d_ph, d_ops, nr, d_part, n_tiles);
-        KT_CHECK_LAUNCH("k_fused_adj");
+        if (!jk.empty()) {
+            const size_t smem = 2 * (size_t {1} << K) * sizeof(C) + static_cast<size_t>(nr) * ADJ_WARPS * sizeof(double);
+            const int nops = std::max(1, fb.op_end - fb.op_begin);
+            std::vector<T> mats(8 * static_cast<size_t>(nops), T(0));
+            for (int j = 0; j < fb.op_end - fb.op_begin; ++j) {
+                for (int e = 0; e < 8; ++e) {
+                    mats[8 * static_cast<size_t>(j) + e] = plan.ops[static_cast<size_t>(fb.op_begin + j)].m[e];
+                }
+            }
+            void* pa = psi.amps;
+            void* la = lam.amps;
+            unsigned long long nt = n_tiles;
+            double* pp = d_part;
+            int nrr = nr;
+            void* args[] = {&pa, &la, &nt, &pp, &nrr, mats.data()};
+            KT_CUDA(cudaLaunchKernel(jk[b], dim3(static_cast<unsigned>(grid)), dim3(static_cast<unsigned>(threads)), args,
+                                     smem, psi.stream));
+            jit_cache().launches += 1;
+        } else {
+            const size_t smem = 2 * (size_t {1} << K) * sizeof(C) +
+                                static_cast<size_t>(fb.op_end - fb.op_begin) * sizeof(FOpA<T>) +
+                                static_cast<size_t>(nr) * ADJ_WARPS * sizeof(double);
+            k_fused_adj<T><<<grid, threads, smem, psi.stream>>>(static_cast<C*>(psi.amps), static_cast<C*>(lam.amps),
+                                                                d_blk + b, d_ph, d_ops, nr, d_part, n_tiles);
+            KT_CHECK_LAUNCH("k_fused_adj");
+        }
         if (nr > 0) {
             k_adj_rows<<<(nr + 127) / 128, 128, 0, psi.stream>>>(d_part, grid, d_rows + row_off, nr, dev_grad);
             KT_CHECK_LAUNCH("k_adj_rows");
@@ -2043,8 +2420,8 @@ int32_t jit_compile_only_t(int n, const std::vector<LGate>& gates, int64_t* n_ke
     for (size_t b = 0; b < plan.blocks.size(); ++b) {
         const std::string name = "kt_jc" + std::to_string(b);
         TmaCfg c;
-        c.groups = tuning().jit_tma_groups;
-        c.stages = std::max(tuning().jit_tma_stages, c.groups + 1);
+        c.groups = 1;
+        c.stages = std::max(tuning().jit_tma_stages, 2);
         c.geom = tma_geom(plan.blocks[b], n);
         const bool bt = tma && c.geom.ok;
         const int bthreads = bt ? c.groups * threads + 32 : threads;
@@ -2062,6 +2439,53 @@ int32_t jit_compile_only_t(int n, const std::vector<LGate>& gates, int64_t* n_ke
 }
 
 }  // namespace
+
+int32_t jit_adjoint_compile_only(int n, int32_t dtype, const std::vector<AdjGate>& gates, int64_t* n_kernels)
+{
+    auto run = [&](auto tag) -> int32_t {
+        using T = decltype(tag);
+        constexpr int RB = CfgA<T>::RB;
+        constexpr int L = CfgA<T>::L;
+        *n_kernels = 0;
+        if (n < RB + 5 || gates.empty()) {
+            return KT_OK;
+        }
+        const int K = std::min(n, RB + TB256);
+        std::vector<LGate> lg;
+        std::vector<AdjExtra> ex;
+        for (const auto& g : gates) {
+            lg.push_back(g.adj);
+            ex.push_back(AdjExtra {g.row, g.gen});
+        }
+        const auto pbs = form_blocks(lg, n, K, L, static_cast<size_t>(std::min(ADJ_MAX_OPS, tuning().fused_max_ops)));
+        Plan<T, FOpA<T>> plan;
+        for (const auto& pb : pbs) {
+            std::vector<AdjExtra> local(ex.size());
+            int32_t r = 0;
+            for (int gi : pb.gates) {
+                local[gi] = ex[gi];
+                if (ex[gi].row >= 0) {
+                    local[gi].row = r++;
+                }
+            }
+            plan_block<T, CfgA<T>, FOpA<T>>(pb, lg, n, plan, local.data());
+        }
+        std::vector<std::string> sources(1, JIT_PRELUDE);
+        std::vector<std::vector<std::string>> names(1);
+        for (size_t b = 0; b < plan.blocks.size(); ++b) {
+            const std::string name = "kt_jac" + std::to_string(b);
+            sources[0] += "extern \"C\" __global__ void __launch_bounds__(256, 2) " + name + jit_adj_body<T>(plan, b, RB) + "\n";
+            names[0].push_back(name);
+        }
+        std::vector<std::vector<const void*>> got;
+        if (const int32_t rc = jit_compile(sources, names, got, false); rc != KT_OK) {
+            return rc;
+        }
+        *n_kernels = static_cast<int64_t>(plan.blocks.size());
+        return KT_OK;
+    };
+    return dtype == KT_C64 ? run(float {}) : run(double {});
+}
 
 int32_t jit_async_error()
 {

@@ -141,6 +141,8 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
                     std::vector<std::vector<const void*>>& kernels, bool load = true);
 // host-only: plan an apply and compile its block kernels without loading them
 int32_t jit_compile_only(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* n_kernels);
+// host-only: plan the fused adjoint sweep `gates` and compile its block kernels
+int32_t jit_adjoint_compile_only(int n, int32_t dtype, const std::vector<AdjGate>& gates, int64_t* n_kernels);
 // KT_ERR_TIMEOUT (once) if a TMA block kernel's bounded wait ran out in an
 // apply whose error word has reached the host since the last call; KT_OK otherwise
 int32_t jit_async_error();
@@ -211,9 +213,10 @@ struct Tuning
     int jit_scale_ops {1};       // complex128 blocks: uncontrolled real / RX-like ops divided by m00 (one FMA per component)
     int jit_remat {1};           // 1: thread-index terms recomputed every tile, not held across the tile loop
     long long batch_spin_limit {1LL << 25};  // polls of the batch queue before a CTA gives up (~10 s)
+    int adjoint_jit {2};         // fused adjoint blocks as run-time compiled kernels: 0 never, 1 always,
+                                 // 2 from the second backward sweep of a circuit structure
     int jit_tma {0};             // 1: complex128 compiled blocks move tiles with TMA tensor copies, pipelined
-    int jit_tma_groups {1};      // TMA blocks: tiles in flight per CTA on separate thread groups (1 or 2)
-    int jit_tma_stages {3};      // TMA blocks: shared-memory tile buffers per CTA (2..6)
+    int jit_tma_stages {3};      // TMA blocks: shared-memory tile buffers per CTA (2..4)
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);

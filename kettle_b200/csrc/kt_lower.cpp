@@ -102,12 +102,12 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.fused_reg_bits = (v == 3) ? 3 : 4;
     } else if (name == "jit_remat") {
         t.jit_remat = (v != 0) ? 1 : 0;
+    } else if (name == "adjoint_jit") {
+        t.adjoint_jit = static_cast<int>(std::max(0LL, std::min(2LL, v)));
     } else if (name == "jit_tma") {
         t.jit_tma = (v != 0) ? 1 : 0;
-    } else if (name == "jit_tma_groups") {
-        t.jit_tma_groups = static_cast<int>(std::max(1LL, std::min(2LL, v)));
     } else if (name == "jit_tma_stages") {
-        t.jit_tma_stages = static_cast<int>(std::max(2LL, std::min(6LL, v)));
+        t.jit_tma_stages = static_cast<int>(std::max(2LL, std::min(4LL, v)));
     } else if (name == "batch_spin_limit") {
         t.batch_spin_limit = std::max(1LL, std::min(1000000000000LL, v));
     } else if (name == "jit_scale_ops") {
@@ -197,10 +197,10 @@ bool tuning_get(const char* name, long long* value)
         *value = t.fused_reg_bits;
     } else if (n == "jit_remat") {
         *value = t.jit_remat;
+    } else if (n == "adjoint_jit") {
+        *value = t.adjoint_jit;
     } else if (n == "jit_tma") {
         *value = t.jit_tma;
-    } else if (n == "jit_tma_groups") {
-        *value = t.jit_tma_groups;
     } else if (n == "jit_tma_stages") {
         *value = t.jit_tma_stages;
     } else if (n == "batch_spin_limit") {

@@ -157,3 +157,21 @@ def test_every_documented_knob_is_known_with_its_documented_default():
     for name, _, default in rows:
         if default:
             assert got[name] == int(default), (name, got[name], default)
+
+
+def test_adjoint_blocks_compile_on_the_host():
+    # adjoint_jit = 1: kt_jit_compile_only compiles the fused adjoint blocks of
+    # the circuit's backward sweep (complex128 and complex64)
+    from kettle_b200 import workloads as W
+    old = capi.tuning_get("adjoint_jit")
+    try:
+        capi.tuning_set("adjoint_jit", 1)
+        g, p = W.hea(14, 3, seed=3)
+        mixed = W.random_layers(13, 2, seed=4, mixed=True)
+        mixed["param"][::3] = np.arange(mixed[::3].size)
+        mp = np.linspace(0.1, 2.0, mixed[::3].size)
+        assert capi.jit_compile_only(14, g, p) >= 1
+        assert capi.jit_compile_only(13, mixed, mp) >= 1
+        assert capi.jit_compile_only(13, mixed, mp, dtype=capi.KT_C64) >= 1
+    finally:
+        capi.tuning_set("adjoint_jit", old)

@@ -107,3 +107,36 @@ def test_fused_deep_blocks(engine):
     e1, g1, _ = _grad(n, gates, params, strings, coeffs, fused=True)
     assert e0 == e1
     assert np.abs(g0 - g1).max() < 1e-11
+
+
+def _with_adjoint_jit(mode, fn):
+    old = capi.tuning_get("adjoint_jit")
+    capi.tuning_set("adjoint_jit", mode)
+    try:
+        return fn()
+    finally:
+        capi.tuning_set("adjoint_jit", old)
+
+
+@pytest.mark.parametrize("n,dtype,checkpoint", [(9, capi.KT_C128, 0), (13, capi.KT_C128, 0), (17, capi.KT_C128, 0),
+                                                (14, capi.KT_C128, 25), (13, capi.KT_C64, 0)])
+def test_compiled_adjoint_blocks_equal_interpreted(engine, n, dtype, checkpoint):
+    """Run-time compiled adjoint blocks (adjoint_jit = 1: gradient terms and
+    U^dagger bodies as straight-line code) against the interpreted fused
+    blocks (adjoint_jit = 0): the same energy and gradient (1e-12; complex64
+    1e-5), the state un-applied back to |0...0>; repeated with new parameters
+    (plan cache, kernels reused)."""
+    gates, params = _mixed_param_circuit(n, 100 + n)
+    strings, coeffs = W.random_paulis(n, 30, seed=n)
+    coeffs = coeffs.real.astype(np.complex128)
+    tol = 1e-12 if dtype == capi.KT_C128 else 1e-5
+    for shift in (0.0, 0.37):
+        p = params + shift
+        e0, g0, _ = _with_adjoint_jit(0, lambda: _grad(n, gates, p, strings, coeffs, True, checkpoint, dtype))
+        s0 = capi.jit_stats()
+        e1, g1, b1 = _with_adjoint_jit(1, lambda: _grad(n, gates, p, strings, coeffs, True, checkpoint, dtype))
+        s1 = capi.jit_stats()
+        assert not s1["failed"] and s1["launches"] > s0["launches"]
+        assert abs(e0 - e1) < tol
+        assert np.abs(g0 - g1).max() < tol
+        assert abs(b1[0] - 1) < 10 * tol and np.abs(b1[1:]).max() < 10 * tol
