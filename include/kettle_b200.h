@@ -234,6 +234,13 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  * Unknown names return KT_ERR_INVALID. */
 int32_t kt_tuning_set(const char* name, int64_t value);
 int32_t kt_tuning_get(const char* name, int64_t* value);
+/* Host-only, complex128: per fused block of an apply of n_qubits, four doubles
+ * {ops, layout phases, transposes, FP64 instructions per amplitude of the
+ * compiled block (a model of its gate bodies)}; up to `capacity` blocks are
+ * written, n_blocks gets the count.  Instrumentation (new): it gives each
+ * block's compute bounds beside its HBM bound. */
+int32_t kt_plan_blocks(int32_t n_qubits, const kt_gate* gates, int64_t n_gates, const double* params,
+                       int64_t n_params, double* out, int64_t capacity, int64_t* n_blocks);
 /* Run-time compiled block kernels so far, fused-block launches through them,
  * and 1 if run-time compilation was unavailable or failed (new). */
 int32_t kt_jit_stats(int64_t* kernels_compiled, int64_t* block_launches, int32_t* failed);

@@ -80,6 +80,7 @@ _SIGS = {
     "kt_sv_apply": ([P, P, I64, P, I64, I32], I32),
     "kt_sv_apply_stats": ([P, C.POINTER(I64), DP], I32),
     "kt_dm_apply_stats": ([P, C.POINTER(I64), DP], I32),
+    "kt_plan_blocks": ([I32, P, I64, P, I64, P, I64, C.POINTER(I64)], I32),
     "kt_sv_tensor_product": ([P, P, P], I32),
     "kt_sv_diagonal_expectation": ([P, P, P], I32),
     "kt_sample_probabilities": ([P, U64, P, I64, P, I32, P], I32),
@@ -182,6 +183,18 @@ def plan_order(n_qubits: int, gates: np.ndarray, params: np.ndarray | None = Non
     check(lib().kt_plan_order(n_qubits, dtype, ptr(g), g.size, ptr(p), 0 if p is None else p.size,
                               ptr(out), out.size, C.byref(cnt)))
     return out[:cnt.value].copy()
+
+
+def plan_blocks(n_qubits: int, gates: np.ndarray, params: np.ndarray | None = None) -> np.ndarray:
+    """Per fused block of a complex128 apply: [ops, phases, transposes, FP64 per amplitude] (kt_plan_blocks)."""
+    g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+    p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+    cap = max(1, g.size)
+    out = np.zeros(4 * cap, dtype=np.float64)
+    nb = I64(0)
+    check(lib().kt_plan_blocks(n_qubits, ptr(g), g.size, ptr(p), 0 if p is None else p.size, ptr(out), cap,
+                               C.byref(nb)))
+    return out[: 4 * nb.value].reshape(-1, 4)
 
 
 def jit_stats() -> dict:

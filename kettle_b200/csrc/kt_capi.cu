@@ -407,6 +407,30 @@ int32_t kt_plan_stats(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int
     });
 }
 
+int32_t kt_plan_blocks(int32_t n_qubits, const kt_gate* gates, int64_t n_gates, const double* params, int64_t n_params,
+                       double* out, int64_t capacity, int64_t* n_blocks)
+{
+    return guard([&]() -> int32_t {
+        if (n_blocks == nullptr || capacity < 0 || (capacity > 0 && out == nullptr)) {
+            return invalid("bad output array");
+        }
+        if (n_qubits < 1 || n_qubits > 40 || n_gates < 0 || (n_gates > 0 && gates == nullptr)) {
+            return invalid("bad qubit count or gate array");
+        }
+        std::vector<kt::LGate> lg;
+        if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, n_qubits, lg); rc != KT_OK) {
+            return rc;
+        }
+        std::vector<double> v;
+        if (const int32_t rc = kt::plan_blocks(n_qubits, lg, v); rc != KT_OK) {
+            return rc;
+        }
+        *n_blocks = static_cast<int64_t>(v.size() / 4);
+        std::copy(v.begin(), v.begin() + static_cast<std::ptrdiff_t>(std::min<size_t>(v.size(), 4 * static_cast<size_t>(capacity))), out);
+        return KT_OK;
+    });
+}
+
 int32_t kt_plan_order(int32_t n_qubits, int32_t dtype, const kt_gate* gates, int64_t n_gates, const double* params,
                       int64_t n_params, int64_t* order, int64_t capacity, int64_t* count)
 {

@@ -2616,6 +2616,55 @@ void plan_only(int n, const std::vector<LGate>& gates, int64_t* blocks, int64_t*
 
 }  // namespace
 
+// Per block of a complex128 apply: {ops, layout phases, transposes, FP64
+// instructions per amplitude of its compiled form}.  The FP64 count is a
+// model of the generated gate bodies: per pair a general gate costs 16 (12
+// scaled), a real or RX-like one 8 (4 scaled), an anti-diagonal one 8, a
+// swap 0, a diagonal one on a register bit 8 (4 one-sided), a diagonal
+// factor on a thread or tile-external bit 8; a control on a register bit or
+// outside the tile halves the work, one on a thread bit masks lanes without
+// saving issue slots.
+int32_t plan_blocks(int n, const std::vector<LGate>& gates, std::vector<double>& out)
+{
+    out.clear();
+    Plan<double> plan;
+    int K = 0;
+    bool rb3 = false;
+    if (const int32_t rc = fused_plan<double>(n, gates, plan, &K, &rb3); rc != KT_OK) {
+        return rc;
+    }
+    for (size_t b = 0; b < plan.blocks.size(); ++b) {
+        const FBlock& fb = plan.blocks[b];
+        const JitScale js = jit_scale_plan(plan, b);
+        double per_pair = 0.0;
+        for (int o = fb.op_begin; o < fb.op_end; ++o) {
+            const FOp<double>& op = plan.ops[static_cast<size_t>(o)];
+            const int sc = jit_scale_code(plan, b, o - fb.op_begin, js);
+            double c = 0.0;
+            switch (op.kind) {
+                case OP_GEN: c = sc == 4 ? 12.0 : 16.0; break;
+                case OP_GENR: c = (sc == 1 || sc == 2) ? 4.0 : 8.0; break;
+                case OP_RXL: c = sc == 3 ? 4.0 : 8.0; break;
+                case OP_ANTI: c = 8.0; break;
+                case OP_SWAP: c = 0.0; break;
+                default: c = (op.tslot != NO_SLOT && (op.kind == OP_DIAG1 || sc == 5)) ? 4.0 : 8.0; break;
+            }
+            if (op.cslot != NO_SLOT) {
+                c *= 0.5;
+            }
+            if (op.cglob != 0) {
+                c *= 0.5;
+            }
+            per_pair += c;
+        }
+        out.push_back(static_cast<double>(fb.op_end - fb.op_begin));
+        out.push_back(static_cast<double>(fb.phase_end - fb.phase_begin));
+        out.push_back(static_cast<double>(fb.phase_end - fb.phase_begin - 1));
+        out.push_back(per_pair / 2.0);
+    }
+    return KT_OK;
+}
+
 int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases,
                    int64_t* ops, int64_t* transposes, std::vector<int32_t>* order)
 {

@@ -154,6 +154,7 @@ int32_t jit_prepare(State& s, const std::vector<LGate>& gates);
 void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed);
 // host-only: what the fused planner makes of a gate stream; *order (if given)
 // receives the planned gates in the order they take effect
+int32_t plan_blocks(int n, const std::vector<LGate>& gates, std::vector<double>& out);
 int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* blocks, int64_t* phases,
                    int64_t* ops, int64_t* transposes, std::vector<int32_t>* order = nullptr);
 

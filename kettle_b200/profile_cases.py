@@ -23,6 +23,13 @@ Cases and the kernels they run:
   sweep        k_sweep (one pass per gate)
   state_ops    k_sv_tensor_product, k_sv_diag_expect, k_dm_block_norms, k_dm_collapse
   batch        k_batch_persist, k_batch_small, k_batch_patch
+  dense_block  the tensor-core question: 40 random gates on qubits 0..4 of a
+               complex64 state applied by the engine (one fused pass of
+               compiled SIMT blocks) against the same 32 x 32 unitary applied
+               as a dense GEMM by cuBLAS through torch, in FP32 on the CUDA
+               cores and in TF32 on the tensor cores; prints times (CUDA
+               events, best of reps) and the largest amplitude error of each
+               against the complex128 engine result
 """
 from __future__ import annotations
 
@@ -172,6 +179,108 @@ def case_batch(n, reps):
     for _ in range(1 + reps):
         b.evaluate(params)
     b.close()
+
+
+class _DeviceArray:
+    """A raw device buffer seen by torch (__cuda_array_interface__)."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3}
+
+
+def case_dense_block(n, reps):
+    import json
+
+    import torch
+
+    k = 5
+    rng = np.random.default_rng(16)
+    names = ["H", "RX", "RY", "RZ", "U", "CX", "CRY", "CP"]
+    recs = []
+    for _ in range(40):
+        name = names[int(rng.integers(len(names)))]
+        t = int(rng.integers(k))
+        if name in ("CX", "CRY", "CP"):
+            c = int((t + 1 + rng.integers(k - 1)) % k)
+            recs.append(W.gate(name, t, control=c, angle=float(rng.uniform(0, 2 * np.pi))))
+        elif name == "U":
+            recs.append(W.gate("U", t, u=W.random_unitaries(int(rng.integers(1 << 30)), 1)[0]))
+        else:
+            recs.append(W.gate(name, t, angle=float(rng.uniform(0, 2 * np.pi))))
+    gates = np.concatenate(recs)
+    # the block's 32 x 32 unitary: its columns are the engine's images of the basis states
+    cols = []
+    for b in range(1 << k):
+        sv = capi.Statevector(k)
+        sv.set_basis(b)
+        sv.apply(gates)
+        cols.append(sv.download())
+        sv.close()
+    U = np.stack(cols, axis=1)
+    # real form of y = U x on interleaved (re, im) pairs: yr = xr @ Mr
+    Mr = np.zeros((2 << k, 2 << k))
+    Mr[0::2, 0::2] = U.real.T
+    Mr[1::2, 0::2] = -U.imag.T
+    Mr[0::2, 1::2] = U.imag.T
+    Mr[1::2, 1::2] = U.real.T
+    N2 = 2 << n
+    init = W.random_layers(n, 1, seed=17, mixed=True)
+    want = capi.Statevector(n)
+    want.apply(init)
+    want.apply(gates)
+    tw = torch.as_tensor(_DeviceArray(want.device_ptr(), N2, "<f8"), device="cuda")
+    s64 = capi.Statevector(n, capi.KT_C64)
+    t64 = torch.as_tensor(_DeviceArray(s64.device_ptr(), N2, "<f4"), device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        best = None
+        for _ in range(1 + reps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            best = t if best is None else min(best, t)
+        return best
+
+    def max_err(x):
+        worst = 0.0
+        chunk = 1 << 26
+        for a in range(0, N2, chunk):
+            worst = max(worst, float((tw[a:a + chunk] - x[a:a + chunk].double()).abs().max()))
+        return worst
+
+    s64.set_basis(0)
+    s64.apply(init)
+    x0 = t64.clone()
+    s64.prepare(gates)
+
+    def eng():
+        t64.copy_(x0)
+        s64.apply(gates)
+
+    copy_t = timed(lambda: t64.copy_(x0))
+    t_eng = timed(eng) - copy_t
+    err_eng = max_err(t64)
+    xr = x0.view(-1, 2 << k)
+    y = torch.empty_like(xr)
+    m32 = torch.as_tensor(Mr, dtype=torch.float32, device="cuda")
+    out = {"qubits": n, "block_qubits": k, "gates": int(gates.size), "state_bytes": 4 * N2,
+           "engine": {"seconds": t_eng, "max_abs_error": err_eng}}
+    for name, tf32 in (("gemm_fp32", False), ("gemm_tf32", True)):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        t = timed(lambda: torch.matmul(xr, m32, out=y))
+        out[name] = {"seconds": t, "max_abs_error": max_err(y.view(-1))}
+    torch.backends.cuda.matmul.allow_tf32 = False
+    for key in ("engine", "gemm_fp32", "gemm_tf32"):
+        out[key]["alg_gbs"] = 2 * 4 * N2 / out[key]["seconds"] / 1e9
+    print(json.dumps(out))
+    s64.close()
+    want.close()
 
 
 CASES = {k[5:]: v for k, v in globals().items() if k.startswith("case_")}
