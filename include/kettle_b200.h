@@ -206,6 +206,10 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               one unscaled uncontrolled gate of the block (or
  *                               every amplitude before the store); below 1e-150 the
  *                               apply runs on the precompiled kernels
+ *   jit_lean_sync      0 or 1   (1) a compiled block's transpose into a phase that
+ *                               stores where it loads (no permutation folded into
+ *                               it) skips its second barrier: each thread's next
+ *                               writes go to the slots it read itself
  *   adjoint_jit        0, 1, 2  (2) fused adjoint blocks as kernels compiled at run
  *                               time (NVRTC: gradient terms and U^dagger bodies as
  *                               straight-line code): 0 never, 1 always, 2 from the

@@ -1047,7 +1047,15 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm, con
             for (int i = 0; i < R; ++i) {
                 s += "            v[" + std::to_string(i) + "] = sm[lo ^ " + std::to_string(reg_xor(cur.rsw, i)) + "u];\n";
             }
-            s += tbar + "        }\n";
+            // The barrier after the reads keeps the next transpose's writes from
+            // overwriting slots other threads have not read yet.  When this
+            // phase stores where it loaded (no permutation folded into its
+            // store side), each thread's next writes go to exactly the slots
+            // it read itself, so no other thread can still need them and the
+            // barrier is dropped (jit_lean_sync) -- except after the tile's last
+            // transpose, whose slots the next tile's first writes may reuse.
+            const bool lean = tuning().jit_lean_sync != 0 && p < last && identity_store(cur);
+            s += (lean ? std::string() : tbar) + "        }\n";
         }
         // Diagonal ops whose target (and controls, if any) are thread or
         // tile-external bits scale all of a thread's amplitudes by one factor;
@@ -1588,6 +1596,7 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
                                std::to_string(tuning().jit_prefetch) + std::to_string(tuning().jit_merge_diag) +
                                std::to_string(tuning().jit_skip_io) + std::to_string(tuning().jit_fence) +
                                std::to_string(tuning().jit_scale_ops) + std::to_string(tuning().jit_remat) +
+                               std::to_string(tuning().jit_lean_sync) +
                                (use_tma ? "/tma" + std::to_string(tma_cfg[0].groups) + "x" +
                                               std::to_string(tma_cfg[0].stages)
                                         : std::string());
@@ -2308,7 +2317,7 @@ int32_t run_adjoint_sweep(State& psi, State& lam, const std::vector<AdjGate>& ga
     // compiled blocks: adjoint_jit = 1 always, 2 from a structure's second sweep
     std::vector<const void*> jk;
     const int jmode = tuning().adjoint_jit;
-    if (threads == 256 && (jmode == 1 || (jmode == 2 && sweeps_before >= 1))) {
+    if (threads >= 32 && threads <= 256 && (jmode == 1 || (jmode == 2 && sweeps_before >= 1))) {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) {
             dev = 0;

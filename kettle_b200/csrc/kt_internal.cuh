@@ -216,6 +216,7 @@ struct Tuning
     long long batch_spin_limit {1LL << 25};  // polls of the batch queue before a CTA gives up (~10 s)
     int adjoint_jit {2};         // fused adjoint blocks as run-time compiled kernels: 0 never, 1 always,
                                  // 2 from the second backward sweep of a circuit structure
+    int jit_lean_sync {1};       // 1: compiled blocks drop a transpose's second barrier where the phase stores where it loaded
     int jit_tma {0};             // 1: complex128 compiled blocks move tiles with TMA tensor copies, pipelined
     int jit_tma_stages {3};      // TMA blocks: shared-memory tile buffers per CTA (2..4)
 };

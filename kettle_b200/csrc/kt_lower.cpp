@@ -104,6 +104,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.jit_remat = (v != 0) ? 1 : 0;
     } else if (name == "adjoint_jit") {
         t.adjoint_jit = static_cast<int>(std::max(0LL, std::min(2LL, v)));
+    } else if (name == "jit_lean_sync") {
+        t.jit_lean_sync = (v != 0) ? 1 : 0;
     } else if (name == "jit_tma") {
         t.jit_tma = (v != 0) ? 1 : 0;
     } else if (name == "jit_tma_stages") {
@@ -199,6 +201,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.jit_remat;
     } else if (n == "adjoint_jit") {
         *value = t.adjoint_jit;
+    } else if (n == "jit_lean_sync") {
+        *value = t.jit_lean_sync;
     } else if (n == "jit_tma") {
         *value = t.jit_tma;
     } else if (n == "jit_tma_stages") {
