@@ -206,6 +206,8 @@ struct kt_adjoint_s
     kt::DevBuf dev;     // hsum tables, partials, gradients
     kt::DevBuf fused_work;  // plans and partials of the fused sweep
     bool forward_done {false};
+    uint64_t last_structure {0};  // gate kinds, qubits and parameter slots of the previous forward
+    int64_t repeats {0};          // consecutive forwards of that structure
 };
 
 namespace
@@ -326,6 +328,27 @@ int32_t kt_adjoint_forward(kt_adjoint a, const kt_gate* gates, int64_t n_gates, 
         if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, psi.n_bits, lg); rc != KT_OK) {
             return rc;
         }
+        // a forward of the structure this handle just ran (a training or VQE
+        // loop) runs its fused blocks compiled, like the backward sweep
+        // (adjoint_jit = 2 from the second call; 1 always), whatever the
+        // state's size
+        uint64_t sig = 0xcbf29ce484222325ULL ^ static_cast<uint64_t>(n_gates);
+        for (int64_t i = 0; i < n_gates; ++i) {
+            const uint64_t v = static_cast<uint64_t>(gates[i].op) | (static_cast<uint64_t>(gates[i].target) << 8) |
+                               (static_cast<uint64_t>(gates[i].control) << 28) |
+                               (static_cast<uint64_t>(gates[i].param >= 0 ? 1 : 0) << 48);
+            sig = (sig ^ v) * 0x100000001b3ULL;
+            sig ^= sig >> 29;
+        }
+        a->repeats = (sig == a->last_structure) ? a->repeats + 1 : 0;
+        a->last_structure = sig;
+        const int jmode = kt::tuning().adjoint_jit;
+        psi.force_jit = jmode == 1 || (jmode == 2 && a->repeats >= 1);
+        struct Reset
+        {
+            kt::State& s;
+            ~Reset() { s.force_jit = false; }
+        } reset_force {psi};
         // backward records: U^dagger and dU/dtheta
         a->gates.clear();
         a->gates.reserve(lg.size());

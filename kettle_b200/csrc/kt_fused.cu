@@ -1531,7 +1531,7 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
     *rc = KT_OK;
     const int n = s.n_bits;
     const int mode = tuning().fused_jit;
-    const bool want = compile_only || mode == 1 || (mode == 2 && n >= tuning().jit_min_qubits);
+    const bool want = compile_only || mode == 1 || (mode == 2 && (n >= tuning().jit_min_qubits || s.force_jit));
     if (!want) {
         return false;
     }
@@ -1616,7 +1616,7 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
         if (ready) {
             jk = st.kernels;
         }
-        compile = compile || st.prepared || st.applies >= jit_after_applies(n, sizeof(C));
+        compile = compile || st.prepared || s.force_jit || st.applies >= jit_after_applies(n, sizeof(C));
     }
     if (!ready) {
         if (!compile ||

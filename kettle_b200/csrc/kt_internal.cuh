@@ -65,6 +65,7 @@ struct State
     cudaStream_t stream {nullptr};
     DevBuf scratch;          // reductions, CDF, plans
     DevBuf scratch2;
+    bool force_jit {false};      // fused applies run compiled blocks whatever fused_jit's size rule says
     int64_t last_launches {0};   // kernels launched by the last apply
     double last_alg_bytes {0.0};  // algorithmic bytes of the last apply
     uint64_t n_amps() const { return uint64_t {1} << n_bits; }
