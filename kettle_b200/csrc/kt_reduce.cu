@@ -72,54 +72,100 @@ struct PauliSlot
     int32_t pad;
 };
 
-// grid: (blocks, n_slots).  partial[(first + j) * gridDim.x + blockIdx.x]
-template <typename C>
-__global__ void __launch_bounds__(RED_THREADS) k_pauli(const C* __restrict__ a, int n, const PauliSlot* __restrict__ slots,
-                                                       const uint64_t* __restrict__ zmask, double* __restrict__ partial)
+// The slot's work with MAXG >= count accumulators and U grid-stride steps
+// (their loads) in flight per thread.  Each thread still adds its terms in the order
+// of the plain grid-stride loop (k, k + stride, ...), so the partials do not
+// depend on MAXG or U.
+template <typename C, int MAXG, int U>
+__device__ __forceinline__ void pauli_slot(const C* __restrict__ a, int n, const PauliSlot& sl,
+                                           const uint64_t* __restrict__ zmask, double* __restrict__ partial)
 {
-    const PauliSlot sl = slots[blockIdx.y];
-    uint64_t zs[PAULI_MAXG];
-    double acc[PAULI_MAXG];
-    int par[PAULI_MAXG];
+    uint64_t zs[MAXG];
+    double acc[MAXG];
+    int par[MAXG];
 #pragma unroll
-    for (int j = 0; j < PAULI_MAXG; ++j) {
+    for (int j = 0; j < MAXG; ++j) {
         zs[j] = (j < sl.count) ? zmask[sl.first + j] : 0;
         par[j] = __popcll(sl.x & zs[j]) & 1;
         acc[j] = 0.0;
     }
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (sl.h < 0) {
         const uint64_t N = uint64_t {1} << n;
-        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-            const double2 v = to_d2(a[i]);
+        auto add = [&](uint64_t i, double2 v) {
             const double p = v.x * v.x + v.y * v.y;
 #pragma unroll
-            for (int j = 0; j < PAULI_MAXG; ++j) {
+            for (int j = 0; j < MAXG; ++j) {
                 if (j < sl.count) {
                     acc[j] += (__popcll(i & zs[j]) & 1) ? -p : p;
                 }
             }
+        };
+        for (; k + (U - 1) * stride < N; k += U * stride) {
+            double2 v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                v[u] = to_d2(a[k + u * stride]);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                add(k + u * stride, v[u]);
+            }
+        }
+        for (; k < N; k += stride) {
+            add(k, to_d2(a[k]));
         }
     } else {
         const uint64_t half = uint64_t {1} << (n - 1);
-        for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < half; k += stride) {
-            const uint64_t i = insert_zero_bit(k, sl.h);
-            const uint64_t jj = i ^ sl.x;
-            const double2 ai = to_d2(a[i]);
-            const double2 aj = to_d2(a[jj]);
+        auto add = [&](uint64_t i, double2 ai, double2 aj) {
             // v = conj(a_j) * a_i
             const double vr = aj.x * ai.x + aj.y * ai.y;
             const double vi = aj.x * ai.y - aj.y * ai.x;
 #pragma unroll
-            for (int j = 0; j < PAULI_MAXG; ++j) {
+            for (int j = 0; j < MAXG; ++j) {
                 if (j < sl.count) {
                     const double t = par[j] ? vi : vr;
                     acc[j] += (__popcll(i & zs[j]) & 1) ? -t : t;
                 }
             }
+        };
+        for (; k + (U - 1) * stride < half; k += U * stride) {
+            double2 ai[U], aj[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint64_t i = insert_zero_bit(k + u * stride, sl.h);
+                ai[u] = to_d2(a[i]);
+                aj[u] = to_d2(a[i ^ sl.x]);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                add(insert_zero_bit(k + u * stride, sl.h), ai[u], aj[u]);
+            }
+        }
+        for (; k < half; k += stride) {
+            const uint64_t i = insert_zero_bit(k, sl.h);
+            add(i, to_d2(a[i]), to_d2(a[i ^ sl.x]));
         }
     }
-    block_reduce_store<PAULI_MAXG>(acc, sl.count, partial + (uint64_t)sl.first * gridDim.x + blockIdx.x, gridDim.x);
+    block_reduce_store<MAXG>(acc, sl.count, partial + (uint64_t)sl.first * gridDim.x + blockIdx.x, gridDim.x);
+}
+
+// grid: (blocks, n_slots).  partial[(first + j) * gridDim.x + blockIdx.x].
+// A slot of one string (the usual case: distinct X/Y masks) runs without the
+// other accumulators' predicated code and keeps 4 pair loads in flight.
+template <typename C>
+__global__ void __launch_bounds__(RED_THREADS) k_pauli(const C* __restrict__ a, int n, const PauliSlot* __restrict__ slots,
+                                                       const uint64_t* __restrict__ zmask, double* __restrict__ partial)
+{
+    const PauliSlot sl = slots[blockIdx.y];
+    if (sl.count == 1) {
+        pauli_slot<C, 1, 4>(a, n, sl, zmask, partial);
+    } else if (sl.count <= 4) {
+        pauli_slot<C, 4, 4>(a, n, sl, zmask, partial);
+    } else {
+        pauli_slot<C, PAULI_MAXG, 2>(a, n, sl, zmask, partial);
+    }
 }
 
 // One thread per string: fixed-order sum of the per-block partials, then the

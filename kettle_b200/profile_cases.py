@@ -14,10 +14,11 @@ Cases and the kernels they run:
   sample       k_probs, k_tile_*, k_exact_chain, k_last_below, k_seq_*  (kt_sv_sample, exact tier)
   sample_fast  k_probs, k_chunk_sums, k_chunk_offsets, k_sample_bound, k_sample_fast  (2^22 amplitudes)
   dm_pauli     k_dm_pauli, k_dm_pauli_finalize    (kt_dm_expect on a 13-qubit density matrix)
-  hpsi         k_hsum                              (lambda = H psi of the adjoint forward pass)
+  hpsi         k_hsum                              (lambda = H psi, formed when the adjoint backward starts)
   adjoint      k_fused_adj, k_adj_rows             (fused adjoint backward blocks)
   dm_ops       k_partial_trace, k_tensor_product, k_trace_square
-  norm         k_fused_norm or compiled blocks, k_norm_final  (complex64 renormalising apply)
+  norm         compiled blocks (prepared plan; k_fused_norm with fused_jit=0), k_norm_final
+               (complex64 renormalising apply)
   blocks       kt_jb* (run-time compiled blocks of the benchmark circuit family)
   fused        k_fused (the precompiled fused-block interpreter)
   sweep        k_sweep (one pass per gate)
@@ -87,6 +88,7 @@ def case_hpsi(n, reps):
     for _ in range(1 + reps):
         sv.set_basis(0)
         adj.forward(gates, params, strings, coeffs)
+        adj.backward()
     adj.close()
     sv.close()
 
@@ -121,6 +123,7 @@ def case_dm_ops(n, reps):
 def case_norm(n, reps):
     g = W.random_layers(n, 2, seed=10, mixed=True)
     sv = capi.Statevector(n, capi.KT_C64)
+    sv.prepare(g)
     for _ in range(1 + reps):
         sv.set_basis(0)
         sv.apply(g)
