@@ -376,6 +376,16 @@ int32_t kt_sv_tensor_product(kt_sv left, kt_sv right, kt_sv out);
  * state/state.cpp:174-188); the sum is taken in another order, so the result
  * agrees within FP64 rounding. */
 int32_t kt_sv_diagonal_expectation(kt_sv sv, const double* eigenvalues, double* out_re_im);
+/* A dense unitary U on qubits 0..4 of a complex64 state of 12 to 34 qubits,
+ * psi <- (I (x) U) psi, as a GEMM on the tensor cores (tcgen05): u is U as
+ * 32 x 32 complex entries, row-major, interleaved doubles, U[b][a] mapping
+ * basis state a to b.  passes = 3 splits both operands into TF32 parts
+ * (hi rounded to nearest, lo the remainder) and sums three TF32 products in
+ * FP32, passes = 4 adds the fourth (lo lo): about FP32 accuracy; passes = 1
+ * is one plain TF32 product (10-bit mantissas, about 1e-3 relative error).  New: it
+ * measures where a dense block on the tensor cores pays against the gate
+ * bodies of the fused blocks; the fused planner does not call it. */
+int32_t kt_sv_apply_dense5(kt_sv sv, const double* u, int32_t passes);
 /* Shots from a caller's probability vector (n doubles, host): the sampler of
  * kt_sv_sample on those values, bit-exact to the reference's sequential CDF
  * and lower_bound (calculations/measurements.cpp:58-159, the

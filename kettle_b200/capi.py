@@ -83,6 +83,7 @@ _SIGS = {
     "kt_plan_blocks": ([I32, P, I64, P, I64, P, I64, C.POINTER(I64)], I32),
     "kt_sv_tensor_product": ([P, P, P], I32),
     "kt_sv_diagonal_expectation": ([P, P, P], I32),
+    "kt_sv_apply_dense5": ([P, P, I32], I32),
     "kt_sample_probabilities": ([P, U64, P, I64, P, I32, P], I32),
     "kt_dm_measure_probs": ([P, U32, DP, DP], I32),
     "kt_dm_collapse": ([P, U32, I32, C.c_double], I32),
@@ -362,6 +363,14 @@ class Statevector:
         out = np.empty(2, dtype=np.float64)
         check(lib().kt_sv_diagonal_expectation(self._h, ptr(lam), ptr(out)))
         return complex(out[0], out[1])
+
+    def apply_dense5(self, u, passes: int = 3):
+        """The 32 x 32 unitary `u` on qubits 0..4 of a complex64 state, on the tensor cores (kt_sv_apply_dense5;
+        passes 3 or 4: TF32 split products of about FP32 accuracy, 1: plain TF32)."""
+        m = np.ascontiguousarray(u, dtype=np.complex128)
+        if m.shape != (32, 32):
+            raise ValueError("u must be 32 x 32")
+        check(lib().kt_sv_apply_dense5(self._h, ptr(m), passes))
 
 
 def sample_probabilities(probabilities, canonicals, mode: int = 0, stream: int | None = None) -> np.ndarray:

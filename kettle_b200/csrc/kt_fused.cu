@@ -2688,4 +2688,25 @@ int32_t plan_stats(int n, int32_t dtype, const std::vector<LGate>& gates, int64_
     return KT_OK;
 }
 
+bool tma_encode_rows_f32(void* base, uint64_t row_floats, uint64_t rows, uint32_t box_floats, uint32_t box_rows,
+                         void* out)
+{
+    EncodeTiledFn fn = encode_tiled();
+    if (fn == nullptr) {
+        return false;
+    }
+    const cuuint64_t dims[2] = {row_floats, rows};
+    const cuuint64_t strides[1] = {row_floats * sizeof(float)};
+    const cuuint32_t box[2] = {box_floats, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(static_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+unsigned int* async_error_word(int dev, unsigned int** host)
+{
+    return tma_err_word(dev, host);
+}
+
 }  // namespace kt

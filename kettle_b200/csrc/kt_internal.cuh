@@ -144,6 +144,14 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
 int32_t jit_compile_only(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* n_kernels);
 // host-only: plan the fused adjoint sweep `gates` and compile its block kernels
 int32_t jit_adjoint_compile_only(int n, int32_t dtype, const std::vector<AdjGate>& gates, int64_t* n_kernels);
+// a tensor map (written to `out`, 128 bytes) over `rows` rows of `row_floats`
+// float32 each, boxes of box_rows x box_floats with the 128-byte swizzle;
+// false when the driver entry point is missing or rejects the geometry
+bool tma_encode_rows_f32(void* base, uint64_t row_floats, uint64_t rows, uint32_t box_floats, uint32_t box_rows,
+                         void* out);
+// the device's error word set by kernels whose bounded waits ran out (and its
+// pinned host copy, which jit_async_error reads); nullptr on failure
+unsigned int* async_error_word(int dev, unsigned int** host);
 // KT_ERR_TIMEOUT (once) if a TMA block kernel's bounded wait ran out in an
 // apply whose error word has reached the host since the last call; KT_OK otherwise
 int32_t jit_async_error();

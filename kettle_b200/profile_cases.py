@@ -27,8 +27,10 @@ Cases and the kernels they run:
   dense_block  the tensor-core question: 40 random gates on qubits 0..4 of a
                complex64 state applied by the engine (one fused pass of
                compiled SIMT blocks) against the same 32 x 32 unitary applied
-               as a dense GEMM by cuBLAS through torch, in FP32 on the CUDA
-               cores and in TF32 on the tensor cores; prints times (CUDA
+               as a dense GEMM: by the engine's own tcgen05 kernel
+               (kt_sv_apply_dense5: four, three and one TF32 products) and by
+               cuBLAS through torch, in FP32 on the CUDA cores and in TF32
+               on the tensor cores; prints times (CUDA
                events, best of reps) and the largest amplitude error of each
                against the complex128 engine result
 """
@@ -269,17 +271,24 @@ def case_dense_block(n, reps):
     copy_t = timed(lambda: t64.copy_(x0))
     t_eng = timed(eng) - copy_t
     err_eng = max_err(t64)
+    tc = {}
+    for name, passes in (("tcgen05_4xtf32", 4), ("tcgen05_3xtf32", 3), ("tcgen05_tf32", 1)):
+        def run_tc(p=passes):
+            t64.copy_(x0)
+            s64.apply_dense5(U, p)
+        t = timed(run_tc) - copy_t
+        tc[name] = {"seconds": t, "max_abs_error": max_err(t64)}
     xr = x0.view(-1, 2 << k)
     y = torch.empty_like(xr)
     m32 = torch.as_tensor(Mr, dtype=torch.float32, device="cuda")
     out = {"qubits": n, "block_qubits": k, "gates": int(gates.size), "state_bytes": 4 * N2,
-           "engine": {"seconds": t_eng, "max_abs_error": err_eng}}
+           "engine": {"seconds": t_eng, "max_abs_error": err_eng}, **tc}
     for name, tf32 in (("gemm_fp32", False), ("gemm_tf32", True)):
         torch.backends.cuda.matmul.allow_tf32 = tf32
         t = timed(lambda: torch.matmul(xr, m32, out=y))
         out[name] = {"seconds": t, "max_abs_error": max_err(y.view(-1))}
     torch.backends.cuda.matmul.allow_tf32 = False
-    for key in ("engine", "gemm_fp32", "gemm_tf32"):
+    for key in ("engine", "tcgen05_4xtf32", "tcgen05_3xtf32", "tcgen05_tf32", "gemm_fp32", "gemm_tf32"):
         out[key]["alg_gbs"] = 2 * 4 * N2 / out[key]["seconds"] / 1e9
     print(json.dumps(out))
     s64.close()
