@@ -231,6 +231,17 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               10 s): the evaluation then stops and
  *                               kt_batch_evaluate returns KT_ERR_TIMEOUT; the value
  *                               is taken when the batch is created (its graph)
+ *   batch_small_max_qubits 0..13 (13) batch items of at most this many qubits
+ *                               run whole in shared memory, one CTA each (within
+ *                               11..12 for complex128 and 12..13 for complex64: what
+ *                               fits, and an HBM item needs a whole forward tile);
+ *                               taken when the batch is created
+ *   batch_jit_min_qubits 0..64 (13) batch items in HBM with at least this many
+ *                               qubits run run-time compiled block kernels (one
+ *                               launch per block for all items of one plan
+ *                               structure) instead of the persistent kernel's
+ *                               interpreted blocks; 0: never.  Taken when the batch
+ *                               is created; needs NVRTC and one memory wave
  *   fused_reg_bits     3 or 4   (4) complex128 amplitudes per thread in fused blocks
  *                               (2^4; or 2^3 with twice the warps: 12-qubit tiles of
  *                               512 threads, 2 CTAs per SM, or 11-qubit tiles of 256
@@ -421,6 +432,10 @@ int32_t kt_dm_upload(kt_dm dm, const double* host_colmajor, uint64_t n_elems);
 int32_t kt_dm_download(kt_dm dm, double* host_colmajor, uint64_t n_elems);
 int32_t kt_dm_apply(kt_dm dm, const kt_gate* gates, int64_t n_gates,
                     const double* params, int64_t n_params, int32_t mode);
+/* kt_sv_prepare for a density matrix (new): plan the 2n-bit gate stream that
+ * kt_dm_apply of these gates runs and compile its fused block kernels now, so
+ * every apply of the same circuit structure runs them from the first. */
+int32_t kt_dm_prepare(kt_dm dm, const kt_gate* gates, int64_t n_gates, const double* params, int64_t n_params);
 /* Tr(P_k rho) per string and sum_k c_k phase_k Tr(P_k rho) (new: the reference
  * has no density-matrix expectation value). */
 int32_t kt_dm_expect(kt_dm dm, const kt_pauli* strings, int64_t n_strings,
@@ -518,6 +533,10 @@ int32_t kt_batch_evaluate(kt_batch b, const double* params, double* energies,
 int32_t kt_batch_stats(kt_batch b, int64_t* small_items, int64_t* large_items,
                        int64_t* waves, int64_t* jobs, int64_t* units,
                        int64_t* launches, double* alg_bytes, double* device_bytes);
+/* HBM items that run run-time compiled block kernels (batch_jit_min_qubits):
+ * the plan-structure classes they form (one launch per block per class) and
+ * how many items those hold (instrumentation). */
+int32_t kt_batch_compiled(kt_batch b, int64_t* classes, int64_t* items);
 int32_t kt_batch_destroy(kt_batch b);
 
 int32_t kt_batch_run(const kt_batch_item* items, int64_t n_items,

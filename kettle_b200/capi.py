@@ -106,6 +106,7 @@ _SIGS = {
     "kt_dm_upload": ([P, P, U64], I32),
     "kt_dm_download": ([P, P, U64], I32),
     "kt_dm_apply": ([P, P, I64, P, I64, I32], I32),
+    "kt_dm_prepare": ([P, P, I64, P, I64], I32),
     "kt_dm_expect": ([P, P, I64, P, P, P], I32),
     "kt_dm_trace": ([P, P], I32),
     "kt_dm_probabilities": ([P, P], I32),
@@ -120,6 +121,7 @@ _SIGS = {
     "kt_batch_set_stream": ([P, P], I32),
     "kt_batch_evaluate": ([P, P, P, P], I32),
     "kt_batch_stats": ([P] + [C.POINTER(I64)] * 6 + [DP, DP], I32),
+    "kt_batch_compiled": ([P, C.POINTER(I64), C.POINTER(I64)], I32),
     "kt_batch_destroy": ([P], I32),
     "kt_batch_run": ([P, I64, P, I64, P, I64, P, P, I64, I32, P, P, P], I32),
 }
@@ -425,6 +427,12 @@ class DensityMatrix:
         p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
         check(lib().kt_dm_apply(self._h, ptr(g), g.size, ptr(p), 0 if p is None else p.size, mode))
 
+    def prepare(self, gates: np.ndarray, params: np.ndarray | None = None):
+        """Compile the fused block kernels of this circuit on the density matrix now (kt_dm_prepare)."""
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        check(lib().kt_dm_prepare(self._h, ptr(g), g.size, ptr(p), 0 if p is None else p.size))
+
     def measure_probs(self, qubit: int):
         """P(0), P(1) of an M gate on `qubit` as the reference defines them (kt_dm_measure_probs)."""
         p0 = C.c_double()
@@ -609,4 +617,8 @@ class Batch:
         out = {k: x.value for k, x in zip(keys, v)}
         out["alg_bytes"] = a.value
         out["device_bytes"] = d.value
+        cl, ci = I64(), I64()
+        check(lib().kt_batch_compiled(self._h, C.byref(cl), C.byref(ci)))
+        out["compiled_classes"] = cl.value
+        out["compiled_items"] = ci.value
         return out

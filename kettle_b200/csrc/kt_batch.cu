@@ -38,6 +38,8 @@
 #include <numeric>
 #include <string>
 #include <thread>
+#include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "kt_fused.cuh"
@@ -110,6 +112,8 @@ struct BPatch
     int32_t op;      // KT_OP_* of the gate
     int64_t index;   // record index in its table
     int64_t param;   // index into the parameter vector
+    int32_t one_sided;  // the record is a one-sided diagonal diag(1, m11 / m00) (see one_sided_diagonals)
+    int32_t pad;
 };
 
 struct RowSrc
@@ -245,7 +249,16 @@ __global__ void k_batch_patch(const double* __restrict__ params, const BPatch* _
     double u[8], d[8];
     rotation(p.op, params[p.param], u, d);
     const double ua[8] = {u[0], -u[1], u[4], -u[5], u[2], -u[3], u[6], -u[7]};
-    if (p.table == TAB_FWD) {
+    if (p.one_sided != 0) {
+        // diag(u00, u11) as diag(1, u11 / u00); |u00| = 1 (RZ, P): U^dagger the conjugates
+        const double r = u[6] * u[0] + u[7] * u[1];
+        const double i = u[7] * u[0] - u[6] * u[1];
+        T* m = (p.table == TAB_FWD) ? fops[p.index].m : bops[p.index].m;
+        const double one[8] = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, r, (p.table == TAB_FWD) ? i : -i};
+        for (int e = 0; e < 8; ++e) {
+            m[e] = static_cast<T>(one[e]);
+        }
+    } else if (p.table == TAB_FWD) {
         for (int e = 0; e < 8; ++e) {
             fops[p.index].m[e] = static_cast<T>(u[e]);
         }
@@ -400,6 +413,112 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_small(const SItem* __restri
     }
 }
 
+// lambda = H psi over the amplitudes [j0, j1) of one item and this thread's
+// share of Re <psi|lambda> (HJ amplitudes per thread at a time: HJ
+// independent gathers per string in flight); j1 - j0 is a multiple of
+// B_THREADS * HJ
+template <typename T>
+__device__ double ham_range(const typename CxT<T>::type* psi, typename CxT<T>::type* lam, const BStr* st, int n_str,
+                            uint64_t j0, uint64_t j1, int with_grad)
+{
+    // lambda in the state's precision (FP32 terms for complex64, whose lambda
+    // is stored in FP32 anyway); the energy in FP64
+    using C = typename CxT<T>::type;
+    double e = 0.0;
+    for (uint64_t jb = j0 + threadIdx.x; jb < j1; jb += B_THREADS * HJ) {
+        T lr[HJ], li[HJ];
+#pragma unroll
+        for (int k = 0; k < HJ; ++k) {
+            lr[k] = 0;
+            li[k] = 0;
+        }
+        for (int s = 0; s < n_str; ++s) {
+            const BStr bs = st[s];
+            const T cr = static_cast<T>(bs.cr), ci = static_cast<T>(bs.ci);
+            C pv[HJ];
+#pragma unroll
+            for (int k = 0; k < HJ; ++k) {
+                pv[k] = __ldcg(psi + ((jb + static_cast<uint64_t>(k) * B_THREADS) ^ bs.x));
+            }
+#pragma unroll
+            for (int k = 0; k < HJ; ++k) {
+                const uint64_t src = (jb + static_cast<uint64_t>(k) * B_THREADS) ^ bs.x;
+                const T sg = (__popcll(src & bs.z) & 1) ? T(-1) : T(1);
+                lr[k] += sg * (cr * pv[k].x - ci * pv[k].y);
+                li[k] += sg * (cr * pv[k].y + ci * pv[k].x);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < HJ; ++k) {
+            const uint64_t j = jb + static_cast<uint64_t>(k) * B_THREADS;
+            const double2 pj = to_d2(__ldcg(psi + j));
+            e += pj.x * static_cast<double>(lr[k]) + pj.y * static_cast<double>(li[k]);
+            if (with_grad) {
+                lam[j] = make_cx<T>(lr[k], li[k]);
+            }
+        }
+    }
+    return e;
+}
+
+// ---------------------------------------------------------------------------
+// items in HBM that run compiled block kernels: every launch serves the items
+// of one plan structure, blockIdx.y the item (see jit_batch_compile)
+
+// |0...0> into every listed state
+template <typename C>
+__global__ void k_batch_basis(void* const* __restrict__ states, uint64_t n_amps)
+{
+    C* a = static_cast<C*>(states[blockIdx.y]);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_amps;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        a[i] = (i == 0) ? C {1, 0} : C {0, 0};
+    }
+}
+
+// lambda = H psi and the energy partials of the listed items, which have
+// n_chunks chunks of 2^K amplitudes each: epart[ebase[item] + chunk].  The
+// units (item, chunk) are taken in item-major order by all CTAs at once, so
+// the CTAs work on one item at a time and its psi[j ^ x] gathers stay in L2.
+template <typename T>
+__global__ void __launch_bounds__(B_THREADS) k_batch_ham_items(typename CxT<T>::type* __restrict__ arena,
+                                                               const BInst* __restrict__ insts,
+                                                               const int64_t* __restrict__ list,
+                                                               const int64_t* __restrict__ ebase,
+                                                               const BStr* __restrict__ strs, double* __restrict__ epart,
+                                                               int K, int with_grad, uint64_t n_items, uint64_t n_chunks)
+{
+    using C = typename CxT<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[B_THREADS / 32];
+    BStr* sst = reinterpret_cast<BStr*>(smem_raw);
+    const uint64_t chunk = uint64_t {1} << K;
+    int64_t staged = -1;
+    for (uint64_t u = blockIdx.x; u < n_items * n_chunks; u += gridDim.x) {
+        const int64_t item = static_cast<int64_t>(u / n_chunks);
+        const uint64_t c = u % n_chunks;
+        const BInst inst = insts[list[item]];
+        const BStr* st = strs + inst.str;
+        if (inst.n_str <= HAM_SMEM_STRINGS) {
+            if (item != staged) {
+                __syncthreads();  // every thread is done with the previous item's strings
+                for (int s = threadIdx.x; s < inst.n_str; s += B_THREADS) {
+                    sst[s] = st[s];
+                }
+                __syncthreads();
+                staged = item;
+            }
+            st = sst;
+        }
+        const double e = block_sum(ham_range<T>(arena + inst.psi, arena + inst.lam, st, inst.n_str, c * chunk,
+                                                (c + 1) * chunk, with_grad),
+                                   red);
+        if (threadIdx.x == 0) {
+            epart[ebase[item] + static_cast<int64_t>(c)] = e;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // items in HBM: the persistent work-queue kernel
 template <typename T>
@@ -516,42 +635,9 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_batch_persist(BArgs<T> A)
             }
             __syncthreads();
             C* lam = A.arena + inst.lam;
-            double e = 0.0;
-            const uint64_t j0 = t0 << chunk_bits, j1 = t1 << chunk_bits;
-            // HJ amplitudes per thread at a time: HJ independent gathers per string in flight
-            for (uint64_t jb = j0 + t; jb < j1; jb += B_THREADS * HJ) {
-                double lr[HJ], li[HJ];
-#pragma unroll
-                for (int k = 0; k < HJ; ++k) {
-                    lr[k] = 0.0;
-                    li[k] = 0.0;
-                }
-                for (int s = 0; s < inst.n_str; ++s) {
-                    const BStr bs = st[s];
-                    double2 pv[HJ];
-#pragma unroll
-                    for (int k = 0; k < HJ; ++k) {
-                        pv[k] = to_d2(__ldcg(psi + ((jb + static_cast<uint64_t>(k) * B_THREADS) ^ bs.x)));
-                    }
-#pragma unroll
-                    for (int k = 0; k < HJ; ++k) {
-                        const uint64_t src = (jb + static_cast<uint64_t>(k) * B_THREADS) ^ bs.x;
-                        const double sg = (__popcll(src & bs.z) & 1) ? -1.0 : 1.0;
-                        lr[k] += sg * (bs.cr * pv[k].x - bs.ci * pv[k].y);
-                        li[k] += sg * (bs.cr * pv[k].y + bs.ci * pv[k].x);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < HJ; ++k) {
-                    const uint64_t j = jb + static_cast<uint64_t>(k) * B_THREADS;
-                    const double2 pj = to_d2(__ldcg(psi + j));
-                    e += pj.x * lr[k] + pj.y * li[k];
-                    if (A.with_grad) {
-                        lam[j] = make_cx<T>(static_cast<T>(lr[k]), static_cast<T>(li[k]));
-                    }
-                }
-            }
-            e = block_sum(e, red);
+            const double e = block_sum(ham_range<T>(psi, lam, st, inst.n_str, t0 << chunk_bits, t1 << chunk_bits,
+                                                    A.with_grad),
+                                       red);
             if (t == 0) {
                 A.epart[job.part + wu.y] = e;
             }
@@ -684,9 +770,40 @@ struct ItemPlan
     std::vector<std::pair<int64_t, int32_t>> bpatch;  // (local adjoint op, gate index)
     std::vector<int32_t> slot;                        // gate -> slot
     std::vector<uint8_t> opcode;                      // gate -> KT_OP_*
+    std::vector<uint8_t> fone, bone;                  // op -> made one-sided (one_sided_diagonals)
+    uint64_t key {0};                                 // structure of both plans (plan_structure_key)
     int32_t rc {KT_OK};
     std::string err;
 };
+
+// A hash of everything the text of an item's batched block kernels depends
+// on: the qubit count, the blocks, phases and op records of both plans (the
+// records without their matrices) and the rows of every adjoint block.  The
+// planner value-initialises its records, so equal structures hash equal.
+template <typename T>
+uint64_t plan_structure_key(const ItemPlan<T>& ip, int q)
+{
+    std::string bytes;
+    auto add = [&](const void* p, size_t n) { bytes.append(static_cast<const char*>(p), n); };
+    add(&q, sizeof(q));
+    auto add_plan = [&](const auto& plan) {
+        const uint64_t counts[3] = {plan.blocks.size(), plan.phases.size(), plan.ops.size()};
+        add(counts, sizeof(counts));
+        add(plan.blocks.data(), plan.blocks.size() * sizeof(FBlock));
+        add(plan.phases.data(), plan.phases.size() * sizeof(FPhase));
+        for (auto op : plan.ops) {
+            std::memset(static_cast<void*>(op.m), 0, sizeof(op.m));
+            add(&op, sizeof(op));
+        }
+    };
+    add_plan(ip.fwd);
+    add_plan(ip.bwd);
+    for (const auto& r : ip.rows_of_block) {
+        const uint64_t n = r.size();
+        add(&n, sizeof(n));
+    }
+    return std::hash<std::string> {}(bytes);
+}
 
 template <typename P>
 bool phases_fit(const P& plan)
@@ -697,6 +814,43 @@ bool phases_fit(const P& plan)
         }
     }
     return true;
+}
+
+// An item's energy and gradient do not depend on a global phase of psi: the
+// energy is <psi|H|psi>, lambda = H psi carries psi's phase, and every
+// gradient term is bilinear in conj(lambda) and psi.  So an uncontrolled
+// diagonal op with |m00| = 1 (RZ, P, literal phases) may run as the
+// one-sided diag(1, m11 / m00) in both sweeps: it drops the same unit factor
+// from psi and lambda, and touches half the amplitudes.  Returns, per op,
+// whether it was rewritten (its patch then writes the one-sided form).
+template <typename P>
+std::vector<uint8_t> one_sided_diagonals(P& plan)
+{
+    std::vector<uint8_t> flag(plan.ops.size(), 0);
+    for (size_t o = 0; o < plan.ops.size(); ++o) {
+        auto& op = plan.ops[o];
+        if (op.kind != OP_DIAG || op.cslot != NO_SLOT || op.cthr != 0 || op.cglob != 0) {
+            continue;
+        }
+        const double m0r = static_cast<double>(op.m[0]), m0i = static_cast<double>(op.m[1]);
+        const double m1r = static_cast<double>(op.m[6]), m1i = static_cast<double>(op.m[7]);
+        if (std::abs(m0r * m0r + m0i * m0i - 1.0) > 1e-12) {
+            continue;
+        }
+        // m11 conj(m00)
+        const double r = m1r * m0r + m1i * m0i;
+        const double i = m1i * m0r - m1r * m0i;
+        for (int e = 0; e < 8; ++e) {
+            op.m[e] = 0;
+        }
+        op.m[0] = 1;
+        using E = std::remove_reference_t<decltype(op.m[0])>;
+        op.m[6] = static_cast<E>(r);
+        op.m[7] = static_cast<E>(i);
+        op.kind = OP_DIAG1;
+        flag[o] = 1;
+    }
+    return flag;
 }
 
 template <typename T>
@@ -780,6 +934,9 @@ void plan_item(const kt_batch_item& it, const kt_gate* gates, bool with_grad, It
         set_error(KT_ERR_INVALID, "batch planner produced too many phases");
         ip.err = last_error_cstr();
     }
+    ip.fone = one_sided_diagonals(ip.fwd);
+    ip.bone = one_sided_diagonals(ip.bwd);
+    ip.key = plan_structure_key(ip, q);
 }
 
 template <typename P>
@@ -800,6 +957,37 @@ void append_plan(P& dst, const P& src)
         dst.phases.push_back(p);
     }
     dst.ops.insert(dst.ops.end(), src.ops.begin(), src.ops.end());
+}
+
+template <typename P>
+BatchPlanView view_of(const P& plan)
+{
+    BatchPlanView v;
+    v.blocks = plan.blocks.data();
+    v.n_blocks = static_cast<int64_t>(plan.blocks.size());
+    v.phases = plan.phases.data();
+    v.n_phases = static_cast<int64_t>(plan.phases.size());
+    v.ops = plan.ops.data();
+    v.n_ops = static_cast<int64_t>(plan.ops.size());
+    v.rec_bytes[0] = static_cast<int64_t>(sizeof(FBlock));
+    v.rec_bytes[1] = static_cast<int64_t>(sizeof(FPhase));
+    v.rec_bytes[2] = static_cast<int64_t>(sizeof(typename decltype(plan.ops)::value_type));
+    return v;
+}
+
+// tile qubits of the batch's forward and adjoint blocks (256-thread tiles)
+template <typename T>
+constexpr int K_FWD = Cfg<T>::RB + TB256;
+template <typename T>
+constexpr int K_BWD = CfgA<T>::RB + TB256;
+
+// CTAs per item of a compiled class launch: about four per SM over the class,
+// at most one per tile
+int32_t ctas_per_item(size_t n_items, int64_t tiles)
+{
+    const int64_t want = (4 * static_cast<int64_t>(sm_count()) + static_cast<int64_t>(n_items) - 1) /
+                         static_cast<int64_t>(n_items);
+    return static_cast<int32_t>(std::max<int64_t>(1, std::min<int64_t>(tiles, want)));
 }
 
 int64_t units_for(int64_t n_tiles, int32_t* tiles_per_unit)
@@ -854,6 +1042,14 @@ struct kt_batch_s
     cudaGraph_t graph {nullptr};
     cudaGraphExec_t exec {nullptr};
     cudaStream_t user {nullptr};
+    // compiled classes: streams their chains run on inside the graph, and the
+    // programs holding their kernels (unloaded with the batch)
+    static constexpr int N_CLASS_STREAMS = 4;
+    cudaStream_t cs[N_CLASS_STREAMS] {};
+    cudaEvent_t cev[N_CLASS_STREAMS] {};
+    std::vector<cudaLibrary_t> libs;
+    int64_t n_classes {0};
+    int64_t n_compiled_items {0};
 };
 
 namespace kt
@@ -865,6 +1061,14 @@ void release(kt_batch_s* b)
 {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
+    for (int i = 0; i < kt_batch_s::N_CLASS_STREAMS; ++i) {
+        if (b->cev[i]) cudaEventDestroy(b->cev[i]);
+        if (b->cs[i]) cudaStreamDestroy(b->cs[i]);
+    }
+    for (cudaLibrary_t lib : b->libs) {
+        cudaLibraryUnload(lib);
+    }
+    b->libs.clear();
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
     if (b->s0) cudaStreamDestroy(b->s0);
@@ -892,7 +1096,9 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
                const kt_pauli* strings, const double* coeffs, int32_t with_grad, kt_batch_s* B)
 {
     using C = typename CxT<T>::type;
-    const int qsmall = (sizeof(T) == 8) ? 12 : 13;
+    // shared-memory items: at most what fits (12 / 13 qubits), at least one
+    // below a forward tile, since an HBM item needs a whole tile of 2^K_FWD amplitudes
+    const int qsmall = std::max(K_FWD<T> - 1, std::min((sizeof(T) == 8) ? 12 : 13, tuning().batch_small_max_qubits));
     std::vector<int64_t> small, large;
     for (int64_t b = 0; b < n_items; ++b) {
         (items[b].n_qubits <= qsmall ? small : large).push_back(b);
@@ -1022,6 +1228,77 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         B->n_waves = large.empty() ? 0 : w + 1;
     }
 
+    // --- compiled classes: HBM items of at least batch_jit_min_qubits qubits
+    // whose plans have one structure share batched block kernels, one launch
+    // per block for all of them (single memory wave only)
+    struct Class
+    {
+        std::vector<size_t> members;           // large-item indices
+        int q {0};
+        int32_t cpi_f {1}, cpi_a {1};          // CTAs per item: forward blocks, adjoint blocks
+        std::vector<int32_t> rows;             // gradient rows of each adjoint block
+        std::vector<const void*> fk, bk;       // kernels
+        int32_t fsmem {0};
+        std::vector<int32_t> bsmem;
+    };
+    std::vector<Class> cls;
+    std::vector<int32_t> class_of(large.size(), -1);
+    const int jit_min = tuning().batch_jit_min_qubits;
+    if (jit_min > 0 && B->n_waves == 1 && !large.empty() && jit_available(nullptr)) {
+        std::unordered_map<uint64_t, int32_t> by_key;
+        for (size_t k = 0; k < large.size(); ++k) {
+            if (items[large[k]].n_qubits < jit_min) {
+                continue;
+            }
+            auto it = by_key.find(ips[k].key);
+            if (it == by_key.end() || cls[static_cast<size_t>(it->second)].members.size() >= 65535) {
+                it = by_key.insert_or_assign(ips[k].key, static_cast<int32_t>(cls.size())).first;
+                cls.emplace_back();
+            }
+            class_of[k] = it->second;
+            cls[static_cast<size_t>(it->second)].members.push_back(k);
+        }
+        std::vector<BatchPlanView> fv, bv;
+        for (Class& c : cls) {
+            const ItemPlan<T>& rep = ips[c.members.front()];
+            c.q = items[large[c.members.front()]].n_qubits;
+            c.cpi_f = ctas_per_item(c.members.size(), int64_t {1} << (c.q - K_FWD<T>));
+            c.cpi_a = ctas_per_item(c.members.size(), int64_t {1} << (c.q - K_BWD<T>));
+            for (const auto& r : rep.rows_of_block) {
+                c.rows.push_back(static_cast<int32_t>(r.size()));
+            }
+            fv.push_back(view_of(rep.fwd));
+            bv.push_back(view_of(rep.bwd));
+        }
+        std::vector<std::vector<const void*>> fk, bk;
+        std::vector<int32_t> fsm;
+        std::vector<std::vector<int32_t>> bsm;
+        if (!cls.empty()) {
+            if (jit_batch_compile(sizeof(T) == 8 ? KT_C128 : KT_C64, fv, bv, fk, bk, fsm, bsm, B->libs) == KT_OK) {
+                for (size_t c = 0; c < cls.size(); ++c) {
+                    cls[c].fk = fk[c];
+                    cls[c].bk = bk[c];
+                    cls[c].fsmem = fsm[c];
+                    cls[c].bsmem = bsm[c];
+                }
+            } else {
+                // run-time compilation failed: every item runs in the persistent kernel
+                for (cudaLibrary_t lib : B->libs) {
+                    cudaLibraryUnload(lib);
+                }
+                B->libs.clear();
+                cls.clear();
+                std::fill(class_of.begin(), class_of.end(), -1);
+                cudaGetLastError();
+            }
+        }
+    }
+    B->n_classes = static_cast<int64_t>(cls.size());
+    // per compiled item: its op records in the merged tables (per block), the
+    // Hamiltonian partials' base and each adjoint block's partials' base
+    std::vector<std::vector<int64_t>> item_fop(large.size()), item_bop(large.size()), item_pbase(large.size());
+    std::vector<int64_t> item_ebase(large.size(), 0);
+
     Plan<T> gf;
     Plan<T, FOpA<T>> gb;
     std::vector<BInst> insts(large.size());
@@ -1048,7 +1325,48 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         const int64_t fo0 = static_cast<int64_t>(gf.ops.size());
         append_plan(gf, ip.fwd);
         for (const auto& [lop, g] : ip.fpatch) {
-            patches.push_back(BPatch {TAB_FWD, ip.opcode[g], fo0 + lop, it.param_offset + ip.slot[g]});
+            patches.push_back(BPatch {TAB_FWD, ip.opcode[g], fo0 + lop, it.param_offset + ip.slot[g],
+                                      ip.fone[static_cast<size_t>(lop)], 0});
+        }
+        if (class_of[k] >= 0) {
+            // a compiled class's item: its blocks run as class launches, no jobs
+            const Class& c = cls[static_cast<size_t>(class_of[k])];
+            for (const auto& fb : ip.fwd.blocks) {
+                item_fop[k].push_back(fo0 + fb.op_begin);
+            }
+            alg += (1.0 + 2.0 * static_cast<double>(ip.fwd.blocks.size())) * state_bytes;  // |0...0>, then the blocks
+            item_ebase[k] = epart_size;
+            const int32_t n_chunks = static_cast<int32_t>(int64_t {1} << (c.q - K_FWD<T>));
+            esrc.push_back(ESrc {epart_size, n_chunks, 0, large[k]});
+            epart_size += n_chunks;
+            alg += (with_grad ? 2.0 : 1.0) * state_bytes;
+            if (with_grad) {
+                const int64_t bo0 = static_cast<int64_t>(gb.ops.size());
+                append_plan(gb, ip.bwd);
+                for (const auto& [lop, g] : ip.bpatch) {
+                    patches.push_back(BPatch {TAB_BWD, ip.opcode[g], bo0 + lop, it.param_offset + ip.slot[g],
+                                              ip.bone[static_cast<size_t>(lop)], 0});
+                }
+                const int64_t row0 = static_cast<int64_t>(row_param.size());
+                for (int32_t sl : ip.row_slot) {
+                    row_param.push_back(it.param_offset + sl);
+                }
+                row_src.resize(row_param.size() - static_cast<size_t>(small_rows_end));
+                for (size_t b = 0; b < ip.bwd.blocks.size(); ++b) {
+                    item_bop[k].push_back(bo0 + ip.bwd.blocks[b].op_begin);
+                    item_pbase[k].push_back(part_size);
+                    const auto& rows = ip.rows_of_block[b];
+                    for (size_t r = 0; r < rows.size(); ++r) {
+                        const int64_t grow = row0 + rows[r];
+                        row_src[static_cast<size_t>(grow - small_rows_end)] =
+                            RowSrc {part_size + static_cast<int64_t>(r) * c.cpi_a, c.cpi_a, 0};
+                    }
+                    part_size += static_cast<int64_t>(rows.size()) * c.cpi_a;
+                    alg += 4.0 * state_bytes;
+                }
+            }
+            ip = ItemPlan<T>();
+            continue;
         }
         for (size_t b = 0; b < ip.fwd.blocks.size(); ++b) {
             BJob j {};
@@ -1083,7 +1401,8 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
             const int64_t bo0 = static_cast<int64_t>(gb.ops.size());
             append_plan(gb, ip.bwd);
             for (const auto& [lop, g] : ip.bpatch) {
-                patches.push_back(BPatch {TAB_BWD, ip.opcode[g], bo0 + lop, it.param_offset + ip.slot[g]});
+                patches.push_back(BPatch {TAB_BWD, ip.opcode[g], bo0 + lop, it.param_offset + ip.slot[g],
+                                          ip.bone[static_cast<size_t>(lop)], 0});
             }
             const int64_t row0 = static_cast<int64_t>(row_param.size());
             for (int32_t s : ip.row_slot) {
@@ -1124,7 +1443,9 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
     {
         std::vector<std::vector<size_t>> by_wave(static_cast<size_t>(B->n_waves));
         for (size_t k = 0; k < large.size(); ++k) {
-            by_wave[static_cast<size_t>(wave_of[k])].push_back(k);
+            if (!chain[k].empty()) {  // compiled items have no jobs
+                by_wave[static_cast<size_t>(wave_of[k])].push_back(k);
+            }
         }
         for (size_t w = 0; w < by_wave.size(); ++w) {
             auto chain_cost = [&](size_t k) {
@@ -1194,6 +1515,35 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
     const size_t o_esrc = lay.add(esrc.size() * sizeof(ESrc));
     const size_t o_pfirst = lay.add(p_first.size() * sizeof(int64_t));
     const size_t o_prows = lay.add(p_rows.size() * sizeof(int64_t));
+    // compiled classes' launch arrays, 8-byte words per class: states, lambdas,
+    // item (BInst) indices, energy bases, then per forward block the items' op
+    // records, per adjoint block their op records and partials' bases
+    struct ClassWords
+    {
+        size_t a, l, list, ebase;
+        std::vector<size_t> fop, bop, pbase;
+    };
+    std::vector<ClassWords> cw(cls.size());
+    size_t n_words = 0;
+    for (size_t c = 0; c < cls.size(); ++c) {
+        const size_t n = cls[c].members.size();
+        const size_t k0 = cls[c].members.front();
+        cw[c].a = n_words;
+        cw[c].l = n_words + n;
+        cw[c].list = n_words + 2 * n;
+        cw[c].ebase = n_words + 3 * n;
+        n_words += 4 * n;
+        for (size_t b = 0; b < item_fop[k0].size(); ++b) {
+            cw[c].fop.push_back(n_words);
+            n_words += n;
+        }
+        for (size_t b = 0; b < item_bop[k0].size(); ++b) {
+            cw[c].bop.push_back(n_words);
+            cw[c].pbase.push_back(n_words + n);
+            n_words += 2 * n;
+        }
+    }
+    const size_t o_cls = lay.add(n_words * sizeof(uint64_t));
     const size_t upload_end = lay.size;  // everything above is uploaded once, here
     const size_t o_params = lay.add(static_cast<size_t>(n_params) * sizeof(double));
     const size_t o_part = lay.add(static_cast<size_t>(part_size) * sizeof(double));
@@ -1243,6 +1593,31 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         put(o_esrc, esrc.data(), esrc.size() * sizeof(ESrc));
         put(o_pfirst, p_first.data(), p_first.size() * sizeof(int64_t));
         put(o_prows, p_rows.data(), p_rows.size() * sizeof(int64_t));
+        if (n_words > 0) {
+            // device addresses: the arena's states and the merged op tables in this block
+            std::vector<uint64_t> words(n_words, 0);
+            const uint64_t arena0 = reinterpret_cast<uint64_t>(B->arena);
+            const uint64_t fops0 = reinterpret_cast<uint64_t>(B->meta) + o_fops;
+            const uint64_t bops0 = reinterpret_cast<uint64_t>(B->meta) + o_bops;
+            for (size_t c = 0; c < cls.size(); ++c) {
+                const auto& mem = cls[c].members;
+                for (size_t i = 0; i < mem.size(); ++i) {
+                    const size_t k = mem[i];
+                    words[cw[c].a + i] = arena0 + static_cast<uint64_t>(insts[k].psi) * sizeof(C);
+                    words[cw[c].l + i] = arena0 + static_cast<uint64_t>(insts[k].lam) * sizeof(C);
+                    words[cw[c].list + i] = static_cast<uint64_t>(k);
+                    words[cw[c].ebase + i] = static_cast<uint64_t>(item_ebase[k]);
+                    for (size_t b = 0; b < cw[c].fop.size(); ++b) {
+                        words[cw[c].fop[b] + i] = fops0 + static_cast<uint64_t>(item_fop[k][b]) * sizeof(FOp<T>);
+                    }
+                    for (size_t b = 0; b < cw[c].bop.size(); ++b) {
+                        words[cw[c].bop[b] + i] = bops0 + static_cast<uint64_t>(item_bop[k][b]) * sizeof(FOpA<T>);
+                        words[cw[c].pbase[b] + i] = static_cast<uint64_t>(item_pbase[k][b]);
+                    }
+                }
+            }
+            put(o_cls, words.data(), n_words * sizeof(uint64_t));
+        }
         KT_CUDA(cudaMemcpy(B->meta, host.data(), upload_end, cudaMemcpyHostToDevice));
     }
     KT_CUDA(cudaMallocHost(reinterpret_cast<void**>(&B->h_params),
@@ -1252,6 +1627,11 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
     KT_CUDA(cudaStreamCreateWithFlags(&B->s1, cudaStreamNonBlocking));
     KT_CUDA(cudaEventCreateWithFlags(&B->ev_fork, cudaEventDisableTiming));
     KT_CUDA(cudaEventCreateWithFlags(&B->ev_join, cudaEventDisableTiming));
+    const int n_cs = std::min<int>(kt_batch_s::N_CLASS_STREAMS, static_cast<int>(cls.size()));
+    for (int i = 0; i < n_cs; ++i) {
+        KT_CUDA(cudaStreamCreateWithFlags(&B->cs[i], cudaStreamNonBlocking));
+        KT_CUDA(cudaEventCreateWithFlags(&B->cev[i], cudaEventDisableTiming));
+    }
 
     char* M = static_cast<char*>(B->meta);
     auto at = [&](size_t off) { return static_cast<void*>(M + off); };
@@ -1334,7 +1714,63 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         ++launches;
     }
     chk(cudaEventRecord(B->ev_join, s1));
+    // compiled classes: one chain per class (|0...0>, forward blocks, lambda = H psi
+    // and the energy partials, adjoint blocks), the classes spread over streams
+    for (int i = 0; i < n_cs; ++i) {
+        chk(cudaStreamWaitEvent(B->cs[i], B->ev_fork, 0));
+    }
+    {
+        uint64_t* words_dev = static_cast<uint64_t*>(at(o_cls));
+        C* arena = static_cast<C*>(B->arena);
+        for (size_t c = 0; c < cls.size(); ++c) {
+            const Class& cl = cls[c];
+            cudaStream_t st = B->cs[c % static_cast<size_t>(n_cs)];
+            const unsigned n = static_cast<unsigned>(cl.members.size());
+            void* a_list = words_dev + cw[c].a;
+            void* l_list = words_dev + cw[c].l;
+            k_batch_basis<C><<<dim3(static_cast<unsigned>(cl.cpi_f), n), B_THREADS, 0, st>>>(
+                static_cast<void* const*>(a_list), uint64_t {1} << cl.q);
+            chk(cudaGetLastError());
+            ++launches;
+            unsigned long long nt_f = 1ULL << (cl.q - K_FWD<T>);
+            for (size_t b = 0; b < cl.fk.size(); ++b) {
+                void* o_list = words_dev + cw[c].fop[b];
+                void* args[] = {&a_list, &o_list, &nt_f};
+                chk(cudaLaunchKernel(cl.fk[b], dim3(static_cast<unsigned>(cl.cpi_f), n), dim3(B_THREADS), args,
+                                     static_cast<size_t>(cl.fsmem), st));
+                ++launches;
+            }
+            const uint64_t n_chunks = uint64_t {1} << (cl.q - K_FWD<T>);
+            const unsigned ham_grid = static_cast<unsigned>(
+                std::min<uint64_t>(n_chunks * n, static_cast<uint64_t>(4 * sm_count())));
+            k_batch_ham_items<T><<<ham_grid, B_THREADS, ham_smem, st>>>(
+                arena, static_cast<const BInst*>(at(o_insts)), reinterpret_cast<const int64_t*>(words_dev + cw[c].list),
+                reinterpret_cast<const int64_t*>(words_dev + cw[c].ebase), static_cast<const BStr*>(at(o_strs)),
+                static_cast<double*>(at(o_epart)), K_FWD<T>, with_grad, static_cast<uint64_t>(n), n_chunks);
+            chk(cudaGetLastError());
+            ++launches;
+            if (with_grad) {
+                unsigned long long nt_a = 1ULL << (cl.q - K_BWD<T>);
+                double* part = static_cast<double*>(at(o_part));
+                for (size_t b = 0; b < cl.bk.size(); ++b) {
+                    void* o_list = words_dev + cw[c].bop[b];
+                    void* pbase = words_dev + cw[c].pbase[b];
+                    int rows = cl.rows[b];
+                    void* args[] = {&a_list, &l_list, &o_list, &pbase, &part, &nt_a, &rows};
+                    chk(cudaLaunchKernel(cl.bk[b], dim3(static_cast<unsigned>(cl.cpi_a), n), dim3(B_THREADS), args,
+                                         static_cast<size_t>(cl.bsmem[b]), st));
+                    ++launches;
+                }
+            }
+        }
+    }
+    for (int i = 0; i < n_cs; ++i) {
+        chk(cudaEventRecord(B->cev[i], B->cs[i]));
+    }
     for (size_t w = 0; w < q_init.size(); ++w) {
+        if (wave_jobs[w] == 0) {
+            continue;  // every item of the wave runs compiled kernels
+        }
         BArgs<T> a {};
         a.arena = static_cast<C*>(B->arena);
         a.jobs = static_cast<const BJob*>(at(o_jobs));
@@ -1362,6 +1798,9 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
         ++launches;
     }
     chk(cudaStreamWaitEvent(s0, B->ev_join, 0));
+    for (int i = 0; i < n_cs; ++i) {
+        chk(cudaStreamWaitEvent(s0, B->cev[i], 0));
+    }
     if (!esrc.empty()) {
         const int64_t n = static_cast<int64_t>(esrc.size());
         k_batch_energy<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s0>>>(
@@ -1398,6 +1837,10 @@ int32_t create(const kt_batch_item* items, int64_t n_items, const kt_gate* gates
     B->alg_bytes = alg;
     B->n_small = static_cast<int64_t>(small.size());
     B->n_large = static_cast<int64_t>(large.size());
+    B->n_compiled_items = 0;
+    for (const Class& c : cls) {
+        B->n_compiled_items += static_cast<int64_t>(c.members.size());
+    }
     return KT_OK;
 }
 
@@ -1508,6 +1951,16 @@ int32_t kt_batch_stats(kt_batch b, int64_t* small_items, int64_t* large_items, i
     if (launches) *launches = b->launches;
     if (alg_bytes) *alg_bytes = b->alg_bytes;
     if (device_bytes) *device_bytes = static_cast<double>(b->device_bytes);
+    return KT_OK;
+}
+
+int32_t kt_batch_compiled(kt_batch b, int64_t* classes, int64_t* items)
+{
+    if (b == nullptr) {
+        return kt::fail(KT_ERR_INVALID, "batch is NULL");
+    }
+    if (classes) *classes = b->n_classes;
+    if (items) *items = b->n_compiled_items;
     return KT_OK;
 }
 

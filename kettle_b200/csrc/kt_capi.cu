@@ -712,6 +712,30 @@ int32_t kt_dm_apply(kt_dm dm, const kt_gate* gates, int64_t n_gates, const doubl
     });
 }
 
+int32_t kt_dm_prepare(kt_dm dm, const kt_gate* gates, int64_t n_gates, const double* params, int64_t n_params)
+{
+    return guard([&]() -> int32_t {
+        if (dm == nullptr) {
+            return invalid("null handle");
+        }
+        if (n_gates < 0 || (n_gates > 0 && gates == nullptr)) {
+            return invalid("bad gate array");
+        }
+        std::vector<kt::LGate> lg;
+        if (const int32_t rc = kt::lower_gates(gates, n_gates, params, n_params, dm->n, lg); rc != KT_OK) {
+            return rc;
+        }
+        // the same 2n-bit gate stream kt_dm_apply plans
+        std::vector<kt::LGate> both;
+        both.reserve(2 * lg.size());
+        for (const auto& g : lg) {
+            both.push_back(g);
+            both.push_back(kt::conj_shifted(g, dm->n));
+        }
+        return kt::jit_prepare(dm->st, both);
+    });
+}
+
 int32_t kt_dm_expect(kt_dm dm, const kt_pauli* strings, int64_t n_strings, const double* coeffs, double* out_terms,
                      double* out_total)
 {

@@ -27,6 +27,7 @@
 //  * Loads and stores use a layout whose lane bits are the L lowest qubits:
 //    each warp instruction touches whole 128-byte lines.
 #include <algorithm>
+#include <cstddef>
 #include <complex>
 #include <cmath>
 #include <cstdio>
@@ -408,6 +409,39 @@ inline bool jit_async(int K, size_t elem_bytes)
     return tuning().jit_async_load != 0 && 2 * (size_t {1} << K) * elem_bytes <= 227 * 1024;
 }
 
+// Batched block kernels (the batch engine's HBM items of one circuit
+// structure): one launch runs a block on many states, blockIdx.y selecting
+// the item.  Every item has its own state and its own op records (the batch
+// writes their matrices from the parameters on the device), so the
+// generated code reads an op's matrix from the item's record at a literal
+// byte offset instead of a kernel parameter; scaled forms, which need the
+// matrices on the host, are off.  Set for the duration of a generation.
+struct JitBatch
+{
+    size_t op_bytes {0};  // bytes of one op record
+    size_t m_off {0};     // byte offset of the matrix in a record
+};
+thread_local const JitBatch* tl_batch = nullptr;
+
+struct JitBatchScope
+{
+    explicit JitBatchScope(const JitBatch* b) { tl_batch = b; }
+    ~JitBatchScope() { tl_batch = nullptr; }
+    JitBatchScope(const JitBatchScope&) = delete;
+    JitBatchScope& operator=(const JitBatchScope&) = delete;
+};
+
+// the text of matrix entry e of op j of the block being generated
+template <typename T>
+std::string jit_mref(int j, int e)
+{
+    if (tl_batch != nullptr) {
+        const size_t off = static_cast<size_t>(j) * tl_batch->op_bytes + tl_batch->m_off + static_cast<size_t>(e) * sizeof(T);
+        return "kt_ldm<$T>(ob, " + std::to_string(off) + "u)";
+    }
+    return "M.m[" + std::to_string(8 * j + e) + "]";
+}
+
 // Scaled forms of the run-time compiled blocks (complex128, jit_scale_ops).
 // An uncontrolled op may run divided by its m00 != 0:
 //   1 / 2  real with m11 = +m00 / -m00:  [[1, p], [q, +-1]]
@@ -425,7 +459,8 @@ int jit_scaled(const FOp<T>& op)
     if constexpr (!std::is_same<T, double>::value) {
         return 0;
     } else {
-        if (tuning().jit_scale_ops == 0 || op.cslot != NO_SLOT || op.cthr != 0 || op.cglob != 0) {
+        if (tuning().jit_scale_ops == 0 || tl_batch != nullptr || op.cslot != NO_SLOT || op.cthr != 0 ||
+            op.cglob != 0) {
             return 0;
         }
         const bool nz = op.m[0] != 0.0 || op.m[1] != 0.0;
@@ -462,7 +497,7 @@ JitScale jit_scale_plan(const Plan<T>& plan, size_t b)
     if constexpr (!std::is_same<T, double>::value) {
         return js;
     }
-    if (tuning().jit_scale_ops == 0) {
+    if (tuning().jit_scale_ops == 0 || tl_batch != nullptr) {
         return js;
     }
     for (int j = 0; j < nops && js.sink < 0; ++j) {
@@ -502,8 +537,8 @@ void jit_emit_op(std::string& s, const FOp<T>& op, int j, int sc)
         return std::string("f.crt = ") + std::to_string(cs) + "; f.template run<" + std::to_string(ts) + ", " +
                (cs < 0 ? "-1" : "CS_RT") + ">();";
     };
-    // the op's matrix entries: the kernel's constant-bank parameter
-    auto m = [&](int e) { return "M.m[" + std::to_string(8 * j + e) + "]"; };
+    // the op's matrix entries: the kernel's constant-bank parameter (batched: the item's op record)
+    auto m = [&](int e) { return jit_mref<T>(j, e); };
     auto cx = [&](int e) { return "make_cx<$T>(" + m(e) + ", " + m(e + 1) + ")"; };
     std::string guard;
     if (op.cglob != 0) {
@@ -782,6 +817,8 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm, con
     if (tma) {
         s += "(const __grid_constant__ kt::KtTmap tm, void* a_, unsigned long long n_tiles, unsigned int* err_, "
              "const __grid_constant__ $M<" + std::to_string(8 * (nops + (scale_slot ? 1 : 0))) + "> M)\n{\n";
+    } else if (tl_batch != nullptr) {
+        s += "(void* const* a_list, const unsigned char* const* o_list, unsigned long long n_tiles)\n{\n";
     } else {
         s += std::string("(void* a_, unsigned long long n_tiles, ") + (norm ? "kt::NormArgs na, " : "") +
              "const __grid_constant__ $M<" + std::to_string(8 * (nops + (scale_slot ? 1 : 0))) + "> M)\n{\n";
@@ -858,7 +895,12 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm, con
         s += "    const uint32_t t = threadIdx.x & " + std::to_string(GT - 1) + "u;\n";
         s += "    C* sm = nullptr;\n";
     } else {
-        s += "    C* __restrict__ a = static_cast<C*>(a_);\n";
+        if (tl_batch != nullptr) {
+            s += "    C* __restrict__ a = static_cast<C*>(a_list[blockIdx.y]);\n";
+            s += "    const unsigned char* __restrict__ ob = o_list[blockIdx.y];\n";
+        } else {
+            s += "    C* __restrict__ a = static_cast<C*>(a_);\n";
+        }
         s += "    extern __shared__ __align__(16) unsigned char smem_raw[];\n";
         s += "    C* sm = reinterpret_cast<C*>(smem_raw);\n";
         s += "    const uint32_t t = threadIdx.x;\n";
@@ -1087,9 +1129,7 @@ std::string jit_block_body(const Plan<T>& plan, size_t b, int RB, bool norm, con
                 const FOp<T>& op = plan.ops[static_cast<size_t>(o)];
                 const int j = o - fb.op_begin;
                 const bool one_sided = op.kind == OP_DIAG1 || jit_scale_code(plan, b, j, js) == 5;
-                auto cx = [&](int e) {
-                    return "make_cx<$T>(M.m[" + std::to_string(8 * j + e) + "], M.m[" + std::to_string(8 * j + e + 1) + "])";
-                };
+                auto cx = [&](int e) { return "make_cx<$T>(" + jit_mref<T>(j, e) + ", " + jit_mref<T>(j, e + 1) + ")"; };
                 std::string cond;
                 if (op.cglob != 0) {
                     cond += "((base & " + jit_hex(op.cglob) + ") == " + jit_hex(op.cglob) + ")";
@@ -1263,6 +1303,10 @@ constexpr const char* JIT_PRELUDE =
     "    for (int i = 0; i < N; ++i) {\n"
     "        asm volatile(\"\" : \"+f\"(v[i].x), \"+f\"(v[i].y));\n"
     "    }\n"
+    "}\n\n"
+    "// a matrix entry of an item's op record (batched block kernels)\n"
+    "template <typename T>\n__device__ __forceinline__ T kt_ldm(const unsigned char* p, unsigned off)\n{\n"
+    "    return __ldg(reinterpret_cast<const T*>(p + off));\n"
     "}\n\n";
 
 constexpr size_t JIT_MAX_KERNELS = 4096;
@@ -1946,11 +1990,23 @@ std::string jit_adj_body(const Plan<T, FOpA<T>>& plan, size_t b, int RB)
     };
     std::string s;
     s.reserve(32768);
-    s += "(void* psi_, void* lam_, unsigned long long n_tiles, double* partial, int n_rows, const __grid_constant__ $M<" +
-         std::to_string(8 * nops) + "> M)\n{\n";
+    if (tl_batch != nullptr) {
+        s += "(void* const* p_list, void* const* l_list, const unsigned char* const* o_list, const long long* pbase, "
+             "double* partial, unsigned long long n_tiles, int n_rows)\n{\n";
+    } else {
+        s += "(void* psi_, void* lam_, unsigned long long n_tiles, double* partial, int n_rows, const __grid_constant__ $M<" +
+             std::to_string(8 * nops) + "> M)\n{\n";
+    }
     s += "    using namespace kt;\n    using C = $C;\n";
     s += "    constexpr int RB = " + std::to_string(RB) + ";\n";
-    s += "    C* __restrict__ psi = static_cast<C*>(psi_);\n    C* __restrict__ lam = static_cast<C*>(lam_);\n";
+    if (tl_batch != nullptr) {
+        s += "    C* __restrict__ psi = static_cast<C*>(p_list[blockIdx.y]);\n"
+             "    C* __restrict__ lam = static_cast<C*>(l_list[blockIdx.y]);\n"
+             "    const unsigned char* __restrict__ ob = o_list[blockIdx.y];\n"
+             "    partial += pbase[blockIdx.y];\n";
+    } else {
+        s += "    C* __restrict__ psi = static_cast<C*>(psi_);\n    C* __restrict__ lam = static_cast<C*>(lam_);\n";
+    }
     s += "    extern __shared__ __align__(16) unsigned char smem_raw[];\n";
     s += "    C* smp = reinterpret_cast<C*>(smem_raw);\n";
     s += "    C* sml = smp + " + std::to_string(1 << fb.K) + ";\n";
@@ -2448,6 +2504,144 @@ int32_t jit_compile_only_t(int n, const std::vector<LGate>& gates, int64_t* n_ke
 }
 
 }  // namespace
+
+namespace
+{
+
+// a plan of the batch engine rebuilt from its raw records (same types in both units)
+template <typename T, typename O>
+bool plan_from_view(const BatchPlanView& v, Plan<T, O>& plan)
+{
+    if (v.rec_bytes[0] != static_cast<int64_t>(sizeof(FBlock)) || v.rec_bytes[1] != static_cast<int64_t>(sizeof(FPhase)) ||
+        v.rec_bytes[2] != static_cast<int64_t>(sizeof(O))) {
+        return false;
+    }
+    plan.blocks.resize(static_cast<size_t>(v.n_blocks));
+    plan.phases.resize(static_cast<size_t>(v.n_phases));
+    plan.ops.resize(static_cast<size_t>(v.n_ops));
+    if (v.n_blocks > 0) std::memcpy(plan.blocks.data(), v.blocks, plan.blocks.size() * sizeof(FBlock));
+    if (v.n_phases > 0) std::memcpy(plan.phases.data(), v.phases, plan.phases.size() * sizeof(FPhase));
+    if (v.n_ops > 0) std::memcpy(static_cast<void*>(plan.ops.data()), v.ops, plan.ops.size() * sizeof(O));
+    return true;
+}
+
+template <typename T>
+int32_t jit_batch_compile_t(const std::vector<BatchPlanView>& fwd, const std::vector<BatchPlanView>& bwd,
+                            std::vector<std::vector<const void*>>& fk, std::vector<std::vector<const void*>>& bk,
+                            std::vector<int32_t>& fwd_smem, std::vector<std::vector<int32_t>>& bwd_smem,
+                            std::vector<cudaLibrary_t>& libs)
+{
+    using C = typename CxT<T>::type;
+    const std::string bounds = "__launch_bounds__(256, 2)";
+    std::vector<std::string> texts;          // unique kernel bodies (launch bounds first)
+    std::vector<int32_t> smem;               // dynamic shared memory of each
+    std::vector<char> is_adj;
+    std::unordered_map<std::string, size_t> index;
+    auto intern = [&](std::string text, int32_t bytes, bool adj) {
+        auto it = index.find(text);
+        if (it != index.end()) {
+            smem[it->second] = std::max(smem[it->second], bytes);
+            return it->second;
+        }
+        const size_t i = texts.size();
+        index.emplace(text, i);
+        texts.push_back(std::move(text));
+        smem.push_back(bytes);
+        is_adj.push_back(adj ? 1 : 0);
+        return i;
+    };
+    std::vector<std::vector<size_t>> fidx(fwd.size()), bidx(bwd.size());
+    fwd_smem.assign(fwd.size(), 0);
+    bwd_smem.assign(bwd.size(), {});
+    {
+        const JitBatch jb {sizeof(FOp<T>), offsetof(FOp<T>, m)};
+        JitBatchScope scope(&jb);
+        for (size_t c = 0; c < fwd.size(); ++c) {
+            Plan<T> plan;
+            if (!plan_from_view(fwd[c], plan)) {
+                set_error(KT_ERR_INVALID, "batched block kernels: plan record sizes differ");
+                return KT_ERR_INVALID;
+            }
+            for (size_t b = 0; b < plan.blocks.size(); ++b) {
+                const int K = plan.blocks[b].K;
+                const int32_t bytes = static_cast<int32_t>((size_t {1} << K) * sizeof(C) * (jit_async(K, sizeof(C)) ? 2 : 1));
+                fwd_smem[c] = std::max(fwd_smem[c], bytes);
+                fidx[c].push_back(intern(bounds + jit_block_body<T>(plan, b, Cfg<T>::RB, false, nullptr), bytes, false));
+            }
+        }
+    }
+    {
+        const JitBatch jb {sizeof(FOpA<T>), offsetof(FOpA<T>, m)};
+        JitBatchScope scope(&jb);
+        for (size_t c = 0; c < bwd.size(); ++c) {
+            Plan<T, FOpA<T>> plan;
+            if (!plan_from_view(bwd[c], plan)) {
+                set_error(KT_ERR_INVALID, "batched block kernels: plan record sizes differ");
+                return KT_ERR_INVALID;
+            }
+            for (size_t b = 0; b < plan.blocks.size(); ++b) {
+                const FBlock& fb = plan.blocks[b];
+                int rows = 0;
+                for (int o = fb.op_begin; o < fb.op_end; ++o) {
+                    rows = std::max(rows, plan.ops[static_cast<size_t>(o)].row + 1);
+                }
+                const int32_t bytes = static_cast<int32_t>(2 * (size_t {1} << fb.K) * sizeof(C) +
+                                                           static_cast<size_t>(std::max(rows, 1)) * ADJ_WARPS * sizeof(double));
+                bwd_smem[c].push_back(bytes);
+                bidx[c].push_back(intern(bounds + jit_adj_body<T>(plan, b, CfgA<T>::RB), bytes, true));
+            }
+        }
+    }
+    // programs of a few kernels each, compiled on parallel host threads
+    const size_t per_prog = 4;
+    const size_t n_prog = std::max<size_t>(1, (texts.size() + per_prog - 1) / per_prog);
+    std::vector<std::string> sources(n_prog, JIT_PRELUDE);
+    std::vector<std::vector<std::string>> names(n_prog);
+    for (size_t i = 0; i < texts.size(); ++i) {
+        const size_t w = i / per_prog;
+        const std::string name = std::string(is_adj[i] ? "kt_jab" : "kt_jbb") + std::to_string(i);
+        sources[w] += "extern \"C\" __global__ void " + bounds + " " + name + texts[i].substr(bounds.size()) + "\n";
+        names[w].push_back(name);
+    }
+    std::vector<std::vector<const void*>> got;
+    if (!texts.empty()) {
+        if (const int32_t rc = jit_compile(sources, names, got, true, &libs); rc != KT_OK) {
+            return rc;
+        }
+    }
+    std::vector<const void*> handle(texts.size());
+    int dev = 0;
+    KT_CUDA(cudaGetDevice(&dev));
+    for (size_t i = 0; i < texts.size(); ++i) {
+        handle[i] = got[i / per_prog][i % per_prog];
+        KT_CUDA(cudaKernelSetAttributeForDevice(reinterpret_cast<cudaKernel_t>(const_cast<void*>(handle[i])),
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem[i], dev));
+    }
+    fk.assign(fwd.size(), {});
+    bk.assign(bwd.size(), {});
+    for (size_t c = 0; c < fwd.size(); ++c) {
+        for (size_t i : fidx[c]) {
+            fk[c].push_back(handle[i]);
+        }
+    }
+    for (size_t c = 0; c < bwd.size(); ++c) {
+        for (size_t i : bidx[c]) {
+            bk[c].push_back(handle[i]);
+        }
+    }
+    return KT_OK;
+}
+
+}  // namespace
+
+int32_t jit_batch_compile(int32_t dtype, const std::vector<BatchPlanView>& fwd, const std::vector<BatchPlanView>& bwd,
+                          std::vector<std::vector<const void*>>& fk, std::vector<std::vector<const void*>>& bk,
+                          std::vector<int32_t>& fwd_smem, std::vector<std::vector<int32_t>>& bwd_smem,
+                          std::vector<cudaLibrary_t>& libs)
+{
+    return dtype == KT_C128 ? jit_batch_compile_t<double>(fwd, bwd, fk, bk, fwd_smem, bwd_smem, libs)
+                            : jit_batch_compile_t<float>(fwd, bwd, fk, bk, fwd_smem, bwd_smem, libs);
+}
 
 int32_t jit_adjoint_compile_only(int n, int32_t dtype, const std::vector<AdjGate>& gates, int64_t* n_kernels)
 {

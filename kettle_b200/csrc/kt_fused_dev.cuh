@@ -549,6 +549,19 @@ __device__ __forceinline__ double re_cj(double2 a, double2 b)
     return a.x * b.x + a.y * b.y;  // Re(conj(a) b)
 }
 
+// complex64 states: a thread's terms of one op are formed and summed in FP32
+// (the amplitudes carry FP32 precision; at most 2^RB terms), and only that
+// sum joins the FP64 accumulator
+__device__ __forceinline__ float im_cj(float2 a, float2 b)
+{
+    return a.x * b.y - a.y * b.x;
+}
+
+__device__ __forceinline__ float re_cj(float2 a, float2 b)
+{
+    return a.x * b.x + a.y * b.y;
+}
+
 // generator on register slot S (control register slot CS)
 template <typename T, int RB, int GENK>
 struct GradRegF
@@ -561,23 +574,26 @@ struct GradRegF
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
+        using R = T;  // the terms' precision: FP64 for complex128, FP32 for complex64
+        R sum = 0;
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
             if (lower_of_pair<S, CS>(i, crt)) {
                 const int j = i | (1 << S);
-                const double2 l0 = to_d2(l[i]), l1 = to_d2(l[j]);
-                const double2 p0 = to_d2(p[i]), p1 = to_d2(p[j]);
+                const C l0 = l[i], l1 = l[j];
+                const C p0 = p[i], p1 = p[j];
                 if constexpr (GENK == GEN_X) {
-                    acc += im_cj(l0, p1) + im_cj(l1, p0);
+                    sum += im_cj(l0, p1) + im_cj(l1, p0);
                 } else if constexpr (GENK == GEN_Y) {
-                    acc += re_cj(l1, p0) - re_cj(l0, p1);
+                    sum += re_cj(l1, p0) - re_cj(l0, p1);
                 } else if constexpr (GENK == GEN_Z) {
-                    acc += im_cj(l0, p0) - im_cj(l1, p1);
+                    sum += im_cj(l0, p0) - im_cj(l1, p1);
                 } else {
-                    acc -= im_cj(l1, p1);
+                    sum -= im_cj(l1, p1);
                 }
             }
         }
+        acc += static_cast<double>(sum);
     }
 };
 
@@ -594,12 +610,14 @@ struct GradAllF
     template <int S, int CS>
     __device__ __forceinline__ void run()
     {
+        T sum = 0;
 #pragma unroll
         for (int i = 0; i < (1 << RB); ++i) {
             if (ctrl_on<CS>(i, crt)) {
-                acc += im_cj(to_d2(l[i]), to_d2(p[i]));
+                sum += im_cj(l[i], p[i]);
             }
         }
+        acc += static_cast<double>(sum);
     }
 };
 

@@ -138,8 +138,36 @@ bool jit_available(std::string* why);
 // host threads a run-time compile uses
 int jit_threads();
 // (load = false: compile only, no device needed)
+// (owned: the loaded programs go there for the caller to unload, instead of
+// the process-wide list jit_unload_all empties)
 int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<std::vector<std::string>>& names,
-                    std::vector<std::vector<const void*>>& kernels, bool load = true);
+                    std::vector<std::vector<const void*>>& kernels, bool load = true,
+                    std::vector<cudaLibrary_t>* owned = nullptr);
+// A plan of the batch engine handed to the generator as raw records of the
+// fused planner's types (FBlock, FPhase, and FOp<T> or FOpA<T>), which both
+// translation units define alike; rec_bytes guards against a mismatch.
+struct BatchPlanView
+{
+    const void* blocks {nullptr};
+    int64_t n_blocks {0};
+    const void* phases {nullptr};
+    int64_t n_phases {0};
+    const void* ops {nullptr};
+    int64_t n_ops {0};
+    int64_t rec_bytes[3] {0, 0, 0};  // sizeof FBlock, FPhase, op record
+};
+// Batched compiled block kernels of the batch engine: for every forward plan
+// one kernel per block, (void* const* states, const unsigned char* const*
+// op_records, unsigned long long n_tiles), blockIdx.y the item; for every
+// adjoint plan one per block, (void* const* psi, void* const* lambda, const
+// unsigned char* const* op_records, const long long* partial_base, double*
+// partial, unsigned long long n_tiles, int n_rows).  Identical kernels are
+// compiled once; fwd_smem / bwd_smem get each kernel's dynamic shared memory
+// (set as its limit on the current device); the programs go to `libs`.
+int32_t jit_batch_compile(int32_t dtype, const std::vector<BatchPlanView>& fwd, const std::vector<BatchPlanView>& bwd,
+                          std::vector<std::vector<const void*>>& fk, std::vector<std::vector<const void*>>& bk,
+                          std::vector<int32_t>& fwd_smem, std::vector<std::vector<int32_t>>& bwd_smem,
+                          std::vector<cudaLibrary_t>& libs);
 // host-only: plan an apply and compile its block kernels without loading them
 int32_t jit_compile_only(int n, int32_t dtype, const std::vector<LGate>& gates, int64_t* n_kernels);
 // host-only: plan the fused adjoint sweep `gates` and compile its block kernels
@@ -223,6 +251,10 @@ struct Tuning
     int jit_scale_ops {1};       // complex128 blocks: uncontrolled real / RX-like ops divided by m00 (one FMA per component)
     int jit_remat {1};           // 1: thread-index terms recomputed every tile, not held across the tile loop
     long long batch_spin_limit {1LL << 25};  // polls of the batch queue before a CTA gives up (~10 s)
+    int batch_small_max_qubits {13};         // batch items of at most this many qubits run in shared memory
+                                             // (capped at 12 for complex128, 13 for complex64: what fits)
+    int batch_jit_min_qubits {13};           // batch HBM items of at least this many qubits run compiled
+                                             // block kernels shared by every item of one plan structure (0: never)
     int adjoint_jit {2};         // fused adjoint blocks as run-time compiled kernels: 0 never, 1 always,
                                  // 2 from the second backward sweep of a circuit structure
     int jit_lean_sync {1};       // 1: compiled blocks drop a transpose's second barrier where the phase stores where it loaded

@@ -169,7 +169,7 @@ void jit_unload_all()
 }
 
 int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<std::vector<std::string>>& names,
-                    std::vector<std::vector<const void*>>& kernels, bool load)
+                    std::vector<std::vector<const void*>>& kernels, bool load, std::vector<cudaLibrary_t>* owned)
 {
     std::string why;
     if (!jit_available(&why)) {
@@ -236,7 +236,9 @@ int32_t jit_compile(const std::vector<std::string>& sources, const std::vector<s
         }
         cudaLibrary_t lib = nullptr;
         KT_CUDA(cudaLibraryLoadData(&lib, cubins[i].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
-        {
+        if (owned != nullptr) {
+            owned->push_back(lib);  // the caller unloads it (jit_unload_all leaves it alone)
+        } else {
             std::lock_guard<std::mutex> lock(g_libs_mutex);
             g_libs.push_back(lib);
         }

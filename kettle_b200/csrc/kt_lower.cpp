@@ -112,6 +112,10 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.jit_tma_stages = static_cast<int>(std::max(2LL, std::min(4LL, v)));
     } else if (name == "batch_spin_limit") {
         t.batch_spin_limit = std::max(1LL, std::min(1000000000000LL, v));
+    } else if (name == "batch_small_max_qubits") {
+        t.batch_small_max_qubits = static_cast<int>(std::max(0LL, std::min(13LL, v)));
+    } else if (name == "batch_jit_min_qubits") {
+        t.batch_jit_min_qubits = static_cast<int>(std::max(0LL, std::min(64LL, v)));
     } else if (name == "jit_scale_ops") {
         t.jit_scale_ops = (v != 0) ? 1 : 0;
     } else if (name == "plan_schedule") {
@@ -209,6 +213,10 @@ bool tuning_get(const char* name, long long* value)
         *value = t.jit_tma_stages;
     } else if (n == "batch_spin_limit") {
         *value = t.batch_spin_limit;
+    } else if (n == "batch_small_max_qubits") {
+        *value = t.batch_small_max_qubits;
+    } else if (n == "batch_jit_min_qubits") {
+        *value = t.batch_jit_min_qubits;
     } else if (n == "jit_scale_ops") {
         *value = t.jit_scale_ops;
     } else if (n == "plan_schedule") {

@@ -1,8 +1,9 @@
 """Batch engine (kt_batch) against the single-circuit adjoint path, item by
 item: same energies and gradients (1e-10, complex128) for items that run in
-shared memory and items that run from HBM in the persistent work-queue
-kernel, across graph replays with new parameters, with shared parameter
-slots, without gradients, and in complex64 (1e-3 of complex128)."""
+shared memory, items that run from HBM in the persistent work-queue kernel
+and items that run run-time compiled block kernels shared by their plan
+structure class, across graph replays with new parameters, with shared
+parameter slots, without gradients, and in complex64 (1e-3 of complex128)."""
 import numpy as np
 import pytest
 
@@ -194,11 +195,14 @@ def test_batch_wait_limit_returns_timeout_and_the_context_stays_usable(engine):
     params = np.concatenate(params)
     items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
     old = capi.tuning_get("batch_spin_limit")
+    old_jit = capi.tuning_get("batch_jit_min_qubits")
     capi.tuning_set("batch_spin_limit", 2)
+    capi.tuning_set("batch_jit_min_qubits", 0)  # these items run in the persistent kernel
     try:
         b = capi.Batch(items, gates, strings, coeffs, n_params)
     finally:
         capi.tuning_set("batch_spin_limit", old)
+        capi.tuning_set("batch_jit_min_qubits", old_jit)
     with pytest.raises(capi.KettleError) as e:
         b.evaluate(params)
     assert e.value.code == capi.KT_ERR_TIMEOUT
@@ -209,3 +213,75 @@ def test_batch_wait_limit_returns_timeout_and_the_context_stays_usable(engine):
     want_e, want_g = _one_by_one(circuits, params)
     assert np.abs(energies - want_e).max() < 1e-10
     assert np.abs(grads - want_g).max() < 1e-10
+
+
+def _with_knob(name, value, fn):
+    old = capi.tuning_get(name)
+    capi.tuning_set(name, value)
+    try:
+        return fn()
+    finally:
+        capi.tuning_set(name, old)
+
+
+def _class_items(seed):
+    """HBM items in repeated structures: HEA at 14, 15 and 17 qubits (four
+    items each, own parameters and Hamiltonians), a mixed-gate circuit at 16
+    qubits twice, and single items at 13 and 14 qubits."""
+    circuits, params = [], []
+    spec = [(14, 3)] * 4 + [(15, 2)] * 4 + [(17, 4)] * 4 + [(13, 2), (14, 5)]
+    for k, (n, layers) in enumerate(spec):
+        g, p = W.hea(n, layers, seed=seed + k)
+        s, c = W.random_paulis(n, 10 + k, seed=seed + 50 + k)
+        circuits.append((n, g, p.size, s, c))
+        params.append(p)
+    g, p0 = _mixed(16, seed + 7)
+    for k in range(2):
+        s, c = W.random_paulis(16, 15, seed=seed + 90 + k)
+        circuits.append((16, g, p0.size, s, c))
+        params.append(p0 + 0.1 * k)
+    return circuits, np.concatenate(params)
+
+
+def test_batch_compiled_classes_match_single_path(engine):
+    """batch_jit_min_qubits = 14: every HBM item of 14 or more qubits runs the
+    batched compiled kernels of its class (the four-item HEA groups, the
+    mixed circuit pair, single items as classes of one); energies and
+    gradients equal the single-circuit path (1e-10) and the persistent
+    kernel's (1e-11), on two evaluations with new parameters."""
+    circuits, params = _class_items(300)
+    items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
+    b = _with_knob("batch_jit_min_qubits", 14, lambda: capi.Batch(items, gates, strings, coeffs, n_params))
+    st = b.stats()
+    assert st["compiled_items"] == 15 and st["compiled_classes"] == 5, st
+    p_ref = _with_knob("batch_jit_min_qubits", 0, lambda: capi.Batch(items, gates, strings, coeffs, n_params))
+    assert p_ref.stats()["compiled_items"] == 0
+    for shift in (0.0, 0.21):
+        p = params + shift
+        e, g = b.evaluate(p)
+        e0, g0 = p_ref.evaluate(p)
+        e1, g1 = _one_by_one(circuits, p)
+        assert np.abs(e - e1).max() < 1e-10 and np.abs(g - g1).max() < 1e-10
+        assert np.abs(e - e0).max() < 1e-11 and np.abs(g - g0).max() < 1e-11
+    b.close()
+    p_ref.close()
+
+
+def test_batch_compiled_without_gradients_and_complex64(engine):
+    circuits, params = _class_items(400)
+    items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
+    mk = lambda **kw: _with_knob("batch_jit_min_qubits", 15, lambda: capi.Batch(items, gates, strings, coeffs,
+                                                                                n_params, **kw))
+    b = mk(with_grad=False)
+    assert b.stats()["compiled_items"] == 10
+    e, g = b.evaluate(params)
+    assert g is None
+    e1, _ = _one_by_one(circuits, params)
+    assert np.abs(e - e1).max() < 1e-10
+    b.close()
+    b64 = mk(dtype=capi.KT_C64)
+    assert b64.stats()["compiled_items"] == 10
+    e64, g64 = b64.evaluate(params)
+    b64.close()
+    _, g1 = _one_by_one(circuits, params)
+    assert np.abs(e64 - e1).max() < 1e-3 and np.abs(g64 - g1).max() < 1e-3
