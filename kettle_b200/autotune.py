@@ -165,3 +165,88 @@ def autotune(n_qubits: int, dtype: int = capi.KT_C128, tune_qubits: int | None =
     if use_cache:
         save(n_qubits, dtype, best, table, path)
     return best
+
+
+# ---------------------------------------------------------------------------
+# Batches (kt_batch).  A batch reads its knobs when it is created: which HBM
+# items run the compiled class kernels (`batch_jit_min_qubits`, 0 = none: the
+# persistent kernel's interpreted blocks), how large an item may be to run
+# whole in shared memory (`batch_small_max_qubits`), and the fusion depth of
+# its blocks (`fused_max_ops`).  The tile is the 256-thread CTA's.  Every
+# candidate computes the same energies and gradients up to FP64 rounding.
+
+BATCH_KNOBS = ("batch_jit_min_qubits", "batch_small_max_qubits", "fused_max_ops")
+BATCH_GRID = {
+    "batch_jit_min_qubits": (13, 16, 0),
+    "batch_small_max_qubits": (13, 12),
+    "fused_max_ops": (128, 256),
+}
+
+
+def batch_candidates(grid: dict | None = None) -> list[dict]:
+    """All batch knob combinations of `grid` (defaults to BATCH_GRID), in a fixed order."""
+    g = dict(BATCH_GRID)
+    if grid:
+        g.update(grid)
+    return [dict(zip(BATCH_KNOBS, combo)) for combo in itertools.product(*(g[k] for k in BATCH_KNOBS))]
+
+
+def batch_gpu_timer(batch_args: tuple, params, dtype: int = capi.KT_C128, reps: int = 2):
+    """A timer that creates the batch (`batch_args` as capi.batch_items returns
+    them) with the given knobs, evaluates it once, and returns the mean seconds
+    of `reps` more evaluations (CUDA events; creation and compilation are not
+    timed)."""
+    import torch
+
+    items, gates, strings, coeffs, n_params = batch_args
+    stream = torch.cuda.Stream()
+
+    def timer(knobs: dict) -> float:
+        set_knobs(knobs)
+        b = capi.Batch(items, gates, strings, coeffs, n_params, dtype=dtype)
+        try:
+            b.set_stream(stream.cuda_stream)
+            b.evaluate(params)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                b.evaluate(params)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps / 1e3
+        finally:
+            b.close()
+
+    return timer
+
+
+def autotune_batch(batch_args: tuple, params, dtype: int = capi.KT_C128, grid: dict | None = None,
+                   use_cache: bool = True, path: pathlib.Path | None = None, timer=None) -> dict:
+    """Pick and set the fastest batch knobs for this batch's shape.  The cache
+    key is the GPU, the dtype and the item count with the largest item's qubits
+    (`batch|<items>x<max qubits>` in place of a qubit count)."""
+    items = batch_args[0]
+    shape = f"batch|{len(items)}x{int(max(items['n_qubits']))}"
+    if use_cache:
+        hit = load(shape, dtype, path)  # type: ignore[arg-type]
+        if hit is not None:
+            return hit
+    own = timer is None
+    if own:
+        timer = batch_gpu_timer(batch_args, params, dtype)
+    saved = {k: capi.tuning_get(k) for k in BATCH_KNOBS}
+
+    def timed(knobs: dict) -> float:
+        set_knobs(knobs)
+        return timer(knobs)
+
+    try:
+        best, table = search(timed, batch_candidates(grid))
+    finally:
+        set_knobs(saved)
+    set_knobs(best)
+    if use_cache:
+        save(shape, dtype, best, table, path)  # type: ignore[arg-type]
+    return best

@@ -23,7 +23,9 @@ Cases and the kernels they run:
   fused        k_fused (the precompiled fused-block interpreter)
   sweep        k_sweep (one pass per gate)
   state_ops    k_sv_tensor_product, k_sv_diag_expect, k_dm_block_norms, k_dm_collapse
-  batch        k_batch_persist, k_batch_small, k_batch_patch
+  batch        k_batch_persist, k_batch_small, k_batch_patch (batch_jit_min_qubits=0: the interpreted blocks)
+  batch_class  kt_jbb*, kt_jab*, k_batch_ham_items, k_batch_basis: one compiled class of 48 items
+               (20 qubits, 4 layers, 20 strings: 768 MiB of states per launch)
   dense_block  the tensor-core question: 40 random gates on qubits 0..4 of a
                complex64 state applied by the engine (one fused pass of
                compiled SIMT blocks) against the same 32 x 32 unitary applied
@@ -180,7 +182,22 @@ def case_state_ops(n, reps):
 def case_batch(n, reps):
     circuits, params = W.hea_batch(64, seed=15, qubits=(10, min(n, 20)), layers=(2, 6), n_strings=20)
     items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
+    old = capi.tuning_get("batch_jit_min_qubits")
+    capi.tuning_set("batch_jit_min_qubits", 0)
+    try:
+        b = capi.Batch(items, gates, strings, coeffs, n_params)
+    finally:
+        capi.tuning_set("batch_jit_min_qubits", old)
+    for _ in range(1 + reps):
+        b.evaluate(params)
+    b.close()
+
+
+def case_batch_class(n, reps):
+    circuits, params = W.hea_batch(48, seed=16, qubits=(20, 20), layers=(4, 4), n_strings=20)
+    items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
     b = capi.Batch(items, gates, strings, coeffs, n_params)
+    assert b.stats()["compiled_classes"] == 1
     for _ in range(1 + reps):
         b.evaluate(params)
     b.close()

@@ -55,3 +55,30 @@ def test_autotune_sets_caches_and_restores(tmp_path):
 def test_unknown_knob_is_rejected():
     with pytest.raises(capi.KettleError):
         capi.tuning_set("no_such_knob", 1)
+
+
+def test_batch_autotune_picks_sets_and_caches(tmp_path):
+    """The batch grid (compiled-class threshold, shared-memory limit, fusion
+    depth): every candidate is live while timed, the fastest is left set, the
+    table is cached under the batch's shape key, and the previous knobs can be
+    restored."""
+    import numpy as np
+    before = {k: capi.tuning_get(k) for k in AT.BATCH_KNOBS}
+    items = np.zeros(3, dtype=capi.BATCH_ITEM_DTYPE)
+    items["n_qubits"] = [12, 18, 20]
+    seen = []
+
+    def fake(knobs):
+        seen.append(dict(knobs))
+        assert {k: capi.tuning_get(k) for k in AT.BATCH_KNOBS} == knobs
+        return (2.0 if knobs["batch_jit_min_qubits"] == 0 else 1.0) + (0.5 if knobs["fused_max_ops"] == 128 else 0.0)
+
+    grid = {"batch_jit_min_qubits": (0, 16), "batch_small_max_qubits": (13,), "fused_max_ops": (128, 256)}
+    path = tmp_path / "b.json"
+    best = AT.autotune_batch((items, None, None, None, 0), None, capi.KT_C128, grid=grid, timer=fake, use_cache=False)
+    assert best == {"batch_jit_min_qubits": 16, "batch_small_max_qubits": 13, "fused_max_ops": 256}
+    assert len(seen) == 4 and len(AT.batch_candidates()) == 12
+    assert {k: capi.tuning_get(k) for k in AT.BATCH_KNOBS} == best
+    AT.save("batch|3x20", capi.KT_C128, best, [], path=path, device="fake-gpu")
+    assert "fake-gpu|c128|batch|3x20" in json.loads(path.read_text())
+    AT.set_knobs(before)

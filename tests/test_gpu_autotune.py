@@ -37,3 +37,27 @@ def test_autotune_on_device(engine, tmp_path):
         assert AT.load(20, path=tmp_path / "t.json") == best
     finally:
         AT.set_knobs(before)
+
+
+def test_batch_autotune_on_device(engine, tmp_path):
+    """autotune_batch over compiled classes on / off and two fusion depths on a
+    small mixed batch: every candidate gives the same energies and gradients
+    (1e-11), the fastest is left set and cached."""
+    circuits, params = W.hea_batch(24, seed=9, qubits=(11, 16), layers=(2, 4), n_strings=8)
+    args = capi.batch_items(circuits)
+    before = {k: capi.tuning_get(k) for k in AT.BATCH_KNOBS}
+    grid = {"batch_jit_min_qubits": (13, 0), "batch_small_max_qubits": (12,), "fused_max_ops": (128, 256)}
+    results = []
+    try:
+        for knobs in AT.batch_candidates(grid):
+            AT.set_knobs(knobs)
+            b = capi.Batch(*args)
+            results.append(b.evaluate(params))
+            b.close()
+        for e, g in results[1:]:
+            assert np.abs(e - results[0][0]).max() < 1e-11 and np.abs(g - results[0][1]).max() < 1e-11
+        best = AT.autotune_batch(args, params, grid=grid, path=tmp_path / "b.json")
+        assert {k: capi.tuning_get(k) for k in AT.BATCH_KNOBS} == best
+        assert AT.load(f"batch|24x{int(max(args[0]['n_qubits']))}", capi.KT_C128, path=tmp_path / "b.json") == best
+    finally:
+        AT.set_knobs(before)
