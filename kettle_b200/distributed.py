@@ -96,3 +96,83 @@ class ShardedBatch:
         if self.local is not None:
             self.local.close()
             self.local = None
+
+
+# ---------------------------------------------------------------------------
+# Pauli-string lists and parameter-shift shifts, the other independent units.
+# Every rank holds the same state (the statevector path runs as replicas),
+# evaluates its share of the units, and one SUM all-reduce of a vector with
+# one slot per unit — each slot written by exactly one rank — assembles the
+# values on every rank; totals are then formed in unit order, so every rank
+# gets the same bits.
+
+def shard_strings(x_masks, world: int) -> list[list[int]]:
+    """String indices per rank.  Strings with one X/Y mask share one read of
+    the state (k_pauli's slot), so whole mask groups are assigned, by the
+    longest-processing-time rule on their cost (one state read per 16
+    strings of the group)."""
+    groups: dict[int, list[int]] = {}
+    for i, x in enumerate(x_masks):
+        groups.setdefault(int(x), []).append(i)
+    keys = list(groups)
+    costs = [float((len(groups[k]) + 15) // 16) for k in keys]
+    out: list[list[int]] = [[] for _ in range(world)]
+    for r, sel in enumerate(shard_items(costs, world)):
+        for g in sel:
+            out[r].extend(groups[keys[g]])
+    return [sorted(s) for s in out]
+
+
+def shard_params(n_params: int, world: int) -> list[list[int]]:
+    """Parameter indices per rank for the parameter-shift rule (two shifted
+    energies of equal cost per parameter): round robin."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    return [list(range(r, n_params, world)) for r in range(world)]
+
+
+def gather_units(values_local, indices, n: int, dist=None, group=None, device=None) -> np.ndarray:
+    """The full vector of n unit values on every rank: `values_local[k]`
+    (real or complex) belongs to unit `indices[k]`."""
+    vals = np.asarray(values_local)
+    cplx = np.iscomplexobj(vals)
+    full = np.zeros(n, dtype=np.complex128 if cplx else np.float64)
+    full[np.asarray(indices, dtype=np.int64)] = vals
+    if dist is None:
+        return full
+    import torch
+    flat = np.concatenate([full.real, full.imag]) if cplx else full
+    t = torch.from_numpy(np.ascontiguousarray(flat)).to(device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    out = t.cpu().numpy()
+    return out[:n] + 1j * out[n:] if cplx else out.copy()
+
+
+def sharded_expectation(evaluate_terms, strings, coeffs, rank: int, world: int, dist=None, group=None,
+                        device=None):
+    """<H> = sum_k c_k <P_k> of this rank's replica with the strings sharded:
+    `evaluate_terms(strings_subset, coeffs_subset)` returns this rank's terms
+    (complex, the strings' phases included; e.g. capi.Statevector.expect's
+    first result).  Returns (all terms, total), the same on every rank."""
+    strings = np.ascontiguousarray(strings, dtype=capi.PAULI_DTYPE)
+    c = np.ones(strings.size, dtype=np.complex128) if coeffs is None else np.asarray(coeffs, dtype=np.complex128)
+    mine = shard_strings(strings["x"], world)[rank]
+    local = evaluate_terms(strings[mine], c[mine]) if mine else np.zeros(0, dtype=np.complex128)
+    terms = gather_units(np.asarray(local, dtype=np.complex128), mine, strings.size, dist, group, device)
+    return terms, complex(np.sum(c * terms))
+
+
+def sharded_parameter_shift(energy, params, rank: int, world: int, dist=None, group=None, device=None,
+                            shift: float = np.pi / 2) -> np.ndarray:
+    """dE/dθ_p = (E(θ + s e_p) − E(θ − s e_p)) / 2 (the rule for RX/RY/RZ
+    slots, s = π/2) with the parameters sharded over ranks; `energy(θ)` runs
+    on this rank's GPU.  The full gradient on every rank."""
+    p = np.asarray(params, dtype=np.float64)
+    mine = shard_params(p.size, world)[rank]
+    local = []
+    for k in mine:
+        up, dn = p.copy(), p.copy()
+        up[k] += shift
+        dn[k] -= shift
+        local.append(0.5 * (float(energy(up)) - float(energy(dn))))
+    return gather_units(np.asarray(local, dtype=np.float64), mine, p.size, dist, group, device)
