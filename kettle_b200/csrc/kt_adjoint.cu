@@ -37,7 +37,6 @@ using kt::KIND_DIAG;
 using kt::KIND_GEN;
 
 constexpr int ADJ_THREADS = 256;
-constexpr int HSUM_MAXS = 8;
 
 struct HGroup
 {
@@ -52,32 +51,92 @@ struct HTerm
     double wr, wi;  // c * phase * i^{#Y} * (-1)^{popcount(x & z)}
 };
 
-// lambda[j] = sum_groups sum_s w_s (-1)^{popcount(j & z_s)} psi[j ^ x]
+// lambda[j] = sum_groups sum_s w_s (-1)^{popcount(j & z_s)} psi[j ^ x], and
+// each block's FP64 partial of Re <psi|lambda> (the energy) in
+// epart[blockIdx.x].  A thread takes 4 consecutive outputs j0 .. j0 + 3
+// (j0 a multiple of 4) at a time: one gather of the 4 partners per group, and
+// per term one popcount of j0 & z (the low two bits of j0 are zero, so the
+// 4 signs differ only by the parity of k & z for k < 4).  Groups and terms are
+// staged in shared memory when they fit (`staged`).  lambda is formed in
+// FP64 and stored in the state's precision; the energy uses the FP64 values.
 template <typename C>
 __global__ void __launch_bounds__(ADJ_THREADS) k_hsum(const C* __restrict__ psi, C* __restrict__ lam, uint64_t N,
                                                       const HGroup* __restrict__ groups, int n_groups,
-                                                      const HTerm* __restrict__ terms)
+                                                      const HTerm* __restrict__ terms, int n_terms, int staged,
+                                                      double* __restrict__ epart)
 {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < N; j += stride) {
-        double ar = 0.0, ai = 0.0;
-        for (int g = 0; g < n_groups; ++g) {
-            const HGroup gr = groups[g];
-            const double2 p = kt::to_d2(psi[j ^ gr.x]);
-            double fr = 0.0, fi = 0.0;
-            for (int s = gr.first; s < gr.first + gr.count; ++s) {
-                const HTerm t = terms[s];
-                const bool neg = __popcll(j & t.z) & 1;
-                fr += neg ? -t.wr : t.wr;
-                fi += neg ? -t.wi : t.wi;
-            }
-            ar += fr * p.x - fi * p.y;
-            ai += fr * p.y + fi * p.x;
+    extern __shared__ __align__(16) unsigned char hs_raw[];
+    __shared__ double red[ADJ_THREADS / 32];
+    const HGroup* gp = groups;
+    const HTerm* tp = terms;
+    if (staged) {
+        auto* sg = reinterpret_cast<HGroup*>(hs_raw);
+        auto* st = reinterpret_cast<HTerm*>(hs_raw + ((static_cast<size_t>(n_groups) * sizeof(HGroup) + 15) & ~size_t {15}));
+        for (int i = threadIdx.x; i < n_groups; i += blockDim.x) {
+            sg[i] = groups[i];
         }
-        C o;
-        o.x = ar;
-        o.y = ai;
-        lam[j] = o;
+        for (int i = threadIdx.x; i < n_terms; i += blockDim.x) {
+            st[i] = terms[i];
+        }
+        __syncthreads();
+        gp = sg;
+        tp = st;
+    }
+    double e = 0.0;
+    const int kmax = N < 4 ? static_cast<int>(N) : 4;  // states of 1 or 2 amplitudes
+    const uint64_t stride = 4ULL * gridDim.x * blockDim.x;
+    for (uint64_t j0 = 4ULL * (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x); j0 < N; j0 += stride) {
+        double ar[4] = {0.0, 0.0, 0.0, 0.0}, ai[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int g = 0; g < n_groups; ++g) {
+            const HGroup gr = gp[g];
+            double2 pv[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                pv[k] = k < kmax ? kt::to_d2(psi[(j0 + k) ^ gr.x]) : make_double2(0.0, 0.0);
+            }
+            double fr[4] = {0.0, 0.0, 0.0, 0.0}, fi[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int s = gr.first; s < gr.first + gr.count; ++s) {
+                const HTerm t = tp[s];
+                const int par = __popcll(j0 & t.z) & 1;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const bool neg = (par ^ (__popc(static_cast<unsigned>(k) & static_cast<unsigned>(t.z)) & 1)) != 0;
+                    fr[k] += neg ? -t.wr : t.wr;
+                    fi[k] += neg ? -t.wi : t.wi;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                ar[k] += fr[k] * pv[k].x - fi[k] * pv[k].y;
+                ai[k] += fr[k] * pv[k].y + fi[k] * pv[k].x;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k < kmax) {
+                const double2 pj = kt::to_d2(psi[j0 + k]);
+                e += pj.x * ar[k] + pj.y * ai[k];
+                C o;
+                o.x = ar[k];
+                o.y = ai[k];
+                lam[j0 + k] = o;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_down_sync(0xffffffffU, e, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = e;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < ADJ_THREADS / 32; ++w) {
+            b += red[w];
+        }
+        epart[blockIdx.x] = b;
     }
 }
 
@@ -203,7 +262,8 @@ struct kt_adjoint_s
     int64_t n_params {0};
     std::vector<HGroup> hgroups;
     std::vector<HTerm> hterms;
-    kt::DevBuf dev;     // hsum tables, partials, gradients
+    kt::DevBuf dev;     // partials and gradients of the backward sweep
+    kt::DevBuf hdev;    // the Hamiltonian's groups and terms, the energy partials (forward)
     kt::DevBuf fused_work;  // plans and partials of the fused sweep
     bool forward_done {false};
     uint64_t last_structure {0};  // gate kinds, qubits and parameter slots of the previous forward
@@ -306,6 +366,7 @@ int32_t kt_adjoint_destroy(kt_adjoint a)
         a->lam.scratch.release();
         a->lam.scratch2.release();
         a->dev.release();
+        a->hdev.release();
         a->fused_work.release();
         delete a;
     }
@@ -445,11 +506,50 @@ int32_t kt_adjoint_forward(kt_adjoint a, const kt_gate* gates, int64_t n_gates, 
             }
             a->hgroups.push_back(gr);
         }
-        double total[2];
-        if (const int32_t rc = kt::expect_paulis(psi, strings, n_strings, coeffs, nullptr, total); rc != KT_OK) {
+        // lambda = H psi now (the backward starts from it) and the energy
+        // Re <psi|lambda> from its FP64 values: one pass per X/Y-mask group
+        kt::State& lam = a->lam;
+        const uint64_t N = psi.n_amps();
+        auto al = [](size_t v) { return (v + 255) & ~size_t {255}; };
+        const size_t gbytes = a->hgroups.size() * sizeof(HGroup);
+        const size_t tbytes = a->hterms.size() * sizeof(HTerm);
+        const int hblocks = static_cast<int>(std::min<uint64_t>(std::max<uint64_t>(1, (N / 4 + ADJ_THREADS - 1) / ADJ_THREADS),
+                                                                static_cast<uint64_t>(kt::sm_count()) * 8));
+        const size_t off_t = al(gbytes);
+        const size_t off_e = al(off_t + tbytes);
+        if (const int32_t rc = a->hdev.reserve(al(off_e + static_cast<size_t>(hblocks) * sizeof(double))); rc != KT_OK) {
             return rc;
         }
-        *energy = total[0];
+        char* hb = static_cast<char*>(a->hdev.ptr);
+        auto* d_groups = reinterpret_cast<HGroup*>(hb);
+        auto* d_terms = reinterpret_cast<HTerm*>(hb + off_t);
+        auto* d_epart = reinterpret_cast<double*>(hb + off_e);
+        KT_CUDA(cudaMemcpyAsync(d_groups, a->hgroups.data(), gbytes, cudaMemcpyHostToDevice, psi.stream));
+        KT_CUDA(cudaMemcpyAsync(d_terms, a->hterms.data(), tbytes, cudaMemcpyHostToDevice, psi.stream));
+        const size_t staged_bytes = al(gbytes) + tbytes;
+        const int staged = staged_bytes <= 48 * 1024 ? 1 : 0;
+        const size_t hsmem = staged ? staged_bytes : 0;
+        const int ng = static_cast<int>(a->hgroups.size());
+        const int nt = static_cast<int>(a->hterms.size());
+        if (psi.dtype == KT_C128) {
+            k_hsum<double2><<<hblocks, ADJ_THREADS, hsmem, psi.stream>>>(static_cast<const double2*>(psi.amps),
+                                                                         static_cast<double2*>(lam.amps), N, d_groups,
+                                                                         ng, d_terms, nt, staged, d_epart);
+        } else {
+            k_hsum<float2><<<hblocks, ADJ_THREADS, hsmem, psi.stream>>>(static_cast<const float2*>(psi.amps),
+                                                                        static_cast<float2*>(lam.amps), N, d_groups,
+                                                                        ng, d_terms, nt, staged, d_epart);
+        }
+        KT_CHECK_LAUNCH("k_hsum");
+        std::vector<double> ep(static_cast<size_t>(hblocks));
+        if (const int32_t rc = kt::copy_d2h(ep.data(), d_epart, ep.size() * sizeof(double), psi.stream); rc != KT_OK) {
+            return rc;
+        }
+        double total = 0.0;
+        for (const double v : ep) {
+            total += v;  // block order: the same bits on every call
+        }
+        *energy = total;
         a->forward_done = true;
         return KT_OK;
     } catch (const std::exception& e) {
@@ -481,35 +581,16 @@ int32_t kt_adjoint_backward(kt_adjoint a, double* grad, int64_t n_params)
             n_grad += b.slot >= 0 ? 1 : 0;
         }
         auto al = [](size_t v) { return (v + 255) & ~size_t {255}; };
-        const size_t off_g = 0;
-        const size_t off_t = al(a->hgroups.size() * sizeof(HGroup));
-        const size_t off_part = al(off_t + a->hterms.size() * sizeof(HTerm));
+        const size_t off_part = 0;
         const size_t off_out = al(off_part + static_cast<size_t>(std::max(1, n_grad)) * blocks * sizeof(double));
         const size_t need = al(off_out + static_cast<size_t>(std::max(1, n_grad)) * sizeof(double));
         if (const int32_t rc = a->dev.reserve(need); rc != KT_OK) {
             return rc;
         }
         char* base = static_cast<char*>(a->dev.ptr);
-        auto* d_groups = reinterpret_cast<HGroup*>(base + off_g);
-        auto* d_terms = reinterpret_cast<HTerm*>(base + off_t);
         auto* d_part = reinterpret_cast<double*>(base + off_part);
         auto* d_out = reinterpret_cast<double*>(base + off_out);
-        KT_CUDA(cudaMemcpyAsync(d_groups, a->hgroups.data(), a->hgroups.size() * sizeof(HGroup), cudaMemcpyHostToDevice,
-                                psi.stream));
-        KT_CUDA(cudaMemcpyAsync(d_terms, a->hterms.data(), a->hterms.size() * sizeof(HTerm), cudaMemcpyHostToDevice,
-                                psi.stream));
-        const int hblocks = static_cast<int>(std::min<uint64_t>((N + ADJ_THREADS - 1) / ADJ_THREADS,
-                                                                static_cast<uint64_t>(kt::sm_count()) * 8));
-        if (psi.dtype == KT_C128) {
-            k_hsum<double2><<<hblocks, ADJ_THREADS, 0, psi.stream>>>(static_cast<const double2*>(psi.amps),
-                                                                     static_cast<double2*>(lam.amps), N, d_groups,
-                                                                     static_cast<int>(a->hgroups.size()), d_terms);
-        } else {
-            k_hsum<float2><<<hblocks, ADJ_THREADS, 0, psi.stream>>>(static_cast<const float2*>(psi.amps),
-                                                                    static_cast<float2*>(lam.amps), N, d_groups,
-                                                                    static_cast<int>(a->hgroups.size()), d_terms);
-        }
-        KT_CHECK_LAUNCH("k_hsum");
+        // lambda = H psi was formed by the forward pass
         // backward sweep
         const int64_t G = static_cast<int64_t>(a->gates.size());
         const int64_t k = a->checkpoint_every;

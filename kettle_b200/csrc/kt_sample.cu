@@ -455,6 +455,37 @@ __global__ void __launch_bounds__(256) k_tile_sums(const double* __restrict__ p,
     }
 }
 
+// 0 + 1 fused, for the state's own probabilities without readout noise:
+// |a_i|^2 exactly as k_probs writes them (round-to-nearest products and sum,
+// no contraction) and each tile's FP64 sum on the way (any order, as above)
+template <typename C>
+__global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, uint64_t N, double* __restrict__ p,
+                                                     double* __restrict__ tsum)
+{
+    __shared__ double sh[8];
+    const uint64_t beg = static_cast<uint64_t>(blockIdx.x) * XS_TILE;
+    const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+    double acc = 0.0;
+    for (uint64_t i = beg + threadIdx.x; i < end; i += 256) {
+        const double2 v = to_d2(a[i]);
+        const double q = __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
+        p[i] = q;
+        acc += q;
+    }
+    acc = warp_sum_d(acc);
+    if ((threadIdx.x & 31) == 0) {
+        sh[threadIdx.x >> 5] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            t += sh[w];
+        }
+        tsum[blockIdx.x] = t;
+    }
+}
+
 // 1b. one block: approximate start value of every tile, and its binade guess
 __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restrict__ tsum, uint64_t n_tiles,
                                                            int* __restrict__ code)
@@ -655,6 +686,11 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const double* __restr
                                                            const int* __restrict__ code,
                                                            const double* __restrict__ carry, double* __restrict__ cdf)
 {
+    // warp w holds the tile's elements [w * 32 * XS_EPT, (w + 1) * 32 * XS_EPT)
+    // as XS_EPT rows of 32 consecutive elements, one per lane, so every load
+    // and store of a row is one coalesced 256-byte access; the integer prefix
+    // runs row by row (a warp scan per row, the warp's earlier rows carried)
+    // after a block scan of the warp totals, in element order
     __shared__ unsigned long long sh[32];
     const double c0 = carry[blockIdx.x];
     if (c0 < 0.0) {
@@ -662,12 +698,14 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const double* __restr
     }
     const uint64_t beg = static_cast<uint64_t>(blockIdx.x) * XS_TILE;
     const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
-    const uint64_t b0 = beg + static_cast<uint64_t>(threadIdx.x) * XS_EPT;
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    const uint64_t wb = beg + static_cast<uint64_t>(threadIdx.x >> 5) * (32 * XS_EPT) + lane;
     const int c = code[blockIdx.x];
     if (c == TILE_ZERO) {
         for (int k = 0; k < XS_EPT; ++k) {
-            if (b0 + k < end) {
-                cdf[b0 + k] = c0;
+            const uint64_t g = wb + static_cast<uint64_t>(k) * 32;
+            if (g < end) {
+                cdf[g] = c0;
             }
         }
         return;
@@ -679,22 +717,59 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const double* __restr
     unsigned long long run = 0;
 #pragma unroll
     for (int k = 0; k < XS_EPT; ++k) {
-        r[k] = (b0 + k < end) ? static_cast<unsigned long long>(rint(p[b0 + k] * inv_u)) : 0ULL;
+        const uint64_t g = wb + static_cast<uint64_t>(k) * 32;
+        r[k] = (g < end) ? static_cast<unsigned long long>(rint(p[g] * inv_u)) : 0ULL;
         run += r[k];
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        run += __shfl_xor_sync(0xffffffffU, run, o);  // the warp's total, in every lane
+    }
     unsigned long long total;
-    unsigned long long acc = m + block_excl_scan_u64(run, sh, total);
+    const unsigned long long before = block_excl_scan_u64(lane == 0 ? run : 0ULL, sh, total);
+    unsigned long long acc = m + __shfl_sync(0xffffffffU, before, 0);
 #pragma unroll
     for (int k = 0; k < XS_EPT; ++k) {
-        acc += r[k];
-        if (b0 + k < end) {
-            cdf[b0 + k] = static_cast<double>(acc) * u;
+        unsigned long long x = r[k];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffU, x, o);
+            if (lane >= o) {
+                x += y;
+            }
         }
+        const uint64_t g = wb + static_cast<uint64_t>(k) * 32;
+        if (g < end) {
+            cdf[g] = static_cast<double>(acc + x) * u;
+        }
+        acc += __shfl_sync(0xffffffffU, x, 31);
     }
 }
 
 // cumulative_end_offset_ (measurements.cpp:235-256): the last value strictly
 // below `last`, found as the largest index holding one.
+// The same index by binary search, for a non-decreasing CDF (every
+// probability >= 0, so each sequential sum is at least the one before): the
+// first index whose value is not below the last one.
+__global__ void k_last_below_sorted(const double* __restrict__ cdf, uint64_t N, unsigned long long* __restrict__ idx1)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) {
+        return;
+    }
+    const double last = cdf[N - 1];
+    uint64_t lo = 0, len = N;
+    while (len > 0) {
+        const uint64_t half = len / 2;
+        if (cdf[lo + half] < last) {
+            lo = lo + half + 1;
+            len = len - half - 1;
+        } else {
+            len = half;
+        }
+    }
+    *idx1 = static_cast<unsigned long long>(lo);
+}
+
 __global__ void k_last_below(const double* __restrict__ cdf, uint64_t N, unsigned long long* __restrict__ idx1)
 {
     const double last = cdf[N - 1];
@@ -804,10 +879,21 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     auto* d_ints = reinterpret_cast<unsigned long long*>(base + off_ints);
     auto* d_carry = reinterpret_cast<double*>(base + off_carry);
 
+    // the exact tier straight away (above the fast tier's size) on the state's
+    // own noiseless probabilities: their pass also forms the tile sums
+    const bool fused_tiles = host_probs == nullptr && noise == nullptr && !(mode == 0 && N <= (uint64_t {1} << 22));
     if (host_probs != nullptr) {
         if (const int32_t rc = copy_h2d(dp, host_probs, N * 8, s.stream); rc != KT_OK) {
             return rc;
         }
+    } else if (fused_tiles) {
+        const unsigned nt = static_cast<unsigned>((N + XS_TILE - 1) / XS_TILE);
+        if (s.dtype == KT_C128) {
+            k_probs_tiles<double2><<<nt, 256, 0, s.stream>>>(static_cast<const double2*>(s.amps), N, dp, d_tsum);
+        } else {
+            k_probs_tiles<float2><<<nt, 256, 0, s.stream>>>(static_cast<const float2*>(s.amps), N, dp, d_tsum);
+        }
+        KT_CHECK_LAUNCH("k_probs_tiles");
     } else if (const int32_t rc = device_probabilities(s, noise, dp); rc != KT_OK) {
         return rc;
     }
@@ -840,8 +926,10 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     }
     if (unc != 0) {
         const uint64_t n_tiles = (N + XS_TILE - 1) / XS_TILE;
-        k_tile_sums<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_tsum);
-        KT_CHECK_LAUNCH("k_tile_sums");
+        if (!fused_tiles) {
+            k_tile_sums<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_tsum);
+            KT_CHECK_LAUNCH("k_tile_sums");
+        }
         k_tile_guess<<<1, XS_THREADS, 0, s.stream>>>(d_tsum, n_tiles, d_code);
         KT_CHECK_LAUNCH("k_tile_guess");
         k_tile_ints<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_code, d_ints);
@@ -850,10 +938,16 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
         KT_CHECK_LAUNCH("k_exact_chain");
         k_tile_write<<<static_cast<unsigned>(n_tiles), XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf);
         KT_CHECK_LAUNCH("k_tile_write");
-        KT_CUDA(cudaMemsetAsync(d_nz, 0, 8, s.stream));
-        const unsigned lb_blocks = static_cast<unsigned>(std::min<uint64_t>((N + 255) / 256, sm_count() * 8ULL));
-        k_last_below<<<lb_blocks, 256, 0, s.stream>>>(dcdf, N, d_nz);
-        KT_CHECK_LAUNCH("k_last_below");
+        if (host_probs == nullptr) {
+            // |a_i|^2 (and readout noise, a mix of them) are never negative
+            k_last_below_sorted<<<1, 32, 0, s.stream>>>(dcdf, N, d_nz);
+            KT_CHECK_LAUNCH("k_last_below_sorted");
+        } else {
+            KT_CUDA(cudaMemsetAsync(d_nz, 0, 8, s.stream));
+            const unsigned lb_blocks = static_cast<unsigned>(std::min<uint64_t>((N + 255) / 256, sm_count() * 8ULL));
+            k_last_below<<<lb_blocks, 256, 0, s.stream>>>(dcdf, N, d_nz);
+            KT_CHECK_LAUNCH("k_last_below");
+        }
         k_seq_bound<<<1, 32, 0, s.stream>>>(dcdf, N, d_nz, d_bound);
         KT_CHECK_LAUNCH("k_seq_bound");
         k_seq_search<<<static_cast<unsigned>((ns + 127) / 128), 128, 0, s.stream>>>(dcdf, N, d_bound, d_canon, n_shots,
