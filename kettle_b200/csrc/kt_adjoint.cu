@@ -16,6 +16,7 @@
 // restores psi from them instead of relying on un-applying alone.  When no
 // copy fits (large qubit counts), the sweep runs on psi and lambda only.
 #include <algorithm>
+#include <complex>
 #include <cmath>
 #include <map>
 #include <vector>
@@ -137,6 +138,20 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_hsum(const C* __restrict__ psi,
             b += red[w];
         }
         epart[blockIdx.x] = b;
+    }
+}
+
+// a *= (re + i im)
+template <typename C>
+__global__ void k_scale_state(C* __restrict__ a, uint64_t N, double re, double im)
+{
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < N;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const double2 v = kt::to_d2(a[i]);
+        C o;
+        o.x = v.x * re - v.y * im;
+        o.y = v.x * im + v.y * re;
+        a[i] = o;
     }
 }
 
@@ -609,6 +624,15 @@ int32_t kt_adjoint_backward(kt_adjoint a, double* grad, int64_t n_params)
             }
             const int64_t seg = (k > 0) ? k : std::max<int64_t>(G, 1);
             const int64_t n_seg = (G + seg - 1) / seg;
+            // Without checkpoints, an uncontrolled diagonal U^dagger with
+            // |m00| = 1 (RZ, literal phases) runs one-sided, diag(1, m11 / m00),
+            // on psi and lambda: every gradient term is bilinear in conj(lambda)
+            // and psi, so the common unit factor m00 they both drop leaves it
+            // unchanged, and half the amplitudes are touched.  psi gets the
+            // product of the dropped factors back at the end.  (A checkpoint
+            // restores psi alone, so with checkpoints every op keeps its form.)
+            const bool one_sided = a->checkpoints.empty();
+            std::complex<double> dropped(1.0, 0.0);
             for (int64_t j = n_seg - 1; j >= 0; --j) {
                 const int64_t g0 = j * seg;
                 const int64_t g1 = std::min<int64_t>(G, g0 + seg);
@@ -623,11 +647,35 @@ int32_t kt_adjoint_backward(kt_adjoint a, double* grad, int64_t n_params)
                     ag.adj = a->gates[g].adj;
                     ag.gen = a->gates[g].gen;
                     ag.row = row_of[g];
+                    if (one_sided && ag.adj.kind == KIND_DIAG && ag.adj.control < 0 && (ag.adj.flags & 1) == 0) {
+                        const std::complex<double> m00(ag.adj.m[0], ag.adj.m[1]), m11(ag.adj.m[6], ag.adj.m[7]);
+                        if (std::abs(std::norm(m00) - 1.0) < 1e-12) {
+                            const std::complex<double> r = m11 * std::conj(m00);
+                            ag.adj.m[0] = 1.0;
+                            ag.adj.m[1] = 0.0;
+                            ag.adj.m[6] = r.real();
+                            ag.adj.m[7] = r.imag();
+                            ag.adj.flags |= 1;
+                            dropped *= m00;
+                        }
+                    }
                     sweep.push_back(ag);
                 }
                 if (const int32_t rc = kt::adjoint_sweep_fused(psi, lam, sweep, d_out, a->fused_work); rc != KT_OK) {
                     return rc;
                 }
+            }
+            if (dropped != std::complex<double>(1.0, 0.0)) {
+                const unsigned sb = static_cast<unsigned>(std::min<uint64_t>((N + ADJ_THREADS - 1) / ADJ_THREADS,
+                                                                             static_cast<uint64_t>(kt::sm_count()) * 8));
+                if (psi.dtype == KT_C128) {
+                    k_scale_state<double2><<<sb, ADJ_THREADS, 0, psi.stream>>>(static_cast<double2*>(psi.amps), N,
+                                                                             dropped.real(), dropped.imag());
+                } else {
+                    k_scale_state<float2><<<sb, ADJ_THREADS, 0, psi.stream>>>(static_cast<float2*>(psi.amps), N,
+                                                                            dropped.real(), dropped.imag());
+                }
+                KT_CHECK_LAUNCH("k_scale_state");
             }
             std::vector<double> rows_f(static_cast<size_t>(std::max(1, n_grad)));
             if (n_grad > 0) {

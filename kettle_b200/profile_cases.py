@@ -11,10 +11,10 @@ launch of the kernel it captures.  The states are sized past the 126 MB L2
 
 Cases and the kernels they run:
   pauli        k_pauli, k_pauli_finalize          (kt_sv_expect, 32 strings)
-  sample       k_probs, k_tile_*, k_exact_chain, k_last_below, k_seq_*  (kt_sv_sample, exact tier)
+  sample       k_probs_tiles, k_tile_*, k_exact_chain, k_last_below_sorted, k_seq_*  (kt_sv_sample, exact tier)
   sample_fast  k_probs, k_chunk_sums, k_chunk_offsets, k_sample_bound, k_sample_fast  (2^22 amplitudes)
   dm_pauli     k_dm_pauli, k_dm_pauli_finalize    (kt_dm_expect on a 13-qubit density matrix)
-  hpsi         k_hsum                              (lambda = H psi, formed when the adjoint backward starts)
+  hpsi         k_hsum                              (lambda = H psi and the energy, in the adjoint forward)
   adjoint      k_fused_adj, k_adj_rows             (fused adjoint backward blocks)
   dm_ops       k_partial_trace, k_tensor_product, k_trace_square
   norm         compiled blocks (prepared plan; k_fused_norm with fused_jit=0), k_norm_final
