@@ -2525,6 +2525,26 @@ bool plan_from_view(const BatchPlanView& v, Plan<T, O>& plan)
     return true;
 }
 
+// Batched kernels stay loaded for the life of the process, in a cache of
+// their own (the single-state cache unloads its programs when it fills), so
+// a later batch with classes of the same structure skips their compile.  Past
+// BATCH_CACHE_MAX kernels a batch compiles, and owns, the ones it misses.
+constexpr size_t BATCH_CACHE_MAX = 8192;
+
+struct BatchKernelCache
+{
+    std::mutex m;
+    std::unordered_map<std::string, const void*> kernels;  // launch bounds + body -> kernel
+    std::map<std::pair<const void*, int>, int32_t> smem;   // (kernel, device) -> shared-memory limit set
+    std::vector<cudaLibrary_t> libs;                        // never unloaded
+};
+
+BatchKernelCache& batch_kernel_cache()
+{
+    static BatchKernelCache* c = new BatchKernelCache();  // outlives every batch, never destroyed
+    return *c;
+}
+
 template <typename T>
 int32_t jit_batch_compile_t(const std::vector<BatchPlanView>& fwd, const std::vector<BatchPlanView>& bwd,
                             std::vector<std::vector<const void*>>& fk, std::vector<std::vector<const void*>>& bk,
@@ -2592,30 +2612,55 @@ int32_t jit_batch_compile_t(const std::vector<BatchPlanView>& fwd, const std::ve
             }
         }
     }
-    // programs of a few kernels each, compiled on parallel host threads
-    const size_t per_prog = 4;
-    const size_t n_prog = std::max<size_t>(1, (texts.size() + per_prog - 1) / per_prog);
-    std::vector<std::string> sources(n_prog, JIT_PRELUDE);
-    std::vector<std::vector<std::string>> names(n_prog);
+    BatchKernelCache& cache = batch_kernel_cache();
+    std::lock_guard<std::mutex> lock(cache.m);
+    std::vector<const void*> handle(texts.size(), nullptr);
+    std::vector<size_t> missing;
     for (size_t i = 0; i < texts.size(); ++i) {
-        const size_t w = i / per_prog;
-        const std::string name = std::string(is_adj[i] ? "kt_jab" : "kt_jbb") + std::to_string(i);
-        sources[w] += "extern \"C\" __global__ void " + bounds + " " + name + texts[i].substr(bounds.size()) + "\n";
-        names[w].push_back(name);
-    }
-    std::vector<std::vector<const void*>> got;
-    if (!texts.empty()) {
-        if (const int32_t rc = jit_compile(sources, names, got, true, &libs); rc != KT_OK) {
-            return rc;
+        auto it = cache.kernels.find(texts[i]);
+        if (it != cache.kernels.end()) {
+            handle[i] = it->second;
+        } else {
+            missing.push_back(i);
         }
     }
-    std::vector<const void*> handle(texts.size());
+    if (!missing.empty()) {
+        // programs of a few kernels each, compiled on parallel host threads
+        const bool keep = cache.kernels.size() + missing.size() <= BATCH_CACHE_MAX;
+        const size_t per_prog = 4;
+        const size_t n_prog = (missing.size() + per_prog - 1) / per_prog;
+        std::vector<std::string> sources(n_prog, JIT_PRELUDE);
+        std::vector<std::vector<std::string>> names(n_prog);
+        for (size_t m = 0; m < missing.size(); ++m) {
+            const size_t i = missing[m];
+            const std::string name = std::string(is_adj[i] ? "kt_jab" : "kt_jbb") + std::to_string(m);
+            sources[m / per_prog] += "extern \"C\" __global__ void " + bounds + " " + name +
+                                     texts[i].substr(bounds.size()) + "\n";
+            names[m / per_prog].push_back(name);
+        }
+        std::vector<std::vector<const void*>> got;
+        if (const int32_t rc = jit_compile(sources, names, got, true, keep ? &cache.libs : &libs); rc != KT_OK) {
+            return rc;
+        }
+        for (size_t m = 0; m < missing.size(); ++m) {
+            handle[missing[m]] = got[m / per_prog][m % per_prog];
+            if (keep) {
+                cache.kernels.emplace(texts[missing[m]], handle[missing[m]]);
+            }
+        }
+    }
     int dev = 0;
     KT_CUDA(cudaGetDevice(&dev));
     for (size_t i = 0; i < texts.size(); ++i) {
-        handle[i] = got[i / per_prog][i % per_prog];
-        KT_CUDA(cudaKernelSetAttributeForDevice(reinterpret_cast<cudaKernel_t>(const_cast<void*>(handle[i])),
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem[i], dev));
+        // cached kernels remember their limit per device; a batch's own ones are set every time
+        const bool cached = cache.kernels.count(texts[i]) != 0;
+        int32_t dummy = 0;
+        int32_t& set = cached ? cache.smem[std::make_pair(handle[i], dev)] : dummy;
+        if (set < smem[i]) {
+            KT_CUDA(cudaKernelSetAttributeForDevice(reinterpret_cast<cudaKernel_t>(const_cast<void*>(handle[i])),
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem[i], dev));
+            set = smem[i];
+        }
     }
     fk.assign(fwd.size(), {});
     bk.assign(bwd.size(), {});

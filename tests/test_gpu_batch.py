@@ -285,3 +285,20 @@ def test_batch_compiled_without_gradients_and_complex64(engine):
     b64.close()
     _, g1 = _one_by_one(circuits, params)
     assert np.abs(e64 - e1).max() < 1e-3 and np.abs(g64 - g1).max() < 1e-3
+
+
+def test_batch_compiled_kernels_shared_between_batches(engine):
+    """A second batch of the same plan structures takes its compiled kernels
+    from the process-wide cache: it evaluates the same values, also after the
+    first batch is destroyed."""
+    circuits, params = _class_items(500)
+    items, gates, strings, coeffs, n_params = capi.batch_items(circuits)
+    mk = lambda: _with_knob("batch_jit_min_qubits", 14, lambda: capi.Batch(items, gates, strings, coeffs, n_params))
+    b1 = mk()
+    e1, g1 = b1.evaluate(params)
+    b2 = mk()
+    b1.close()
+    e2, g2 = b2.evaluate(params)
+    b2.close()
+    assert b2 is not b1
+    assert np.array_equal(e1, e2) and np.array_equal(g1, g2)
