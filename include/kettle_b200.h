@@ -175,7 +175,9 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               constant): 0 never, 1 always, 2 (default) once a
  *                               circuit structure has been applied often enough to
  *                               repay the compile (jit_after) on states of
- *                               >= jit_min_qubits qubits, or after kt_sv_prepare;
+ *                               >= jit_min_qubits qubits, or after kt_sv_prepare /
+ *                               kt_dm_prepare (a prepared structure runs compiled
+ *                               at any size);
  *                               without NVRTC, or if a compile fails, the
  *                               precompiled kernels run (kt_jit_stats)
  *   jit_after          0..1e6   (0) the apply at which fused_jit = 2 compiles; 0 estimates

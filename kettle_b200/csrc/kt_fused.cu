@@ -1575,7 +1575,14 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
     *rc = KT_OK;
     const int n = s.n_bits;
     const int mode = tuning().fused_jit;
-    const bool want = compile_only || mode == 1 || (mode == 2 && (n >= tuning().jit_min_qubits || s.force_jit));
+    bool want = compile_only || mode == 1 || (mode == 2 && (n >= tuning().jit_min_qubits || s.force_jit));
+    if (!want && mode == 2) {
+        // a plan compiled ahead (kt_sv_prepare / kt_dm_prepare) runs compiled at any size
+        JitCache& jc = jit_cache();
+        std::lock_guard<std::mutex> lock(jc.m);
+        const auto it = jc.plans.find(plan_key);
+        want = it != jc.plans.end() && it->second.prepared;
+    }
     if (!want) {
         return false;
     }

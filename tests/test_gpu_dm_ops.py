@@ -1,6 +1,7 @@
 """Density-matrix operations on the GPU (kt_dm_partial_trace, kt_dm_tensor_product,
 kt_dm_trace_of_square) against the reference's outputs (tests/golden/golden_dm_ops.npz)
-and the oracle on seeded inputs up to 12 qubits.
+and the oracle on seeded inputs up to 12 qubits; and a density matrix whose
+circuit was compiled ahead (kt_dm_prepare).
 
 Partial traces add the same values in the same grouping as the reference's
 one-qubit-at-a-time sequence (state/density_matrix.cpp:231-278), so complex128
@@ -10,6 +11,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN
+from kettle_b200 import capi
 
 pytestmark = pytest.mark.gpu
 
@@ -123,3 +125,28 @@ def test_complex64_storage(engine, port):
     t = small.tensor_product(d)
     np.testing.assert_allclose(t.download(), port.dm_tensor_product(2, _rho(2, 12), 7, rho), rtol=0, atol=1e-6)
     assert abs(d.trace_of_square() - port.dm_trace_of_square(7, rho)) < 1e-6
+
+
+def test_prepared_density_matrix_runs_compiled_blocks(engine, port):
+    """kt_dm_prepare compiles the blocks of the 2n-bit gate stream kt_dm_apply
+    plans: the next apply of that circuit launches them (jit_stats) and gives
+    the unprepared result (1e-12) and the oracle's rho (1e-12)."""
+    from conftest import basis
+    from kettle_b200 import workloads as W
+    n = 7
+    gates = W.random_layers(n, 6, seed=31, mixed=True)
+    plain = capi.DensityMatrix(n)
+    plain.apply(gates)
+    want = plain.download()
+    plain.close()
+    dm = capi.DensityMatrix(n)
+    dm.prepare(gates)
+    before = capi.jit_stats()
+    dm.apply(gates)
+    after = capi.jit_stats()
+    got = dm.download()
+    dm.close()
+    assert not after["failed"] and after["launches"] > before["launches"]
+    assert np.abs(got - want).max() < 1e-12
+    psi = port.apply(n, basis(n), gates)
+    assert np.abs(got - np.outer(psi, psi.conj())).max() < 1e-12
