@@ -228,6 +228,8 @@ int32_t kt_canonicals_mt19937(uint32_t seed, int64_t n, double* out);
  *                               KT_ERR_TIMEOUT
  *   jit_tma_stages     2..4     (3) tile buffers per CTA (the kernel must fit 227 KB
  *                               of shared memory)
+ *   jit_tma_ctas       1 or 2   (1) TMA-pipelined CTAs per SM; with 2 each must fit
+ *                               113 KB (e.g. 11-qubit tiles, 3 stages)
  *   batch_spin_limit   1..1e12  (33554432) polls of an empty job queue after which a
  *                               CTA of a batch's persistent kernel gives up (about
  *                               10 s): the evaluation then stops and

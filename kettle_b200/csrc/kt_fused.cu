@@ -1614,7 +1614,10 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
         const size_t tile_bytes = (size_t {1} << K) * sizeof(C);
         const size_t need = static_cast<size_t>(stages) * tile_bytes + 1024 + 16 * static_cast<size_t>(stages);
         const int tthreads = groups * threads + 32;
-        bool ok = need <= 227 * 1024 && tthreads <= 1024 && (groups * threads) % 32 == 0;
+        // jit_tma_ctas = 2: two such CTAs per SM, each within half of the SM's shared memory
+        const int ctas = tuning().jit_tma_ctas;
+        const size_t cap = ctas == 2 ? size_t {113} * 1024 : size_t {227} * 1024;
+        bool ok = need <= cap && tthreads <= 1024 && (groups * threads) % 32 == 0;
         for (size_t b = 0; ok && b < plan.blocks.size(); ++b) {
             TmaCfg c;
             c.groups = groups;
@@ -1625,8 +1628,8 @@ bool jit_launch(State& s, const Plan<T>& plan, uint64_t plan_key, int K, bool rb
         }
         if (ok) {
             threads = tthreads;
-            minb = 1;
-            grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()));
+            minb = ctas;
+            grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sm_count()) * static_cast<uint64_t>(ctas));
             smem = need;
             smem_attr = static_cast<int>(need);
         } else {
@@ -2498,7 +2501,7 @@ int32_t jit_compile_only_t(int n, const std::vector<LGate>& gates, int64_t* n_ke
         const bool bt = tma && c.geom.ok;
         const int bthreads = bt ? c.groups * threads + 32 : threads;
         sources[0] += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(bthreads) + ", " +
-                      std::to_string(bt || threads > 256 ? 1 : 2) + ") " + name +
+                      std::to_string(bt ? tuning().jit_tma_ctas : (threads > 256 ? 1 : 2)) + ") " + name +
                       jit_block_body<T>(plan, b, RB, norm, bt ? &c : nullptr) + "\n";
         names[0].push_back(name);
     }

@@ -260,6 +260,7 @@ struct Tuning
     int jit_lean_sync {1};       // 1: compiled blocks drop a transpose's second barrier where the phase stores where it loaded
     int jit_tma {0};             // 1: complex128 compiled blocks move tiles with TMA tensor copies, pipelined
     int jit_tma_stages {3};      // TMA blocks: shared-memory tile buffers per CTA (2..4)
+    int jit_tma_ctas {1};        // TMA blocks: CTAs per SM (1 or 2: each within half the shared memory)
 };
 Tuning& tuning();
 bool tuning_set(const char* name, long long value);

@@ -108,6 +108,8 @@ bool set_knob(Tuning& t, const std::string& name, long long v)
         t.jit_lean_sync = (v != 0) ? 1 : 0;
     } else if (name == "jit_tma") {
         t.jit_tma = (v != 0) ? 1 : 0;
+    } else if (name == "jit_tma_ctas") {
+        t.jit_tma_ctas = (v >= 2) ? 2 : 1;
     } else if (name == "jit_tma_stages") {
         t.jit_tma_stages = static_cast<int>(std::max(2LL, std::min(4LL, v)));
     } else if (name == "batch_spin_limit") {
@@ -209,6 +211,8 @@ bool tuning_get(const char* name, long long* value)
         *value = t.jit_lean_sync;
     } else if (n == "jit_tma") {
         *value = t.jit_tma;
+    } else if (n == "jit_tma_ctas") {
+        *value = t.jit_tma_ctas;
     } else if (n == "jit_tma_stages") {
         *value = t.jit_tma_stages;
     } else if (n == "batch_spin_limit") {

@@ -270,12 +270,14 @@ def test_scaled_ops_out_of_range_fall_back(jit, port):
     {"jit_tma": 1, "jit_tma_stages": 2},
     {"jit_tma": 1, "jit_tma_stages": 4, "fused_tile_bits": 11},
     {"jit_tma": 1, "fused_reg_bits": 3},
+    {"jit_tma": 1, "jit_tma_ctas": 2, "fused_tile_bits": 11, "fused_reg_bits": 3},
+    {"jit_tma": 1, "jit_tma_ctas": 2, "fused_tile_bits": 11},
 ])
 @pytest.mark.parametrize("n,layers,seed", [(13, 4, 81), (18, 4, 82), (22, 3, 83)])
 def test_tma_blocks_match_oracle(jit, port, knobs, n, layers, seed):
     """TMA-pipelined compiled blocks (tiles moved by tensor copies into
-    swizzled stage buffers, a producer warp, one tile group per CTA):
-    the oracle's amplitudes; from 13 qubits (two tiles) to 22 (every tile
+    swizzled stage buffers, a producer warp, one tile group per CTA, one or
+    two CTAs per SM): the oracle's amplitudes; from 13 qubits (two tiles) to 22 (every tile
     shape the planner makes, including tiles with more than four runs)."""
     old = {k: capi.tuning_get(k) for k in knobs}
     try:
