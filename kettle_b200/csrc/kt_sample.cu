@@ -256,7 +256,10 @@ __global__ void k_sample_fast(const double* __restrict__ p, const double* __rest
 //     units is passed over in O(1) (its start value is recorded); any other
 //     tile is computed element by element from the exact s (the same integer
 //     scan, with one IEEE add for each tie, huge term or binade exit);
-//  4. every recorded tile writes its CDF from its exact start value.
+//  4. every recorded tile writes its CDF from its exact start value: all of
+//     them for a caller's probability vector; for the state's own
+//     probabilities only the tiles that the bound and the shots land in,
+//     found from the exact tile start values (k_shot_tiles below).
 // A wrong guess only sends a tile down the element-by-element path: the
 // result never depends on the approximate sums.
 constexpr int XS_THREADS = 1024;
@@ -594,11 +597,14 @@ __global__ void __launch_bounds__(256) k_tile_ints(const double* __restrict__ p,
 }
 
 // 3. one block: the exact running value through all tiles.  carry[t] gets the
-// exact value before tile t, or -1 when the tile's CDF was written here.
+// exact value before tile t, or -1 when the tile's CDF was written here;
+// tstart[t] the exact value before tile t in every case, and tstart[n_tiles]
+// the last CDF value (so tstart[t + 1] is tile t's last CDF value).
 __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const double* __restrict__ p, uint64_t N, uint64_t n_tiles,
                                                             const int* __restrict__ code,
                                                             const unsigned long long* __restrict__ ints,
-                                                            double* __restrict__ carry, double* __restrict__ cdf)
+                                                            double* __restrict__ carry, double* __restrict__ tstart,
+                                                            double* __restrict__ cdf)
 {
     __shared__ XState X;
     __shared__ unsigned long long t_sh;
@@ -647,7 +653,9 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const double* __rest
         __syncthreads();
         const unsigned int first = first_sh;
         if (static_cast<unsigned int>(t) < first) {
-            carry[tile] = normal ? static_cast<double>(m + excl) * u : s;
+            const double c0 = normal ? static_cast<double>(m + excl) * u : s;
+            carry[tile] = c0;
+            tstart[tile] = c0;
             if (static_cast<unsigned int>(t) + 1 == first) {
                 m_sh = m + excl + I;
             }
@@ -670,6 +678,9 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const double* __rest
         // tile `bad`, element by element from the exact value
         const uint64_t beg = bad * XS_TILE;
         const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+        if (t == 0) {
+            tstart[bad] = s_sh;
+        }
         const double s_out = exact_range(p, beg, end, s_sh, cdf, X);
         __syncthreads();
         if (t == 0) {
@@ -679,12 +690,18 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const double* __rest
         }
         __syncthreads();
     }
+    if (t == 0) {
+        tstart[n_tiles] = s_sh;
+    }
 }
 
-// 4. the CDF of every tile passed over in step 3, from its exact start value
+// 4. the CDF of every tile passed over in step 3 (list == nullptr: block b
+// writes tile b), or of the *count tiles in `list`, from its exact start value
 __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const double* __restrict__ p, uint64_t N,
                                                            const int* __restrict__ code,
-                                                           const double* __restrict__ carry, double* __restrict__ cdf)
+                                                           const double* __restrict__ carry, double* __restrict__ cdf,
+                                                           const unsigned long long* __restrict__ list,
+                                                           const unsigned int* __restrict__ count)
 {
     // warp w holds the tile's elements [w * 32 * XS_EPT, (w + 1) * 32 * XS_EPT)
     // as XS_EPT rows of 32 consecutive elements, one per lane, so every load
@@ -692,15 +709,22 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const double* __restr
     // runs row by row (a warp scan per row, the warp's earlier rows carried)
     // after a block scan of the warp totals, in element order
     __shared__ unsigned long long sh[32];
-    const double c0 = carry[blockIdx.x];
+    uint64_t tile = blockIdx.x;
+    if (list != nullptr) {
+        if (blockIdx.x >= *count) {
+            return;
+        }
+        tile = list[blockIdx.x];
+    }
+    const double c0 = carry[tile];
     if (c0 < 0.0) {
         return;
     }
-    const uint64_t beg = static_cast<uint64_t>(blockIdx.x) * XS_TILE;
+    const uint64_t beg = tile * XS_TILE;
     const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
     const int lane = static_cast<int>(threadIdx.x & 31);
     const uint64_t wb = beg + static_cast<uint64_t>(threadIdx.x >> 5) * (32 * XS_EPT) + lane;
-    const int c = code[blockIdx.x];
+    const int c = code[tile];
     if (c == TILE_ZERO) {
         for (int k = 0; k < XS_EPT; ++k) {
             const uint64_t g = wb + static_cast<uint64_t>(k) * 32;
@@ -748,28 +772,6 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const double* __restr
 
 // cumulative_end_offset_ (measurements.cpp:235-256): the last value strictly
 // below `last`, found as the largest index holding one.
-// The same index by binary search, for a non-decreasing CDF (every
-// probability >= 0, so each sequential sum is at least the one before): the
-// first index whose value is not below the last one.
-__global__ void k_last_below_sorted(const double* __restrict__ cdf, uint64_t N, unsigned long long* __restrict__ idx1)
-{
-    if (threadIdx.x != 0 || blockIdx.x != 0) {
-        return;
-    }
-    const double last = cdf[N - 1];
-    uint64_t lo = 0, len = N;
-    while (len > 0) {
-        const uint64_t half = len / 2;
-        if (cdf[lo + half] < last) {
-            lo = lo + half + 1;
-            len = len - half - 1;
-        } else {
-            len = half;
-        }
-    }
-    *idx1 = static_cast<unsigned long long>(lo);
-}
-
 __global__ void k_last_below(const double* __restrict__ cdf, uint64_t N, unsigned long long* __restrict__ idx1)
 {
     const double last = cdf[N - 1];
@@ -824,6 +826,117 @@ __global__ void k_seq_search(const double* __restrict__ cdf, uint64_t N, const d
     out[s] = lo < N ? lo : N - 1;
 }
 
+// The searches above on a CDF written only where they look.  For a
+// non-decreasing CDF (the state's own probabilities are never negative)
+// lower_bound(cdf, v) lies in the first tile whose last value, tstart[t + 1],
+// is not below v: every element of the tiles before it is at most their last
+// value, which is below v.  So the distribution bound and every shot first
+// pick their tile from the n_tiles + 1 exact tile start values, the tiles
+// picked (at most one per shot, plus the bound's) get their CDF written, and
+// each search finishes inside its tile: the same indices as the searches over
+// the whole CDF, without writing the 8 B per amplitude of the other tiles.
+
+// the first t in [0, n_tiles) with tstart[t + 1] >= v, or n_tiles
+__device__ __forceinline__ uint64_t tile_of(const double* __restrict__ tstart, uint64_t n_tiles, double v)
+{
+    uint64_t lo = 0, len = n_tiles;
+    while (len > 0) {
+        const uint64_t half = len / 2;
+        if (tstart[lo + half + 1] < v) {
+            lo = lo + half + 1;
+            len = len - half - 1;
+        } else {
+            len = half;
+        }
+    }
+    return lo;
+}
+
+// lower_bound(cdf + beg, cdf + end, v) - cdf
+__device__ __forceinline__ uint64_t lower_bound_in(const double* __restrict__ cdf, uint64_t beg, uint64_t end, double v)
+{
+    uint64_t lo = beg, len = end - beg;
+    while (len > 0) {
+        const uint64_t half = len / 2;
+        if (cdf[lo + half] < v) {
+            lo = lo + half + 1;
+            len = len - half - 1;
+        } else {
+            len = half;
+        }
+    }
+    return lo;
+}
+
+// the tile holding lower_bound(cdf, last), listed alone for k_tile_write
+__global__ void k_bound_tile(const double* __restrict__ tstart, uint64_t n_tiles, unsigned long long* __restrict__ list,
+                             unsigned int* __restrict__ count)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) {
+        return;
+    }
+    const uint64_t t = tile_of(tstart, n_tiles, tstart[n_tiles]);
+    list[0] = t < n_tiles ? t : n_tiles - 1;
+    *count = 1;
+}
+
+// cumulative_end_offset_ and the distribution bound (measurements.cpp:235-256,
+// 288-295) from the bound tile's CDF: j = lower_bound(cdf, last), second =
+// cdf[j - 1] (the previous tile's last value, tstart[t], when j starts tile t)
+__global__ void k_sparse_bound(const double* __restrict__ cdf, uint64_t N, const double* __restrict__ tstart,
+                               uint64_t n_tiles, const unsigned long long* __restrict__ list, double* __restrict__ bound)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) {
+        return;
+    }
+    const double last = tstart[n_tiles];
+    const uint64_t t = list[0];
+    const uint64_t beg = t * XS_TILE;
+    const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+    const uint64_t j = lower_bound_in(cdf, beg, end, last);
+    const double second = (j == 0) ? 0.0 : (j == beg ? tstart[t] : cdf[j - 1]);
+    const double offset = __dmul_rn(__dsub_rn(last, second), 1.0e-4);
+    *bound = __dsub_rn(last, offset);
+}
+
+// each shot's tile; every tile some shot picks is listed once
+__global__ void k_shot_tiles(const double* __restrict__ tstart, uint64_t n_tiles, const double* __restrict__ bound,
+                             const double* __restrict__ canon, int64_t n_shots,
+                             unsigned long long* __restrict__ shot_tile, int* __restrict__ hit,
+                             unsigned long long* __restrict__ list, unsigned int* __restrict__ count)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_shots) {
+        return;
+    }
+    const double u = __dadd_rn(__dmul_rn(canon[s], __dsub_rn(*bound, 0.0)), 0.0);
+    const uint64_t t = tile_of(tstart, n_tiles, u);
+    shot_tile[s] = t;
+    if (t < n_tiles && atomicExch(&hit[t], 1) == 0) {
+        list[atomicAdd(count, 1U)] = t;
+    }
+}
+
+__global__ void k_shot_search(const double* __restrict__ cdf, uint64_t N, uint64_t n_tiles,
+                              const double* __restrict__ bound, const double* __restrict__ canon, int64_t n_shots,
+                              const unsigned long long* __restrict__ shot_tile, uint64_t* __restrict__ out)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_shots) {
+        return;
+    }
+    const uint64_t t = shot_tile[s];
+    if (t >= n_tiles) {
+        out[s] = N - 1;  // u above every CDF value: lower_bound gives N, clamped as k_seq_search does
+        return;
+    }
+    const double u = __dadd_rn(__dmul_rn(canon[s], __dsub_rn(*bound, 0.0)), 0.0);
+    const uint64_t beg = t * XS_TILE;
+    const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+    const uint64_t lo = lower_bound_in(cdf, beg, end, u);
+    out[s] = lo < N ? lo : N - 1;
+}
+
 }  // namespace
 
 namespace
@@ -860,7 +973,12 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     const size_t off_code = al(off_tsum + n_xt * 8);
     const size_t off_ints = al(off_code + n_xt * 4);
     const size_t off_carry = al(off_ints + n_xt * 8);
-    if (const int32_t rc = s.scratch.reserve(off_carry + n_xt * 8); rc != KT_OK) {
+    const size_t off_tstart = al(off_carry + n_xt * 8);
+    const size_t off_hit = al(off_tstart + (n_xt + 1) * 8);
+    const size_t off_list = al(off_hit + n_xt * 4);
+    const size_t off_count = al(off_list + n_xt * 8);
+    const size_t off_stile = al(off_count + 8);
+    if (const int32_t rc = s.scratch.reserve(off_stile + ns * 8); rc != KT_OK) {
         return rc;
     }
     double* dp = static_cast<double*>(s.scratch2.ptr);
@@ -878,6 +996,11 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     auto* d_code = reinterpret_cast<int*>(base + off_code);
     auto* d_ints = reinterpret_cast<unsigned long long*>(base + off_ints);
     auto* d_carry = reinterpret_cast<double*>(base + off_carry);
+    auto* d_tstart = reinterpret_cast<double*>(base + off_tstart);
+    auto* d_hit = reinterpret_cast<int*>(base + off_hit);
+    auto* d_list = reinterpret_cast<unsigned long long*>(base + off_list);
+    auto* d_count = reinterpret_cast<unsigned int*>(base + off_count);
+    auto* d_stile = reinterpret_cast<unsigned long long*>(base + off_stile);
 
     // the exact tier straight away (above the fast tier's size) on the state's
     // own noiseless probabilities: their pass also forms the tile sums
@@ -934,25 +1057,44 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
         KT_CHECK_LAUNCH("k_tile_guess");
         k_tile_ints<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_code, d_ints);
         KT_CHECK_LAUNCH("k_tile_ints");
-        k_exact_chain<<<1, XS_THREADS, 0, s.stream>>>(dp, N, n_tiles, d_code, d_ints, d_carry, dcdf);
+        k_exact_chain<<<1, XS_THREADS, 0, s.stream>>>(dp, N, n_tiles, d_code, d_ints, d_carry, d_tstart, dcdf);
         KT_CHECK_LAUNCH("k_exact_chain");
-        k_tile_write<<<static_cast<unsigned>(n_tiles), XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf);
-        KT_CHECK_LAUNCH("k_tile_write");
+        const unsigned shot_blocks = static_cast<unsigned>((ns + 127) / 128);
         if (host_probs == nullptr) {
-            // |a_i|^2 (and readout noise, a mix of them) are never negative
-            k_last_below_sorted<<<1, 32, 0, s.stream>>>(dcdf, N, d_nz);
-            KT_CHECK_LAUNCH("k_last_below_sorted");
+            // |a_i|^2 (and readout noise, a mix of them) are never negative: the
+            // CDF never decreases, and only the tiles the searches land in are written
+            k_bound_tile<<<1, 32, 0, s.stream>>>(d_tstart, n_tiles, d_list, d_count);
+            KT_CHECK_LAUNCH("k_bound_tile");
+            k_tile_write<<<1, XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf, d_list, d_count);
+            KT_CHECK_LAUNCH("k_tile_write");
+            k_sparse_bound<<<1, 32, 0, s.stream>>>(dcdf, N, d_tstart, n_tiles, d_list, d_bound);
+            KT_CHECK_LAUNCH("k_sparse_bound");
+            KT_CUDA(cudaMemsetAsync(d_hit, 0, n_tiles * 4, s.stream));
+            KT_CUDA(cudaMemsetAsync(d_count, 0, 4, s.stream));
+            k_shot_tiles<<<shot_blocks, 128, 0, s.stream>>>(d_tstart, n_tiles, d_bound, d_canon, n_shots, d_stile,
+                                                           d_hit, d_list, d_count);
+            KT_CHECK_LAUNCH("k_shot_tiles");
+            const unsigned n_write = static_cast<unsigned>(std::min<uint64_t>(ns, n_tiles));
+            k_tile_write<<<n_write, XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf, d_list, d_count);
+            KT_CHECK_LAUNCH("k_tile_write");
+            k_shot_search<<<shot_blocks, 128, 0, s.stream>>>(dcdf, N, n_tiles, d_bound, d_canon, n_shots, d_stile,
+                                                            d_out);
+            KT_CHECK_LAUNCH("k_shot_search");
         } else {
+            // a caller's vector may hold negative entries: the whole CDF, and the
+            // reference's scan for the end offset
+            k_tile_write<<<static_cast<unsigned>(n_tiles), XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf,
+                                                                                      nullptr, nullptr);
+            KT_CHECK_LAUNCH("k_tile_write");
             KT_CUDA(cudaMemsetAsync(d_nz, 0, 8, s.stream));
             const unsigned lb_blocks = static_cast<unsigned>(std::min<uint64_t>((N + 255) / 256, sm_count() * 8ULL));
             k_last_below<<<lb_blocks, 256, 0, s.stream>>>(dcdf, N, d_nz);
             KT_CHECK_LAUNCH("k_last_below");
+            k_seq_bound<<<1, 32, 0, s.stream>>>(dcdf, N, d_nz, d_bound);
+            KT_CHECK_LAUNCH("k_seq_bound");
+            k_seq_search<<<shot_blocks, 128, 0, s.stream>>>(dcdf, N, d_bound, d_canon, n_shots, d_out);
+            KT_CHECK_LAUNCH("k_seq_search");
         }
-        k_seq_bound<<<1, 32, 0, s.stream>>>(dcdf, N, d_nz, d_bound);
-        KT_CHECK_LAUNCH("k_seq_bound");
-        k_seq_search<<<static_cast<unsigned>((ns + 127) / 128), 128, 0, s.stream>>>(dcdf, N, d_bound, d_canon, n_shots,
-                                                                                     d_out);
-        KT_CHECK_LAUNCH("k_seq_search");
         if (n_rescanned) {
             *n_rescanned = 1;
         }
