@@ -305,6 +305,34 @@ __device__ __forceinline__ unsigned long long block_excl_scan_u64(unsigned long 
     return r;
 }
 
+// Where the exact tier reads probability i: a vector (a caller's, or the
+// state's with readout noise, written by the probability pass), or the
+// state's own |a_i|^2 formed on the spot exactly as the probability pass
+// forms them (round-to-nearest products and sum, no contraction), so the
+// noiseless state path never writes the 8 B per amplitude vector.
+struct ProbVec
+{
+    const double* __restrict__ p;
+    __device__ __forceinline__ double operator[](uint64_t i) const { return p[i]; }
+};
+
+template <typename C>
+struct ProbAmps
+{
+    const C* __restrict__ a;
+    __device__ __forceinline__ double operator[](uint64_t i) const
+    {
+        const double2 v = to_d2(a[i]);
+        return __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
+    }
+};
+
+// Tile integer sums for these binades are formed during the probability pass
+// (candidate k: the binade [2^(-k-1), 2^-k), units 2^(-k-53)): a normalised
+// state's running sum starts most tiles in [1/16, 1), so only the other
+// tiles are read a second time by k_tile_ints.
+constexpr int N_CAND = 4;
+
 // shared state of the element-by-element path
 struct XState
 {
@@ -316,8 +344,8 @@ struct XState
 
 // cdf[beg, end) as the sequential sum continued from the exact value s_in, by
 // the whole block (XS_THREADS threads); returns the value after element end-1.
-__device__ double exact_range(const double* __restrict__ p, uint64_t beg, uint64_t end, double s_in,
-                              double* __restrict__ cdf, XState& X)
+template <typename P>
+__device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in, double* __restrict__ cdf, XState& X)
 {
     const int t = threadIdx.x;
     __syncthreads();
@@ -458,26 +486,88 @@ __global__ void __launch_bounds__(256) k_tile_sums(const double* __restrict__ p,
     }
 }
 
-// 0 + 1 fused, for the state's own probabilities without readout noise:
-// |a_i|^2 exactly as k_probs writes them (round-to-nearest products and sum,
-// no contraction) and each tile's FP64 sum on the way (any order, as above)
+// 0 + 1 + 2 fused, for the state's own probabilities without readout noise:
+// each tile's FP64 sum of |a_i|^2 (any order, as above) and its integer sums
+// in the N_CAND candidate binades with their tie / huge-term flags (bit k of
+// cflag), as k_tile_ints forms them; the probabilities are not stored
 template <typename C>
-__global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, uint64_t N, double* __restrict__ p,
-                                                     double* __restrict__ tsum)
+__global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, uint64_t N, double* __restrict__ tsum,
+                                                     unsigned long long* __restrict__ cints, int* __restrict__ cflag)
 {
     __shared__ double sh[8];
+    __shared__ unsigned long long shi[N_CAND][8];
+    __shared__ int flag_sh;
+    if (threadIdx.x == 0) {
+        flag_sh = 0;
+    }
+    const ProbAmps<C> p {a};
     const uint64_t beg = static_cast<uint64_t>(blockIdx.x) * XS_TILE;
     const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
     double acc = 0.0;
+    // x_k = q 2^(53+k) = 2^k x_0: with x_0 = fl + F (fl an integer, F in [0, 1)),
+    // rint(x_k) = 2^k fl + floor(2^k F + 1/2) away from ties, and with the top
+    // four bits of F as T = floor(16 F) (exact: 16 F is a scaling) that is
+    // (T + 2^(3-k)) >> (4-k); x_k is a tie when 2^(k+1) F is an odd integer,
+    // i.e. 16 F is an integer with T's low 4-k bits equal to 2^(3-k).
+    unsigned long long sfl = 0;  // sum of fl
+    unsigned int small[N_CAND];
+#pragma unroll
+    for (int k = 0; k < N_CAND; ++k) {
+        small[k] = 0;
+    }
+    int fl = 0;
     for (uint64_t i = beg + threadIdx.x; i < end; i += 256) {
-        const double2 v = to_d2(a[i]);
-        const double q = __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
-        p[i] = q;
+        const double q = p[i];
         acc += q;
+        const double x0 = q * 0x1p53;  // exact: a power of two
+        if (!(x0 < 0x1p47)) {
+            // 2^50 units and more in some candidate binade (or inf / NaN)
+#pragma unroll
+            for (int k = 0; k < N_CAND; ++k) {
+                if (!(x0 < static_cast<double>(1ULL << (50 - k)))) {
+                    fl |= 1 << k;
+                }
+            }
+        }
+        const double f0 = floor(x0);
+        const double y = (x0 - f0) * 16.0;  // exact
+        const double ty = floor(y);
+        const unsigned int T = static_cast<unsigned int>(ty);
+        const bool whole = (y == ty);
+        sfl += static_cast<unsigned long long>(f0);
+#pragma unroll
+        for (int k = 0; k < N_CAND; ++k) {
+            small[k] += (T + (8u >> k)) >> (4 - k);
+            if (whole && (T & ((16u >> k) - 1u)) == (8u >> k)) {
+                fl |= 1 << k;
+            }
+        }
+    }
+    unsigned long long ci[N_CAND];
+#pragma unroll
+    for (int k = 0; k < N_CAND; ++k) {
+        // can wrap only when candidate k is flagged (a term of 2^50 units or
+        // more), and a flagged candidate's sum is never used
+        ci[k] = (sfl << k) + small[k];
     }
     acc = warp_sum_d(acc);
+#pragma unroll
+    for (int k = 0; k < N_CAND; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ci[k] += __shfl_down_sync(0xffffffffU, ci[k], o);
+        }
+    }
+    __syncthreads();  // flag_sh is cleared
+    if (fl != 0) {
+        atomicOr(&flag_sh, fl);
+    }
     if ((threadIdx.x & 31) == 0) {
         sh[threadIdx.x >> 5] = acc;
+#pragma unroll
+        for (int k = 0; k < N_CAND; ++k) {
+            shi[k][threadIdx.x >> 5] = ci[k];
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -486,12 +576,25 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
             t += sh[w];
         }
         tsum[blockIdx.x] = t;
+        for (int k = 0; k < N_CAND; ++k) {
+            unsigned long long v = 0;
+            for (int w = 0; w < 8; ++w) {
+                v += shi[k][w];
+            }
+            cints[static_cast<uint64_t>(blockIdx.x) * N_CAND + k] = v;
+        }
+        cflag[blockIdx.x] = flag_sh;
     }
 }
 
 // 1b. one block: approximate start value of every tile, and its binade guess
+// (with cints: a tile guessed in a candidate binade takes that binade's
+// integer sum, or goes dirty when the probability pass flagged it there)
 __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restrict__ tsum, uint64_t n_tiles,
-                                                           int* __restrict__ code)
+                                                           int* __restrict__ code,
+                                                           const unsigned long long* __restrict__ cints,
+                                                           const int* __restrict__ cflag,
+                                                           unsigned long long* __restrict__ ints)
 {
     __shared__ double sh[32];
     const int t = threadIdx.x;
@@ -543,19 +646,29 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restr
                 c = e0;
             }
         }
+        if (cints != nullptr && c <= 0 && c > -N_CAND) {
+            const int j = -c;
+            if ((cflag[k] >> j) & 1) {
+                c = TILE_DIRTY;
+            } else {
+                ints[k] = cints[k * N_CAND + static_cast<uint64_t>(j)];
+            }
+        }
         code[k] = c;
         a0 = a1;
     }
 }
 
 // 2. integer sum of a tile in the units of its guessed binade; flags demote it
-__global__ void __launch_bounds__(256) k_tile_ints(const double* __restrict__ p, uint64_t N, int* __restrict__ code,
-                                                   unsigned long long* __restrict__ ints)
+// (with_cand: tiles guessed in a candidate binade have theirs already)
+template <typename P>
+__global__ void __launch_bounds__(256) k_tile_ints(const P p, uint64_t N, int* __restrict__ code,
+                                                   unsigned long long* __restrict__ ints, int with_cand)
 {
     __shared__ unsigned long long sh[8];
     __shared__ int flag_sh;
     const int c = code[blockIdx.x];
-    if (c == TILE_ZERO || c == TILE_DIRTY) {
+    if (c == TILE_ZERO || c == TILE_DIRTY || (with_cand && c <= 0 && c > -N_CAND)) {
         return;
     }
     if (threadIdx.x == 0) {
@@ -600,7 +713,8 @@ __global__ void __launch_bounds__(256) k_tile_ints(const double* __restrict__ p,
 // exact value before tile t, or -1 when the tile's CDF was written here;
 // tstart[t] the exact value before tile t in every case, and tstart[n_tiles]
 // the last CDF value (so tstart[t + 1] is tile t's last CDF value).
-__global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const double* __restrict__ p, uint64_t N, uint64_t n_tiles,
+template <typename P>
+__global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const P p, uint64_t N, uint64_t n_tiles,
                                                             const int* __restrict__ code,
                                                             const unsigned long long* __restrict__ ints,
                                                             double* __restrict__ carry, double* __restrict__ tstart,
@@ -697,7 +811,8 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const double* __rest
 
 // 4. the CDF of every tile passed over in step 3 (list == nullptr: block b
 // writes tile b), or of the *count tiles in `list`, from its exact start value
-__global__ void __launch_bounds__(XS_THREADS) k_tile_write(const double* __restrict__ p, uint64_t N,
+template <typename P>
+__global__ void __launch_bounds__(XS_THREADS) k_tile_write(const P p, uint64_t N,
                                                            const int* __restrict__ code,
                                                            const double* __restrict__ carry, double* __restrict__ cdf,
                                                            const unsigned long long* __restrict__ list,
@@ -942,6 +1057,73 @@ __global__ void k_shot_search(const double* __restrict__ cdf, uint64_t N, uint64
 namespace
 {
 
+// device buffers of the exact tier
+struct ExactBufs
+{
+    uint64_t N, n_tiles;
+    int64_t n_shots;
+    int* code;
+    unsigned long long* ints;
+    double* carry;
+    double* tstart;
+    double* cdf;
+    int* hit;
+    unsigned long long* list;
+    unsigned int* count;
+    unsigned long long* stile;
+    unsigned long long* nz;
+    double* bound;
+    const double* canon;
+    uint64_t* out;
+};
+
+// steps 2-4 of the exact tier and the searches, reading probabilities from p.
+// sorted: every probability is >= 0 (the state's own), so the CDF never
+// decreases and only the tiles the searches land in are written.
+template <typename P>
+int32_t exact_tail(cudaStream_t st, const P p, const ExactBufs& b, bool with_cand, bool sorted)
+{
+    const uint64_t N = b.N, n_tiles = b.n_tiles;
+    k_tile_ints<P><<<static_cast<unsigned>(n_tiles), 256, 0, st>>>(p, N, b.code, b.ints, with_cand ? 1 : 0);
+    KT_CHECK_LAUNCH("k_tile_ints");
+    k_exact_chain<P><<<1, XS_THREADS, 0, st>>>(p, N, n_tiles, b.code, b.ints, b.carry, b.tstart, b.cdf);
+    KT_CHECK_LAUNCH("k_exact_chain");
+    const unsigned shot_blocks = static_cast<unsigned>((b.n_shots + 127) / 128);
+    if (sorted) {
+        k_bound_tile<<<1, 32, 0, st>>>(b.tstart, n_tiles, b.list, b.count);
+        KT_CHECK_LAUNCH("k_bound_tile");
+        k_tile_write<P><<<1, XS_THREADS, 0, st>>>(p, N, b.code, b.carry, b.cdf, b.list, b.count);
+        KT_CHECK_LAUNCH("k_tile_write");
+        k_sparse_bound<<<1, 32, 0, st>>>(b.cdf, N, b.tstart, n_tiles, b.list, b.bound);
+        KT_CHECK_LAUNCH("k_sparse_bound");
+        KT_CUDA(cudaMemsetAsync(b.hit, 0, n_tiles * 4, st));
+        KT_CUDA(cudaMemsetAsync(b.count, 0, 4, st));
+        k_shot_tiles<<<shot_blocks, 128, 0, st>>>(b.tstart, n_tiles, b.bound, b.canon, b.n_shots, b.stile, b.hit, b.list,
+                                                  b.count);
+        KT_CHECK_LAUNCH("k_shot_tiles");
+        const unsigned n_write = static_cast<unsigned>(std::min<uint64_t>(static_cast<uint64_t>(b.n_shots), n_tiles));
+        k_tile_write<P><<<n_write, XS_THREADS, 0, st>>>(p, N, b.code, b.carry, b.cdf, b.list, b.count);
+        KT_CHECK_LAUNCH("k_tile_write");
+        k_shot_search<<<shot_blocks, 128, 0, st>>>(b.cdf, N, n_tiles, b.bound, b.canon, b.n_shots, b.stile, b.out);
+        KT_CHECK_LAUNCH("k_shot_search");
+        return KT_OK;
+    }
+    // a caller's vector may hold negative entries: the whole CDF, and the
+    // reference's scan for the end offset
+    k_tile_write<P><<<static_cast<unsigned>(n_tiles), XS_THREADS, 0, st>>>(p, N, b.code, b.carry, b.cdf, nullptr,
+                                                                           nullptr);
+    KT_CHECK_LAUNCH("k_tile_write");
+    KT_CUDA(cudaMemsetAsync(b.nz, 0, 8, st));
+    const unsigned lb_blocks = static_cast<unsigned>(std::min<uint64_t>((N + 255) / 256, sm_count() * 8ULL));
+    k_last_below<<<lb_blocks, 256, 0, st>>>(b.cdf, N, b.nz);
+    KT_CHECK_LAUNCH("k_last_below");
+    k_seq_bound<<<1, 32, 0, st>>>(b.cdf, N, b.nz, b.bound);
+    KT_CHECK_LAUNCH("k_seq_bound");
+    k_seq_search<<<shot_blocks, 128, 0, st>>>(b.cdf, N, b.bound, b.canon, b.n_shots, b.out);
+    KT_CHECK_LAUNCH("k_seq_search");
+    return KT_OK;
+}
+
 // The sampler over N probabilities: the state's own (|a_i|^2 with its noise)
 // or, with host_probs, a caller's vector uploaded as it is.
 int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double* noise, const double* canonicals,
@@ -978,7 +1160,9 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     const size_t off_list = al(off_hit + n_xt * 4);
     const size_t off_count = al(off_list + n_xt * 8);
     const size_t off_stile = al(off_count + 8);
-    if (const int32_t rc = s.scratch.reserve(off_stile + ns * 8); rc != KT_OK) {
+    const size_t off_cints = al(off_stile + ns * 8);
+    const size_t off_cflag = al(off_cints + n_xt * N_CAND * 8);
+    if (const int32_t rc = s.scratch.reserve(off_cflag + n_xt * 4); rc != KT_OK) {
         return rc;
     }
     double* dp = static_cast<double*>(s.scratch2.ptr);
@@ -1001,9 +1185,12 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     auto* d_list = reinterpret_cast<unsigned long long*>(base + off_list);
     auto* d_count = reinterpret_cast<unsigned int*>(base + off_count);
     auto* d_stile = reinterpret_cast<unsigned long long*>(base + off_stile);
+    auto* d_cints = reinterpret_cast<unsigned long long*>(base + off_cints);
+    auto* d_cflag = reinterpret_cast<int*>(base + off_cflag);
 
     // the exact tier straight away (above the fast tier's size) on the state's
-    // own noiseless probabilities: their pass also forms the tile sums
+    // own noiseless probabilities: their pass forms the tile sums and the
+    // candidate integer sums, and stores no probabilities
     const bool fused_tiles = host_probs == nullptr && noise == nullptr && !(mode == 0 && N <= (uint64_t {1} << 22));
     if (host_probs != nullptr) {
         if (const int32_t rc = copy_h2d(dp, host_probs, N * 8, s.stream); rc != KT_OK) {
@@ -1012,9 +1199,11 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     } else if (fused_tiles) {
         const unsigned nt = static_cast<unsigned>((N + XS_TILE - 1) / XS_TILE);
         if (s.dtype == KT_C128) {
-            k_probs_tiles<double2><<<nt, 256, 0, s.stream>>>(static_cast<const double2*>(s.amps), N, dp, d_tsum);
+            k_probs_tiles<double2><<<nt, 256, 0, s.stream>>>(static_cast<const double2*>(s.amps), N, d_tsum, d_cints,
+                                                             d_cflag);
         } else {
-            k_probs_tiles<float2><<<nt, 256, 0, s.stream>>>(static_cast<const float2*>(s.amps), N, dp, d_tsum);
+            k_probs_tiles<float2><<<nt, 256, 0, s.stream>>>(static_cast<const float2*>(s.amps), N, d_tsum, d_cints,
+                                                            d_cflag);
         }
         KT_CHECK_LAUNCH("k_probs_tiles");
     } else if (const int32_t rc = device_probabilities(s, noise, dp); rc != KT_OK) {
@@ -1053,47 +1242,21 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
             k_tile_sums<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_tsum);
             KT_CHECK_LAUNCH("k_tile_sums");
         }
-        k_tile_guess<<<1, XS_THREADS, 0, s.stream>>>(d_tsum, n_tiles, d_code);
+        k_tile_guess<<<1, XS_THREADS, 0, s.stream>>>(d_tsum, n_tiles, d_code, fused_tiles ? d_cints : nullptr, d_cflag,
+                                                     d_ints);
         KT_CHECK_LAUNCH("k_tile_guess");
-        k_tile_ints<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_code, d_ints);
-        KT_CHECK_LAUNCH("k_tile_ints");
-        k_exact_chain<<<1, XS_THREADS, 0, s.stream>>>(dp, N, n_tiles, d_code, d_ints, d_carry, d_tstart, dcdf);
-        KT_CHECK_LAUNCH("k_exact_chain");
-        const unsigned shot_blocks = static_cast<unsigned>((ns + 127) / 128);
-        if (host_probs == nullptr) {
-            // |a_i|^2 (and readout noise, a mix of them) are never negative: the
-            // CDF never decreases, and only the tiles the searches land in are written
-            k_bound_tile<<<1, 32, 0, s.stream>>>(d_tstart, n_tiles, d_list, d_count);
-            KT_CHECK_LAUNCH("k_bound_tile");
-            k_tile_write<<<1, XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf, d_list, d_count);
-            KT_CHECK_LAUNCH("k_tile_write");
-            k_sparse_bound<<<1, 32, 0, s.stream>>>(dcdf, N, d_tstart, n_tiles, d_list, d_bound);
-            KT_CHECK_LAUNCH("k_sparse_bound");
-            KT_CUDA(cudaMemsetAsync(d_hit, 0, n_tiles * 4, s.stream));
-            KT_CUDA(cudaMemsetAsync(d_count, 0, 4, s.stream));
-            k_shot_tiles<<<shot_blocks, 128, 0, s.stream>>>(d_tstart, n_tiles, d_bound, d_canon, n_shots, d_stile,
-                                                           d_hit, d_list, d_count);
-            KT_CHECK_LAUNCH("k_shot_tiles");
-            const unsigned n_write = static_cast<unsigned>(std::min<uint64_t>(ns, n_tiles));
-            k_tile_write<<<n_write, XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf, d_list, d_count);
-            KT_CHECK_LAUNCH("k_tile_write");
-            k_shot_search<<<shot_blocks, 128, 0, s.stream>>>(dcdf, N, n_tiles, d_bound, d_canon, n_shots, d_stile,
-                                                            d_out);
-            KT_CHECK_LAUNCH("k_shot_search");
+        const ExactBufs xb {N,     n_tiles, n_shots, d_code,  d_ints, d_carry, d_tstart, dcdf,
+                            d_hit, d_list,  d_count, d_stile, d_nz,   d_bound, d_canon,  d_out};
+        int32_t rc = KT_OK;
+        if (!fused_tiles) {
+            rc = exact_tail(s.stream, ProbVec {dp}, xb, false, host_probs == nullptr);
+        } else if (s.dtype == KT_C128) {
+            rc = exact_tail(s.stream, ProbAmps<double2> {static_cast<const double2*>(s.amps)}, xb, true, true);
         } else {
-            // a caller's vector may hold negative entries: the whole CDF, and the
-            // reference's scan for the end offset
-            k_tile_write<<<static_cast<unsigned>(n_tiles), XS_THREADS, 0, s.stream>>>(dp, N, d_code, d_carry, dcdf,
-                                                                                      nullptr, nullptr);
-            KT_CHECK_LAUNCH("k_tile_write");
-            KT_CUDA(cudaMemsetAsync(d_nz, 0, 8, s.stream));
-            const unsigned lb_blocks = static_cast<unsigned>(std::min<uint64_t>((N + 255) / 256, sm_count() * 8ULL));
-            k_last_below<<<lb_blocks, 256, 0, s.stream>>>(dcdf, N, d_nz);
-            KT_CHECK_LAUNCH("k_last_below");
-            k_seq_bound<<<1, 32, 0, s.stream>>>(dcdf, N, d_nz, d_bound);
-            KT_CHECK_LAUNCH("k_seq_bound");
-            k_seq_search<<<shot_blocks, 128, 0, s.stream>>>(dcdf, N, d_bound, d_canon, n_shots, d_out);
-            KT_CHECK_LAUNCH("k_seq_search");
+            rc = exact_tail(s.stream, ProbAmps<float2> {static_cast<const float2*>(s.amps)}, xb, true, true);
+        }
+        if (rc != KT_OK) {
+            return rc;
         }
         if (n_rescanned) {
             *n_rescanned = 1;

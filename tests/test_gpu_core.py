@@ -377,6 +377,26 @@ def test_sampling_large_state_exact(engine, port):
     assert np.array_equal(idx, port.sample(n, port.probabilities(n, psi), can))
 
 
+@pytest.mark.parametrize("n,mode", [(18, 1), (23, 0)])
+def test_sampling_complex64_state(engine, port, n, mode):
+    """A complex64 state's shots: |a_i|^2 is formed from the FP32 amplitudes
+    widened to FP64, so the oracle's sequential CDF over the stored values
+    (downloaded, exact in complex128) gives the same indices, also for
+    draws placed on tile boundaries."""
+    sv = capi.Statevector(n, capi.KT_C64)
+    sv.upload(random_state(n, 40 + n))
+    stored = sv.download()
+    probs = port.probabilities(n, stored)
+    rng = np.random.default_rng(n)
+    tiles = np.arange(0, 1 << n, 16384)
+    pos = np.unique(np.clip(np.concatenate([tiles - 1, tiles, rng.integers(0, 1 << n, 500)]), 0, (1 << n) - 1))
+    can = np.concatenate([_exact_probes(probs, pos[:: max(1, pos.size // 1500)]), port.canonicals(13, 2000)])
+    idx, rescanned = sv.sample(can, mode=mode)
+    assert rescanned == 1
+    assert np.array_equal(idx, port.sample(n, probs, can))
+    sv.close()
+
+
 def _exact_probes(probs, positions):
     """Canonicals c whose drawn value u = c * bound lands exactly on the
     sequential CDF value at `positions` or one ulp above it: a device CDF that
