@@ -11,7 +11,8 @@ launch of the kernel it captures.  The states are sized past the 126 MB L2
 
 Cases and the kernels they run:
   pauli        k_pauli, k_pauli_finalize          (kt_sv_expect, 32 strings)
-  sample       k_probs_tiles, k_tile_*, k_exact_chain, k_last_below_sorted, k_seq_*  (kt_sv_sample, exact tier)
+  sample       k_probs_tiles, k_tile_*, k_exact_chain, k_bound_tile, k_sparse_bound, k_shot_*
+               (kt_sv_sample, exact tier, on a dense state)
   sample_fast  k_probs, k_chunk_sums, k_chunk_offsets, k_sample_bound, k_sample_fast  (2^22 amplitudes)
   dm_pauli     k_dm_pauli, k_dm_pauli_finalize    (kt_dm_expect on a 13-qubit density matrix)
   hpsi         k_hsum                              (lambda = H psi and the energy, in the adjoint forward)
@@ -63,7 +64,11 @@ def case_pauli(n, reps):
 
 
 def case_sample(n, reps):
-    sv = _random_state(n, 3)
+    # eight mixed layers: a dense, Porter-Thomas-like distribution, as the
+    # benchmark circuit's final state is
+    sv = capi.Statevector(n)
+    sv.set_basis(0)
+    sv.apply(W.random_layers(n, 8, seed=3, mixed=True))
     can = capi.canonicals_mt19937(4, 4096)
     for _ in range(1 + reps):
         sv.sample(can)
