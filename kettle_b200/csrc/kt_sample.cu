@@ -414,7 +414,11 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
             X.viol = XS_TILE;
         }
         __syncthreads();
-        atomicMin(&X.viol, bad);
+        // one shared atomic per warp, not per thread: same-address atomics serialise
+        bad = __reduce_min_sync(0xffffffffU, bad);
+        if ((t & 31) == 0) {
+            atomicMin(&X.viol, bad);
+        }
         __syncthreads();
         const uint64_t tile_len = (end - i) < XS_TILE ? (end - i) : XS_TILE;
         const unsigned int v = X.viol < tile_len ? X.viol : static_cast<unsigned int>(tile_len);
@@ -761,8 +765,9 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const P p, uint64_t 
         if (ok && normal && m + excl + I >= TWO53) {
             ok = false;
         }
-        if (!ok) {
-            atomicMin(&first_sh, static_cast<unsigned int>(t));
+        const unsigned int wmin = __reduce_min_sync(0xffffffffU, ok ? 0xffffffffU : static_cast<unsigned int>(t));
+        if ((t & 31) == 0 && wmin != 0xffffffffU) {
+            atomicMin(&first_sh, wmin);
         }
         __syncthreads();
         const unsigned int first = first_sh;
