@@ -593,73 +593,93 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
 
 // 1b. one block: approximate start value of every tile, and its binade guess
 // (with cints: a tile guessed in a candidate binade takes that binade's
-// integer sum, or goes dirty when the probability pass flagged it there)
+// integer sum, or goes dirty when the probability pass flagged it there).
+// The tile sums pass through shared memory GUESS_PER x XS_THREADS at a time:
+// loaded coalesced, each thread then scans GUESS_PER consecutive ones.
+constexpr int GUESS_PER = 4;
+constexpr int GUESS_CHUNK = GUESS_PER * XS_THREADS;
+
 __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restrict__ tsum, uint64_t n_tiles,
                                                            int* __restrict__ code,
                                                            const unsigned long long* __restrict__ cints,
                                                            const int* __restrict__ cflag,
                                                            unsigned long long* __restrict__ ints)
 {
+    __shared__ double st[GUESS_CHUNK];
     __shared__ double sh[32];
     const int t = threadIdx.x;
-    const uint64_t per = (n_tiles + XS_THREADS - 1) / XS_THREADS;
-    const uint64_t b = static_cast<uint64_t>(t) * per;
-    const uint64_t e = b + per < n_tiles ? b + per : n_tiles;
-    double local = 0.0;
-    for (uint64_t k = b; k < e; ++k) {
-        local += tsum[k];
-    }
-    // exclusive block scan of the thread sums (FP64, approximate)
     const int lane = t & 31, warp = t >> 5;
-    double x = local;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const double y = __shfl_up_sync(0xffffffffU, x, o);
-        if (lane >= o) {
-            x += y;
+    double carry = 0.0;  // approximate sum of the chunks before this one (the same in every thread)
+    for (uint64_t c0 = 0; c0 < n_tiles; c0 += GUESS_CHUNK) {
+        for (int j = t; j < GUESS_CHUNK; j += XS_THREADS) {
+            const uint64_t k = c0 + static_cast<uint64_t>(j);
+            st[j] = k < n_tiles ? tsum[k] : 0.0;
         }
-    }
-    if (lane == 31) {
-        sh[warp] = x;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        double w = sh[lane];
+        __syncthreads();
+        double loc[GUESS_PER];
+        double local = 0.0;
+#pragma unroll
+        for (int i = 0; i < GUESS_PER; ++i) {
+            loc[i] = st[t * GUESS_PER + i];
+            local += loc[i];
+        }
+        // exclusive block scan of the thread sums (FP64, approximate)
+        double x = local;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const double y = __shfl_up_sync(0xffffffffU, w, o);
+            const double y = __shfl_up_sync(0xffffffffU, x, o);
             if (lane >= o) {
-                w += y;
+                x += y;
             }
         }
-        sh[lane] = w;
-    }
-    __syncthreads();
-    double a0 = ((warp > 0) ? sh[warp - 1] : 0.0) + (x - local);
-    for (uint64_t k = b; k < e; ++k) {
-        const double ts = tsum[k];
-        const double a1 = a0 + ts;
-        int c = TILE_DIRTY;
-        if (ts == 0.0) {
-            c = TILE_ZERO;
-        } else if (a0 >= 2.0 * TINY) {
-            int e0, e1;
-            frexp(a0 * (1.0 - 0x1p-20), &e0);
-            frexp(a1 * (1.0 + 0x1p-20), &e1);
-            if (e0 == e1) {
-                c = e0;
-            }
+        if (lane == 31) {
+            sh[warp] = x;
         }
-        if (cints != nullptr && c <= 0 && c > -N_CAND) {
-            const int j = -c;
-            if ((cflag[k] >> j) & 1) {
-                c = TILE_DIRTY;
-            } else {
-                ints[k] = cints[k * N_CAND + static_cast<uint64_t>(j)];
+        __syncthreads();
+        if (warp == 0) {
+            double w = sh[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double y = __shfl_up_sync(0xffffffffU, w, o);
+                if (lane >= o) {
+                    w += y;
+                }
             }
+            sh[lane] = w;
         }
-        code[k] = c;
-        a0 = a1;
+        __syncthreads();
+        double a0 = carry + ((warp > 0) ? sh[warp - 1] : 0.0) + (x - local);
+#pragma unroll
+        for (int i = 0; i < GUESS_PER; ++i) {
+            const uint64_t k = c0 + static_cast<uint64_t>(t * GUESS_PER + i);
+            const double ts = loc[i];
+            const double a1 = a0 + ts;
+            if (k < n_tiles) {
+                int c = TILE_DIRTY;
+                if (ts == 0.0) {
+                    c = TILE_ZERO;
+                } else if (a0 >= 2.0 * TINY) {
+                    int e0, e1;
+                    frexp(a0 * (1.0 - 0x1p-20), &e0);
+                    frexp(a1 * (1.0 + 0x1p-20), &e1);
+                    if (e0 == e1) {
+                        c = e0;
+                    }
+                }
+                if (cints != nullptr && c <= 0 && c > -N_CAND) {
+                    const int j = -c;
+                    if ((cflag[k] >> j) & 1) {
+                        c = TILE_DIRTY;
+                    } else {
+                        ints[k] = cints[k * N_CAND + static_cast<uint64_t>(j)];
+                    }
+                }
+                code[k] = c;
+            }
+            a0 = a1;
+        }
+        carry += sh[31];
+        __syncthreads();  // st and sh are reused by the next chunk
     }
 }
 
