@@ -244,18 +244,21 @@ __global__ void k_sample_fast(const double* __restrict__ p, const double* __rest
 // exact tier -------------------------------------------------------------------
 // The sequential sum s_i = fl(s_{i-1} + p_i) of std::partial_sum, computed
 // exactly.  While s stays in one binade [2^(E-1), 2^E) every representable
-// value is a multiple of u = 2^(E-53), so (no tie, no binade exit)
-// fl(s + p) = s + rint(p / u) * u exactly: a run of additions is an integer
-// prefix sum.  The array is cut into tiles of XS_TILE elements:
+// value is a multiple of u = 2^(E-53), so (no binade exit)
+// fl(s + p) = s + rint(p / u) * u exactly away from ties, and an exact tie
+// (p / u = n + 1/2) rounds s / u + n to even: a run of additions is an
+// integer prefix sum, or a composition of run maps (RunMap below) where it
+// holds ties.  The array is cut into tiles of XS_TILE elements:
 //  1. tile sums (FP64, any order) and their exclusive scan give each tile an
 //     approximate start value, hence a guess of its binade (or "all zero");
-//  2. every tile with a guess sums rint(p / u) in uint64, flagging exact ties
-//     (.5) and huge terms (>= 2^50 units);
+//  2. every tile with a guess sums rint(p / u) in uint64, flagging huge terms
+//     (>= 2^50 units) and listing the tiles with exact ties, whose run maps
+//     are composed in element order (k_tile_runs);
 //  3. one block walks the tiles in order with the exact running value s: a
-//     tile whose guess is s's binade, has no flag and does not reach 2^53
-//     units is passed over in O(1) (its start value is recorded); any other
-//     tile is computed element by element from the exact s (the same integer
-//     scan, with one IEEE add for each tie, huge term or binade exit);
+//     tile whose guess is s's binade, has no huge term and does not reach
+//     2^53 units is passed over in O(1) (its start value is recorded); any
+//     other tile is computed element by element from the exact s (the same
+//     run-map scan, with one IEEE add for each huge term or binade exit);
 //  4. every recorded tile writes its CDF from its exact start value: all of
 //     them for a caller's probability vector; for the state's own
 //     probabilities only the tiles that the bound and the shots land in,
@@ -333,10 +336,97 @@ struct ProbAmps
 // tiles are read a second time by k_tile_ints.
 constexpr int N_CAND = 4;
 
+// A run of additions inside one binade, as a function of the running value v
+// in that binade's units: v -> v + S, or, once the run holds an exact tie,
+// v -> v + S + ((v + c) & 1).  A tie element p = (n + 1/2) u gives
+// fl(v u + p) = (v + n + ((v + n) & 1)) u (round half to even), so after it
+// the parity of the running value no longer depends on v, and runs compose
+// in order in the same form.  c: bit 0 the parity offset, bit 1 "has a tie".
+struct RunMap
+{
+    unsigned long long S;
+    int c;
+};
+
+__device__ __forceinline__ unsigned long long run_apply(const RunMap& a, unsigned long long v)
+{
+    return v + a.S + ((a.c & 2) ? ((v + static_cast<unsigned long long>(a.c)) & 1ULL) : 0ULL);
+}
+
+// run a, then run b
+__device__ __forceinline__ RunMap run_then(const RunMap& a, const RunMap& b)
+{
+    if (a.c & 2) {
+        const unsigned long long pa = (a.S + static_cast<unsigned long long>(a.c)) & 1ULL;  // parity after a
+        const unsigned long long inc = b.S + ((b.c & 2) ? ((pa + static_cast<unsigned long long>(b.c)) & 1ULL) : 0ULL);
+        return RunMap {a.S + inc, a.c};
+    }
+    if (b.c & 2) {
+        return RunMap {a.S + b.S, static_cast<int>((a.S + static_cast<unsigned long long>(b.c)) & 1ULL) | 2};
+    }
+    return RunMap {a.S + b.S, 0};
+}
+
+// one element's run, q = p / u (the caller has excluded huge terms)
+__device__ __forceinline__ RunMap run_of(double q)
+{
+    const double f = floor(q);
+    if ((q - f) == 0.5) {
+        const unsigned long long n = static_cast<unsigned long long>(f);
+        return RunMap {n, static_cast<int>(n & 1ULL) | 2};
+    }
+    return RunMap {static_cast<unsigned long long>(rint(q)), 0};
+}
+
+__device__ __forceinline__ RunMap shfl_up_run(const RunMap& a, int o)
+{
+    return RunMap {__shfl_up_sync(0xffffffffU, a.S, o), __shfl_up_sync(0xffffffffU, a.c, o)};
+}
+
+// inclusive scan of the lanes' runs in lane order
+__device__ __forceinline__ RunMap warp_scan_runs(RunMap x)
+{
+    const int lane = static_cast<int>(threadIdx.x & 31);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const RunMap y = shfl_up_run(x, o);
+        if (lane >= o) {
+            x = run_then(y, x);
+        }
+    }
+    return x;
+}
+
+// exclusive scan of the threads' runs in thread order (XS_THREADS threads);
+// sh holds 32 runs
+__device__ __forceinline__ RunMap block_excl_scan_runs(const RunMap v, RunMap* sh)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const RunMap x = warp_scan_runs(v);
+    if (lane == 31) {
+        sh[warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const RunMap w = warp_scan_runs(sh[lane]);
+        __syncwarp();
+        sh[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    RunMap in_warp = shfl_up_run(x, 1);
+    if (lane == 0) {
+        in_warp = RunMap {0, 0};
+    }
+    const RunMap r = (warp > 0) ? run_then(sh[warp - 1], in_warp) : in_warp;
+    __syncthreads();
+    return r;
+}
+
 // shared state of the element-by-element path
 struct XState
 {
-    unsigned long long sh[32];
+    RunMap shr[32];
     double s;
     unsigned long long i;
     unsigned int viol;
@@ -378,33 +468,39 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
         const double inv_u = ldexp(1.0, 53 - E);  // 1 / ulp(s)
         const double u = ldexp(1.0, E - 53);
         const unsigned long long m = static_cast<unsigned long long>(s * inv_u);  // exact, in [2^52, 2^53)
-        unsigned long long r[XS_EPT];
-        unsigned int bad = XS_TILE;  // first flagged local index
-        unsigned long long run = 0;
         const uint64_t b0 = i + static_cast<uint64_t>(t) * XS_EPT;
-#pragma unroll
-        for (int k = 0; k < XS_EPT; ++k) {
-            const uint64_t g = b0 + k;
-            double q = 0.0;
-            if (g < end) {
-                q = p[g] * inv_u;
+        // this thread's element k as a run (ties included); a huge term ends
+        // the integer path and counts as nothing here.  The probabilities are
+        // read again at each use rather than held (64 registers per thread)
+        auto elem = [&](int k, bool& big) -> RunMap {
+            const uint64_t g = b0 + static_cast<uint64_t>(k);
+            big = false;
+            if (g >= end) {
+                return RunMap {0ULL, 0};
             }
-            const double f = floor(q);
-            const bool tie = (q - f) == 0.5;
-            const bool big = !(q < 1125899906842624.0);  // 2^50 (also catches inf)
-            if ((tie || big) && g < end && bad == XS_TILE) {
+            const double q = p[g] * inv_u;
+            if (!(q < 1125899906842624.0)) {  // 2^50 (also catches inf)
+                big = true;
+                return RunMap {0ULL, 0};
+            }
+            return run_of(q);
+        };
+        unsigned int bad = XS_TILE;  // first huge term or binade exit (local index)
+        RunMap tm {0ULL, 0};
+        for (int k = 0; k < XS_EPT; ++k) {
+            bool big;
+            const RunMap e = elem(k, big);
+            if (big && bad == XS_TILE) {
                 bad = t * XS_EPT + k;
             }
-            r[k] = big ? 0ULL : static_cast<unsigned long long>(rint(q));
-            run += r[k];
+            tm = run_then(tm, e);
         }
-        unsigned long long total;
-        const unsigned long long excl = block_excl_scan_u64(run, X.sh, total);
-        // binade exit: first element whose running sum reaches 2^53 units
-        unsigned long long acc = m + excl;
-#pragma unroll
+        const RunMap ex = block_excl_scan_runs(tm, X.shr);
+        // binade exit: first element whose running value reaches 2^53 units
+        unsigned long long acc = run_apply(ex, m);
         for (int k = 0; k < XS_EPT; ++k) {
-            acc += r[k];
+            bool big;
+            acc = run_apply(elem(k, big), acc);
             const unsigned int li = t * XS_EPT + k;
             if (acc >= TWO53 && li < bad) {
                 bad = li;
@@ -423,13 +519,17 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
         const uint64_t tile_len = (end - i) < XS_TILE ? (end - i) : XS_TILE;
         const unsigned int v = X.viol < tile_len ? X.viol : static_cast<unsigned int>(tile_len);
         // commit the elements before v
-        acc = m + excl;
-#pragma unroll
+        acc = run_apply(ex, m);
         for (int k = 0; k < XS_EPT; ++k) {
-            acc += r[k];
+            bool big;
+            acc = run_apply(elem(k, big), acc);
             const unsigned int li = t * XS_EPT + k;
             if (li < v) {
                 cdf[i + li] = static_cast<double>(acc) * u;
+                if (v == tile_len && li + 1 == tile_len) {
+                    X.s = static_cast<double>(acc) * u;  // every element of the window went in
+                    X.i = i + tile_len;
+                }
             }
         }
         if (v < tile_len) {
@@ -444,10 +544,11 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
             } else {
                 const unsigned int owner = (v - 1) / XS_EPT;
                 if (static_cast<unsigned int>(t) == owner) {
-                    unsigned long long a2 = m + excl;
+                    unsigned long long a2 = run_apply(ex, m);
                     for (int k = 0; k < XS_EPT; ++k) {
                         if (t * XS_EPT + k < v) {
-                            a2 += r[k];
+                            bool big;
+                            a2 = run_apply(elem(k, big), a2);
                         }
                     }
                     const double before = static_cast<double>(a2) * u;
@@ -457,9 +558,6 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
                     X.i = i + v + 1;
                 }
             }
-        } else if (t == 0) {
-            X.s = static_cast<double>(m + total) * u;
-            X.i = i + tile_len;
         }
         __syncthreads();
     }
@@ -492,8 +590,9 @@ __global__ void __launch_bounds__(256) k_tile_sums(const double* __restrict__ p,
 
 // 0 + 1 + 2 fused, for the state's own probabilities without readout noise:
 // each tile's FP64 sum of |a_i|^2 (any order, as above) and its integer sums
-// in the N_CAND candidate binades with their tie / huge-term flags (bit k of
-// cflag), as k_tile_ints forms them; the probabilities are not stored
+// in the N_CAND candidate binades with their flags, as k_tile_ints forms them
+// (cflag bit k: a tie in candidate k, bit 8 + k: a huge term); the
+// probabilities are not stored
 template <typename C>
 __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, uint64_t N, double* __restrict__ tsum,
                                                      unsigned long long* __restrict__ cints, int* __restrict__ cflag)
@@ -529,7 +628,7 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
 #pragma unroll
             for (int k = 0; k < N_CAND; ++k) {
                 if (!(x0 < static_cast<double>(1ULL << (50 - k)))) {
-                    fl |= 1 << k;
+                    fl |= 1 << (8 + k);
                 }
             }
         }
@@ -550,8 +649,8 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
     unsigned long long ci[N_CAND];
 #pragma unroll
     for (int k = 0; k < N_CAND; ++k) {
-        // can wrap only when candidate k is flagged (a term of 2^50 units or
-        // more), and a flagged candidate's sum is never used
+        // can wrap only when candidate k has a term of 2^50 units or more, and
+        // such a candidate's sum is never used
         ci[k] = (sfl << k) + small[k];
     }
     acc = warp_sum_d(acc);
@@ -593,7 +692,8 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
 
 // 1b. one block: approximate start value of every tile, and its binade guess
 // (with cints: a tile guessed in a candidate binade takes that binade's
-// integer sum, or goes dirty when the probability pass flagged it there).
+// integer sum; a huge term there makes it dirty, a tie lists it in tie_list
+// for k_tile_runs).
 // The tile sums pass through shared memory GUESS_PER x XS_THREADS at a time:
 // loaded coalesced, each thread then scans GUESS_PER consecutive ones.
 constexpr int GUESS_PER = 4;
@@ -603,7 +703,9 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restr
                                                            int* __restrict__ code,
                                                            const unsigned long long* __restrict__ cints,
                                                            const int* __restrict__ cflag,
-                                                           unsigned long long* __restrict__ ints)
+                                                           unsigned long long* __restrict__ ints,
+                                                           int* __restrict__ tie, unsigned long long* __restrict__ tie_list,
+                                                           unsigned int* __restrict__ tie_count)
 {
     __shared__ double st[GUESS_CHUNK];
     __shared__ double sh[32];
@@ -666,15 +768,21 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restr
                         c = e0;
                     }
                 }
+                int has_tie = 0;
                 if (cints != nullptr && c <= 0 && c > -N_CAND) {
                     const int j = -c;
-                    if ((cflag[k] >> j) & 1) {
+                    const int f = cflag[k];
+                    if ((f >> (8 + j)) & 1) {
                         c = TILE_DIRTY;
+                    } else if ((f >> j) & 1) {
+                        has_tie = 1;
+                        tie_list[atomicAdd(tie_count, 1U)] = k;
                     } else {
                         ints[k] = cints[k * N_CAND + static_cast<uint64_t>(j)];
                     }
                 }
                 code[k] = c;
+                tie[k] = has_tie;
             }
             a0 = a1;
         }
@@ -683,11 +791,14 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restr
     }
 }
 
-// 2. integer sum of a tile in the units of its guessed binade; flags demote it
-// (with_cand: tiles guessed in a candidate binade have theirs already)
+// 2. integer sum of a tile in the units of its guessed binade; a huge term
+// makes it dirty, an exact tie lists it for k_tile_runs (with_cand: tiles
+// guessed in a candidate binade have theirs already)
 template <typename P>
 __global__ void __launch_bounds__(256) k_tile_ints(const P p, uint64_t N, int* __restrict__ code,
-                                                   unsigned long long* __restrict__ ints, int with_cand)
+                                                   unsigned long long* __restrict__ ints, int with_cand,
+                                                   int* __restrict__ tie, unsigned long long* __restrict__ tie_list,
+                                                   unsigned int* __restrict__ tie_count)
 {
     __shared__ unsigned long long sh[8];
     __shared__ int flag_sh;
@@ -703,19 +814,24 @@ __global__ void __launch_bounds__(256) k_tile_ints(const P p, uint64_t N, int* _
     const uint64_t beg = static_cast<uint64_t>(blockIdx.x) * XS_TILE;
     const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
     unsigned long long acc = 0;
-    bool flag = false;
+    int fl = 0;  // bit 0: an exact tie, bit 1: a huge term (2^50 units and more, or inf / NaN)
     for (uint64_t i = beg + threadIdx.x; i < end; i += 256) {
         const double q = p[i] * inv_u;
         const double f = floor(q);
-        flag = flag || ((q - f) == 0.5) || !(q < 1125899906842624.0);
-        acc += flag ? 0ULL : static_cast<unsigned long long>(rint(q));
+        if ((q - f) == 0.5) {
+            fl |= 1;
+        }
+        if (!(q < 1125899906842624.0)) {
+            fl |= 2;
+        }
+        acc += (fl & 2) ? 0ULL : static_cast<unsigned long long>(rint(q));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         acc += __shfl_down_sync(0xffffffffU, acc, o);
     }
-    if (flag) {
-        flag_sh = 1;
+    if (fl != 0) {
+        atomicOr(&flag_sh, fl);
     }
     if ((threadIdx.x & 31) == 0) {
         sh[threadIdx.x >> 5] = acc;
@@ -727,9 +843,66 @@ __global__ void __launch_bounds__(256) k_tile_ints(const P p, uint64_t N, int* _
             s += sh[w];
         }
         ints[blockIdx.x] = s;
-        if (flag_sh) {
+        if (flag_sh & 2) {
             code[blockIdx.x] = TILE_DIRTY;
+        } else if (flag_sh & 1) {
+            tie[blockIdx.x] = 1;
+            tie_list[atomicAdd(tie_count, 1U)] = blockIdx.x;
         }
+    }
+}
+
+// 2b. the run map (RunMap) of every listed tile with a tie, in the units of
+// its guessed binade: each thread composes XS_EPT consecutive elements in
+// order, then the block composes the threads' runs in order
+template <typename P>
+__global__ void __launch_bounds__(XS_THREADS) k_tile_runs(const P p, uint64_t N, int* __restrict__ code,
+                                                          const unsigned long long* __restrict__ tie_list,
+                                                          const unsigned int* __restrict__ tie_count,
+                                                          unsigned long long* __restrict__ run_s,
+                                                          int* __restrict__ run_c)
+{
+    __shared__ RunMap sh[32];
+    __shared__ int big_sh;
+    const int t = threadIdx.x;
+    const unsigned int count = *tie_count;
+    for (unsigned int li = blockIdx.x; li < count; li += gridDim.x) {
+        const uint64_t tile = tie_list[li];
+        const int c = code[tile];
+        if (t == 0) {
+            big_sh = 0;
+        }
+        __syncthreads();
+        const double inv_u = ldexp(1.0, 53 - c);
+        const uint64_t beg = tile * XS_TILE;
+        const uint64_t end = beg + XS_TILE < N ? beg + XS_TILE : N;
+        RunMap r {0, 0};
+        bool big = false;
+        const uint64_t b0 = beg + static_cast<uint64_t>(t) * XS_EPT;
+#pragma unroll
+        for (int k = 0; k < XS_EPT; ++k) {
+            const uint64_t g = b0 + k;
+            if (g < end) {
+                const double q = p[g] * inv_u;
+                big = big || !(q < 1125899906842624.0);
+                r = run_then(r, run_of(big ? 0.0 : q));
+            }
+        }
+        if (big) {
+            big_sh = 1;
+        }
+        // the block's composition in thread order: an exclusive scan, then
+        // the last thread's run appended
+        const RunMap before = block_excl_scan_runs(r, sh);
+        if (t == XS_THREADS - 1) {
+            const RunMap all = run_then(before, r);
+            run_s[tile] = all.S;
+            run_c[tile] = all.c;
+            if (big_sh) {
+                code[tile] = TILE_DIRTY;  // not reached: the tile was flagged for its ties only
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -741,6 +914,9 @@ template <typename P>
 __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const P p, uint64_t N, uint64_t n_tiles,
                                                             const int* __restrict__ code,
                                                             const unsigned long long* __restrict__ ints,
+                                                            const int* __restrict__ tie,
+                                                            const unsigned long long* __restrict__ run_s,
+                                                            const int* __restrict__ run_c,
                                                             double* __restrict__ carry, double* __restrict__ tstart,
                                                             double* __restrict__ cdf)
 {
@@ -778,11 +954,16 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const P p, uint64_t 
         }
         const uint64_t tile = t0 + static_cast<uint64_t>(t);
         const int c = tile < n_tiles ? code[tile] : TILE_DIRTY;
-        const unsigned long long I = (tile < n_tiles && c != TILE_ZERO && c != TILE_DIRTY) ? ints[tile] : 0ULL;
-        unsigned long long total;
-        const unsigned long long excl = block_excl_scan_u64(I, X.sh, total);
+        // the tile's additions as a run: its integer sum, or its run map when it holds a tie
+        RunMap R {0ULL, 0};
+        if (tile < n_tiles && c != TILE_ZERO && c != TILE_DIRTY) {
+            R = tie[tile] ? RunMap {run_s[tile], run_c[tile]} : RunMap {ints[tile], 0};
+        }
+        const RunMap ex = block_excl_scan_runs(R, X.shr);
+        const unsigned long long mt = run_apply(ex, m);  // the exact value before the tile, in units
+        const unsigned long long me = run_apply(R, mt);  // and after it
         bool ok = tile < n_tiles && (c == TILE_ZERO || (normal && c == E));
-        if (ok && normal && m + excl + I >= TWO53) {
+        if (ok && normal && me >= TWO53) {
             ok = false;
         }
         const unsigned int wmin = __reduce_min_sync(0xffffffffU, ok ? 0xffffffffU : static_cast<unsigned int>(t));
@@ -792,11 +973,11 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const P p, uint64_t 
         __syncthreads();
         const unsigned int first = first_sh;
         if (static_cast<unsigned int>(t) < first) {
-            const double c0 = normal ? static_cast<double>(m + excl) * u : s;
+            const double c0 = normal ? static_cast<double>(mt) * u : s;
             carry[tile] = c0;
             tstart[tile] = c0;
             if (static_cast<unsigned int>(t) + 1 == first) {
-                m_sh = m + excl + I;
+                m_sh = me;
             }
         }
         __syncthreads();
@@ -841,7 +1022,8 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const P p, uint64_t N
                                                            const int* __restrict__ code,
                                                            const double* __restrict__ carry, double* __restrict__ cdf,
                                                            const unsigned long long* __restrict__ list,
-                                                           const unsigned int* __restrict__ count)
+                                                           const unsigned int* __restrict__ count,
+                                                           const int* __restrict__ tie)
 {
     // warp w holds the tile's elements [w * 32 * XS_EPT, (w + 1) * 32 * XS_EPT)
     // as XS_EPT rows of 32 consecutive elements, one per lane, so every load
@@ -849,6 +1031,7 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const P p, uint64_t N
     // runs row by row (a warp scan per row, the warp's earlier rows carried)
     // after a block scan of the warp totals, in element order
     __shared__ unsigned long long sh[32];
+    __shared__ RunMap shr[32];
     uint64_t tile = blockIdx.x;
     if (list != nullptr) {
         if (blockIdx.x >= *count) {
@@ -877,6 +1060,41 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_write(const P p, uint64_t N
     const double inv_u = ldexp(1.0, 53 - c);
     const double u = ldexp(1.0, c - 53);
     const unsigned long long m = static_cast<unsigned long long>(c0 * inv_u);
+    if (tie[tile]) {
+        // the same rows, composed as run maps (a tie's rounding depends on the
+        // parity of the value before it): each warp's run over its rows, a block
+        // scan of those in warp order, then every row's lane scan from the
+        // exact value before it
+        // (the probabilities are read twice rather than held: this path is
+        // rare, and 1024 threads have 64 registers each)
+        const int warp = static_cast<int>(threadIdx.x >> 5);
+        RunMap w {0ULL, 0};
+        for (int k = 0; k < XS_EPT; ++k) {
+            const uint64_t g = wb + static_cast<uint64_t>(k) * 32;
+            const RunMap row = warp_scan_runs((g < end) ? run_of(p[g] * inv_u) : RunMap {0ULL, 0});
+            w = run_then(w, RunMap {__shfl_sync(0xffffffffU, row.S, 31), __shfl_sync(0xffffffffU, row.c, 31)});
+        }
+        if (lane == 0) {
+            shr[warp] = w;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const RunMap x = warp_scan_runs(shr[lane]);
+            __syncwarp();
+            shr[lane] = x;  // inclusive over warps
+        }
+        __syncthreads();
+        unsigned long long acc = (warp > 0) ? run_apply(shr[warp - 1], m) : m;
+        for (int k = 0; k < XS_EPT; ++k) {
+            const uint64_t g = wb + static_cast<uint64_t>(k) * 32;
+            const RunMap x = warp_scan_runs((g < end) ? run_of(p[g] * inv_u) : RunMap {0ULL, 0});
+            if (g < end) {
+                cdf[g] = static_cast<double>(run_apply(x, acc)) * u;
+            }
+            acc = run_apply(RunMap {__shfl_sync(0xffffffffU, x.S, 31), __shfl_sync(0xffffffffU, x.c, 31)}, acc);
+        }
+        return;
+    }
     unsigned long long r[XS_EPT];
     unsigned long long run = 0;
 #pragma unroll
@@ -1096,6 +1314,11 @@ struct ExactBufs
     unsigned long long* list;
     unsigned int* count;
     unsigned long long* stile;
+    int* tie;
+    unsigned long long* run_s;
+    int* run_c;
+    unsigned long long* tie_list;
+    unsigned int* tie_count;
     unsigned long long* nz;
     double* bound;
     const double* canon;
@@ -1109,15 +1332,20 @@ template <typename P>
 int32_t exact_tail(cudaStream_t st, const P p, const ExactBufs& b, bool with_cand, bool sorted)
 {
     const uint64_t N = b.N, n_tiles = b.n_tiles;
-    k_tile_ints<P><<<static_cast<unsigned>(n_tiles), 256, 0, st>>>(p, N, b.code, b.ints, with_cand ? 1 : 0);
+    k_tile_ints<P><<<static_cast<unsigned>(n_tiles), 256, 0, st>>>(p, N, b.code, b.ints, with_cand ? 1 : 0, b.tie,
+                                                                     b.tie_list, b.tie_count);
     KT_CHECK_LAUNCH("k_tile_ints");
-    k_exact_chain<P><<<1, XS_THREADS, 0, st>>>(p, N, n_tiles, b.code, b.ints, b.carry, b.tstart, b.cdf);
+    k_tile_runs<P><<<static_cast<unsigned>(sm_count()), XS_THREADS, 0, st>>>(p, N, b.code, b.tie_list, b.tie_count,
+                                                                             b.run_s, b.run_c);
+    KT_CHECK_LAUNCH("k_tile_runs");
+    k_exact_chain<P><<<1, XS_THREADS, 0, st>>>(p, N, n_tiles, b.code, b.ints, b.tie, b.run_s, b.run_c, b.carry,
+                                               b.tstart, b.cdf);
     KT_CHECK_LAUNCH("k_exact_chain");
     const unsigned shot_blocks = static_cast<unsigned>((b.n_shots + 127) / 128);
     if (sorted) {
         k_bound_tile<<<1, 32, 0, st>>>(b.tstart, n_tiles, b.list, b.count);
         KT_CHECK_LAUNCH("k_bound_tile");
-        k_tile_write<P><<<1, XS_THREADS, 0, st>>>(p, N, b.code, b.carry, b.cdf, b.list, b.count);
+        k_tile_write<P><<<1, XS_THREADS, 0, st>>>(p, N, b.code, b.carry, b.cdf, b.list, b.count, b.tie);
         KT_CHECK_LAUNCH("k_tile_write");
         k_sparse_bound<<<1, 32, 0, st>>>(b.cdf, N, b.tstart, n_tiles, b.list, b.bound);
         KT_CHECK_LAUNCH("k_sparse_bound");
@@ -1127,7 +1355,7 @@ int32_t exact_tail(cudaStream_t st, const P p, const ExactBufs& b, bool with_can
                                                   b.count);
         KT_CHECK_LAUNCH("k_shot_tiles");
         const unsigned n_write = static_cast<unsigned>(std::min<uint64_t>(static_cast<uint64_t>(b.n_shots), n_tiles));
-        k_tile_write<P><<<n_write, XS_THREADS, 0, st>>>(p, N, b.code, b.carry, b.cdf, b.list, b.count);
+        k_tile_write<P><<<n_write, XS_THREADS, 0, st>>>(p, N, b.code, b.carry, b.cdf, b.list, b.count, b.tie);
         KT_CHECK_LAUNCH("k_tile_write");
         k_shot_search<<<shot_blocks, 128, 0, st>>>(b.cdf, N, n_tiles, b.bound, b.canon, b.n_shots, b.stile, b.out);
         KT_CHECK_LAUNCH("k_shot_search");
@@ -1136,7 +1364,7 @@ int32_t exact_tail(cudaStream_t st, const P p, const ExactBufs& b, bool with_can
     // a caller's vector may hold negative entries: the whole CDF, and the
     // reference's scan for the end offset
     k_tile_write<P><<<static_cast<unsigned>(n_tiles), XS_THREADS, 0, st>>>(p, N, b.code, b.carry, b.cdf, nullptr,
-                                                                           nullptr);
+                                                                           nullptr, b.tie);
     KT_CHECK_LAUNCH("k_tile_write");
     KT_CUDA(cudaMemsetAsync(b.nz, 0, 8, st));
     const unsigned lb_blocks = static_cast<unsigned>(std::min<uint64_t>((N + 255) / 256, sm_count() * 8ULL));
@@ -1187,7 +1415,12 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     const size_t off_stile = al(off_count + 8);
     const size_t off_cints = al(off_stile + ns * 8);
     const size_t off_cflag = al(off_cints + n_xt * N_CAND * 8);
-    if (const int32_t rc = s.scratch.reserve(off_cflag + n_xt * 4); rc != KT_OK) {
+    const size_t off_tie = al(off_cflag + n_xt * 4);
+    const size_t off_runs = al(off_tie + n_xt * 4);
+    const size_t off_runc = al(off_runs + n_xt * 8);
+    const size_t off_tlist = al(off_runc + n_xt * 4);
+    const size_t off_tcount = al(off_tlist + n_xt * 8);
+    if (const int32_t rc = s.scratch.reserve(off_tcount + 8); rc != KT_OK) {
         return rc;
     }
     double* dp = static_cast<double*>(s.scratch2.ptr);
@@ -1212,6 +1445,11 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
     auto* d_stile = reinterpret_cast<unsigned long long*>(base + off_stile);
     auto* d_cints = reinterpret_cast<unsigned long long*>(base + off_cints);
     auto* d_cflag = reinterpret_cast<int*>(base + off_cflag);
+    auto* d_tie = reinterpret_cast<int*>(base + off_tie);
+    auto* d_runs = reinterpret_cast<unsigned long long*>(base + off_runs);
+    auto* d_runc = reinterpret_cast<int*>(base + off_runc);
+    auto* d_tlist = reinterpret_cast<unsigned long long*>(base + off_tlist);
+    auto* d_tcount = reinterpret_cast<unsigned int*>(base + off_tcount);
 
     // the exact tier straight away (above the fast tier's size) on the state's
     // own noiseless probabilities: their pass forms the tile sums and the
@@ -1267,11 +1505,13 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
             k_tile_sums<<<static_cast<unsigned>(n_tiles), 256, 0, s.stream>>>(dp, N, d_tsum);
             KT_CHECK_LAUNCH("k_tile_sums");
         }
+        KT_CUDA(cudaMemsetAsync(d_tcount, 0, 4, s.stream));
         k_tile_guess<<<1, XS_THREADS, 0, s.stream>>>(d_tsum, n_tiles, d_code, fused_tiles ? d_cints : nullptr, d_cflag,
-                                                     d_ints);
+                                                     d_ints, d_tie, d_tlist, d_tcount);
         KT_CHECK_LAUNCH("k_tile_guess");
-        const ExactBufs xb {N,     n_tiles, n_shots, d_code,  d_ints, d_carry, d_tstart, dcdf,
-                            d_hit, d_list,  d_count, d_stile, d_nz,   d_bound, d_canon,  d_out};
+        const ExactBufs xb {N,      n_tiles, n_shots, d_code,  d_ints,  d_carry, d_tstart, dcdf,   d_hit,
+                            d_list, d_count, d_stile, d_tie,   d_runs,  d_runc,  d_tlist,  d_tcount, d_nz,
+                            d_bound, d_canon, d_out};
         int32_t rc = KT_OK;
         if (!fused_tiles) {
             rc = exact_tail(s.stream, ProbVec {dp}, xb, false, host_probs == nullptr);
