@@ -426,6 +426,7 @@ __device__ __forceinline__ RunMap block_excl_scan_runs(const RunMap v, RunMap* s
 // shared state of the element-by-element path
 struct XState
 {
+    unsigned long long sh[32];
     RunMap shr[32];
     double s;
     unsigned long long i;
@@ -470,8 +471,9 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
         const unsigned long long m = static_cast<unsigned long long>(s * inv_u);  // exact, in [2^52, 2^53)
         const uint64_t b0 = i + static_cast<uint64_t>(t) * XS_EPT;
         // this thread's element k as a run (ties included); a huge term ends
-        // the integer path and counts as nothing here.  The probabilities are
-        // read again at each use rather than held (64 registers per thread)
+        // the integer path and counts as nothing here.  Only a window that
+        // holds a tie takes this form: its probabilities are read again at
+        // each use rather than held (64 registers per thread)
         auto elem = [&](int k, bool& big) -> RunMap {
             const uint64_t g = b0 + static_cast<uint64_t>(k);
             big = false;
@@ -485,22 +487,55 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
             }
             return run_of(q);
         };
+        unsigned long long r[XS_EPT];
         unsigned int bad = XS_TILE;  // first huge term or binade exit (local index)
-        RunMap tm {0ULL, 0};
+        unsigned long long run = 0;
+        int has_tie = 0;
+#pragma unroll
         for (int k = 0; k < XS_EPT; ++k) {
-            bool big;
-            const RunMap e = elem(k, big);
-            if (big && bad == XS_TILE) {
+            const uint64_t g = b0 + k;
+            double q = 0.0;
+            if (g < end) {
+                q = p[g] * inv_u;
+            }
+            const double f = floor(q);
+            const bool big = !(q < 1125899906842624.0);  // 2^50 (also catches inf)
+            if (big && g < end && bad == XS_TILE) {
                 bad = t * XS_EPT + k;
             }
-            tm = run_then(tm, e);
+            if ((q - f) == 0.5 && g < end) {
+                has_tie = 1;
+            }
+            r[k] = big ? 0ULL : static_cast<unsigned long long>(rint(q));
+            run += r[k];
         }
-        const RunMap ex = block_excl_scan_runs(tm, X.shr);
-        // binade exit: first element whose running value reaches 2^53 units
-        unsigned long long acc = run_apply(ex, m);
-        for (int k = 0; k < XS_EPT; ++k) {
+        const bool ties = __syncthreads_or(has_tie) != 0;
+        // the exact value before this thread's first element, in units
+        unsigned long long start;
+        if (!ties) {
+            unsigned long long total;
+            start = m + block_excl_scan_u64(run, X.sh, total);
+        } else {
+            RunMap tm {0ULL, 0};
+            for (int k = 0; k < XS_EPT; ++k) {
+                bool big;
+                tm = run_then(tm, elem(k, big));
+            }
+            start = run_apply(block_excl_scan_runs(tm, X.shr), m);
+        }
+        // the value after element k, from the value before it
+        auto step = [&](int k, unsigned long long a) -> unsigned long long {
+            if (!ties) {
+                return a + r[k];
+            }
             bool big;
-            acc = run_apply(elem(k, big), acc);
+            return run_apply(elem(k, big), a);
+        };
+        // binade exit: first element whose running value reaches 2^53 units
+        unsigned long long acc = start;
+#pragma unroll
+        for (int k = 0; k < XS_EPT; ++k) {
+            acc = step(k, acc);
             const unsigned int li = t * XS_EPT + k;
             if (acc >= TWO53 && li < bad) {
                 bad = li;
@@ -519,10 +554,10 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
         const uint64_t tile_len = (end - i) < XS_TILE ? (end - i) : XS_TILE;
         const unsigned int v = X.viol < tile_len ? X.viol : static_cast<unsigned int>(tile_len);
         // commit the elements before v
-        acc = run_apply(ex, m);
+        acc = start;
+#pragma unroll
         for (int k = 0; k < XS_EPT; ++k) {
-            bool big;
-            acc = run_apply(elem(k, big), acc);
+            acc = step(k, acc);
             const unsigned int li = t * XS_EPT + k;
             if (li < v) {
                 cdf[i + li] = static_cast<double>(acc) * u;
@@ -544,11 +579,10 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
             } else {
                 const unsigned int owner = (v - 1) / XS_EPT;
                 if (static_cast<unsigned int>(t) == owner) {
-                    unsigned long long a2 = run_apply(ex, m);
+                    unsigned long long a2 = start;
                     for (int k = 0; k < XS_EPT; ++k) {
                         if (t * XS_EPT + k < v) {
-                            bool big;
-                            a2 = run_apply(elem(k, big), a2);
+                            a2 = step(k, a2);
                         }
                     }
                     const double before = static_cast<double>(a2) * u;
@@ -954,14 +988,21 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const P p, uint64_t 
         }
         const uint64_t tile = t0 + static_cast<uint64_t>(t);
         const int c = tile < n_tiles ? code[tile] : TILE_DIRTY;
-        // the tile's additions as a run: its integer sum, or its run map when it holds a tie
-        RunMap R {0ULL, 0};
-        if (tile < n_tiles && c != TILE_ZERO && c != TILE_DIRTY) {
-            R = tie[tile] ? RunMap {run_s[tile], run_c[tile]} : RunMap {ints[tile], 0};
+        // the tile's additions as a run: its integer sum, or its run map when
+        // it holds a tie (the plain integer scan when no tile of the step does)
+        const bool live = tile < n_tiles && c != TILE_ZERO && c != TILE_DIRTY;
+        const bool tile_tie = live && tie[tile] != 0;
+        unsigned long long mt, me;  // the exact value before and after the tile, in units
+        if (__syncthreads_or(tile_tie) == 0) {
+            const unsigned long long I = live ? ints[tile] : 0ULL;
+            unsigned long long total;
+            mt = m + block_excl_scan_u64(I, X.sh, total);
+            me = mt + I;
+        } else {
+            const RunMap R = tile_tie ? RunMap {run_s[tile], run_c[tile]} : RunMap {live ? ints[tile] : 0ULL, 0};
+            mt = run_apply(block_excl_scan_runs(R, X.shr), m);
+            me = run_apply(R, mt);
         }
-        const RunMap ex = block_excl_scan_runs(R, X.shr);
-        const unsigned long long mt = run_apply(ex, m);  // the exact value before the tile, in units
-        const unsigned long long me = run_apply(R, mt);  // and after it
         bool ok = tile < n_tiles && (c == TILE_ZERO || (normal && c == E));
         if (ok && normal && me >= TWO53) {
             ok = false;
