@@ -333,8 +333,18 @@ struct ProbAmps
 // Tile integer sums for these binades are formed during the probability pass
 // (candidate k: the binade [2^(-k-1), 2^-k), units 2^(-k-53)): a normalised
 // state's running sum starts most tiles in [1/16, 1), so only the other
-// tiles are read a second time by k_tile_ints.
+// tiles are read a second time by k_tile_ints.  Four candidates for
+// complex128 amplitudes, whose pass is bound by DRAM with the arithmetic
+// hidden; two for complex64, whose 8-byte amplitudes leave less time per
+// element (tiles in [1/4, 1): the second read covers about a fifth of them).
+// N_CAND is the layout stride of the candidate sums.
 constexpr int N_CAND = 4;
+
+template <typename C>
+constexpr int cand_count()
+{
+    return sizeof(C) == 16 ? 4 : 2;
+}
 
 // A run of additions inside one binade, as a function of the running value v
 // in that binade's units: v -> v + S, or, once the run holds an exact tie,
@@ -624,15 +634,16 @@ __global__ void __launch_bounds__(256) k_tile_sums(const double* __restrict__ p,
 
 // 0 + 1 + 2 fused, for the state's own probabilities without readout noise:
 // each tile's FP64 sum of |a_i|^2 (any order, as above) and its integer sums
-// in the N_CAND candidate binades with their flags, as k_tile_ints forms them
+// in the cand_count<C>() candidate binades with their flags, as k_tile_ints forms them
 // (cflag bit k: a tie in candidate k, bit 8 + k: a huge term); the
 // probabilities are not stored
 template <typename C>
 __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, uint64_t N, double* __restrict__ tsum,
                                                      unsigned long long* __restrict__ cints, int* __restrict__ cflag)
 {
+    constexpr int NC = cand_count<C>();
     __shared__ double sh[8];
-    __shared__ unsigned long long shi[N_CAND][8];
+    __shared__ unsigned long long shi[NC][8];
     __shared__ int flag_sh;
     if (threadIdx.x == 0) {
         flag_sh = 0;
@@ -647,9 +658,9 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
     // (T + 2^(3-k)) >> (4-k); x_k is a tie when 2^(k+1) F is an odd integer,
     // i.e. 16 F is an integer with T's low 4-k bits equal to 2^(3-k).
     unsigned long long sfl = 0;  // sum of fl
-    unsigned int small[N_CAND];
+    unsigned int small[NC];
 #pragma unroll
-    for (int k = 0; k < N_CAND; ++k) {
+    for (int k = 0; k < NC; ++k) {
         small[k] = 0;
     }
     int fl = 0;
@@ -660,7 +671,7 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
         if (!(x0 < 0x1p47)) {
             // 2^50 units and more in some candidate binade (or inf / NaN)
 #pragma unroll
-            for (int k = 0; k < N_CAND; ++k) {
+            for (int k = 0; k < NC; ++k) {
                 if (!(x0 < static_cast<double>(1ULL << (50 - k)))) {
                     fl |= 1 << (8 + k);
                 }
@@ -673,23 +684,23 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
         const bool whole = (y == ty);
         sfl += static_cast<unsigned long long>(f0);
 #pragma unroll
-        for (int k = 0; k < N_CAND; ++k) {
+        for (int k = 0; k < NC; ++k) {
             small[k] += (T + (8u >> k)) >> (4 - k);
             if (whole && (T & ((16u >> k) - 1u)) == (8u >> k)) {
                 fl |= 1 << k;
             }
         }
     }
-    unsigned long long ci[N_CAND];
+    unsigned long long ci[NC];
 #pragma unroll
-    for (int k = 0; k < N_CAND; ++k) {
+    for (int k = 0; k < NC; ++k) {
         // can wrap only when candidate k has a term of 2^50 units or more, and
         // such a candidate's sum is never used
         ci[k] = (sfl << k) + small[k];
     }
     acc = warp_sum_d(acc);
 #pragma unroll
-    for (int k = 0; k < N_CAND; ++k) {
+    for (int k = 0; k < NC; ++k) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             ci[k] += __shfl_down_sync(0xffffffffU, ci[k], o);
@@ -702,7 +713,7 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
     if ((threadIdx.x & 31) == 0) {
         sh[threadIdx.x >> 5] = acc;
 #pragma unroll
-        for (int k = 0; k < N_CAND; ++k) {
+        for (int k = 0; k < NC; ++k) {
             shi[k][threadIdx.x >> 5] = ci[k];
         }
     }
@@ -713,7 +724,7 @@ __global__ void __launch_bounds__(256) k_probs_tiles(const C* __restrict__ a, ui
             t += sh[w];
         }
         tsum[blockIdx.x] = t;
-        for (int k = 0; k < N_CAND; ++k) {
+        for (int k = 0; k < NC; ++k) {
             unsigned long long v = 0;
             for (int w = 0; w < 8; ++w) {
                 v += shi[k][w];
@@ -739,7 +750,7 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restr
                                                            const int* __restrict__ cflag,
                                                            unsigned long long* __restrict__ ints,
                                                            int* __restrict__ tie, unsigned long long* __restrict__ tie_list,
-                                                           unsigned int* __restrict__ tie_count)
+                                                           unsigned int* __restrict__ tie_count, int n_cand)
 {
     __shared__ double st[GUESS_CHUNK];
     __shared__ double sh[32];
@@ -803,7 +814,7 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restr
                     }
                 }
                 int has_tie = 0;
-                if (cints != nullptr && c <= 0 && c > -N_CAND) {
+                if (cints != nullptr && c <= 0 && c > -n_cand) {
                     const int j = -c;
                     const int f = cflag[k];
                     if ((f >> (8 + j)) & 1) {
@@ -826,18 +837,18 @@ __global__ void __launch_bounds__(XS_THREADS) k_tile_guess(const double* __restr
 }
 
 // 2. integer sum of a tile in the units of its guessed binade; a huge term
-// makes it dirty, an exact tie lists it for k_tile_runs (with_cand: tiles
-// guessed in a candidate binade have theirs already)
+// makes it dirty, an exact tie lists it for k_tile_runs (tiles guessed in one
+// of the n_cand candidate binades have theirs already)
 template <typename P>
 __global__ void __launch_bounds__(256) k_tile_ints(const P p, uint64_t N, int* __restrict__ code,
-                                                   unsigned long long* __restrict__ ints, int with_cand,
+                                                   unsigned long long* __restrict__ ints, int n_cand,
                                                    int* __restrict__ tie, unsigned long long* __restrict__ tie_list,
                                                    unsigned int* __restrict__ tie_count)
 {
     __shared__ unsigned long long sh[8];
     __shared__ int flag_sh;
     const int c = code[blockIdx.x];
-    if (c == TILE_ZERO || c == TILE_DIRTY || (with_cand && c <= 0 && c > -N_CAND)) {
+    if (c == TILE_ZERO || c == TILE_DIRTY || (c <= 0 && c > -n_cand)) {
         return;
     }
     if (threadIdx.x == 0) {
@@ -1370,10 +1381,10 @@ struct ExactBufs
 // sorted: every probability is >= 0 (the state's own), so the CDF never
 // decreases and only the tiles the searches land in are written.
 template <typename P>
-int32_t exact_tail(cudaStream_t st, const P p, const ExactBufs& b, bool with_cand, bool sorted)
+int32_t exact_tail(cudaStream_t st, const P p, const ExactBufs& b, int n_cand, bool sorted)
 {
     const uint64_t N = b.N, n_tiles = b.n_tiles;
-    k_tile_ints<P><<<static_cast<unsigned>(n_tiles), 256, 0, st>>>(p, N, b.code, b.ints, with_cand ? 1 : 0, b.tie,
+    k_tile_ints<P><<<static_cast<unsigned>(n_tiles), 256, 0, st>>>(p, N, b.code, b.ints, n_cand, b.tie,
                                                                      b.tie_list, b.tie_count);
     KT_CHECK_LAUNCH("k_tile_ints");
     k_tile_runs<P><<<static_cast<unsigned>(sm_count()), XS_THREADS, 0, st>>>(p, N, b.code, b.tie_list, b.tie_count,
@@ -1547,19 +1558,20 @@ int32_t sample_core(State& s, uint64_t N, const double* host_probs, const double
             KT_CHECK_LAUNCH("k_tile_sums");
         }
         KT_CUDA(cudaMemsetAsync(d_tcount, 0, 4, s.stream));
+        const int n_cand = !fused_tiles ? 0 : (s.dtype == KT_C128 ? cand_count<double2>() : cand_count<float2>());
         k_tile_guess<<<1, XS_THREADS, 0, s.stream>>>(d_tsum, n_tiles, d_code, fused_tiles ? d_cints : nullptr, d_cflag,
-                                                     d_ints, d_tie, d_tlist, d_tcount);
+                                                     d_ints, d_tie, d_tlist, d_tcount, n_cand);
         KT_CHECK_LAUNCH("k_tile_guess");
         const ExactBufs xb {N,      n_tiles, n_shots, d_code,  d_ints,  d_carry, d_tstart, dcdf,   d_hit,
                             d_list, d_count, d_stile, d_tie,   d_runs,  d_runc,  d_tlist,  d_tcount, d_nz,
                             d_bound, d_canon, d_out};
         int32_t rc = KT_OK;
         if (!fused_tiles) {
-            rc = exact_tail(s.stream, ProbVec {dp}, xb, false, host_probs == nullptr);
+            rc = exact_tail(s.stream, ProbVec {dp}, xb, 0, host_probs == nullptr);
         } else if (s.dtype == KT_C128) {
-            rc = exact_tail(s.stream, ProbAmps<double2> {static_cast<const double2*>(s.amps)}, xb, true, true);
+            rc = exact_tail(s.stream, ProbAmps<double2> {static_cast<const double2*>(s.amps)}, xb, n_cand, true);
         } else {
-            rc = exact_tail(s.stream, ProbAmps<float2> {static_cast<const float2*>(s.amps)}, xb, true, true);
+            rc = exact_tail(s.stream, ProbAmps<float2> {static_cast<const float2*>(s.amps)}, xb, n_cand, true);
         }
         if (rc != KT_OK) {
             return rc;
