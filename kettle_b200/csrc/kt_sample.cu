@@ -268,6 +268,7 @@ __global__ void k_sample_fast(const double* __restrict__ p, const double* __rest
 constexpr int XS_THREADS = 1024;
 constexpr int XS_EPT = 16;
 constexpr int XS_TILE = XS_THREADS * XS_EPT;
+constexpr int XS_STAGE = XS_TILE + XS_TILE / 16;  // a staged tile, one pad double per 16 elements
 constexpr int TILE_ZERO = -100000;    // every p in the tile is +0: s passes unchanged
 constexpr int TILE_DIRTY = -200000;   // no binade guess, or a flagged term
 constexpr double TINY = 0x1p-900;     // below this the running value is summed with IEEE adds
@@ -443,13 +444,28 @@ struct XState
     unsigned int viol;
 };
 
-// cdf[beg, end) as the sequential sum continued from the exact value s_in, by
-// the whole block (XS_THREADS threads); returns the value after element end-1.
+// cdf[beg, end) (at most XS_TILE elements) as the sequential sum continued
+// from the exact value s_in, by the whole block (XS_THREADS threads); returns
+// the value after element end-1.  The probabilities are staged once in st
+// (XS_STAGE doubles of shared memory, element j at j + j / 16: a thread's
+// XS_EPT consecutive elements then fall on distinct bank pairs), so a window
+// that restarts after a binade exit re-reads shared memory, not DRAM; each
+// committed CDF value replaces its probability there (no later window reads
+// it), and the tile's CDF is stored with coalesced writes at the end.
 template <typename P>
-__device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in, double* __restrict__ cdf, XState& X)
+__device__ double exact_range(const P src, uint64_t beg, uint64_t end, double s_in, double* __restrict__ cdf, XState& X,
+                              double* __restrict__ st)
 {
     const int t = threadIdx.x;
+    const uint64_t len = end - beg;
+    auto slot = [&](uint64_t g) -> double& {
+        const uint64_t j = g - beg;
+        return st[j + (j >> 4)];
+    };
     __syncthreads();
+    for (uint64_t j = static_cast<uint64_t>(t); j < len; j += XS_THREADS) {
+        st[j + (j >> 4)] = src[beg + j];
+    }
     if (t == 0) {
         X.s = s_in;
         X.i = beg;
@@ -466,9 +482,9 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
         if (s < TINY) {
             // zero or tiny running value (subnormal spacing, huge 1/ulp): plain IEEE steps
             if (t == 0) {
-                const double nv = __dadd_rn(s, p[i]);
+                const double nv = __dadd_rn(s, slot(i));
                 X.s = nv;
-                cdf[i] = nv;
+                slot(i) = nv;
                 X.i = i + 1;
             }
             __syncthreads();
@@ -490,7 +506,7 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
             if (g >= end) {
                 return RunMap {0ULL, 0};
             }
-            const double q = p[g] * inv_u;
+            const double q = slot(g) * inv_u;
             if (!(q < 1125899906842624.0)) {  // 2^50 (also catches inf)
                 big = true;
                 return RunMap {0ULL, 0};
@@ -506,7 +522,7 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
             const uint64_t g = b0 + k;
             double q = 0.0;
             if (g < end) {
-                q = p[g] * inv_u;
+                q = slot(g) * inv_u;
             }
             const double f = floor(q);
             const bool big = !(q < 1125899906842624.0);  // 2^50 (also catches inf)
@@ -563,14 +579,19 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
         __syncthreads();
         const uint64_t tile_len = (end - i) < XS_TILE ? (end - i) : XS_TILE;
         const unsigned int v = X.viol < tile_len ? X.viol : static_cast<unsigned int>(tile_len);
-        // commit the elements before v
+        // commit the elements before v (each thread reads and then replaces
+        // only its own elements; before_v is the value just before element v)
         acc = start;
+        unsigned long long before_v = start;
 #pragma unroll
         for (int k = 0; k < XS_EPT; ++k) {
             acc = step(k, acc);
             const unsigned int li = t * XS_EPT + k;
+            if (li + 1 == v) {
+                before_v = acc;
+            }
             if (li < v) {
-                cdf[i + li] = static_cast<double>(acc) * u;
+                slot(i + li) = static_cast<double>(acc) * u;
                 if (v == tile_len && li + 1 == tile_len) {
                     X.s = static_cast<double>(acc) * u;  // every element of the window went in
                     X.i = i + tile_len;
@@ -581,29 +602,26 @@ __device__ double exact_range(const P p, uint64_t beg, uint64_t end, double s_in
             // element v gets one IEEE add onto the value just before it
             if (v == 0) {
                 if (t == 0) {
-                    const double nv = __dadd_rn(s, p[i]);
-                    cdf[i] = nv;
+                    const double nv = __dadd_rn(s, slot(i));
+                    slot(i) = nv;
                     X.s = nv;
                     X.i = i + 1;
                 }
             } else {
                 const unsigned int owner = (v - 1) / XS_EPT;
                 if (static_cast<unsigned int>(t) == owner) {
-                    unsigned long long a2 = start;
-                    for (int k = 0; k < XS_EPT; ++k) {
-                        if (t * XS_EPT + k < v) {
-                            a2 = step(k, a2);
-                        }
-                    }
-                    const double before = static_cast<double>(a2) * u;
-                    const double nv = __dadd_rn(before, p[i + v]);
-                    cdf[i + v] = nv;
+                    const double before = static_cast<double>(before_v) * u;
+                    const double nv = __dadd_rn(before, slot(i + v));
+                    slot(i + v) = nv;
                     X.s = nv;
                     X.i = i + v + 1;
                 }
             }
         }
         __syncthreads();
+    }
+    for (uint64_t j = static_cast<uint64_t>(t); j < len; j += XS_THREADS) {
+        cdf[beg + j] = st[j + (j >> 4)];
     }
     return X.s;
 }
@@ -965,6 +983,7 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const P p, uint64_t 
                                                             double* __restrict__ carry, double* __restrict__ tstart,
                                                             double* __restrict__ cdf)
 {
+    extern __shared__ double stage[];  // XS_STAGE doubles: the tile exact_range works on
     __shared__ XState X;
     __shared__ unsigned long long t_sh;
     __shared__ double s_sh;
@@ -1053,7 +1072,7 @@ __global__ void __launch_bounds__(XS_THREADS) k_exact_chain(const P p, uint64_t 
         if (t == 0) {
             tstart[bad] = s_sh;
         }
-        const double s_out = exact_range(p, beg, end, s_sh, cdf, X);
+        const double s_out = exact_range(p, beg, end, s_sh, cdf, X, stage);
         __syncthreads();
         if (t == 0) {
             carry[bad] = -1.0;
@@ -1390,8 +1409,10 @@ int32_t exact_tail(cudaStream_t st, const P p, const ExactBufs& b, int n_cand, b
     k_tile_runs<P><<<static_cast<unsigned>(sm_count()), XS_THREADS, 0, st>>>(p, N, b.code, b.tie_list, b.tie_count,
                                                                              b.run_s, b.run_c);
     KT_CHECK_LAUNCH("k_tile_runs");
-    k_exact_chain<P><<<1, XS_THREADS, 0, st>>>(p, N, n_tiles, b.code, b.ints, b.tie, b.run_s, b.run_c, b.carry,
-                                               b.tstart, b.cdf);
+    constexpr int stage_bytes = XS_STAGE * static_cast<int>(sizeof(double));
+    KT_CUDA(cudaFuncSetAttribute(k_exact_chain<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes));
+    k_exact_chain<P><<<1, XS_THREADS, stage_bytes, st>>>(p, N, n_tiles, b.code, b.ints, b.tie, b.run_s, b.run_c,
+                                                         b.carry, b.tstart, b.cdf);
     KT_CHECK_LAUNCH("k_exact_chain");
     const unsigned shot_blocks = static_cast<unsigned>((b.n_shots + 127) / 128);
     if (sorted) {
