@@ -463,8 +463,21 @@ __device__ double exact_range(const P src, uint64_t beg, uint64_t end, double s_
         return st[j + (j >> 4)];
     };
     __syncthreads();
-    for (uint64_t j = static_cast<uint64_t>(t); j < len; j += XS_THREADS) {
-        st[j + (j >> 4)] = src[beg + j];
+    {
+        // all XS_EPT loads of a thread in flight before the first store
+        double v[XS_EPT];
+#pragma unroll
+        for (int k = 0; k < XS_EPT; ++k) {
+            const uint64_t j = static_cast<uint64_t>(t) + static_cast<uint64_t>(k) * XS_THREADS;
+            v[k] = j < len ? src[beg + j] : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < XS_EPT; ++k) {
+            const uint64_t j = static_cast<uint64_t>(t) + static_cast<uint64_t>(k) * XS_THREADS;
+            if (j < len) {
+                st[j + (j >> 4)] = v[k];
+            }
+        }
     }
     if (t == 0) {
         X.s = s_in;
@@ -620,8 +633,12 @@ __device__ double exact_range(const P src, uint64_t beg, uint64_t end, double s_
         }
         __syncthreads();
     }
-    for (uint64_t j = static_cast<uint64_t>(t); j < len; j += XS_THREADS) {
-        cdf[beg + j] = st[j + (j >> 4)];
+#pragma unroll
+    for (int k = 0; k < XS_EPT; ++k) {
+        const uint64_t j = static_cast<uint64_t>(t) + static_cast<uint64_t>(k) * XS_THREADS;
+        if (j < len) {
+            cdf[beg + j] = st[j + (j >> 4)];
+        }
     }
     return X.s;
 }
