@@ -263,6 +263,14 @@ int32_t kt_plan_blocks(int32_t n_qubits, const kt_gate* gates, int64_t n_gates, 
 /* Run-time compiled block kernels so far, fused-block launches through them,
  * and 1 if run-time compilation was unavailable or failed (new). */
 int32_t kt_jit_stats(int64_t* kernels_compiled, int64_t* block_launches, int32_t* failed);
+/* Host-only: programs this process has compiled with NVRTC, and programs it
+ * took as cubins from the on-disk cache instead (new).  The cache is on when
+ * the environment variable KT_JIT_CACHE_DIR names a directory: every compiled
+ * cubin is kept there under a hash of its source, the embedded device
+ * headers, the compile options and NVRTC's version, and a later process that
+ * generates the same source loads it (a file whose second hash or content
+ * hash does not match is compiled again and replaced). */
+int32_t kt_jit_cache_stats(int64_t* nvrtc_compiles, int64_t* disk_hits);
 /* Host-only: plan an apply of n_qubits in `dtype` and compile its block kernels
  * with NVRTC without loading them (no GPU needed); n_kernels = blocks compiled.
  * With adjoint_jit = 1 it compiles instead the fused adjoint blocks of the

@@ -66,6 +66,7 @@ _SIGS = {
     "kt_tuning_set": ([C.c_char_p, I64], I32),
     "kt_tuning_get": ([C.c_char_p, C.POINTER(I64)], I32),
     "kt_jit_stats": ([P, P, P], I32),
+    "kt_jit_cache_stats": ([P, P], I32),
     "kt_sv_prepare": ([P, P, I64, P, I64], I32),
     "kt_jit_compile_only": ([I32, I32, P, I64, P, I64, P], I32),
     "kt_sv_create": ([I32, I32, C.POINTER(P)], I32),
@@ -205,6 +206,13 @@ def jit_stats() -> dict:
     k, l, f = I64(0), I64(0), I32(0)
     check(lib().kt_jit_stats(C.byref(k), C.byref(l), C.byref(f)))
     return {"kernels": int(k.value), "launches": int(l.value), "failed": bool(f.value)}
+
+
+def jit_cache_stats() -> dict:
+    """NVRTC compiles run in this process, and cubins loaded from KT_JIT_CACHE_DIR instead."""
+    c, h = I64(0), I64(0)
+    check(lib().kt_jit_cache_stats(C.byref(c), C.byref(h)))
+    return {"nvrtc_compiles": int(c.value), "disk_hits": int(h.value)}
 
 
 def jit_compile_only(n_qubits: int, gates: np.ndarray, params: np.ndarray | None = None, dtype: int = KT_C128) -> int:

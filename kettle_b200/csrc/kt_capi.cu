@@ -249,6 +249,15 @@ int32_t kt_jit_stats(int64_t* kernels_compiled, int64_t* block_launches, int32_t
     return KT_OK;
 }
 
+int32_t kt_jit_cache_stats(int64_t* nvrtc_compiles, int64_t* disk_hits)
+{
+    if (nvrtc_compiles == nullptr || disk_hits == nullptr) {
+        return invalid("null pointer");
+    }
+    kt::jit_cache_stats(nvrtc_compiles, disk_hits);
+    return KT_OK;
+}
+
 // ---- statevector --------------------------------------------------------------
 
 int32_t kt_sv_create(int32_t n_qubits, int32_t dtype, kt_sv* out)

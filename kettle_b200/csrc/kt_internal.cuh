@@ -189,6 +189,8 @@ void jit_unload_all();
 int32_t jit_prepare(State& s, const std::vector<LGate>& gates);
 // kernels compiled so far, block launches through them, and whether compiling failed
 void jit_stats(int64_t* compiled, int64_t* launches, int32_t* failed);
+// NVRTC compiles run in this process, and cubins taken from KT_JIT_CACHE_DIR instead
+void jit_cache_stats(int64_t* nvrtc_compiles, int64_t* disk_hits);
 // host-only: what the fused planner makes of a gate stream; *order (if given)
 // receives the planned gates in the order they take effect
 int32_t plan_blocks(int n, const std::vector<LGate>& gates, std::vector<double>& out);

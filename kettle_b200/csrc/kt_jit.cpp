@@ -12,9 +12,19 @@
 // The generated sources include the fused device header; its text (and that
 // of the header it includes) is embedded at build time (kt_jit_headers.inc,
 // written by kettle_b200/build.py into the build directory).
+//
+// KT_JIT_CACHE_DIR (unset: off) keeps every compiled cubin in that directory,
+// so another process that generates the same source loads it instead of
+// compiling it again.  A file is named by a 64-bit hash of everything the
+// cubin depends on (the source, the embedded headers, the compile options and
+// NVRTC's version) and carries a second, independent hash of the same and a
+// hash of its own bytes; a file that fails either check is compiled again and
+// replaced.  Files are written under a temporary name and renamed into place.
 #include <dlfcn.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -44,6 +54,7 @@ struct Nvrtc
     decltype(&nvrtcGetCUBIN) cubin {nullptr};
     decltype(&nvrtcDestroyProgram) destroy {nullptr};
     decltype(&nvrtcGetErrorString) error_string {nullptr};
+    decltype(&nvrtcVersion) version {nullptr};
     bool ok {false};
     std::string why;
 };
@@ -73,6 +84,7 @@ Nvrtc& nvrtc()
         lib.cubin = reinterpret_cast<decltype(lib.cubin)>(sym("nvrtcGetCUBIN"));
         lib.destroy = reinterpret_cast<decltype(lib.destroy)>(sym("nvrtcDestroyProgram"));
         lib.error_string = reinterpret_cast<decltype(lib.error_string)>(sym("nvrtcGetErrorString"));
+        lib.version = reinterpret_cast<decltype(lib.version)>(sym("nvrtcVersion"));
         lib.ok = lib.create && lib.compile && lib.log_size && lib.log && lib.cubin_size && lib.cubin && lib.destroy &&
                  lib.error_string;
         if (!lib.ok) {
@@ -82,9 +94,104 @@ Nvrtc& nvrtc()
     return lib;
 }
 
-// one source -> one cubin (empty on failure, with the reason in `err`); with
-// `info`, ptxas also reports each kernel's registers and spill bytes there
-std::vector<char> compile_one(const std::string& source, std::string& err, std::string* info = nullptr)
+constexpr const char* JIT_OPTS[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device", "--fmad=true",
+                                   "--extra-device-vectorization", "--ptxas-options=-v"};
+
+std::atomic<int64_t> g_nvrtc_compiles {0};
+std::atomic<int64_t> g_disk_hits {0};
+
+// FNV-1a, 64 bits, continued from h
+uint64_t fnv1a(const void* data, size_t n, uint64_t h)
+{
+    const auto* b = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < n; ++i) {
+        h = (h ^ b[i]) * 0x100000001b3ULL;
+    }
+    return h;
+}
+
+// the two cache hashes of one source: FNV-1a from two different starting
+// values over the same material (source, embedded headers, options, NVRTC
+// version)
+void cache_keys(const std::string& source, uint64_t& k1, uint64_t& k2)
+{
+    static const std::string common = [] {
+        std::string c;
+        for (int i = 0; i < KT_JIT_N_HEADERS; ++i) {
+            c += KT_JIT_HEADER_NAMES[i];
+            c += '\n';
+            c += KT_JIT_HEADER_TEXT[i];
+            c += '\0';
+        }
+        for (const char* o : JIT_OPTS) {
+            c += o;
+            c += '\0';
+        }
+        int major = 0, minor = 0;
+        if (nvrtc().version != nullptr) {
+            nvrtc().version(&major, &minor);
+        }
+        c += "nvrtc " + std::to_string(major) + "." + std::to_string(minor);
+        return c;
+    }();
+    k1 = fnv1a(source.data(), source.size(), fnv1a(common.data(), common.size(), 0xcbf29ce484222325ULL));
+    k2 = fnv1a(source.data(), source.size(), fnv1a(common.data(), common.size(), 0x84222325cbf29ce4ULL));
+}
+
+constexpr uint64_t CACHE_MAGIC = 0x3130434a54494a4bULL;  // "KJITJC01"
+
+std::string cache_path(const char* dir, uint64_t k1)
+{
+    char name[40];
+    std::snprintf(name, sizeof(name), "/kt_%016llx.cubin", static_cast<unsigned long long>(k1));
+    return std::string(dir) + name;
+}
+
+// a cached cubin, or empty
+std::vector<char> cache_load(const char* dir, uint64_t k1, uint64_t k2)
+{
+    std::vector<char> out;
+    FILE* f = std::fopen(cache_path(dir, k1).c_str(), "rb");
+    if (f == nullptr) {
+        return out;
+    }
+    uint64_t head[4] = {0, 0, 0, 0};  // magic, second key, hash of the cubin, its size
+    if (std::fread(head, sizeof(head), 1, f) == 1 && head[0] == CACHE_MAGIC && head[1] == k2 &&
+        head[3] > 0 && head[3] < (uint64_t {1} << 30)) {
+        out.resize(static_cast<size_t>(head[3]));
+        if (std::fread(out.data(), 1, out.size(), f) != out.size() ||
+            fnv1a(out.data(), out.size(), 0xcbf29ce484222325ULL) != head[2]) {
+            out.clear();
+        }
+    }
+    std::fclose(f);
+    return out;
+}
+
+void cache_store(const char* dir, uint64_t k1, uint64_t k2, const std::vector<char>& cubin)
+{
+    const std::string path = cache_path(dir, k1);
+    const std::string tmp = path + ".tmp" + std::to_string(static_cast<long long>(getpid())) + "_" +
+                            std::to_string(std::hash<std::thread::id> {}(std::this_thread::get_id()));
+    FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (f == nullptr) {
+        return;  // an unwritable cache only costs the next process a compile
+    }
+    const uint64_t head[4] = {CACHE_MAGIC, k2, fnv1a(cubin.data(), cubin.size(), 0xcbf29ce484222325ULL),
+                              static_cast<uint64_t>(cubin.size())};
+    const bool ok = std::fwrite(head, sizeof(head), 1, f) == 1 &&
+                    std::fwrite(cubin.data(), 1, cubin.size(), f) == cubin.size();
+    if (std::fclose(f) == 0 && ok) {
+        std::rename(tmp.c_str(), path.c_str());
+    } else {
+        std::remove(tmp.c_str());
+    }
+}
+
+// one source -> one cubin by NVRTC (empty on failure, with the reason in
+// `err`); with `info`, ptxas also reports each kernel's registers and spill
+// bytes there
+std::vector<char> compile_one_nvrtc(const std::string& source, std::string& err, std::string* info)
 {
     Nvrtc& L = nvrtc();
     nvrtcProgram prog = nullptr;
@@ -94,10 +201,9 @@ std::vector<char> compile_one(const std::string& source, std::string& err, std::
         err = std::string("nvrtcCreateProgram: ") + L.error_string(r);
         return {};
     }
-    const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device", "--fmad=true",
-                          "--extra-device-vectorization", "--ptxas-options=-v"};
-    const int n_opts = static_cast<int>(sizeof(opts) / sizeof(opts[0])) - (info != nullptr ? 0 : 1);
-    r = L.compile(prog, n_opts, opts);
+    g_nvrtc_compiles.fetch_add(1);
+    const int n_opts = static_cast<int>(sizeof(JIT_OPTS) / sizeof(JIT_OPTS[0])) - (info != nullptr ? 0 : 1);
+    r = L.compile(prog, n_opts, JIT_OPTS);
     if (r != NVRTC_SUCCESS) {
         size_t n = 0;
         L.log_size(prog, &n);
@@ -124,6 +230,29 @@ std::vector<char> compile_one(const std::string& source, std::string& err, std::
         L.cubin(prog, out.data());
     }
     L.destroy(&prog);
+    return out;
+}
+
+// one source -> one cubin (empty on failure, with the reason in `err`); with
+// `info`, ptxas also reports each kernel's registers and spill bytes there
+std::vector<char> compile_one(const std::string& source, std::string& err, std::string* info = nullptr)
+{
+    // KT_JIT_CACHE_DIR: a cubin compiled before from the same material
+    const char* cache_dir = std::getenv("KT_JIT_CACHE_DIR");
+    const bool cached = cache_dir != nullptr && *cache_dir != '\0' && info == nullptr;
+    uint64_t k1 = 0, k2 = 0;
+    if (cached) {
+        cache_keys(source, k1, k2);
+        std::vector<char> hit = cache_load(cache_dir, k1, k2);
+        if (!hit.empty()) {
+            g_disk_hits.fetch_add(1);
+            return hit;
+        }
+    }
+    std::vector<char> out = compile_one_nvrtc(source, err, info);
+    if (cached && !out.empty()) {
+        cache_store(cache_dir, k1, k2, out);
+    }
     return out;
 }
 
@@ -158,6 +287,12 @@ namespace
 std::mutex g_libs_mutex;
 std::vector<cudaLibrary_t> g_libs;  // every loaded program, until jit_unload_all
 }  // namespace
+
+void jit_cache_stats(int64_t* nvrtc_compiles, int64_t* disk_hits)
+{
+    *nvrtc_compiles = g_nvrtc_compiles.load();
+    *disk_hits = g_disk_hits.load();
+}
 
 void jit_unload_all()
 {
