@@ -2635,7 +2635,10 @@ int32_t jit_batch_compile_t(const std::vector<BatchPlanView>& fwd, const std::ve
         }
     }
     if (!missing.empty()) {
-        // programs of a few kernels each, compiled on parallel host threads
+        // programs of a few kernels each, compiled on parallel host threads;
+        // grouped in the order of their texts, so the same kernels always make
+        // the same programs (and hit the on-disk cubin cache in a new process)
+        std::sort(missing.begin(), missing.end(), [&](size_t x, size_t y) { return texts[x] < texts[y]; });
         const bool keep = cache.kernels.size() + missing.size() <= BATCH_CACHE_MAX;
         const size_t per_prog = 4;
         const size_t n_prog = (missing.size() + per_prog - 1) / per_prog;

@@ -13,7 +13,8 @@
 // of the header it includes) is embedded at build time (kt_jit_headers.inc,
 // written by kettle_b200/build.py into the build directory).
 //
-// KT_JIT_CACHE_DIR (unset: off) keeps every compiled cubin in that directory,
+// KT_JIT_CACHE_DIR (unset: off) keeps every compiled cubin in that directory
+// (created if missing),
 // so another process that generates the same source loads it instead of
 // compiling it again.  A file is named by a 64-bit hash of everything the
 // cubin depends on (the source, the embedded headers, the compile options and
@@ -21,6 +22,7 @@
 // hash of its own bytes; a file that fails either check is compiled again and
 // replaced.  Files are written under a temporary name and renamed into place.
 #include <dlfcn.h>
+#include <sys/stat.h>
 #include <unistd.h>
 
 #include <algorithm>
@@ -168,8 +170,20 @@ std::vector<char> cache_load(const char* dir, uint64_t k1, uint64_t k2)
     return out;
 }
 
+// the cache directory and its missing parents (mkdir -p)
+void cache_mkdir(const char* dir)
+{
+    std::string d(dir);
+    for (size_t pos = 1; pos <= d.size(); ++pos) {
+        if (pos == d.size() || d[pos] == '/') {
+            mkdir(d.substr(0, pos).c_str(), 0755);  // an existing directory is fine
+        }
+    }
+}
+
 void cache_store(const char* dir, uint64_t k1, uint64_t k2, const std::vector<char>& cubin)
 {
+    cache_mkdir(dir);
     const std::string path = cache_path(dir, k1);
     const std::string tmp = path + ".tmp" + std::to_string(static_cast<long long>(getpid())) + "_" +
                             std::to_string(std::hash<std::thread::id> {}(std::this_thread::get_id()));

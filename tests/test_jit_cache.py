@@ -6,6 +6,7 @@
 * a different circuit gets its own file;
 * a file that fails its checks (truncated, or bytes changed) is compiled
   again and replaced, and the next compile loads it;
+* a missing cache directory is created;
 * without the variable nothing is read or written."""
 from kettle_b200 import capi
 from kettle_b200 import workloads as W
@@ -52,6 +53,13 @@ def test_cubins_are_reused_checked_and_replaced(tmp_path, monkeypatch):
 
     # no temporary files are left behind
     assert all(p.suffix == ".cubin" for p in tmp_path.iterdir())
+
+
+def test_cache_directory_is_created(tmp_path, monkeypatch):
+    d = tmp_path / "a" / "b"
+    monkeypatch.setenv("KT_JIT_CACHE_DIR", str(d))
+    assert capi.jit_compile_only(14, W.random_layers(14, 2, seed=8, mixed=True)) >= 1
+    assert len(_files(d)) == 1
 
 
 def test_no_cache_without_the_variable(tmp_path, monkeypatch):
