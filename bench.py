@@ -311,13 +311,107 @@ def batch_bench_sharded(stream, count, world, rank, dist, reps=2):
     return out
 
 
-def batch_bench(stream, count=4096, reps=2, sample_every=32):
+def _batch_ref_strings(n):
+    """Pauli terms timed per qubit count: about half a second of single-core
+    reference work (a term costs a copy of the state and one sweep per
+    non-identity site, ~0.75 n + 1 sweeps of 32 B x 2^n at ~2.5 GB/s), 2..50."""
+    est = (0.75 * n + 1) * 32.0 * (1 << n) / 2.5e9
+    return int(min(50, max(2, 0.5 / est)))
+
+
+def _batch_ref_worker(samples):
+    """One spawned process of the batch CPU baseline: for each (n, layer
+    gates, params, strings, coeffs) sample, the seconds of one ansatz layer
+    through ket::simulate on a held reference Statevector and the seconds per
+    term of expectation_value on the state it leaves (the reference library
+    from oracle/_ref).  Returns {n: (layer_s, term_s)}."""
+    from oracle.oracle import ref
+    R = ref()
+    out = {}
+    for n, layer, params, strings, coeffs in samples:
+        held = R.held_state(n)
+        try:
+            t_layer = held.time(layer, params)
+        finally:
+            held.close()
+        amps = np.zeros(1 << n, dtype=np.complex128)
+        amps[0] = 1.0
+        t0 = time.perf_counter()
+        R.expect(n, amps, strings, coeffs)
+        out[n] = (t_layer, (time.perf_counter() - t0) / len(strings))
+    return out
+
+
+def batch_cpu_reference(circuits, processes=None):
+    """The reference's CPU throughput on the batch workload, with every host
+    core busy: `processes` independent processes (default: the CPUs this
+    process may run on, at most 64), started with spawn, each timing the same
+    bounded sample at once, so each one's figures carry the memory-bandwidth
+    contention of a full host.  The sample is one instance per qubit count of
+    the batch: its first ansatz layer (3 n gates: RY, RZ, CZ ring) through
+    ket::simulate and a few of its Pauli terms through expectation_value.
+    Each process's figures are scaled to every instance of the batch (its
+    layers, its 50 terms) for one energy, and x (1 + 2 P) for the energy and
+    the parameter-shift gradient (the reference has no adjoint); the host's
+    throughput is the sum of the processes' rates."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    from kettle_b200.capi import OP
+    if processes is None:
+        processes = min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count())
+    first = {}
+    for n, gates, n_params, strings, coeffs in circuits:
+        if n not in first:
+            first[n] = (gates, strings, coeffs)
+    samples = []
+    for n in sorted(first):
+        gates, strings, coeffs = first[n]
+        ops = gates["op"].astype(int)
+        # one layer: the gates up to and including the n-th CZ
+        cz = np.flatnonzero(ops == OP["CZ"])
+        end = int(cz[n - 1]) + 1 if cz.size >= n else gates.size
+        k = _batch_ref_strings(n)
+        n_par = int(gates["param"].max()) + 1
+        params = np.linspace(-1.0, 1.0, max(1, n_par))
+        samples.append((n, gates[:end], params, strings[:k], coeffs[:k]))
+    t0 = time.perf_counter()
+    with cf.ProcessPoolExecutor(max_workers=processes, mp_context=mp.get_context("spawn")) as ex:
+        per_proc = list(ex.map(_batch_ref_worker, [samples] * processes))
+    wall = time.perf_counter() - t0
+    # (qubits, layers, parameters, terms) of every instance; a layer ends its CZ ring of n gates
+    shape = [(n, max(1, round(int((gates["op"].astype(int) == OP["CZ"]).sum()) / n)), n_params, strings.size)
+             for n, gates, n_params, strings, coeffs in circuits]
+    rate_energy = rate_grad = 0.0
+    for times in per_proc:
+        t_e = t_g = 0.0
+        for n, d, n_params, n_str in shape:
+            t_layer, t_term = times[n]
+            e = d * t_layer + n_str * t_term
+            t_e += e
+            t_g += (1 + 2 * n_params) * e
+        rate_energy += len(circuits) / t_e
+        rate_grad += len(circuits) / t_g
+    qs = sorted(first)
+    return {"instances_per_s": rate_grad, "energy_only_instances_per_s": rate_energy, "unit": "instances/s",
+            "processes": processes, "cores": processes, "kind": "reference", "host": host_cpu(),
+            "wall_s": wall,
+            "sample": f"{processes} independent processes at once, each timing one instance per qubit count "
+                      f"({qs[0]}..{qs[-1]}): its first layer through ket::simulate and 2..50 of its terms through "
+                      f"expectation_value; scaled to all {len(circuits)} instances (layers, 50 terms) and x (1 + 2 P) "
+                      "for the parameter-shift gradient",
+            "seconds_per_layer_process0": {int(n): per_proc[0][n][0] for n in qs},
+            "seconds_per_term_process0": {int(n): per_proc[0][n][1] for n in qs}}
+
+
+def batch_bench(stream, count=4096, reps=2, sample_every=32, cpu_ref=False):
     """Energies and adjoint gradients of `count` hardware-efficient-ansatz
     instances (qubits uniform over 10..22, 2..10 layers, 50 random Pauli
     strings each) through one kt_batch evaluation (a CUDA graph holding the
     persistent launches), complex128 and complex64, against the same instances
     evaluated one at a time through kt_adjoint (every `sample_every`-th
-    instance timed, the time scaled to all of them)."""
+    instance timed, the time scaled to all of them) and, with `cpu_ref`,
+    against the reference on every host core (batch_cpu_reference)."""
     import torch
     from kettle_b200 import capi
     from kettle_b200 import workloads as W
@@ -404,6 +498,15 @@ def batch_bench(stream, count=4096, reps=2, sample_every=32):
     out["max_abs_dgrad_vs_one_at_a_time"] = float(dg)
     out["c64_vs_c128"] = {"max_abs_denergy": float(np.abs(e64 - e128).max()),
                           "max_abs_dgrad": float(np.abs(g64 - g128).max())}
+    if cpu_ref:
+        from oracle.oracle import ref_available
+        if ref_available():
+            try:
+                cpu = batch_cpu_reference(circuits)
+                out["cpu_reference"] = cpu
+                out["speedup_vs_cpu_reference_c128"] = out["c128"]["instances_per_s"] / cpu["instances_per_s"]
+            except Exception as exc:  # the baseline is reported, never required
+                out["cpu_reference"] = {"value": None, "error": str(exc)}
     return out
 
 
@@ -846,7 +949,7 @@ def run_engine(args):
         if world > 1:
             line["batch"] = batch_bench_sharded(stream, args.batch, world, rank, dist)
         else:
-            line["batch"] = batch_bench(stream, count=args.batch)
+            line["batch"] = batch_bench(stream, count=args.batch, cpu_ref=not args.no_cpu_baseline)
     if not args.no_configs and world == 1:
         line["configs"] = config_legs(stream, cpu=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
