@@ -319,6 +319,26 @@ def _batch_ref_strings(n):
     return int(min(50, max(2, 0.5 / est)))
 
 
+def _free_host_bytes():
+    """Host memory this process may still use: MemAvailable, lowered to the
+    cgroup's remaining allowance where one is set."""
+    free = float("inf")
+    try:
+        for line in pathlib.Path("/proc/meminfo").read_text().splitlines():
+            if line.startswith("MemAvailable:"):
+                free = int(line.split()[1]) * 1024.0
+    except (OSError, ValueError, IndexError):
+        pass
+    try:
+        cg = pathlib.Path("/sys/fs/cgroup")
+        limit = (cg / "memory.max").read_text().strip()
+        if limit != "max":
+            free = min(free, int(limit) - int((cg / "memory.current").read_text()))
+    except (OSError, ValueError):
+        pass
+    return free if free != float("inf") else 8e9
+
+
 def _batch_ref_worker(samples):
     """One spawned process of the batch CPU baseline: for each (n, layer
     gates, params, strings, coeffs) sample, the seconds of one ansatz layer
@@ -360,6 +380,9 @@ def batch_cpu_reference(circuits, processes=None):
     from kettle_b200.capi import OP
     if processes is None:
         processes = min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count())
+        # a process peaks near 0.2 GB (a 22-qubit state, its copy, the library):
+        # keep them all within half of the host memory that is free
+        processes = max(1, min(processes, int(_free_host_bytes() / 2 / 0.5e9)))
     first = {}
     for n, gates, n_params, strings, coeffs in circuits:
         if n not in first:
