@@ -29,6 +29,9 @@
 //                                        include/kettle/operator/pauli/{sparse_pauli_string,pauli_operator}.hpp
 //   ket::QuantumNoise, calculate_probabilities_raw, perform_measurements_*
 //                                        include/kettle/calculations/{probabilities,measurements}.hpp
+//   bitstring / index conversions, marginal strips, random states and unitaries, projection
+//                                        include/kettle/state/{qubit_state_conversion,marginal,random,
+//                                        project_state}.hpp, include/kettle/gates/random_u_gates.hpp
 // New (no reference counterpart): expectation_value(PauliOperator, DensityMatrix),
 // ket::adjoint_gradient, ket::DType (complex64 storage).
 #pragma once
@@ -152,6 +155,14 @@ auto rx_gate(double angle) noexcept -> Matrix2X2;
 auto ry_gate(double angle) noexcept -> Matrix2X2;
 auto rz_gate(double angle) noexcept -> Matrix2X2;
 auto p_gate(double angle) noexcept -> Matrix2X2;
+
+// Haar-random U(2) (gates/random_u_gates.hpp:18-34): four uniform [0, 1)
+// draws from the generator (three phases, then the mixing angle).  The seeded
+// form starts a fresh std::mt19937(seed); the bare form seeds from
+// std::random_device.
+auto generate_random_unitary2x2(std::mt19937& prng) -> Matrix2X2;
+auto generate_random_unitary2x2(int seed) -> Matrix2X2;
+auto generate_random_unitary2x2() -> Matrix2X2;
 
 // ---- parameters -------------------------------------------------------------------
 namespace param
@@ -547,6 +558,29 @@ auto bitstring_to_state_index(const std::string& bitstring, Endian input_endian 
 auto state_index_to_bitstring(std::size_t i_state, std::size_t n_qubits, Endian endian = Endian::LITTLE) -> std::string;
 auto endian_flip(std::size_t value, std::size_t n_relevant_bits) -> std::size_t;
 
+// state/qubit_state_conversion.hpp:14-61: a "dynamic bitset" holds one
+// std::uint8_t (0 or 1) per qubit, in the order of the bitstring's characters.
+auto state_index_to_dynamic_bitset(std::size_t i_state, std::size_t n_qubits, Endian input_endian)
+    -> std::vector<std::uint8_t>;
+auto dynamic_bitset_to_bitstring(const std::vector<std::uint8_t>& bits) -> std::string;
+auto dynamic_bitset_to_state_index(const std::vector<std::uint8_t>& dyn_bitset, Endian input_endian) -> std::size_t;
+auto bitstring_to_dynamic_bitset(const std::string& bitstring) -> std::vector<std::uint8_t>;
+auto bitstring_to_state_index_little_endian(const std::string& bitstring) -> std::size_t;
+auto bitstring_to_state_index_big_endian(const std::string& bitstring) -> std::size_t;
+auto state_index_to_bitstring_little_endian(std::size_t i_state, std::size_t n_qubits) -> std::string;
+auto state_index_to_bitstring_big_endian(std::size_t i_state, std::size_t n_qubits) -> std::string;
+auto state_index_to_dynamic_bitset_little_endian(std::size_t i_state, std::size_t n_qubits) -> std::vector<std::uint8_t>;
+auto state_index_to_dynamic_bitset_big_endian(std::size_t i_state, std::size_t n_qubits) -> std::vector<std::uint8_t>;
+auto dynamic_bitset_to_state_index_little_endian(const std::vector<std::uint8_t>& dyn_bitset) -> std::size_t;
+auto dynamic_bitset_to_state_index_big_endian(const std::vector<std::uint8_t>& dyn_bitset) -> std::size_t;
+// 0.b1 b2 b3 ... in base 2, b1 the first character (LITTLE) or the last (BIG)
+auto binary_fraction_expansion(const std::string& bitstring, Endian endian = Endian::LITTLE) -> double;
+
+// state/marginal.hpp:9-11: drop the marginal characters ('x') of a marginal
+// bitstring from its right (left) end; they must all sit at that end.
+auto rstrip_marginal_bits(const std::string& marginal_bitstring) -> std::string;
+auto lstrip_marginal_bits(const std::string& marginal_bitstring) -> std::string;
+
 class Statevector
 {
 public:
@@ -597,6 +631,22 @@ auto inner_product_norm_squared(const Statevector& left, const Statevector& righ
 auto tensor_product(const Statevector& left, const Statevector& right) -> Statevector;
 auto diagonal_expectation_value(const std::vector<std::complex<double>>& eigenvalues, const Statevector& state)
     -> std::complex<double>;
+
+// state/random.hpp:15-25: magnitudes uniform in [1e-3, 10) normalised, phases
+// uniform in [0, 2 pi), drawn in that order; the state is built on the host
+// and uploaded.  The seeded form starts a fresh std::mt19937(seed).
+auto generate_random_state(std::size_t n_qubits, std::mt19937& prng) -> Statevector;
+auto generate_random_state(std::size_t n_qubits, int seed) -> Statevector;
+auto generate_random_state(std::size_t n_qubits) -> Statevector;
+
+// state/project_state.hpp:18-23: the amplitudes whose qubits `qubit_indices`
+// hold `expected_measurements`, renormalised, as a state of the remaining
+// qubits (in their original order).  Throws when every qubit is projected,
+// an index is out of range, a value is not 0 or 1, the two lists differ in
+// length, or the remaining norm is below `minimum_norm_tol`.
+auto project_statevector(const Statevector& statevector, const std::vector<std::size_t>& qubit_indices,
+                         const std::vector<std::uint8_t>& expected_measurements,
+                         double minimum_norm_tol = PROJECTION_NORMALIZATION_TOLERANCE) -> Statevector;
 
 // Column-major N x N host matrix (element (r, c) at r + c * N), the element
 // order of the reference's Eigen::MatrixXcd.

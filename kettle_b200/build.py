@@ -117,13 +117,14 @@ def build_front_end(verbose: bool = False, force: bool = False) -> pathlib.Path:
         text = _run(cmd)
         if verbose and text.strip():
             print(text)
-    # the drop-in demonstration program against this front end
-    demo_src = ROOT / "tests" / "cpp" / "dropin_main.cpp"
-    demo = LIB / "dropin_b200"
-    if demo_src.exists() and (force or _stale(demo, [demo_src, out] + headers)):
-        cxx = shutil.which("g++") or "g++"
-        _run([cxx, "-std=c++20", "-O2", "-ffp-contract=off", f"-I{INCLUDE}", str(demo_src), f"-L{LIB}", "-lket_b200", "-lkettle_b200",
-              "-Wl,-rpath,$ORIGIN", "-o", str(demo)])
+    # the drop-in demonstration programs against this front end
+    for src_name, exe_name in (("dropin_main.cpp", "dropin_b200"), ("dropin_host_main.cpp", "dropin_host_b200")):
+        demo_src = ROOT / "tests" / "cpp" / src_name
+        demo = LIB / exe_name
+        if demo_src.exists() and (force or _stale(demo, [demo_src, out] + headers)):
+            cxx = shutil.which("g++") or "g++"
+            _run([cxx, "-std=c++20", "-O2", "-ffp-contract=off", f"-I{INCLUDE}", str(demo_src), f"-L{LIB}", "-lket_b200",
+                  "-lkettle_b200", "-Wl,-rpath,$ORIGIN", "-o", str(demo)])
     return out
 
 

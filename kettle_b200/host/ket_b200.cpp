@@ -192,6 +192,43 @@ auto rz_gate(double a) noexcept -> Matrix2X2
 }
 auto p_gate(double a) noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {std::cos(a), std::sin(a)}}; }
 
+auto generate_random_unitary2x2(std::mt19937& prng) -> Matrix2X2
+{
+    // gates/random_u_gates.cpp:13-36: U = e^{i a} [[cos p e^{i f}, sin p e^{i c}], [-sin p e^{-i c}, cos p e^{-i f}]]
+    // with a, f, c uniform in [0, 2 pi) and p = asin(sqrt(u)), u uniform in [0, 1)
+    // (Haar measure on U(2)); the products and quotients are formed in the
+    // reference's order so the matrices agree bit for bit
+    auto unit = std::uniform_real_distribution<double> {0.0, 1.0};
+    const double two_pi = 2.0 * M_PI;
+    const double a = two_pi * unit(prng);
+    const double f = two_pi * unit(prng);
+    const double c = two_pi * unit(prng);
+    const double p = std::asin(std::sqrt(unit(prng)));
+    const std::complex<double> phase {std::cos(a), std::sin(a)};
+    const std::complex<double> ef {std::cos(f), std::sin(f)};
+    const std::complex<double> ec {std::cos(c), std::sin(c)};
+    const double cp = std::cos(p);
+    const double sp = std::sin(p);
+    Matrix2X2 m;
+    m.elem00 = phase * cp * ef;
+    m.elem01 = phase * sp * ec;
+    m.elem10 = -phase * sp / ec;
+    m.elem11 = phase * cp / ef;
+    return m;
+}
+
+auto generate_random_unitary2x2(int seed) -> Matrix2X2
+{
+    auto prng = make_prng(seed);
+    return generate_random_unitary2x2(prng);
+}
+
+auto generate_random_unitary2x2() -> Matrix2X2
+{
+    auto prng = make_prng(std::nullopt);
+    return generate_random_unitary2x2(prng);
+}
+
 // ---- parameters ----------------------------------------------------------------------
 
 auto param::ParameterIdHash::operator()(const ParameterID& id) const noexcept -> std::size_t
@@ -792,7 +829,10 @@ auto endian_flip(std::size_t value, std::size_t n_relevant_bits) -> std::size_t
 
 auto bitstring_to_state_index(const std::string& bitstring, Endian input_endian) -> std::size_t
 {
-    check_bitstring(bitstring);
+    // state/qubit_state_conversion.cpp:35-53: any string of '0' / '1', the empty one included
+    if (!std::all_of(bitstring.begin(), bitstring.end(), [](char c) { return c == '0' || c == '1'; })) {
+        check_bitstring(bitstring);
+    }
     std::size_t big = 0;
     for (char c : bitstring) {
         big = (big << 1U) + (c == '1' ? 1U : 0U);
@@ -802,16 +842,150 @@ auto bitstring_to_state_index(const std::string& bitstring, Endian input_endian)
 
 auto state_index_to_bitstring(std::size_t i_state, std::size_t n_qubits, Endian endian) -> std::string
 {
-    std::string out(n_qubits, '0');
-    for (std::size_t q = 0; q < n_qubits; ++q) {
-        const char c = ((i_state >> q) & 1U) ? '1' : '0';
-        if (endian == Endian::LITTLE) {
-            out[q] = c;
-        } else {
-            out[n_qubits - q - 1] = c;
-        }
+    const auto bits = state_index_to_dynamic_bitset(i_state, n_qubits, endian);
+    return dynamic_bitset_to_bitstring(bits);
+}
+
+auto state_index_to_dynamic_bitset(std::size_t i_state, std::size_t n_qubits, Endian input_endian)
+    -> std::vector<std::uint8_t>
+{
+    // state/qubit_state_conversion.cpp:55-81: qubit q is bit q of the index
+    if (n_qubits < 64 && i_state >= (std::size_t {1} << n_qubits)) {
+        throw std::runtime_error {"The state index exceeds the number of possible states."};
+    }
+    std::vector<std::uint8_t> bits(n_qubits, 0);
+    for (std::size_t q = 0; q < n_qubits && q < 64; ++q) {
+        const auto pos = input_endian == Endian::LITTLE ? q : n_qubits - 1 - q;
+        bits[pos] = static_cast<std::uint8_t>((i_state >> q) & 1U);
+    }
+    return bits;
+}
+
+auto dynamic_bitset_to_bitstring(const std::vector<std::uint8_t>& bits) -> std::string
+{
+    std::string out;
+    out.reserve(bits.size());
+    for (auto b : bits) {
+        out.push_back(b == 0 ? '0' : '1');
     }
     return out;
+}
+
+auto dynamic_bitset_to_state_index(const std::vector<std::uint8_t>& dyn_bitset, Endian input_endian) -> std::size_t
+{
+    return bitstring_to_state_index(dynamic_bitset_to_bitstring(dyn_bitset), input_endian);
+}
+
+auto bitstring_to_dynamic_bitset(const std::string& bitstring) -> std::vector<std::uint8_t>
+{
+    if (!std::all_of(bitstring.begin(), bitstring.end(), [](char c) { return c == '0' || c == '1'; })) {
+        check_bitstring(bitstring);
+    }
+    std::vector<std::uint8_t> bits;
+    bits.reserve(bitstring.size());
+    for (char c : bitstring) {
+        bits.push_back(c == '0' ? 0 : 1);
+    }
+    return bits;
+}
+
+auto bitstring_to_state_index_little_endian(const std::string& bitstring) -> std::size_t
+{
+    return bitstring_to_state_index(bitstring, Endian::LITTLE);
+}
+
+auto bitstring_to_state_index_big_endian(const std::string& bitstring) -> std::size_t
+{
+    return bitstring_to_state_index(bitstring, Endian::BIG);
+}
+
+auto state_index_to_bitstring_little_endian(std::size_t i_state, std::size_t n_qubits) -> std::string
+{
+    return state_index_to_bitstring(i_state, n_qubits, Endian::LITTLE);
+}
+
+auto state_index_to_bitstring_big_endian(std::size_t i_state, std::size_t n_qubits) -> std::string
+{
+    return state_index_to_bitstring(i_state, n_qubits, Endian::BIG);
+}
+
+auto state_index_to_dynamic_bitset_little_endian(std::size_t i_state, std::size_t n_qubits) -> std::vector<std::uint8_t>
+{
+    return state_index_to_dynamic_bitset(i_state, n_qubits, Endian::LITTLE);
+}
+
+auto state_index_to_dynamic_bitset_big_endian(std::size_t i_state, std::size_t n_qubits) -> std::vector<std::uint8_t>
+{
+    return state_index_to_dynamic_bitset(i_state, n_qubits, Endian::BIG);
+}
+
+auto dynamic_bitset_to_state_index_little_endian(const std::vector<std::uint8_t>& dyn_bitset) -> std::size_t
+{
+    return dynamic_bitset_to_state_index(dyn_bitset, Endian::LITTLE);
+}
+
+auto dynamic_bitset_to_state_index_big_endian(const std::vector<std::uint8_t>& dyn_bitset) -> std::size_t
+{
+    return dynamic_bitset_to_state_index(dyn_bitset, Endian::BIG);
+}
+
+auto binary_fraction_expansion(const std::string& bitstring, Endian endian) -> double
+{
+    // state/qubit_state_conversion.cpp:153-182: the digit read first has weight 1/2,
+    // the next 1/4, ...; halving and adding in that order gives the same rounding
+    if (!std::all_of(bitstring.begin(), bitstring.end(), [](char c) { return c == '0' || c == '1'; })) {
+        check_bitstring(bitstring);
+    }
+    double value = 0.0;
+    double weight = 1.0;
+    const auto n = bitstring.size();
+    for (std::size_t k = 0; k < n; ++k) {
+        const char c = endian == Endian::LITTLE ? bitstring[k] : bitstring[n - 1 - k];
+        weight *= 0.5;
+        if (c == '1') {
+            value += weight;
+        }
+    }
+    return value;
+}
+
+namespace
+{
+
+// state/marginal.cpp:48-78: true when no '0' / '1' lies beyond the first
+// marginal character, reading from the kept end towards the stripped one
+bool marginals_only_at_end(const std::string& s, bool right_end)
+{
+    bool seen_marginal = false;
+    const auto n = s.size();
+    for (std::size_t k = 0; k < n; ++k) {
+        const char c = right_end ? s[k] : s[n - 1 - k];
+        if (c == 'x') {
+            seen_marginal = true;
+        } else if (seen_marginal) {
+            return false;
+        }
+    }
+    return true;
+}
+
+}  // namespace
+
+auto rstrip_marginal_bits(const std::string& marginal_bitstring) -> std::string
+{
+    if (!marginals_only_at_end(marginal_bitstring, true)) {
+        throw std::runtime_error {"The bitstring '" + marginal_bitstring + "' cannot be rstripped of its marginal bits\n"};
+    }
+    return marginal_bitstring.substr(0, std::min(marginal_bitstring.find('x'), marginal_bitstring.size()));
+}
+
+auto lstrip_marginal_bits(const std::string& marginal_bitstring) -> std::string
+{
+    if (!marginals_only_at_end(marginal_bitstring, false)) {
+        throw std::runtime_error {"The bitstring '" + marginal_bitstring + "' cannot be lstripped of its marginal bits\n"};
+    }
+    const auto first_kept = marginal_bitstring.find_first_not_of('x');
+    return first_kept == std::string::npos ? std::string {} : marginal_bitstring.substr(first_kept);
 }
 
 // ---- Statevector ------------------------------------------------------------------------------
@@ -1064,6 +1238,102 @@ auto diagonal_expectation_value(const std::vector<std::complex<double>>& eigenva
     double out[2] = {0.0, 0.0};
     check(kt_sv_diagonal_expectation(state.device(), reinterpret_cast<const double*>(eigenvalues.data()), out));
     return {out[0], out[1]};
+}
+
+auto generate_random_state(std::size_t n_qubits, std::mt19937& prng) -> Statevector
+{
+    // state/random.cpp:19-58: every magnitude first, then one phase per amplitude
+    if (n_qubits == 0) {
+        throw std::runtime_error {"Cannot generate a quantum state with 0 qubits.\n"};
+    }
+    const std::size_t n_states = std::size_t {1} << n_qubits;
+    auto draw_magnitude = std::uniform_real_distribution<double> {1.0e-3, 1.0e1};
+    auto draw_phase = std::uniform_real_distribution<double> {0.0, 2.0 * M_PI};
+    std::vector<double> mags(n_states);
+    for (auto& m : mags) {
+        m = draw_magnitude(prng);
+    }
+    double sum_sq = 0.0;  // summed in index order
+    for (double m : mags) {
+        sum_sq = sum_sq + m * m;
+    }
+    const double scale = 1.0 / std::sqrt(sum_sq);
+    std::vector<std::complex<double>> amps(n_states);
+    for (std::size_t i = 0; i < n_states; ++i) {
+        const double phase = draw_phase(prng);
+        const double r = scale * mags[i];
+        amps[i] = {r * std::cos(phase), r * std::sin(phase)};
+    }
+    return Statevector {std::move(amps)};
+}
+
+auto generate_random_state(std::size_t n_qubits, int seed) -> Statevector
+{
+    auto prng = make_prng(seed);
+    return generate_random_state(n_qubits, prng);
+}
+
+auto generate_random_state(std::size_t n_qubits) -> Statevector
+{
+    auto prng = make_prng(std::nullopt);
+    return generate_random_state(n_qubits, prng);
+}
+
+auto project_statevector(const Statevector& statevector, const std::vector<std::size_t>& qubit_indices,
+                         const std::vector<std::uint8_t>& expected_measurements, double minimum_norm_tol) -> Statevector
+{
+    // state/project_state.cpp:19-115, checks in the reference's order
+    const auto n = statevector.n_qubits();
+    if (qubit_indices.size() == n) {
+        throw std::runtime_error {"ERROR: cannot collapse all qubits, remaining state won't exist.\n"};
+    }
+    if (!qubit_indices.empty() && *std::max_element(qubit_indices.begin(), qubit_indices.end()) >= n) {
+        throw std::runtime_error {"ERROR: qubit indices exceed the number of qubits in the statevector.\n"};
+    }
+    if (!std::all_of(expected_measurements.begin(), expected_measurements.end(),
+                     [](std::uint8_t v) { return v == 0 || v == 1; })) {
+        throw std::runtime_error {"ERROR: all expected measurements must be 0 or 1.\n"};
+    }
+    if (qubit_indices.size() != expected_measurements.size()) {
+        throw std::runtime_error {"ERROR: mismatch in number of qubit indices and number of expected measurements.\n"};
+    }
+    // the projected qubits as a mask and the value they must hold
+    std::size_t mask = 0;
+    std::size_t want = 0;
+    bool contradictory = false;
+    for (std::size_t k = 0; k < qubit_indices.size(); ++k) {
+        const std::size_t bit = std::size_t {1} << qubit_indices[k];
+        const std::size_t val = expected_measurements[k] ? bit : 0;
+        if ((mask & bit) && (want & bit) != val) {
+            contradictory = true;  // one qubit asked for both 0 and 1: nothing matches
+        }
+        mask |= bit;
+        want |= val;
+    }
+    std::vector<std::complex<double>> kept;
+    if (qubit_indices.size() < n) {
+        kept.reserve(std::size_t {1} << (n - qubit_indices.size()));
+    }
+    if (!contradictory) {
+        for (std::size_t i = 0; i < statevector.n_states(); ++i) {
+            if ((i & mask) == want) {
+                kept.push_back(statevector[i]);
+            }
+        }
+    }
+    double sum_sq = 0.0;
+    for (const auto& a : kept) {
+        sum_sq += std::norm(a);
+    }
+    const double root = std::sqrt(sum_sq);
+    if (root < minimum_norm_tol) {
+        throw std::runtime_error {"The state cannot be normalized; norm of remaining amplitudes is 0.0\n"};
+    }
+    const double inv = 1.0 / root;
+    for (auto& a : kept) {
+        a *= inv;
+    }
+    return Statevector {std::move(kept)};
 }
 
 // ---- DensityMatrix ------------------------------------------------------------------------------
