@@ -141,6 +141,7 @@ auto almost_eq(const std::complex<double>& left, const std::complex<double>& rig
                double tolerance_sq = COMPLEX_ALMOST_EQ_TOLERANCE_SQ) noexcept -> bool;
 
 // gate matrices (gates/common_u_gates.cpp)
+auto i_gate() noexcept -> Matrix2X2;
 auto h_gate() noexcept -> Matrix2X2;
 auto x_gate() noexcept -> Matrix2X2;
 auto y_gate() noexcept -> Matrix2X2;
@@ -155,6 +156,10 @@ auto rx_gate(double angle) noexcept -> Matrix2X2;
 auto ry_gate(double angle) noexcept -> Matrix2X2;
 auto rz_gate(double angle) noexcept -> Matrix2X2;
 auto p_gate(double angle) noexcept -> Matrix2X2;
+// gates/common_u_gates.hpp:39-41: the matrix of a fixed gate (H .. SXDAG) or
+// an angle gate (RX, RY, RZ, P), uncontrolled or controlled; other gates throw
+auto non_angle_gate(Gate gate) -> Matrix2X2;
+auto angle_gate(Gate gate, double angle) -> Matrix2X2;
 
 // Haar-random U(2) (gates/random_u_gates.hpp:18-34): four uniform [0, 1)
 // draws from the generator (three phases, then the mixing angle).  The seeded
@@ -791,6 +796,11 @@ public:
     void overwrite(std::size_t qubit_index, PauliTerm term);
     void remove(std::size_t qubit_index);
     [[nodiscard]] auto contains_index(std::size_t qubit_index) const noexcept -> bool;
+    // operator/pauli/sparse_pauli_string.hpp:116-119: the same qubit count and the
+    // same non-identity terms on the same qubits (in any order); == also
+    // compares the phase
+    [[nodiscard]] auto equal_up_to_phase(const SparsePauliString& other) const -> bool;
+    friend auto operator==(const SparsePauliString& left, const SparsePauliString& right) -> bool;
 
     // The string as X/Z masks with its total phase (terms applied in order, as
     // simulate(SparsePauliString) applies them, simulate_pauli.cpp:58-87).

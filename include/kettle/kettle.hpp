@@ -6,3 +6,4 @@
 #include "kettle/ket_b200.hpp"
 #include "kettle/ket_b200_io.hpp"
 #include "kettle/ket_b200_circuit_ops.hpp"
+#include "kettle/ket_b200_nlocal.hpp"

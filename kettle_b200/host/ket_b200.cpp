@@ -165,6 +165,7 @@ namespace
 constexpr double SQ12 = 0.70710678118654752440;
 }
 
+auto i_gate() noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {1, 0}}; }
 auto h_gate() noexcept -> Matrix2X2 { return {{SQ12, 0}, {SQ12, 0}, {SQ12, 0}, {-SQ12, 0}}; }
 auto x_gate() noexcept -> Matrix2X2 { return {{0, 0}, {1, 0}, {1, 0}, {0, 0}}; }
 auto y_gate() noexcept -> Matrix2X2 { return {{0, 0}, {0, -1}, {0, 1}, {0, 0}}; }
@@ -191,6 +192,36 @@ auto rz_gate(double a) noexcept -> Matrix2X2
     return {{c, -s}, {0, 0}, {0, 0}, {c, s}};
 }
 auto p_gate(double a) noexcept -> Matrix2X2 { return {{1, 0}, {0, 0}, {0, 0}, {std::cos(a), std::sin(a)}}; }
+
+auto non_angle_gate(Gate gate) -> Matrix2X2
+{
+    // gates/common_u_gates.cpp:172-207: a controlled gate maps to the matrix it controls
+    switch (gate) {
+    case Gate::H: case Gate::CH: return h_gate();
+    case Gate::X: case Gate::CX: return x_gate();
+    case Gate::Y: case Gate::CY: return y_gate();
+    case Gate::Z: case Gate::CZ: return z_gate();
+    case Gate::S: case Gate::CS: return s_gate();
+    case Gate::SDAG: case Gate::CSDAG: return sdag_gate();
+    case Gate::T: case Gate::CT: return t_gate();
+    case Gate::TDAG: case Gate::CTDAG: return tdag_gate();
+    case Gate::SX: case Gate::CSX: return sx_gate();
+    case Gate::SXDAG: case Gate::CSXDAG: return sxdag_gate();
+    default: throw std::runtime_error {"UNREACHABLE: dev error, invalid non-angle gate provided\n"};
+    }
+}
+
+auto angle_gate(Gate gate, double angle) -> Matrix2X2
+{
+    // gates/common_u_gates.cpp:209-226
+    switch (gate) {
+    case Gate::RX: case Gate::CRX: return rx_gate(angle);
+    case Gate::RY: case Gate::CRY: return ry_gate(angle);
+    case Gate::RZ: case Gate::CRZ: return rz_gate(angle);
+    case Gate::P: case Gate::CP: return p_gate(angle);
+    default: throw std::runtime_error {"UNREACHABLE: dev error, invalid angle gate provided\n"};
+    }
+}
 
 auto generate_random_unitary2x2(std::mt19937& prng) -> Matrix2X2
 {
@@ -1882,6 +1913,31 @@ void SparsePauliString::remove(std::size_t qubit_index)
 auto SparsePauliString::contains_index(std::size_t qubit_index) const noexcept -> bool
 {
     return std::any_of(terms_.begin(), terms_.end(), [&](const auto& p) { return p.first == qubit_index; });
+}
+
+auto SparsePauliString::equal_up_to_phase(const SparsePauliString& other) const -> bool
+{
+    // sparse_pauli_string.cpp:165-179: identity terms do not count, and the
+    // order the terms were added in does not matter
+    if (n_qubits_ != other.n_qubits_) {
+        return false;
+    }
+    const auto canonical = [](const std::vector<std::pair<std::size_t, PauliTerm>>& terms) {
+        std::vector<std::pair<std::size_t, PauliTerm>> out;
+        for (const auto& t : terms) {
+            if (t.second != PauliTerm::I) {
+                out.push_back(t);
+            }
+        }
+        std::stable_sort(out.begin(), out.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        return out;
+    };
+    return canonical(terms_) == canonical(other.terms_);
+}
+
+auto operator==(const SparsePauliString& left, const SparsePauliString& right) -> bool
+{
+    return left.phase_ == right.phase_ && left.equal_up_to_phase(right);
 }
 
 auto SparsePauliString::to_record() const -> kt_pauli

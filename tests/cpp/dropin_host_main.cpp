@@ -5,7 +5,9 @@
 //   dropin_host <mode>
 //     host    bitstring / state-index / dynamic-bitset conversions, binary
 //             fraction expansions, marginal strips, seeded random 2x2
-//             unitaries, and the errors of each (no GPU is touched)
+//             unitaries, n-local ansatz circuits, integer ranges, gate
+//             matrices by kind, Pauli-string equality, and the errors of
+//             each (no GPU is touched)
 //     states  seeded random states and projections of them (the front end
 //             keeps states on the GPU)
 //
@@ -53,6 +55,8 @@ void show_matrix(const char* tag, int key, const ket::Matrix2X2& m)
     }
     std::printf("\n");
 }
+
+void nlocal_and_helpers();
 
 void host_mode()
 {
@@ -131,6 +135,115 @@ void host_mode()
     auto prng = std::mt19937 {20240};
     for (int k = 0; k < 8; ++k) {
         show_matrix("ustream", k, ket::generate_random_unitary2x2(prng));
+    }
+    nlocal_and_helpers();
+}
+
+template <typename Integer>
+void show_range(const char* tag, const std::vector<Integer>& v)
+{
+    std::printf("%s %zu", tag, v.size());
+    for (auto x : v) {
+        std::printf(" %lld", static_cast<long long>(x));
+    }
+    std::printf("\n");
+}
+
+void show_nlocal(int key, std::size_t n, const std::vector<ket::GeneralGate>& rot, const std::vector<ket::GeneralGate>& ent,
+                 ket::NLocalEntangelement kind, std::size_t reps, ket::SkipLastRotationLayerFlag flag)
+{
+    try {
+        auto [circuit, ids] = ket::n_local(n, rot, ent, kind, reps, flag);
+        std::printf("nlocal %d n=%zu elements=%zu params=%zu\n", key, circuit.n_qubits(), circuit.n_circuit_elements(),
+                    ids.size());
+        int k = 0;
+        for (const auto& el : circuit) {
+            const auto& gi = el.get_gate();
+            std::printf("nlgate %d %d %d %zu %zu %a\n", key, k++, static_cast<int>(gi.gate), gi.arg0, gi.arg1, gi.arg2);
+        }
+        for (std::size_t j = 0; j < ids.size(); ++j) {
+            circuit.set_parameter_value(ids[j], 0.125 * static_cast<double>(j + 1));
+        }
+        for (std::size_t j = 0; j < ids.size(); ++j) {
+            const auto& data = circuit.parameter_data_map().at(ids[j]);
+            std::printf("nlparam %d %zu %zu %a\n", key, j, data.count, data.value ? *data.value : -1.0);
+        }
+    } catch (const std::exception& e) {
+        show_error("nlocal", e);
+    }
+}
+
+void nlocal_and_helpers()
+{
+    using G = ket::Gate;
+    using CG = ket::CompoundGate;
+    using NE = ket::NLocalEntangelement;
+    using SK = ket::SkipLastRotationLayerFlag;
+    show_nlocal(0, 2, {G::RZ, G::RY}, {G::CX}, NE::LINEAR, 1, SK::FALSE);
+    show_nlocal(1, 4, {G::RY, G::H}, {G::CZ}, NE::FULL, 2, SK::FALSE);
+    show_nlocal(2, 5, {G::RX, G::CRY}, {G::CP}, NE::LINEAR, 2, SK::TRUE);
+    show_nlocal(3, 4, {CG::CCX, G::RZ}, {CG::CCZ, G::CX}, NE::FULL, 1, SK::FALSE);
+    show_nlocal(4, 6, {G::X, G::CH, CG::CCY}, {CG::CCY, G::CSX}, NE::LINEAR, 1, SK::FALSE);
+    show_nlocal(5, 3, {G::P, G::SX}, {G::CRZ}, NE::LINEAR, 3, SK::TRUE);
+    show_nlocal(6, 4, {G::RY}, {G::CRX}, NE::FULL, 1, SK::FALSE);   // the reference's FULL angle-gate loop
+    show_nlocal(7, 1, {G::RY}, {G::CRX}, NE::FULL, 1, SK::FALSE);
+    show_nlocal(8, 1, {G::RY}, {CG::CCX}, NE::LINEAR, 1, SK::FALSE);
+    show_nlocal(9, 3, {G::U}, {G::CX}, NE::LINEAR, 1, SK::FALSE);
+    show_nlocal(10, 3, {G::RY}, {G::H}, NE::LINEAR, 1, SK::FALSE);
+    show_nlocal(11, 3, {G::M}, {G::CX}, NE::LINEAR, 1, SK::FALSE);
+    show_nlocal(12, 3, {}, {}, NE::LINEAR, 2, SK::FALSE);
+
+    show_range("ar0", ket::arange(std::size_t {6}));
+    show_range("ar1", ket::arange(5));
+    show_range("ar2", ket::arange(-3));
+    show_range("ar3", ket::arange(2, 11, 3));
+    show_range("ar4", ket::arange(10, 1, -4));
+    show_range("ar5", ket::arange(std::size_t {7}, std::size_t {2}, -2));
+    show_range("ar6", ket::arange(4, 4));
+    show_range("ar7", ket::arange(1, 5, -1));
+    show_range("rv0", ket::revarange(std::size_t {5}));
+    show_range("rv1", ket::revarange(-1, 8, 3));
+    show_range("rv2", ket::revarange(9, 0, -2));
+    try {
+        (void)ket::arange(0, 5, 0);
+    } catch (const std::exception& e) {
+        show_error("arange_step", e);
+    }
+
+    show_matrix("mi", 0, ket::i_gate());
+    int k = 0;
+    for (auto g : {G::H, G::X, G::Y, G::Z, G::S, G::SDAG, G::T, G::TDAG, G::SX, G::SXDAG, G::CH, G::CX, G::CY, G::CZ,
+                   G::CS, G::CSDAG, G::CT, G::CTDAG, G::CSX, G::CSXDAG}) {
+        show_matrix("mna", k++, ket::non_angle_gate(g));
+    }
+    k = 0;
+    for (auto g : {G::RX, G::RY, G::RZ, G::P, G::CRX, G::CRY, G::CRZ, G::CP}) {
+        const double angle = 0.3 + 0.7 * k;
+        show_matrix("ma", k++, ket::angle_gate(g, angle));
+    }
+    try {
+        (void)ket::non_angle_gate(G::RX);
+    } catch (const std::exception& e) {
+        show_error("non_angle", e);
+    }
+    try {
+        (void)ket::angle_gate(G::H, 1.0);
+    } catch (const std::exception& e) {
+        show_error("angle", e);
+    }
+
+    using P = ket::PauliTerm;
+    const auto a = ket::SparsePauliString {{{0, P::X}, {2, P::Z}, {3, P::Y}}, 5};
+    const auto b = ket::SparsePauliString {{{3, P::Y}, {1, P::I}, {0, P::X}, {2, P::Z}}, 5, ket::PauliPhase::MINUS_ONE};
+    const auto c = ket::SparsePauliString {{{0, P::X}, {2, P::Z}, {3, P::Y}}, 6};
+    const auto d = ket::SparsePauliString {{{0, P::X}, {2, P::Z}, {3, P::X}}, 5};
+    const auto e = ket::SparsePauliString {{P::X, P::I, P::Z, P::Y, P::I}};
+    const ket::SparsePauliString* all[] = {&a, &b, &c, &d, &e};
+    for (int i = 0; i < 5; ++i) {
+        for (int j = 0; j < 5; ++j) {
+            std::printf("peq %d %d %d %d\n", i, j, static_cast<int>(all[i]->equal_up_to_phase(*all[j])),
+                        static_cast<int>(*all[i] == *all[j]));
+        }
     }
 }
 
