@@ -6,8 +6,11 @@
 //     host    bitstring / state-index / dynamic-bitset conversions, binary
 //             fraction expansions, marginal strips, seeded random 2x2
 //             unitaries, n-local ansatz circuits, integer ranges, gate
-//             matrices by kind, Pauli-string equality, and the errors of
-//             each (no GPU is touched)
+//             matrices by kind, Pauli-string equality, circuit adders and
+//             compound gates, transpiled circuits, classical registers and
+//             control-flow predicates, 2x2 matrix arithmetic, Pauli strings
+//             and operators, readout noise, memory-to-counts, and the errors
+//             of each (no GPU is touched)
 //     states  seeded random states and projections of them (the front end
 //             keeps states on the GPU)
 //
@@ -57,6 +60,7 @@ void show_matrix(const char* tag, int key, const ket::Matrix2X2& m)
 }
 
 void nlocal_and_helpers();
+void host_objects();
 
 void host_mode()
 {
@@ -137,6 +141,7 @@ void host_mode()
         show_matrix("ustream", k, ket::generate_random_unitary2x2(prng));
     }
     nlocal_and_helpers();
+    host_objects();
 }
 
 template <typename Integer>
@@ -244,6 +249,159 @@ void nlocal_and_helpers()
             std::printf("peq %d %d %d %d\n", i, j, static_cast<int>(all[i]->equal_up_to_phase(*all[j])),
                         static_cast<int>(*all[i] == *all[j]));
         }
+    }
+}
+
+void show_circuit(const char* tag, int key, const ket::QuantumCircuit& c)
+{
+    std::printf("%s %d n=%zu bits=%zu elements=%zu\n", tag, key, c.n_qubits(), c.n_bits(), c.n_circuit_elements());
+    int k = 0;
+    for (const auto& el : c) {
+        if (!el.is_gate()) {
+            std::printf("%s %d %d nongate\n", tag, key, k++);
+            continue;
+        }
+        const auto& gi = el.get_gate();
+        std::printf("%s %d %d %d %zu %zu %a", tag, key, k++, static_cast<int>(gi.gate), gi.arg0, gi.arg1, gi.arg2);
+        if (gi.unitary_ptr) {
+            const auto& m = *gi.unitary_ptr;
+            for (const auto& z : {m.elem00, m.elem01, m.elem10, m.elem11}) {
+                std::printf(" %a %a", z.real(), z.imag());
+            }
+        }
+        std::printf("\n");
+    }
+}
+
+#define KET_TRY(tag, expr)                  \
+    try {                                   \
+        expr;                               \
+        std::printf("noerr %s\n", tag);     \
+    } catch (const std::exception& e) {     \
+        show_error(tag, e);                 \
+    }
+
+void host_objects()
+{
+    // circuit adders: range errors, pop_back, compound gates' primitive sequences
+    auto c = ket::QuantumCircuit {3};
+    KET_TRY("x_range", c.add_x_gate(3));
+    KET_TRY("cx_target_range", c.add_cx_gate(0, 3));
+    KET_TRY("cx_control_range", c.add_cx_gate(4, 0));
+    KET_TRY("rx_range", c.add_rx_gate(5, 0.1));
+    KET_TRY("crz_range", c.add_crz_gate(1, 9, 0.1));
+    KET_TRY("m_bit_range", c.add_m_gate(0, 7));
+    KET_TRY("m_qubit_range", c.add_m_gate(3));
+    KET_TRY("u_range", c.add_u_gate(ket::h_gate(), 3));
+    KET_TRY("ccx_range", c.add_ccx_gate(0, 1, 3));
+    KET_TRY("swap_range", c.add_swap_gate(0, 3));
+    {
+        auto e = ket::QuantumCircuit {2};
+        KET_TRY("pop_empty", e.pop_back());
+    }
+    auto cc = ket::QuantumCircuit {5};
+    cc.add_ccx_gate(0, 1, 2);
+    cc.add_ccy_gate(4, 2, 0);
+    cc.add_ccz_gate(1, 3, 4);
+    cc.add_ccu_gate(ket::generate_random_unitary2x2(5), 2, 0, 4);
+    cc.add_swap_gate(1, 3);
+    cc.add_cswap_gate(0, 2, 4);
+    cc.add_qft_gate({0, 1, 2, 3});
+    cc.add_iqft_gate({4, 2, 1});
+    cc.add_u_gate(ket::generate_random_unitary2x2(6), 1);
+    cc.add_cu_gate(ket::generate_random_unitary2x2(7), 3, 2);
+    show_circuit("ccirc", 0, cc);
+    show_circuit("ctrans", 0, ket::transpile_to_primitive(cc));
+    auto joined = ket::append_circuits(cc, cc);
+    std::printf("joined %zu\n", joined.n_circuit_elements());
+    cc.pop_back();
+    std::printf("popped %zu\n", cc.n_circuit_elements());
+
+    // classical register and control-flow predicates
+    auto reg = ket::ClassicalRegister {3};
+    reg.set(1, 1);
+    reg.set(2, 0);
+    std::printf("creg %d %d %d %d\n", static_cast<int>(reg.is_measured(0)), static_cast<int>(reg.is_measured(1)),
+                reg.get(1), reg.get(2));
+    KET_TRY("creg_get_unmeasured", (void)reg.get(0));
+    // (no out-of-range register indices: the reference does not check them)
+    KET_TRY("creg_set_value", reg.set(0, 2));
+    using K = ket::ControlFlowBooleanKind;
+    KET_TRY("pred_sizes", ket::ControlFlowPredicate({0, 1}, {1}, K::IF));
+    KET_TRY("pred_bits", ket::ControlFlowPredicate({0}, {2}, K::IF));
+    KET_TRY("pred_empty", ket::ControlFlowPredicate({}, {}, K::IF));
+    {
+        const auto p_if = ket::ControlFlowPredicate({1, 2}, {1, 0}, K::IF);
+        const auto p_not = ket::ControlFlowPredicate({1, 2}, {1, 0}, K::IF_NOT);
+        const auto p_other = ket::ControlFlowPredicate({1}, {0}, K::IF);
+        std::printf("pred %d %d %d\n", static_cast<int>(p_if(reg)), static_cast<int>(p_not(reg)),
+                    static_cast<int>(p_other(reg)));
+        const auto p_unmeasured = ket::ControlFlowPredicate({0}, {1}, K::IF);
+        KET_TRY("pred_unmeasured", (void)p_unmeasured(reg));
+    }
+
+    // 2x2 matrices
+    int key = 0;
+    for (int seed : {21, 22, 23}) {
+        const auto u = ket::generate_random_unitary2x2(seed);
+        const auto v = ket::generate_random_unitary2x2(seed + 100);
+        show_matrix("mprod", key, u * v);
+        show_matrix("msum", key, u + v);
+        show_matrix("mscale", key, u * std::complex<double> {0.5, -1.25});
+        show_matrix("mscale2", key, std::complex<double> {-2.0, 0.75} * v);
+        show_matrix("mdag", key, ket::conjugate_transpose(u));
+        show_matrix("msqrt", key, ket::matrix_square_root(u));
+        const auto det = ket::determinant(u);
+        const auto tr = ket::trace(u);
+        std::printf("mdet %d %a %a %a %a %d %d\n", key, det.real(), det.imag(), tr.real(), tr.imag(),
+                    static_cast<int>(ket::almost_eq(u, u)), static_cast<int>(ket::almost_eq(u, v)));
+        auto w = u;
+        w *= v;
+        w += u;
+        w *= 2.0;
+        show_matrix("minplace", key, w);
+        ++key;
+    }
+    for (const auto& g : {ket::x_gate(), ket::h_gate(), ket::z_gate(), ket::sx_gate(), ket::t_gate()}) {
+        show_matrix("msqrt_fixed", key++, ket::matrix_square_root(g));
+    }
+
+    // Pauli strings and operators
+    using P = ket::PauliTerm;
+    auto sp = ket::SparsePauliString {4};
+    sp.add(1, P::X);
+    sp.add(3, P::Z);
+    KET_TRY("pauli_add_twice", sp.add(1, P::Y));
+    KET_TRY("pauli_add_range", sp.add(4, P::Y));
+    KET_TRY("pauli_at_missing", (void)sp.at(2));
+    sp.overwrite(1, P::Y);
+    sp.overwrite(0, P::Z);
+    sp.remove(3);
+    sp.remove(2);
+    std::printf("pstr %zu %d %d %d %d\n", sp.size(), static_cast<int>(sp.at(1)), static_cast<int>(sp.at(0)),
+                static_cast<int>(sp.contains_index(3)), static_cast<int>(sp.contains_index(0)));
+    KET_TRY("pauli_zero_qubits", ket::SparsePauliString {0});
+    auto op = ket::PauliOperator {4};
+    op.add({{0.5, -0.25}, sp});
+    KET_TRY("pauliop_qubits", op.add({{1.0, 0.0}, ket::SparsePauliString {3}}));
+    std::printf("pop %zu %zu\n", op.size(), op.n_qubits());
+
+    // readout noise
+    auto nz = ket::QuantumNoise {3};
+    nz.set(1, 0.25);
+    std::printf("noise %a %a\n", nz.get(0), nz.get(1));
+    KET_TRY("noise_value", nz.set(1, 1.5));
+    KET_TRY("noise_negative", nz.set(1, -0.1));
+    KET_TRY("noise_range", nz.set(5, 0.1));
+    KET_TRY("noise_get_range", (void)nz.get(7));
+
+    // measurement memory to counts and fractions
+    const std::vector<std::size_t> memory = {3, 1, 3, 0, 7, 3, 1, 0, 0, 3};
+    for (const auto& [k, v] : ket::memory_to_counts(memory)) {
+        std::printf("mcount %zu %zu\n", k, v);
+    }
+    for (const auto& [k, v] : ket::memory_to_fractions(memory)) {
+        std::printf("mfrac %zu %a\n", k, v);
     }
 }
 

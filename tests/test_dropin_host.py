@@ -1,7 +1,11 @@
-"""Drop-in check of kettle's host-side utilities: tests/cpp/dropin_host_main.cpp
+"""Drop-in check of kettle's host-side API: tests/cpp/dropin_host_main.cpp
 uses only the kettle C++ API (bitstring / state-index / dynamic-bitset
 conversions, binary fraction expansions, marginal strips, seeded random 2x2
-unitaries and random states, state projections).  Built against the reference
+unitaries and random states, state projections, n-local circuits, integer
+ranges, circuit adders and compound gates with their range errors,
+transpiled circuits, classical registers and control-flow predicates, 2x2
+matrix arithmetic and square roots, Pauli strings and operators, readout
+noise, memory-to-counts).  Built against the reference
 (oracle/_ref/dropin_host_ref, from the reference's own sources) and against
 this engine's ket:: front end (kettle_b200/lib/dropin_host_b200), both must
 print the same text; doubles are printed in hexadecimal, so equal text is
