@@ -11,8 +11,9 @@
 //             control-flow predicates, 2x2 matrix arithmetic, Pauli strings
 //             and operators, readout noise, memory-to-counts, and the errors
 //             of each (no GPU is touched)
-//     states  seeded random states and projections of them (the front end
-//             keeps states on the GPU)
+//     states  seeded random states and projections of them, and the io/
+//             text formats (statevector save / load, numpy text, Pauli
+//             operator text); the front end keeps states on the GPU
 //
 // Doubles are printed as hexadecimal floating point, so equal text means
 // equal bits.  Uses only the public kettle API.
@@ -21,6 +22,7 @@
 #include <cstdio>
 #include <exception>
 #include <random>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -470,6 +472,57 @@ void states_mode()
         show_error("project_norm", e);
     }
     show_state("proj_basis", 0, ket::project_statevector(zero_one, {1}, {1}));
+
+    // the text formats of io/: a random state saved in both endians (the
+    // text itself compared), loaded back, read from numpy's complex text;
+    // a Hamiltonian read from the "re im : (q, P)" text
+    const auto io_state = ket::generate_random_state(4, 31);
+    key = 0;
+    for (const auto endian : {ket::Endian::LITTLE, ket::Endian::BIG}) {
+        std::ostringstream text;
+        ket::save_statevector(text, io_state, endian);
+        std::istringstream lines {text.str()};
+        std::string line;
+        int k = 0;
+        while (std::getline(lines, line)) {
+            std::printf("svline %d %d [%s]\n", key, k++, line.c_str());
+        }
+        std::istringstream in {text.str()};
+        show_state("svload", key, ket::load_statevector(in));
+        ++key;
+    }
+    std::ostringstream np_text;
+    np_text << 3 << '\n';
+    char buf[96];
+    const auto np_src = ket::generate_random_state(3, 32);
+    for (std::size_t i = 0; i < np_src.n_states(); ++i) {
+        const auto v = np_src[i];
+        std::snprintf(buf, sizeof(buf), (i % 2 == 0) ? "(%.17g%+.17gj)\n" : "(%.8e%+.8ej)\n", v.real(), v.imag());
+        np_text << buf;
+    }
+    for (const auto endian : {ket::Endian::LITTLE, ket::Endian::BIG}) {
+        std::istringstream np_in {np_text.str()};
+        show_state("npload", static_cast<int>(endian == ket::Endian::BIG), ket::read_numpy_statevector(np_in, endian));
+    }
+    std::istringstream ham_in {
+        "0.5 -0.25 : (0, X) (2, Z)\n"
+        "-1.125 0 : (1, Y)\n"
+        "3.0e-2 1.5e-1 : (0, Z) (1, Z) (2, X)\n"
+        "0.75 0.0 :\n"};
+    try {
+        const auto ham = ket::read_pauli_operator(ham_in, 3);
+        int t = 0;
+        for (const auto& ws : ham.weighted_pauli_strings()) {
+            std::printf("ham %d %a %a %d", t++, ws.coefficient.real(), ws.coefficient.imag(),
+                        static_cast<int>(ws.pauli_string.phase()));
+            for (const auto& [q, term] : ws.pauli_string.terms()) {
+                std::printf(" %zu:%d", q, static_cast<int>(term));
+            }
+            std::printf("\n");
+        }
+    } catch (const std::exception& e) {
+        show_error("ham", e);
+    }
 }
 
 }  // namespace

@@ -5,7 +5,8 @@ unitaries and random states, state projections, n-local circuits, integer
 ranges, circuit adders and compound gates with their range errors,
 transpiled circuits, classical registers and control-flow predicates, 2x2
 matrix arithmetic and square roots, Pauli strings and operators, readout
-noise, memory-to-counts).  Built against the reference
+noise, memory-to-counts; and, holding states, random states, projections
+and the io/ text formats).  Built against the reference
 (oracle/_ref/dropin_host_ref, from the reference's own sources) and against
 this engine's ket:: front end (kettle_b200/lib/dropin_host_b200), both must
 print the same text; doubles are printed in hexadecimal, so equal text is

@@ -1,5 +1,7 @@
 """The state part of the host-utility drop-in check on a GPU: seeded random
-states and projections of them through the engine (states in GPU memory),
+states, projections of them and the io/ text formats (statevector save and
+load, numpy text, Pauli-operator text) through the engine (states in GPU
+memory),
 against the reference build of tests/cpp/dropin_host_main.cpp, text for text
 (doubles in hexadecimal: bit for bit).  The CPU suite runs the same program
 over host-memory stand-ins of the state calls (tests/test_dropin_host.py)."""
