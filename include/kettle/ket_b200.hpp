@@ -37,6 +37,7 @@
 #pragma once
 
 #include <array>
+#include <compare>
 #include <complex>
 #include <cstddef>
 #include <cstdint>
@@ -236,6 +237,8 @@ public:
     [[nodiscard]] auto bit_indices_to_check() const -> const std::vector<std::size_t>& { return bit_indices_to_check_; }
     [[nodiscard]] auto expected_bits() const -> const std::vector<int>& { return expected_bits_; }
     [[nodiscard]] auto control_kind() const -> ControlFlowBooleanKind { return control_kind_; }
+    // circuit/control_flow_predicate.hpp:47: member-wise, in declaration order
+    friend auto operator<=>(const ControlFlowPredicate& left, const ControlFlowPredicate& right) noexcept = default;
 
 private:
     std::vector<std::size_t> bit_indices_to_check_;

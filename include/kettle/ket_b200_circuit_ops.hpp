@@ -1,7 +1,7 @@
 // ket_b200_circuit_ops.hpp — circuit transforms on the host: joining circuits
 // and lowering U / CU gates to primitive gates.
 //
-// Mirrors include/kettle/circuit_operations/{append_circuits,transpile_to_primitive}.hpp
+// Mirrors include/kettle/circuit_operations/{append_circuits,transpile_to_primitive,compare_circuits}.hpp
 // of the reference: the same functions, results and error messages.  The
 // engine applies U and CU gates natively, so transpiling is never needed to
 // simulate; it is here for code that inspects or exports primitive circuits.
@@ -23,5 +23,15 @@ auto append_circuits(QuantumCircuit left, const QuantumCircuit& right) -> Quantu
 // Primitive gates, M gates, loggers and (recursively) control flow are kept.
 auto transpile_to_primitive(const QuantumCircuit& circuit, double tolerance_sq = COMPLEX_ALMOST_EQ_TOLERANCE_SQ)
     -> QuantumCircuit;
+
+// circuit_operations/compare_circuits.hpp:42-46: gate by gate, loggers
+// skipped.  Two gates match when they act on the same qubits with matrices
+// within `tol_sq` (a primitive gate and a U gate of its matrix match);
+// M gates match on qubit and bit; if / if-else statements on equal
+// predicates and (recursively) matching subcircuits.  Angles bound to
+// parameters take the circuit's parameter values (every parameter must have
+// one).
+auto almost_eq(const QuantumCircuit& left, const QuantumCircuit& right, double tol_sq = COMPLEX_ALMOST_EQ_TOLERANCE_SQ)
+    -> bool;
 
 }  // namespace ket

@@ -160,4 +160,130 @@ auto transpile_to_primitive(const QuantumCircuit& circuit, double tolerance_sq) 
     return out;
 }
 
+namespace
+{
+
+// the matrix a gate applies to its target (the controlled matrix for a
+// controlled gate), with a bound parameter's value for its angle
+auto target_matrix(const GateInfo& g, const param::ParameterDataMap& params) -> Matrix2X2
+{
+    if (g.gate == Gate::U || g.gate == Gate::CU) {
+        return *g.unitary_ptr;
+    }
+    const bool angle = (g.gate >= Gate::RX && g.gate <= Gate::P) || (g.gate >= Gate::CRX && g.gate <= Gate::CP);
+    if (!angle) {
+        return non_angle_gate(g.gate);
+    }
+    double theta = g.arg2;
+    if (g.parameter) {
+        theta = *params.at(*g.parameter).value;
+    }
+    return angle_gate(g.gate, theta);
+}
+
+auto is_controlled_gate(Gate g) -> bool
+{
+    return (g >= Gate::CH && g <= Gate::CP) || g == Gate::CU;
+}
+
+auto only_loggers_from(const QuantumCircuit& c, std::size_t i) -> bool
+{
+    for (; i < c.n_circuit_elements(); ++i) {
+        if (!c[i].is_circuit_logger()) {
+            return false;
+        }
+    }
+    return true;
+}
+
+void require_parameter_values(const param::ParameterDataMap& params)
+{
+    // parameter/parameter_expression.cpp:84-99: every parameter needs a value
+    for (const auto& [id, data] : params) {
+        if (!data.value) {
+            throw std::runtime_error {"ERROR: cannot perform simulation with an uninitialized parameter value.\n"};
+        }
+    }
+}
+
+}  // namespace
+
+auto almost_eq(const QuantumCircuit& left, const QuantumCircuit& right, double tol_sq) -> bool
+{
+    // circuit_operations/compare_circuits.cpp:128-231
+    if (left.n_qubits() != right.n_qubits() || left.n_bits() != right.n_bits()) {
+        return false;
+    }
+    require_parameter_values(left.parameter_data_map());
+    require_parameter_values(right.parameter_data_map());
+    std::size_t il = 0;
+    std::size_t ir = 0;
+    while (il < left.n_circuit_elements() && ir < right.n_circuit_elements()) {
+        const auto& a = left[il];
+        if (a.is_circuit_logger()) {
+            ++il;
+            continue;
+        }
+        const auto& b = right[ir];
+        if (b.is_circuit_logger()) {
+            ++ir;
+            continue;
+        }
+        if (a.is_control_flow() && b.is_control_flow()) {
+            const auto& ca = a.get_control_flow();
+            const auto& cb = b.get_control_flow();
+            if (ca.is_if_statement() && cb.is_if_statement()) {
+                const auto& sa = ca.get_if_statement();
+                const auto& sb = cb.get_if_statement();
+                if (sa.predicate() != sb.predicate() || !almost_eq(*sa.circuit(), *sb.circuit(), tol_sq)) {
+                    return false;
+                }
+            } else if (ca.is_if_else_statement() && cb.is_if_else_statement()) {
+                const auto& sa = ca.get_if_else_statement();
+                const auto& sb = cb.get_if_else_statement();
+                if (sa.predicate() != sb.predicate() || !almost_eq(*sa.if_circuit(), *sb.if_circuit(), tol_sq) ||
+                    !almost_eq(*sa.else_circuit(), *sb.else_circuit(), tol_sq)) {
+                    return false;
+                }
+            } else {
+                return false;
+            }
+        } else if (a.is_gate() && b.is_gate()) {
+            const auto& ga = a.get_gate();
+            const auto& gb = b.get_gate();
+            const bool ma = ga.gate == Gate::M;
+            const bool mb = gb.gate == Gate::M;
+            if (ma != mb) {
+                return false;
+            }
+            if (ma) {
+                if (ga.arg0 != gb.arg0 || ga.arg1 != gb.arg1) {
+                    return false;
+                }
+            } else {
+                // both as (controlled) U gates: same kind, same qubits, close matrices
+                if (is_controlled_gate(ga.gate) != is_controlled_gate(gb.gate) || ga.arg0 != gb.arg0 ||
+                    (is_controlled_gate(ga.gate) && ga.arg1 != gb.arg1)) {
+                    return false;
+                }
+                if (!almost_eq(target_matrix(ga, left.parameter_data_map()),
+                               target_matrix(gb, right.parameter_data_map()), tol_sq)) {
+                    return false;
+                }
+            }
+        } else {
+            return false;
+        }
+        ++il;
+        ++ir;
+    }
+    if (il == left.n_circuit_elements() && ir < right.n_circuit_elements()) {
+        return only_loggers_from(right, ir);
+    }
+    if (il < left.n_circuit_elements() && ir == right.n_circuit_elements()) {
+        return only_loggers_from(left, il);
+    }
+    return true;
+}
+
 }  // namespace ket

@@ -397,6 +397,87 @@ void host_objects()
     KET_TRY("noise_range", nz.set(5, 0.1));
     KET_TRY("noise_get_range", (void)nz.get(7));
 
+    // circuit comparison (loggers skipped, primitive gates against U gates of
+    // their matrices, bound angles, M gates, control flow) and predicate order
+    {
+        auto a = ket::QuantumCircuit {3};
+        a.add_x_gate(0);
+        a.add_rx_gate(1, 0.75);
+        a.add_cp_gate(2, 0, -1.25);
+        a.add_m_gate(1);
+        auto b = ket::QuantumCircuit {3};
+        b.add_classical_register_circuit_logger();
+        b.add_u_gate(ket::x_gate(), 0);
+        b.add_u_gate(ket::rx_gate(0.75), 1);
+        b.add_statevector_circuit_logger();
+        b.add_cu_gate(ket::p_gate(-1.25), 2, 0);
+        b.add_m_gate(1);
+        b.add_classical_register_circuit_logger();
+        auto c = ket::QuantumCircuit {3};
+        c.add_x_gate(0);
+        const auto id = c.add_rx_gate(1, 0.1, ket::param::parameterized {});
+        c.add_cp_gate(2, 0, -1.25);
+        c.add_m_gate(1);
+        auto d = a;
+        d.add_h_gate(2);
+        auto e = ket::QuantumCircuit {3};
+        e.add_rx_gate(1, 0.75);
+        e.add_x_gate(0);
+        e.add_cp_gate(2, 0, -1.25);
+        e.add_m_gate(1);
+        auto f = ket::QuantumCircuit {3};
+        f.add_x_gate(0);
+        f.add_rx_gate(1, 0.75);
+        f.add_cp_gate(0, 2, -1.25);
+        f.add_m_gate(1, 2);
+        auto g = ket::QuantumCircuit {3, 5};
+        g.add_x_gate(0);
+        KET_TRY("cmp_unset_param", (void)ket::almost_eq(a, c));
+        c.set_parameter_value(id, 0.75);
+        auto sub0 = ket::QuantumCircuit {3};
+        sub0.add_h_gate(1);
+        auto sub1 = ket::QuantumCircuit {3};
+        sub1.add_u_gate(ket::h_gate(), 1);
+        auto cf0 = a;
+        cf0.add_if_statement(1, sub0);
+        auto cf1 = a;
+        cf1.add_if_statement(1, sub1);
+        auto cf2 = a;
+        cf2.add_if_not_statement(1, sub1);
+        auto cf3 = a;
+        cf3.add_if_else_statement(1, sub0, sub1);
+        auto cf4 = a;
+        cf4.add_if_else_statement(1, sub1, sub0);
+        const ket::QuantumCircuit* all[] = {&a, &b, &c, &d, &e, &f, &g, &cf0, &cf1, &cf2, &cf3, &cf4};
+        constexpr int n_all = 12;
+        for (int i = 0; i < n_all; ++i) {
+            std::printf("ceq %d", i);
+            for (int j = 0; j < n_all; ++j) {
+                std::printf(" %d", static_cast<int>(ket::almost_eq(*all[i], *all[j])));
+            }
+            std::printf("\n");
+        }
+        auto near = ket::QuantumCircuit {1};
+        near.add_rx_gate(0, 0.5 + 1.0e-9);
+        auto far = ket::QuantumCircuit {1};
+        far.add_rx_gate(0, 0.5 + 1.0e-3);
+        auto base = ket::QuantumCircuit {1};
+        base.add_rx_gate(0, 0.5);
+        std::printf("ctol %d %d %d\n", static_cast<int>(ket::almost_eq(base, near)),
+                    static_cast<int>(ket::almost_eq(base, far)), static_cast<int>(ket::almost_eq(base, far, 1.0e-4)));
+        using K = ket::ControlFlowBooleanKind;
+        const ket::ControlFlowPredicate preds[] = {
+            ket::ControlFlowPredicate({0, 1}, {1, 0}, K::IF), ket::ControlFlowPredicate({0, 1}, {1, 0}, K::IF_NOT),
+            ket::ControlFlowPredicate({0, 2}, {1, 0}, K::IF), ket::ControlFlowPredicate({0, 1}, {0, 1}, K::IF),
+            ket::ControlFlowPredicate({0}, {1}, K::IF)};
+        for (int i = 0; i < 5; ++i) {
+            for (int j = 0; j < 5; ++j) {
+                std::printf("predcmp %d %d %d %d %d\n", i, j, static_cast<int>(preds[i] == preds[j]),
+                            static_cast<int>(preds[i] != preds[j]), static_cast<int>(preds[i] < preds[j]));
+            }
+        }
+    }
+
     // measurement memory to counts and fractions
     const std::vector<std::size_t> memory = {3, 1, 3, 0, 7, 3, 1, 0, 0, 3};
     for (const auto& [k, v] : ket::memory_to_counts(memory)) {
